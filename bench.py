@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark of the operator-method pricing path on B200.
+
+Workload (one step = one full lattice solve): the stochastic-volatility lattice with
+48 vol states x 128 log-spot states (d = 6144), dt0 = 2^-16, 14 squarings to P(0.25),
+chaining to 16 quarterly maturities, backward induction of 128 call payoffs with FP64
+discounting -> 2048 quotes.  The generator is rebuilt on the device every step.
+
+Metric: priced quotes per second, split-BF16 tensor-core path (default) at <= 1e-5
+absolute error versus an FP64 solve of the same lattice; the plain FP32 path and the
+error of both are reported in the same line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--mode bf16x3|fp32]
+
+Under torchrun every rank solves its own replica (the lattice does not shard; "replicas
+only"), timing is the max over ranks, value is the job total.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SV = dict(nx=128, nv=48, x_lo=0.05, x_hi=5.0, v_lo=0.05, v_hi=1.0, rate=0.03, kappa=2.0, theta=0.04, xi=0.6, rho=-0.7)
+PERIOD, NMAT, NK, DT0 = 0.25, 16, 128, 2.0 ** -16
+STRIKES = [0.5 + j / 127.0 for j in range(NK)]
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d["hbm_gbs"], d["bf16_tflops"], d.get("bf16_tflops_sustained", d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index, self.proc, self.f = index, None, None
+
+    def __enter__(self):
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = [r.split(",") for r in Path(self.f.name).read_text().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def fp64_reference_quotes(lat, plan, torch):
+    """Plain FP64 restatement of the solve with torch on the device (accuracy check only,
+    outside the timed region): dense L from the ELL generator, (I + dt L)^(2^niter) with
+    row renormalisation, chaining, payoff induction, discounting."""
+    d = lat.d
+    dev = lat.device
+    cols = lat.cols.view(d, -1).long()
+    vals = lat.vals.view(d, -1)
+    L = torch.zeros(d, d, dtype=torch.float64, device=dev)
+    mask = cols >= 0
+    rows = torch.arange(d, device=dev).unsqueeze(1).expand_as(cols)
+    L.index_put_((rows[mask], cols[mask]), vals[mask], accumulate=True)
+    P = torch.eye(d, dtype=torch.float64, device=dev) + plan.dt * L
+    del L
+    for _ in range(plan.niter):
+        P = P @ P
+        P /= P.sum(dim=1, keepdim=True)
+    K = torch.tensor(STRIKES, dtype=torch.float64, device=dev)
+    G = torch.clamp(lat.x.unsqueeze(1) - K.unsqueeze(0), min=0.0)
+    out = []
+    Pm = P
+    for m in range(1, NMAT + 1):
+        if m > 1:
+            Pm = Pm @ P
+            Pm /= Pm.sum(dim=1, keepdim=True)
+        out.append(math.exp(-lat.rate * PERIOD * m) * (Pm[lat.y0] @ G))
+    return torch.stack(out)
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    from oplib_b200 import _lib
+    from oplib_b200.model import MODES, Lattice, bind_stream
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    stream = torch.cuda.current_stream(dev)
+    bind_stream(dev)
+    mode = MODES[args.mode]
+    sv = dict(SV)
+    sv["rho"] = SV["rho"] + 0.001 * rank  # independent replica per rank
+    lat = Lattice.stoch_vol(**sv, device=dev)
+    plan = lat.plan(PERIOD, DT0)
+    strikes = torch.tensor(STRIKES, dtype=torch.float64, device=dev)
+    ws = lat.workspace(NK, mode)
+    quotes = torch.empty(NMAT, NK, dtype=torch.float64, device=dev)
+    desc = lat.desc(plan, PERIOD, NMAT, strikes)
+    d = lat.d
+
+    def build_generator():
+        _lib.call("opb_sv_generator_ell", sv["nx"], sv["nv"], sv["x_lo"], sv["x_hi"], sv["v_lo"], sv["v_hi"],
+                  sv["rate"], sv["kappa"], sv["theta"], sv["xi"], sv["rho"], lat.cols.data_ptr(),
+                  lat.vals.data_ptr(), lat.x.data_ptr())
+
+    def step():
+        build_generator()
+        _lib.call("opb_lattice_solve", C.byref(desc), mode, ws.data_ptr(), ws.numel(), quotes.data_ptr(), None)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    assert lib.opb_tc_error() == 0
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clocks = clk.summary()
+
+    # ---- end to end through the C ABI: pinned host strikes in, quotes out, every step
+    h_strikes = torch.tensor(STRIKES, dtype=torch.float64).pin_memory()
+    h_quotes = torch.empty(NMAT, NK, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        strikes.copy_(h_strikes, non_blocking=True)
+        step()
+        h_quotes.copy_(quotes, non_blocking=True)
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+
+    # ---- dominant kernel timed alone with CUDA events on the launching stream
+    hbm, bf16_burst, bf16_sus, src = _peaks()
+    kern = {}
+    if mode == MODES["bf16x3"]:
+        Ah = torch.empty(d, d, dtype=torch.bfloat16, device=dev).normal_(0, 1e-3)
+        Al = torch.empty_like(Ah).normal_(0, 1e-6)
+        X = torch.empty(d, d, dtype=torch.float32, device=dev).normal_()
+        rs = torch.empty(lib.opb_gemm_bf16x3_nparts(d) * d, dtype=torch.float64, device=dev)
+        args_g = (d, d, d, Ah.data_ptr(), Al.data_ptr(), d, Ah.data_ptr(), Al.data_ptr(), d, 1.0, X.data_ptr(), 2.0,
+                  X.data_ptr(), d, rs.data_ptr())
+        for _ in range(3):
+            _lib.call("opb_gemm_bf16x3", *args_g)
+        torch.cuda.synchronize()
+        n_rep = 20
+        e0.record(stream)
+        for _ in range(n_rep):
+            _lib.call("opb_gemm_bf16x3", *args_g)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        k_ms = e0.elapsed_time(e1) / n_rep
+        mma_flops = 3 * 2.0 * d ** 3
+        achieved = mma_flops / (k_ms * 1e-3) / 1e12
+        kern = {"bound": "tensor", "achieved": round(achieved, 1), "peak": bf16_burst, "unit": "TFLOP/s",
+                "frac": round(achieved / bf16_burst, 4), "traffic": None, "peak_source": f"{src} burst bf16",
+                "kernel": "k_tc_gemm<256,2> (E-form squaring, 6144^3 x 3 BF16 products)",
+                "avg_launch_ms": round(k_ms, 4), "useful_tflops": round(achieved / 3, 1)}
+        del Ah, Al, X, rs
+    else:
+        A = torch.empty(d, d, dtype=torch.float32, device=dev).uniform_()
+        Cc = torch.empty_like(A)
+        for _ in range(2):
+            _lib.call("opb_sgemm_batched_rm", d, d, d, A.data_ptr(), 0, A.data_ptr(), 0, Cc.data_ptr(), 0, 1)
+        torch.cuda.synchronize()
+        n_rep = 5
+        e0.record(stream)
+        for _ in range(n_rep):
+            _lib.call("opb_sgemm_batched_rm", d, d, d, A.data_ptr(), 0, A.data_ptr(), 0, Cc.data_ptr(), 0, 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        k_ms = e0.elapsed_time(e1) / n_rep
+        achieved = 2.0 * d ** 3 / (k_ms * 1e-3) / 1e12
+        kern = {"bound": "fp32-simt", "achieved": round(achieved, 2), "peak": 74.4, "unit": "TFLOP/s",
+                "frac": round(achieved / 74.4, 4), "traffic": None,
+                "peak_source": "nominal FP32 FMA (148 SM x 128 lanes x 2 x 1.965 GHz)",
+                "kernel": "k_sgemm_rm (128x128 SIMT tile)", "avg_launch_ms": round(k_ms, 4)}
+        del A, Cc
+
+    # ---- accuracy of this step's quotes vs an FP64 solve of the same lattice
+    step()
+    torch.cuda.synchronize()
+    q_ref = fp64_reference_quotes(lat, plan, torch)
+    err = float((quotes - q_ref).abs().max().item())
+    # the plain FP32 path on the same lattice (comparison arm), timed the same way
+    extra = {}
+    if args.compare and mode == MODES["bf16x3"]:
+        m32 = MODES["fp32"]
+        ws32 = lat.workspace(NK, m32)
+        q32 = torch.empty_like(quotes)
+        _lib.call("opb_lattice_solve", C.byref(desc), m32, ws32.data_ptr(), ws32.numel(), q32.data_ptr(), None)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        _lib.call("opb_lattice_solve", C.byref(desc), m32, ws32.data_ptr(), ws32.numel(), q32.data_ptr(), None)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms32 = e0.elapsed_time(e1)
+        extra = {"fp32_quotes_per_s": round(NMAT * NK * world / (ms32 * 1e-3), 1), "fp32_ms_per_solve": round(ms32, 2),
+                 "fp32_max_abs_err_vs_fp64": float((q32 - q_ref).abs().max().item()),
+                 "speedup_vs_fp32": round(ms32 / ms, 2)}
+        del ws32
+
+    quotes_per_step = NMAT * NK * world
+    value = quotes_per_step / (ms * 1e-3)
+    # gpu launches per step (library kernels): generator, E0 scatter, split, niter*(gemm+renorm),
+    # add_identity, split, payoff, nmat*(price gemm + discount), (nmat-1)*(chain gemm + renorm)
+    if mode == MODES["bf16x3"]:
+        launches = 1 + 1 + 1 + 2 * plan.niter + 1 + 1 + 1 + 2 * NMAT + 2 * (NMAT - 1)
+    else:
+        launches = 1 + 2 + (3 if mode == 1 else 1) * plan.niter + 1 + 2 * NMAT + (3 if mode == 1 else 1) * (NMAT - 1)
+    out = {
+        "metric": "priced quotes/sec at <=1e-5 abs err vs FP64 (split-BF16 tensor-core lattice vs plain FP32)",
+        "value": round(value, 1), "unit": "quotes/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16x3->fp32 (fp64 renorm/discount)" if mode == 2 else "fp32", "data": "synthetic",
+        "config": {"workload": "SV lattice 48 vol x 128 spot = 6144 states, dt0=2^-16, 14 squarings + 15 chains, "
+                               "128 strikes x 16 quarterly maturities (2048 quotes/solve)",
+                   "d": d, "niter": plan.niter, "nmat": NMAT, "nK": NK, "mode": args.mode,
+                   "parallelism": f"replicas x{world}", "l2": "operands 151-302 MB per matrix > 126 MB L2"},
+        "max_abs_err_vs_fp64": err,
+        "e2e": {"value": round(quotes_per_step / (ms_e2e * 1e-3), 1), "unit": "quotes/s",
+                "h2d_bytes_per_step": NK * 8, "d2h_bytes_per_step": NMAT * NK * 8},
+        "gpu_launches": launches * args.steps,
+        "roofline": kern,
+        "clocks": clocks,
+    }
+    out.update(extra)
+    return out
+
+
+def cpu_baseline(samples: int = 2):
+    """FP64 oracle path on the host cores: one 6144^3 DGEMM (torch-CPU, MKL) timed and
+    scaled to the 29 products of a solve (squarings and chains dominate; the
+    O(d^2) work is ignored)."""
+    import torch
+    d = 6144
+    nth = os.cpu_count() or 1
+    torch.set_num_threads(nth)
+    a = torch.rand(d, d, dtype=torch.float64)
+    b = torch.rand(d, d, dtype=torch.float64)
+    _ = a[:512, :512] @ b[:512, :512]
+    t = []
+    for _ in range(samples):
+        t0 = time.perf_counter()
+        _ = a @ b
+        t.append(time.perf_counter() - t0)
+    tg = min(t)
+    solve_s = 29 * tg
+    return {"value": round(NMAT * NK / solve_s, 3), "unit": "quotes/s", "cores": nth, "kind": "port",
+            "sample": f"{samples} x FP64 {d}^3 DGEMM (torch-CPU/MKL, {nth} threads) = {tg:.3f}s each, x29 "
+                      "products per solve extrapolated"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--mode", default="bf16x3", choices=["bf16x3", "fp32", "fp32_plain"])
+    ap.add_argument("--no-compare", dest="compare", action="store_false")
+    ap.add_argument("--no-cpu-baseline", dest="cpu", action="store_false")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        t0 = time.perf_counter()
+        vals = []
+        for _ in range(args.warmup):
+            cpu_baseline(1)
+        for _ in range(args.steps):
+            vals.append(cpu_baseline(1))
+        v = statistics.median(x["value"] for x in vals)
+        cb = dict(vals[0])
+        cb["value"] = v
+        line = {"impl": "reference", "metric": "priced quotes/sec (FP64 oracle port on host cores)", "value": v,
+                "unit": "quotes/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(NMAT * NK / v * 1e3, 1), "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "SV lattice 6144 states, 29 products per solve, 2048 quotes",
+                           "parallelism": "host threads"},
+                "cpu_baseline": cb, "e2e": {"value": v, "unit": "quotes/s", "h2d_bytes_per_step": 0,
+                                            "d2h_bytes_per_step": 0},
+                "wall_s": round(time.perf_counter() - t0, 1)}
+        print(json.dumps(line))
+        return 0
+
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    out = run_b200(args, rank, world, local_rank)
+    if rank == 0:
+        if args.cpu:
+            out["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,228 @@
+/*
+ * opcuda-b200: B200-native (sm_100a) replacement of OPLib's opcuda C-ABI for the
+ * operator-method pricing path (generator exponentiation by repeated squaring, payoff
+ * backward induction, Markov-chain Monte Carlo).
+ *
+ * Library: libopcuda_b200.so.  Every function is extern "C".
+ *
+ * Differences from the reference ABI, applied uniformly:
+ *   - device pointers are 64-bit (uint64_t handles or typed pointers); the reference
+ *     passes them as 32-bit `unsigned` (oplib/opcuda/util.cu:209-213), which truncates
+ *     addresses on a 64-bit host;
+ *   - every entry point returns an int status: 0 = success, negative = argument error
+ *     detected on the host (OPB_E_*), positive = cudaError_t.  The last status of the
+ *     calling thread is also returned by opcuda_get_status(), which is how the
+ *     reference's callers read it (oplib/opcuda/util.cu:204-207);
+ *   - work is ordered on a per-thread library stream (opb_set_stream; default: the
+ *     legacy default stream).  Calls that the reference makes blocking (memcpy, mc1f)
+ *     stay blocking.
+ * Names, argument order and column-major semantics of the opcuda_* entry points are the
+ * reference's.  opb_* entry points are new B200 forms (source-major storage).
+ */
+#ifndef OPCUDA_B200_H
+#define OPCUDA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define OPB_OK 0
+#define OPB_E_ARG (-1)
+#define OPB_E_NULL (-2)
+#define OPB_E_ALIGN (-3)
+#define OPB_E_UNSUPPORTED (-4)
+#define OPB_E_NOMEM (-5)
+#define OPB_E_TIMEOUT (-6)
+#define OPB_E_STATE (-7)
+
+/* precision modes of opb_lattice_solve */
+#define OPB_FP32_PLAIN 0  /* FP32 SIMT products, reference semantics (no renormalisation) */
+#define OPB_FP32_RENORM 1 /* FP32 SIMT products + FP64 row renormalisation */
+#define OPB_BF16X3 2      /* split-BF16 tcgen05 products (E-form squaring) + FP64 renormalisation */
+
+/* ------------------------------------------------------------------ runtime support */
+/* replaces oplib/opcuda/util.cu:204-207 (unsigned opcuda_get_status()) */
+int opcuda_get_status(void);
+/* replaces oplib/opcuda/util.cu:123-126 (cuBLAS init); creates the CUDA context */
+int opcuda_cublas_init(void);
+/* replaces oplib/opcuda/util.cu:287-290 */
+int opcuda_shutdown(void);
+/* replaces oplib/opcuda/util.cu:131-133 (void) */
+int opcuda_thread_synchronize(void);
+/* replaces oplib/opcuda/util.cu:139-141 (void) */
+int opcuda_set_device(int dev);
+/* replaces oplib/opcuda/util.cu:148-153 */
+int opcuda_get_device(void);
+/* replaces oplib/opcuda/util.cu:156-161 */
+int opcuda_device_get_count(void);
+/* replaces oplib/opcuda/util.cu:240-245 */
+int opcuda_device_count(void);
+/* replaces oplib/opcuda/util.cu:163-170 (the reference leaves the name unset) */
+int opcuda_device_get_name(char *name, int len, int dev);
+/* replaces oplib/opcuda/util.cu:172-179 (unsigned *bytes; the reference leaves it unset) */
+int opcuda_device_total_memory(uint64_t *bytes, int dev);
+/* replaces oplib/opcuda/util.cu:248-253 */
+int opcuda_multi_processor_count(int dev);
+/* replaces oplib/opcuda/util.cu:255-260 */
+int opcuda_max_threads_per_block(int dev);
+/* replaces oplib/opcuda/util.cu:209-214 (unsigned opcuda_mem_alloc(unsigned sz)) */
+uint64_t opcuda_mem_alloc(uint64_t sz);
+/* replaces oplib/opcuda/util.cu:217-221 */
+int opcuda_mem_free_device(uint64_t ptr);
+/* replaces oplib/opcuda/util.cu:223-230 */
+uint64_t opcuda_mem_alloc_host(uint64_t sz);
+/* replaces oplib/opcuda/util.cu:232-236 */
+int opcuda_mem_free_host(uint64_t hptr);
+/* replace oplib/opcuda/util.cu:182-200 (blocking copies) */
+int opcuda_memcpy_h2d(uint64_t dptr, uint64_t hptr, uint64_t sz);
+int opcuda_memcpy_d2h(uint64_t dptr, uint64_t hptr, uint64_t sz);
+int opcuda_memcpy_d2d(uint64_t dptr2, uint64_t dptr1, uint64_t sz);
+/* replace oplib/opcuda/util.cu:62-113 (wall-clock timers) */
+void opcuda_create_timer(void);
+void opcuda_reset_timer(void);
+void opcuda_stop_timer(void);
+double opcuda_get_timer_value(void);
+/* replaces oplib/opcuda/util.cu:263-282 */
+int opcuda_scopy(int n, uint64_t x, int incx, uint64_t y, int incy);
+/* replaces oplib/opcuda/scopy2.cu:137-143 */
+int opcuda_scopy1(uint64_t destination, uint64_t source, uint64_t n);
+/* replace oplib/opcuda/sset.cu:54-74 */
+int opcuda_ssetall(uint64_t x, int n, float c, int incx);
+int opcuda_ssetone(uint64_t x, int n, float c, int i);
+
+/* new: library stream of the calling thread (a cudaStream_t as an integer), version,
+ * status text, and a test hook making the n-th next opcuda_mem_alloc fail */
+int opb_set_stream(uint64_t stream);
+uint64_t opb_get_stream(void);
+const char *opb_version(void);
+const char *opb_status_string(int status);
+int opb_test_fail_next_alloc(int n);
+
+/* ------------------------------------------------------------------ GEMM / GEMV (FP32) */
+/* replaces oplib/opcuda/sgemm.cu:41-44: column-major C = alpha*A*B + beta*C */
+int opcuda_sgemm(int m, int n, int k, float alpha, uint64_t A, int lda, uint64_t B, int ldb, float beta,
+                 uint64_t C, int ldc);
+/* replaces oplib/opcuda/ssqmm.cu:174-179: C_i = A_i * B_i for ni column-major d x d
+ * matrices; A_i, B_i, C_i are device arrays of ni 64-bit device pointers */
+int opcuda_ssqmm(int d, int ni, uint64_t A_i, uint64_t B_i, uint64_t C_i);
+/* replaces oplib/opcuda/sgemm4.cu:148-154: argptr_bid is a device array of nblocks
+ * 64-bit pointers to task records {int32 i, bx, by, m, n, k; uint64 A, B, C}
+ * (opb_sgemm4_task_size() bytes); block computes C rows [64bx, 64bx+64) x cols
+ * [16by, 16by+16) of the column-major C = A*B with lda = m, ldb = k, ldc = m */
+int opcuda_sgemm4(int nblocks, uint64_t argptr_bid);
+int opb_sgemm4_task_size(void);
+/* new: row-major strided batch C_z = A_z * B_z (M x K times K x N) */
+int opb_sgemm_batched_rm(int M, int N, int K, const float *A, long long sA, const float *B, long long sB, float *C,
+                         long long sC, int batch);
+/* replace oplib/opcuda/sgemv.cu:44-62 */
+int opcuda_sgemv(int m, int n, float alpha, uint64_t A, int lda, uint64_t x, int incx, float beta, uint64_t y,
+                 int incy);
+int opcuda_sgemvT(int m, int n, float alpha, uint64_t A, int lda, uint64_t x, int incx, float beta, uint64_t y,
+                  int incy);
+/* replaces oplib/opcuda/sgemv3.cu:163-176: Z[col1[c] + row] = sum_k A[row + d*k] Z[col0[c] + k]
+ * (column offsets in elements; entries at or after the first col1 >= 2*nz*d are skipped) */
+int opcuda_sgemv3(int d, int nz, int ncol, uint64_t A, uint64_t B, uint64_t col0ptr, uint64_t col1ptr);
+/* replaces oplib/opcuda/sgemv4.cu:174-180: task records {int32 i, bx, by, d, nz, ncol;
+ * uint64 A, Z, col0, col1} (opb_sgemv4_task_size() bytes); rows [128bx, 128bx+128) of the
+ * 16 list entries starting at 16by */
+int opcuda_sgemv4(int nblocks, uint64_t argptr_bid);
+int opb_sgemv4_task_size(void);
+/* replaces oplib/opcuda/sdot2.cu:72-83: c[h] = sum_{y<n} a[h + m*y] * b[h + m*y], h < m */
+int opcuda_sdot2(uint64_t aptr, uint64_t bptr, uint64_t cptr, int m, int n);
+
+/* ------------------------------------------------------------------ kernels from generators */
+/* replace oplib/opcuda/sek.cu:106-137: column-major U = (I + dt*gen) [/(1 + dt*r*lambda)],
+ * formed in FP64 and rounded once */
+int opcuda_sek(int d, uint64_t genPtr, float dt, uint64_t tpkerPtr);
+int opcuda_sekd(int d, uint64_t genPtr, float dt, uint64_t tpkerPtr, uint64_t rPtr);
+int opcuda_sekd_lambda(int d, uint64_t genPtr, float dt, uint64_t tpkerPtr, uint64_t rPtr, uint64_t lambdaPtr);
+/* replaces oplib/opcuda/sglvg.cu:104-125: dense column-major LV generators for ni periods
+ * from per-node column-major 2x2 inverses invm[4d] and pars = [drift (ni*d); vol (ni*d)] */
+int opcuda_sglvg(uint64_t gen_yy_i, int ni, int d, uint64_t invmat, uint64_t pars);
+/* new (device generator builders, FP64, ELL form: row y holds w (col, val) pairs, col -1 = empty) */
+int opb_lv_params(int d, double lo, double hi, double s0, double level, double skew, double width, double floor_,
+                  double r, double *x, double *drift, double *vol);
+int opb_lv_generator_ell(int d, const double *x, const double *drift, const double *vol, int *cols, double *vals);
+int opb_sv_generator_ell(int nx, int nv, double x_lo, double x_hi, double v_lo, double v_hi, double r, double kappa,
+                         double theta, double xi, double rho, int *cols, double *vals, double *x_y);
+int opb_ell_maxdiag(int d, int w, const int *cols, const double *vals, unsigned long long *dscratch,
+                    double *out_host);
+/* new: the squaring plan of one interval (oplib/opmodel/models/CModel Common.cs:289-307) */
+int opb_plan_interval(double maxdiag, double delta_t, double dt0, int *niter, double *dt_j);
+
+/* ------------------------------------------------------------------ split-BF16 tensor-core GEMM */
+/* new: C = alpha*(Ahi*Bhi^T + Ahi*Blo^T + Alo*Bhi^T) + beta*Cin, row-major, K-major operands
+ * (A: M x K, B: N x K), M % 128 == 0, N % 64 == 0, K % 64 == 0, 16-byte aligned; rowsum
+ * (optional) receives FP64 row sums of C per N tile: rowsum[t*M + row],
+ * t < opb_gemm_bf16x3_nparts(N).  Replaces the FP32 SIMT products of oplib/opcuda/ssqmm.cu. */
+typedef uint16_t opb_bf16; /* storage of one bfloat16 */
+int opb_gemm_bf16x3(int M, int N, int K, const opb_bf16 *Ahi, const opb_bf16 *Alo, long long lda,
+                    const opb_bf16 *Bhi, const opb_bf16 *Blo, long long ldb, float alpha, const float *Cin,
+                    float beta, float *C, long long ldc, double *rowsum);
+int opb_gemm_bf16x3_nparts(int N);
+/* reads and clears the device error word of the tensor-core kernels (0 = none) */
+int opb_tc_error(void);
+
+/* ------------------------------------------------------------------ lattice solve */
+typedef struct opb_lattice_desc {
+    int d;                   /* states */
+    int y0;                  /* quoted state */
+    int ell_width;           /* > 0: ELL generator (gen_cols, gen_vals); 0: dense gen_dense */
+    const int *gen_cols;     /* device [d*ell_width] */
+    const double *gen_vals;  /* device [d*ell_width] FP64 */
+    const double *gen_dense; /* device [d*d] FP64, row-major (row = source state) */
+    const double *x;         /* device [d] spot per state */
+    double dt;               /* elementary step = period * 2^-niter */
+    int niter;               /* squarings */
+    int nmat;                /* maturities T_m = m*period, m = 1..nmat */
+    double period;
+    double rate;             /* discount rate */
+    int nK;                  /* strikes */
+    const double *strikes;   /* device [nK] */
+} opb_lattice_desc;
+/* new: the device branch of CModel.exe_mc_plan (oplib/opmodel/models/CModel Common.cs:651-669)
+ * plus payoff backward induction: quotes[(m-1)*nK + k] = exp(-rate*T_m) * (P(T_m) G)[y0, k],
+ * G[z, k] = (x_z - K_k)^+; V_all (optional) receives all states [nmat][d][nK]. */
+unsigned long long opb_lattice_workspace_size(int d, int nK, int mode);
+int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
+                      double *quotes, double *V_all);
+/* new: transition kernel P(period) only (device d x d FP32, source-major), e.g. the MC step
+ * kernel; nmat, nK and strikes of L are ignored */
+int opb_lattice_kernel(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
+                       float *P_out);
+
+/* ------------------------------------------------------------------ cumulative rows, MC */
+/* replaces oplib/opcuda/sck.cu:88-93: nm column-major kernels -> cumulative normalised rows */
+int opcuda_sck(int d, int nm, uint64_t tpker_yy_m, uint64_t ctpker_yy_m);
+/* new: source-major cumulative rows; per-row bracket table (nb a power of two, d <= 65535),
+ * the device analogue of CModel Host Double.cs:434-455 */
+int opb_sck_rm(int d, int nrows, const float *P, float *C);
+int opb_guide_table(int d, int nrows, int nb, const float *C, uint32_t *guide);
+/* replace oplib/opcuda/smc.cu:87-106 */
+int opcuda_mc_load_mt_gpu(const char *MT_stream, long sz);
+int opcuda_mc_nrng(void);
+int opcuda_mc_status_sz(void);
+/* replaces oplib/opcuda/smc.cu:137-156: first uint32 at host_seedptr is the base seed;
+ * mtptr is the device continuation record (opcuda_mc_status_sz() words) */
+int opcuda_mc_setseed(uint64_t host_seedptr, uint64_t mtptr);
+/* replaces oplib/opcuda/smc.cu:610-656 (per-path MT19937 streams; nk <= 623, d <= 32767) */
+int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk, int d, uint64_t ctpker_m_yy, uint64_t m_k,
+                uint64_t yhostptr);
+/* replaces oplib/opcuda/smc.cu:731-736 (nscen % 4096 == 0, nscen/4096 <= 623) */
+int opcuda_mt_benchmark(uint64_t mtptr, uint64_t unif_ptr, int nscen);
+/* new: MT19937 Monte Carlo, path p seeded init_genrand(seed + path0 + p); see mc.cu */
+int opb_mc_scratch_blocks(long long npaths);
+int opb_mc_mt19937(const float *C, long long row_stride, long long col_stride, const uint32_t *guide, int nb, int d,
+                   int y0, int nsteps, uint32_t seed, unsigned long long path0, long long npaths, short *ypaths,
+                   const double *x, double strike, double barrier, double disc, double *scratch, double *sums);
+int opb_mt19937_raw(uint32_t seed, long long nstreams, int n, uint32_t *out);
+int opb_mt_uniforms(uint32_t seed, long long nstreams, int nper, float *unif);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPCUDA_B200_H */

@@ -1,0 +1,411 @@
+// Split-BF16 GEMM on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+//   C[M,N] = alpha * (Ahi.Bhi^T + Ahi.Blo^T + Alo.Bhi^T) + beta * Cin[M,N]
+//
+// A = Ahi + Alo and B = Bhi + Blo are FP32 matrices split into two BF16 parts
+// (hi = bf16(a), lo = bf16(a - hi)); the three products carry about 16 mantissa bits per
+// operand and accumulate in FP32 in tensor memory.  This replaces the FP32 SIMT squaring
+// of oplib/opcuda/ssqmm.cu:119-179 on the lattice path.  Operands are K-major (rows of A
+// and rows of B^T contiguous), M % 128 == 0, N % BN == 0, K % 64 == 0.
+//
+// Structure (one 128 x BN output tile per CTA, 128 threads):
+//   warp 0, one lane : TMA producer -- 4 tiled bulk-tensor loads per K-block (Ahi, Alo,
+//                      Bhi, Blo; 128B swizzle; no multicast) into a STAGES-deep ring,
+//                      completion tracked by mbarrier transaction counts.
+//   warp 1, one lane : MMA issuer -- per 16-wide K step three tcgen05.mma.kind::f16
+//                      (BF16 x BF16 -> FP32) into one TMEM accumulator of BN columns;
+//                      tcgen05.commit releases each stage and finally signals the
+//                      epilogue.
+//   all 4 warps      : epilogue -- tcgen05.ld of the thread's accumulator row, the
+//                      alpha/beta update, FP32 stores and the FP64 row sum of the stored
+//                      values (rowsum[n_tile * M + row], used by the row renormalisation).
+// Every mbarrier wait is bounded by a %globaltimer deadline; on expiry the kernel records
+// an error code in g_tc_error, drains its outstanding copies and MMAs, frees TMEM and
+// returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <mutex>
+
+#include "common.cuh"
+#include "lattice.h"
+
+namespace opb {
+
+__device__ int g_tc_error = 0;
+
+constexpr int TC_BM = 128;
+constexpr int TC_BK = 64;  // 64 bf16 = 128 bytes = one swizzle row
+constexpr unsigned long long TC_WAIT_NS = 4000000000ull;  // 4 s per wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: true when the phase completed, false on timeout or abort.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag,
+                                          unsigned long long limit_ns) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = gtimer();
+    while (true) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (gtimer() - t0 > limit_ns) return false;
+    }
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+        : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major, 128-byte swizzle UMMA shared-memory descriptor: 8-row core groups 1024 bytes
+// apart (SBO), LBO unused for swizzled K-major (1), descriptor version 1 (sm_100).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)1 << 16;            // LBO
+    d |= (uint64_t)(1024 >> 4) << 32;  // SBO
+    d |= (uint64_t)1 << 46;            // version
+    d |= (uint64_t)2 << 61;            // SWIZZLE_128B
+    return d;
+}
+
+// kind::f16 instruction descriptor: D = F32, A = B = BF16, both K-major, N, M = 128.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <int BN, int STAGES>
+struct TcCfg {
+    static constexpr int A_BYTES = TC_BM * TC_BK * 2;  // one of Ahi/Alo
+    static constexpr int B_BYTES = BN * TC_BK * 2;     // one of Bhi/Blo
+    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+};
+
+struct TcParams {
+    int M, N, K;
+    float *C;
+    long long ldc;
+    const float *Cin;
+    float alpha, beta;
+    double *rowsum;
+};
+
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(128, 1)
+    k_tc_gemm(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
+              const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p) {
+    using Cfg = TcCfg<BN, STAGES>;
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    uint8_t *gbase = smem_raw + (base - raw);
+    // barrier block after the stages
+    uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + STAGES * Cfg::STAGE_BYTES);
+    const uint32_t bar0 = smem_u32(bars);
+    auto full_bar = [&](int s) { return bar0 + 8u * s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+    const uint32_t done_bar = bar0 + 8u * (2 * STAGES);
+    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bars + 2 * STAGES + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * STAGES + 2);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * TC_BM;
+    const int nk = p.K / TC_BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        mbar_init(done_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 0) {
+        const uint32_t slot = smem_u32(const_cast<uint32_t *>(tmem_slot));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer
+            int issued = 0;
+            bool ok = true;
+            for (int kb = 0; kb < nk; kb++) {
+                const int s = kb % STAGES;
+                if (kb >= STAGES) {
+                    if (!mbar_wait(empty_bar(s), ((kb / STAGES) + 1) & 1, abort_flag, TC_WAIT_NS)) {
+                        ok = false;
+                        break;
+                    }
+                }
+                const uint32_t st = base + s * Cfg::STAGE_BYTES;
+                mbar_expect_tx(full_bar(s), Cfg::STAGE_BYTES);
+                const int kx = kb * TC_BK;
+                tma_load_2d(st, &mAhi, full_bar(s), kx, m0);
+                tma_load_2d(st + Cfg::A_BYTES, &mAlo, full_bar(s), kx, m0);
+                tma_load_2d(st + 2 * Cfg::A_BYTES, &mBhi, full_bar(s), kx, n0);
+                tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, &mBlo, full_bar(s), kx, n0);
+                issued++;
+            }
+            if (!ok) {
+                atomicExch(&g_tc_error, 1);
+                *abort_flag = 1;
+                // drain the copies that may still be in flight (at most STAGES)
+                const int first = issued > STAGES ? issued - STAGES : 0;
+                for (int kb = first; kb < issued; kb++)
+                    (void)mbar_wait(full_bar(kb % STAGES), (kb / STAGES) & 1, abort_flag, 100000000ull);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer
+            const uint32_t idesc = umma_idesc_bf16(BN);
+            bool ok = true;
+            for (int kb = 0; kb < nk; kb++) {
+                const int s = kb % STAGES;
+                if (!mbar_wait(full_bar(s), (kb / STAGES) & 1, abort_flag, TC_WAIT_NS)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t st = base + s * Cfg::STAGE_BYTES;
+                const uint64_t dAh = umma_desc_sw128(st);
+                const uint64_t dAl = umma_desc_sw128(st + Cfg::A_BYTES);
+                const uint64_t dBh = umma_desc_sw128(st + 2 * Cfg::A_BYTES);
+                const uint64_t dBl = umma_desc_sw128(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES);
+#pragma unroll
+                for (int k16 = 0; k16 < TC_BK / 16; k16++) {
+                    const uint64_t adv = (uint64_t)((k16 * 32) >> 4);  // +32 bytes along K
+                    const uint32_t acc0 = (kb > 0 || k16 > 0) ? 1u : 0u;
+                    umma_bf16(tmem, dAh + adv, dBh + adv, idesc, acc0);
+                    umma_bf16(tmem, dAh + adv, dBl + adv, idesc, 1u);
+                    umma_bf16(tmem, dAl + adv, dBh + adv, idesc, 1u);
+                }
+                umma_commit(empty_bar(s));
+            }
+            if (!ok) {
+                atomicExch(&g_tc_error, 2);
+                *abort_flag = 1;
+            }
+            umma_commit(done_bar);  // arrives once every issued MMA has completed
+        }
+        __syncwarp();
+    }
+
+    // ---------------- epilogue (all 128 threads; warp w owns TMEM lanes 32w..32w+31)
+    bool ok = mbar_wait(done_bar, 0, abort_flag, TC_WAIT_NS);
+    tc_fence_after();
+    if (!ok) atomicExch(&g_tc_error, 3);
+    if (ok && !*abort_flag) {
+        const int row = m0 + warp * 32 + lane;
+        float *crow = p.C + (long long)row * p.ldc + n0;
+        const float *cin = p.Cin ? p.Cin + (long long)row * p.ldc + n0 : nullptr;
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        double rs = 0.0;
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+            uint32_t v[32];
+            tmem_ld32(trow + (uint32_t)c0, v);
+#pragma unroll
+            for (int j = 0; j < 32; j += 4) {
+                float4 o;
+                o.x = p.alpha * __uint_as_float(v[j + 0]);
+                o.y = p.alpha * __uint_as_float(v[j + 1]);
+                o.z = p.alpha * __uint_as_float(v[j + 2]);
+                o.w = p.alpha * __uint_as_float(v[j + 3]);
+                if (cin) {
+                    const float4 ci = *reinterpret_cast<const float4 *>(cin + c0 + j);
+                    o.x = fmaf(p.beta, ci.x, o.x);
+                    o.y = fmaf(p.beta, ci.y, o.y);
+                    o.z = fmaf(p.beta, ci.z, o.z);
+                    o.w = fmaf(p.beta, ci.w, o.w);
+                }
+                *reinterpret_cast<float4 *>(crow + c0 + j) = o;
+                rs += (double)o.x + (double)o.y + (double)o.z + (double)o.w;
+            }
+        }
+        if (p.rowsum) p.rowsum[(long long)blockIdx.x * p.M + row] = rs;
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+    }
+}
+
+// ------------------------------------------------------------------ host side
+
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// rows x K bf16 row-major matrix (leading dimension ld elements), box = box_rows x 64.
+static int make_map(CUtensorMap *m, const void *ptr, long long rows, long long K, long long ld, int box_rows) {
+    auto enc = get_encode();
+    if (!enc) return OPB_E_UNSUPPORTED;
+    cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+    cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? OPB_OK : OPB_E_ARG;
+}
+
+int tc_gemm_tile_n(int N) {
+    if (N % 256 == 0) return 256;
+    if (N % 128 == 0) return 128;
+    if (N % 64 == 0) return 64;
+    return 0;
+}
+
+int tc_gemm_nparts(int N) {
+    int bn = tc_gemm_tile_n(N);
+    return bn ? N / bn : 0;
+}
+
+int tc_gemm_check(const TcGemmArgs &a) {
+    if (a.M <= 0 || a.N <= 0 || a.K <= 0) return OPB_E_ARG;
+    if (a.M % TC_BM || a.K % TC_BK || !tc_gemm_tile_n(a.N)) return OPB_E_UNSUPPORTED;
+    if (!a.Ahi || !a.Alo || !a.Bhi || !a.Blo || !a.C) return OPB_E_NULL;
+    if (a.lda < a.K || a.ldb < a.K || a.ldc < a.N) return OPB_E_ARG;
+    // TMA: 16-byte aligned bases and row strides; float4 epilogue: 16-byte aligned rows
+    if (!aligned(a.Ahi, 16) || !aligned(a.Alo, 16) || !aligned(a.Bhi, 16) || !aligned(a.Blo, 16)) return OPB_E_ALIGN;
+    if ((a.lda * 2) % 16 || (a.ldb * 2) % 16 || a.ldc % 4 || !aligned(a.C, 16)) return OPB_E_ALIGN;
+    if (a.Cin && !aligned(a.Cin, 16)) return OPB_E_ALIGN;
+    return OPB_OK;
+}
+
+template <int BN, int STAGES>
+static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
+    using Cfg = TcCfg<BN, STAGES>;
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+        if (e != cudaSuccess) return (int)e;
+        attr_set[dev] = true;
+    }
+    CUtensorMap mAh, mAl, mBh, mBl;
+    int r;
+    if ((r = make_map(&mAh, a.Ahi, a.M, a.K, a.lda, TC_BM)) != OPB_OK) return r;
+    if ((r = make_map(&mAl, a.Alo, a.M, a.K, a.lda, TC_BM)) != OPB_OK) return r;
+    if ((r = make_map(&mBh, a.Bhi, a.N, a.K, a.ldb, BN)) != OPB_OK) return r;
+    if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN)) != OPB_OK) return r;
+    TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
+    dim3 grid(a.N / BN, a.M / TC_BM);
+    k_tc_gemm<BN, STAGES><<<grid, 128, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl, p);
+    return (int)cudaGetLastError();
+}
+
+int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
+    int c = tc_gemm_check(a);
+    if (c != OPB_OK) return c;
+    switch (tc_gemm_tile_n(a.N)) {
+        case 256: return launch_tc_impl<256, 2>(a, s);
+        case 128: return launch_tc_impl<128, 3>(a, s);
+        case 64: return launch_tc_impl<64, 4>(a, s);
+        default: return OPB_E_UNSUPPORTED;
+    }
+}
+
+}  // namespace opb
+
+using namespace opb;
+
+// Split-BF16 GEMM with typed pointers (row-major, K-major operands; see top of file).
+OPB_API int opb_gemm_bf16x3(int M, int N, int K, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo, long long lda,
+                            const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long ldb, float alpha,
+                            const float *Cin, float beta, float *C, long long ldc, double *rowsum) {
+    TcGemmArgs a{};
+    a.M = M; a.N = N; a.K = K; a.Ahi = Ahi; a.Alo = Alo; a.Bhi = Bhi; a.Blo = Blo; a.lda = lda; a.ldb = ldb;
+    a.C = C; a.ldc = ldc; a.Cin = Cin; a.alpha = alpha; a.beta = beta; a.rowsum = rowsum;
+    return set_status(launch_tc_gemm(a, stream()));
+}
+
+OPB_API int opb_gemm_bf16x3_nparts(int N) { return tc_gemm_nparts(N); }
+
+// Reads and clears the tensor-core kernels' device error word (0 = no bounded wait expired).
+OPB_API int opb_tc_error(void) {
+    int v = 0, z = 0;
+    OPB_TRY(cudaMemcpyFromSymbol(&v, g_tc_error, sizeof(int)));
+    OPB_TRY(cudaMemcpyToSymbol(g_tc_error, &z, sizeof(int)));
+    set_status(OPB_OK);
+    return v;
+}

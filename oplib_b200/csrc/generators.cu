@@ -1,0 +1,222 @@
+// Generator builders on the device, in FP64, emitting the sparse (ELL) form consumed by
+// the lattice solve.
+//
+// Local volatility (width 3, columns y-1, y, y+1): per interior node the down/up rates
+// solve [dm dp; dm^2 dp^2] p = [drift, vol^2] with dm = x[y-1]-x[y], dp = x[y+1]-x[y]
+// (oplib/opmodel/types/S1DGrid.cs:78-147 builds the 2x2 inverses,
+// oplib/opmodel/models/CLVModel.cs:86-136 applies them); boundary nodes are absorbing;
+// the diagonal is minus the row sum.
+//
+// Stochastic volatility (width 7): spot x log-spaced (nx), variance V = sigma_v^2 with
+// sigma_v log-spaced (nv), state y = ix + nx*iv (oplib/opmodel/types/S2DGrid.cs:142).
+// Heston variance dynamics dV = kappa(theta - V)dt + xi sqrt(V) dW2 with spot-variance
+// correlation rho, carried by two diagonal moves at a common rate q capped so that they
+// never carry more variance than the target in either direction; axial rates from the
+// per-direction 2x2 moment systems (the block-diagonal 4x4 invm of S2DGrid.pregen,
+// S2DGrid.cs:123-245); negative rates clamped to zero and a spot drift fix-up to r*x
+// (oplib/opmodel/models/CSVModel.cs:331-376).  The correlation term is a project
+// extension: the reference's SV generator has none.
+#include <cstring>
+
+#include "common.cuh"
+#include "lattice.h"
+
+namespace opb {
+
+__global__ void k_lv_ell(int d, const double *__restrict__ x, const double *__restrict__ drift,
+                         const double *__restrict__ vol, int *__restrict__ cols, double *__restrict__ vals) {
+    int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= d) return;
+    double pm = 0.0, pp = 0.0;
+    if (y > 0 && y < d - 1) {
+        const double dm = x[y - 1] - x[y], dp = x[y + 1] - x[y];
+        const double a = drift[y], v = vol[y], b = v * v;
+        const double det = dm * dp * dp - dp * dm * dm;
+        pm = (dp * dp * a - dp * b) / det;
+        pp = (-dm * dm * a + dm * b) / det;
+    }
+    int *c = cols + 3LL * y;
+    double *v = vals + 3LL * y;
+    c[0] = y > 0 ? y - 1 : -1;
+    v[0] = y > 0 ? pm : 0.0;
+    c[1] = y;
+    v[1] = -((y > 0 ? pm : 0.0) + (y < d - 1 ? pp : 0.0));
+    c[2] = y < d - 1 ? y + 1 : -1;
+    v[2] = y < d - 1 ? pp : 0.0;
+}
+
+// sigma(x) = max(floor, level + skew*exp(-((x-1)/width)^2)); x_i = lo*(hi/lo)^(i/(n-1));
+// drift = r*x, vol = sigma(x)*x.  Writes x, drift and vol.
+__global__ void k_lv_params(int d, double lo, double hi, double s0, double level, double skew, double width,
+                            double floor_, double r, double *__restrict__ x, double *__restrict__ drift,
+                            double *__restrict__ vol) {
+    int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= d) return;
+    double xv = s0 * lo * pow(hi / lo, (double)y / (double)(d - 1));
+    double z = (xv - 1.0) / width;
+    double sg = level + skew * exp(-z * z);
+    sg = sg > floor_ ? sg : floor_;
+    x[y] = xv;
+    drift[y] = r * xv;
+    vol[y] = sg * xv;
+}
+
+struct SvArgs {
+    int nx, nv;
+    double x_lo, x_hi, v_lo, v_hi, r, kappa, theta, xi, rho;
+};
+
+__device__ __forceinline__ double sv_xs(const SvArgs &a, int ix) {
+    return a.x_lo * pow(a.x_hi / a.x_lo, (double)ix / (double)(a.nx - 1));
+}
+__device__ __forceinline__ double sv_V(const SvArgs &a, int iv) {
+    double s = a.v_lo * pow(a.v_hi / a.v_lo, (double)iv / (double)(a.nv - 1));
+    return s * s;
+}
+
+__global__ void k_sv_ell(SvArgs a, int *__restrict__ cols, double *__restrict__ vals, double *__restrict__ x_y) {
+    const int d = a.nx * a.nv;
+    int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= d) return;
+    const int ix = y % a.nx, iv = y / a.nx;
+    int c[7];
+    double v[7];
+    for (int j = 0; j < 7; j++) { c[j] = -1; v[j] = 0.0; }
+    const double x = sv_xs(a, ix);
+    if (x_y) x_y[y] = x;
+    c[6] = y;
+    if (ix == 0 || ix == a.nx - 1) {  // absorbing spot boundary
+        cols[7LL * y + 0] = y; vals[7LL * y + 0] = 0.0;
+        for (int j = 1; j < 7; j++) { cols[7LL * y + j] = -1; vals[7LL * y + j] = 0.0; }
+        return;
+    }
+    const double V = sv_V(a, iv);
+    const double var_x = V * x * x, var_v = a.xi * a.xi * V, cov = a.rho * a.xi * V * x;
+    const double mu_x = a.r * x, mu_v = a.kappa * (a.theta - V);
+    const double xm = sv_xs(a, ix - 1), xp = sv_xs(a, ix + 1);
+    const double dxm = xm - x, dxp = xp - x;
+    // slots: 0 x-1, 1 x+1, 2 v-1, 3 v+1, 4 diag A, 5 diag B, 6 self
+    c[0] = y - 1; c[1] = y + 1;
+    double q = 0.0, ex = 0.0, ev = 0.0, ex2 = 0.0, ev2 = 0.0;
+    double dxa = 0, dva = 0, dxb = 0, dvb = 0;
+    if (iv > 0 && iv < a.nv - 1 && a.rho != 0.0) {
+        const double dvm = sv_V(a, iv - 1) - V, dvp = sv_V(a, iv + 1) - V;
+        if (a.rho < 0.0) {
+            dxa = dxp; dva = dvm; c[4] = (ix + 1) + a.nx * (iv - 1);
+            dxb = dxm; dvb = dvp; c[5] = (ix - 1) + a.nx * (iv + 1);
+        } else {
+            dxa = dxp; dva = dvp; c[4] = (ix + 1) + a.nx * (iv + 1);
+            dxb = dxm; dvb = dvm; c[5] = (ix - 1) + a.nx * (iv - 1);
+        }
+        const double cx = dxa * dva + dxb * dvb;
+        const double sx2 = dxa * dxa + dxb * dxb, sv2 = dva * dva + dvb * dvb;
+        q = cov / cx;
+        q = fmin(q, var_x / sx2);
+        q = fmin(q, var_v / sv2);
+        q = fmax(q, 0.0);
+        v[4] = q; v[5] = q;
+        ex = q * (dxa + dxb); ev = q * (dva + dvb); ex2 = q * sx2; ev2 = q * sv2;
+    }
+    {
+        const double aa = mu_x - ex, bb = var_x - ex2;
+        const double det = dxm * dxp * dxp - dxp * dxm * dxm;
+        v[0] = (dxp * dxp * aa - dxp * bb) / det;
+        v[1] = (-dxm * dxm * aa + dxm * bb) / det;
+    }
+    if (iv > 0 && iv < a.nv - 1) {
+        const double dvm = sv_V(a, iv - 1) - V, dvp = sv_V(a, iv + 1) - V;
+        const double aa = mu_v - ev, bb = var_v - ev2;
+        const double det = dvm * dvp * dvp - dvp * dvm * dvm;
+        c[2] = y - a.nx; v[2] = (dvp * dvp * aa - dvp * bb) / det;
+        c[3] = y + a.nx; v[3] = (-dvm * dvm * aa + dvm * bb) / det;
+    } else if (iv == 0) {
+        c[3] = y + a.nx; v[3] = fmax(mu_v, 0.0) / (sv_V(a, 1) - V);
+    } else {
+        c[2] = y - a.nx; v[2] = fmin(mu_v, 0.0) / (sv_V(a, iv - 1) - V);
+    }
+    // clamp, drift of the clamped stencil, fix-up
+    double drift = 0.0;
+    for (int j = 0; j < 6; j++) {
+        if (c[j] < 0) continue;
+        if (v[j] < 0.0) v[j] = 0.0;
+        const int tx = c[j] % a.nx;
+        const double dxj = (tx == ix) ? 0.0 : (tx == ix - 1 ? dxm : dxp);
+        drift += v[j] * dxj;
+    }
+    if (drift > mu_x) v[0] += (drift - mu_x) / (x - xm);
+    else v[1] += (mu_x - drift) / (xp - x);
+    double tot = 0.0;
+    for (int j = 0; j < 6; j++)
+        if (c[j] >= 0) tot += v[j];
+    v[6] = -tot;
+    for (int j = 0; j < 7; j++) {
+        cols[7LL * y + j] = c[j];
+        vals[7LL * y + j] = c[j] >= 0 ? v[j] : 0.0;
+    }
+}
+
+// max over rows of |L_yy| for an ELL generator (column == row entry).
+__global__ void k_maxdiag(int d, int w, const int *__restrict__ cols, const double *__restrict__ vals,
+                          unsigned long long *__restrict__ out_bits) {
+    double m = 0.0;
+    for (int y = blockIdx.x * blockDim.x + threadIdx.x; y < d; y += gridDim.x * blockDim.x)
+        for (int j = 0; j < w; j++)
+            if (cols[(long long)y * w + j] == y) m = fmax(m, fabs(vals[(long long)y * w + j]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out_bits, (unsigned long long)__double_as_longlong(m));  // m >= 0
+}
+
+}  // namespace opb
+
+using namespace opb;
+
+OPB_API int opb_lv_params(int d, double lo, double hi, double s0, double level, double skew, double width,
+                          double floor_, double r, double *x, double *drift, double *vol) {
+    OPB_REQUIRE(d >= 3, OPB_E_ARG);
+    OPB_REQUIRE(x && drift && vol, OPB_E_NULL);
+    OPB_REQUIRE(lo > 0.0 && hi > lo && width > 0.0, OPB_E_ARG);
+    k_lv_params<<<(d + 255) / 256, 256, 0, stream()>>>(d, lo, hi, s0, level, skew, width, floor_, r, x, drift, vol);
+    return launch_check();
+}
+
+// LV generator in ELL form (width 3) from per-node spot values, drifts and vols.
+OPB_API int opb_lv_generator_ell(int d, const double *x, const double *drift, const double *vol, int *cols,
+                                 double *vals) {
+    OPB_REQUIRE(d >= 3, OPB_E_ARG);
+    OPB_REQUIRE(x && drift && vol && cols && vals, OPB_E_NULL);
+    k_lv_ell<<<(d + 255) / 256, 256, 0, stream()>>>(d, x, drift, vol, cols, vals);
+    return launch_check();
+}
+
+// SV generator in ELL form (width 7); x_y (optional) receives the spot value per state.
+OPB_API int opb_sv_generator_ell(int nx, int nv, double x_lo, double x_hi, double v_lo, double v_hi, double r,
+                                 double kappa, double theta, double xi, double rho, int *cols, double *vals,
+                                 double *x_y) {
+    OPB_REQUIRE(nx >= 3 && nv >= 3, OPB_E_ARG);
+    OPB_REQUIRE(x_lo > 0.0 && x_hi > x_lo && v_lo > 0.0 && v_hi > v_lo && xi >= 0.0, OPB_E_ARG);
+    OPB_REQUIRE(rho > -1.0 && rho < 1.0, OPB_E_ARG);
+    OPB_REQUIRE(cols && vals, OPB_E_NULL);
+    SvArgs a{nx, nv, x_lo, x_hi, v_lo, v_hi, r, kappa, theta, xi, rho};
+    int d = nx * nv;
+    k_sv_ell<<<(d + 127) / 128, 128, 0, stream()>>>(a, cols, vals, x_y);
+    return launch_check();
+}
+
+// max |L_yy| (blocking: the value is returned to the host for the squaring plan).
+// dscratch: one device word (8 bytes) owned by the caller.
+OPB_API int opb_ell_maxdiag(int d, int w, const int *cols, const double *vals, unsigned long long *dscratch,
+                            double *out_host) {
+    OPB_REQUIRE(d > 0 && w > 0, OPB_E_ARG);
+    OPB_REQUIRE(cols && vals && dscratch && out_host, OPB_E_NULL);
+    OPB_TRY(cudaMemsetAsync(dscratch, 0, sizeof(unsigned long long), stream()));
+    int g = (d + 255) / 256;
+    k_maxdiag<<<g < 1024 ? g : 1024, 256, 0, stream()>>>(d, w, cols, vals, dscratch);
+    unsigned long long bits = 0;
+    OPB_TRY(cudaMemcpyAsync(&bits, dscratch, sizeof(bits), cudaMemcpyDeviceToHost, stream()));
+    OPB_TRY(cudaStreamSynchronize(stream()));
+    double v;
+    std::memcpy(&v, &bits, sizeof(v));
+    *out_host = v;
+    return set_status(OPB_OK);
+}

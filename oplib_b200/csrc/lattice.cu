@@ -1,0 +1,260 @@
+// Lattice solve: U0 = I + dt*L (FP64 build) -> niter squarings -> chaining to nmat
+// maturities -> backward induction of call payoffs -> FP64 discounting -> quotes.
+//
+// This is the device half of the reference's CModel.exe_mc_plan on the device branch
+// (oplib/opmodel/models/CModel Common.cs:651-669 -> device_mc_sfex, sminit, smk, smcopy;
+// CModel Device.cs:186-295), restated for one interval length (period) and a maturity
+// ladder T_m = m * period, m = 1..nmat, plus the payoff induction V_m = P(T_m) . G that
+// the reference exposes as sgemv kernels (oplib/opcuda/sgemv3.cu, sgemv4.cu).
+//
+// Precision modes
+//   OPB_FP32_PLAIN   : FP32 SIMT squaring and chaining exactly as the reference's FP32
+//                      device path (no renormalisation).
+//   OPB_FP32_RENORM  : the same with FP64 row renormalisation after every product.
+//   OPB_BF16X3       : split-BF16 tensor-core products.  Squaring runs on E = U - I
+//                      (E' = 2E + E.E, so the O(dt*L) information in U0 is not lost to
+//                      BF16 rounding of entries near 1), FP64 row renormalisation after
+//                      every product, chaining and pricing in split-BF16 as well.
+// All launches go to the library stream without host synchronisation, so a whole solve
+// can be captured in a CUDA graph.  The caller owns every buffer (workspace included),
+// as with the reference's CArray buffers (oplib/opmodel/types/CArray.cs:550-590).
+#include <cmath>
+
+#include "common.cuh"
+#include "lattice.h"
+
+enum { OPB_FP32_PLAIN = 0, OPB_FP32_RENORM = 1, OPB_BF16X3 = 2 };
+
+struct opb_lattice_desc {
+    int d;                     // states
+    int y0;                    // quoted state
+    int ell_width;             // > 0: generator given as ELL (gen_cols, gen_vals); 0: dense gen_dense
+    const int *gen_cols;       // device [d * ell_width], column index or -1
+    const double *gen_vals;    // device [d * ell_width], FP64 rates
+    const double *gen_dense;   // device [d * d] FP64, row-major (source-major)
+    const double *x;           // device [d] spot value per state
+    double dt;                 // elementary step: period * 2^-niter
+    int niter;                 // squarings
+    int nmat;                  // maturities T_m = m * period
+    double period;
+    double rate;               // continuously compounded discount rate
+    int nK;                    // strikes
+    const double *strikes;     // device [nK]
+};
+
+namespace {
+
+struct Ws {
+    // carve a workspace into 256-byte aligned pieces
+    char *p;
+    size_t used;
+    template <class T>
+    T *take(size_t n) {
+        size_t off = (used + 255) & ~size_t(255);
+        T *r = reinterpret_cast<T *>(p ? p + off : nullptr);
+        used = off + n * sizeof(T);
+        return r;
+    }
+};
+
+struct Bufs {
+    float *X, *Pa, *Pb, *G, *V;
+    __nv_bfloat16 *Ahi, *Alo, *Bhi, *Blo, *GThi, *GTlo;
+    double *part;
+};
+
+Bufs carve(Ws &w, int d, int nK, int mode) {
+    Bufs b{};
+    size_t dd = (size_t)d * d;
+    b.X = w.take<float>(dd);
+    b.Pa = w.take<float>(dd);
+    if (mode != OPB_BF16X3) b.Pb = w.take<float>(dd);
+    b.V = w.take<float>((size_t)d * nK);
+    if (mode == OPB_BF16X3) {
+        b.Ahi = w.take<__nv_bfloat16>(dd);
+        b.Alo = w.take<__nv_bfloat16>(dd);
+        b.Bhi = w.take<__nv_bfloat16>(dd);
+        b.Blo = w.take<__nv_bfloat16>(dd);
+        b.GThi = w.take<__nv_bfloat16>((size_t)d * nK);
+        b.GTlo = w.take<__nv_bfloat16>((size_t)d * nK);
+        int np = opb::tc_gemm_nparts(d);
+        b.part = w.take<double>((size_t)(np > 0 ? np : 1) * d);
+    } else {
+        b.G = w.take<float>((size_t)d * nK);
+        b.part = w.take<double>((size_t)d);
+    }
+    return b;
+}
+
+#define LT(expr)                         \
+    do {                                 \
+        int _r = (expr);                 \
+        if (_r != 0) return _r;          \
+    } while (0)
+
+int solve_fp32(const opb_lattice_desc &L, int mode, Bufs &b, double *quotes, double *V_all, cudaStream_t s,
+               float *P_out) {
+    const int d = L.d, nK = L.nK;
+    // U0 in FP32 from FP64 arithmetic
+    if (L.ell_width > 0) LT(opb::launch_ek_ell(d, L.ell_width, L.gen_cols, L.gen_vals, L.dt, 0, b.X, s));
+    else LT(opb::launch_ek_dense(d, L.gen_dense, L.dt, 0, b.X, s));
+    float *buf[3] = {b.X, b.Pa, b.Pb};
+    int cur = 0, nxt = 1;
+    for (int r = 0; r < L.niter; r++) {
+        LT(opb::sgemm_rm(d, d, d, 1.f, buf[cur], d, buf[cur], d, 0.f, buf[nxt], d, s));
+        if (mode == OPB_FP32_RENORM) {
+            LT(opb::launch_rowsum(d, buf[nxt], b.part, s));
+            LT(opb::launch_renorm(d, buf[nxt], b.part, 1, 0, nullptr, nullptr, nullptr, nullptr, s));
+        }
+        int t = cur; cur = nxt; nxt = t;
+    }
+    // buf[cur] = P(period); the chain alternates between the two other buffers
+    float *P1 = buf[cur];
+    if (P_out) return (int)cudaMemcpyAsync(P_out, P1, sizeof(float) * (size_t)d * d, cudaMemcpyDeviceToDevice, s);
+    float *chain[2];
+    for (int i = 0, k = 0; i < 3; i++)
+        if (i != cur) chain[k++] = buf[i];
+    LT(opb::launch_payoff(d, nK, L.x, L.strikes, b.G, nullptr, nullptr, s));
+    const float *Pm = P1;
+    for (int m = 1; m <= L.nmat; m++) {
+        if (m > 1) {
+            float *out = chain[m & 1 ? 1 : 0];
+            LT(opb::sgemm_rm(d, d, d, 1.f, Pm, d, P1, d, 0.f, out, d, s));
+            if (mode == OPB_FP32_RENORM) {
+                LT(opb::launch_rowsum(d, out, b.part, s));
+                LT(opb::launch_renorm(d, out, b.part, 1, 0, nullptr, nullptr, nullptr, nullptr, s));
+            }
+            Pm = out;
+        }
+        LT(opb::sgemm_rm(d, nK, d, 1.f, Pm, d, b.G, nK, 0.f, b.V, nK, s));
+        const double disc = std::exp(-L.rate * L.period * m);
+        LT(opb::launch_discount(d, nK, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d * nK : nullptr, L.y0,
+                                quotes + (size_t)(m - 1) * nK, s));
+    }
+    return 0;
+}
+
+int solve_bf16x3(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, cudaStream_t s, float *P_out) {
+    const int d = L.d, nK = L.nK;
+    const int np = opb::tc_gemm_nparts(d);
+    // E0 = dt*L in FP32 (FP64 arithmetic), then its splits
+    if (L.ell_width > 0) LT(opb::launch_ek_ell(d, L.ell_width, L.gen_cols, L.gen_vals, L.dt, 1, b.X, s));
+    else LT(opb::launch_ek_dense(d, L.gen_dense, L.dt, 1, b.X, s));
+    LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s));
+    opb::TcGemmArgs g{};
+    g.M = d; g.N = d; g.K = d; g.lda = d; g.ldb = d; g.ldc = d;
+    g.Ahi = b.Ahi; g.Alo = b.Alo; g.Bhi = b.Bhi; g.Blo = b.Blo;
+    for (int r = 0; r < L.niter; r++) {
+        // D = 2E + E.E in place of E, with FP64 row-sum partials
+        g.C = b.X; g.Cin = b.X; g.alpha = 1.f; g.beta = 2.f; g.rowsum = b.part;
+        LT(opb::launch_tc_gemm(g, s));
+        const bool last = (r + 1 == L.niter);
+        LT(opb::launch_renorm(d, b.X, b.part, np, 1, last ? nullptr : b.Ahi, b.Alo, last ? nullptr : b.Bhi, b.Blo, s));
+    }
+    // P1 = I + E; splits of P1 (row-major: A of the first chain / pricing; transposed: B of every chain)
+    LT(opb::launch_add_identity(d, b.X, s));
+    if (P_out) return (int)cudaMemcpyAsync(P_out, b.X, sizeof(float) * (size_t)d * d, cudaMemcpyDeviceToDevice, s);
+    LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s));
+    LT(opb::launch_payoff(d, nK, L.x, L.strikes, nullptr, b.GThi, b.GTlo, s));
+    opb::TcGemmArgs pg{};
+    pg.M = d; pg.N = nK; pg.K = d; pg.lda = d; pg.ldb = d; pg.ldc = nK;
+    pg.Ahi = b.Ahi; pg.Alo = b.Alo; pg.Bhi = b.GThi; pg.Blo = b.GTlo; pg.C = b.V; pg.alpha = 1.f; pg.beta = 0.f;
+    for (int m = 1; m <= L.nmat; m++) {
+        if (m > 1) {
+            // P_m = P_{m-1} . P1 (A splits hold P_{m-1}), renormalise, split row-major into A
+            g.C = b.Pa; g.Cin = nullptr; g.alpha = 1.f; g.beta = 0.f; g.rowsum = b.part;
+            LT(opb::launch_tc_gemm(g, s));
+            LT(opb::launch_renorm(d, b.Pa, b.part, np, 0, b.Ahi, b.Alo, nullptr, nullptr, s));
+        }
+        LT(opb::launch_tc_gemm(pg, s));
+        const double disc = std::exp(-L.rate * L.period * m);
+        LT(opb::launch_discount(d, nK, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d * nK : nullptr, L.y0,
+                                quotes + (size_t)(m - 1) * nK, s));
+    }
+    return 0;
+}
+
+int check_desc(const opb_lattice_desc *L, int mode) {
+    if (!L) return OPB_E_NULL;
+    if (L->d <= 0 || L->y0 < 0 || L->y0 >= L->d || L->niter < 0 || L->nmat < 1 || L->nK < 1) return OPB_E_ARG;
+    if (!(L->dt > 0.0) || !(L->period > 0.0)) return OPB_E_ARG;
+    if (!L->x || !L->strikes) return OPB_E_NULL;
+    if (L->ell_width > 0) {
+        if (!L->gen_cols || !L->gen_vals) return OPB_E_NULL;
+    } else if (!L->gen_dense) {
+        return OPB_E_NULL;
+    }
+    if (mode < OPB_FP32_PLAIN || mode > OPB_BF16X3) return OPB_E_ARG;
+    if (mode == OPB_BF16X3) {
+        if (L->d % 128 != 0) return OPB_E_UNSUPPORTED;
+        if (!opb::tc_gemm_tile_n(L->nK) || opb::tc_gemm_tile_n(L->d) == 0) return OPB_E_UNSUPPORTED;
+    }
+    return OPB_OK;
+}
+
+}  // namespace
+
+// Workspace bytes for opb_lattice_solve.
+OPB_API unsigned long long opb_lattice_workspace_size(int d, int nK, int mode) {
+    if (d <= 0 || nK <= 0) return 0;
+    Ws w{nullptr, 0};
+    (void)carve(w, d, nK, mode);
+    return (unsigned long long)w.used + 256;
+}
+
+// Solves one lattice.  quotes: device [nmat * nK] FP64 (quotes[(m-1)*nK + k] is the
+// price at state y0 of the call with strike k and maturity m*period).  V_all (optional):
+// device [nmat * d * nK] FP64 prices at every state.  workspace: device, at least
+// opb_lattice_workspace_size(d, nK, mode) bytes.
+OPB_API int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
+                              double *quotes, double *V_all) {
+    int c = check_desc(L, mode);
+    if (c == OPB_OK && !quotes) c = OPB_E_NULL;
+    if (c != OPB_OK) return opb::set_status(c);
+    OPB_REQUIRE(workspace, OPB_E_NULL);
+    OPB_REQUIRE(ws_bytes >= opb_lattice_workspace_size(L->d, L->nK, mode), OPB_E_ARG);
+    Ws w{reinterpret_cast<char *>(workspace), 0};
+    size_t off = (256 - (reinterpret_cast<uintptr_t>(workspace) & 255)) & 255;
+    w.p += off;
+    Bufs b = carve(w, L->d, L->nK, mode);
+    cudaStream_t s = opb::stream();
+    int r = (mode == OPB_BF16X3) ? solve_bf16x3(*L, b, quotes, V_all, s, nullptr)
+                                 : solve_fp32(*L, mode, b, quotes, V_all, s, nullptr);
+    return opb::set_status(r);
+}
+
+// Transition kernel only: P_out (device, d x d FP32, source-major) = P(period) after
+// niter squarings of U0 (no chaining, no pricing; nmat, nK and strikes are ignored).
+OPB_API int opb_lattice_kernel(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
+                               float *P_out) {
+    OPB_REQUIRE(L != nullptr, OPB_E_NULL);
+    opb_lattice_desc L2 = *L;
+    L2.nmat = 1;
+    if (L2.nK < 1) L2.nK = 64;
+    if (!L2.strikes) L2.strikes = reinterpret_cast<const double *>(L2.x);
+    int c = check_desc(&L2, mode);
+    if (c != OPB_OK) return opb::set_status(c);
+    OPB_REQUIRE(workspace && P_out, OPB_E_NULL);
+    OPB_REQUIRE(ws_bytes >= opb_lattice_workspace_size(L2.d, L2.nK, mode), OPB_E_ARG);
+    Ws w{reinterpret_cast<char *>(workspace), 0};
+    size_t off = (256 - (reinterpret_cast<uintptr_t>(workspace) & 255)) & 255;
+    w.p += off;
+    Bufs b = carve(w, L2.d, L2.nK, mode);
+    cudaStream_t s = opb::stream();
+    int r = (mode == OPB_BF16X3) ? solve_bf16x3(L2, b, nullptr, nullptr, s, P_out)
+                                 : solve_fp32(L2, mode, b, nullptr, nullptr, s, P_out);
+    return opb::set_status(r);
+}
+
+// The reference's plan rule for one interval (oplib/opmodel/models/CModel Common.cs:289-307):
+// dt = min(0.5 / maxdiag, dt0), niter = ceil(log2(DeltaT / dt)), dt_j = DeltaT * 2^-niter.
+OPB_API int opb_plan_interval(double maxdiag, double delta_t, double dt0, int *niter, double *dt_j) {
+    OPB_REQUIRE(niter && dt_j, OPB_E_NULL);
+    OPB_REQUIRE(delta_t > 0.0 && dt0 > 0.0 && maxdiag >= 0.0, OPB_E_ARG);
+    double dt = maxdiag > 0.0 ? 0.5 / maxdiag : dt0;
+    if (dt > dt0) dt = dt0;
+    int n = (int)std::ceil(std::log(delta_t / dt) / std::log(2.0));
+    *niter = n;
+    *dt_j = delta_t * std::pow(2.0, -n);
+    return opb::set_status(OPB_OK);
+}

@@ -1,0 +1,53 @@
+// Internal launcher declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace opb {
+
+// gemm_simt.cu
+int sgemm_rm(int M, int N, int K, float alpha, const float *A, int lda, const float *B, int ldb, float beta,
+             float *C, int ldc, cudaStream_t s);
+
+// lattice_kernels.cu
+int launch_ek_ell(int d, int w, const int *cols, const double *vals, double dt, int eform, float *out,
+                  cudaStream_t s);
+int launch_ek_dense(int d, const double *L, double dt, int eform, float *out, cudaStream_t s);
+int launch_split(int rows, int cols, const float *X, long long ld, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
+                 __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, long long ldt, cudaStream_t s);
+int launch_rowsum(int d, const float *X, double *partial, cudaStream_t s);
+int launch_renorm(int d, float *X, const double *partial, int nparts, int eform, __nv_bfloat16 *Ahi,
+                  __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s);
+int launch_add_identity(int d, float *X, cudaStream_t s);
+int launch_payoff(int d, int nK, const double *x, const double *K, float *G, __nv_bfloat16 *GThi,
+                  __nv_bfloat16 *GTlo, cudaStream_t s);
+int launch_discount(int d, int nK, const float *V32, double disc, double *V64, int y0, double *quotes,
+                    cudaStream_t s);
+
+// gemm_tc.cu -- split-BF16 tensor-core GEMM.
+//   C[M,N] = alpha * (Ahi.Bhi^T + Ahi.Blo^T + Alo.Bhi^T) + beta * Cin[M,N]
+// A* are M x K row-major (K-major), B* are N x K row-major (the K-major form of the
+// K x N right operand).  If rowsum != nullptr the epilogue writes FP64 partial row sums
+// of the stored C values: rowsum[(n-tile) * M + row].
+struct TcGemmArgs {
+    int M, N, K;
+    const __nv_bfloat16 *Ahi, *Alo, *Bhi, *Blo;
+    long long lda, ldb;   // elements
+    float *C;
+    long long ldc;
+    const float *Cin;     // may alias C
+    float alpha, beta;
+    double *rowsum;       // optional
+};
+int tc_gemm_tile_n(int N);                    // tile width chosen for N (0 if unsupported)
+int tc_gemm_check(const TcGemmArgs &a);       // argument/alignment check, OPB_* code
+int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s);
+int tc_gemm_nparts(int N);                    // number of row-sum partials written
+
+// sck.cu
+int launch_sck_rm(int d, int nrows, const float *P, float *C, cudaStream_t s);
+int launch_guide(int d, int nrows, int nb, const float *C, uint32_t *guide, cudaStream_t s);
+
+}  // namespace opb

@@ -1,0 +1,312 @@
+// Element-wise and row-wise kernels of the lattice path (all HBM-bound).
+//
+// Storage is source-major (row y = source state, element (y, z) at y*d + z); it is the
+// transpose of the reference's (y1 + d*y2) storage, so a row here is a column there.
+//
+//   ek       : U0 = I + dt*L built in FP64 on the device and rounded once to FP32, or
+//              its "E-form" E0 = U0 - I = dt*L (oplib/opcuda/sek.cu:40-59;
+//              oplib/opmodel/models/CModel Host Double.cs:89-121).
+//   renorm   : FP64 row sums, then every row divided by its sum (probability
+//              conservation after each squaring; no reference counterpart).  In E-form
+//              the identity is carried implicitly: with D = 2E + E.E and s = 1 + sum(D_y.),
+//              E_new[y,z] = (D[y,z] - [z==y]*sum(D_y.)) / s_y, which equals
+//              (I + D)/s - I exactly.
+//   split    : a = hi + lo with hi = bf16(a), lo = bf16(a - hi), written row-major (the
+//              K-major A operand) and transposed (the K-major B operand) for the
+//              tensor-core GEMM.
+//   payoff / discount : call payoffs G[z,k] = (x_z - K_k)^+ and the FP64 discounting of
+//              the backward-induction result.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "lattice.h"
+
+namespace opb {
+
+__global__ void k_zero_set_diag(int d, float *__restrict__ U, float v) {
+    int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y < d) U[(long long)y * d + y] = v;
+}
+
+// ELL generator: row y holds w (col, val) pairs; col < 0 marks padding.
+__global__ void k_ek_scatter_ell(int d, int w, const int *__restrict__ cols, const double *__restrict__ vals,
+                                 double dt, int eform, float *__restrict__ out, long long ld) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)d * w) return;
+    int y = (int)(t / w);
+    int z = cols[t];
+    if (z < 0 || z >= d) return;
+    double v = dt * vals[t];
+    if (!eform && z == y) v += 1.0;
+    out[(long long)y * ld + z] = (float)v;
+}
+
+// Dense FP64 generator, row-major (source-major).
+__global__ void k_ek_dense(int d, const double *__restrict__ L, double dt, int eform, float *__restrict__ out) {
+    long long n = (long long)d * d;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int y = (int)(t / d), z = (int)(t - (long long)y * d);
+        double v = dt * L[t];
+        if (!eform && z == y) v += 1.0;
+        out[t] = (float)v;
+    }
+}
+
+__device__ __forceinline__ void split2(float f, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+    hi = __float2bfloat16_rn(f);
+    lo = __float2bfloat16_rn(f - __bfloat162float(hi));  // exact difference in FP32
+}
+
+// 32x32 tiles, 256 threads.  X is (rows x cols) row-major with leading dimension ld.
+// Writes hi/lo of X (row-major, ld) and of X^T (cols x rows, leading dimension ldt).
+__global__ void k_split_tr(int rows, int cols, const float *__restrict__ X, long long ld,
+                           __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
+                           __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo, long long ldt) {
+    __shared__ __nv_bfloat16 th[32][34], tl[32][34];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+#pragma unroll
+    for (int i = ty; i < 32; i += 8) {
+        int r = r0 + i, c = c0 + tx;
+        __nv_bfloat16 h = __float2bfloat16_rn(0.f), l = h;
+        if (r < rows && c < cols) {
+            split2(X[(long long)r * ld + c], h, l);
+            if (Ahi) {
+                Ahi[(long long)r * ld + c] = h;
+                Alo[(long long)r * ld + c] = l;
+            }
+        }
+        th[i][tx] = h;
+        tl[i][tx] = l;
+    }
+    if (!Bhi) return;
+    __syncthreads();
+#pragma unroll
+    for (int i = ty; i < 32; i += 8) {
+        int c = c0 + i, r = r0 + tx;
+        if (r < rows && c < cols) {
+            Bhi[(long long)c * ldt + r] = th[tx][i];
+            Blo[(long long)c * ldt + r] = tl[tx][i];
+        }
+    }
+}
+
+// FP64 row sums of an FP32 matrix, one block per row -> partial[row].
+__global__ void k_rowsum(int d, const float *__restrict__ X, double *__restrict__ partial) {
+    const int y = blockIdx.x;
+    const float *row = X + (long long)y * d;
+    double s = 0.0;
+    for (int z = threadIdx.x; z < d; z += blockDim.x) s += (double)row[z];
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) partial[y] = s;
+    }
+}
+
+// Row renormalisation from FP64 row-sum partials (nparts partial sums per row, laid out
+// partial[p*d + y]).  In place on X; optionally emits the hi/lo split of the result
+// (row-major and transposed).
+__global__ void k_renorm(int d, float *__restrict__ X, const double *__restrict__ partial, int nparts, int eform,
+                         __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
+                         __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo) {
+    __shared__ double s_sum[32], s_inv[32];
+    __shared__ __nv_bfloat16 th[32][34], tl[32][34];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    if (ty == 0) {
+        double s = 0.0;
+        int r = r0 + tx;
+        if (r < d)
+            for (int p = 0; p < nparts; p++) s += partial[(long long)p * d + r];
+        s_sum[tx] = s;
+        double den = eform ? 1.0 + s : s;
+        s_inv[tx] = den != 0.0 ? 1.0 / den : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = ty; i < 32; i += 8) {
+        int r = r0 + i, c = c0 + tx;
+        __nv_bfloat16 h = __float2bfloat16_rn(0.f), l = h;
+        if (r < d && c < d) {
+            long long o = (long long)r * d + c;
+            double v = (double)X[o];
+            if (eform && r == c) v -= s_sum[i];
+            float f = (float)(v * s_inv[i]);
+            X[o] = f;
+            if (Ahi) {
+                split2(f, h, l);
+                Ahi[o] = h;
+                Alo[o] = l;
+            }
+        }
+        th[i][tx] = h;
+        tl[i][tx] = l;
+    }
+    if (!Bhi) return;
+    __syncthreads();
+#pragma unroll
+    for (int i = ty; i < 32; i += 8) {
+        int c = c0 + i, r = r0 + tx;
+        if (r < d && c < d) {
+            Bhi[(long long)c * d + r] = th[tx][i];
+            Blo[(long long)c * d + r] = tl[tx][i];
+        }
+    }
+}
+
+// E-form -> P-form: P = I + E (in place), FP32.
+__global__ void k_add_identity(int d, float *__restrict__ X) {
+    int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y < d) {
+        long long o = (long long)y * d + y;
+        X[o] = (float)(1.0 + (double)X[o]);
+    }
+}
+
+// G[z, k] = (x_z - K_k)^+ (FP32, d x nK row-major) and its split transpose
+// G^T hi/lo (nK x d) for the tensor-core pricing GEMM.
+__global__ void k_payoff(int d, int nK, const double *__restrict__ x, const double *__restrict__ K,
+                         float *__restrict__ G, __nv_bfloat16 *__restrict__ GThi, __nv_bfloat16 *__restrict__ GTlo) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)d * nK) return;
+    int z = (int)(t / nK), k = (int)(t - (long long)z * nK);
+    double g = x[z] - K[k];
+    float f = (float)(g > 0.0 ? g : 0.0);
+    if (G) G[t] = f;
+    if (GThi) {
+        __nv_bfloat16 h, l;
+        split2(f, h, l);
+        GThi[(long long)k * d + z] = h;
+        GTlo[(long long)k * d + z] = l;
+    }
+}
+
+// V64[y, k] = disc * V32[y, k]; quotes[k] = V64[y0, k].
+__global__ void k_discount(int d, int nK, const float *__restrict__ V32, double disc, double *__restrict__ V64,
+                           int y0, double *__restrict__ quotes) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)d * nK) return;
+    double v = disc * (double)V32[t];
+    if (V64) V64[t] = v;
+    int y = (int)(t / nK);
+    if (quotes && y == y0) quotes[t - (long long)y * nK] = v;
+}
+
+// ------------------------------------------------------------------ host launchers
+
+static inline int blocks_for(long long n, int threads) { return (int)((n + threads - 1) / threads); }
+
+int launch_ek_ell(int d, int w, const int *cols, const double *vals, double dt, int eform, float *out,
+                  cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float) * (size_t)d * d, s);
+    if (e != cudaSuccess) return (int)e;
+    if (!eform) k_zero_set_diag<<<blocks_for(d, 256), 256, 0, s>>>(d, out, 1.0f);
+    long long n = (long long)d * w;
+    if (n > 0) k_ek_scatter_ell<<<blocks_for(n, 256), 256, 0, s>>>(d, w, cols, vals, dt, eform, out, d);
+    return (int)cudaGetLastError();
+}
+
+int launch_ek_dense(int d, const double *L, double dt, int eform, float *out, cudaStream_t s) {
+    long long n = (long long)d * d;
+    int b = blocks_for(n, 256);
+    int cap = 16 * num_sms();
+    k_ek_dense<<<b < cap ? b : cap, 256, 0, s>>>(d, L, dt, eform, out);
+    return (int)cudaGetLastError();
+}
+
+int launch_split(int rows, int cols, const float *X, long long ld, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
+                 __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, long long ldt, cudaStream_t s) {
+    dim3 g((cols + 31) / 32, (rows + 31) / 32);
+    k_split_tr<<<g, 256, 0, s>>>(rows, cols, X, ld, Ahi, Alo, Bhi, Blo, ldt);
+    return (int)cudaGetLastError();
+}
+
+int launch_rowsum(int d, const float *X, double *partial, cudaStream_t s) {
+    k_rowsum<<<d, 256, 0, s>>>(d, X, partial);
+    return (int)cudaGetLastError();
+}
+
+int launch_renorm(int d, float *X, const double *partial, int nparts, int eform, __nv_bfloat16 *Ahi,
+                  __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s) {
+    dim3 g((d + 31) / 32, (d + 31) / 32);
+    k_renorm<<<g, 256, 0, s>>>(d, X, partial, nparts, eform, Ahi, Alo, Bhi, Blo);
+    return (int)cudaGetLastError();
+}
+
+int launch_add_identity(int d, float *X, cudaStream_t s) {
+    k_add_identity<<<blocks_for(d, 256), 256, 0, s>>>(d, X);
+    return (int)cudaGetLastError();
+}
+
+int launch_payoff(int d, int nK, const double *x, const double *K, float *G, __nv_bfloat16 *GThi,
+                  __nv_bfloat16 *GTlo, cudaStream_t s) {
+    long long n = (long long)d * nK;
+    k_payoff<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, x, K, G, GThi, GTlo);
+    return (int)cudaGetLastError();
+}
+
+int launch_discount(int d, int nK, const float *V32, double disc, double *V64, int y0, double *quotes,
+                    cudaStream_t s) {
+    long long n = (long long)d * nK;
+    k_discount<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, V32, disc, V64, y0, quotes);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace opb
+
+// ------------------------------------------------------------------ reference ek entry points
+
+// U = I + dt*gen for a column-major d x d FP32 generator (oplib/opcuda/sek.cu:40-59,106-115).
+// The sum is formed in FP64 and rounded once.
+__global__ void k_sek(int d, const float *__restrict__ gen, float dt, float *__restrict__ out,
+                      const float *__restrict__ r, const float *__restrict__ lambda) {
+    long long n = (long long)d * d;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int y1 = (int)(t % d), y2 = (int)(t / d);  // column-major: t = y1 + d*y2
+        double v = (double)dt * (double)gen[t] + (y1 == y2 ? 1.0 : 0.0);
+        if (r) {
+            double rr = (double)r[y1];
+            if (lambda) rr *= (double)lambda[0];
+            v /= 1.0 + (double)dt * rr;  // oplib/opcuda/sek.cu:78,100
+        }
+        out[t] = (float)v;
+    }
+}
+
+static int sek_common(int d, uint64_t gen, float dt, uint64_t tpk, uint64_t r, uint64_t lambda) {
+    OPB_REQUIRE(d >= 0, OPB_E_ARG);
+    if (d == 0) return opb::set_status(OPB_OK);
+    OPB_REQUIRE(gen != 0 && tpk != 0, OPB_E_NULL);
+    long long n = (long long)d * d;
+    int b = (int)((n + 255) / 256);
+    int cap = 16 * opb::num_sms();
+    k_sek<<<b < cap ? b : cap, 256, 0, opb::stream()>>>(d, reinterpret_cast<const float *>(gen), dt,
+                                                         reinterpret_cast<float *>(tpk),
+                                                         reinterpret_cast<const float *>(r),
+                                                         reinterpret_cast<const float *>(lambda));
+    return opb::launch_check();
+}
+
+OPB_API int opcuda_sek(int d, uint64_t genPtr, float dt, uint64_t tpkerPtr) {
+    return sek_common(d, genPtr, dt, tpkerPtr, 0, 0);
+}
+
+OPB_API int opcuda_sekd(int d, uint64_t genPtr, float dt, uint64_t tpkerPtr, uint64_t rPtr) {
+    OPB_REQUIRE(rPtr != 0, OPB_E_NULL);
+    return sek_common(d, genPtr, dt, tpkerPtr, rPtr, 0);
+}
+
+OPB_API int opcuda_sekd_lambda(int d, uint64_t genPtr, float dt, uint64_t tpkerPtr, uint64_t rPtr,
+                               uint64_t lambdaPtr) {
+    OPB_REQUIRE(rPtr != 0 && lambdaPtr != 0, OPB_E_NULL);
+    return sek_common(d, genPtr, dt, tpkerPtr, rPtr, lambdaPtr);
+}

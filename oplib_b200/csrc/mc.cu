@@ -1,0 +1,340 @@
+// Markov-chain Monte Carlo on a lattice, driven by one MT19937 stream per path.
+//
+// Path p draws its uniforms from MT19937 seeded with init_genrand(seed + p) (Matsumoto &
+// Nishimura 1998; the seeding recurrence 1812433253*(x ^ x>>30) + i is the one the
+// reference's twisters use, oplib/opcuda/smc.cu:127-131) and consumes the first
+// genrand_int32 outputs in order, one per step.  Each step converts the output to
+// u = ((float)x + 1.0f) * 2^-32 in (0, 1] (oplib/opcuda/smc.cu:329) and moves to the
+// smallest state z with u < C[y, z], capped at d-1 (oplib/opcuda/smc.cu:336-350).
+//
+// B200 design: one thread per path with the whole generator in registers.  The first
+// n <= 623 outputs of a freshly seeded MT19937 only need one regeneration of the state,
+// and every regenerated word is an XOR of tw() terms of initial words mt[j], each of
+// which is a forward recurrence from the seed.  The kernel walks that recurrence with a
+// few cursors (and one saved word, mt[397]) instead of storing 624 words per path, so
+// no local or shared memory is used for RNG state:
+//   i <  227 : mt'[i] = mt[i+397] ^ tw(mt[i], mt[i+1])
+//   i <  454 : mt'[i] = mt[i+170] ^ tw(mt[i-227], mt[i-226]) ^ tw(mt[i], mt[i+1])
+//   i <  623 : mt'[i] = mt[i-57] ^ tw(mt[i-454], mt[i-453]) ^ tw(mt[i-227], mt[i-226])
+//                       ^ tw(mt[i], mt[i+1])
+// The inverse-CDF search starts from the guide-table bracket of the previous state's row
+// (about one probe per step) and falls back to the full row without a guide table.
+// Payoffs (discretely monitored down-and-out call, arithmetic-Asian call) are reduced per
+// path in registers and per block in FP64; the optional int16 state output uses the
+// reference's layout y_sk[path + npaths*k] (oplib/opcuda/smc.cu:331).
+#include "common.cuh"
+#include "lattice.h"
+
+namespace opb {
+
+__device__ __forceinline__ uint32_t mt_init_next(uint32_t v, uint32_t i) {
+    return 1812433253u * (v ^ (v >> 30)) + i;
+}
+__device__ __forceinline__ uint32_t mt_tw(uint32_t a, uint32_t b) {
+    uint32_t y = (a & 0x80000000u) | (b & 0x7fffffffu);
+    return (y >> 1) ^ ((b & 1u) ? 0x9908b0dfu : 0u);
+}
+__device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
+    y ^= (y >> 11);
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= (y >> 18);
+    return y;
+}
+
+// Calls f(k, x_k) for the first n (<= 623) outputs of MT19937 seeded with `seed`.
+template <class F>
+__device__ __forceinline__ void mt19937_first(uint32_t seed, int n, F &&f) {
+    // cursor A at i: (a0, a1) = (mt[i], mt[i+1])
+    uint32_t a0 = seed, a1 = mt_init_next(seed, 1u);
+    // cursor B at i + 397
+    uint32_t b = seed;
+#pragma unroll 1
+    for (uint32_t j = 1; j <= 397; j++) b = mt_init_next(b, j);
+    const uint32_t m397 = b;
+    uint32_t bi = 397;
+    int i = 0;
+    const int n1 = n < 227 ? n : 227;
+#pragma unroll 1
+    for (; i < n1; i++) {
+        f(i, mt_temper(b ^ mt_tw(a0, a1)));
+        a0 = a1; a1 = mt_init_next(a1, (uint32_t)i + 2u);
+        bi++; b = mt_init_next(b, bi);
+    }
+    if (i >= n) return;
+    // phase 2: cursor C at i-227 from the seed, cursor B restarted at 397
+    uint32_t c0 = seed, c1 = mt_init_next(seed, 1u);
+    b = m397; bi = 397;
+    const int n2 = n < 454 ? n : 454;
+#pragma unroll 1
+    for (; i < n2; i++) {
+        f(i, mt_temper(b ^ mt_tw(c0, c1) ^ mt_tw(a0, a1)));
+        a0 = a1; a1 = mt_init_next(a1, (uint32_t)i + 2u);
+        c0 = c1; c1 = mt_init_next(c1, (uint32_t)(i - 227) + 2u);
+        bi++; b = mt_init_next(b, bi);
+    }
+    if (i >= n) return;
+    // phase 3: cursor D at i-454 from the seed, B restarted at 397 (= i-57 at i = 454)
+    uint32_t d0 = seed, d1 = mt_init_next(seed, 1u);
+    b = m397; bi = 397;
+#pragma unroll 1
+    for (; i < n; i++) {
+        f(i, mt_temper(b ^ mt_tw(d0, d1) ^ mt_tw(c0, c1) ^ mt_tw(a0, a1)));
+        a0 = a1; a1 = mt_init_next(a1, (uint32_t)i + 2u);
+        c0 = c1; c1 = mt_init_next(c1, (uint32_t)(i - 227) + 2u);
+        d0 = d1; d1 = mt_init_next(d1, (uint32_t)(i - 454) + 2u);
+        bi++; b = mt_init_next(b, bi);
+    }
+}
+
+__device__ __forceinline__ float mt_uniform_open0(uint32_t x) {
+    float f = __uint2float_rn(x);
+    f = __fadd_rn(f, 1.0f);
+    return __fmul_rn(f, 2.3283064365386963e-10f);  // * 2^-32, exact
+}
+
+struct McArgs {
+    const float *C;          // cumulative rows, element (y, z) at y*rs + z*cs
+    long long rs, cs;
+    const int *m_k;          // optional: kernel index per step (matrix stride ms)
+    long long ms;
+    const uint32_t *guide;   // optional [d][nb] brackets (row-major rows only)
+    int nb;
+    int d, y0, nsteps;
+    uint32_t seed;
+    unsigned long long path0;
+    long long npaths;
+    short *ypaths;           // optional, y[p + npaths*k]
+    const double *x;         // optional node values (payoffs)
+    double strike, barrier, disc;
+    double *block_sums;      // [gridDim.x * 2]
+};
+
+__global__ void __launch_bounds__(256) k_mc(McArgs a) {
+    double s_bar = 0.0, s_asi = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const float nbf = (float)a.nb;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < a.npaths; p += stride) {
+        const uint32_t seed = a.seed + (uint32_t)(a.path0 + (unsigned long long)p);
+        int y = a.y0;
+        double xmin = 1e300, xsum = 0.0, xlast = 0.0;
+        mt19937_first(seed, a.nsteps, [&](int k, uint32_t bits) {
+            const float u = mt_uniform_open0(bits);
+            const float *row = a.C + (long long)y * a.rs + (a.m_k ? (long long)__ldg(a.m_k + k) * a.ms : 0LL);
+            int lo = 0, hi = a.d - 1;
+            if (a.guide) {
+                int bkt = (int)__fmul_rn(u, nbf);
+                bkt = bkt < a.nb ? bkt : a.nb - 1;
+                uint32_t g = __ldg(a.guide + (long long)y * a.nb + bkt);
+                lo = (int)(g & 0xffffu);
+                hi = (int)(g >> 16);
+            }
+            while (lo < hi) {
+                int mid = (lo + hi) >> 1;
+                if (u < __ldg(row + (long long)mid * a.cs)) hi = mid; else lo = mid + 1;
+            }
+            y = lo;
+            if (a.ypaths) a.ypaths[p + a.npaths * (long long)k] = (short)y;
+            if (a.x) {
+                double xv = __ldg(a.x + y);
+                xmin = xv < xmin ? xv : xmin;
+                xsum += xv;
+                xlast = xv;
+            }
+        });
+        if (a.x) {
+            double pay = xlast - a.strike;
+            if (xmin > a.barrier && pay > 0.0) s_bar += a.disc * pay;
+            double avg = xsum / (double)a.nsteps - a.strike;
+            if (avg > 0.0) s_asi += a.disc * avg;
+        }
+    }
+    if (!a.block_sums) return;
+    __shared__ double red[2][8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s_bar += __shfl_xor_sync(0xffffffffu, s_bar, o);
+        s_asi += __shfl_xor_sync(0xffffffffu, s_asi, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[0][w] = s_bar; red[1][w] = s_asi; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) { t0 += red[0][i]; t1 += red[1][i]; }
+        a.block_sums[2 * blockIdx.x] = t0;
+        a.block_sums[2 * blockIdx.x + 1] = t1;
+    }
+}
+
+// Deterministic final reduction of the per-block sums (fixed order, one block).
+__global__ void k_reduce_pairs(int n, const double *__restrict__ in, double *__restrict__ out) {
+    __shared__ double r0[256], r1[256];
+    double t0 = 0.0, t1 = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) { t0 += in[2 * i]; t1 += in[2 * i + 1]; }
+    r0[threadIdx.x] = t0; r1[threadIdx.x] = t1;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) { r0[threadIdx.x] += r0[threadIdx.x + s]; r1[threadIdx.x] += r1[threadIdx.x + s]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { out[0] = r0[0]; out[1] = r1[0]; }
+}
+
+// Uniform-generation throughput kernel (the gmt workload): stream s of nstreams writes
+// its first nper uniforms u = x * 2^-32 (oplib/opcuda/smc.cu:711-714) to
+// unif[s + nstreams*j].
+__global__ void __launch_bounds__(256) k_mt_bench(uint32_t seed, long long nstreams, int nper, float *__restrict__ unif) {
+    long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= nstreams) return;
+    mt19937_first(seed + (uint32_t)s, nper, [&](int j, uint32_t bits) {
+        unif[s + nstreams * (long long)j] = __fmul_rn(__uint2float_rn(bits), 2.3283064365386963e-10f);
+    });
+}
+
+// Raw outputs, for parity tests of the generator itself: out[s*n + j].
+__global__ void k_mt_raw(uint32_t seed, long long nstreams, int n, uint32_t *__restrict__ out) {
+    long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s >= nstreams) return;
+    mt19937_first(seed + (uint32_t)s, n, [&](int j, uint32_t bits) { out[s * n + j] = bits; });
+}
+
+int mc_grid(long long npaths) {
+    long long b = (npaths + 255) / 256;
+    long long cap = 8LL * num_sms();  // 8 x 256 threads per SM resident
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace opb
+
+using namespace opb;
+
+// Monte Carlo over npaths paths with ids path0 .. path0+npaths-1.  C holds cumulative
+// rows with element (y, z) at y*row_stride + z*col_stride (row_stride = d, col_stride = 1
+// for source-major storage; 1 and d for the reference's column-major storage).  guide
+// (optional, source-major rows only) is the opb_guide_table of C with nb buckets.
+// ypaths (optional) receives int16 states y[p + npaths*k].  x (optional, d doubles)
+// enables the fused payoffs; sums[0] / sums[1] receive the discounted barrier / Asian
+// payoff sums.  scratch must hold 2*opb_mc_scratch_blocks(npaths) doubles.
+OPB_API int opb_mc_scratch_blocks(long long npaths) { return mc_grid(npaths); }
+
+OPB_API int opb_mc_mt19937(const float *C, long long row_stride, long long col_stride, const uint32_t *guide,
+                           int nb, int d, int y0, int nsteps, uint32_t seed, unsigned long long path0,
+                           long long npaths, short *ypaths, const double *x, double strike, double barrier,
+                           double disc, double *scratch, double *sums) {
+    OPB_REQUIRE(d > 0 && d <= 32767 && y0 >= 0 && y0 < d, OPB_E_ARG);
+    OPB_REQUIRE(nsteps >= 1 && nsteps <= 623, OPB_E_UNSUPPORTED);
+    OPB_REQUIRE(npaths >= 0, OPB_E_ARG);
+    OPB_REQUIRE(C != nullptr, OPB_E_NULL);
+    if (guide) OPB_REQUIRE(nb >= 1 && nb <= 4096 && (nb & (nb - 1)) == 0 && col_stride == 1, OPB_E_ARG);
+    if (x) OPB_REQUIRE(scratch != nullptr && sums != nullptr, OPB_E_NULL);
+    if (npaths == 0) return set_status(OPB_OK);
+    McArgs a{};
+    a.C = C; a.rs = row_stride; a.cs = col_stride; a.guide = guide; a.nb = nb;
+    a.d = d; a.y0 = y0; a.nsteps = nsteps; a.seed = seed; a.path0 = path0; a.npaths = npaths;
+    a.ypaths = ypaths; a.x = x; a.strike = strike; a.barrier = barrier; a.disc = disc;
+    a.block_sums = x ? scratch : nullptr;
+    int grid = mc_grid(npaths);
+    k_mc<<<grid, 256, 0, stream()>>>(a);
+    if (x) k_reduce_pairs<<<1, 256, 0, stream()>>>(grid, scratch, sums);
+    return launch_check();
+}
+
+OPB_API int opb_mt19937_raw(uint32_t seed, long long nstreams, int n, uint32_t *out) {
+    OPB_REQUIRE(nstreams >= 0 && n >= 1 && n <= 623, OPB_E_ARG);
+    if (nstreams == 0) return set_status(OPB_OK);
+    OPB_REQUIRE(out != nullptr, OPB_E_NULL);
+    k_mt_raw<<<(int)((nstreams + 255) / 256), 256, 0, stream()>>>(seed, nstreams, n, out);
+    return launch_check();
+}
+
+// ---------------------------------------------------------------- reference MC entry points
+//
+// The reference keeps 4096 MT607 twister states in a device buffer between calls
+// (oplib/opcuda/smc.cu:118-156, 610-656).  Here the status buffer holds the generator's
+// continuation record instead: word 0 = base seed, words 1-2 = the next path id (64-bit).
+// Successive opcuda_mc1f calls continue with fresh paths, which keeps the reference's
+// "successive batches continue the same streams" contract with per-path MT19937 streams.
+
+OPB_API int opcuda_mc_nrng(void) { return 1 << 20; }   // independent streams per call (advisory)
+OPB_API int opcuda_mc_status_sz(void) { return 4; }    // uint32 words of continuation record
+
+// Accepted for ABI compatibility: MT19937 needs no per-stream parameter file
+// (the reference's MersenneTwister.dat, oplib/opcuda/smc.cu:87-96).
+OPB_API int opcuda_mc_load_mt_gpu(const char *MT_stream, long sz) {
+    (void)MT_stream;
+    (void)sz;
+    return set_status(OPB_OK);
+}
+
+// host_seedptr: host array whose first uint32 is the base seed (the reference passes
+// 4096 seeds, one per twister).  mtptr: device status buffer of opcuda_mc_status_sz() words.
+OPB_API int opcuda_mc_setseed(uint64_t host_seedptr, uint64_t mtptr) {
+    OPB_REQUIRE(host_seedptr != 0 && mtptr != 0, OPB_E_NULL);
+    uint32_t rec[4];
+    rec[0] = reinterpret_cast<const uint32_t *>(host_seedptr)[0];
+    rec[1] = rec[2] = rec[3] = 0;
+    OPB_TRY(cudaMemcpyAsync(reinterpret_cast<void *>(mtptr), rec, sizeof(rec), cudaMemcpyHostToDevice, stream()));
+    OPB_TRY(cudaStreamSynchronize(stream()));
+    return set_status(OPB_OK);
+}
+
+// Semantics of oplib/opcuda/smc.cu:610-656 with per-path MT19937: nscen paths of nk
+// steps from state y0 over the column-major cumulative kernels ctpker_m_yy (kernel m_k[k]
+// at step k), writing int16 states y_sk[p + nscen*k] and copying them to yhostptr
+// (blocking, as the reference does).  Unlike the reference (d < 1024 only,
+// smc.cu:622) any d <= 32767 is accepted; nk <= 623.
+OPB_API int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk, int d, uint64_t ctpker_m_yy,
+                        uint64_t m_k, uint64_t yhostptr) {
+    OPB_REQUIRE(mtptr != 0 && y_sk != 0 && ctpker_m_yy != 0 && m_k != 0, OPB_E_NULL);
+    OPB_REQUIRE(d > 0 && d <= 32767 && y0 >= 0 && y0 < d && nscen >= 0, OPB_E_ARG);
+    OPB_REQUIRE(nk >= 1 && nk <= 623, OPB_E_UNSUPPORTED);
+    uint32_t rec[4];
+    OPB_TRY(cudaMemcpyAsync(rec, reinterpret_cast<const void *>(mtptr), sizeof(rec), cudaMemcpyDeviceToHost, stream()));
+    OPB_TRY(cudaStreamSynchronize(stream()));
+    unsigned long long path0 = (unsigned long long)rec[1] | ((unsigned long long)rec[2] << 32);
+    if (nscen > 0) {
+        McArgs a{};
+        a.C = reinterpret_cast<const float *>(ctpker_m_yy);
+        a.rs = 1; a.cs = d; a.m_k = reinterpret_cast<const int *>(m_k); a.ms = (long long)d * d;
+        a.d = d; a.y0 = y0; a.nsteps = nk; a.seed = rec[0]; a.path0 = path0; a.npaths = nscen;
+        a.ypaths = reinterpret_cast<short *>(y_sk);
+        k_mc<<<mc_grid(nscen), 256, 0, stream()>>>(a);
+        OPB_TRY(cudaGetLastError());
+    }
+    path0 += (unsigned long long)nscen;
+    rec[1] = (uint32_t)(path0 & 0xffffffffull);
+    rec[2] = (uint32_t)(path0 >> 32);
+    OPB_TRY(cudaMemcpyAsync(reinterpret_cast<void *>(mtptr), rec, sizeof(rec), cudaMemcpyHostToDevice, stream()));
+    if (yhostptr != 0 && nscen > 0)
+        OPB_TRY(cudaMemcpyAsync(reinterpret_cast<void *>(yhostptr), reinterpret_cast<const void *>(y_sk),
+                                sizeof(short) * (size_t)nscen * nk, cudaMemcpyDeviceToHost, stream()));
+    OPB_TRY(cudaStreamSynchronize(stream()));
+    return set_status(OPB_OK);
+}
+
+// Uniform throughput benchmark (oplib/opcuda/smc.cu:664-736): nscen uniforms from
+// opcuda_mc_nrng-independent per-stream MT19937 generators -- 4096 streams of nscen/4096
+// values each (nscen/4096 <= 623), stream s seeded with base seed + s.
+OPB_API int opcuda_mt_benchmark(uint64_t mtptr, uint64_t unif_ptr, int nscen) {
+    OPB_REQUIRE(mtptr != 0 && unif_ptr != 0, OPB_E_NULL);
+    OPB_REQUIRE(nscen >= 0 && nscen % 4096 == 0, OPB_E_ARG);
+    int nper = nscen / 4096;
+    OPB_REQUIRE(nper <= 623, OPB_E_UNSUPPORTED);
+    if (nper == 0) return set_status(OPB_OK);
+    uint32_t rec[4];
+    OPB_TRY(cudaMemcpyAsync(rec, reinterpret_cast<const void *>(mtptr), sizeof(rec), cudaMemcpyDeviceToHost, stream()));
+    OPB_TRY(cudaStreamSynchronize(stream()));
+    k_mt_bench<<<4096 / 256, 256, 0, stream()>>>(rec[0], 4096, nper, reinterpret_cast<float *>(unif_ptr));
+    return launch_check();
+}
+
+// Uniform generation with typed pointers: nstreams streams (seed + s) x nper values.
+OPB_API int opb_mt_uniforms(uint32_t seed, long long nstreams, int nper, float *unif) {
+    OPB_REQUIRE(nstreams >= 0 && nper >= 1 && nper <= 623, OPB_E_ARG);
+    if (nstreams == 0) return set_status(OPB_OK);
+    OPB_REQUIRE(unif != nullptr, OPB_E_NULL);
+    k_mt_bench<<<(int)((nstreams + 255) / 256), 256, 0, stream()>>>(seed, nstreams, nper, unif);
+    return launch_check();
+}

@@ -1,0 +1,192 @@
+"""Host-side model API over the opcuda-b200 C ABI.
+
+Mirrors the roles of the reference's managed model layer for this path:
+``CLVModel``/``CSVModel`` build a generator (``mkgen``), ``CModel.make_mc_plan`` derives the
+squaring plan, ``CModel.exe_mc_plan`` exponentiates and chains, and the Monte Carlo runs
+over cumulative step kernels (``oplib/opmodel/models/CModel Common.cs:138-669``,
+``CModel Device.cs:142-367``).  All arithmetic runs in the CUDA library; torch provides
+device memory and streams only.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib
+from ._lib import LatticeDesc, call
+
+FP32_PLAIN, FP32_RENORM, BF16X3 = 0, 1, 2
+MODES = {"fp32_plain": FP32_PLAIN, "fp32": FP32_RENORM, "fp32_renorm": FP32_RENORM, "bf16x3": BF16X3}
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream_handle(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def bind_stream(device: torch.device | None = None) -> None:
+    """Order library work on torch's current stream of ``device``."""
+    dev = torch.device("cuda") if device is None else device
+    _lib.load().opb_set_stream(_stream_handle(dev))
+
+
+@dataclass
+class Plan:
+    niter: int
+    dt: float
+    maxdiag: float
+
+
+class Lattice:
+    """A discretised Markov generator on the device in ELL form (FP64) plus the spot
+    value of every state.  Build with :meth:`local_vol` or :meth:`stoch_vol`."""
+
+    def __init__(self, d: int, cols: torch.Tensor, vals: torch.Tensor, x: torch.Tensor, y0: int, rate: float):
+        self.d, self.cols, self.vals, self.x, self.y0, self.rate = d, cols, vals, x, y0, rate
+        self.width = cols.numel() // d
+        self.device = x.device
+
+    # ---------------------------------------------------------------- builders (mkgen)
+    @classmethod
+    def local_vol(cls, n=512, level=0.2, skew=0.1, width=0.5, rate=0.03, floor=0.0, lo=0.05, hi=5.0, s0=1.0,
+                  device="cuda"):
+        """Local-vol lattice on log-spaced nodes x_i = s0*lo*(hi/lo)^(i/(n-1)) with
+        sigma(x) = max(floor, level + skew*exp(-((x-1)/width)^2)), drift r*x."""
+        dev = torch.device(device)
+        bind_stream(dev)
+        x = torch.empty(n, dtype=torch.float64, device=dev)
+        drift = torch.empty_like(x)
+        vol = torch.empty_like(x)
+        call("opb_lv_params", n, lo, hi, s0, level, skew, width, floor, rate, _ptr(x), _ptr(drift), _ptr(vol))
+        return cls.from_drift_vol(x, drift, vol, rate, s0)
+
+    @classmethod
+    def from_drift_vol(cls, x: torch.Tensor, drift: torch.Tensor, vol: torch.Tensor, rate: float, s0: float = 1.0):
+        """LV generator from per-node drift and vol (``CLVModel.mkgen``)."""
+        n = x.numel()
+        bind_stream(x.device)
+        cols = torch.empty(3 * n, dtype=torch.int32, device=x.device)
+        vals = torch.empty(3 * n, dtype=torch.float64, device=x.device)
+        call("opb_lv_generator_ell", n, _ptr(x), _ptr(drift), _ptr(vol), _ptr(cols), _ptr(vals))
+        y0 = int(torch.argmin(torch.abs(x - s0)).item())
+        return cls(n, cols, vals, x.contiguous(), y0, rate)
+
+    @classmethod
+    def stoch_vol(cls, nx=128, nv=48, x_lo=0.05, x_hi=5.0, v_lo=0.05, v_hi=1.0, rate=0.03, kappa=2.0, theta=0.04,
+                  xi=0.6, rho=-0.7, s0=1.0, device="cuda"):
+        """2-D (spot, variance) lattice; the quoted state is the spot node nearest s0 at
+        the vol state nearest sqrt(theta)."""
+        dev = torch.device(device)
+        bind_stream(dev)
+        d = nx * nv
+        cols = torch.empty(7 * d, dtype=torch.int32, device=dev)
+        vals = torch.empty(7 * d, dtype=torch.float64, device=dev)
+        x = torch.empty(d, dtype=torch.float64, device=dev)
+        call("opb_sv_generator_ell", nx, nv, x_lo, x_hi, v_lo, v_hi, rate, kappa, theta, xi, rho, _ptr(cols),
+             _ptr(vals), _ptr(x))
+        ix = min(range(nx), key=lambda i: abs(x_lo * (x_hi / x_lo) ** (i / (nx - 1)) - s0))
+        iv = min(range(nv), key=lambda j: abs(v_lo * (v_hi / v_lo) ** (j / (nv - 1)) - math.sqrt(theta)))
+        return cls(d, cols, vals, x, ix + nx * iv, rate)
+
+    # ---------------------------------------------------------------- plan
+    def maxdiag(self) -> float:
+        scratch = torch.empty(1, dtype=torch.int64, device=self.device)
+        out = C.c_double()
+        bind_stream(self.device)
+        call("opb_ell_maxdiag", self.d, self.width, _ptr(self.cols), _ptr(self.vals), _ptr(scratch), C.byref(out))
+        return out.value
+
+    def plan(self, period: float, dt0: float, maxdiag: float | None = None) -> Plan:
+        """``CModel Common.cs:289-307``: dt = min(0.5/max|L_yy|, dt0), niter = ceil(log2(period/dt))."""
+        md = self.maxdiag() if maxdiag is None else maxdiag
+        n = C.c_int()
+        dt = C.c_double()
+        call("opb_plan_interval", md, period, dt0, C.byref(n), C.byref(dt))
+        return Plan(n.value, dt.value, md)
+
+    # ---------------------------------------------------------------- solve
+    def desc(self, plan: Plan, period: float, nmat: int, strikes: torch.Tensor | None) -> LatticeDesc:
+        L = LatticeDesc()
+        L.d, L.y0, L.ell_width = self.d, self.y0, self.width
+        L.gen_cols, L.gen_vals, L.gen_dense, L.x = _ptr(self.cols), _ptr(self.vals), None, _ptr(self.x)
+        L.dt, L.niter, L.nmat, L.period, L.rate = plan.dt, plan.niter, nmat, period, self.rate
+        L.nK = 0 if strikes is None else strikes.numel()
+        L.strikes = _ptr(strikes)
+        return L
+
+    def workspace(self, nK: int, mode: int) -> torch.Tensor:
+        n = _lib.load().opb_lattice_workspace_size(self.d, nK, mode)
+        return torch.empty(int(n), dtype=torch.uint8, device=self.device)
+
+    def solve(self, strikes, nmat: int, period: float, dt0: float, mode="bf16x3", plan: Plan | None = None,
+              all_states: bool = False, workspace: torch.Tensor | None = None):
+        """Quotes[m, k] = exp(-r T_m) (P(T_m) G)[y0, k], T_m = m*period.  Returns
+        (quotes [nmat, nK] FP64, V_all [nmat, d, nK] or None)."""
+        mode = MODES[mode] if isinstance(mode, str) else mode
+        strikes = torch.as_tensor(strikes, dtype=torch.float64, device=self.device)
+        plan = plan or self.plan(period, dt0)
+        ws = workspace if workspace is not None else self.workspace(strikes.numel(), mode)
+        quotes = torch.empty(nmat, strikes.numel(), dtype=torch.float64, device=self.device)
+        V = torch.empty(nmat, self.d, strikes.numel(), dtype=torch.float64, device=self.device) if all_states else None
+        L = self.desc(plan, period, nmat, strikes)
+        bind_stream(self.device)
+        call("opb_lattice_solve", C.byref(L), mode, _ptr(ws), ws.numel(), _ptr(quotes), _ptr(V))
+        return quotes, V
+
+    def kernel(self, period: float, dt0: float, mode="fp32", plan: Plan | None = None) -> torch.Tensor:
+        """Transition kernel P(period) as a d x d FP32 source-major matrix."""
+        mode = MODES[mode] if isinstance(mode, str) else mode
+        plan = plan or self.plan(period, dt0)
+        nk = 64
+        ws = self.workspace(nk, mode)
+        P = torch.empty(self.d, self.d, dtype=torch.float32, device=self.device)
+        L = self.desc(plan, period, 1, None)
+        L.nK = nk
+        bind_stream(self.device)
+        call("opb_lattice_kernel", C.byref(L), mode, _ptr(ws), ws.numel(), _ptr(P))
+        return P
+
+
+# -------------------------------------------------------------------- Monte Carlo
+
+def cumulative_rows(P: torch.Tensor) -> torch.Tensor:
+    """Cumulative normalised rows (``sck``) of a source-major FP32 kernel."""
+    d = P.shape[1]
+    Cm = torch.empty_like(P)
+    bind_stream(P.device)
+    call("opb_sck_rm", d, P.shape[0], _ptr(P), _ptr(Cm))
+    return Cm
+
+
+def guide_table(Cm: torch.Tensor, nb: int = 64) -> torch.Tensor:
+    d = Cm.shape[1]
+    g = torch.empty(Cm.shape[0] * nb, dtype=torch.int32, device=Cm.device)
+    bind_stream(Cm.device)
+    call("opb_guide_table", d, Cm.shape[0], nb, _ptr(Cm), _ptr(g))
+    return g
+
+
+def mc_run(Cm: torch.Tensor, y0: int, nsteps: int, seed: int, npaths: int, path0: int = 0,
+           guide: torch.Tensor | None = None, nb: int = 64, x: torch.Tensor | None = None, strike: float = 1.0,
+           barrier: float = 0.7, disc: float = 1.0, want_paths: bool = False, scratch: torch.Tensor | None = None):
+    """MT19937 Monte Carlo over ``npaths`` paths (ids path0..).  Returns
+    (sums[2] FP64 tensor or None, int16 paths [nsteps, npaths] or None)."""
+    d = Cm.shape[1]
+    dev = Cm.device
+    ypaths = torch.empty(nsteps, npaths, dtype=torch.int16, device=dev) if want_paths else None
+    sums = None
+    if x is not None:
+        nblk = _lib.load().opb_mc_scratch_blocks(npaths)
+        if scratch is None or scratch.numel() < 2 * nblk:
+            scratch = torch.empty(2 * nblk, dtype=torch.float64, device=dev)
+        sums = torch.empty(2, dtype=torch.float64, device=dev)
+    bind_stream(dev)
+    call("opb_mc_mt19937", _ptr(Cm), d, 1, _ptr(guide), nb if guide is not None else 0, d, y0, nsteps,
+         seed & 0xFFFFFFFF, path0, npaths, _ptr(ypaths), _ptr(x), strike, barrier, disc, _ptr(scratch), _ptr(sums))
+    return sums, ypaths

@@ -1,0 +1,565 @@
+"""CPU FP64 oracle for the operator-method pricing path.
+
+TEST INFRASTRUCTURE ONLY.  This module restates, in numpy (FP64), the algorithm of
+OPLib's host double-precision path so that the CUDA library can be checked against it.
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
+may import it; nothing in the ``oplib_b200`` package does.
+
+Parity status: OPLib ships no golden vectors for this path.  The pieces of this oracle
+are pinned as follows (see ``tests/test_oracle.py``):
+
+* MT19937: against libstdc++ ``std::mt19937`` (compiled from ``oracle/oracle_c.c``'s
+  twin test program) and numpy's ``MT19937._legacy_seeding``; and against the C++
+  standard's requirement that the 10000th output of a default-seeded (5489) engine is
+  4123659995.
+* Lattice pricing: against the Black-Scholes closed form (the reference's only known-
+  answer test, ``tests/bstest/Program.cs:11-37``), against ``scipy.linalg.expm``, and
+  by probability conservation / semigroup identities.
+* The reference implementation itself cannot be built here: its CPU path needs Intel
+  MKL (``oplib/opc/rangen.cpp:36``), its model layer needs .NET, and its CUDA path
+  passes 32-bit device pointers (``oplib/opcuda/util.cu:170-175``).
+
+Layout convention.  The reference stores the transition element (source y1 -> target
+y2) at ``y1 + d*y2`` (column-major with rows = source; ``oplib/opmodel/models/
+CLVModel.cs:122,130``).  This oracle works with dense numpy matrices ``P[y1, y2]`` in
+C (row-major) order, i.e. row = source; the two agree element by element.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# ---------------------------------------------------------------------------------
+# Grids
+# ---------------------------------------------------------------------------------
+
+
+def log_grid(n: int, lo: float = 0.05, hi: float = 5.0, s0: float = 1.0) -> np.ndarray:
+    """Log-spaced spot nodes x_i = s0*lo*(hi/lo)**(i/(n-1)), i = 0..n-1.
+
+    Replaces the pivot/spacing grid of ``oplib/opmodel/types/SGrid.cs:492-593`` (the
+    lattice configurations are defined on log-spaced nodes)."""
+    i = np.arange(n, dtype=np.float64)
+    return s0 * lo * (hi / lo) ** (i / (n - 1))
+
+
+def nearest_node(x: np.ndarray, s0: float = 1.0) -> int:
+    """Index of the node nearest to the spot (the reference's ``grid.y0``)."""
+    return int(np.argmin(np.abs(x - s0)))
+
+
+def centred_log_grid(n: int, s0: float, width: float, i0: int) -> np.ndarray:
+    """Log-spaced nodes with node ``i0`` exactly at ``s0`` (used by the Black-Scholes
+    known-answer test so that the priced node is the spot itself)."""
+    h = width / (n - 1)
+    i = np.arange(n, dtype=np.float64)
+    return s0 * np.exp((i - i0) * h)
+
+
+# ---------------------------------------------------------------------------------
+# Generators
+# ---------------------------------------------------------------------------------
+
+
+def lv_invm(x: np.ndarray) -> np.ndarray:
+    """Per-node inverse of the 2x2 moment matrix [[dm, dp], [dm^2, dp^2]].
+
+    Follows ``oplib/opmodel/types/S1DGrid.cs:78-147`` (``pregen``): dm = x[i-1]-x[i],
+    dp = x[i+1]-x[i]; the first and last nodes get the boundary rows of
+    S1DGrid.cs:95-128.  Returns an array (d, 2, 2) of inverses (row-major 2x2)."""
+    d = x.shape[0]
+    inv = np.zeros((d, 2, 2))
+    for i in range(d):
+        m = np.zeros((2, 2))
+        m[0, 0] = x[i - 1] - x[i] if i > 0 else 1.0
+        m[0, 1] = x[i + 1] - x[i] if i < d - 1 else 1.0
+        if 0 < i < d - 1:
+            m[1, 0] = m[0, 0] ** 2
+            m[1, 1] = m[0, 1] ** 2
+        elif i == 0:
+            m[1, 0], m[1, 1] = 0.0, 1.0
+        else:
+            m[1, 0], m[1, 1] = 1.0, 0.0
+        inv[i] = np.linalg.inv(m)
+    return inv
+
+
+def lv_generator(x: np.ndarray, drift: np.ndarray, vol: np.ndarray) -> np.ndarray:
+    """Tridiagonal birth-death generator L[y1, y2] of a local-volatility diffusion.
+
+    Follows ``oplib/opmodel/models/CLVModel.cs:86-136`` (``host_d_gen``): per interior
+    node, the down/up rates solve the moment system with right-hand side
+    [drift, vol^2] (drift = r*x, vol = sigma(x)*x in spot units); the boundary nodes
+    get zero rates (absorbing); the diagonal is minus the row sum."""
+    d = x.shape[0]
+    inv = lv_invm(x)
+    L = np.zeros((d, d))
+    for i in range(d):
+        if 0 < i < d - 1:
+            rhs = np.array([drift[i], vol[i] ** 2])
+        else:
+            rhs = np.zeros(2)
+        p = inv[i] @ rhs
+        s = 0.0
+        if i > 0:
+            L[i, i - 1] = p[0]
+            s += p[0]
+        if i < d - 1:
+            L[i, i + 1] = p[1]
+            s += p[1]
+        L[i, i] = -s
+    return L
+
+
+def lv_generator_fast(x: np.ndarray, drift: np.ndarray, vol: np.ndarray) -> np.ndarray:
+    """Vectorised restatement of :func:`lv_generator` (same arithmetic, closed-form 2x2
+    solve), for large lattices."""
+    d = x.shape[0]
+    dm = np.zeros(d)
+    dp = np.zeros(d)
+    dm[1:] = x[:-1] - x[1:]
+    dp[:-1] = x[1:] - x[:-1]
+    det = dm * dp * dp - dp * dm * dm
+    inner = np.zeros(d, dtype=bool)
+    inner[1:-1] = True
+    a = np.where(inner, drift, 0.0)
+    b = np.where(inner, vol ** 2, 0.0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        pm = np.where(inner, (dp * dp * a - dp * b) / det, 0.0)
+        pp = np.where(inner, (-dm * dm * a + dm * b) / det, 0.0)
+    L = np.zeros((d, d))
+    idx = np.arange(d)
+    L[idx[1:], idx[1:] - 1] = pm[1:]
+    L[idx[:-1], idx[:-1] + 1] = pp[:-1]
+    L[idx, idx] = -(pm + pp)
+    return L
+
+
+def lv_sigma(x: np.ndarray, level=0.2, skew=0.1, width=0.5, floor=0.0) -> np.ndarray:
+    """sigma(x) = level + skew*exp(-((x-1)/width)^2), floored at ``floor``."""
+    s = level + skew * np.exp(-(((x - 1.0) / width) ** 2))
+    return np.maximum(s, floor)
+
+
+@dataclass
+class SVSpec:
+    """Stochastic-volatility lattice: spot nodes x (nx) times vol states sigma_v (nv).
+
+    State index y = ix + nx*iv, as in ``oplib/opmodel/types/S2DGrid.cs:142``."""
+
+    nx: int = 128
+    nv: int = 48
+    x_lo: float = 0.05
+    x_hi: float = 5.0
+    v_lo: float = 0.05
+    v_hi: float = 1.0
+    r: float = 0.03
+    kappa: float = 2.0
+    theta: float = 0.04
+    xi: float = 0.6
+    rho: float = -0.7
+
+    @property
+    def d(self) -> int:
+        return self.nx * self.nv
+
+
+def sv_generator(spec: SVSpec) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """2-D (spot, variance) generator with a correlation stencil.
+
+    Structure follows ``oplib/opmodel/types/S2DGrid.cs:123-245`` (per node, separate
+    2x2 moment systems in the spot and in the vol direction, i.e. the block-diagonal
+    4x4 ``invm``) and ``oplib/opmodel/models/CSVModel.cs:187-379`` (negative rates
+    clamped to zero, then a drift fix-up so that the spot drift is exactly r*x).
+
+    Project extension (the reference has no spot-vol correlation term): Heston
+    dynamics in the variance V = sigma_v^2, dV = kappa(theta - V)dt + xi sqrt(V) dW2,
+    d<W1, W2> = rho dt, give Cov(dx, dV) = rho*xi*V*x dt.  It is carried by two
+    diagonal moves, (+x, -v) and (-x, +v) for rho < 0 (or (+,+), (-,-) for rho > 0),
+    at a common rate q chosen so that the diagonal moves reproduce the covariance,
+    capped so that the diagonal moves never carry more variance than the target
+    variance in either direction (there the stencil cannot represent the full
+    correlation; the effective correlation is reduced).  The axial rates then
+    match the remaining first and second moments.  Spot-boundary nodes are absorbing
+    (as in the local-vol model); vol-boundary nodes match the variance drift only
+    (as S2DGrid.cs:209-224 does).
+
+    Returns (L, x_y, v_y): dense generator and per-state spot and vol values."""
+    nx, nv = spec.nx, spec.nv
+    d = nx * nv
+    xs = log_grid(nx, spec.x_lo, spec.x_hi)
+    vs = spec.v_lo * (spec.v_hi / spec.v_lo) ** (np.arange(nv) / (nv - 1))
+    V = vs ** 2
+    L = np.zeros((d, d))
+    sgn = -1 if spec.rho < 0 else 1
+
+    def idx(ix, iv):
+        return ix + nx * iv
+
+    for iv in range(nv):
+        for ix in range(nx):
+            y = idx(ix, iv)
+            if ix == 0 or ix == nx - 1:
+                continue  # absorbing spot boundary
+            x = xs[ix]
+            v = V[iv]
+            var_x = v * x * x
+            var_v = spec.xi ** 2 * v
+            cov = spec.rho * spec.xi * v * x
+            mu_x = spec.r * x
+            mu_v = spec.kappa * (spec.theta - v)
+            dxm, dxp = xs[ix - 1] - x, xs[ix + 1] - x
+            rates = {}
+            q = 0.0
+            ex = ev = ex2 = ev2 = 0.0
+            if 0 < iv < nv - 1 and spec.rho != 0.0:
+                dvm, dvp = V[iv - 1] - v, V[iv + 1] - v
+                if sgn < 0:
+                    moves = [(dxp, dvm, idx(ix + 1, iv - 1)), (dxm, dvp, idx(ix - 1, iv + 1))]
+                else:
+                    moves = [(dxp, dvp, idx(ix + 1, iv + 1)), (dxm, dvm, idx(ix - 1, iv - 1))]
+                cx = sum(m[0] * m[1] for m in moves)
+                sx2 = sum(m[0] ** 2 for m in moves)
+                sv2 = sum(m[1] ** 2 for m in moves)
+                q = cov / cx
+                q = min(q, var_x / sx2, var_v / sv2)
+                q = max(q, 0.0)
+                for (ddx, ddv, t) in moves:
+                    rates[t] = rates.get(t, 0.0) + q
+                ex = q * sum(m[0] for m in moves)
+                ev = q * sum(m[1] for m in moves)
+                ex2 = q * sx2
+                ev2 = q * sv2
+            # spot direction: [dxm dxp; dxm^2 dxp^2] p = [mu_x - ex, var_x - ex2]
+            a, b = mu_x - ex, var_x - ex2
+            det = dxm * dxp * dxp - dxp * dxm * dxm
+            pxm = (dxp * dxp * a - dxp * b) / det
+            pxp = (-dxm * dxm * a + dxm * b) / det
+            rates[idx(ix - 1, iv)] = rates.get(idx(ix - 1, iv), 0.0) + pxm
+            rates[idx(ix + 1, iv)] = rates.get(idx(ix + 1, iv), 0.0) + pxp
+            # vol direction
+            if 0 < iv < nv - 1:
+                dvm, dvp = V[iv - 1] - v, V[iv + 1] - v
+                a, b = mu_v - ev, var_v - ev2
+                det = dvm * dvp * dvp - dvp * dvm * dvm
+                pvm = (dvp * dvp * a - dvp * b) / det
+                pvp = (-dvm * dvm * a + dvm * b) / det
+                rates[idx(ix, iv - 1)] = rates.get(idx(ix, iv - 1), 0.0) + pvm
+                rates[idx(ix, iv + 1)] = rates.get(idx(ix, iv + 1), 0.0) + pvp
+            elif iv == 0:
+                dvp = V[1] - v
+                rates[idx(ix, 1)] = max(mu_v, 0.0) / dvp
+            else:
+                dvm = V[iv - 1] - v
+                rates[idx(ix, iv - 1)] = min(mu_v, 0.0) / dvm
+            # clamp negatives (CSVModel.cs:342-345), then spot drift fix-up (353-373)
+            drift = 0.0
+            for t in list(rates):
+                if rates[t] < 0.0:
+                    rates[t] = 0.0
+                tx = t % nx
+                drift += rates[t] * (xs[tx] - x)
+            if drift > mu_x:
+                t = idx(ix - 1, iv)
+                rates[t] += (drift - mu_x) / (x - xs[ix - 1])
+            else:
+                t = idx(ix + 1, iv)
+                rates[t] += (mu_x - drift) / (xs[ix + 1] - x)
+            tot = 0.0
+            for t, rt in rates.items():
+                L[y, t] += rt
+                tot += rt
+            L[y, y] -= tot
+    x_y = np.tile(xs, nv)
+    v_y = np.repeat(vs, nx)
+    return L, x_y, v_y
+
+
+# ---------------------------------------------------------------------------------
+# Plan, kernels, squaring, chaining
+# ---------------------------------------------------------------------------------
+
+
+def plan_niter(L: np.ndarray, delta_t: float, dt0: float) -> tuple[int, float]:
+    """Number of squarings and the elementary time step for one interval.
+
+    ``oplib/opmodel/models/CModel Common.cs:289-307``: dt = min(0.5/max|L_yy|, dt0),
+    niter = ceil(log2(DeltaT/dt)), dt_j = DeltaT * 2^-niter."""
+    maxdiag = float(np.max(np.abs(np.diag(L))))
+    dt = 0.5 / maxdiag if maxdiag > 0 else dt0
+    if dt > dt0:
+        dt = dt0
+    niter = int(math.ceil(math.log(delta_t / dt) / math.log(2.0)))
+    return niter, delta_t * 2.0 ** (-niter)
+
+
+def ek(L: np.ndarray, dt: float) -> np.ndarray:
+    """U0 = I + dt*L (``oplib/opmodel/models/CModel Host Double.cs:89-121``;
+    ``oplib/opcuda/sek.cu:40-59``)."""
+    U = dt * L
+    U[np.diag_indices_from(U)] += 1.0
+    return U
+
+
+def renormalise(P: np.ndarray) -> np.ndarray:
+    """Rows divided by their FP64 sums (probability conservation)."""
+    s = P.sum(axis=1)
+    return P / s[:, None]
+
+
+def square(U: np.ndarray, niter: int, renorm: bool = False) -> np.ndarray:
+    """niter repeated squarings U <- U.U in FP64 (``CModel Host Double.cs:125-197``,
+    ping-pong through ``opc_dgemm``).  ``renorm`` renormalises rows after every level."""
+    P = U.copy()
+    for _ in range(niter):
+        P = P @ P
+        if renorm:
+            P = renormalise(P)
+    return P
+
+
+def chain(P1: np.ndarray, nmat: int) -> list[np.ndarray]:
+    """P(j*T) = P((j-1)*T) . P(T), j = 1..nmat (the chaining GEMMs of
+    ``CModel Host Double.cs:227-277``, tpk_m <- tpk_m . xtpk_j)."""
+    out = [P1]
+    for _ in range(nmat - 1):
+        out.append(out[-1] @ P1)
+    return out
+
+
+def payoff_calls(x: np.ndarray, strikes: np.ndarray) -> np.ndarray:
+    """G[y, k] = (x_y - K_k)^+."""
+    return np.maximum(x[:, None] - strikes[None, :], 0.0)
+
+
+def price_from_kernels(Ps: list[np.ndarray], x: np.ndarray, strikes: np.ndarray,
+                       r: float, mats: np.ndarray) -> np.ndarray:
+    """Backward induction V_T = P_T . G for every maturity (all source states), with
+    discounting exp(-r T).  Returns V[m, y, k]."""
+    G = payoff_calls(x, strikes)
+    return np.stack([math.exp(-r * T) * (P @ G) for P, T in zip(Ps, mats)])
+
+
+# ---------------------------------------------------------------------------------
+# Lattice configurations
+# ---------------------------------------------------------------------------------
+
+
+@dataclass
+class LVLattice:
+    n: int = 512
+    level: float = 0.2
+    skew: float = 0.1
+    width: float = 0.5
+    r: float = 0.03
+    floor: float = 0.0
+    dt0: float = 2.0 ** -14
+    period: float = 0.25
+    nmat: int = 8
+    strikes: np.ndarray = field(default_factory=lambda: 0.5 + np.arange(64) / 63.0)
+
+    def grid(self):
+        return log_grid(self.n)
+
+    def generator(self):
+        x = self.grid()
+        sig = lv_sigma(x, self.level, self.skew, self.width, self.floor)
+        return lv_generator_fast(x, self.r * x, sig * x), x
+
+    @property
+    def maturities(self):
+        return self.period * np.arange(1, self.nmat + 1)
+
+
+def solve_lattice_fp64(L: np.ndarray, x: np.ndarray, strikes: np.ndarray, r: float,
+                       period: float, nmat: int, dt0: float, renorm: bool = True):
+    """Full FP64 solve: plan, U0, squarings, chaining, pricing.  Returns
+    (V[m, y, k], niter, dt)."""
+    niter, dt = plan_niter(L, period, dt0)
+    U0 = ek(L, dt)
+    P1 = square(U0, niter, renorm=renorm)
+    Ps = chain(P1, nmat)
+    mats = period * np.arange(1, nmat + 1)
+    return price_from_kernels(Ps, x, strikes, r, mats), niter, dt
+
+
+# ---------------------------------------------------------------------------------
+# Cumulative rows and sampling
+# ---------------------------------------------------------------------------------
+
+
+def cumrows_f32(P: np.ndarray) -> np.ndarray:
+    """Cumulative normalised rows in FP32, sequential left-to-right sums.
+
+    ``oplib/opcuda/sck.cu:43-84``: C[y, 0] = P[y, 0]; C[y, z] = C[y, z-1] + P[y, z]
+    (FP32 running sum); then every entry is divided by the row total and clamped at 1.
+    The FP32 operations are done one at a time so that the rounding sequence is the
+    one a sequential FP32 loop performs."""
+    P32 = np.maximum(np.asarray(P, dtype=np.float32), np.float32(0.0))  # negatives count as 0
+    d = P32.shape[1]
+    C = np.empty_like(P32)
+    acc = P32[:, 0].copy()
+    C[:, 0] = acc
+    for z in range(1, d):
+        acc = (acc + P32[:, z]).astype(np.float32)
+        C[:, z] = acc
+    tot = acc
+    C = (C / tot[:, None]).astype(np.float32)
+    return np.minimum(C, np.float32(1.0))
+
+
+def uniform_f32(x: np.ndarray) -> np.ndarray:
+    """u = ((float)x + 1.0f) * 2^-32 in FP32 (``oplib/opcuda/smc.cu:329``), u in (0,1]."""
+    f = x.astype(np.float32)
+    f = (f + np.float32(1.0)).astype(np.float32)
+    return (f * np.float32(2.0 ** -32)).astype(np.float32)
+
+
+def sample_next(Crow: np.ndarray, u: np.ndarray) -> np.ndarray:
+    """Smallest y with u < C[y], capped at d-1 (``oplib/opcuda/smc.cu:336-350``).
+
+    ``Crow`` is (npaths, d) float32, ``u`` (npaths,) float32."""
+    d = Crow.shape[1]
+    cnt = (Crow <= u[:, None]).sum(axis=1)  # rows are non-decreasing
+    return np.minimum(cnt, d - 1)
+
+
+# ---------------------------------------------------------------------------------
+# MT19937 (Matsumoto & Nishimura 1998, init_genrand of the 2002 reference code)
+# ---------------------------------------------------------------------------------
+
+_MT_N, _MT_M = 624, 397
+_MT_A = np.uint32(0x9908B0DF)
+_UPPER = np.uint32(0x80000000)
+_LOWER = np.uint32(0x7FFFFFFF)
+
+
+def mt19937_init(seeds: np.ndarray) -> np.ndarray:
+    """init_genrand for a vector of seeds: mt[0] = s, mt[i] = 1812433253 *
+    (mt[i-1] ^ (mt[i-1] >> 30)) + i (mod 2^32).  The same recurrence seeds the
+    reference's twisters (``oplib/opcuda/smc.cu:127-131``).  Returns (nseeds, 624)."""
+    seeds = np.asarray(seeds, dtype=np.uint64) & np.uint64(0xFFFFFFFF)
+    mt = np.empty((seeds.shape[0], _MT_N), dtype=np.uint64)
+    mt[:, 0] = seeds
+    mask = np.uint64(0xFFFFFFFF)
+    for i in range(1, _MT_N):
+        prev = mt[:, i - 1]
+        mt[:, i] = (np.uint64(1812433253) * (prev ^ (prev >> np.uint64(30))) + np.uint64(i)) & mask
+    return mt.astype(np.uint32)
+
+
+def mt19937_twist(mt: np.ndarray) -> np.ndarray:
+    """One full regeneration of the 624-word state (genrand_int32's refill loop)."""
+    mt = mt.copy()
+    n = _MT_N
+    for k in range(n):
+        y = (mt[:, k] & _UPPER) | (mt[:, (k + 1) % n] & _LOWER)
+        mag = np.where((y & np.uint32(1)) != 0, _MT_A, np.uint32(0))
+        mt[:, k] = mt[:, (k + _MT_M) % n] ^ (y >> np.uint32(1)) ^ mag
+    return mt
+
+
+def mt19937_temper(y: np.ndarray) -> np.ndarray:
+    y = y ^ (y >> np.uint32(11))
+    y = y ^ ((y << np.uint32(7)) & np.uint32(0x9D2C5680))
+    y = y ^ ((y << np.uint32(15)) & np.uint32(0xEFC60000))
+    y = y ^ (y >> np.uint32(18))
+    return y
+
+
+def mt19937_outputs(seeds: np.ndarray, count: int) -> np.ndarray:
+    """First ``count`` genrand_int32 outputs of each seeded stream, (nseeds, count)."""
+    st = mt19937_init(seeds)
+    outs = []
+    while sum(o.shape[1] for o in outs) < count:
+        st = mt19937_twist(st)
+        outs.append(mt19937_temper(st))
+    return np.concatenate(outs, axis=1)[:, :count]
+
+
+# ---------------------------------------------------------------------------------
+# Monte Carlo on a lattice (per-path MT19937 streams)
+# ---------------------------------------------------------------------------------
+
+
+def mc_paths(C: np.ndarray, y0: int, seed: int, path_ids: np.ndarray, nsteps: int) -> np.ndarray:
+    """State paths y[p, k] (k = 1..nsteps) with path p drawing from MT19937
+    init_genrand(seed + p) and consuming its outputs in order, one per step.
+
+    The step loop follows ``oplib/opcuda/smc.cu:307-366`` (one uniform per step, inverse
+    CDF over the row of the previous state)."""
+    seeds = (np.uint64(seed) + path_ids.astype(np.uint64)) & np.uint64(0xFFFFFFFF)
+    raw = mt19937_outputs(seeds, nsteps)
+    y = np.full(path_ids.shape[0], y0, dtype=np.int64)
+    out = np.empty((path_ids.shape[0], nsteps), dtype=np.int16)
+    for k in range(nsteps):
+        u = uniform_f32(raw[:, k])
+        y = sample_next(C[y], u)
+        out[:, k] = y
+    return out
+
+
+def mc_payoffs(paths: np.ndarray, x: np.ndarray, strike: float, barrier: float,
+               r: float, T: float) -> dict:
+    """Discounted barrier (down-and-out call, discretely monitored at every step) and
+    arithmetic-Asian call payoffs per path, plus their means."""
+    xv = x[paths.astype(np.int64)]
+    disc = math.exp(-r * T)
+    alive = xv.min(axis=1) > barrier
+    barrier_pay = disc * np.where(alive, np.maximum(xv[:, -1] - strike, 0.0), 0.0)
+    asian_pay = disc * np.maximum(xv.mean(axis=1) - strike, 0.0)
+    return {"barrier": barrier_pay, "asian": asian_pay}
+
+
+# ---------------------------------------------------------------------------------
+# Black-Scholes (``tests/bstest/BSPricer.cs:7-65``) and implied volatility
+# ---------------------------------------------------------------------------------
+
+
+def norm_cdf(z):
+    return 0.5 * (1.0 + np.vectorize(math.erf)(np.asarray(z) / math.sqrt(2.0)))
+
+
+def bs_call(s, k, r, sigma, t):
+    s, k, sigma, t = map(np.asarray, (s, k, sigma, t))
+    sq = sigma * np.sqrt(t)
+    d1 = (np.log(s / k) + (r + 0.5 * sigma * sigma) * t) / sq
+    d2 = d1 - sq
+    return s * norm_cdf(d1) - k * np.exp(-r * t) * norm_cdf(d2)
+
+
+def implied_vol(price, s, k, r, t, lo=1e-4, hi=5.0, iters=100):
+    """Bisection inversion of the Black-Scholes call price (vectorised)."""
+    price, k, t = np.broadcast_arrays(np.asarray(price, float), np.asarray(k, float),
+                                      np.asarray(t, float))
+    a = np.full(price.shape, lo)
+    b = np.full(price.shape, hi)
+    for _ in range(iters):
+        m = 0.5 * (a + b)
+        too_high = bs_call(s, k, r, m, t) > price
+        b = np.where(too_high, m, b)
+        a = np.where(too_high, a, m)
+    return 0.5 * (a + b)
+
+
+# ---------------------------------------------------------------------------------
+# Split-BF16 emulation (numerical model of the tensor-core squaring, for analysis)
+# ---------------------------------------------------------------------------------
+
+
+def bf16_round(a: np.ndarray) -> np.ndarray:
+    """Round FP32 values to BF16 (round to nearest even), returned as FP32."""
+    a32 = np.ascontiguousarray(a, dtype=np.float32)
+    u = a32.view(np.uint32).astype(np.uint64)
+    lsb = (u >> np.uint64(16)) & np.uint64(1)
+    u = (u + np.uint64(0x7FFF) + lsb) & np.uint64(0xFFFF0000)
+    return u.astype(np.uint32).view(np.float32)
+
+
+def split_bf16(a: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    a32 = np.asarray(a, dtype=np.float32)
+    hi = bf16_round(a32)
+    lo = bf16_round((a32 - hi).astype(np.float32))
+    return hi, lo

@@ -1,0 +1,243 @@
+"""GPU parity of the GEMM / GEMV kernels behind the opcuda ABI.
+
+Floating-point kernels are compared with FP64 references of the same operation:
+- split-BF16 tcgen05 GEMM: FP64 product of the same BF16 parts; FP32 accumulation over
+  K terms gives |err| <= 2e-6 * sum|a||b| (the test bound);
+- FP32 SIMT GEMM / GEMV: FP64 product of the FP32 inputs, relative 1e-5 (the reference's
+  own GPU-vs-MKL checks use 2e-3 and 1e-3, benchmarks/gsgemm4/Program.cs:229-291,
+  benchmarks/gsgemv4/Program.cs:329-391).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16_dev(a32: np.ndarray, dev):
+    u = np.ascontiguousarray(a32, dtype=np.float32).view(np.uint32) >> np.uint32(16)
+    return torch.from_numpy(u.astype(np.uint16).view(np.int16)).to(dev).view(torch.bfloat16)
+
+
+def _split_dev(a, dev):
+    hi, lo = O.split_bf16(a)
+    return _bf16_dev(hi, dev), _bf16_dev(lo, dev), hi.astype(np.float64), lo.astype(np.float64)
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 64, 64), (256, 128, 192), (384, 256, 512), (128, 384, 128),
+                                   (512, 512, 1024)])
+def test_bf16x3_gemm_matches_fp64_of_split(cuda, M, N, K):
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(M + N + K)
+    A = rng.random((M, K)).astype(np.float32)
+    B = rng.random((N, K)).astype(np.float32)  # K-major right operand (rows of B^T)
+    Cin = rng.standard_normal((M, N)).astype(np.float32)
+    Ah, Al, ah, al = _split_dev(A, cuda)
+    Bh, Bl, bh, bl = _split_dev(B, cuda)
+    Cd = torch.from_numpy(Cin).to(cuda)
+    Cout = torch.empty_like(Cd)
+    nparts = lib.opb_gemm_bf16x3_nparts(N)
+    rs = torch.empty(nparts * M, dtype=torch.float64, device=cuda)
+    torch.cuda.synchronize()
+    st = lib.opb_gemm_bf16x3(M, N, K, Ah.data_ptr(), Al.data_ptr(), K, Bh.data_ptr(), Bl.data_ptr(), K,
+                             0.5, Cd.data_ptr(), 2.0, Cout.data_ptr(), N, rs.data_ptr())
+    assert st == 0
+    torch.cuda.synchronize()
+    assert lib.opb_tc_error() == 0
+    ref = 0.5 * (ah @ bh.T + ah @ bl.T + al @ bh.T) + 2.0 * Cin.astype(np.float64)
+    got = Cout.cpu().numpy().astype(np.float64)
+    scale = 0.5 * (np.abs(ah) + np.abs(al)) @ (np.abs(bh) + np.abs(bl)).T + 2 * np.abs(Cin)
+    assert np.all(np.abs(got - ref) <= 2e-6 * scale + 1e-30), np.max(np.abs(got - ref) / scale)
+    # FP64 row sums of the stored values, per N tile
+    parts = rs.cpu().numpy().reshape(nparts, M)
+    bn = N // nparts
+    for t in range(nparts):
+        assert np.allclose(parts[t], got[:, t * bn:(t + 1) * bn].sum(axis=1), rtol=1e-12, atol=1e-9)
+
+
+def test_bf16x3_gemm_in_place(cuda):
+    """C may alias Cin (the E-form squaring updates E in place)."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    M = N = K = 256
+    rng = np.random.default_rng(7)
+    E = (rng.random((M, K)) * 1e-2).astype(np.float32)
+    Ah, Al, ah, al = _split_dev(E, cuda)
+    Bh, Bl, bh, bl = _split_dev(np.ascontiguousarray(E.T), cuda)
+    X = torch.from_numpy(E).to(cuda)
+    assert lib.opb_gemm_bf16x3(M, N, K, Ah.data_ptr(), Al.data_ptr(), K, Bh.data_ptr(), Bl.data_ptr(), K, 1.0,
+                               X.data_ptr(), 2.0, X.data_ptr(), N, None) == 0
+    torch.cuda.synchronize()
+    ref = ah @ bh.T + ah @ bl.T + al @ bh.T + 2.0 * E.astype(np.float64)
+    assert np.abs(X.cpu().numpy() - ref).max() < 1e-7
+
+
+def test_bf16x3_rejects_unsupported_shapes(cuda):
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    t = torch.zeros(128 * 128, dtype=torch.bfloat16, device=cuda)
+    c = torch.zeros(128 * 128, dtype=torch.float32, device=cuda)
+    p = t.data_ptr()
+    assert lib.opb_gemm_bf16x3(100, 128, 128, p, p, 128, p, p, 128, 1.0, None, 0.0, c.data_ptr(), 128, None) == -4
+    assert lib.opb_gemm_bf16x3(128, 128, 96, p, p, 128, p, p, 128, 1.0, None, 0.0, c.data_ptr(), 128, None) == -4
+    assert lib.opb_gemm_bf16x3(128, 128, 128, p + 2, p, 128, p, p, 128, 1.0, None, 0.0, c.data_ptr(), 128,
+                               None) == -3
+
+
+@pytest.mark.parametrize("m,n,k", [(64, 64, 64), (100, 37, 129), (576, 576, 576), (7, 300, 5)])
+def test_opcuda_sgemm_column_major(cuda, m, n, k):
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(m * n + k)
+    A = rng.standard_normal((m, k)).astype(np.float32)
+    B = rng.standard_normal((k, n)).astype(np.float32)
+    C0 = rng.standard_normal((m, n)).astype(np.float32)
+    dA = torch.from_numpy(np.asfortranarray(A).ravel(order="K").copy()).to(cuda)
+    dB = torch.from_numpy(np.asfortranarray(B).ravel(order="K").copy()).to(cuda)
+    dC = torch.from_numpy(np.asfortranarray(C0).ravel(order="K").copy()).to(cuda)
+    assert lib.opcuda_sgemm(m, n, k, 1.5, dA.data_ptr(), m, dB.data_ptr(), k, -0.5, dC.data_ptr(), m) == 0
+    torch.cuda.synchronize()
+    got = dC.cpu().numpy().reshape(n, m).T
+    ref = 1.5 * A.astype(np.float64) @ B.astype(np.float64) - 0.5 * C0
+    assert np.abs(got - ref).max() <= 1e-5 * (1 + np.abs(ref).max())
+
+
+def test_opcuda_ssqmm_pointer_tables(cuda):
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    d, ni = 96, 3
+    rng = np.random.default_rng(1)
+    mats = [rng.random((d, d)).astype(np.float32) / d for _ in range(ni)]
+    A = [torch.from_numpy(np.asfortranarray(m).ravel(order="K").copy()).to(cuda) for m in mats]
+    Cs = [torch.empty(d * d, device=cuda) for _ in range(ni)]
+    tA = torch.tensor([a.data_ptr() for a in A], dtype=torch.int64, device=cuda)
+    tC = torch.tensor([c.data_ptr() for c in Cs], dtype=torch.int64, device=cuda)
+    assert lib.opcuda_ssqmm(d, ni, tA.data_ptr(), tA.data_ptr(), tC.data_ptr()) == 0
+    torch.cuda.synchronize()
+    for m, c in zip(mats, Cs):
+        got = c.cpu().numpy().reshape(d, d).T
+        ref = m.astype(np.float64) @ m.astype(np.float64)
+        assert np.abs(got - ref).max() < 1e-5 * np.abs(ref).max()
+
+
+def test_opcuda_sgemm4_task_table(cuda):
+    """40-GEMM grouped call in the shape of benchmarks/gsgemm4 (reduced sizes)."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(2)
+    tasks, mats, outs = [], [], []
+    for i, (m, n, k) in enumerate([(128, 32, 64), (64, 48, 80), (192, 16, 128)]):
+        A = rng.standard_normal((m, k)).astype(np.float32)
+        B = rng.standard_normal((k, n)).astype(np.float32)
+        dA = torch.from_numpy(np.asfortranarray(A).ravel(order="K").copy()).to(cuda)
+        dB = torch.from_numpy(np.asfortranarray(B).ravel(order="K").copy()).to(cuda)
+        dC = torch.zeros(m * n, device=cuda)
+        mats.append((A, B, dA, dB))
+        outs.append(dC)
+        for bx in range((m + 63) // 64):
+            for by in range((n + 15) // 16):
+                tasks.append((i, bx, by, m, n, k, dA.data_ptr(), dB.data_ptr(), dC.data_ptr()))
+    sz = lib.opb_sgemm4_task_size()
+    rec = np.zeros((len(tasks), sz // 8), dtype=np.int64)
+    for t, (i, bx, by, m, n, k, a, b, c) in enumerate(tasks):
+        ints = np.array([i, bx, by, m, n, k], dtype=np.int32).view(np.int64)
+        rec[t, :3] = ints
+        rec[t, 3:6] = [a, b, c]
+    drec = torch.from_numpy(rec.ravel()).to(cuda)
+    ptrs = torch.tensor([drec.data_ptr() + t * sz for t in range(len(tasks))], dtype=torch.int64, device=cuda)
+    assert lib.opcuda_sgemm4(len(tasks), ptrs.data_ptr()) == 0
+    torch.cuda.synchronize()
+    for (A, B, _, _), dC in zip(mats, outs):
+        m, n = A.shape[0], B.shape[1]
+        got = dC.cpu().numpy().reshape(n, m).T
+        ref = A.astype(np.float64) @ B
+        assert np.abs(got - ref).max() / (1 + np.abs(ref).max()) < 2e-3 * 1e-2
+
+
+def test_opcuda_sgemv_family(cuda):
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(4)
+    m, n = 300, 200
+    A = rng.standard_normal((m, n)).astype(np.float32)
+    x = rng.standard_normal(n).astype(np.float32)
+    xt = rng.standard_normal(m).astype(np.float32)
+    dA = torch.from_numpy(np.asfortranarray(A).ravel(order="K").copy()).to(cuda)
+    dx, dxt = torch.from_numpy(x).to(cuda), torch.from_numpy(xt).to(cuda)
+    y = torch.ones(m, device=cuda)
+    yt = torch.ones(n, device=cuda)
+    assert lib.opcuda_sgemv(m, n, 2.0, dA.data_ptr(), m, dx.data_ptr(), 1, 0.5, y.data_ptr(), 1) == 0
+    assert lib.opcuda_sgemvT(m, n, 1.0, dA.data_ptr(), m, dxt.data_ptr(), 1, 0.0, yt.data_ptr(), 1) == 0
+    torch.cuda.synchronize()
+    assert np.allclose(y.cpu().numpy(), 2 * A.astype(np.float64) @ x + 0.5, rtol=1e-5, atol=1e-4)
+    assert np.allclose(yt.cpu().numpy(), A.T.astype(np.float64) @ xt, rtol=1e-5, atol=1e-4)
+    # sdot2: c[h] = sum_y a[h + nh*y] b[h + nh*y]
+    nh, dd = 37, 91
+    a = rng.standard_normal(nh * dd).astype(np.float32)
+    b = rng.standard_normal(nh * dd).astype(np.float32)
+    da, db, dc = torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda), torch.empty(nh, device=cuda)
+    assert lib.opcuda_sdot2(da.data_ptr(), db.data_ptr(), dc.data_ptr(), nh, dd) == 0
+    torch.cuda.synchronize()
+    ref = (a.astype(np.float64) * b).reshape(dd, nh).sum(axis=0)
+    assert np.allclose(dc.cpu().numpy(), ref, rtol=1e-5, atol=1e-4)
+
+
+def test_opcuda_sgemv3_columns_and_sentinel(cuda):
+    """Z[:, col1] = A Z[:, col0] for a column list; untouched columns keep their values
+    (the non-clobbering check of benchmarks/gsgemv4/Program.cs:345-359)."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(5)
+    d, nz = 200, 10
+    A = (rng.random((d, d)) / d).astype(np.float32)
+    Z = rng.standard_normal((2 * nz, d)).astype(np.float32)  # column j at offset j*d
+    col0 = [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 0, 1, 2, 3, 4, 5, 6, 7]
+    col1 = [10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 2 * nz, 2 * nz, 2 * nz, 2 * nz, 2 * nz, 2 * nz, 2 * nz, 2 * nz]
+    dA = torch.from_numpy(np.asfortranarray(A).ravel(order="K").copy()).to(cuda)
+    dZ = torch.from_numpy(Z.ravel().copy()).to(cuda)
+    c0 = torch.tensor([c * d for c in col0], dtype=torch.int32, device=cuda)
+    c1 = torch.tensor([c * d for c in col1], dtype=torch.int32, device=cuda)
+    assert lib.opcuda_sgemv3(d, nz, len(col0), dA.data_ptr(), dZ.data_ptr(), c0.data_ptr(), c1.data_ptr()) == 0
+    torch.cuda.synchronize()
+    got = dZ.cpu().numpy().reshape(2 * nz, d)
+    for j in range(nz):
+        assert np.allclose(got[nz + j], A.astype(np.float64) @ Z[j], rtol=1e-5, atol=1e-5)
+        assert np.array_equal(got[j], Z[j])
+
+
+def test_opcuda_sek_fp64_sum(cuda):
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    d = 77
+    rng = np.random.default_rng(6)
+    gen = rng.standard_normal((d, d)).astype(np.float32)
+    dg = torch.from_numpy(np.asfortranarray(gen).ravel(order="K").copy()).to(cuda)
+    out = torch.empty(d * d, device=cuda)
+    dt = np.float32(1e-3)
+    assert lib.opcuda_sek(d, dg.data_ptr(), float(dt), out.data_ptr()) == 0
+    torch.cuda.synchronize()
+    ref = (np.eye(d) + np.float64(dt) * gen.astype(np.float64)).astype(np.float32)
+    assert np.array_equal(out.cpu().numpy().reshape(d, d).T, ref)
+
+
+def test_opcuda_sglvg_matches_oracle_generator(cuda):
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    d = 64
+    x = O.log_grid(d)
+    sig = O.lv_sigma(x)
+    inv = O.lv_invm(x)  # row-major 2x2 inverses
+    invm = np.stack([inv[:, 0, 0], inv[:, 1, 0], inv[:, 0, 1], inv[:, 1, 1]], axis=1).ravel().astype(np.float32)
+    pars = np.concatenate([0.03 * x, sig * x]).astype(np.float32)
+    dg = torch.empty(d * d, device=cuda)
+    di, dp = torch.from_numpy(invm).to(cuda), torch.from_numpy(pars).to(cuda)
+    assert lib.opcuda_sglvg(dg.data_ptr(), 1, d, di.data_ptr(), dp.data_ptr()) == 0
+    torch.cuda.synchronize()
+    got = dg.cpu().numpy().reshape(d, d).T  # column-major -> [source, target]
+    ref = O.lv_generator(x, 0.03 * x, sig * x)
+    assert np.allclose(got, ref, rtol=2e-4, atol=1e-3 * np.abs(ref).max())

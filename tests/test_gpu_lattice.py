@@ -1,0 +1,139 @@
+"""GPU parity of the lattice path against the FP64 oracle.
+
+Tolerances (absolute price error, S0 = 1):
+- OPB_BF16X3 and OPB_FP32_RENORM: <= 1e-5 versus the FP64 solve (the target accuracy);
+- OPB_FP32_PLAIN (the reference's FP32 semantics, no renormalisation) is reported and
+  bounded by 5e-4; its error is what the FP64 renormalisation removes.
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _lv(n=512, **kw):
+    from oplib_b200.model import Lattice
+    return Lattice.local_vol(n=n, **kw)
+
+
+def test_lv_generator_matches_oracle(cuda):
+    lat = _lv(300, level=0.25, skew=-0.2, width=0.4, rate=0.02)
+    torch.cuda.synchronize()
+    x = lat.x.cpu().numpy()
+    assert np.allclose(x, O.log_grid(300), rtol=1e-14)
+    ref = O.lv_generator_fast(x, 0.02 * x, O.lv_sigma(x, 0.25, -0.2, 0.4) * x)
+    cols = lat.cols.cpu().numpy().reshape(-1, 3)
+    vals = lat.vals.cpu().numpy().reshape(-1, 3)
+    dense = np.zeros((300, 300))
+    for y in range(300):
+        for c, v in zip(cols[y], vals[y]):
+            if c >= 0:
+                dense[y, c] += v
+    assert np.allclose(dense, ref, rtol=1e-12, atol=1e-9)
+    assert abs(lat.maxdiag() - np.abs(np.diag(ref)).max()) < 1e-9
+
+
+def test_sv_generator_matches_oracle(cuda):
+    from oplib_b200.model import Lattice
+    spec = O.SVSpec(nx=20, nv=9)
+    lat = Lattice.stoch_vol(nx=20, nv=9)
+    torch.cuda.synchronize()
+    ref, xy, _ = O.sv_generator(spec)
+    cols = lat.cols.cpu().numpy().reshape(-1, 7)
+    vals = lat.vals.cpu().numpy().reshape(-1, 7)
+    dense = np.zeros_like(ref)
+    for y in range(spec.d):
+        for c, v in zip(cols[y], vals[y]):
+            if c >= 0:
+                dense[y, c] += v
+    assert np.allclose(dense, ref, rtol=1e-11, atol=1e-9)
+    assert np.allclose(lat.x.cpu().numpy(), xy, rtol=1e-14)
+
+
+@pytest.fixture(scope="module")
+def config0_fp64():
+    cfg = O.LVLattice()
+    L, x = cfg.generator()
+    V, niter, dt = O.solve_lattice_fp64(L, x, cfg.strikes, cfg.r, cfg.period, cfg.nmat, cfg.dt0)
+    return cfg, V, O.nearest_node(x)
+
+
+@pytest.mark.parametrize("mode,tol", [("bf16x3", 1e-5), ("fp32", 1e-5), ("fp32_plain", 5e-4)])
+def test_config0_quotes_vs_fp64(cuda, config0_fp64, mode, tol):
+    cfg, V, y0 = config0_fp64
+    lat = _lv()
+    assert lat.y0 == y0
+    q, Vall = lat.solve(cfg.strikes, cfg.nmat, cfg.period, cfg.dt0, mode=mode, all_states=True)
+    torch.cuda.synchronize()
+    from oplib_b200 import _lib
+    assert _lib.load().opb_tc_error() == 0
+    err = np.abs(q.cpu().numpy() - V[:, y0, :]).max()
+    print(f"config0 {mode}: max abs quote error {err:.3e}")
+    assert err <= tol
+    # all source states (the backward induction result), same bound away from the far boundary
+    errall = np.abs(Vall.cpu().numpy() - V).max()
+    assert errall <= 5 * tol
+
+
+def test_kernel_matches_fp64_and_conserves(cuda):
+    cfg = O.LVLattice(n=256)
+    L, x = cfg.generator()
+    niter, dt = O.plan_niter(L, 1 / 252, cfg.dt0)
+    P64 = O.square(O.ek(L, dt), niter, renorm=True)
+    lat = _lv(256)
+    for mode in ["fp32", "bf16x3"]:
+        P = lat.kernel(1 / 252, cfg.dt0, mode=mode).cpu().numpy().astype(np.float64)
+        assert np.abs(P - P64).max() < 2e-5, mode
+        assert np.abs(P.sum(axis=1) - 1).max() < 1e-6, mode
+
+
+def test_sv_small_bf16x3_vs_fp64(cuda):
+    """A reduced stochastic-vol lattice (d = 32 x 8 = 256) in all three modes."""
+    from oplib_b200.model import Lattice
+    spec = O.SVSpec(nx=32, nv=8)
+    L, xy, _ = O.sv_generator(spec)
+    strikes = 0.7 + np.arange(64) / 100
+    lat = Lattice.stoch_vol(nx=32, nv=8)
+    niter, dt = O.plan_niter(L, 0.25, 2.0 ** -16)
+    U = O.ek(L, dt)
+    P = O.square(U, niter, renorm=True)
+    Ps = O.chain(P, 4)
+    Vref = O.price_from_kernels(Ps, xy, strikes, spec.r, 0.25 * np.arange(1, 5))
+    for mode, tol in [("bf16x3", 1e-5), ("fp32", 1e-5)]:
+        q, _ = lat.solve(strikes, 4, 0.25, 2.0 ** -16, mode=mode)
+        err = np.abs(q.cpu().numpy() - Vref[:, lat.y0, :]).max()
+        print(f"sv256 {mode}: {err:.3e}")
+        assert err <= tol, (mode, err)
+
+
+def test_black_scholes_lattice_on_gpu(cuda):
+    """The reference's known-answer test (tests/bstest/Program.cs:11-37) through the
+    device path: GBM, spot on a node, split-BF16 squaring."""
+    from oplib_b200.model import Lattice
+    n, i0 = 1024, 511
+    x = torch.from_numpy(O.centred_log_grid(n, 100.0, 8.0, i0)).to(cuda)
+    lat = Lattice.from_drift_vol(x, 0.05 * x, 0.25 * x, 0.05, s0=100.0)
+    assert lat.y0 == i0
+    q, _ = lat.solve([100.0], 4, 0.25, 2.0 ** -14, mode="bf16x3")
+    price = q.cpu().numpy()[3, 0]
+    assert abs(price - 12.33600) < 0.2  # lattice discretisation on a 1024-node grid
+    q32, _ = lat.solve([100.0], 4, 0.25, 2.0 ** -14, mode="fp32")
+    assert abs(price - q32.cpu().numpy()[3, 0]) < 1e-3
+
+
+def test_workspace_too_small_is_rejected(cuda):
+    from oplib_b200 import _lib
+    from oplib_b200.model import BF16X3
+    lat = _lv(256)
+    plan = lat.plan(0.25, 2.0 ** -14)
+    strikes = torch.linspace(0.5, 1.5, 64, dtype=torch.float64, device=cuda)
+    L = lat.desc(plan, 0.25, 2, strikes)
+    ws = torch.empty(1024, dtype=torch.uint8, device=cuda)
+    q = torch.empty(2, 64, dtype=torch.float64, device=cuda)
+    import ctypes as C
+    assert _lib.load().opb_lattice_solve(C.byref(L), BF16X3, ws.data_ptr(), 1024, q.data_ptr(), None) == -1

@@ -1,0 +1,152 @@
+"""CPU tests of the oracle itself: pins against independent implementations, the
+reference's known-answer test and mathematical identities (no GPU)."""
+import math
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from oracle import oracle_c as OC
+
+ROOT = Path(__file__).resolve().parents[1]
+GOLD = ROOT / "tests" / "golden"
+
+
+def _std_mt(seed, count, skip=0):
+    exe = ROOT / "oracle" / "mt_std_check"
+    if not exe.exists():
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), "-s"], check=True)
+    out = subprocess.run([str(exe), str(seed), str(count), str(skip)], capture_output=True, text=True, check=True)
+    return np.array([int(v) for v in out.stdout.split()], dtype=np.uint64).astype(np.uint32)
+
+
+def test_mt19937_cpp_standard_value():
+    # C++11 [rand.predef]: the 10000th output of a default-constructed mt19937 is 4123659995
+    assert int(OC.mt_outputs(5489, 10000)[-1]) == 4123659995
+    assert int(O.mt19937_outputs(np.array([5489]), 10000)[0, -1]) == 4123659995
+
+
+@pytest.mark.parametrize("seed", [0, 1, 5489, 12345, 2**32 - 1, 20260])
+def test_mt19937_matches_libstdcxx_and_numpy(seed):
+    std = _std_mt(seed, 1300)
+    c = OC.mt_outputs(seed, 1300)
+    py = O.mt19937_outputs(np.array([seed]), 1300)[0]
+    g = np.random.MT19937()
+    g._legacy_seeding(seed)
+    npy = g.random_raw(1300).astype(np.uint32)
+    assert np.array_equal(std, c)
+    assert np.array_equal(std, py)
+    assert np.array_equal(std, npy)
+
+
+def test_mt19937_golden_fixture():
+    gold = np.load(GOLD / "mt19937.npz")
+    for seed, ref in zip(gold["seeds"], gold["outputs"]):
+        assert np.array_equal(OC.mt_outputs(int(seed), ref.shape[0]), ref)
+
+
+def test_uniform_conversion_edges():
+    u = O.uniform_f32(np.array([0, 1, 2**24, 2**32 - 1, 2**31], dtype=np.uint32))
+    assert u[0] == np.float32(2.0 ** -32)
+    assert u[3] == np.float32(1.0)  # (float)(2^32-1) rounds to 2^32
+    for x in [0, 1, 255, 2**24 + 1, 2**32 - 1, 123456789]:
+        assert OC.load().oracle_uniform_f32(x) == O.uniform_f32(np.array([x], np.uint32))[0]
+
+
+def test_black_scholes_closed_form():
+    # tests/bstest/Program.cs:11-19: S=K=100, r=0.05, sigma=0.25, T=1
+    assert abs(float(O.bs_call(100.0, 100.0, 0.05, 0.25, 1.0)) - 12.33600) < 5e-5
+    iv = O.implied_vol(O.bs_call(1.0, 1.1, 0.02, 0.3, 0.7), 1.0, 1.1, 0.02, 0.7)
+    assert abs(float(iv) - 0.3) < 1e-9
+
+
+def test_lattice_black_scholes_known_answer():
+    """The reference's KAT (tests/bstest) as a lattice price: GBM on a log grid with the
+    spot on a node, FP64 squaring, price vs the closed form."""
+    n, i0, s0 = 1024, 511, 100.0
+    x = O.centred_log_grid(n, s0, width=8.0, i0=i0)
+    r, sig = 0.05, 0.25
+    L = O.lv_generator_fast(x, r * x, sig * x)
+    niter, dt = O.plan_niter(L, 1.0, 2.0 ** -14)
+    P = O.square(O.ek(L, dt), niter, renorm=True)
+    price = math.exp(-r) * (P[i0] @ np.maximum(x - 100.0, 0.0))
+    assert abs(price - 12.33600) < 2e-3 * 100 / 100  # lattice discretisation error, spot units
+
+
+def test_generator_rows_and_expm():
+    cfg = O.LVLattice(n=128)
+    L, x = cfg.generator()
+    assert np.allclose(L.sum(axis=1), 0.0, atol=1e-9)
+    assert (L - np.diag(np.diag(L)) >= 0).all()
+    niter, dt = O.plan_niter(L, 0.25, cfg.dt0)
+    P = O.square(O.ek(L, dt), niter)
+    from scipy.linalg import expm
+    assert np.abs(P - expm(L * 0.25)).max() < 1e-4  # first-order splitting error of (I+dt L)^(2^n)
+    assert np.abs(P.sum(axis=1) - 1).max() < 1e-12  # probability conservation
+
+
+def test_lv_generator_vectorised_matches_loop():
+    x = O.log_grid(64)
+    sig = O.lv_sigma(x)
+    assert np.allclose(O.lv_generator(x, 0.03 * x, sig * x), O.lv_generator_fast(x, 0.03 * x, sig * x),
+                       rtol=1e-12, atol=1e-9)
+
+
+def test_semigroup():
+    cfg = O.LVLattice(n=96)
+    L, x = cfg.generator()
+    niter, dt = O.plan_niter(L, 0.25, cfg.dt0)
+    P1 = O.square(O.ek(L, dt), niter)
+    P2 = O.square(O.ek(L, dt), niter + 1)
+    assert np.abs(P1 @ P1 - P2).max() < 1e-12
+
+
+def test_sv_generator_properties():
+    spec = O.SVSpec(nx=24, nv=8)
+    L, xy, vy = O.sv_generator(spec)
+    off = L - np.diag(np.diag(L))
+    assert (off >= 0).all()
+    assert np.allclose(L.sum(axis=1), 0, atol=1e-9)
+    # interior spot drift is exactly r*x after the fix-up
+    drift = L @ xy
+    inner = [y for y in range(spec.d) if 0 < y % spec.nx < spec.nx - 1]
+    assert np.allclose(drift[inner], spec.r * xy[inner], rtol=1e-9, atol=1e-12)
+
+
+def test_config0_golden_quotes():
+    gold = np.load(GOLD / "lattice_lv512.npz")
+    cfg = O.LVLattice()
+    L, x = cfg.generator()
+    V, niter, dt = O.solve_lattice_fp64(L, x, cfg.strikes, cfg.r, cfg.period, cfg.nmat, cfg.dt0)
+    y0 = O.nearest_node(x)
+    assert niter == int(gold["niter"]) == 12
+    assert np.abs(V[:, y0, :] - gold["quotes"]).max() < 1e-12
+
+
+def test_sck_c_matches_numpy():
+    rng = np.random.default_rng(3)
+    P = rng.random((40, 77)).astype(np.float32)
+    P[3, 5] = -1e-9  # rounding residue counts as zero
+    P /= P.sum(axis=1, keepdims=True)
+    assert np.array_equal(OC.sck(P), O.cumrows_f32(P))
+
+
+def test_mc_c_matches_numpy():
+    cfg = O.LVLattice(n=64)
+    L, x = cfg.generator()
+    niter, dt = O.plan_niter(L, 1 / 252, cfg.dt0)
+    P = O.square(O.ek(L, dt), niter)
+    Cm = O.cumrows_f32(P)
+    paths_c, _ = OC.mc_paths(Cm, 32, 5489, 0, 300, 40)
+    paths_py = O.mc_paths(Cm, 32, 5489, np.arange(300), 40)
+    assert np.array_equal(paths_c, paths_py)
+
+
+def test_mc_golden_fixture():
+    gold = np.load(GOLD / "mc_small.npz")
+    paths, sums = OC.mc_paths(gold["C"], int(gold["y0"]), int(gold["seed"]), 0, gold["paths"].shape[0],
+                              gold["paths"].shape[1], x=gold["x"], disc=float(gold["disc"]))
+    assert np.array_equal(paths, gold["paths"])
+    assert np.allclose(sums, gold["sums"], rtol=1e-12)
