@@ -193,6 +193,9 @@ int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspace, unsi
  * kernel; nmat, nK and strikes of L are ignored */
 int opb_lattice_kernel(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
                        float *P_out);
+/* new: issue every tensor-core product of the solve as s K-slices summed in the FP32
+ * epilogue (shorter in-TMEM accumulation chains); 0 (default) = automatic */
+int opb_set_ksplit(int s);
 
 /* ------------------------------------------------------------------ cumulative rows, MC */
 /* replaces oplib/opcuda/sck.cu:88-93: nm column-major kernels -> cumulative normalised rows */

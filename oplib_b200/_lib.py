@@ -94,6 +94,7 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_lattice_workspace_size": (ull, [i32, i32, i32]),
     "opb_lattice_solve": (i32, [C.POINTER(LatticeDesc), i32, vp, ull, vp, vp]),
     "opb_lattice_kernel": (i32, [C.POINTER(LatticeDesc), i32, vp, ull, vp]),
+    "opb_set_ksplit": (i32, [i32]),
     # cumulative rows / MC
     "opcuda_sck": (i32, [i32, i32, u64, u64]),
     "opb_sck_rm": (i32, [i32, i32, vp, vp]),

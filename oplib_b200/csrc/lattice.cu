@@ -43,6 +43,7 @@ struct opb_lattice_desc {
 };
 
 namespace {
+int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s);
 
 struct Ws {
     // carve a workspace into 256-byte aligned pieces
@@ -63,9 +64,12 @@ struct Bufs {
     double *part;
 };
 
+inline int padded_nk(int nK, int mode) { return mode == OPB_BF16X3 ? (nK + 63) / 64 * 64 : nK; }
+
 Bufs carve(Ws &w, int d, int nK, int mode) {
     Bufs b{};
     size_t dd = (size_t)d * d;
+    nK = padded_nk(nK, mode);
     b.X = w.take<float>(dd);
     b.Pa = w.take<float>(dd);
     if (mode != OPB_BF16X3) b.Pb = w.take<float>(dd);
@@ -114,7 +118,7 @@ int solve_fp32(const opb_lattice_desc &L, int mode, Bufs &b, double *quotes, dou
     float *chain[2];
     for (int i = 0, k = 0; i < 3; i++)
         if (i != cur) chain[k++] = buf[i];
-    LT(opb::launch_payoff(d, nK, L.x, L.strikes, b.G, nullptr, nullptr, s));
+    LT(opb::launch_payoff(d, nK, nK, L.x, L.strikes, b.G, nullptr, nullptr, s));
     const float *Pm = P1;
     for (int m = 1; m <= L.nmat; m++) {
         if (m > 1) {
@@ -128,8 +132,35 @@ int solve_fp32(const opb_lattice_desc &L, int mode, Bufs &b, double *quotes, dou
         }
         LT(opb::sgemm_rm(d, nK, d, 1.f, Pm, d, b.G, nK, 0.f, b.V, nK, s));
         const double disc = std::exp(-L.rate * L.period * m);
-        LT(opb::launch_discount(d, nK, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d * nK : nullptr, L.y0,
+        LT(opb::launch_discount(d, nK, nK, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d * nK : nullptr, L.y0,
                                 quotes + (size_t)(m - 1) * nK, s));
+    }
+    return 0;
+}
+
+// Issue every tensor-core product as S K-slices accumulated through the FP32 epilogue
+// (C = slice + 1*C, round-to-nearest), which shortens each in-TMEM accumulation chain:
+// the tensor cores truncate the FP32 accumulator, a bias of about half an ulp per MMA.
+// 0 = automatic: 2 slices for K > 2048 (keeps the truncated in-TMEM FP32 accumulation
+// chain at <= 96 MMA instructions per 16-wide step group), else 1.
+int g_ksplit = 0;
+
+int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s) {
+    int S = g_ksplit > 0 ? g_ksplit : (a.K > 2048 ? 2 : 1);
+    int kb = a.K / 64;
+    if (S <= 1 || kb < S || kb % S) return opb::launch_tc_gemm(a, s);
+    const int kslice = a.K / S;
+    for (int i = 0; i < S; i++) {
+        opb::TcGemmArgs t = a;
+        t.K = kslice;
+        t.Ahi = a.Ahi + (size_t)i * kslice;
+        t.Alo = a.Alo + (size_t)i * kslice;
+        t.Bhi = a.Bhi + (size_t)i * kslice;
+        t.Blo = a.Blo + (size_t)i * kslice;
+        if (i > 0) { t.Cin = a.C; t.beta = 1.f; }
+        if (i + 1 < S) t.rowsum = nullptr;
+        int r = opb::launch_tc_gemm(t, s);
+        if (r) return r;
     }
     return 0;
 }
@@ -147,7 +178,7 @@ int solve_bf16x3(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_a
     for (int r = 0; r < L.niter; r++) {
         // D = 2E + E.E in place of E, with FP64 row-sum partials
         g.C = b.X; g.Cin = b.X; g.alpha = 1.f; g.beta = 2.f; g.rowsum = b.part;
-        LT(opb::launch_tc_gemm(g, s));
+        LT(tc_gemm_ksplit(g, s));
         const bool last = (r + 1 == L.niter);
         LT(opb::launch_renorm(d, b.X, b.part, np, 1, last ? nullptr : b.Ahi, b.Alo, last ? nullptr : b.Bhi, b.Blo, s));
     }
@@ -155,20 +186,21 @@ int solve_bf16x3(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_a
     LT(opb::launch_add_identity(d, b.X, s));
     if (P_out) return (int)cudaMemcpyAsync(P_out, b.X, sizeof(float) * (size_t)d * d, cudaMemcpyDeviceToDevice, s);
     LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s));
-    LT(opb::launch_payoff(d, nK, L.x, L.strikes, nullptr, b.GThi, b.GTlo, s));
+    const int nKp = padded_nk(nK, OPB_BF16X3);
+    LT(opb::launch_payoff(d, nK, nKp, L.x, L.strikes, nullptr, b.GThi, b.GTlo, s));
     opb::TcGemmArgs pg{};
-    pg.M = d; pg.N = nK; pg.K = d; pg.lda = d; pg.ldb = d; pg.ldc = nK;
+    pg.M = d; pg.N = nKp; pg.K = d; pg.lda = d; pg.ldb = d; pg.ldc = nKp;
     pg.Ahi = b.Ahi; pg.Alo = b.Alo; pg.Bhi = b.GThi; pg.Blo = b.GTlo; pg.C = b.V; pg.alpha = 1.f; pg.beta = 0.f;
     for (int m = 1; m <= L.nmat; m++) {
         if (m > 1) {
             // P_m = P_{m-1} . P1 (A splits hold P_{m-1}), renormalise, split row-major into A
             g.C = b.Pa; g.Cin = nullptr; g.alpha = 1.f; g.beta = 0.f; g.rowsum = b.part;
-            LT(opb::launch_tc_gemm(g, s));
+            LT(tc_gemm_ksplit(g, s));
             LT(opb::launch_renorm(d, b.Pa, b.part, np, 0, b.Ahi, b.Alo, nullptr, nullptr, s));
         }
-        LT(opb::launch_tc_gemm(pg, s));
+        LT(tc_gemm_ksplit(pg, s));
         const double disc = std::exp(-L.rate * L.period * m);
-        LT(opb::launch_discount(d, nK, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d * nK : nullptr, L.y0,
+        LT(opb::launch_discount(d, nK, nKp, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d * nK : nullptr, L.y0,
                                 quotes + (size_t)(m - 1) * nK, s));
     }
     return 0;
@@ -187,12 +219,18 @@ int check_desc(const opb_lattice_desc *L, int mode) {
     if (mode < OPB_FP32_PLAIN || mode > OPB_BF16X3) return OPB_E_ARG;
     if (mode == OPB_BF16X3) {
         if (L->d % 128 != 0) return OPB_E_UNSUPPORTED;
-        if (!opb::tc_gemm_tile_n(L->nK) || opb::tc_gemm_tile_n(L->d) == 0) return OPB_E_UNSUPPORTED;
+        if (opb::tc_gemm_tile_n(L->d) == 0) return OPB_E_UNSUPPORTED;
     }
     return OPB_OK;
 }
 
 }  // namespace
+
+OPB_API int opb_set_ksplit(int s) {
+    OPB_REQUIRE(s >= 0 && s <= 64, OPB_E_ARG);
+    g_ksplit = s;
+    return opb::set_status(OPB_OK);
+}
 
 // Workspace bytes for opb_lattice_solve.
 OPB_API unsigned long long opb_lattice_workspace_size(int d, int nK, int mode) {

@@ -21,9 +21,9 @@ int launch_rowsum(int d, const float *X, double *partial, cudaStream_t s);
 int launch_renorm(int d, float *X, const double *partial, int nparts, int eform, __nv_bfloat16 *Ahi,
                   __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s);
 int launch_add_identity(int d, float *X, cudaStream_t s);
-int launch_payoff(int d, int nK, const double *x, const double *K, float *G, __nv_bfloat16 *GThi,
+int launch_payoff(int d, int nK, int ldk, const double *x, const double *K, float *G, __nv_bfloat16 *GThi,
                   __nv_bfloat16 *GTlo, cudaStream_t s);
-int launch_discount(int d, int nK, const float *V32, double disc, double *V64, int y0, double *quotes,
+int launch_discount(int d, int nK, int ldk, const float *V32, double disc, double *V64, int y0, double *quotes,
                     cudaStream_t s);
 
 // gemm_tc.cu -- split-BF16 tensor-core GEMM.

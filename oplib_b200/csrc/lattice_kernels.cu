@@ -173,12 +173,13 @@ __global__ void k_add_identity(int d, float *__restrict__ X) {
 
 // G[z, k] = (x_z - K_k)^+ (FP32, d x nK row-major) and its split transpose
 // G^T hi/lo (nK x d) for the tensor-core pricing GEMM.
-__global__ void k_payoff(int d, int nK, const double *__restrict__ x, const double *__restrict__ K,
+// Strike columns nK..ldk-1 (padding to the tensor-core tile width) get zero payoffs.
+__global__ void k_payoff(int d, int nK, int ldk, const double *__restrict__ x, const double *__restrict__ K,
                          float *__restrict__ G, __nv_bfloat16 *__restrict__ GThi, __nv_bfloat16 *__restrict__ GTlo) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= (long long)d * nK) return;
-    int z = (int)(t / nK), k = (int)(t - (long long)z * nK);
-    double g = x[z] - K[k];
+    if (t >= (long long)d * ldk) return;
+    int z = (int)(t / ldk), k = (int)(t - (long long)z * ldk);
+    double g = k < nK ? x[z] - K[k] : 0.0;
     float f = (float)(g > 0.0 ? g : 0.0);
     if (G) G[t] = f;
     if (GThi) {
@@ -189,15 +190,15 @@ __global__ void k_payoff(int d, int nK, const double *__restrict__ x, const doub
     }
 }
 
-// V64[y, k] = disc * V32[y, k]; quotes[k] = V64[y0, k].
-__global__ void k_discount(int d, int nK, const float *__restrict__ V32, double disc, double *__restrict__ V64,
-                           int y0, double *__restrict__ quotes) {
+// V64[y, k] = disc * V32[y, k] (V32 leading dimension ldk >= nK); quotes[k] = V64[y0, k].
+__global__ void k_discount(int d, int nK, int ldk, const float *__restrict__ V32, double disc,
+                           double *__restrict__ V64, int y0, double *__restrict__ quotes) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)d * nK) return;
-    double v = disc * (double)V32[t];
+    int y = (int)(t / nK), k = (int)(t - (long long)y * nK);
+    double v = disc * (double)V32[(long long)y * ldk + k];
     if (V64) V64[t] = v;
-    int y = (int)(t / nK);
-    if (quotes && y == y0) quotes[t - (long long)y * nK] = v;
+    if (quotes && y == y0) quotes[k] = v;
 }
 
 // ------------------------------------------------------------------ host launchers
@@ -246,17 +247,17 @@ int launch_add_identity(int d, float *X, cudaStream_t s) {
     return (int)cudaGetLastError();
 }
 
-int launch_payoff(int d, int nK, const double *x, const double *K, float *G, __nv_bfloat16 *GThi,
+int launch_payoff(int d, int nK, int ldk, const double *x, const double *K, float *G, __nv_bfloat16 *GThi,
                   __nv_bfloat16 *GTlo, cudaStream_t s) {
-    long long n = (long long)d * nK;
-    k_payoff<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, x, K, G, GThi, GTlo);
+    long long n = (long long)d * ldk;
+    k_payoff<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, x, K, G, GThi, GTlo);
     return (int)cudaGetLastError();
 }
 
-int launch_discount(int d, int nK, const float *V32, double disc, double *V64, int y0, double *quotes,
+int launch_discount(int d, int nK, int ldk, const float *V32, double disc, double *V64, int y0, double *quotes,
                     cudaStream_t s) {
     long long n = (long long)d * nK;
-    k_discount<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, V32, disc, V64, y0, quotes);
+    k_discount<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, V32, disc, V64, y0, quotes);
     return (int)cudaGetLastError();
 }
 

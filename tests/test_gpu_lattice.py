@@ -75,8 +75,9 @@ def test_config0_quotes_vs_fp64(cuda, config0_fp64, mode, tol):
     err = np.abs(q.cpu().numpy() - V[:, y0, :]).max()
     print(f"config0 {mode}: max abs quote error {err:.3e}")
     assert err <= tol
-    # all source states (the backward induction result), same bound away from the far boundary
-    errall = np.abs(Vall.cpu().numpy() - V).max()
+    # all source states (the backward induction result): relative to the option value
+    # (values reach ~4.5 at the far spot boundary)
+    errall = (np.abs(Vall.cpu().numpy() - V) / np.maximum(1.0, np.abs(V))).max()
     assert errall <= 5 * tol
 
 
@@ -119,7 +120,7 @@ def test_black_scholes_lattice_on_gpu(cuda):
     x = torch.from_numpy(O.centred_log_grid(n, 100.0, 8.0, i0)).to(cuda)
     lat = Lattice.from_drift_vol(x, 0.05 * x, 0.25 * x, 0.05, s0=100.0)
     assert lat.y0 == i0
-    q, _ = lat.solve([100.0], 4, 0.25, 2.0 ** -14, mode="bf16x3")
+    q, _ = lat.solve([100.0], 4, 0.25, 2.0 ** -14, mode="bf16x3")  # nK = 1: padded to the tile internally
     price = q.cpu().numpy()[3, 0]
     assert abs(price - 12.33600) < 0.2  # lattice discretisation on a 1024-node grid
     q32, _ = lat.solve([100.0], 4, 0.25, 2.0 ** -14, mode="fp32")
