@@ -221,6 +221,17 @@ int opb_mc_scratch_blocks(long long npaths);
 int opb_mc_mt19937(const float *C, long long row_stride, long long col_stride, const uint32_t *guide, int nb, int d,
                    int y0, int nsteps, uint32_t seed, unsigned long long path0, long long npaths, short *ypaths,
                    const double *x, double strike, double barrier, double disc, double *scratch, double *sums);
+/* new, no counterpart in the reference: opb_mc_mt19937 without the scratch argument, for
+ * callers that must not let the library allocate device memory (a host framework that owns
+ * the device-memory budget, or a loop that cannot afford cudaMalloc's implicit device
+ * synchronisation).  The payoff partial sums use a fixed 64 KiB device array inside the
+ * library (held by every GPU that loads it until exit); results are bit-identical to
+ * opb_mc_mt19937.  Grids above 4096 blocks (devices with more than 512 SMs) return
+ * OPB_E_UNSUPPORTED.  The first call on a device looks up the array's device address (make
+ * it before any stream capture); calls that overlap on the GPU share the array and race. */
+int opb_mc_mt19937_noalloc(const float *C, long long row_stride, long long col_stride, const uint32_t *guide, int nb,
+                           int d, int y0, int nsteps, uint32_t seed, unsigned long long path0, long long npaths,
+                           short *ypaths, const double *x, double strike, double barrier, double disc, double *sums);
 int opb_mt19937_raw(uint32_t seed, long long nstreams, int n, uint32_t *out);
 int opb_mt_uniforms(uint32_t seed, long long nstreams, int nper, float *unif);
 

@@ -107,6 +107,8 @@ PROTOTYPES: dict[str, tuple] = {
     "opcuda_mt_benchmark": (i32, [u64, u64, i32]),
     "opb_mc_scratch_blocks": (i32, [i64]),
     "opb_mc_mt19937": (i32, [vp, i64, i64, vp, i32, i32, i32, i32, u32, ull, i64, vp, vp, f64, f64, f64, vp, vp]),
+    "opb_mc_mt19937_noalloc": (i32, [vp, i64, i64, vp, i32, i32, i32, i32, u32, ull, i64, vp, vp, f64, f64, f64,
+                                     vp]),
     "opb_mt19937_raw": (i32, [u32, i64, i32, vp]),
     "opb_mt_uniforms": (i32, [u32, i64, i32, vp]),
 }

@@ -22,6 +22,8 @@
 // Payoffs (discretely monitored down-and-out call, arithmetic-Asian call) are reduced per
 // path in registers and per block in FP64; the optional int16 state output uses the
 // reference's layout y_sk[path + npaths*k] (oplib/opcuda/smc.cu:331).
+#include <mutex>
+
 #include "common.cuh"
 #include "lattice.h"
 
@@ -337,4 +339,67 @@ OPB_API int opb_mt_uniforms(uint32_t seed, long long nstreams, int nper, float *
     OPB_REQUIRE(unif != nullptr, OPB_E_NULL);
     k_mt_bench<<<(int)((nstreams + 255) / 256), 256, 0, stream()>>>(seed, nstreams, nper, unif);
     return launch_check();
+}
+
+// ---------------------------------------------------------------- allocation-free variant
+//
+// Some callers cannot let a library allocate device memory: a host framework that owns
+// the whole device-memory budget and hands libraries only the buffers it has accounted
+// for (a managed P/Invoke pricing engine is the typical case), or a latency-critical
+// pricing loop that cannot afford cudaMalloc's implicit device-wide synchronisation.
+// opb_mc_mt19937_noalloc serves them: it is opb_mc_mt19937 without the scratch argument.
+// The per-block payoff partial sums live in a fixed file-scope device array of
+// OPB_MC_NOALLOC_MAX_BLOCKS x 2 doubles (64 KiB), which every GPU that loads the library
+// keeps until the process exits.  The grid is the one opb_mc_mt19937 uses for the same
+// npaths (at most 8 blocks per SM), so results are bit-identical to it; a grid larger than
+// the array -- only possible on a device with more than 512 SMs -- is rejected with
+// OPB_E_UNSUPPORTED.  All calls share the array and it keeps the last call's contents (each
+// call overwrites the partials of the blocks it launches before reading them), so calls
+// that overlap on the GPU -- concurrent streams, or several host threads -- race on it and
+// must be serialised by the caller.
+//
+// Host code cannot use the array's name as a device address, so the device address is
+// looked up with cudaGetSymbolAddress once per device, with that device current, by the
+// first call made on that device; make that first call before any stream capture.
+
+#define OPB_MC_NOALLOC_MAX_BLOCKS 4096
+
+static __device__ __align__(256) double g_mc_noalloc_scratch[2 * OPB_MC_NOALLOC_MAX_BLOCKS];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[64] = {nullptr};
+
+int noalloc_scratch(double **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (int)e;
+    if (dev < 0 || dev >= 64) return OPB_E_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_mc_noalloc_scratch);
+        if (e != cudaSuccess) return (int)e;
+        g_noalloc_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return OPB_OK;
+}
+
+}  // namespace
+
+OPB_API int opb_mc_mt19937_noalloc(const float *C, long long row_stride, long long col_stride,
+                                   const uint32_t *guide, int nb, int d, int y0, int nsteps, uint32_t seed,
+                                   unsigned long long path0, long long npaths, short *ypaths, const double *x,
+                                   double strike, double barrier, double disc, double *sums) {
+    OPB_REQUIRE(npaths >= 0, OPB_E_ARG);
+    OPB_REQUIRE(mc_grid(npaths) <= OPB_MC_NOALLOC_MAX_BLOCKS, OPB_E_UNSUPPORTED);
+    double *scratch = nullptr;
+    if (x) {
+        int r = noalloc_scratch(&scratch);
+        if (r != OPB_OK) return set_status(r);
+    }
+    return opb_mc_mt19937(C, row_stride, col_stride, guide, nb, d, y0, nsteps, seed, path0, npaths, ypaths, x,
+                          strike, barrier, disc, scratch, sums);
 }
