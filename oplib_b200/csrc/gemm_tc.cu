@@ -8,17 +8,21 @@
 // of oplib/opcuda/ssqmm.cu:119-179 on the lattice path.  Operands are K-major (rows of A
 // and rows of B^T contiguous), M % 128 == 0, N % BN == 0, K % 64 == 0.
 //
-// Structure (one 128 x BN output tile per CTA, 128 threads):
-//   warp 0, one lane : TMA producer -- 4 tiled bulk-tensor loads per K-block (Ahi, Alo,
-//                      Bhi, Blo; 128B swizzle; no multicast) into a STAGES-deep ring,
-//                      completion tracked by mbarrier transaction counts.
-//   warp 1, one lane : MMA issuer -- per 16-wide K step three tcgen05.mma.kind::f16
-//                      (BF16 x BF16 -> FP32) into one TMEM accumulator of BN columns;
-//                      tcgen05.commit releases each stage and finally signals the
-//                      epilogue.
-//   all 4 warps      : epilogue -- tcgen05.ld of the thread's accumulator row, the
-//                      alpha/beta update, FP32 stores and the FP64 row sum of the stored
-//                      values (rowsum[n_tile * M + row], used by the row renormalisation).
+// Structure (persistent: one CTA per SM over 128 x BN output tiles):
+//   TMA warp, one lane : 4 tiled bulk-tensor loads per K-block (Ahi, Alo, Bhi, Blo; 128B
+//                        swizzle; no multicast) into a STAGES-deep ring, completion
+//                        tracked by mbarrier transaction counts.
+//   MMA warp, one lane : per 16-wide K step three tcgen05.mma.kind::f16 (BF16 x BF16 ->
+//                        FP32) into one of two TMEM accumulators (BN columns each), one
+//                        accumulator per chunk of 2 K-blocks; tcgen05.commit releases
+//                        each stage and hands each finished chunk to the epilogue.
+//   epilogue warps     : (4 lane quadrants x BN/128 column groups) tcgen05.ld of each
+//                        finished chunk into FP32 round-to-nearest register sums; after a
+//                        tile's last chunk, the alpha/beta update, FP32 stores and FP64
+//                        row sums of the stored values (rowsum[group * M + row], one per
+//                        128 columns, used by the row renormalisation).
+// The tensor cores truncate their FP32 accumulator (about half an ulp per MMA); chunked
+// accumulation bounds that bias by 24 MMAs instead of 3K/16.
 // Every mbarrier wait is bounded by a %globaltimer deadline; on expiry the kernel records
 // an error code in g_tc_error, drains its outstanding copies and MMAs, frees TMEM and
 // returns.
@@ -134,6 +138,12 @@ struct TcCfg {
     static constexpr int B_BYTES = BN * TC_BK * 2;     // one of Bhi/Blo
     static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+    static constexpr int CPT = BN < 128 ? BN : 128;        // accumulator columns per epilogue thread
+    static constexpr int HALVES = BN / CPT;                 // column groups per TMEM lane
+    static constexpr int EPI_WARPS = 4 * HALVES;            // epilogue warps (4 lane quadrants x groups)
+    static constexpr int THREADS = 32 * (EPI_WARPS + 2);    // + TMA producer warp + MMA warp
+    static constexpr int TMEM_COLS = 2 * BN;                // two accumulators (ping-pong chunks)
+    static constexpr int CHUNK = 2;                         // K-blocks accumulated in TMEM per chunk
 };
 
 struct TcParams {
@@ -145,41 +155,67 @@ struct TcParams {
     double *rowsum;
 };
 
+// Persistent kernel: one CTA per SM walks the output tiles t = blockIdx.x + i*gridDim.x
+// (grouped raster, 8 M-tiles per group).  The K loop of a tile runs in chunks of
+// CHUNK K-blocks; chunk g accumulates in TMEM accumulator g&1 starting from zero, and the
+// epilogue warps add each finished chunk into FP32 register sums (round to nearest) while
+// the MMA warp fills the other accumulator.  The tensor cores' truncating accumulation
+// thus spans only 12*CHUNK MMA instructions, and the tile's final store overlaps the next
+// tile's MMAs.
 template <int BN, int STAGES>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
               const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p) {
     using Cfg = TcCfg<BN, STAGES>;
+    constexpr int EPI = Cfg::EPI_WARPS;
+    constexpr int CPT = Cfg::CPT;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t *gbase = smem_raw + (base - raw);
-    // barrier block after the stages
     uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + STAGES * Cfg::STAGE_BYTES);
     const uint32_t bar0 = smem_u32(bars);
     auto full_bar = [&](int s) { return bar0 + 8u * s; };
     auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
-    const uint32_t done_bar = bar0 + 8u * (2 * STAGES);
-    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bars + 2 * STAGES + 1);
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * STAGES + 2);
+    auto accf_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + a); };      // MMA -> epilogue
+    auto acce_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + 2 + a); };  // epilogue -> MMA
+    const uint32_t drain_bar = bar0 + 8u * (2 * STAGES + 4);
+    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bars + 2 * STAGES + 5);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * STAGES + 6);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * TC_BM;
     const int nk = p.K / TC_BK;
+    const int nchunks = (nk + Cfg::CHUNK - 1) / Cfg::CHUNK;
+    const int mtiles = p.M / TC_BM, ntiles_n = p.N / BN, ntiles = mtiles * ntiles_n;
+    auto tile_coords = [&](int t, int &m0, int &n0) {
+        const int GM = 8;
+        const int per_group = GM * ntiles_n;
+        const int group = t / per_group;
+        const int first_m = group * GM;
+        const int gm = min(mtiles - first_m, GM);
+        const int r = t - group * per_group;
+        m0 = (first_m + r % gm) * TC_BM;
+        n0 = (r / gm) * BN;
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
             mbar_init(full_bar(s), 1);
             mbar_init(empty_bar(s), 1);
         }
-        mbar_init(done_bar, 1);
+        for (int a = 0; a < 2; a++) {
+            mbar_init(accf_bar(a), 1);
+            mbar_init(acce_bar(a), EPI * 32);
+        }
+        mbar_init(drain_bar, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     if (warp == 0) {
         const uint32_t slot = smem_u32(const_cast<uint32_t *>(tmem_slot));
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(BN)
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+                     "r"(Cfg::TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -188,113 +224,153 @@ __global__ void __launch_bounds__(128, 1)
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0) {
+    if (warp == EPI) {
         if (lane == 0) {
             // ---------------- TMA producer
-            int issued = 0;
+            long kbg = 0;  // K-blocks issued over the CTA's lifetime (stage ring position)
             bool ok = true;
-            for (int kb = 0; kb < nk; kb++) {
-                const int s = kb % STAGES;
-                if (kb >= STAGES) {
-                    if (!mbar_wait(empty_bar(s), ((kb / STAGES) + 1) & 1, abort_flag, TC_WAIT_NS)) {
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                int m0, n0;
+                tile_coords(t, m0, n0);
+                for (int kb = 0; kb < nk; kb++, kbg++) {
+                    const int s = (int)(kbg % STAGES);
+                    if (kbg >= STAGES &&
+                        !mbar_wait(empty_bar(s), (uint32_t)(((kbg / STAGES) + 1) & 1), abort_flag, TC_WAIT_NS)) {
                         ok = false;
                         break;
                     }
+                    const uint32_t st = base + s * Cfg::STAGE_BYTES;
+                    mbar_expect_tx(full_bar(s), Cfg::STAGE_BYTES);
+                    const int kx = kb * TC_BK;
+                    tma_load_2d(st, &mAhi, full_bar(s), kx, m0);
+                    tma_load_2d(st + Cfg::A_BYTES, &mAlo, full_bar(s), kx, m0);
+                    tma_load_2d(st + 2 * Cfg::A_BYTES, &mBhi, full_bar(s), kx, n0);
+                    tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, &mBlo, full_bar(s), kx, n0);
                 }
-                const uint32_t st = base + s * Cfg::STAGE_BYTES;
-                mbar_expect_tx(full_bar(s), Cfg::STAGE_BYTES);
-                const int kx = kb * TC_BK;
-                tma_load_2d(st, &mAhi, full_bar(s), kx, m0);
-                tma_load_2d(st + Cfg::A_BYTES, &mAlo, full_bar(s), kx, m0);
-                tma_load_2d(st + 2 * Cfg::A_BYTES, &mBhi, full_bar(s), kx, n0);
-                tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, &mBlo, full_bar(s), kx, n0);
-                issued++;
             }
             if (!ok) {
                 atomicExch(&g_tc_error, 1);
                 *abort_flag = 1;
-                // drain the copies that may still be in flight (at most STAGES)
-                const int first = issued > STAGES ? issued - STAGES : 0;
-                for (int kb = first; kb < issued; kb++)
-                    (void)mbar_wait(full_bar(kb % STAGES), (kb / STAGES) & 1, abort_flag, 100000000ull);
+                const long first = kbg > STAGES ? kbg - STAGES : 0;
+                for (long k = first; k < kbg; k++)
+                    (void)mbar_wait(full_bar((int)(k % STAGES)), (uint32_t)((k / STAGES) & 1), abort_flag,
+                                    100000000ull);
             }
         }
         __syncwarp();
-    } else if (warp == 1) {
+    } else if (warp == EPI + 1) {
         if (lane == 0) {
             // ---------------- MMA issuer
             const uint32_t idesc = umma_idesc_bf16(BN);
+            long kbg = 0, g = 0;  // K-blocks consumed, chunks issued
             bool ok = true;
-            for (int kb = 0; kb < nk; kb++) {
-                const int s = kb % STAGES;
-                if (!mbar_wait(full_bar(s), (kb / STAGES) & 1, abort_flag, TC_WAIT_NS)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t st = base + s * Cfg::STAGE_BYTES;
-                const uint64_t dAh = umma_desc_sw128(st);
-                const uint64_t dAl = umma_desc_sw128(st + Cfg::A_BYTES);
-                const uint64_t dBh = umma_desc_sw128(st + 2 * Cfg::A_BYTES);
-                const uint64_t dBl = umma_desc_sw128(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES);
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                for (int c = 0; c < nchunks && ok; c++, g++) {
+                    const int a = (int)(g & 1);
+                    if (g >= 2 && !mbar_wait(acce_bar(a), (uint32_t)(((g >> 1) + 1) & 1), abort_flag, TC_WAIT_NS)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t dacc = tmem + (uint32_t)(a * BN);
+                    const int kb_end = min(nk, (c + 1) * Cfg::CHUNK);
+                    for (int kb = c * Cfg::CHUNK; kb < kb_end; kb++, kbg++) {
+                        const int s = (int)(kbg % STAGES);
+                        if (!mbar_wait(full_bar(s), (uint32_t)((kbg / STAGES) & 1), abort_flag, TC_WAIT_NS)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t st = base + s * Cfg::STAGE_BYTES;
+                        const uint64_t dAh = umma_desc_sw128(st);
+                        const uint64_t dAl = umma_desc_sw128(st + Cfg::A_BYTES);
+                        const uint64_t dBh = umma_desc_sw128(st + 2 * Cfg::A_BYTES);
+                        const uint64_t dBl = umma_desc_sw128(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES);
 #pragma unroll
-                for (int k16 = 0; k16 < TC_BK / 16; k16++) {
-                    const uint64_t adv = (uint64_t)((k16 * 32) >> 4);  // +32 bytes along K
-                    const uint32_t acc0 = (kb > 0 || k16 > 0) ? 1u : 0u;
-                    umma_bf16(tmem, dAh + adv, dBh + adv, idesc, acc0);
-                    umma_bf16(tmem, dAh + adv, dBl + adv, idesc, 1u);
-                    umma_bf16(tmem, dAl + adv, dBh + adv, idesc, 1u);
+                        for (int k16 = 0; k16 < TC_BK / 16; k16++) {
+                            const uint64_t adv = (uint64_t)((k16 * 32) >> 4);  // +32 bytes along K
+                            const uint32_t acc0 = (kb > c * Cfg::CHUNK || k16 > 0) ? 1u : 0u;
+                            umma_bf16(dacc, dAh + adv, dBh + adv, idesc, acc0);
+                            umma_bf16(dacc, dAh + adv, dBl + adv, idesc, 1u);
+                            umma_bf16(dacc, dAl + adv, dBh + adv, idesc, 1u);
+                        }
+                        umma_commit(empty_bar(s));
+                    }
+                    if (ok) umma_commit(accf_bar(a));
                 }
-                umma_commit(empty_bar(s));
             }
             if (!ok) {
                 atomicExch(&g_tc_error, 2);
                 *abort_flag = 1;
             }
-            umma_commit(done_bar);  // arrives once every issued MMA has completed
+            umma_commit(drain_bar);  // arrives once every issued MMA has completed
+            (void)mbar_wait(drain_bar, 0, abort_flag, TC_WAIT_NS);
         }
         __syncwarp();
-    }
-
-    // ---------------- epilogue (all 128 threads; warp w owns TMEM lanes 32w..32w+31)
-    bool ok = mbar_wait(done_bar, 0, abort_flag, TC_WAIT_NS);
-    tc_fence_after();
-    if (!ok) atomicExch(&g_tc_error, 3);
-    if (ok && !*abort_flag) {
-        const int row = m0 + warp * 32 + lane;
-        float *crow = p.C + (long long)row * p.ldc + n0;
-        const float *cin = p.Cin ? p.Cin + (long long)row * p.ldc + n0 : nullptr;
-        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-        double rs = 0.0;
-#pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 32) {
-            uint32_t v[32];
-            tmem_ld32(trow + (uint32_t)c0, v);
+    } else {
+        // ---------------- epilogue warps: lane quadrant q, column group h
+        const int q = warp & 3, h = warp >> 2;
+        const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+        float sum[CPT];
+        long g = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+            int m0, n0;
+            tile_coords(t, m0, n0);
 #pragma unroll
-            for (int j = 0; j < 32; j += 4) {
+            for (int j = 0; j < CPT; j++) sum[j] = 0.f;
+            for (int c = 0; c < nchunks; c++, g++) {
+                const int a = (int)(g & 1);
+                if (!mbar_wait(accf_bar(a), (uint32_t)((g >> 1) & 1), abort_flag, TC_WAIT_NS)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t tacc = tmem + lane_base + (uint32_t)(a * BN + h * CPT);
+#pragma unroll
+                for (int j = 0; j < CPT / 32; j++) {
+                    uint32_t v[32];
+                    tmem_ld32(tacc + (uint32_t)(32 * j), v);
+#pragma unroll
+                    for (int i = 0; i < 32; i++)
+                        sum[32 * j + i] = __fadd_rn(sum[32 * j + i], __uint_as_float(v[i]));
+                }
+                tc_fence_before();
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acce_bar(a)) : "memory");
+            }
+            if (!ok || *abort_flag) break;
+            const int row = m0 + q * 32 + lane;
+            const int col0 = n0 + h * CPT;
+            float *crow = p.C + (long long)row * p.ldc + col0;
+            const float *cin = p.Cin ? p.Cin + (long long)row * p.ldc + col0 : nullptr;
+            double rs = 0.0;
+#pragma unroll
+            for (int j = 0; j < CPT; j += 4) {
                 float4 o;
-                o.x = p.alpha * __uint_as_float(v[j + 0]);
-                o.y = p.alpha * __uint_as_float(v[j + 1]);
-                o.z = p.alpha * __uint_as_float(v[j + 2]);
-                o.w = p.alpha * __uint_as_float(v[j + 3]);
+                o.x = p.alpha * sum[j + 0];
+                o.y = p.alpha * sum[j + 1];
+                o.z = p.alpha * sum[j + 2];
+                o.w = p.alpha * sum[j + 3];
                 if (cin) {
-                    const float4 ci = *reinterpret_cast<const float4 *>(cin + c0 + j);
+                    const float4 ci = *reinterpret_cast<const float4 *>(cin + j);
                     o.x = fmaf(p.beta, ci.x, o.x);
                     o.y = fmaf(p.beta, ci.y, o.y);
                     o.z = fmaf(p.beta, ci.z, o.z);
                     o.w = fmaf(p.beta, ci.w, o.w);
                 }
-                *reinterpret_cast<float4 *>(crow + c0 + j) = o;
+                *reinterpret_cast<float4 *>(crow + j) = o;
                 rs += (double)o.x + (double)o.y + (double)o.z + (double)o.w;
             }
+            if (p.rowsum) p.rowsum[(long long)(col0 / CPT) * p.M + row] = rs;
         }
-        if (p.rowsum) p.rowsum[(long long)blockIdx.x * p.M + row] = rs;
+        if (!ok) atomicExch(&g_tc_error, 3);
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS)
+                     : "memory");
     }
 }
 
@@ -334,9 +410,11 @@ int tc_gemm_tile_n(int N) {
     return 0;
 }
 
+// Row-sum partials: one per 128-column group (64 for the 64-wide tile).
 int tc_gemm_nparts(int N) {
     int bn = tc_gemm_tile_n(N);
-    return bn ? N / bn : 0;
+    if (!bn) return 0;
+    return N / (bn < 128 ? bn : 128);
 }
 
 int tc_gemm_check(const TcGemmArgs &a) {
@@ -369,8 +447,9 @@ static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
     if ((r = make_map(&mBh, a.Bhi, a.N, a.K, a.ldb, BN)) != OPB_OK) return r;
     if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN)) != OPB_OK) return r;
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
-    dim3 grid(a.N / BN, a.M / TC_BM);
-    k_tc_gemm<BN, STAGES><<<grid, 128, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl, p);
+    const int ntiles = (a.M / TC_BM) * (a.N / BN);
+    const int grid = ntiles < num_sms() ? ntiles : num_sms();
+    k_tc_gemm<BN, STAGES><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl, p);
     return (int)cudaGetLastError();
 }
 

@@ -141,12 +141,11 @@ int solve_fp32(const opb_lattice_desc &L, int mode, Bufs &b, double *quotes, dou
 // Issue every tensor-core product as S K-slices accumulated through the FP32 epilogue
 // (C = slice + 1*C, round-to-nearest), which shortens each in-TMEM accumulation chain:
 // the tensor cores truncate the FP32 accumulator, a bias of about half an ulp per MMA.
-// 0 = automatic: 2 slices for K > 2048 (keeps the truncated in-TMEM FP32 accumulation
-// chain at <= 96 MMA instructions per 16-wide step group), else 1.
+// 0 = automatic (one launch: the GEMM kernel already sums K in chunks of 2 K-blocks).
 int g_ksplit = 0;
 
 int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s) {
-    int S = g_ksplit > 0 ? g_ksplit : (a.K > 2048 ? 2 : 1);
+    int S = g_ksplit > 0 ? g_ksplit : 1;
     int kb = a.K / 64;
     if (S <= 1 || kb < S || kb % S) return opb::launch_tc_gemm(a, s);
     const int kslice = a.K / S;
@@ -180,7 +179,8 @@ int solve_bf16x3(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_a
         g.C = b.X; g.Cin = b.X; g.alpha = 1.f; g.beta = 2.f; g.rowsum = b.part;
         LT(tc_gemm_ksplit(g, s));
         const bool last = (r + 1 == L.niter);
-        LT(opb::launch_renorm(d, b.X, b.part, np, 1, last ? nullptr : b.Ahi, b.Alo, last ? nullptr : b.Bhi, b.Blo, s));
+        LT(opb::launch_renorm(d, b.X, b.part, np, 1, last ? nullptr : b.Ahi, last ? nullptr : b.Alo,
+                              last ? nullptr : b.Bhi, last ? nullptr : b.Blo, s));
     }
     // P1 = I + E; splits of P1 (row-major: A of the first chain / pricing; transposed: B of every chain)
     LT(opb::launch_add_identity(d, b.X, s));

@@ -162,6 +162,71 @@ __global__ void k_renorm(int d, float *__restrict__ X, const double *__restrict_
     }
 }
 
+// Vectorised form of k_renorm for d % 64 == 0: 64 x 64 tiles, 256 threads, float4 loads
+// and stores of X, 8-byte stores of four BF16 parts, and the transposed parts staged
+// through shared memory so that every global access is a contiguous run per warp.
+__global__ void __launch_bounds__(256) k_renorm64(int d, float *__restrict__ X, const double *__restrict__ partial,
+                                                  int nparts, int eform, __nv_bfloat16 *__restrict__ Ahi,
+                                                  __nv_bfloat16 *__restrict__ Alo, __nv_bfloat16 *__restrict__ Bhi,
+                                                  __nv_bfloat16 *__restrict__ Blo) {
+    __shared__ double s_sum[64], s_inv[64];
+    __shared__ __nv_bfloat16 th[64][72], tl[64][72];
+    const int tid = threadIdx.x;
+    const int r0 = blockIdx.y * 64, c0 = blockIdx.x * 64;
+    if (tid < 64) {
+        double s = 0.0;
+        const int r = r0 + tid;
+        for (int p = 0; p < nparts; p++) s += partial[(long long)p * d + r];
+        s_sum[tid] = s;
+        const double den = eform ? 1.0 + s : s;
+        s_inv[tid] = den != 0.0 ? 1.0 / den : 0.0;
+    }
+    __syncthreads();
+    const int lc = (tid & 15) * 4;
+#pragma unroll
+    for (int pass = 0; pass < 4; pass++) {
+        const int lr = pass * 16 + (tid >> 4);
+        const int r = r0 + lr;
+        const long long o = (long long)r * d + c0 + lc;
+        float4 v = *reinterpret_cast<const float4 *>(X + o);
+        const double su = s_sum[lr], inv = s_inv[lr];
+        float f[4] = {v.x, v.y, v.z, v.w};
+        __nv_bfloat16 h[4], l[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            double x = (double)f[j];
+            if (eform && r == c0 + lc + j) x -= su;
+            f[j] = (float)(x * inv);
+            split2(f[j], h[j], l[j]);
+            th[lr][lc + j] = h[j];
+            tl[lr][lc + j] = l[j];
+        }
+        *reinterpret_cast<float4 *>(X + o) = make_float4(f[0], f[1], f[2], f[3]);
+        if (Ahi) {
+            *reinterpret_cast<uint2 *>(Ahi + o) = make_uint2(
+                (uint32_t)__bfloat16_as_ushort(h[0]) | ((uint32_t)__bfloat16_as_ushort(h[1]) << 16),
+                (uint32_t)__bfloat16_as_ushort(h[2]) | ((uint32_t)__bfloat16_as_ushort(h[3]) << 16));
+            *reinterpret_cast<uint2 *>(Alo + o) = make_uint2(
+                (uint32_t)__bfloat16_as_ushort(l[0]) | ((uint32_t)__bfloat16_as_ushort(l[1]) << 16),
+                (uint32_t)__bfloat16_as_ushort(l[2]) | ((uint32_t)__bfloat16_as_ushort(l[3]) << 16));
+        }
+    }
+    if (!Bhi) return;
+    __syncthreads();
+    // transposed: output row (c0 + orow) holds input rows r0 + lc .. r0 + lc + 3
+#pragma unroll
+    for (int pass = 0; pass < 4; pass++) {
+        const int orow = pass * 16 + (tid >> 4);
+        const long long o = (long long)(c0 + orow) * d + r0 + lc;
+        *reinterpret_cast<uint2 *>(Bhi + o) = make_uint2(
+            (uint32_t)__bfloat16_as_ushort(th[lc + 0][orow]) | ((uint32_t)__bfloat16_as_ushort(th[lc + 1][orow]) << 16),
+            (uint32_t)__bfloat16_as_ushort(th[lc + 2][orow]) | ((uint32_t)__bfloat16_as_ushort(th[lc + 3][orow]) << 16));
+        *reinterpret_cast<uint2 *>(Blo + o) = make_uint2(
+            (uint32_t)__bfloat16_as_ushort(tl[lc + 0][orow]) | ((uint32_t)__bfloat16_as_ushort(tl[lc + 1][orow]) << 16),
+            (uint32_t)__bfloat16_as_ushort(tl[lc + 2][orow]) | ((uint32_t)__bfloat16_as_ushort(tl[lc + 3][orow]) << 16));
+    }
+}
+
 // E-form -> P-form: P = I + E (in place), FP32.
 __global__ void k_add_identity(int d, float *__restrict__ X) {
     int y = blockIdx.x * blockDim.x + threadIdx.x;
@@ -237,6 +302,11 @@ int launch_rowsum(int d, const float *X, double *partial, cudaStream_t s) {
 
 int launch_renorm(int d, float *X, const double *partial, int nparts, int eform, __nv_bfloat16 *Ahi,
                   __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s) {
+    if (d % 64 == 0 && (Ahi != nullptr) == (Alo != nullptr)) {
+        dim3 g(d / 64, d / 64);
+        k_renorm64<<<g, 256, 0, s>>>(d, X, partial, nparts, eform, Ahi, Alo, Bhi, Blo);
+        return (int)cudaGetLastError();
+    }
     dim3 g((d + 31) / 32, (d + 31) / 32);
     k_renorm<<<g, 256, 0, s>>>(d, X, partial, nparts, eform, Ahi, Alo, Bhi, Blo);
     return (int)cudaGetLastError();
