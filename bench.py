@@ -311,6 +311,159 @@ def cpu_baseline(samples: int = 2):
                       "products per solve extrapolated"}
 
 
+# ----------------------------------------------------------------------------------------
+# Secondary workloads (not the headline line): config 0 (LV lattice), config 2 (Monte
+# Carlo), and the squaring GEMM alone (the profiling case).
+
+def _graph(step, dev, torch):
+    """Capture one step (library launches only, no sync, no allocation) in a CUDA graph."""
+    from oplib_b200.model import bind_stream
+    s = torch.cuda.Stream(dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        bind_stream(dev)
+        g.capture_begin()
+        step()
+        g.capture_end()
+    torch.cuda.current_stream(dev).wait_stream(s)
+    bind_stream(dev)
+    return g
+
+
+def _time(fn, steps, stream, torch):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_lv(args):
+    """Config 0: LV lattice n = 512, dt0 = 2^-14, 12 squarings, 7 chains, 8 quarterly
+    maturities x 64 strikes = 512 quotes per solve; CUDA-graph replay of the solve."""
+    import torch
+    from oplib_b200 import _lib
+    from oplib_b200.model import MODES, Lattice, bind_stream
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    bind_stream(dev)
+    stream = torch.cuda.current_stream(dev)
+    lat = Lattice.local_vol(n=512, device=dev)
+    plan = lat.plan(0.25, 2.0 ** -14)
+    strikes = torch.tensor([0.5 + j / 63 for j in range(64)], dtype=torch.float64, device=dev)
+    out = {}
+    for mname in ["bf16x3", "fp32"]:
+        mode = MODES[mname]
+        ws = lat.workspace(64, mode)
+        q = torch.empty(8, 64, dtype=torch.float64, device=dev)
+        desc = lat.desc(plan, 0.25, 8, strikes)
+
+        def step():
+            _lib.call("opb_lattice_solve", C.byref(desc), mode, ws.data_ptr(), ws.numel(), q.data_ptr(), None)
+        for _ in range(args.warmup):
+            step()
+        g = _graph(step, dev, torch)
+        for _ in range(2):
+            g.replay()
+        ms = _time(g.replay, args.steps, stream, torch)
+        out[mname] = {"ms_per_solve": round(ms, 4), "quotes_per_s": round(512 / (ms * 1e-3), 1)}
+    line = {"metric": "priced quotes/sec, LV lattice n=512 (CUDA-graph replay)", "value": out["bf16x3"]["quotes_per_s"],
+            "unit": "quotes/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": out["bf16x3"]["ms_per_solve"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic",
+            "config": {"workload": "LV lattice 512 nodes, 12 squarings + 7 chains, 64 strikes x 8 maturities",
+                       "niter": plan.niter}, "modes": out}
+    return line
+
+
+def run_mc(args):
+    """Config 2: Monte Carlo on the LV(512) lattice, step kernel dt = 1/252 (7 squarings),
+    2^20 paths x 504 steps, one MT19937 stream per path, barrier (0.7) and Asian calls.
+    One step = step-kernel build + cumulative rows + guide table + the MC kernel."""
+    import torch
+    from oplib_b200 import _lib
+    from oplib_b200.model import Lattice, bind_stream, cumulative_rows, guide_table, mc_run
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    bind_stream(dev)
+    stream = torch.cuda.current_stream(dev)
+    lat = Lattice.local_vol(n=512, device=dev)
+    plan = lat.plan(1 / 252, 2.0 ** -14)
+    npaths, nsteps = 1 << 20, 504
+    disc = math.exp(-0.03 * nsteps / 252)
+    nblk = _lib.load().opb_mc_scratch_blocks(npaths)
+    scratch = torch.empty(2 * nblk, dtype=torch.float64, device=dev)
+    state = {}
+
+    def step(with_kernel=True):
+        if with_kernel:
+            P = lat.kernel(1 / 252, 2.0 ** -14, mode="fp32", plan=plan)
+            Cm = cumulative_rows(P)
+            state["C"], state["g"] = Cm, guide_table(Cm, 64)
+        sums, _ = mc_run(state["C"], lat.y0, nsteps, 5489, npaths, guide=state["g"], x=lat.x, disc=disc,
+                         scratch=scratch)
+        state["sums"] = sums
+
+    for _ in range(args.warmup):
+        step()
+    ms = _time(step, args.steps, stream, torch)
+    ms_mc = _time(lambda: step(False), args.steps, stream, torch)
+    sums = state["sums"].cpu().numpy() / npaths
+    samples = npaths * nsteps
+    line = {"metric": "Monte Carlo path-steps/sec (MT19937 per path, inverse-CDF on FP32 cumulative rows)",
+            "value": round(samples / (ms * 1e-3), 1), "unit": "path-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 RNG + f32 compare", "data": "synthetic",
+            "config": {"workload": "LV(512) lattice, dt=1/252 step kernel, 2^20 paths x 504 steps, barrier 0.7 + "
+                                   "Asian, K=1", "paths": npaths, "steps_per_path": nsteps},
+            "mc_kernel_only": {"ms": round(ms_mc, 3), "path_steps_per_s": round(samples / (ms_mc * 1e-3), 1)},
+            "prices": {"barrier_do_call": float(sums[0]), "asian_call": float(sums[1])}}
+    if args.cpu:
+        from oracle import oracle_c as OC
+        nth = os.cpu_count() or 1
+        Cm = state["C"].cpu().numpy()
+        xs = lat.x.cpu().numpy()
+        n_cpu = 1 << 15
+        t0 = time.perf_counter()
+        OC.mc_paths(Cm, lat.y0, 5489, 0, n_cpu, nsteps, x=xs, disc=disc, want_paths=False, nthreads=nth)
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(n_cpu * nsteps / tc, 1), "unit": "path-steps/s", "cores": nth,
+                                "kind": "port", "sample": f"{n_cpu} paths x {nsteps} steps, C oracle, {nth} threads"}
+    return line
+
+
+def run_gemm(args):
+    """The squaring GEMM alone (split-BF16, E-form: C = E.E + 2E in place) at size d."""
+    import torch
+    from oplib_b200 import _lib
+    from oplib_b200.model import bind_stream
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    bind_stream(dev)
+    lib = _lib.load()
+    d = args.d
+    Ah = torch.empty(d, d, dtype=torch.bfloat16, device=dev).normal_(0, 1e-3)
+    Al = torch.empty_like(Ah).normal_(0, 1e-6)
+    X = torch.empty(d, d, dtype=torch.float32, device=dev).normal_()
+    rs = torch.empty(lib.opb_gemm_bf16x3_nparts(d) * d, dtype=torch.float64, device=dev)
+    a = (d, d, d, Ah.data_ptr(), Al.data_ptr(), d, Ah.data_ptr(), Al.data_ptr(), d, 1.0, X.data_ptr(), 2.0,
+         X.data_ptr(), d, rs.data_ptr())
+    for _ in range(args.warmup):
+        _lib.call("opb_gemm_bf16x3", *a)
+    ms = _time(lambda: _lib.call("opb_gemm_bf16x3", *a), args.steps, torch.cuda.current_stream(dev), torch)
+    _, peak, _, src = _peaks()
+    tf = 3 * 2.0 * d ** 3 / (ms * 1e-3) / 1e12
+    return {"metric": "split-BF16 GEMM MMA TFLOP/s", "value": round(tf, 1), "unit": "TFLOP/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic",
+            "config": {"workload": f"E-form squaring GEMM d={d}"}, "frac_of_peak": round(tf / peak, 4),
+            "peak_source": src}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -320,7 +473,14 @@ def main():
     ap.add_argument("--mode", default="bf16x3", choices=["bf16x3", "fp32", "fp32_plain"])
     ap.add_argument("--no-compare", dest="compare", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu", action="store_false")
+    ap.add_argument("--workload", default="sv", choices=["sv", "lv", "mc", "gemm"],
+                    help="sv = the headline SV lattice solve; the others are secondary measurements")
+    ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
     args = ap.parse_args()
+    if args.workload != "sv" and args.impl == "b200":
+        fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm}[args.workload]
+        print(json.dumps(fn(args)))
+        return 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
