@@ -436,6 +436,55 @@ def run_mc(args):
     return line
 
 
+def run_batch(args):
+    """Config 3: calibration sweep of 512 seeded local-vol lattices, n uniform over
+    {256, 384, ..., 2048}, 32 strikes x 8 quarterly maturities each (131,072 quotes);
+    all lattices' squarings of a level in one persistent launch, the whole sweep replayed
+    from a CUDA graph; autotuned tile shape / work order."""
+    import torch
+    from oplib_b200 import _lib
+    from oplib_b200.model import Batch, bind_stream, calibration_sweep
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    bind_stream(dev)
+    stream = torch.cuda.current_stream(dev)
+    nlat = args.nlat
+    lats, params = calibration_sweep(nlat=nlat, device=dev)
+    strikes = [0.5 + j / 31.0 for j in range(32)]
+    t0 = time.perf_counter()
+    b = Batch(lats, strikes, 8, 0.25, 2.0 ** -14, mode="bf16x3", autotune=True)
+    torch.cuda.synchronize()
+    t_plan = time.perf_counter() - t0
+    q = torch.empty(nlat, 8, 32, dtype=torch.float64, device=dev)
+    for _ in range(args.warmup):
+        b.execute(q)
+    g = _graph(lambda: b.execute(q), dev, torch)
+    g.replay()
+    ms = _time(g.replay, args.steps, stream, torch)
+    nquotes = nlat * 8 * 32
+    useful = sum(2.0 * p["n"] ** 3 * (pl.niter + 7) for p, pl in zip(params, b.plans))
+    line = {"metric": "priced quotes/sec, batched calibration sweep (split-BF16, one launch per level)",
+            "value": round(nquotes / (ms * 1e-3), 1), "unit": "quotes/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic",
+            "config": {"workload": f"{nlat} LV lattices, n in 256..2048 step 128 (seed 20260), 32 strikes x 8 "
+                                   "maturities, CUDA-graph replay", "nlat": nlat,
+                       "niter_range": [min(p.niter for p in b.plans), max(p.niter for p in b.plans)]},
+            "useful_tflops": round(useful / (ms * 1e-3) / 1e12, 1),
+            "mma_tflops": round(3 * useful / (ms * 1e-3) / 1e12, 1),
+            "autotune_ms_level0": [round(x, 3) for x in b.tune_ms], "config_chosen": b.config,
+            "launches_per_sweep": b.launches(), "plan_seconds": round(t_plan, 2)}
+    if args.compare:
+        b32 = Batch(lats, strikes, 8, 0.25, 2.0 ** -14, mode="fp32", autotune=False)
+        q32 = b32.execute()
+        torch.cuda.synchronize()
+        ms32 = _time(lambda: b32.execute(q32), 1, stream, torch)
+        line["fp32_quotes_per_s"] = round(nquotes / (ms32 * 1e-3), 1)
+        line["speedup_vs_fp32"] = round(ms32 / ms, 2)
+        line["max_abs_diff_bf16x3_vs_fp32"] = float((q - q32).abs().max().item())
+    return line
+
+
 def run_gemm(args):
     """The squaring GEMM alone (split-BF16, E-form: C = E.E + 2E in place) at size d."""
     import torch
@@ -473,12 +522,13 @@ def main():
     ap.add_argument("--mode", default="bf16x3", choices=["bf16x3", "fp32", "fp32_plain"])
     ap.add_argument("--no-compare", dest="compare", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu", action="store_false")
-    ap.add_argument("--workload", default="sv", choices=["sv", "lv", "mc", "gemm"],
+    ap.add_argument("--nlat", type=int, default=512, help="lattices for --workload batch")
+    ap.add_argument("--workload", default="sv", choices=["sv", "lv", "mc", "gemm", "batch"],
                     help="sv = the headline SV lattice solve; the others are secondary measurements")
     ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
     args = ap.parse_args()
     if args.workload != "sv" and args.impl == "b200":
-        fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm}[args.workload]
+        fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "batch": run_batch}[args.workload]
         print(json.dumps(fn(args)))
         return 0
 

@@ -197,6 +197,39 @@ int opb_lattice_kernel(const opb_lattice_desc *L, int mode, void *workspace, uns
  * epilogue (shorter in-TMEM accumulation chains); 0 (default) = automatic */
 int opb_set_ksplit(int s);
 
+/* ------------------------------------------------------------------ batched lattices */
+typedef struct opb_batch_desc {
+    int nlat;
+    const int *d;            /* host [nlat], multiples of 128 for OPB_BF16X3, <= 8064 */
+    const int *y0;           /* host [nlat] */
+    const int *niter;        /* host [nlat], >= 1 */
+    const double *dt;        /* host [nlat] */
+    const double *rate;      /* host [nlat] */
+    int ell_width;
+    const int *gen_cols;     /* device [sum(d) * ell_width], columns within the lattice */
+    const double *gen_vals;  /* device [sum(d) * ell_width] */
+    const double *x;         /* device [sum(d)] */
+    int nmat;
+    double period;
+    int nK;                  /* <= 64 */
+    const double *strikes;   /* device [nlat * nK] */
+} opb_batch_desc;
+typedef struct opb_batch_plan opb_batch_plan;
+/* new: many uneven lattices in one persistent tcgen05 launch per squaring level (the
+ * reference batches squarings per level through pointer tables, oplib/opmodel/models/
+ * CModel Common.cs:508-545, and ragged GEMMs through task tables, oplib/opcuda/sgemm4.cu:
+ * 84-154).  plan_create uploads tables into the workspace (blocking); execute issues all
+ * launches asynchronously with no allocation (capturable); quotes [nlat][nmat][nK] FP64. */
+unsigned long long opb_batch_workspace_size(const opb_batch_desc *b, int mode);
+int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *workspace, unsigned long long ws_bytes,
+                          opb_batch_plan **out);
+int opb_batch_plan_destroy(opb_batch_plan *plan);
+int opb_batch_set_config(opb_batch_plan *plan, int cfg, int grid);
+int opb_batch_execute(opb_batch_plan *plan, double *quotes);
+/* times the level-0 launch for the 4 tile/order configurations and keeps the fastest */
+int opb_batch_autotune(opb_batch_plan *plan, int reps, float *ms_out, int *best_cfg);
+int opb_batch_launches(const opb_batch_plan *plan);
+
 /* ------------------------------------------------------------------ cumulative rows, MC */
 /* replaces oplib/opcuda/sck.cu:88-93: nm column-major kernels -> cumulative normalised rows */
 int opcuda_sck(int d, int nm, uint64_t tpker_yy_m, uint64_t ctpker_yy_m);

@@ -95,6 +95,14 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_lattice_solve": (i32, [C.POINTER(LatticeDesc), i32, vp, ull, vp, vp]),
     "opb_lattice_kernel": (i32, [C.POINTER(LatticeDesc), i32, vp, ull, vp]),
     "opb_set_ksplit": (i32, [i32]),
+    # batched lattices
+    "opb_batch_workspace_size": (ull, [vp, i32]),
+    "opb_batch_plan_create": (i32, [vp, i32, vp, ull, vp]),
+    "opb_batch_plan_destroy": (i32, [vp]),
+    "opb_batch_set_config": (i32, [vp, i32, i32]),
+    "opb_batch_execute": (i32, [vp, vp]),
+    "opb_batch_autotune": (i32, [vp, i32, vp, vp]),
+    "opb_batch_launches": (i32, [vp]),
     # cumulative rows / MC
     "opcuda_sck": (i32, [i32, i32, u64, u64]),
     "opb_sck_rm": (i32, [i32, i32, vp, vp]),

@@ -1,0 +1,469 @@
+// Batched solve of many uneven lattices (the calibration-sweep workload).
+//
+// Precedent: the reference's grouped GEMM runs many matrices of different sizes in one
+// launch through a per-block task table (oplib/opcuda/sgemm4.cu:84-154), and its planner
+// batches every interval that still needs squaring at level r into one call
+// (oplib/opmodel/models/CModel Common.cs:508-545, CModel Device.cs:216-228).  Here every
+// squaring level of all lattices is ONE persistent tcgen05 launch over a work list of
+// (lattice, m-tile, n-tile) items, followed by ONE batched FP64 renormalisation launch;
+// chaining and pricing are batched the same way.  The plan (tables, tensor maps, work
+// lists) is built once on the host and uploaded into the caller's workspace; execute()
+// then issues ~4 launches per level with no host synchronisation and no allocation, so a
+// whole sweep can be captured in a CUDA graph and replayed.
+//
+// Tile shape and work order are chosen by opb_batch_autotune, which times the level-0
+// launch for each candidate (BN 128 or 64; items ordered longest-K first or by lattice)
+// with CUDA events and keeps the fastest.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "common.cuh"
+#include "lattice.h"
+
+enum { OPB_FP32_PLAIN_B = 0, OPB_FP32_RENORM_B = 1, OPB_BF16X3_B = 2 };
+
+struct opb_lattice_desc;  // lattice.cu
+extern "C" int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
+                                 double *quotes, double *V_all);
+extern "C" unsigned long long opb_lattice_workspace_size(int d, int nK, int mode);
+
+struct opb_batch_desc {
+    int nlat;
+    const int *d;            // host [nlat], multiples of 128
+    const int *y0;           // host [nlat]
+    const int *niter;        // host [nlat], >= 1
+    const double *dt;        // host [nlat]
+    const double *rate;      // host [nlat]
+    int ell_width;
+    const int *gen_cols;     // device [sum(d) * ell_width], columns within the lattice
+    const double *gen_vals;  // device [sum(d) * ell_width]
+    const double *x;         // device [sum(d)]
+    int nmat;
+    double period;
+    int nK;
+    const double *strikes;   // device [nlat * nK]
+};
+
+namespace {
+
+constexpr int NCFG = 4;  // (bn, order): (128, LPT), (64, LPT), (128, lattice), (64, lattice)
+constexpr int CFG_BN[NCFG] = {128, 64, 128, 64};
+
+// mirror of opb_lattice_desc (lattice.cu), used for the FP32 per-lattice path
+struct LatticeDescMirror {
+    int d, y0, ell_width;
+    const int *gen_cols;
+    const double *gen_vals;
+    const double *gen_dense;
+    const double *x;
+    double dt;
+    int niter, nmat;
+    double period, rate;
+    int nK;
+    const double *strikes;
+};
+
+struct ListRef {
+    size_t off;  // element offset in the work blob
+    int n;
+};
+
+}  // namespace
+
+struct opb_batch_plan {
+    int mode = 0, nlat = 0, nmat = 0, nK = 0, ldk = 64, maxn = 0, cfg = 0, grid = 0;
+    long long total_rows = 0;
+    int ell_width = 0;
+    const int *cols = nullptr;
+    const double *vals = nullptr, *x = nullptr, *strikes = nullptr;
+    double period = 0.0;
+    // device tables
+    opb::BatchLattice *lats = nullptr;
+    opb::TcProblem *sq = nullptr, *chain = nullptr, *price = nullptr;
+    opb::RenormProblem *rn_sq = nullptr, *rn_chain = nullptr;
+    CUtensorMap *maps_sq[2] = {nullptr, nullptr};  // per bn (128, 64)
+    CUtensorMap *maps_price = nullptr;
+    uint32_t *work = nullptr;
+    float *E_base = nullptr;
+    size_t E_bytes = 0;
+    // work lists (offsets into `work`)
+    std::vector<ListRef> gemm_level[NCFG];
+    ListRef gemm_chain[NCFG];
+    ListRef gemm_price;
+    std::vector<ListRef> rn_level;
+    ListRef rn_init, rn_chain_list;
+    // FP32 path
+    std::vector<LatticeDescMirror> fp32_desc;
+    std::vector<char *> fp32_ws;
+    size_t fp32_ws_bytes = 0;
+};
+
+namespace {
+
+struct Carve {
+    char *base;
+    size_t used;
+    template <class T>
+    T *take(size_t n) {
+        size_t off = (used + 255) & ~size_t(255);
+        used = off + n * sizeof(T);
+        return base ? reinterpret_cast<T *>(base + off) : nullptr;
+    }
+};
+
+int check_batch(const opb_batch_desc *b, int mode) {
+    if (!b) return OPB_E_NULL;
+    if (b->nlat < 1 || b->nlat > 65535 || b->nmat < 1 || b->nK < 1 || b->nK > 64) return OPB_E_ARG;
+    if (!b->d || !b->y0 || !b->niter || !b->dt || !b->rate) return OPB_E_NULL;
+    if (!b->gen_cols || !b->gen_vals || !b->x || !b->strikes) return OPB_E_NULL;
+    if (b->ell_width < 1 || !(b->period > 0.0)) return OPB_E_ARG;
+    if (mode < 0 || mode > 2) return OPB_E_ARG;
+    for (int i = 0; i < b->nlat; i++) {
+        int d = b->d[i];
+        if (d < 128 || d > 8064 || b->y0[i] < 0 || b->y0[i] >= d || b->niter[i] < 1 || !(b->dt[i] > 0.0))
+            return OPB_E_ARG;
+        if (mode == OPB_BF16X3_B && d % 128) return OPB_E_UNSUPPORTED;
+    }
+    return OPB_OK;
+}
+
+// Layout of all device buffers and tables; with base == nullptr it only measures.
+size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, std::vector<uint32_t> *work_out) {
+    Carve c{base, 0};
+    const int n = b->nlat;
+    std::vector<long long> off(n + 1, 0);
+    for (int i = 0; i < n; i++) off[i + 1] = off[i] + b->d[i];
+    if (mode != OPB_BF16X3_B) {
+        size_t per_max = 0;
+        std::vector<size_t> sz(n);
+        for (int i = 0; i < n; i++) {
+            sz[i] = opb_lattice_workspace_size(b->d[i], b->nK, mode);
+            per_max = std::max(per_max, sz[i]);
+        }
+        // lattices are solved one after another on one stream, so one workspace suffices
+        char *ws = c.take<char>(per_max);
+        if (P) {
+            P->fp32_ws.assign(1, ws);
+            P->fp32_ws_bytes = per_max;
+        }
+        return c.used + 256;
+    }
+    const int ldk = 64;
+    auto lats = c.take<opb::BatchLattice>(n);
+    auto sq = c.take<opb::TcProblem>(n);
+    auto ch = c.take<opb::TcProblem>(n);
+    auto pr = c.take<opb::TcProblem>(n);
+    auto rs = c.take<opb::RenormProblem>(n);
+    auto rc = c.take<opb::RenormProblem>(n);
+    auto m128 = c.take<CUtensorMap>(4 * (size_t)n);
+    auto m64 = c.take<CUtensorMap>(4 * (size_t)n);
+    auto mp = c.take<CUtensorMap>(4 * (size_t)n);
+    size_t Etot = 0;
+    for (int i = 0; i < n; i++) Etot += (size_t)b->d[i] * b->d[i];
+    float *E = c.take<float>(Etot);
+    float *Pa = c.take<float>(Etot);
+    __nv_bfloat16 *Ah = c.take<__nv_bfloat16>(Etot), *Al = c.take<__nv_bfloat16>(Etot);
+    __nv_bfloat16 *Bh = c.take<__nv_bfloat16>(Etot), *Bl = c.take<__nv_bfloat16>(Etot);
+    float *V = c.take<float>((size_t)off[n] * ldk);
+    __nv_bfloat16 *Gh = c.take<__nv_bfloat16>((size_t)off[n] * ldk), *Gl = c.take<__nv_bfloat16>((size_t)off[n] * ldk);
+    size_t parts = 0;
+    for (int i = 0; i < n; i++) parts += (size_t)(b->d[i] / 64) * b->d[i];
+    double *part = c.take<double>(parts);
+
+    // ---- work lists (host), appended into one blob
+    std::vector<uint32_t> W;
+    std::vector<int> lpt(n), nat(n);
+    std::iota(nat.begin(), nat.end(), 0);
+    lpt = nat;
+    std::stable_sort(lpt.begin(), lpt.end(), [&](int a, int bb) { return b->d[a] > b->d[bb]; });
+    int maxn = 0;
+    for (int i = 0; i < n; i++) maxn = std::max(maxn, b->niter[i]);
+    auto gemm_list = [&](const std::vector<int> &order, int bn, int level, bool chain_or_all) {
+        ListRef r{W.size(), 0};
+        for (int i : order) {
+            if (!chain_or_all && b->niter[i] <= level) continue;
+            const int mt = b->d[i] / 128, nt = b->d[i] / bn;
+            for (int a = 0; a < mt; a++)
+                for (int bb = 0; bb < nt; bb++) W.push_back(((uint32_t)i << 16) | ((uint32_t)a << 8) | (uint32_t)bb);
+        }
+        r.n = (int)(W.size() - r.off);
+        return r;
+    };
+    std::vector<ListRef> gl[NCFG];
+    ListRef gch[NCFG];
+    for (int cfg = 0; cfg < NCFG; cfg++) {
+        const auto &order = cfg < 2 ? lpt : nat;
+        for (int lv = 0; lv < maxn; lv++) gl[cfg].push_back(gemm_list(order, CFG_BN[cfg], lv, false));
+        gch[cfg] = gemm_list(order, CFG_BN[cfg], 0, true);
+    }
+    ListRef gpr{W.size(), 0};
+    for (int i : lpt)
+        for (int a = 0; a < b->d[i] / 128; a++) W.push_back(((uint32_t)i << 16) | ((uint32_t)a << 8));
+    gpr.n = (int)(W.size() - gpr.off);
+    auto rn_list = [&](int level, int kind) {  // kind: 0 init split, 1 squaring level, 2 chain
+        ListRef r{W.size(), 0};
+        for (int i : lpt) {
+            int mode_i;
+            if (kind == 0) mode_i = 0;
+            else if (kind == 2) mode_i = 2;
+            else {
+                if (b->niter[i] <= level) continue;
+                mode_i = (level == b->niter[i] - 1) ? 1 : 0;
+            }
+            const int t = b->d[i] / 64;
+            for (int a = 0; a < t; a++)
+                for (int bb = 0; bb < t; bb++)
+                    W.push_back(((uint32_t)i << 16) | ((uint32_t)mode_i << 14) | ((uint32_t)a << 7) | (uint32_t)bb);
+        }
+        r.n = (int)(W.size() - r.off);
+        return r;
+    };
+    ListRef rinit = rn_list(0, 0);
+    std::vector<ListRef> rl;
+    for (int lv = 0; lv < maxn; lv++) rl.push_back(rn_list(lv, 1));
+    ListRef rch = rn_list(0, 2);
+    uint32_t *work = c.take<uint32_t>(W.size());
+    size_t total = c.used + 256;
+    if (!P) return total;
+
+    // ---- fill the plan and host copies of the tables
+    P->nlat = n; P->nmat = b->nmat; P->nK = b->nK; P->ldk = ldk; P->maxn = maxn;
+    P->total_rows = off[n]; P->ell_width = b->ell_width; P->cols = b->gen_cols; P->vals = b->gen_vals;
+    P->x = b->x; P->strikes = b->strikes; P->period = b->period;
+    P->lats = lats; P->sq = sq; P->chain = ch; P->price = pr; P->rn_sq = rs; P->rn_chain = rc;
+    P->maps_sq[0] = m128; P->maps_sq[1] = m64; P->maps_price = mp; P->work = work;
+    P->E_base = E; P->E_bytes = Etot * sizeof(float);
+    for (int cfg = 0; cfg < NCFG; cfg++) { P->gemm_level[cfg] = gl[cfg]; P->gemm_chain[cfg] = gch[cfg]; }
+    P->gemm_price = gpr; P->rn_level = rl; P->rn_init = rinit; P->rn_chain_list = rch;
+    if (work_out) *work_out = W;
+    return total;
+}
+
+}  // namespace
+
+using opb::set_status;
+
+OPB_API unsigned long long opb_batch_workspace_size(const opb_batch_desc *b, int mode) {
+    if (check_batch(b, mode) != OPB_OK) return 0;
+    return (unsigned long long)layout(b, mode, nullptr, nullptr, nullptr);
+}
+
+// Builds the plan: tables, tensor maps and work lists are written into `workspace`
+// (blocking copies; call once, before any capture).  *out receives a host handle.
+OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *workspace, unsigned long long ws_bytes,
+                                  opb_batch_plan **out) {
+    int c = check_batch(b, mode);
+    if (c != OPB_OK) return set_status(c);
+    OPB_REQUIRE(workspace && out, OPB_E_NULL);
+    size_t need = layout(b, mode, nullptr, nullptr, nullptr);
+    OPB_REQUIRE(ws_bytes >= need, OPB_E_ARG);
+    char *base = reinterpret_cast<char *>(workspace);
+    base += (256 - (reinterpret_cast<uintptr_t>(base) & 255)) & 255;
+    opb_batch_plan *P = new opb_batch_plan();
+    P->mode = mode;
+    std::vector<uint32_t> W;
+    layout(b, mode, P, base, &W);
+    const int n = b->nlat;
+    if (mode != OPB_BF16X3_B) {
+        P->nlat = n; P->nmat = b->nmat; P->nK = b->nK;
+        long long roff = 0;
+        for (int i = 0; i < n; i++) {
+            LatticeDescMirror L{};
+            L.d = b->d[i]; L.y0 = b->y0[i]; L.ell_width = b->ell_width;
+            L.gen_cols = b->gen_cols + roff * b->ell_width; L.gen_vals = b->gen_vals + roff * b->ell_width;
+            L.x = b->x + roff; L.dt = b->dt[i]; L.niter = b->niter[i]; L.nmat = b->nmat; L.period = b->period;
+            L.rate = b->rate[i]; L.nK = b->nK; L.strikes = b->strikes + (size_t)i * b->nK;
+            P->fp32_desc.push_back(L);
+            roff += b->d[i];
+        }
+        *out = P;
+        return set_status(OPB_OK);
+    }
+    // host images of the device tables
+    std::vector<opb::BatchLattice> lats(n);
+    std::vector<opb::TcProblem> sq(n), ch(n), pr(n);
+    std::vector<opb::RenormProblem> rs(n), rc(n);
+    std::vector<CUtensorMap> m128(4 * (size_t)n), m64(4 * (size_t)n), mp(4 * (size_t)n);
+    // recompute buffer pointers exactly as layout() carved them
+    Carve cv{base, 0};
+    cv.take<opb::BatchLattice>(n); cv.take<opb::TcProblem>(n); cv.take<opb::TcProblem>(n); cv.take<opb::TcProblem>(n);
+    cv.take<opb::RenormProblem>(n); cv.take<opb::RenormProblem>(n);
+    cv.take<CUtensorMap>(4 * (size_t)n); cv.take<CUtensorMap>(4 * (size_t)n); cv.take<CUtensorMap>(4 * (size_t)n);
+    size_t Etot = 0;
+    for (int i = 0; i < n; i++) Etot += (size_t)b->d[i] * b->d[i];
+    float *E = cv.take<float>(Etot), *Pa = cv.take<float>(Etot);
+    __nv_bfloat16 *Ah = cv.take<__nv_bfloat16>(Etot), *Al = cv.take<__nv_bfloat16>(Etot);
+    __nv_bfloat16 *Bh = cv.take<__nv_bfloat16>(Etot), *Bl = cv.take<__nv_bfloat16>(Etot);
+    float *V = cv.take<float>((size_t)P->total_rows * P->ldk);
+    __nv_bfloat16 *Gh = cv.take<__nv_bfloat16>((size_t)P->total_rows * P->ldk);
+    __nv_bfloat16 *Gl = cv.take<__nv_bfloat16>((size_t)P->total_rows * P->ldk);
+    size_t parts = 0;
+    for (int i = 0; i < n; i++) parts += (size_t)(b->d[i] / 64) * b->d[i];
+    double *part = cv.take<double>(parts);
+    size_t eo = 0, po = 0;
+    long long ro = 0;
+    int rc_status = OPB_OK;
+    for (int i = 0; i < n && rc_status == OPB_OK; i++) {
+        const int d = b->d[i];
+        opb::BatchLattice &L = lats[i];
+        L.d = d; L.y0 = b->y0[i]; L.row_off = ro; L.dt = b->dt[i]; L.rate = b->rate[i]; L.period = b->period;
+        L.E = E + eo; L.Pa = Pa + eo; L.V = V + (size_t)ro * P->ldk;
+        L.GThi = Gh + (size_t)ro * P->ldk; L.GTlo = Gl + (size_t)ro * P->ldk;
+        double *pi = part + po;
+        sq[i] = opb::TcProblem{d, d, d, 0, L.E, L.E, pi, d, 1.f, 2.f, 0};
+        ch[i] = opb::TcProblem{d, d, d, 0, L.Pa, nullptr, pi, d, 1.f, 0.f, 0};
+        pr[i] = opb::TcProblem{d, P->ldk, d, 0, L.V, nullptr, nullptr, P->ldk, 1.f, 0.f, 0};
+        rs[i] = opb::RenormProblem{d, 0, L.E, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo};
+        rc[i] = opb::RenormProblem{d, 0, L.Pa, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo};
+        rc_status = opb::tc_make_maps(&m128[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 128);
+        if (rc_status == OPB_OK)
+            rc_status = opb::tc_make_maps(&m64[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 64);
+        if (rc_status == OPB_OK)
+            rc_status = opb::tc_make_maps(&mp[4 * (size_t)i], Ah + eo, Al + eo, d, d, L.GThi, L.GTlo, P->ldk, d, d, 64);
+        eo += (size_t)d * d;
+        po += (size_t)(d / 64) * d;
+        ro += d;
+    }
+    if (rc_status != OPB_OK) {
+        delete P;
+        return set_status(rc_status);
+    }
+    auto up = [&](void *dst, const void *src, size_t bytes) -> cudaError_t {
+        return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    };
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = up(P->lats, lats.data(), sizeof(opb::BatchLattice) * n);
+    if (e == cudaSuccess) e = up(P->sq, sq.data(), sizeof(opb::TcProblem) * n);
+    if (e == cudaSuccess) e = up(P->chain, ch.data(), sizeof(opb::TcProblem) * n);
+    if (e == cudaSuccess) e = up(P->price, pr.data(), sizeof(opb::TcProblem) * n);
+    if (e == cudaSuccess) e = up(P->rn_sq, rs.data(), sizeof(opb::RenormProblem) * n);
+    if (e == cudaSuccess) e = up(P->rn_chain, rc.data(), sizeof(opb::RenormProblem) * n);
+    if (e == cudaSuccess) e = up(P->maps_sq[0], m128.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
+    if (e == cudaSuccess) e = up(P->maps_sq[1], m64.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
+    if (e == cudaSuccess) e = up(P->maps_price, mp.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
+    if (e == cudaSuccess) e = up(P->work, W.data(), sizeof(uint32_t) * W.size());
+    if (e != cudaSuccess) {
+        delete P;
+        return opb::set_cuda(e);
+    }
+    P->cfg = 0;
+    P->grid = 0;
+    *out = P;
+    return set_status(OPB_OK);
+}
+
+OPB_API int opb_batch_plan_destroy(opb_batch_plan *P) {
+    delete P;
+    return set_status(OPB_OK);
+}
+
+// Selects the launch configuration: cfg 0..3 = (BN 128, longest-K first), (64, longest
+// first), (128, lattice order), (64, lattice order); grid 0 = one CTA per SM.
+OPB_API int opb_batch_set_config(opb_batch_plan *P, int cfg, int grid) {
+    OPB_REQUIRE(P, OPB_E_NULL);
+    OPB_REQUIRE(cfg >= 0 && cfg < NCFG && grid >= 0, OPB_E_ARG);
+    P->cfg = cfg;
+    P->grid = grid;
+    return set_status(OPB_OK);
+}
+
+namespace {
+
+int level_gemm(opb_batch_plan *P, int cfg, int level, cudaStream_t s) {
+    const ListRef &l = P->gemm_level[cfg][level];
+    const int bi = CFG_BN[cfg] == 128 ? 0 : 1;
+    return opb::launch_tc_gemm_batched(CFG_BN[cfg], P->maps_sq[bi], P->sq, P->work + l.off, l.n, P->grid, s);
+}
+
+}  // namespace
+
+// Executes the plan on the library stream: E0 build, every squaring level (one GEMM +
+// one renormalisation launch each), chaining and pricing.  quotes: device
+// [nlat][nmat][nK] FP64.  No host synchronisation, no allocation (graph-capturable).
+OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
+    OPB_REQUIRE(P && quotes, OPB_E_NULL);
+    cudaStream_t s = opb::stream();
+    int r = 0;
+#define BT(expr)                                  \
+    do {                                          \
+        r = (expr);                               \
+        if (r != 0) return set_status(r);         \
+    } while (0)
+    if (P->mode != OPB_BF16X3_B) {
+        for (int i = 0; i < P->nlat; i++)
+            BT(opb_lattice_solve(reinterpret_cast<const opb_lattice_desc *>(&P->fp32_desc[i]), P->mode, P->fp32_ws[0],
+                                 P->fp32_ws_bytes, quotes + (size_t)i * P->nmat * P->nK, nullptr));
+        return set_status(OPB_OK);
+    }
+    const int cfg = P->cfg, bn = CFG_BN[cfg], pdiv = bn < 128 ? bn : 128;
+    BT((int)cudaMemsetAsync(P->E_base, 0, P->E_bytes, s));
+    BT(opb::launch_ek_batched(P->lats, P->nlat, P->total_rows, P->ell_width, P->cols, P->vals, s));
+    BT(opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_init.off, P->rn_init.n, 0, s));
+    for (int lv = 0; lv < P->maxn; lv++) {
+        BT(level_gemm(P, cfg, lv, s));
+        BT(opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_level[lv].off, P->rn_level[lv].n, pdiv, s));
+    }
+    BT(opb::launch_payoff_batched(P->lats, P->nlat, P->total_rows, P->nK, P->ldk, P->x, P->strikes, s));
+    const int bi = bn == 128 ? 0 : 1;
+    for (int m = 1; m <= P->nmat; m++) {
+        if (m > 1) {
+            const ListRef &l = P->gemm_chain[cfg];
+            BT(opb::launch_tc_gemm_batched(bn, P->maps_sq[bi], P->chain, P->work + l.off, l.n, P->grid, s));
+            BT(opb::launch_renorm_batched(P->rn_chain, P->work + P->rn_chain_list.off, P->rn_chain_list.n, pdiv, s));
+        }
+        BT(opb::launch_tc_gemm_batched(64, P->maps_price, P->price, P->work + P->gemm_price.off, P->gemm_price.n,
+                                       P->grid, s));
+        BT(opb::launch_quotes_batched(P->lats, P->nlat, P->nK, P->ldk, m, P->nmat, quotes, s));
+    }
+#undef BT
+    return set_status(OPB_OK);
+}
+
+// Times the level-0 squaring launch (all lattices active) for every configuration with
+// CUDA events and keeps the fastest; ms[cfg] (optional, 4 entries) receives the times.
+// Blocking; leaves the plan's buffers in an arbitrary state (run execute afterwards).
+OPB_API int opb_batch_autotune(opb_batch_plan *P, int reps, float *ms_out, int *best_cfg) {
+    OPB_REQUIRE(P, OPB_E_NULL);
+    if (P->mode != OPB_BF16X3_B) {
+        if (best_cfg) *best_cfg = 0;
+        return set_status(OPB_OK);
+    }
+    if (reps < 1) reps = 1;
+    cudaStream_t s = opb::stream();
+    cudaEvent_t e0, e1;
+    OPB_TRY(cudaEventCreate(&e0));
+    OPB_TRY(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bc = 0;
+    for (int cfg = 0; cfg < NCFG; cfg++) {
+        int r = level_gemm(P, cfg, 0, s);  // warm-up (also sets the smem attribute)
+        if (r) return set_status(r);
+        OPB_TRY(cudaEventRecord(e0, s));
+        for (int i = 0; i < reps; i++) {
+            r = level_gemm(P, cfg, 0, s);
+            if (r) return set_status(r);
+        }
+        OPB_TRY(cudaEventRecord(e1, s));
+        OPB_TRY(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        OPB_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        ms /= reps;
+        if (ms_out) ms_out[cfg] = ms;
+        if (ms < best) { best = ms; bc = cfg; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    P->cfg = bc;
+    if (best_cfg) *best_cfg = bc;
+    return set_status(OPB_OK);
+}
+
+// Launch counts of one execute() (library kernels and memsets), for accounting.
+OPB_API int opb_batch_launches(const opb_batch_plan *P) {
+    if (!P) return 0;
+    if (P->mode != OPB_BF16X3_B) return -1;
+    return 3 + 2 * P->maxn + 1 + 2 * P->nmat + 2 * (P->nmat - 1);
+}

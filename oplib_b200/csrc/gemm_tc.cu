@@ -30,6 +30,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include <cstring>
 #include <mutex>
 
 #include "common.cuh"
@@ -155,17 +156,28 @@ struct TcParams {
     double *rowsum;
 };
 
-// Persistent kernel: one CTA per SM walks the output tiles t = blockIdx.x + i*gridDim.x
-// (grouped raster, 8 M-tiles per group).  The K loop of a tile runs in chunks of
-// CHUNK K-blocks; chunk g accumulates in TMEM accumulator g&1 starting from zero, and the
-// epilogue warps add each finished chunk into FP32 register sums (round to nearest) while
-// the MMA warp fills the other accumulator.  The tensor cores' truncating accumulation
-// thus spans only 12*CHUNK MMA instructions, and the tile's final store overlaps the next
-// tile's MMAs.
-template <int BN, int STAGES>
+// Batched launches read per-problem tensor maps (4 per problem: Ahi, Alo, Bhi, Blo) and
+// parameters from device tables and walk a work list of packed items
+// (problem << 16 | m-tile << 8 | n-tile).
+struct TcBatch {
+    const CUtensorMap *maps;
+    const TcProblem *probs;
+    const uint32_t *work;
+    int nwork;
+};
+
+// Persistent kernel: one CTA per SM walks the work items t = blockIdx.x + i*gridDim.x
+// (single problem: its tiles in grouped raster, 8 M-tiles per group; batched: the work
+// list).  The K loop of an item runs in chunks of CHUNK K-blocks; chunk g accumulates in
+// TMEM accumulator g&1 starting from zero, and the epilogue warps add each finished chunk
+// into FP32 register sums (round to nearest) while the MMA warp fills the other
+// accumulator.  The tensor cores' truncating accumulation thus spans only 12*CHUNK MMA
+// instructions, and an item's final store overlaps the next item's MMAs.
+template <int BN, int STAGES, bool BATCHED>
 __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
-              const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p) {
+              const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p,
+              TcBatch bt) {
     using Cfg = TcCfg<BN, STAGES>;
     constexpr int EPI = Cfg::EPI_WARPS;
     constexpr int CPT = Cfg::CPT;
@@ -184,18 +196,28 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
     volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * STAGES + 6);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nk = p.K / TC_BK;
-    const int nchunks = (nk + Cfg::CHUNK - 1) / Cfg::CHUNK;
-    const int mtiles = p.M / TC_BM, ntiles_n = p.N / BN, ntiles = mtiles * ntiles_n;
-    auto tile_coords = [&](int t, int &m0, int &n0) {
-        const int GM = 8;
-        const int per_group = GM * ntiles_n;
-        const int group = t / per_group;
-        const int first_m = group * GM;
-        const int gm = min(mtiles - first_m, GM);
-        const int r = t - group * per_group;
-        m0 = (first_m + r % gm) * TC_BM;
-        n0 = (r / gm) * BN;
+    const int mtiles = p.M / TC_BM, ntiles_n = p.N / BN;
+    const int nitems = BATCHED ? bt.nwork : mtiles * ntiles_n;
+    // item t -> (problem, m0, n0, K-blocks)
+    auto get_item = [&](int t, int &prob, int &m0, int &n0, int &nkb) {
+        if constexpr (BATCHED) {
+            const uint32_t w = bt.work[t];
+            prob = (int)(w >> 16);
+            m0 = (int)((w >> 8) & 255u) * TC_BM;
+            n0 = (int)(w & 255u) * BN;
+            nkb = bt.probs[prob].K / TC_BK;
+        } else {
+            const int GM = 8;
+            const int per_group = GM * ntiles_n;
+            const int group = t / per_group;
+            const int first_m = group * GM;
+            const int gm = min(mtiles - first_m, GM);
+            const int r = t - group * per_group;
+            prob = 0;
+            m0 = (first_m + r % gm) * TC_BM;
+            n0 = (r / gm) * BN;
+            nkb = p.K / TC_BK;
+        }
     };
 
     if (threadIdx.x == 0) {
@@ -229,10 +251,14 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
             // ---------------- TMA producer
             long kbg = 0;  // K-blocks issued over the CTA's lifetime (stage ring position)
             bool ok = true;
-            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                int m0, n0;
-                tile_coords(t, m0, n0);
-                for (int kb = 0; kb < nk; kb++, kbg++) {
+            for (int t = blockIdx.x; t < nitems && ok; t += gridDim.x) {
+                int prob, m0, n0, nkb;
+                get_item(t, prob, m0, n0, nkb);
+                const CUtensorMap *mp[4] = {&mAhi, &mAlo, &mBhi, &mBlo};
+                if constexpr (BATCHED) {
+                    for (int i = 0; i < 4; i++) mp[i] = bt.maps + 4 * prob + i;
+                }
+                for (int kb = 0; kb < nkb; kb++, kbg++) {
                     const int s = (int)(kbg % STAGES);
                     if (kbg >= STAGES &&
                         !mbar_wait(empty_bar(s), (uint32_t)(((kbg / STAGES) + 1) & 1), abort_flag, TC_WAIT_NS)) {
@@ -242,10 +268,10 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
                     const uint32_t st = base + s * Cfg::STAGE_BYTES;
                     mbar_expect_tx(full_bar(s), Cfg::STAGE_BYTES);
                     const int kx = kb * TC_BK;
-                    tma_load_2d(st, &mAhi, full_bar(s), kx, m0);
-                    tma_load_2d(st + Cfg::A_BYTES, &mAlo, full_bar(s), kx, m0);
-                    tma_load_2d(st + 2 * Cfg::A_BYTES, &mBhi, full_bar(s), kx, n0);
-                    tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, &mBlo, full_bar(s), kx, n0);
+                    tma_load_2d(st, mp[0], full_bar(s), kx, m0);
+                    tma_load_2d(st + Cfg::A_BYTES, mp[1], full_bar(s), kx, m0);
+                    tma_load_2d(st + 2 * Cfg::A_BYTES, mp[2], full_bar(s), kx, n0);
+                    tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, mp[3], full_bar(s), kx, n0);
                 }
             }
             if (!ok) {
@@ -264,8 +290,11 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
             const uint32_t idesc = umma_idesc_bf16(BN);
             long kbg = 0, g = 0;  // K-blocks consumed, chunks issued
             bool ok = true;
-            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                for (int c = 0; c < nchunks && ok; c++, g++) {
+            for (int t = blockIdx.x; t < nitems && ok; t += gridDim.x) {
+                int prob, m0, n0, nkb;
+                get_item(t, prob, m0, n0, nkb);
+                const int nch = (nkb + Cfg::CHUNK - 1) / Cfg::CHUNK;
+                for (int c = 0; c < nch && ok; c++, g++) {
                     const int a = (int)(g & 1);
                     if (g >= 2 && !mbar_wait(acce_bar(a), (uint32_t)(((g >> 1) + 1) & 1), abort_flag, TC_WAIT_NS)) {
                         ok = false;
@@ -273,7 +302,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
                     }
                     tc_fence_after();
                     const uint32_t dacc = tmem + (uint32_t)(a * BN);
-                    const int kb_end = min(nk, (c + 1) * Cfg::CHUNK);
+                    const int kb_end = min(nkb, (c + 1) * Cfg::CHUNK);
                     for (int kb = c * Cfg::CHUNK; kb < kb_end; kb++, kbg++) {
                         const int s = (int)(kbg % STAGES);
                         if (!mbar_wait(full_bar(s), (uint32_t)((kbg / STAGES) & 1), abort_flag, TC_WAIT_NS)) {
@@ -314,12 +343,13 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
         float sum[CPT];
         long g = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-            int m0, n0;
-            tile_coords(t, m0, n0);
+        for (int t = blockIdx.x; t < nitems && ok; t += gridDim.x) {
+            int prob, m0, n0, nkb;
+            get_item(t, prob, m0, n0, nkb);
+            const int nch = (nkb + Cfg::CHUNK - 1) / Cfg::CHUNK;
 #pragma unroll
             for (int j = 0; j < CPT; j++) sum[j] = 0.f;
-            for (int c = 0; c < nchunks; c++, g++) {
+            for (int c = 0; c < nch; c++, g++) {
                 const int a = (int)(g & 1);
                 if (!mbar_wait(accf_bar(a), (uint32_t)((g >> 1) & 1), abort_flag, TC_WAIT_NS)) {
                     ok = false;
@@ -332,36 +362,47 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
                     uint32_t v[32];
                     tmem_ld32(tacc + (uint32_t)(32 * j), v);
 #pragma unroll
-                    for (int i = 0; i < 32; i++)
-                        sum[32 * j + i] = __fadd_rn(sum[32 * j + i], __uint_as_float(v[i]));
+                    for (int i = 0; i < 32; i++) sum[32 * j + i] = __fadd_rn(sum[32 * j + i], __uint_as_float(v[i]));
                 }
                 tc_fence_before();
                 asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acce_bar(a)) : "memory");
             }
             if (!ok || *abort_flag) break;
+            float *C;
+            const float *Cin;
+            long long ldc;
+            float alpha, beta;
+            double *rowsum;
+            int M;
+            if constexpr (BATCHED) {
+                const TcProblem &pr = bt.probs[prob];
+                C = pr.C; Cin = pr.Cin; ldc = pr.ldc; alpha = pr.alpha; beta = pr.beta; rowsum = pr.rowsum; M = pr.M;
+            } else {
+                C = p.C; Cin = p.Cin; ldc = p.ldc; alpha = p.alpha; beta = p.beta; rowsum = p.rowsum; M = p.M;
+            }
             const int row = m0 + q * 32 + lane;
             const int col0 = n0 + h * CPT;
-            float *crow = p.C + (long long)row * p.ldc + col0;
-            const float *cin = p.Cin ? p.Cin + (long long)row * p.ldc + col0 : nullptr;
+            float *crow = C + (long long)row * ldc + col0;
+            const float *cin = Cin ? Cin + (long long)row * ldc + col0 : nullptr;
             double rs = 0.0;
 #pragma unroll
             for (int j = 0; j < CPT; j += 4) {
                 float4 o;
-                o.x = p.alpha * sum[j + 0];
-                o.y = p.alpha * sum[j + 1];
-                o.z = p.alpha * sum[j + 2];
-                o.w = p.alpha * sum[j + 3];
+                o.x = alpha * sum[j + 0];
+                o.y = alpha * sum[j + 1];
+                o.z = alpha * sum[j + 2];
+                o.w = alpha * sum[j + 3];
                 if (cin) {
                     const float4 ci = *reinterpret_cast<const float4 *>(cin + j);
-                    o.x = fmaf(p.beta, ci.x, o.x);
-                    o.y = fmaf(p.beta, ci.y, o.y);
-                    o.z = fmaf(p.beta, ci.z, o.z);
-                    o.w = fmaf(p.beta, ci.w, o.w);
+                    o.x = fmaf(beta, ci.x, o.x);
+                    o.y = fmaf(beta, ci.y, o.y);
+                    o.z = fmaf(beta, ci.z, o.z);
+                    o.w = fmaf(beta, ci.w, o.w);
                 }
                 *reinterpret_cast<float4 *>(crow + j) = o;
                 rs += (double)o.x + (double)o.y + (double)o.z + (double)o.w;
             }
-            if (p.rowsum) p.rowsum[(long long)(col0 / CPT) * p.M + row] = rs;
+            if (rowsum) rowsum[(long long)(col0 / CPT) * M + row] = rs;
         }
         if (!ok) atomicExch(&g_tc_error, 3);
     }
@@ -429,17 +470,26 @@ int tc_gemm_check(const TcGemmArgs &a) {
     return OPB_OK;
 }
 
-template <int BN, int STAGES>
-static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
+template <int BN, int STAGES, bool BATCHED>
+static int set_smem_attr() {
     using Cfg = TcCfg<BN, STAGES>;
     static bool attr_set[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             Cfg::SMEM);
         if (e != cudaSuccess) return (int)e;
         attr_set[dev] = true;
     }
+    return 0;
+}
+
+template <int BN, int STAGES>
+static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
+    using Cfg = TcCfg<BN, STAGES>;
+    int e0 = set_smem_attr<BN, STAGES, false>();
+    if (e0) return e0;
     CUtensorMap mAh, mAl, mBh, mBl;
     int r;
     if ((r = make_map(&mAh, a.Ahi, a.M, a.K, a.lda, TC_BM)) != OPB_OK) return r;
@@ -449,8 +499,44 @@ static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
     const int ntiles = (a.M / TC_BM) * (a.N / BN);
     const int grid = ntiles < num_sms() ? ntiles : num_sms();
-    k_tc_gemm<BN, STAGES><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl, p);
+    TcBatch none{nullptr, nullptr, nullptr, 0};
+    k_tc_gemm<BN, STAGES, false><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl, p, none);
     return (int)cudaGetLastError();
+}
+
+int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo, long long M, long long lda,
+                 const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long N, long long ldb, long long K, int bn) {
+    int r;
+    if ((r = make_map(&out4[0], Ahi, M, K, lda, TC_BM)) != OPB_OK) return r;
+    if ((r = make_map(&out4[1], Alo, M, K, lda, TC_BM)) != OPB_OK) return r;
+    if ((r = make_map(&out4[2], Bhi, N, K, ldb, bn)) != OPB_OK) return r;
+    if ((r = make_map(&out4[3], Blo, N, K, ldb, bn)) != OPB_OK) return r;
+    return OPB_OK;
+}
+
+template <int BN, int STAGES>
+static int launch_batched_impl(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
+                               int grid, cudaStream_t s) {
+    using Cfg = TcCfg<BN, STAGES>;
+    int e0 = set_smem_attr<BN, STAGES, true>();
+    if (e0) return e0;
+    CUtensorMap dummy;
+    std::memset(&dummy, 0, sizeof(dummy));
+    TcParams p{};
+    TcBatch bt{maps, probs, work, nwork};
+    k_tc_gemm<BN, STAGES, true><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(dummy, dummy, dummy, dummy, p, bt);
+    return (int)cudaGetLastError();
+}
+
+int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
+                           int grid, cudaStream_t s) {
+    if (nwork <= 0) return OPB_OK;
+    if (grid <= 0 || grid > nwork) grid = nwork < num_sms() ? nwork : num_sms();
+    switch (bn) {
+        case 128: return launch_batched_impl<128, 3>(maps, probs, work, nwork, grid, s);
+        case 64: return launch_batched_impl<64, 4>(maps, probs, work, nwork, grid, s);
+        default: return OPB_E_UNSUPPORTED;
+    }
 }
 
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {

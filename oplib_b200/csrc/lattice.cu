@@ -178,14 +178,16 @@ int solve_bf16x3(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_a
         // D = 2E + E.E in place of E, with FP64 row-sum partials
         g.C = b.X; g.Cin = b.X; g.alpha = 1.f; g.beta = 2.f; g.rowsum = b.part;
         LT(tc_gemm_ksplit(g, s));
-        const bool last = (r + 1 == L.niter);
-        LT(opb::launch_renorm(d, b.X, b.part, np, 1, last ? nullptr : b.Ahi, last ? nullptr : b.Alo,
-                              last ? nullptr : b.Bhi, last ? nullptr : b.Blo, s));
+        // the last level emits P1 = I + E and its splits (row-major: A of the first chain and
+        // of pricing; transposed: B of every chain)
+        if (r + 1 == L.niter) LT(opb::launch_renorm_to_p(d, b.X, b.part, np, b.Ahi, b.Alo, b.Bhi, b.Blo, s));
+        else LT(opb::launch_renorm(d, b.X, b.part, np, 1, b.Ahi, b.Alo, b.Bhi, b.Blo, s));
     }
-    // P1 = I + E; splits of P1 (row-major: A of the first chain / pricing; transposed: B of every chain)
-    LT(opb::launch_add_identity(d, b.X, s));
+    if (L.niter == 0) {
+        LT(opb::launch_add_identity(d, b.X, s));
+        LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s));
+    }
     if (P_out) return (int)cudaMemcpyAsync(P_out, b.X, sizeof(float) * (size_t)d * d, cudaMemcpyDeviceToDevice, s);
-    LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s));
     const int nKp = padded_nk(nK, OPB_BF16X3);
     LT(opb::launch_payoff(d, nK, nKp, L.x, L.strikes, nullptr, b.GThi, b.GTlo, s));
     opb::TcGemmArgs pg{};

@@ -1,6 +1,7 @@
 // Internal launcher declarations shared by the library's translation units.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -26,6 +27,33 @@ int launch_payoff(int d, int nK, int ldk, const double *x, const double *K, floa
 int launch_discount(int d, int nK, int ldk, const float *V32, double disc, double *V64, int y0, double *quotes,
                     cudaStream_t s);
 
+// Batched lattice tables (device memory).
+struct BatchLattice {
+    int d, y0;
+    long long row_off;    // first global row (rows of all lattices concatenated)
+    double dt, rate, period;
+    float *E;             // d x d FP32 (E-form, then P1)
+    float *Pa;            // d x d FP32 chain product
+    float *V;             // d x ldk FP32 pricing result
+    __nv_bfloat16 *GThi, *GTlo;  // ldk x d payoff splits
+};
+struct RenormProblem {
+    int d, pad;
+    float *X;
+    const double *partial;
+    __nv_bfloat16 *Ahi, *Alo, *Bhi, *Blo;
+};
+int launch_renorm_to_p(int d, float *X, const double *partial, int nparts, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
+                       __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s);
+// work items: problem << 16 | mode << 14 | tile_r << 7 | tile_c (64 x 64 tiles)
+int launch_renorm_batched(const RenormProblem *probs, const uint32_t *work, int nwork, int parts_div, cudaStream_t s);
+int launch_ek_batched(const BatchLattice *lats, int nlat, long long total_rows, int w, const int *cols,
+                      const double *vals, cudaStream_t s);
+int launch_payoff_batched(const BatchLattice *lats, int nlat, long long total_rows, int nK, int ldk, const double *x,
+                          const double *strikes, cudaStream_t s);
+int launch_quotes_batched(const BatchLattice *lats, int nlat, int nK, int ldk, int m, int nmat, double *quotes,
+                          cudaStream_t s);
+
 // gemm_tc.cu -- split-BF16 tensor-core GEMM.
 //   C[M,N] = alpha * (Ahi.Bhi^T + Ahi.Blo^T + Alo.Bhi^T) + beta * Cin[M,N]
 // A* are M x K row-major (K-major), B* are N x K row-major (the K-major form of the
@@ -45,6 +73,22 @@ int tc_gemm_tile_n(int N);                    // tile width chosen for N (0 if u
 int tc_gemm_check(const TcGemmArgs &a);       // argument/alignment check, OPB_* code
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s);
 int tc_gemm_nparts(int N);                    // number of row-sum partials written
+
+// Batched launches: problem descriptors and tensor maps live in device memory.
+struct TcProblem {
+    int M, N, K, pad;
+    float *C;
+    const float *Cin;
+    double *rowsum;       // partials rowsum[(col/min(bn,128)) * M + row]
+    long long ldc;
+    float alpha, beta;
+    long long pad2;
+};
+int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo, long long M, long long lda,
+                 const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long N, long long ldb, long long K, int bn);
+// work: packed (problem << 16 | m-tile << 8 | n-tile); bn in {64, 128}
+int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
+                           int grid, cudaStream_t s);
 
 // sck.cu
 int launch_sck_rm(int d, int nrows, const float *P, float *C, cudaStream_t s);

@@ -162,24 +162,34 @@ __global__ void k_renorm(int d, float *__restrict__ X, const double *__restrict_
     }
 }
 
-// Vectorised form of k_renorm for d % 64 == 0: 64 x 64 tiles, 256 threads, float4 loads
+// Vectorised renormalisation of one 64 x 64 tile (d % 64 == 0), 256 threads: float4 loads
 // and stores of X, 8-byte stores of four BF16 parts, and the transposed parts staged
 // through shared memory so that every global access is a contiguous run per warp.
-__global__ void __launch_bounds__(256) k_renorm64(int d, float *__restrict__ X, const double *__restrict__ partial,
-                                                  int nparts, int eform, __nv_bfloat16 *__restrict__ Ahi,
-                                                  __nv_bfloat16 *__restrict__ Alo, __nv_bfloat16 *__restrict__ Bhi,
-                                                  __nv_bfloat16 *__restrict__ Blo) {
-    __shared__ double s_sum[64], s_inv[64];
-    __shared__ __nv_bfloat16 th[64][72], tl[64][72];
+// Modes: 0 = E-form in, E-form out; 1 = E-form in, P-form out (P = I + E_new: the last
+// squaring level); 2 = P-form in and out.  nparts = 0 skips the scaling (pure split).
+struct RenormSmem {
+    double s_sum[64], s_inv[64];
+    __nv_bfloat16 th[64][72], tl[64][72];
+};
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) {
+    return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+
+__device__ __forceinline__ void renorm64_tile(RenormSmem &sm, int d, float *__restrict__ X,
+                                              const double *__restrict__ partial, int nparts, int mode,
+                                              __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
+                                              __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo,
+                                              int r0, int c0) {
     const int tid = threadIdx.x;
-    const int r0 = blockIdx.y * 64, c0 = blockIdx.x * 64;
+    const bool eform = mode != 2;
     if (tid < 64) {
         double s = 0.0;
         const int r = r0 + tid;
         for (int p = 0; p < nparts; p++) s += partial[(long long)p * d + r];
-        s_sum[tid] = s;
-        const double den = eform ? 1.0 + s : s;
-        s_inv[tid] = den != 0.0 ? 1.0 / den : 0.0;
+        sm.s_sum[tid] = s;
+        const double den = nparts == 0 ? 1.0 : (eform ? 1.0 + s : s);
+        sm.s_inv[tid] = den != 0.0 ? 1.0 / den : 0.0;
     }
     __syncthreads();
     const int lc = (tid & 15) * 4;
@@ -189,42 +199,112 @@ __global__ void __launch_bounds__(256) k_renorm64(int d, float *__restrict__ X, 
         const int r = r0 + lr;
         const long long o = (long long)r * d + c0 + lc;
         float4 v = *reinterpret_cast<const float4 *>(X + o);
-        const double su = s_sum[lr], inv = s_inv[lr];
+        const double su = sm.s_sum[lr], inv = sm.s_inv[lr];
         float f[4] = {v.x, v.y, v.z, v.w};
         __nv_bfloat16 h[4], l[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             double x = (double)f[j];
-            if (eform && r == c0 + lc + j) x -= su;
-            f[j] = (float)(x * inv);
+            const bool diag = (r == c0 + lc + j);
+            if (eform && diag) x -= su;
+            x *= inv;
+            if (mode == 1 && diag) x += 1.0;
+            f[j] = (float)x;
             split2(f[j], h[j], l[j]);
-            th[lr][lc + j] = h[j];
-            tl[lr][lc + j] = l[j];
+            sm.th[lr][lc + j] = h[j];
+            sm.tl[lr][lc + j] = l[j];
         }
         *reinterpret_cast<float4 *>(X + o) = make_float4(f[0], f[1], f[2], f[3]);
         if (Ahi) {
-            *reinterpret_cast<uint2 *>(Ahi + o) = make_uint2(
-                (uint32_t)__bfloat16_as_ushort(h[0]) | ((uint32_t)__bfloat16_as_ushort(h[1]) << 16),
-                (uint32_t)__bfloat16_as_ushort(h[2]) | ((uint32_t)__bfloat16_as_ushort(h[3]) << 16));
-            *reinterpret_cast<uint2 *>(Alo + o) = make_uint2(
-                (uint32_t)__bfloat16_as_ushort(l[0]) | ((uint32_t)__bfloat16_as_ushort(l[1]) << 16),
-                (uint32_t)__bfloat16_as_ushort(l[2]) | ((uint32_t)__bfloat16_as_ushort(l[3]) << 16));
+            *reinterpret_cast<uint2 *>(Ahi + o) = make_uint2(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]));
+            *reinterpret_cast<uint2 *>(Alo + o) = make_uint2(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]));
         }
     }
     if (!Bhi) return;
     __syncthreads();
-    // transposed: output row (c0 + orow) holds input rows r0 + lc .. r0 + lc + 3
 #pragma unroll
     for (int pass = 0; pass < 4; pass++) {
         const int orow = pass * 16 + (tid >> 4);
         const long long o = (long long)(c0 + orow) * d + r0 + lc;
-        *reinterpret_cast<uint2 *>(Bhi + o) = make_uint2(
-            (uint32_t)__bfloat16_as_ushort(th[lc + 0][orow]) | ((uint32_t)__bfloat16_as_ushort(th[lc + 1][orow]) << 16),
-            (uint32_t)__bfloat16_as_ushort(th[lc + 2][orow]) | ((uint32_t)__bfloat16_as_ushort(th[lc + 3][orow]) << 16));
-        *reinterpret_cast<uint2 *>(Blo + o) = make_uint2(
-            (uint32_t)__bfloat16_as_ushort(tl[lc + 0][orow]) | ((uint32_t)__bfloat16_as_ushort(tl[lc + 1][orow]) << 16),
-            (uint32_t)__bfloat16_as_ushort(tl[lc + 2][orow]) | ((uint32_t)__bfloat16_as_ushort(tl[lc + 3][orow]) << 16));
+        *reinterpret_cast<uint2 *>(Bhi + o) = make_uint2(pack_bf16(sm.th[lc + 0][orow], sm.th[lc + 1][orow]),
+                                                         pack_bf16(sm.th[lc + 2][orow], sm.th[lc + 3][orow]));
+        *reinterpret_cast<uint2 *>(Blo + o) = make_uint2(pack_bf16(sm.tl[lc + 0][orow], sm.tl[lc + 1][orow]),
+                                                         pack_bf16(sm.tl[lc + 2][orow], sm.tl[lc + 3][orow]));
     }
+}
+
+__global__ void __launch_bounds__(256) k_renorm64(int d, float *__restrict__ X, const double *__restrict__ partial,
+                                                  int nparts, int mode, __nv_bfloat16 *__restrict__ Ahi,
+                                                  __nv_bfloat16 *__restrict__ Alo, __nv_bfloat16 *__restrict__ Bhi,
+                                                  __nv_bfloat16 *__restrict__ Blo) {
+    __shared__ RenormSmem sm;
+    renorm64_tile(sm, d, X, partial, nparts, mode, Ahi, Alo, Bhi, Blo, blockIdx.y * 64, blockIdx.x * 64);
+}
+
+// Batched: one block per work item (problem << 16 | mode << 14 | tile_r << 7 | tile_c);
+// nparts of problem i is d_i / parts_div (0 when parts_div == 0: pure split).
+__global__ void __launch_bounds__(256) k_renorm64_batched(const RenormProblem *__restrict__ probs,
+                                                          const uint32_t *__restrict__ work, int parts_div) {
+    __shared__ RenormSmem sm;
+    const uint32_t w = work[blockIdx.x];
+    const RenormProblem &pr = probs[w >> 16];
+    const int mode = (int)((w >> 14) & 3u);
+    const int nparts = parts_div > 0 ? pr.d / parts_div : 0;
+    renorm64_tile(sm, pr.d, pr.X, pr.partial, nparts, mode, pr.Ahi, pr.Alo, mode == 2 ? nullptr : pr.Bhi,
+                  mode == 2 ? nullptr : pr.Blo, (int)((w >> 7) & 127u) * 64, (int)(w & 127u) * 64);
+}
+
+// Batched ELL scatter into zeroed dense E-form matrices: thread per global ELL slot
+// (rows of all lattices concatenated; row_off[i] = first global row of lattice i).
+__global__ void k_ek_scatter_batched(const BatchLattice *__restrict__ lats, int nlat, long long total_rows, int w,
+                                     const int *__restrict__ cols, const double *__restrict__ vals) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= total_rows * w) return;
+    const long long grow = t / w;
+    int lo = 0, hi = nlat - 1;
+    while (lo < hi) {  // last lattice with row_off <= grow
+        int mid = (lo + hi + 1) >> 1;
+        if (lats[mid].row_off <= grow) lo = mid; else hi = mid - 1;
+    }
+    const BatchLattice &L = lats[lo];
+    const int y = (int)(grow - L.row_off);
+    const int z = cols[t];
+    if (z < 0 || z >= L.d) return;
+    L.E[(long long)y * L.d + z] = (float)(L.dt * vals[t]);
+}
+
+// Batched payoff splits: G^T[k][z] = (x_z - K_k)^+ for strikes k < nK of lattice i and 0
+// for the padding columns nK..ldk-1.
+__global__ void k_payoff_batched(const BatchLattice *__restrict__ lats, int nlat, long long total_rows, int nK, int ldk,
+                                 const double *__restrict__ x, const double *__restrict__ strikes) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= total_rows * ldk) return;
+    const long long grow = t / ldk;
+    const int k = (int)(t - grow * ldk);
+    int lo = 0, hi = nlat - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (lats[mid].row_off <= grow) lo = mid; else hi = mid - 1;
+    }
+    const BatchLattice &L = lats[lo];
+    const int z = (int)(grow - L.row_off);
+    double g = k < nK ? x[grow] - strikes[(long long)lo * nK + k] : 0.0;
+    float f = (float)(g > 0.0 ? g : 0.0);
+    __nv_bfloat16 h, l;
+    split2(f, h, l);
+    L.GThi[(long long)k * L.d + z] = h;
+    L.GTlo[(long long)k * L.d + z] = l;
+}
+
+// quotes[(i*nmat + m-1)*nK + k] = exp(-r_i T_m) * V_i[y0_i, k]
+__global__ void k_quotes_batched(const BatchLattice *__restrict__ lats, int nlat, int nK, int ldk, int m, int nmat,
+                                 double *__restrict__ quotes) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nlat * nK) return;
+    int i = t / nK, k = t - i * nK;
+    const BatchLattice &L = lats[i];
+    const double disc = exp(-L.rate * L.period * m);
+    quotes[((long long)i * nmat + (m - 1)) * nK + k] = disc * (double)L.V[(long long)L.y0 * ldk + k];
 }
 
 // E-form -> P-form: P = I + E (in place), FP32.
@@ -304,11 +384,49 @@ int launch_renorm(int d, float *X, const double *partial, int nparts, int eform,
                   __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s) {
     if (d % 64 == 0 && (Ahi != nullptr) == (Alo != nullptr)) {
         dim3 g(d / 64, d / 64);
-        k_renorm64<<<g, 256, 0, s>>>(d, X, partial, nparts, eform, Ahi, Alo, Bhi, Blo);
+        k_renorm64<<<g, 256, 0, s>>>(d, X, partial, nparts, eform ? 0 : 2, Ahi, Alo, Bhi, Blo);
         return (int)cudaGetLastError();
     }
     dim3 g((d + 31) / 32, (d + 31) / 32);
     k_renorm<<<g, 256, 0, s>>>(d, X, partial, nparts, eform, Ahi, Alo, Bhi, Blo);
+    return (int)cudaGetLastError();
+}
+
+// E-form renorm whose output is P = I + E_new with both splits (the last squaring level).
+int launch_renorm_to_p(int d, float *X, const double *partial, int nparts, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
+                       __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s) {
+    if (d % 64) return OPB_E_UNSUPPORTED;
+    dim3 g(d / 64, d / 64);
+    k_renorm64<<<g, 256, 0, s>>>(d, X, partial, nparts, 1, Ahi, Alo, Bhi, Blo);
+    return (int)cudaGetLastError();
+}
+
+int launch_renorm_batched(const RenormProblem *probs, const uint32_t *work, int nwork, int parts_div, cudaStream_t s) {
+    if (nwork <= 0) return OPB_OK;
+    k_renorm64_batched<<<nwork, 256, 0, s>>>(probs, work, parts_div);
+    return (int)cudaGetLastError();
+}
+
+int launch_ek_batched(const BatchLattice *lats, int nlat, long long total_rows, int w, const int *cols,
+                      const double *vals, cudaStream_t s) {
+    long long n = total_rows * w;
+    if (n <= 0) return OPB_OK;
+    k_ek_scatter_batched<<<(int)((n + 255) / 256), 256, 0, s>>>(lats, nlat, total_rows, w, cols, vals);
+    return (int)cudaGetLastError();
+}
+
+int launch_payoff_batched(const BatchLattice *lats, int nlat, long long total_rows, int nK, int ldk, const double *x,
+                          const double *strikes, cudaStream_t s) {
+    long long n = total_rows * ldk;
+    if (n <= 0) return OPB_OK;
+    k_payoff_batched<<<(int)((n + 255) / 256), 256, 0, s>>>(lats, nlat, total_rows, nK, ldk, x, strikes);
+    return (int)cudaGetLastError();
+}
+
+int launch_quotes_batched(const BatchLattice *lats, int nlat, int nK, int ldk, int m, int nmat, double *quotes,
+                          cudaStream_t s) {
+    int n = nlat * nK;
+    k_quotes_batched<<<(n + 255) / 256, 256, 0, s>>>(lats, nlat, nK, ldk, m, nmat, quotes);
     return (int)cudaGetLastError();
 }
 

@@ -190,3 +190,106 @@ def mc_run(Cm: torch.Tensor, y0: int, nsteps: int, seed: int, npaths: int, path0
     call("opb_mc_mt19937", _ptr(Cm), d, 1, _ptr(guide), nb if guide is not None else 0, d, y0, nsteps,
          seed & 0xFFFFFFFF, path0, npaths, _ptr(ypaths), _ptr(x), strike, barrier, disc, _ptr(scratch), _ptr(sums))
     return sums, ypaths
+
+
+# -------------------------------------------------------------------- batched lattices
+
+class BatchDesc(C.Structure):
+    """Mirror of ``opb_batch_desc``."""
+
+    _fields_ = [
+        ("nlat", C.c_int), ("d", C.c_void_p), ("y0", C.c_void_p), ("niter", C.c_void_p), ("dt", C.c_void_p),
+        ("rate", C.c_void_p), ("ell_width", C.c_int), ("gen_cols", C.c_void_p), ("gen_vals", C.c_void_p),
+        ("x", C.c_void_p), ("nmat", C.c_int), ("period", C.c_double), ("nK", C.c_int), ("strikes", C.c_void_p),
+    ]
+
+
+class Batch:
+    """Many uneven lattices solved together: one persistent tensor-core launch and one
+    renormalisation launch per squaring level for all of them (``opb_batch_*``)."""
+
+    def __init__(self, lattices: list, strikes, nmat: int, period: float, dt0: float, mode="bf16x3",
+                 autotune: bool = True):
+        import numpy as np
+        self.mode = MODES[mode] if isinstance(mode, str) else mode
+        self.lats = lattices
+        dev = lattices[0].device
+        self.device = dev
+        self.nlat = len(lattices)
+        self.nmat, self.period = nmat, period
+        K = torch.as_tensor(strikes, dtype=torch.float64)
+        if K.dim() == 1:
+            K = K.unsqueeze(0).expand(self.nlat, -1)
+        self.strikes = K.contiguous().to(dev)
+        self.nK = self.strikes.shape[1]
+        plans = [lat.plan(period, dt0) for lat in lattices]
+        self.plans = plans
+        w = lattices[0].width
+        self.cols = torch.cat([lat.cols for lat in lattices])
+        self.vals = torch.cat([lat.vals for lat in lattices])
+        self.x = torch.cat([lat.x for lat in lattices])
+        self._d = np.array([lat.d for lat in lattices], dtype=np.int32)
+        self._y0 = np.array([lat.y0 for lat in lattices], dtype=np.int32)
+        self._niter = np.array([p.niter for p in plans], dtype=np.int32)
+        self._dt = np.array([p.dt for p in plans], dtype=np.float64)
+        self._rate = np.array([lat.rate for lat in lattices], dtype=np.float64)
+        bd = BatchDesc()
+        bd.nlat, bd.d, bd.y0, bd.niter = self.nlat, self._d.ctypes.data, self._y0.ctypes.data, self._niter.ctypes.data
+        bd.dt, bd.rate, bd.ell_width = self._dt.ctypes.data, self._rate.ctypes.data, w
+        bd.gen_cols, bd.gen_vals, bd.x = _ptr(self.cols), _ptr(self.vals), _ptr(self.x)
+        bd.nmat, bd.period, bd.nK, bd.strikes = nmat, period, self.nK, _ptr(self.strikes)
+        self.desc = bd
+        lib = _lib.load()
+        n = lib.opb_batch_workspace_size(C.byref(bd), self.mode)
+        if n == 0:
+            raise _lib.OpcudaError("opb_batch_workspace_size", -1, "invalid batch description")
+        self.ws = torch.empty(int(n), dtype=torch.uint8, device=dev)
+        self.plan = C.c_void_p()
+        bind_stream(dev)
+        call("opb_batch_plan_create", C.byref(bd), self.mode, _ptr(self.ws), self.ws.numel(), C.byref(self.plan))
+        self.tune_ms = None
+        if autotune and self.mode == BF16X3:
+            ms = (C.c_float * 4)()
+            best = C.c_int()
+            call("opb_batch_autotune", self.plan, 2, ms, C.byref(best))
+            self.tune_ms = list(ms)
+            self.config = best.value
+
+    def set_config(self, cfg: int, grid: int = 0):
+        call("opb_batch_set_config", self.plan, cfg, grid)
+        self.config = cfg
+
+    def execute(self, quotes: torch.Tensor | None = None) -> torch.Tensor:
+        if quotes is None:
+            quotes = torch.empty(self.nlat, self.nmat, self.nK, dtype=torch.float64, device=self.device)
+        bind_stream(self.device)
+        call("opb_batch_execute", self.plan, _ptr(quotes))
+        return quotes
+
+    def launches(self) -> int:
+        return _lib.load().opb_batch_launches(self.plan)
+
+    def __del__(self):
+        try:
+            if getattr(self, "plan", None) is not None and self.plan.value:
+                _lib.load().opb_batch_plan_destroy(self.plan)
+                self.plan = None
+        except Exception:
+            pass
+
+
+def calibration_sweep(nlat=512, seed=20260, sizes=tuple(range(256, 2049, 128)), device="cuda"):
+    """Seeded local-vol lattices of the calibration sweep: n uniform over ``sizes``,
+    level ~ U[0.1, 0.4], skew ~ U[-0.3, 0.3], width ~ U[0.2, 1.0], r ~ U[0, 0.05],
+    sigma(x) = max(0.01, level + skew * exp(-((x - 1)/width)^2))."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    n = rng.choice(np.array(sizes), size=nlat)
+    level = rng.uniform(0.1, 0.4, nlat)
+    skew = rng.uniform(-0.3, 0.3, nlat)
+    width = rng.uniform(0.2, 1.0, nlat)
+    r = rng.uniform(0.0, 0.05, nlat)
+    params = [dict(n=int(n[i]), level=float(level[i]), skew=float(skew[i]), width=float(width[i]), rate=float(r[i]),
+                   floor=0.01) for i in range(nlat)]
+    lats = [Lattice.local_vol(device=device, **p) for p in params]
+    return lats, params

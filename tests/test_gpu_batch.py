@@ -1,0 +1,101 @@
+"""GPU parity of the batched (ragged) lattice solve: every lattice of a small uneven batch
+against the FP64 oracle (<= 1e-5 absolute, the target accuracy) and against the
+single-lattice solve of the same lattice; every launch configuration of the autotuner
+gives the same quotes; the whole sweep replays from a CUDA graph."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [dict(n=128, level=0.25, skew=0.1, width=0.5, rate=0.02, floor=0.01),
+         dict(n=384, level=0.15, skew=-0.2, width=0.3, rate=0.04, floor=0.01),
+         dict(n=256, level=0.35, skew=0.25, width=0.9, rate=0.0, floor=0.01),
+         dict(n=128, level=0.1, skew=-0.3, width=0.2, rate=0.05, floor=0.01),
+         dict(n=512, level=0.2, skew=0.05, width=0.6, rate=0.03, floor=0.01)]
+NMAT, PERIOD, DT0 = 4, 0.25, 2.0 ** -14
+STRIKES = 0.5 + np.arange(32) / 31.0
+
+
+def _oracle_quotes(spec):
+    x = O.log_grid(spec["n"])
+    sig = O.lv_sigma(x, spec["level"], spec["skew"], spec["width"], spec["floor"])
+    L = O.lv_generator_fast(x, spec["rate"] * x, sig * x)
+    V, _, _ = O.solve_lattice_fp64(L, x, STRIKES, spec["rate"], PERIOD, NMAT, DT0)
+    return V[:, O.nearest_node(x), :]
+
+
+@pytest.fixture(scope="module")
+def batch_and_refs(cuda):
+    from oplib_b200.model import Batch, Lattice
+    lats = [Lattice.local_vol(device=cuda, **s) for s in SPECS]
+    refs = [_oracle_quotes(s) for s in SPECS]
+    b = Batch(lats, STRIKES, NMAT, PERIOD, DT0, mode="bf16x3", autotune=True)
+    return lats, refs, b
+
+
+def test_batch_vs_fp64_and_single(batch_and_refs):
+    lats, refs, b = batch_and_refs
+    q = b.execute().cpu().numpy()
+    torch.cuda.synchronize()
+    from oplib_b200 import _lib
+    assert _lib.load().opb_tc_error() == 0
+    assert b.config in range(4) and len(b.tune_ms) == 4
+    for i, lat in enumerate(lats):
+        err = np.abs(q[i] - refs[i]).max()
+        print(f"lattice {i} d={lat.d}: max abs err vs FP64 {err:.2e}")
+        assert err <= 1e-5, (i, err)
+        qs, _ = lat.solve(STRIKES, NMAT, PERIOD, DT0, mode="bf16x3")
+        assert np.abs(q[i] - qs.cpu().numpy()).max() < 2e-7
+
+
+def test_batch_configs_agree(batch_and_refs):
+    lats, refs, b = batch_and_refs
+    outs = []
+    for cfg in range(4):
+        b.set_config(cfg)
+        outs.append(b.execute().cpu().numpy())
+    for o in outs[1:]:
+        assert np.abs(o - outs[0]).max() < 2e-7
+    for i in range(len(lats)):
+        assert np.abs(outs[1][i] - refs[i]).max() <= 1e-5
+
+
+def test_batch_graph_replay(batch_and_refs, cuda):
+    from oplib_b200.model import bind_stream
+    lats, refs, b = batch_and_refs
+    q0 = b.execute()
+    q = torch.empty_like(q0)
+    s = torch.cuda.Stream(cuda)
+    s.wait_stream(torch.cuda.current_stream(cuda))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        bind_stream(cuda)
+        g.capture_begin()
+        b.execute(q)
+        g.capture_end()
+    torch.cuda.current_stream(cuda).wait_stream(s)
+    bind_stream(cuda)
+    q.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(q, q0)
+
+
+def test_batch_fp32_mode(cuda):
+    from oplib_b200.model import Batch, Lattice
+    specs = SPECS[:3]
+    lats = [Lattice.local_vol(device=cuda, **s) for s in specs]
+    b = Batch(lats, STRIKES, NMAT, PERIOD, DT0, mode="fp32")
+    q = b.execute().cpu().numpy()
+    for i, s in enumerate(specs):
+        assert np.abs(q[i] - _oracle_quotes(s)).max() <= 1e-5
+
+
+def test_batch_rejects_bad_sizes(cuda):
+    from oplib_b200.model import Batch, Lattice
+    lats = [Lattice.local_vol(n=200, device=cuda)]
+    with pytest.raises(Exception):
+        Batch(lats, STRIKES, NMAT, PERIOD, DT0, mode="bf16x3")
