@@ -259,6 +259,20 @@ def run_b200(args, rank, world, local_rank):
                  "fp32_max_abs_err_vs_fp64": float((q32 - q_ref).abs().max().item()),
                  "speedup_vs_fp32": round(ms32 / ms, 2)}
         del ws32
+        m16 = MODES["fp16x3"]
+        ws16 = lat.workspace(NK, m16)
+        q16 = torch.empty_like(quotes)
+        _lib.call("opb_lattice_solve", C.byref(desc), m16, ws16.data_ptr(), ws16.numel(), q16.data_ptr(), None)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(3):
+            _lib.call("opb_lattice_solve", C.byref(desc), m16, ws16.data_ptr(), ws16.numel(), q16.data_ptr(), None)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms16 = e0.elapsed_time(e1) / 3
+        extra["fp16x3"] = {"quotes_per_s": round(NMAT * NK * world / (ms16 * 1e-3), 1),
+                           "max_abs_err_vs_fp64": float((q16 - q_ref).abs().max().item())}
+        del ws16
 
     quotes_per_step = NMAT * NK * world
     value = quotes_per_step / (ms * 1e-3)
@@ -436,6 +450,30 @@ def run_mc(args):
     return line
 
 
+def _fp64_lv_quotes(lat, plan, strikes, nmat, period, torch):
+    """FP64 solve of one ELL lattice on the device with torch (accuracy reference)."""
+    d = lat.d
+    cols = lat.cols.view(d, -1).long()
+    vals = lat.vals.view(d, -1)
+    L = torch.zeros(d, d, dtype=torch.float64, device=lat.device)
+    mask = cols >= 0
+    rows = torch.arange(d, device=lat.device).unsqueeze(1).expand_as(cols)
+    L.index_put_((rows[mask], cols[mask]), vals[mask], accumulate=True)
+    P = torch.eye(d, dtype=torch.float64, device=lat.device) + plan.dt * L
+    for _ in range(plan.niter):
+        P = P @ P
+        P /= P.sum(dim=1, keepdim=True)
+    K = torch.tensor(strikes, dtype=torch.float64, device=lat.device)
+    G = torch.clamp(lat.x.unsqueeze(1) - K.unsqueeze(0), min=0.0)
+    out, Pm = [], P
+    for m in range(1, nmat + 1):
+        if m > 1:
+            Pm = Pm @ P
+            Pm /= Pm.sum(dim=1, keepdim=True)
+        out.append(math.exp(-lat.rate * period * m) * (Pm[lat.y0] @ G))
+    return torch.stack(out)
+
+
 def run_batch(args):
     """Config 3: calibration sweep of 512 seeded local-vol lattices, n uniform over
     {256, 384, ..., 2048}, 32 strikes x 8 quarterly maturities each (131,072 quotes);
@@ -451,29 +489,47 @@ def run_batch(args):
     nlat = args.nlat
     lats, params = calibration_sweep(nlat=nlat, device=dev)
     strikes = [0.5 + j / 31.0 for j in range(32)]
-    t0 = time.perf_counter()
-    b = Batch(lats, strikes, 8, 0.25, 2.0 ** -14, mode="bf16x3", autotune=True)
-    torch.cuda.synchronize()
-    t_plan = time.perf_counter() - t0
-    q = torch.empty(nlat, 8, 32, dtype=torch.float64, device=dev)
-    for _ in range(args.warmup):
-        b.execute(q)
-    g = _graph(lambda: b.execute(q), dev, torch)
-    g.replay()
-    ms = _time(g.replay, args.steps, stream, torch)
     nquotes = nlat * 8 * 32
-    useful = sum(2.0 * p["n"] ** 3 * (pl.niter + 7) for p, pl in zip(params, b.plans))
-    line = {"metric": "priced quotes/sec, batched calibration sweep (split-BF16, one launch per level)",
+    order = None
+    res = {}
+    for mname in ["fp16x3", "bf16x3"]:
+        t0 = time.perf_counter()
+        b = Batch(lats, strikes, 8, 0.25, 2.0 ** -14, mode=mname, autotune=True)
+        torch.cuda.synchronize()
+        t_plan = time.perf_counter() - t0
+        q = torch.empty(nlat, 8, 32, dtype=torch.float64, device=dev)
+        for _ in range(args.warmup):
+            b.execute(q)
+        g = _graph(lambda: b.execute(q), dev, torch)
+        g.replay()
+        ms = _time(g.replay, args.steps, stream, torch)
+        if order is None:
+            order = sorted(range(nlat), key=lambda i: -b.plans[i].niter)
+            sample = order[:8] + order[-4:]
+            refs = {i: _fp64_lv_quotes(lats[i], b.plans[i], strikes, 8, 0.25, torch) for i in sample}
+        errs = {int(i): float((q[i] - refs[i]).abs().max().item()) for i in sample}
+        res[mname] = dict(ms=ms, plan_s=t_plan, tune=b.tune_ms, cfg=b.config, launches=b.launches(), errs=errs,
+                          q=q, plans=b.plans)
+        del g, b
+    prim = res["fp16x3"]
+    ms = prim["ms"]
+    useful = sum(2.0 * p["n"] ** 3 * (pl.niter + 7) for p, pl in zip(params, prim["plans"]))
+    line = {"metric": "priced quotes/sec, batched calibration sweep (split tensor-core products, one launch per level)",
             "value": round(nquotes / (ms * 1e-3), 1), "unit": "quotes/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic",
+            "vs_baseline": None, "dtype": "fp16x3", "data": "synthetic",
             "config": {"workload": f"{nlat} LV lattices, n in 256..2048 step 128 (seed 20260), 32 strikes x 8 "
                                    "maturities, CUDA-graph replay", "nlat": nlat,
-                       "niter_range": [min(p.niter for p in b.plans), max(p.niter for p in b.plans)]},
+                       "niter_range": [min(p.niter for p in prim["plans"]), max(p.niter for p in prim["plans"])]},
             "useful_tflops": round(useful / (ms * 1e-3) / 1e12, 1),
             "mma_tflops": round(3 * useful / (ms * 1e-3) / 1e12, 1),
-            "autotune_ms_level0": [round(x, 3) for x in b.tune_ms], "config_chosen": b.config,
-            "launches_per_sweep": b.launches(), "plan_seconds": round(t_plan, 2)}
+            "autotune_ms_level0": [round(x, 3) for x in prim["tune"]], "config_chosen": prim["cfg"],
+            "launches_per_sweep": prim["launches"], "plan_seconds": round(prim["plan_s"], 2),
+            "max_abs_err_vs_fp64_sample": max(prim["errs"].values()), "sample_errs": prim["errs"],
+            "bf16x3": {"quotes_per_s": round(nquotes / (res["bf16x3"]["ms"] * 1e-3), 1),
+                       "max_abs_err_vs_fp64_sample": max(res["bf16x3"]["errs"].values())}}
+    q = prim["q"]
+    b = type("P", (), {"plans": prim["plans"]})
     if args.compare:
         b32 = Batch(lats, strikes, 8, 0.25, 2.0 ** -14, mode="fp32", autotune=False)
         q32 = b32.execute()
@@ -481,7 +537,10 @@ def run_batch(args):
         ms32 = _time(lambda: b32.execute(q32), 1, stream, torch)
         line["fp32_quotes_per_s"] = round(nquotes / (ms32 * 1e-3), 1)
         line["speedup_vs_fp32"] = round(ms32 / ms, 2)
-        line["max_abs_diff_bf16x3_vs_fp32"] = float((q - q32).abs().max().item())
+        line["max_abs_diff_vs_fp32"] = float((q - q32).abs().max().item())
+        line["fp32_max_abs_err_vs_fp64_sample"] = max(
+            float((q32[i] - _fp64_lv_quotes(lats[i], b.plans[i], strikes, 8, 0.25, torch)).abs().max().item())
+            for i in sample)
     return line
 
 
@@ -519,7 +578,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--mode", default="bf16x3", choices=["bf16x3", "fp32", "fp32_plain"])
+    ap.add_argument("--mode", default="bf16x3", choices=["bf16x3", "fp16x3", "fp32", "fp32_plain"])
     ap.add_argument("--no-compare", dest="compare", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu", action="store_false")
     ap.add_argument("--nlat", type=int, default=512, help="lattices for --workload batch")

@@ -42,6 +42,7 @@ extern "C" {
 #define OPB_FP32_PLAIN 0  /* FP32 SIMT products, reference semantics (no renormalisation) */
 #define OPB_FP32_RENORM 1 /* FP32 SIMT products + FP64 row renormalisation */
 #define OPB_BF16X3 2      /* split-BF16 tcgen05 products (E-form squaring) + FP64 renormalisation */
+#define OPB_FP16X3 3      /* as OPB_BF16X3 with FP16 parts of 2^15-scaled values (11+11 bits; same cost) */
 
 /* ------------------------------------------------------------------ runtime support */
 /* replaces oplib/opcuda/util.cu:204-207 (unsigned opcuda_get_status()) */
@@ -163,6 +164,10 @@ int opb_gemm_bf16x3(int M, int N, int K, const opb_bf16 *Ahi, const opb_bf16 *Al
                     const opb_bf16 *Bhi, const opb_bf16 *Blo, long long ldb, float alpha, const float *Cin,
                     float beta, float *C, long long ldc, double *rowsum);
 int opb_gemm_bf16x3_nparts(int N);
+/* new: the same product with FP16 parts (power-of-two-scaled splits; undo the scales in alpha) */
+int opb_gemm_f16x3(int M, int N, int K, const uint16_t *Ahi, const uint16_t *Alo, long long lda, const uint16_t *Bhi,
+                   const uint16_t *Blo, long long ldb, float alpha, const float *Cin, float beta, float *C,
+                   long long ldc, double *rowsum);
 /* reads and clears the device error word of the tensor-core kernels (0 = none) */
 int opb_tc_error(void);
 

@@ -23,7 +23,9 @@
 #include "common.cuh"
 #include "lattice.h"
 
-enum { OPB_FP32_PLAIN_B = 0, OPB_FP32_RENORM_B = 1, OPB_BF16X3_B = 2 };
+enum { OPB_FP32_PLAIN_B = 0, OPB_FP32_RENORM_B = 1, OPB_BF16X3_B = 2, OPB_FP16X3_B = 3 };
+static inline bool tc_mode_b(int m) { return m == OPB_BF16X3_B || m == OPB_FP16X3_B; }
+static constexpr float F16S = 32768.f;  // split scale of FP16 parts (|E|, P <= 1)
 
 struct opb_lattice_desc;  // lattice.cu
 extern "C" int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
@@ -74,6 +76,7 @@ struct ListRef {
 }  // namespace
 
 struct opb_batch_plan {
+    int f16 = 0;
     int mode = 0, nlat = 0, nmat = 0, nK = 0, ldk = 64, maxn = 0, cfg = 0, grid = 0;
     long long total_rows = 0;
     int ell_width = 0;
@@ -120,12 +123,12 @@ int check_batch(const opb_batch_desc *b, int mode) {
     if (!b->d || !b->y0 || !b->niter || !b->dt || !b->rate) return OPB_E_NULL;
     if (!b->gen_cols || !b->gen_vals || !b->x || !b->strikes) return OPB_E_NULL;
     if (b->ell_width < 1 || !(b->period > 0.0)) return OPB_E_ARG;
-    if (mode < 0 || mode > 2) return OPB_E_ARG;
+    if (mode < 0 || mode > 3) return OPB_E_ARG;
     for (int i = 0; i < b->nlat; i++) {
         int d = b->d[i];
         if (d < 128 || d > 8064 || b->y0[i] < 0 || b->y0[i] >= d || b->niter[i] < 1 || !(b->dt[i] > 0.0))
             return OPB_E_ARG;
-        if (mode == OPB_BF16X3_B && d % 128) return OPB_E_UNSUPPORTED;
+        if (tc_mode_b(mode) && d % 128) return OPB_E_UNSUPPORTED;
     }
     return OPB_OK;
 }
@@ -136,7 +139,7 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     const int n = b->nlat;
     std::vector<long long> off(n + 1, 0);
     for (int i = 0; i < n; i++) off[i + 1] = off[i] + b->d[i];
-    if (mode != OPB_BF16X3_B) {
+    if (!tc_mode_b(mode)) {
         size_t per_max = 0;
         std::vector<size_t> sz(n);
         for (int i = 0; i < n; i++) {
@@ -172,6 +175,7 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     size_t parts = 0;
     for (int i = 0; i < n; i++) parts += (size_t)(b->d[i] / 64) * b->d[i];
     double *part = c.take<double>(parts);
+    (void)c.take<float>(n);  // per-lattice FP16 payoff scales
 
     // ---- work lists (host), appended into one blob
     std::vector<uint32_t> W;
@@ -267,7 +271,7 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     std::vector<uint32_t> W;
     layout(b, mode, P, base, &W);
     const int n = b->nlat;
-    if (mode != OPB_BF16X3_B) {
+    if (!tc_mode_b(mode)) {
         P->nlat = n; P->nmat = b->nmat; P->nK = b->nK;
         long long roff = 0;
         for (int i = 0; i < n; i++) {
@@ -303,6 +307,10 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     size_t parts = 0;
     for (int i = 0; i < n; i++) parts += (size_t)(b->d[i] / 64) * b->d[i];
     double *part = cv.take<double>(parts);
+    float *gsc = cv.take<float>(n);
+    const int f16 = mode == OPB_FP16X3_B ? 1 : 0;
+    P->f16 = f16;
+    const float un2 = f16 ? 1.f / (F16S * F16S) : 1.f, un1 = f16 ? 1.f / F16S : 1.f;
     size_t eo = 0, po = 0;
     long long ro = 0;
     int rc_status = OPB_OK;
@@ -312,17 +320,20 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
         L.d = d; L.y0 = b->y0[i]; L.row_off = ro; L.dt = b->dt[i]; L.rate = b->rate[i]; L.period = b->period;
         L.E = E + eo; L.Pa = Pa + eo; L.V = V + (size_t)ro * P->ldk;
         L.GThi = Gh + (size_t)ro * P->ldk; L.GTlo = Gl + (size_t)ro * P->ldk;
+        L.gscale = gsc + i;
         double *pi = part + po;
-        sq[i] = opb::TcProblem{d, d, d, 0, L.E, L.E, pi, d, 1.f, 2.f, 0};
-        ch[i] = opb::TcProblem{d, d, d, 0, L.Pa, nullptr, pi, d, 1.f, 0.f, 0};
-        pr[i] = opb::TcProblem{d, P->ldk, d, 0, L.V, nullptr, nullptr, P->ldk, 1.f, 0.f, 0};
+        sq[i] = opb::TcProblem{d, d, d, 0, L.E, L.E, pi, d, un2, 2.f, 0};
+        ch[i] = opb::TcProblem{d, d, d, 0, L.Pa, nullptr, pi, d, un2, 0.f, 0};
+        pr[i] = opb::TcProblem{d, P->ldk, d, 0, L.V, nullptr, nullptr, P->ldk, un1, 0.f, 0};
         rs[i] = opb::RenormProblem{d, 0, L.E, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo};
         rc[i] = opb::RenormProblem{d, 0, L.Pa, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo};
-        rc_status = opb::tc_make_maps(&m128[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 128);
+        rc_status = opb::tc_make_maps(&m128[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 128, f16);
         if (rc_status == OPB_OK)
-            rc_status = opb::tc_make_maps(&m64[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 64);
+            rc_status =
+                opb::tc_make_maps(&m64[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 64, f16);
         if (rc_status == OPB_OK)
-            rc_status = opb::tc_make_maps(&mp[4 * (size_t)i], Ah + eo, Al + eo, d, d, L.GThi, L.GTlo, P->ldk, d, d, 64);
+            rc_status =
+                opb::tc_make_maps(&mp[4 * (size_t)i], Ah + eo, Al + eo, d, d, L.GThi, L.GTlo, P->ldk, d, d, 64, f16);
         eo += (size_t)d * d;
         po += (size_t)(d / 64) * d;
         ro += d;
@@ -375,7 +386,7 @@ namespace {
 int level_gemm(opb_batch_plan *P, int cfg, int level, cudaStream_t s) {
     const ListRef &l = P->gemm_level[cfg][level];
     const int bi = CFG_BN[cfg] == 128 ? 0 : 1;
-    return opb::launch_tc_gemm_batched(CFG_BN[cfg], P->maps_sq[bi], P->sq, P->work + l.off, l.n, P->grid, s);
+    return opb::launch_tc_gemm_batched(CFG_BN[cfg], P->maps_sq[bi], P->sq, P->work + l.off, l.n, P->grid, s, P->f16);
 }
 
 }  // namespace
@@ -392,31 +403,33 @@ OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
         r = (expr);                               \
         if (r != 0) return set_status(r);         \
     } while (0)
-    if (P->mode != OPB_BF16X3_B) {
+    if (!tc_mode_b(P->mode)) {
         for (int i = 0; i < P->nlat; i++)
             BT(opb_lattice_solve(reinterpret_cast<const opb_lattice_desc *>(&P->fp32_desc[i]), P->mode, P->fp32_ws[0],
                                  P->fp32_ws_bytes, quotes + (size_t)i * P->nmat * P->nK, nullptr));
         return set_status(OPB_OK);
     }
     const int cfg = P->cfg, bn = CFG_BN[cfg], pdiv = bn < 128 ? bn : 128;
+    const float ss = P->f16 ? F16S : 0.f;
     BT((int)cudaMemsetAsync(P->E_base, 0, P->E_bytes, s));
     BT(opb::launch_ek_batched(P->lats, P->nlat, P->total_rows, P->ell_width, P->cols, P->vals, s));
-    BT(opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_init.off, P->rn_init.n, 0, s));
+    BT(opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_init.off, P->rn_init.n, 0, s, ss));
     for (int lv = 0; lv < P->maxn; lv++) {
         BT(level_gemm(P, cfg, lv, s));
-        BT(opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_level[lv].off, P->rn_level[lv].n, pdiv, s));
+        BT(opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_level[lv].off, P->rn_level[lv].n, pdiv, s, ss));
     }
-    BT(opb::launch_payoff_batched(P->lats, P->nlat, P->total_rows, P->nK, P->ldk, P->x, P->strikes, s));
+    BT(opb::launch_payoff_batched(P->lats, P->nlat, P->total_rows, P->nK, P->ldk, P->x, P->strikes, s, P->f16));
     const int bi = bn == 128 ? 0 : 1;
     for (int m = 1; m <= P->nmat; m++) {
         if (m > 1) {
             const ListRef &l = P->gemm_chain[cfg];
-            BT(opb::launch_tc_gemm_batched(bn, P->maps_sq[bi], P->chain, P->work + l.off, l.n, P->grid, s));
-            BT(opb::launch_renorm_batched(P->rn_chain, P->work + P->rn_chain_list.off, P->rn_chain_list.n, pdiv, s));
+            BT(opb::launch_tc_gemm_batched(bn, P->maps_sq[bi], P->chain, P->work + l.off, l.n, P->grid, s, P->f16));
+            BT(opb::launch_renorm_batched(P->rn_chain, P->work + P->rn_chain_list.off, P->rn_chain_list.n, pdiv, s,
+                                          ss));
         }
         BT(opb::launch_tc_gemm_batched(64, P->maps_price, P->price, P->work + P->gemm_price.off, P->gemm_price.n,
-                                       P->grid, s));
-        BT(opb::launch_quotes_batched(P->lats, P->nlat, P->nK, P->ldk, m, P->nmat, quotes, s));
+                                       P->grid, s, P->f16));
+        BT(opb::launch_quotes_batched(P->lats, P->nlat, P->nK, P->ldk, m, P->nmat, quotes, s, P->f16));
     }
 #undef BT
     return set_status(OPB_OK);
@@ -427,7 +440,7 @@ OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
 // Blocking; leaves the plan's buffers in an arbitrary state (run execute afterwards).
 OPB_API int opb_batch_autotune(opb_batch_plan *P, int reps, float *ms_out, int *best_cfg) {
     OPB_REQUIRE(P, OPB_E_NULL);
-    if (P->mode != OPB_BF16X3_B) {
+    if (!tc_mode_b(P->mode)) {
         if (best_cfg) *best_cfg = 0;
         return set_status(OPB_OK);
     }
@@ -464,6 +477,6 @@ OPB_API int opb_batch_autotune(opb_batch_plan *P, int reps, float *ms_out, int *
 // Launch counts of one execute() (library kernels and memsets), for accounting.
 OPB_API int opb_batch_launches(const opb_batch_plan *P) {
     if (!P) return 0;
-    if (P->mode != OPB_BF16X3_B) return -1;
-    return 3 + 2 * P->maxn + 1 + 2 * P->nmat + 2 * (P->nmat - 1);
+    if (!tc_mode_b(P->mode)) return -1;
+    return 3 + 2 * P->maxn + 1 + (P->f16 ? 1 : 0) + 2 * P->nmat + 2 * (P->nmat - 1);
 }

@@ -101,9 +101,11 @@ __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
     return d;
 }
 
-// kind::f16 instruction descriptor: D = F32, A = B = BF16, both K-major, N, M = 128.
-__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+// kind::f16 instruction descriptor: D = F32, A = B = BF16 (format 1) or F16 (format 0),
+// both K-major, N, M = 128.
+__host__ __device__ constexpr uint32_t umma_idesc_16(int n, bool f16) {
+    return (1u << 4) | ((f16 ? 0u : 1u) << 7) | ((f16 ? 0u : 1u) << 10) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(TC_BM >> 4) << 24);
 }
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -173,7 +175,7 @@ struct TcBatch {
 // into FP32 register sums (round to nearest) while the MMA warp fills the other
 // accumulator.  The tensor cores' truncating accumulation thus spans only 12*CHUNK MMA
 // instructions, and an item's final store overlaps the next item's MMAs.
-template <int BN, int STAGES, bool BATCHED>
+template <int BN, int STAGES, bool BATCHED, bool F16>
 __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
               const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p,
@@ -287,7 +289,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
     } else if (warp == EPI + 1) {
         if (lane == 0) {
             // ---------------- MMA issuer
-            const uint32_t idesc = umma_idesc_bf16(BN);
+            const uint32_t idesc = umma_idesc_16(BN, F16);
             long kbg = 0, g = 0;  // K-blocks consumed, chunks issued
             bool ok = true;
             for (int t = blockIdx.x; t < nitems && ok; t += gridDim.x) {
@@ -431,14 +433,15 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 }
 
 // rows x K bf16 row-major matrix (leading dimension ld elements), box = box_rows x 64.
-static int make_map(CUtensorMap *m, const void *ptr, long long rows, long long K, long long ld, int box_rows) {
+static int make_map(CUtensorMap *m, const void *ptr, long long rows, long long K, long long ld, int box_rows,
+                    int f16 = 0) {
     auto enc = get_encode();
     if (!enc) return OPB_E_UNSUPPORTED;
     cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
     cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
     cuuint32_t es[2] = {1, 1};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, es,
+    CUresult r = enc(m, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, es,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? OPB_OK : OPB_E_ARG;
@@ -470,14 +473,14 @@ int tc_gemm_check(const TcGemmArgs &a) {
     return OPB_OK;
 }
 
-template <int BN, int STAGES, bool BATCHED>
+template <int BN, int STAGES, bool BATCHED, bool F16>
 static int set_smem_attr() {
     using Cfg = TcCfg<BN, STAGES>;
     static bool attr_set[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              Cfg::SMEM);
         if (e != cudaSuccess) return (int)e;
         attr_set[dev] = true;
@@ -485,56 +488,59 @@ static int set_smem_attr() {
     return 0;
 }
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, bool F16>
 static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
     using Cfg = TcCfg<BN, STAGES>;
-    int e0 = set_smem_attr<BN, STAGES, false>();
+    int e0 = set_smem_attr<BN, STAGES, false, F16>();
     if (e0) return e0;
     CUtensorMap mAh, mAl, mBh, mBl;
     int r;
-    if ((r = make_map(&mAh, a.Ahi, a.M, a.K, a.lda, TC_BM)) != OPB_OK) return r;
-    if ((r = make_map(&mAl, a.Alo, a.M, a.K, a.lda, TC_BM)) != OPB_OK) return r;
-    if ((r = make_map(&mBh, a.Bhi, a.N, a.K, a.ldb, BN)) != OPB_OK) return r;
-    if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN)) != OPB_OK) return r;
+    if ((r = make_map(&mAh, a.Ahi, a.M, a.K, a.lda, TC_BM, F16)) != OPB_OK) return r;
+    if ((r = make_map(&mAl, a.Alo, a.M, a.K, a.lda, TC_BM, F16)) != OPB_OK) return r;
+    if ((r = make_map(&mBh, a.Bhi, a.N, a.K, a.ldb, BN, F16)) != OPB_OK) return r;
+    if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN, F16)) != OPB_OK) return r;
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
     const int ntiles = (a.M / TC_BM) * (a.N / BN);
     const int grid = ntiles < num_sms() ? ntiles : num_sms();
     TcBatch none{nullptr, nullptr, nullptr, 0};
-    k_tc_gemm<BN, STAGES, false><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl, p, none);
+    k_tc_gemm<BN, STAGES, false, F16><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl, p, none);
     return (int)cudaGetLastError();
 }
 
 int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo, long long M, long long lda,
-                 const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long N, long long ldb, long long K, int bn) {
+                 const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long N, long long ldb, long long K, int bn,
+                 int f16) {
     int r;
-    if ((r = make_map(&out4[0], Ahi, M, K, lda, TC_BM)) != OPB_OK) return r;
-    if ((r = make_map(&out4[1], Alo, M, K, lda, TC_BM)) != OPB_OK) return r;
-    if ((r = make_map(&out4[2], Bhi, N, K, ldb, bn)) != OPB_OK) return r;
-    if ((r = make_map(&out4[3], Blo, N, K, ldb, bn)) != OPB_OK) return r;
+    if ((r = make_map(&out4[0], Ahi, M, K, lda, TC_BM, f16)) != OPB_OK) return r;
+    if ((r = make_map(&out4[1], Alo, M, K, lda, TC_BM, f16)) != OPB_OK) return r;
+    if ((r = make_map(&out4[2], Bhi, N, K, ldb, bn, f16)) != OPB_OK) return r;
+    if ((r = make_map(&out4[3], Blo, N, K, ldb, bn, f16)) != OPB_OK) return r;
     return OPB_OK;
 }
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, bool F16>
 static int launch_batched_impl(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
                                int grid, cudaStream_t s) {
     using Cfg = TcCfg<BN, STAGES>;
-    int e0 = set_smem_attr<BN, STAGES, true>();
+    int e0 = set_smem_attr<BN, STAGES, true, F16>();
     if (e0) return e0;
     CUtensorMap dummy;
     std::memset(&dummy, 0, sizeof(dummy));
     TcParams p{};
     TcBatch bt{maps, probs, work, nwork};
-    k_tc_gemm<BN, STAGES, true><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(dummy, dummy, dummy, dummy, p, bt);
+    k_tc_gemm<BN, STAGES, true, F16><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(dummy, dummy, dummy, dummy, p, bt);
     return (int)cudaGetLastError();
 }
 
 int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                           int grid, cudaStream_t s) {
+                           int grid, cudaStream_t s, int f16) {
     if (nwork <= 0) return OPB_OK;
     if (grid <= 0 || grid > nwork) grid = nwork < num_sms() ? nwork : num_sms();
-    switch (bn) {
-        case 128: return launch_batched_impl<128, 3>(maps, probs, work, nwork, grid, s);
-        case 64: return launch_batched_impl<64, 4>(maps, probs, work, nwork, grid, s);
+    switch (bn * 2 + (f16 ? 1 : 0)) {
+        case 256: return launch_batched_impl<128, 3, false>(maps, probs, work, nwork, grid, s);
+        case 257: return launch_batched_impl<128, 3, true>(maps, probs, work, nwork, grid, s);
+        case 128: return launch_batched_impl<64, 4, false>(maps, probs, work, nwork, grid, s);
+        case 129: return launch_batched_impl<64, 4, true>(maps, probs, work, nwork, grid, s);
         default: return OPB_E_UNSUPPORTED;
     }
 }
@@ -542,10 +548,13 @@ int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *pro
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
     int c = tc_gemm_check(a);
     if (c != OPB_OK) return c;
-    switch (tc_gemm_tile_n(a.N)) {
-        case 256: return launch_tc_impl<256, 2>(a, s);
-        case 128: return launch_tc_impl<128, 3>(a, s);
-        case 64: return launch_tc_impl<64, 4>(a, s);
+    switch (tc_gemm_tile_n(a.N) * 2 + (a.f16 ? 1 : 0)) {
+        case 512: return launch_tc_impl<256, 2, false>(a, s);
+        case 513: return launch_tc_impl<256, 2, true>(a, s);
+        case 256: return launch_tc_impl<128, 3, false>(a, s);
+        case 257: return launch_tc_impl<128, 3, true>(a, s);
+        case 128: return launch_tc_impl<64, 4, false>(a, s);
+        case 129: return launch_tc_impl<64, 4, true>(a, s);
         default: return OPB_E_UNSUPPORTED;
     }
 }
@@ -561,6 +570,20 @@ OPB_API int opb_gemm_bf16x3(int M, int N, int K, const __nv_bfloat16 *Ahi, const
     TcGemmArgs a{};
     a.M = M; a.N = N; a.K = K; a.Ahi = Ahi; a.Alo = Alo; a.Bhi = Bhi; a.Blo = Blo; a.lda = lda; a.ldb = ldb;
     a.C = C; a.ldc = ldc; a.Cin = Cin; a.alpha = alpha; a.beta = beta; a.rowsum = rowsum;
+    return set_status(launch_tc_gemm(a, stream()));
+}
+
+// The same product with FP16 parts (e.g. of a power-of-two-scaled split; undo the scales
+// through alpha).
+OPB_API int opb_gemm_f16x3(int M, int N, int K, const uint16_t *Ahi, const uint16_t *Alo, long long lda,
+                           const uint16_t *Bhi, const uint16_t *Blo, long long ldb, float alpha, const float *Cin,
+                           float beta, float *C, long long ldc, double *rowsum) {
+    TcGemmArgs a{};
+    a.M = M; a.N = N; a.K = K;
+    a.Ahi = reinterpret_cast<const __nv_bfloat16 *>(Ahi); a.Alo = reinterpret_cast<const __nv_bfloat16 *>(Alo);
+    a.Bhi = reinterpret_cast<const __nv_bfloat16 *>(Bhi); a.Blo = reinterpret_cast<const __nv_bfloat16 *>(Blo);
+    a.lda = lda; a.ldb = ldb; a.C = C; a.ldc = ldc; a.Cin = Cin; a.alpha = alpha; a.beta = beta; a.rowsum = rowsum;
+    a.f16 = 1;
     return set_status(launch_tc_gemm(a, stream()));
 }
 

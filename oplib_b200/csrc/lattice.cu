@@ -11,6 +11,8 @@
 //   OPB_FP32_PLAIN   : FP32 SIMT squaring and chaining exactly as the reference's FP32
 //                      device path (no renormalisation).
 //   OPB_FP32_RENORM  : the same with FP64 row renormalisation after every product.
+//   OPB_FP16X3       : as OPB_BF16X3 with FP16 parts of 2^15-scaled values (11 + 11
+//                      significant bits per split instead of 8 + 8; same cost).
 //   OPB_BF16X3       : split-BF16 tensor-core products.  Squaring runs on E = U - I
 //                      (E' = 2E + E.E, so the O(dt*L) information in U0 is not lost to
 //                      BF16 rounding of entries near 1), FP64 row renormalisation after
@@ -23,7 +25,12 @@
 #include "common.cuh"
 #include "lattice.h"
 
-enum { OPB_FP32_PLAIN = 0, OPB_FP32_RENORM = 1, OPB_BF16X3 = 2 };
+enum { OPB_FP32_PLAIN = 0, OPB_FP32_RENORM = 1, OPB_BF16X3 = 2, OPB_FP16X3 = 3 };
+
+// FP16 parts: E-form and P-form entries are bounded by 1 in magnitude, so a 2^15 scale
+// keeps them below the FP16 maximum with 11 + 11 significant bits.
+constexpr float F16_SCALE = 32768.f;
+inline bool tc_mode(int mode) { return mode == OPB_BF16X3 || mode == OPB_FP16X3; }
 
 struct opb_lattice_desc {
     int d;                     // states
@@ -59,12 +66,12 @@ struct Ws {
 };
 
 struct Bufs {
-    float *X, *Pa, *Pb, *G, *V;
+    float *X, *Pa, *Pb, *G, *V, *gscale;
     __nv_bfloat16 *Ahi, *Alo, *Bhi, *Blo, *GThi, *GTlo;
     double *part;
 };
 
-inline int padded_nk(int nK, int mode) { return mode == OPB_BF16X3 ? (nK + 63) / 64 * 64 : nK; }
+inline int padded_nk(int nK, int mode) { return tc_mode(mode) ? (nK + 63) / 64 * 64 : nK; }
 
 Bufs carve(Ws &w, int d, int nK, int mode) {
     Bufs b{};
@@ -72,9 +79,10 @@ Bufs carve(Ws &w, int d, int nK, int mode) {
     nK = padded_nk(nK, mode);
     b.X = w.take<float>(dd);
     b.Pa = w.take<float>(dd);
-    if (mode != OPB_BF16X3) b.Pb = w.take<float>(dd);
+    if (!tc_mode(mode)) b.Pb = w.take<float>(dd);
     b.V = w.take<float>((size_t)d * nK);
-    if (mode == OPB_BF16X3) {
+    b.gscale = w.take<float>(64);
+    if (tc_mode(mode)) {
         b.Ahi = w.take<__nv_bfloat16>(dd);
         b.Alo = w.take<__nv_bfloat16>(dd);
         b.Bhi = w.take<__nv_bfloat16>(dd);
@@ -164,46 +172,55 @@ int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s) {
     return 0;
 }
 
-int solve_bf16x3(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, cudaStream_t s, float *P_out) {
+int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, cudaStream_t s, float *P_out,
+             bool f16) {
     const int d = L.d, nK = L.nK;
     const int np = opb::tc_gemm_nparts(d);
+    const float ss = f16 ? F16_SCALE : 0.f;                    // split scale of E / P parts
+    const float unscale = f16 ? 1.f / (F16_SCALE * F16_SCALE) : 1.f;
     // E0 = dt*L in FP32 (FP64 arithmetic), then its splits
     if (L.ell_width > 0) LT(opb::launch_ek_ell(d, L.ell_width, L.gen_cols, L.gen_vals, L.dt, 1, b.X, s));
     else LT(opb::launch_ek_dense(d, L.gen_dense, L.dt, 1, b.X, s));
-    LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s));
+    LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s, ss));
     opb::TcGemmArgs g{};
-    g.M = d; g.N = d; g.K = d; g.lda = d; g.ldb = d; g.ldc = d;
+    g.M = d; g.N = d; g.K = d; g.lda = d; g.ldb = d; g.ldc = d; g.f16 = f16 ? 1 : 0;
     g.Ahi = b.Ahi; g.Alo = b.Alo; g.Bhi = b.Bhi; g.Blo = b.Blo;
     for (int r = 0; r < L.niter; r++) {
         // D = 2E + E.E in place of E, with FP64 row-sum partials
-        g.C = b.X; g.Cin = b.X; g.alpha = 1.f; g.beta = 2.f; g.rowsum = b.part;
+        g.C = b.X; g.Cin = b.X; g.alpha = unscale; g.beta = 2.f; g.rowsum = b.part;
         LT(tc_gemm_ksplit(g, s));
         // the last level emits P1 = I + E and its splits (row-major: A of the first chain and
         // of pricing; transposed: B of every chain)
-        if (r + 1 == L.niter) LT(opb::launch_renorm_to_p(d, b.X, b.part, np, b.Ahi, b.Alo, b.Bhi, b.Blo, s));
-        else LT(opb::launch_renorm(d, b.X, b.part, np, 1, b.Ahi, b.Alo, b.Bhi, b.Blo, s));
+        if (r + 1 == L.niter) LT(opb::launch_renorm_to_p(d, b.X, b.part, np, b.Ahi, b.Alo, b.Bhi, b.Blo, s, ss));
+        else LT(opb::launch_renorm(d, b.X, b.part, np, 1, b.Ahi, b.Alo, b.Bhi, b.Blo, s, ss));
     }
     if (L.niter == 0) {
         LT(opb::launch_add_identity(d, b.X, s));
-        LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s));
+        LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s, ss));
     }
     if (P_out) return (int)cudaMemcpyAsync(P_out, b.X, sizeof(float) * (size_t)d * d, cudaMemcpyDeviceToDevice, s);
     const int nKp = padded_nk(nK, OPB_BF16X3);
-    LT(opb::launch_payoff(d, nK, nKp, L.x, L.strikes, nullptr, b.GThi, b.GTlo, s));
+    const float *gs = nullptr;
+    if (f16) {
+        LT(opb::launch_payoff_scale(d, L.x, nK, L.strikes, b.gscale, s));
+        gs = b.gscale;
+    }
+    LT(opb::launch_payoff(d, nK, nKp, L.x, L.strikes, nullptr, b.GThi, b.GTlo, s, gs));
     opb::TcGemmArgs pg{};
-    pg.M = d; pg.N = nKp; pg.K = d; pg.lda = d; pg.ldb = d; pg.ldc = nKp;
-    pg.Ahi = b.Ahi; pg.Alo = b.Alo; pg.Bhi = b.GThi; pg.Blo = b.GTlo; pg.C = b.V; pg.alpha = 1.f; pg.beta = 0.f;
+    pg.M = d; pg.N = nKp; pg.K = d; pg.lda = d; pg.ldb = d; pg.ldc = nKp; pg.f16 = g.f16;
+    pg.Ahi = b.Ahi; pg.Alo = b.Alo; pg.Bhi = b.GThi; pg.Blo = b.GTlo; pg.C = b.V; pg.beta = 0.f;
+    pg.alpha = f16 ? 1.f / F16_SCALE : 1.f;  // the payoff scale is undone in the FP64 discount
     for (int m = 1; m <= L.nmat; m++) {
         if (m > 1) {
             // P_m = P_{m-1} . P1 (A splits hold P_{m-1}), renormalise, split row-major into A
-            g.C = b.Pa; g.Cin = nullptr; g.alpha = 1.f; g.beta = 0.f; g.rowsum = b.part;
+            g.C = b.Pa; g.Cin = nullptr; g.alpha = unscale; g.beta = 0.f; g.rowsum = b.part;
             LT(tc_gemm_ksplit(g, s));
-            LT(opb::launch_renorm(d, b.Pa, b.part, np, 0, b.Ahi, b.Alo, nullptr, nullptr, s));
+            LT(opb::launch_renorm(d, b.Pa, b.part, np, 0, b.Ahi, b.Alo, nullptr, nullptr, s, ss));
         }
         LT(tc_gemm_ksplit(pg, s));
         const double disc = std::exp(-L.rate * L.period * m);
         LT(opb::launch_discount(d, nK, nKp, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d * nK : nullptr, L.y0,
-                                quotes + (size_t)(m - 1) * nK, s));
+                                quotes + (size_t)(m - 1) * nK, s, gs));
     }
     return 0;
 }
@@ -218,8 +235,8 @@ int check_desc(const opb_lattice_desc *L, int mode) {
     } else if (!L->gen_dense) {
         return OPB_E_NULL;
     }
-    if (mode < OPB_FP32_PLAIN || mode > OPB_BF16X3) return OPB_E_ARG;
-    if (mode == OPB_BF16X3) {
+    if (mode < OPB_FP32_PLAIN || mode > OPB_FP16X3) return OPB_E_ARG;
+    if (tc_mode(mode)) {
         if (L->d % 128 != 0) return OPB_E_UNSUPPORTED;
         if (opb::tc_gemm_tile_n(L->d) == 0) return OPB_E_UNSUPPORTED;
     }
@@ -258,8 +275,8 @@ OPB_API int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspa
     w.p += off;
     Bufs b = carve(w, L->d, L->nK, mode);
     cudaStream_t s = opb::stream();
-    int r = (mode == OPB_BF16X3) ? solve_bf16x3(*L, b, quotes, V_all, s, nullptr)
-                                 : solve_fp32(*L, mode, b, quotes, V_all, s, nullptr);
+    int r = tc_mode(mode) ? solve_tc(*L, b, quotes, V_all, s, nullptr, mode == OPB_FP16X3)
+                          : solve_fp32(*L, mode, b, quotes, V_all, s, nullptr);
     return opb::set_status(r);
 }
 
@@ -281,8 +298,8 @@ OPB_API int opb_lattice_kernel(const opb_lattice_desc *L, int mode, void *worksp
     w.p += off;
     Bufs b = carve(w, L2.d, L2.nK, mode);
     cudaStream_t s = opb::stream();
-    int r = (mode == OPB_BF16X3) ? solve_bf16x3(L2, b, nullptr, nullptr, s, P_out)
-                                 : solve_fp32(L2, mode, b, nullptr, nullptr, s, P_out);
+    int r = tc_mode(mode) ? solve_tc(L2, b, nullptr, nullptr, s, P_out, mode == OPB_FP16X3)
+                          : solve_fp32(L2, mode, b, nullptr, nullptr, s, P_out);
     return opb::set_status(r);
 }
 

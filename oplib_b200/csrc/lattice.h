@@ -17,15 +17,17 @@ int launch_ek_ell(int d, int w, const int *cols, const double *vals, double dt, 
                   cudaStream_t s);
 int launch_ek_dense(int d, const double *L, double dt, int eform, float *out, cudaStream_t s);
 int launch_split(int rows, int cols, const float *X, long long ld, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
-                 __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, long long ldt, cudaStream_t s);
+                 __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, long long ldt, cudaStream_t s, float sscale = 0.f);
 int launch_rowsum(int d, const float *X, double *partial, cudaStream_t s);
 int launch_renorm(int d, float *X, const double *partial, int nparts, int eform, __nv_bfloat16 *Ahi,
-                  __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s);
+                  __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale = 0.f);
 int launch_add_identity(int d, float *X, cudaStream_t s);
+// dscale (device, optional): FP16 payoff split scale from launch_payoff_scale
+int launch_payoff_scale(int d, const double *x, int nK, const double *K, float *out, cudaStream_t s);
 int launch_payoff(int d, int nK, int ldk, const double *x, const double *K, float *G, __nv_bfloat16 *GThi,
-                  __nv_bfloat16 *GTlo, cudaStream_t s);
+                  __nv_bfloat16 *GTlo, cudaStream_t s, const float *dscale = nullptr);
 int launch_discount(int d, int nK, int ldk, const float *V32, double disc, double *V64, int y0, double *quotes,
-                    cudaStream_t s);
+                    cudaStream_t s, const float *dscale = nullptr);
 
 // Batched lattice tables (device memory).
 struct BatchLattice {
@@ -36,6 +38,7 @@ struct BatchLattice {
     float *Pa;            // d x d FP32 chain product
     float *V;             // d x ldk FP32 pricing result
     __nv_bfloat16 *GThi, *GTlo;  // ldk x d payoff splits
+    float *gscale;        // device scalar: FP16 payoff split scale
 };
 struct RenormProblem {
     int d, pad;
@@ -44,15 +47,16 @@ struct RenormProblem {
     __nv_bfloat16 *Ahi, *Alo, *Bhi, *Blo;
 };
 int launch_renorm_to_p(int d, float *X, const double *partial, int nparts, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
-                       __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s);
+                       __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale = 0.f);
 // work items: problem << 16 | mode << 14 | tile_r << 7 | tile_c (64 x 64 tiles)
-int launch_renorm_batched(const RenormProblem *probs, const uint32_t *work, int nwork, int parts_div, cudaStream_t s);
+int launch_renorm_batched(const RenormProblem *probs, const uint32_t *work, int nwork, int parts_div, cudaStream_t s,
+                          float sscale = 0.f);
 int launch_ek_batched(const BatchLattice *lats, int nlat, long long total_rows, int w, const int *cols,
                       const double *vals, cudaStream_t s);
 int launch_payoff_batched(const BatchLattice *lats, int nlat, long long total_rows, int nK, int ldk, const double *x,
-                          const double *strikes, cudaStream_t s);
+                          const double *strikes, cudaStream_t s, int f16 = 0);
 int launch_quotes_batched(const BatchLattice *lats, int nlat, int nK, int ldk, int m, int nmat, double *quotes,
-                          cudaStream_t s);
+                          cudaStream_t s, int f16 = 0);
 
 // gemm_tc.cu -- split-BF16 tensor-core GEMM.
 //   C[M,N] = alpha * (Ahi.Bhi^T + Ahi.Blo^T + Alo.Bhi^T) + beta * Cin[M,N]
@@ -68,6 +72,7 @@ struct TcGemmArgs {
     const float *Cin;     // may alias C
     float alpha, beta;
     double *rowsum;       // optional
+    int f16;              // 1: FP16 parts (kind::f16 with F16 inputs), 0: BF16 parts
 };
 int tc_gemm_tile_n(int N);                    // tile width chosen for N (0 if unsupported)
 int tc_gemm_check(const TcGemmArgs &a);       // argument/alignment check, OPB_* code
@@ -85,10 +90,11 @@ struct TcProblem {
     long long pad2;
 };
 int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo, long long M, long long lda,
-                 const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long N, long long ldb, long long K, int bn);
+                 const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long N, long long ldb, long long K, int bn,
+                 int f16 = 0);
 // work: packed (problem << 16 | m-tile << 8 | n-tile); bn in {64, 128}
 int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                           int grid, cudaStream_t s);
+                           int grid, cudaStream_t s, int f16 = 0);
 
 // sck.cu
 int launch_sck_rm(int d, int nrows, const float *P, float *C, cudaStream_t s);

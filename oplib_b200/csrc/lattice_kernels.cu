@@ -17,6 +17,7 @@
 //   payoff / discount : call payoffs G[z,k] = (x_z - K_k)^+ and the FP64 discounting of
 //              the backward-induction result.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "common.cuh"
 #include "lattice.h"
@@ -53,16 +54,29 @@ __global__ void k_ek_dense(int d, const double *__restrict__ L, double dt, int e
     }
 }
 
-__device__ __forceinline__ void split2(float f, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
-    hi = __float2bfloat16_rn(f);
-    lo = __float2bfloat16_rn(f - __bfloat162float(hi));  // exact difference in FP32
+// Two-part split of an FP32 value into 16-bit storage.  sscale == 0: BF16 parts,
+// hi = bf16(f), lo = bf16(f - hi).  sscale > 0 (a power of two): FP16 parts of f*sscale,
+// hi = fp16(f*s), lo = fp16(f*s - hi) -- 11 + 11 significant bits instead of 8 + 8; the
+// GEMM removes the scale through alpha.  The differences are exact in FP32.
+__device__ __forceinline__ void split2(float f, __nv_bfloat16 &hi, __nv_bfloat16 &lo, float sscale = 0.f) {
+    if (sscale == 0.f) {
+        hi = __float2bfloat16_rn(f);
+        lo = __float2bfloat16_rn(f - __bfloat162float(hi));
+    } else {
+        const float fs = f * sscale;
+        const __half h = __float2half_rn(fs);
+        const __half l = __float2half_rn(fs - __half2float(h));
+        hi = __ushort_as_bfloat16(__half_as_ushort(h));
+        lo = __ushort_as_bfloat16(__half_as_ushort(l));
+    }
 }
 
 // 32x32 tiles, 256 threads.  X is (rows x cols) row-major with leading dimension ld.
 // Writes hi/lo of X (row-major, ld) and of X^T (cols x rows, leading dimension ldt).
 __global__ void k_split_tr(int rows, int cols, const float *__restrict__ X, long long ld,
                            __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
-                           __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo, long long ldt) {
+                           __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo, long long ldt,
+                           float sscale) {
     __shared__ __nv_bfloat16 th[32][34], tl[32][34];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
@@ -71,7 +85,7 @@ __global__ void k_split_tr(int rows, int cols, const float *__restrict__ X, long
         int r = r0 + i, c = c0 + tx;
         __nv_bfloat16 h = __float2bfloat16_rn(0.f), l = h;
         if (r < rows && c < cols) {
-            split2(X[(long long)r * ld + c], h, l);
+            split2(X[(long long)r * ld + c], h, l, sscale);
             if (Ahi) {
                 Ahi[(long long)r * ld + c] = h;
                 Alo[(long long)r * ld + c] = l;
@@ -116,7 +130,7 @@ __global__ void k_rowsum(int d, const float *__restrict__ X, double *__restrict_
 // (row-major and transposed).
 __global__ void k_renorm(int d, float *__restrict__ X, const double *__restrict__ partial, int nparts, int eform,
                          __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
-                         __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo) {
+                         __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo, float sscale) {
     __shared__ double s_sum[32], s_inv[32];
     __shared__ __nv_bfloat16 th[32][34], tl[32][34];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -142,7 +156,7 @@ __global__ void k_renorm(int d, float *__restrict__ X, const double *__restrict_
             float f = (float)(v * s_inv[i]);
             X[o] = f;
             if (Ahi) {
-                split2(f, h, l);
+                split2(f, h, l, sscale);
                 Ahi[o] = h;
                 Alo[o] = l;
             }
@@ -180,7 +194,7 @@ __device__ __forceinline__ void renorm64_tile(RenormSmem &sm, int d, float *__re
                                               const double *__restrict__ partial, int nparts, int mode,
                                               __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
                                               __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo,
-                                              int r0, int c0) {
+                                              int r0, int c0, float sscale) {
     const int tid = threadIdx.x;
     const bool eform = mode != 2;
     if (tid < 64) {
@@ -210,7 +224,7 @@ __device__ __forceinline__ void renorm64_tile(RenormSmem &sm, int d, float *__re
             x *= inv;
             if (mode == 1 && diag) x += 1.0;
             f[j] = (float)x;
-            split2(f[j], h[j], l[j]);
+            split2(f[j], h[j], l[j], sscale);
             sm.th[lr][lc + j] = h[j];
             sm.tl[lr][lc + j] = l[j];
         }
@@ -236,22 +250,23 @@ __device__ __forceinline__ void renorm64_tile(RenormSmem &sm, int d, float *__re
 __global__ void __launch_bounds__(256) k_renorm64(int d, float *__restrict__ X, const double *__restrict__ partial,
                                                   int nparts, int mode, __nv_bfloat16 *__restrict__ Ahi,
                                                   __nv_bfloat16 *__restrict__ Alo, __nv_bfloat16 *__restrict__ Bhi,
-                                                  __nv_bfloat16 *__restrict__ Blo) {
+                                                  __nv_bfloat16 *__restrict__ Blo, float sscale) {
     __shared__ RenormSmem sm;
-    renorm64_tile(sm, d, X, partial, nparts, mode, Ahi, Alo, Bhi, Blo, blockIdx.y * 64, blockIdx.x * 64);
+    renorm64_tile(sm, d, X, partial, nparts, mode, Ahi, Alo, Bhi, Blo, blockIdx.y * 64, blockIdx.x * 64, sscale);
 }
 
 // Batched: one block per work item (problem << 16 | mode << 14 | tile_r << 7 | tile_c);
 // nparts of problem i is d_i / parts_div (0 when parts_div == 0: pure split).
 __global__ void __launch_bounds__(256) k_renorm64_batched(const RenormProblem *__restrict__ probs,
-                                                          const uint32_t *__restrict__ work, int parts_div) {
+                                                          const uint32_t *__restrict__ work, int parts_div,
+                                                          float sscale) {
     __shared__ RenormSmem sm;
     const uint32_t w = work[blockIdx.x];
     const RenormProblem &pr = probs[w >> 16];
     const int mode = (int)((w >> 14) & 3u);
     const int nparts = parts_div > 0 ? pr.d / parts_div : 0;
     renorm64_tile(sm, pr.d, pr.X, pr.partial, nparts, mode, pr.Ahi, pr.Alo, mode == 2 ? nullptr : pr.Bhi,
-                  mode == 2 ? nullptr : pr.Blo, (int)((w >> 7) & 127u) * 64, (int)(w & 127u) * 64);
+                  mode == 2 ? nullptr : pr.Blo, (int)((w >> 7) & 127u) * 64, (int)(w & 127u) * 64, sscale);
 }
 
 // Batched ELL scatter into zeroed dense E-form matrices: thread per global ELL slot
@@ -276,7 +291,7 @@ __global__ void k_ek_scatter_batched(const BatchLattice *__restrict__ lats, int 
 // Batched payoff splits: G^T[k][z] = (x_z - K_k)^+ for strikes k < nK of lattice i and 0
 // for the padding columns nK..ldk-1.
 __global__ void k_payoff_batched(const BatchLattice *__restrict__ lats, int nlat, long long total_rows, int nK, int ldk,
-                                 const double *__restrict__ x, const double *__restrict__ strikes) {
+                                 const double *__restrict__ x, const double *__restrict__ strikes, int f16) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= total_rows * ldk) return;
     const long long grow = t / ldk;
@@ -291,19 +306,20 @@ __global__ void k_payoff_batched(const BatchLattice *__restrict__ lats, int nlat
     double g = k < nK ? x[grow] - strikes[(long long)lo * nK + k] : 0.0;
     float f = (float)(g > 0.0 ? g : 0.0);
     __nv_bfloat16 h, l;
-    split2(f, h, l);
+    split2(f, h, l, f16 ? L.gscale[0] : 0.f);
     L.GThi[(long long)k * L.d + z] = h;
     L.GTlo[(long long)k * L.d + z] = l;
 }
 
 // quotes[(i*nmat + m-1)*nK + k] = exp(-r_i T_m) * V_i[y0_i, k]
 __global__ void k_quotes_batched(const BatchLattice *__restrict__ lats, int nlat, int nK, int ldk, int m, int nmat,
-                                 double *__restrict__ quotes) {
+                                 double *__restrict__ quotes, int f16) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nlat * nK) return;
     int i = t / nK, k = t - i * nK;
     const BatchLattice &L = lats[i];
-    const double disc = exp(-L.rate * L.period * m);
+    double disc = exp(-L.rate * L.period * m);
+    if (f16) disc /= (double)L.gscale[0];
     quotes[((long long)i * nmat + (m - 1)) * nK + k] = disc * (double)L.V[(long long)L.y0 * ldk + k];
 }
 
@@ -320,7 +336,9 @@ __global__ void k_add_identity(int d, float *__restrict__ X) {
 // G^T hi/lo (nK x d) for the tensor-core pricing GEMM.
 // Strike columns nK..ldk-1 (padding to the tensor-core tile width) get zero payoffs.
 __global__ void k_payoff(int d, int nK, int ldk, const double *__restrict__ x, const double *__restrict__ K,
-                         float *__restrict__ G, __nv_bfloat16 *__restrict__ GThi, __nv_bfloat16 *__restrict__ GTlo) {
+                         float *__restrict__ G, __nv_bfloat16 *__restrict__ GThi, __nv_bfloat16 *__restrict__ GTlo,
+                         const float *__restrict__ dscale) {
+    const float sscale = dscale ? *dscale : 0.f;
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)d * ldk) return;
     int z = (int)(t / ldk), k = (int)(t - (long long)z * ldk);
@@ -329,18 +347,20 @@ __global__ void k_payoff(int d, int nK, int ldk, const double *__restrict__ x, c
     if (G) G[t] = f;
     if (GThi) {
         __nv_bfloat16 h, l;
-        split2(f, h, l);
+        split2(f, h, l, sscale);
         GThi[(long long)k * d + z] = h;
         GTlo[(long long)k * d + z] = l;
     }
 }
 
-// V64[y, k] = disc * V32[y, k] (V32 leading dimension ldk >= nK); quotes[k] = V64[y0, k].
+// V64[y, k] = disc * V32[y, k] / gscale (V32 leading dimension ldk >= nK; gscale = the
+// payoff split scale, 1 without one); quotes[k] = V64[y0, k].
 __global__ void k_discount(int d, int nK, int ldk, const float *__restrict__ V32, double disc,
-                           double *__restrict__ V64, int y0, double *__restrict__ quotes) {
+                           double *__restrict__ V64, int y0, double *__restrict__ quotes, const float *__restrict__ dscale) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)d * nK) return;
     int y = (int)(t / nK), k = (int)(t - (long long)y * nK);
+    if (dscale) disc /= (double)*dscale;
     double v = disc * (double)V32[(long long)y * ldk + k];
     if (V64) V64[t] = v;
     if (quotes && y == y0) quotes[k] = v;
@@ -369,9 +389,9 @@ int launch_ek_dense(int d, const double *L, double dt, int eform, float *out, cu
 }
 
 int launch_split(int rows, int cols, const float *X, long long ld, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
-                 __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, long long ldt, cudaStream_t s) {
+                 __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, long long ldt, cudaStream_t s, float sscale) {
     dim3 g((cols + 31) / 32, (rows + 31) / 32);
-    k_split_tr<<<g, 256, 0, s>>>(rows, cols, X, ld, Ahi, Alo, Bhi, Blo, ldt);
+    k_split_tr<<<g, 256, 0, s>>>(rows, cols, X, ld, Ahi, Alo, Bhi, Blo, ldt, sscale);
     return (int)cudaGetLastError();
 }
 
@@ -381,29 +401,30 @@ int launch_rowsum(int d, const float *X, double *partial, cudaStream_t s) {
 }
 
 int launch_renorm(int d, float *X, const double *partial, int nparts, int eform, __nv_bfloat16 *Ahi,
-                  __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s) {
+                  __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale) {
     if (d % 64 == 0 && (Ahi != nullptr) == (Alo != nullptr)) {
         dim3 g(d / 64, d / 64);
-        k_renorm64<<<g, 256, 0, s>>>(d, X, partial, nparts, eform ? 0 : 2, Ahi, Alo, Bhi, Blo);
+        k_renorm64<<<g, 256, 0, s>>>(d, X, partial, nparts, eform ? 0 : 2, Ahi, Alo, Bhi, Blo, sscale);
         return (int)cudaGetLastError();
     }
     dim3 g((d + 31) / 32, (d + 31) / 32);
-    k_renorm<<<g, 256, 0, s>>>(d, X, partial, nparts, eform, Ahi, Alo, Bhi, Blo);
+    k_renorm<<<g, 256, 0, s>>>(d, X, partial, nparts, eform, Ahi, Alo, Bhi, Blo, sscale);
     return (int)cudaGetLastError();
 }
 
 // E-form renorm whose output is P = I + E_new with both splits (the last squaring level).
 int launch_renorm_to_p(int d, float *X, const double *partial, int nparts, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
-                       __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s) {
+                       __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale) {
     if (d % 64) return OPB_E_UNSUPPORTED;
     dim3 g(d / 64, d / 64);
-    k_renorm64<<<g, 256, 0, s>>>(d, X, partial, nparts, 1, Ahi, Alo, Bhi, Blo);
+    k_renorm64<<<g, 256, 0, s>>>(d, X, partial, nparts, 1, Ahi, Alo, Bhi, Blo, sscale);
     return (int)cudaGetLastError();
 }
 
-int launch_renorm_batched(const RenormProblem *probs, const uint32_t *work, int nwork, int parts_div, cudaStream_t s) {
+int launch_renorm_batched(const RenormProblem *probs, const uint32_t *work, int nwork, int parts_div, cudaStream_t s,
+                          float sscale) {
     if (nwork <= 0) return OPB_OK;
-    k_renorm64_batched<<<nwork, 256, 0, s>>>(probs, work, parts_div);
+    k_renorm64_batched<<<nwork, 256, 0, s>>>(probs, work, parts_div, sscale);
     return (int)cudaGetLastError();
 }
 
@@ -415,18 +436,45 @@ int launch_ek_batched(const BatchLattice *lats, int nlat, long long total_rows, 
     return (int)cudaGetLastError();
 }
 
+// Per-lattice FP16 payoff scales (one block per lattice) into BatchLattice.gscale.
+__global__ void k_payoff_scale_batched(const BatchLattice *__restrict__ lats, const double *__restrict__ x, int nK,
+                                       const double *__restrict__ strikes) {
+    const BatchLattice &L = lats[blockIdx.x];
+    __shared__ double sx[256], sk[256];
+    double mx = -1e300, mk = 1e300;
+    for (int i = threadIdx.x; i < L.d; i += blockDim.x) mx = fmax(mx, x[L.row_off + i]);
+    for (int i = threadIdx.x; i < nK; i += blockDim.x) mk = fmin(mk, strikes[(long long)blockIdx.x * nK + i]);
+    sx[threadIdx.x] = mx;
+    sk[threadIdx.x] = mk;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            sx[threadIdx.x] = fmax(sx[threadIdx.x], sx[threadIdx.x + o]);
+            sk[threadIdx.x] = fmin(sk[threadIdx.x], sk[threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double g = sx[0] - sk[0];
+        int e = g > 0.0 ? (int)floor(log2(16384.0 / g)) : 0;
+        e = e < 0 ? 0 : (e > 60 ? 60 : e);
+        L.gscale[0] = (float)ldexp(1.0, e);
+    }
+}
+
 int launch_payoff_batched(const BatchLattice *lats, int nlat, long long total_rows, int nK, int ldk, const double *x,
-                          const double *strikes, cudaStream_t s) {
+                          const double *strikes, cudaStream_t s, int f16) {
     long long n = total_rows * ldk;
     if (n <= 0) return OPB_OK;
-    k_payoff_batched<<<(int)((n + 255) / 256), 256, 0, s>>>(lats, nlat, total_rows, nK, ldk, x, strikes);
+    if (f16) k_payoff_scale_batched<<<nlat, 256, 0, s>>>(lats, x, nK, strikes);
+    k_payoff_batched<<<(int)((n + 255) / 256), 256, 0, s>>>(lats, nlat, total_rows, nK, ldk, x, strikes, f16);
     return (int)cudaGetLastError();
 }
 
 int launch_quotes_batched(const BatchLattice *lats, int nlat, int nK, int ldk, int m, int nmat, double *quotes,
-                          cudaStream_t s) {
+                          cudaStream_t s, int f16) {
     int n = nlat * nK;
-    k_quotes_batched<<<(n + 255) / 256, 256, 0, s>>>(lats, nlat, nK, ldk, m, nmat, quotes);
+    k_quotes_batched<<<(n + 255) / 256, 256, 0, s>>>(lats, nlat, nK, ldk, m, nmat, quotes, f16);
     return (int)cudaGetLastError();
 }
 
@@ -435,17 +483,48 @@ int launch_add_identity(int d, float *X, cudaStream_t s) {
     return (int)cudaGetLastError();
 }
 
+// Power-of-two scale for FP16 payoff parts: 2^floor(log2(16384 / max payoff)), at least 1,
+// with max payoff = max(x) - min(K) (one block).
+__global__ void k_payoff_scale(int d, const double *__restrict__ x, int nK, const double *__restrict__ K,
+                               float *__restrict__ out) {
+    __shared__ double sx[256], sk[256];
+    double mx = -1e300, mk = 1e300;
+    for (int i = threadIdx.x; i < d; i += blockDim.x) mx = fmax(mx, x[i]);
+    for (int i = threadIdx.x; i < nK; i += blockDim.x) mk = fmin(mk, K[i]);
+    sx[threadIdx.x] = mx;
+    sk[threadIdx.x] = mk;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            sx[threadIdx.x] = fmax(sx[threadIdx.x], sx[threadIdx.x + o]);
+            sk[threadIdx.x] = fmin(sk[threadIdx.x], sk[threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double g = sx[0] - sk[0];
+        int e = g > 0.0 ? (int)floor(log2(16384.0 / g)) : 0;
+        e = e < 0 ? 0 : (e > 60 ? 60 : e);
+        *out = (float)ldexp(1.0, e);
+    }
+}
+
+int launch_payoff_scale(int d, const double *x, int nK, const double *K, float *out, cudaStream_t s) {
+    k_payoff_scale<<<1, 256, 0, s>>>(d, x, nK, K, out);
+    return (int)cudaGetLastError();
+}
+
 int launch_payoff(int d, int nK, int ldk, const double *x, const double *K, float *G, __nv_bfloat16 *GThi,
-                  __nv_bfloat16 *GTlo, cudaStream_t s) {
+                  __nv_bfloat16 *GTlo, cudaStream_t s, const float *dscale) {
     long long n = (long long)d * ldk;
-    k_payoff<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, x, K, G, GThi, GTlo);
+    k_payoff<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, x, K, G, GThi, GTlo, dscale);
     return (int)cudaGetLastError();
 }
 
 int launch_discount(int d, int nK, int ldk, const float *V32, double disc, double *V64, int y0, double *quotes,
-                    cudaStream_t s) {
+                    cudaStream_t s, const float *dscale) {
     long long n = (long long)d * nK;
-    k_discount<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, V32, disc, V64, y0, quotes);
+    k_discount<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, V32, disc, V64, y0, quotes, dscale);
     return (int)cudaGetLastError();
 }
 

@@ -18,8 +18,9 @@ import torch
 from . import _lib
 from ._lib import LatticeDesc, call
 
-FP32_PLAIN, FP32_RENORM, BF16X3 = 0, 1, 2
-MODES = {"fp32_plain": FP32_PLAIN, "fp32": FP32_RENORM, "fp32_renorm": FP32_RENORM, "bf16x3": BF16X3}
+FP32_PLAIN, FP32_RENORM, BF16X3, FP16X3 = 0, 1, 2, 3
+MODES = {"fp32_plain": FP32_PLAIN, "fp32": FP32_RENORM, "fp32_renorm": FP32_RENORM, "bf16x3": BF16X3,
+         "fp16x3": FP16X3}
 
 
 def _ptr(t: torch.Tensor | None) -> int | None:
@@ -248,7 +249,7 @@ class Batch:
         bind_stream(dev)
         call("opb_batch_plan_create", C.byref(bd), self.mode, _ptr(self.ws), self.ws.numel(), C.byref(self.plan))
         self.tune_ms = None
-        if autotune and self.mode == BF16X3:
+        if autotune and self.mode in (BF16X3, FP16X3):
             ms = (C.c_float * 4)()
             best = C.c_int()
             call("opb_batch_autotune", self.plan, 2, ms, C.byref(best))

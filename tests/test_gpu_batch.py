@@ -99,3 +99,14 @@ def test_batch_rejects_bad_sizes(cuda):
     lats = [Lattice.local_vol(n=200, device=cuda)]
     with pytest.raises(Exception):
         Batch(lats, STRIKES, NMAT, PERIOD, DT0, mode="bf16x3")
+
+
+def test_batch_fp16x3_mode(cuda):
+    from oplib_b200.model import Batch, Lattice
+    lats = [Lattice.local_vol(device=cuda, **s) for s in SPECS]
+    b = Batch(lats, STRIKES, NMAT, PERIOD, DT0, mode="fp16x3")
+    q = b.execute().cpu().numpy()
+    for i, s in enumerate(SPECS):
+        err = np.abs(q[i] - _oracle_quotes(s)).max()
+        print(f"fp16x3 lattice {i}: {err:.2e}")
+        assert err <= 1e-5

@@ -62,6 +62,36 @@ def test_bf16x3_gemm_matches_fp64_of_split(cuda, M, N, K):
         assert np.allclose(parts[t], got[:, t * bn:(t + 1) * bn].sum(axis=1), rtol=1e-12, atol=1e-9)
 
 
+def _f16_dev(a32, dev):
+    return torch.from_numpy(np.ascontiguousarray(a32, dtype=np.float16).view(np.int16)).to(dev)
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 64, 128), (256, 256, 512)])
+def test_f16x3_gemm_matches_fp64_of_split(cuda, M, N, K):
+    """FP16 parts of 2^15-scaled operands: hi = fp16(a*s), lo = fp16(a*s - hi)."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(K)
+    s = np.float32(32768.0)
+    A = rng.random((M, K)).astype(np.float32)
+    B = rng.random((N, K)).astype(np.float32)
+    ah = (A * s).astype(np.float16); al = (A * s - ah.astype(np.float32)).astype(np.float16)
+    bh = (B * s).astype(np.float16); bl = (B * s - bh.astype(np.float32)).astype(np.float16)
+    C = torch.empty(M, N, dtype=torch.float32, device=cuda)
+    alpha = 1.0 / (32768.0 * 32768.0)
+    assert lib.opb_gemm_f16x3(M, N, K, _f16_dev(ah, cuda).data_ptr(), _f16_dev(al, cuda).data_ptr(), K,
+                              _f16_dev(bh, cuda).data_ptr(), _f16_dev(bl, cuda).data_ptr(), K, alpha, None, 0.0,
+                              C.data_ptr(), N, None) == 0
+    torch.cuda.synchronize()
+    f = lambda x: x.astype(np.float64)
+    ref = alpha * (f(ah) @ f(bh).T + f(ah) @ f(bl).T + f(al) @ f(bh).T)
+    exact = A.astype(np.float64) @ B.astype(np.float64).T
+    got = C.cpu().numpy().astype(np.float64)
+    assert np.abs(got - ref).max() <= (3 * K / 16 + 8) * 2.0 ** -24 * exact.max()
+    # 22-bit parts: the split product is within ~1e-6 relative of the exact product
+    assert np.abs(ref - exact).max() <= 2e-6 * exact.max()
+
+
 def test_bf16x3_gemm_in_place(cuda):
     """C may alias Cin (the E-form squaring updates E in place)."""
     from oplib_b200 import _lib

@@ -63,7 +63,7 @@ def config0_fp64():
     return cfg, V, O.nearest_node(x)
 
 
-@pytest.mark.parametrize("mode,tol", [("bf16x3", 1e-5), ("fp32", 1e-5), ("fp32_plain", 5e-4)])
+@pytest.mark.parametrize("mode,tol", [("bf16x3", 1e-5), ("fp16x3", 1e-5), ("fp32", 1e-5), ("fp32_plain", 5e-4)])
 def test_config0_quotes_vs_fp64(cuda, config0_fp64, mode, tol):
     cfg, V, y0 = config0_fp64
     lat = _lv()
@@ -87,7 +87,7 @@ def test_kernel_matches_fp64_and_conserves(cuda):
     niter, dt = O.plan_niter(L, 1 / 252, cfg.dt0)
     P64 = O.square(O.ek(L, dt), niter, renorm=True)
     lat = _lv(256)
-    for mode in ["fp32", "bf16x3"]:
+    for mode in ["fp32", "bf16x3", "fp16x3"]:
         P = lat.kernel(1 / 252, cfg.dt0, mode=mode).cpu().numpy().astype(np.float64)
         assert np.abs(P - P64).max() < 2e-5, mode
         assert np.abs(P.sum(axis=1) - 1).max() < 1e-6, mode
@@ -105,7 +105,7 @@ def test_sv_small_bf16x3_vs_fp64(cuda):
     P = O.square(U, niter, renorm=True)
     Ps = O.chain(P, 4)
     Vref = O.price_from_kernels(Ps, xy, strikes, spec.r, 0.25 * np.arange(1, 5))
-    for mode, tol in [("bf16x3", 1e-5), ("fp32", 1e-5)]:
+    for mode, tol in [("bf16x3", 1e-5), ("fp16x3", 1e-5), ("fp32", 1e-5)]:
         q, _ = lat.solve(strikes, 4, 0.25, 2.0 ** -16, mode=mode)
         err = np.abs(q.cpu().numpy() - Vref[:, lat.y0, :]).max()
         print(f"sv256 {mode}: {err:.3e}")
@@ -125,6 +125,9 @@ def test_black_scholes_lattice_on_gpu(cuda):
     assert abs(price - 12.33600) < 0.2  # lattice discretisation on a 1024-node grid
     q32, _ = lat.solve([100.0], 4, 0.25, 2.0 ** -14, mode="fp32")
     assert abs(price - q32.cpu().numpy()[3, 0]) < 1e-3
+    # FP16 parts with a payoff scale derived on the device from max(x) - min(K) (here ~5e3)
+    q16, _ = lat.solve([100.0], 4, 0.25, 2.0 ** -14, mode="fp16x3")
+    assert abs(q16.cpu().numpy()[3, 0] - q32.cpu().numpy()[3, 0]) < 1e-3
 
 
 def test_workspace_too_small_is_rejected(cuda):
