@@ -29,6 +29,8 @@ import tempfile
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -544,6 +546,77 @@ def run_batch(args):
     return line
 
 
+def run_surrogate(args):
+    """Config 4: ensemble of MLP surrogates (8 -> 256 x 4 -> 1, GELU) trained by the
+    library's kernels on ~2^21 quotes that the batched lattice solver generates, then
+    inference on 2^20 held-out quotes on the tensor cores; quotes whose ensemble spread
+    exceeds 5 bp fall back to the lattice.  Reports surrogate quotes/s, the lattice's
+    quotes/s for the same family, fallback rate and errors against the lattice."""
+    import torch
+    from oplib_b200.model import Batch, bind_stream
+    from oplib_b200.surrogate import NMAT, PERIOD, LM, Surrogate, lattice_quotes
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    bind_stream(dev)
+    stream = torch.cuda.current_stream(dev)
+    t0 = time.perf_counter()
+    train = lattice_quotes(args.train_lattices, seed=2026, device=dev)
+    test = lattice_quotes(1024, seed=31337, device=dev)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    sur = Surrogate(members=args.members, device=dev)
+    sur.train(train, epochs=args.epochs, batch=4096, lr=2e-3)
+    n = 1 << 20
+    reps = (n + test.feat.shape[0] - 1) // test.feat.shape[0]
+    feat = test.feat.repeat(reps, 1)[:n].contiguous()
+    base = test.base.repeat(reps)[:n].contiguous()
+    ws = torch.empty(int(sur.lib.opb_mlp_infer_workspace_bytes(n, sur.members)), dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        sur.predict(feat, base, ws)
+    ms_inf = _time(lambda: sur.predict(feat, base, ws), args.steps, stream, torch)
+    # accuracy on the held-out quotes
+    iv, spread = sur.predict(test.feat, test.base, ws)
+    err = (iv - test.iv).abs() * 1e4
+    errb = (test.base - test.iv).abs() * 1e4
+    fb = spread * 1e4 > 5.0
+    acc = ~fb
+    fb_lat = torch.unique(test.lattice[fb]).numel()
+    # lattice throughput for the same family (one 512-lattice sweep of the test distribution)
+    from oplib_b200.model import Lattice
+    rng = np.random.default_rng(7)
+    lats = [Lattice.local_vol(n=int(rng.choice(np.arange(256, 1025, 128))), level=0.25, skew=0.1, width=0.5,
+                              rate=0.02, floor=0.01, device=dev) for _ in range(512)]
+    bt = Batch(lats, np.exp(LM), NMAT, PERIOD, 2.0 ** -14, mode="fp16x3", autotune=True)
+    qq = bt.execute()
+    g = _graph(lambda: bt.execute(qq), dev, torch)
+    g.replay()
+    ms_lat = _time(g.replay, 3, stream, torch)
+    lat_qps = 512 * NMAT * 64 / (ms_lat * 1e-3)
+    sur_qps = n / (ms_inf * 1e-3)
+    # effective: surrogate for accepted quotes, lattice re-solve of every lattice holding a fallback
+    n_test = test.feat.shape[0]
+    eff_s = ms_inf * 1e-3 * n_test / n + (fb_lat / 512) * ms_lat * 1e-3
+    q = lambda x, p: float(torch.quantile(x.float(), p).item()) if x.numel() else float("nan")
+    return {"metric": "surrogate quotes/sec (ensemble MLP on tensor cores) vs lattice quotes/sec",
+            "value": round(sur_qps, 1), "unit": "quotes/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_inf, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 weights/activations, fp32 accumulate", "data": "synthetic (lattice-generated)",
+            "config": {"workload": f"2^20 quotes, ensemble of {sur.members} MLPs 8-256x4-1, trained on "
+                                   f"{train.feat.shape[0]} quotes from {args.train_lattices} lattices, "
+                                   f"{args.epochs} epochs, batch 4096", "members": sur.members},
+            "lattice_quotes_per_s": round(lat_qps, 1), "speedup_vs_lattice": round(sur_qps / lat_qps, 1),
+            "fallback_rate": round(float(fb.float().mean().item()), 4),
+            "fallback_lattices": int(fb_lat), "test_quotes": int(n_test),
+            "accepted_err_bp": {"rms": round(float(err[acc].pow(2).mean().sqrt().item()), 2) if acc.any() else None,
+                                "p99": round(q(err[acc], 0.99), 2), "max": round(float(err[acc].max().item()), 2)
+                                if acc.any() else None},
+            "all_err_bp": {"rms": round(float(err.pow(2).mean().sqrt().item()), 2), "p99": round(q(err, 0.99), 2)},
+            "baseline_err_bp": {"rms": round(float(errb.pow(2).mean().sqrt().item()), 2), "p99": round(q(errb, 0.99), 2)},
+            "effective_quotes_per_s_with_fallback": round(n_test / eff_s, 1),
+            "train_seconds": round(sur.train_seconds, 1), "data_seconds": round(t_data, 1),
+            "final_train_mse": sur.history[-1][2]}
+
+
 def run_gemm(args):
     """The squaring GEMM alone (split-BF16, E-form: C = E.E + 2E in place) at size d."""
     import torch
@@ -582,12 +655,16 @@ def main():
     ap.add_argument("--no-compare", dest="compare", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu", action="store_false")
     ap.add_argument("--nlat", type=int, default=512, help="lattices for --workload batch")
-    ap.add_argument("--workload", default="sv", choices=["sv", "lv", "mc", "gemm", "batch"],
+    ap.add_argument("--train-lattices", type=int, default=2048)
+    ap.add_argument("--members", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--workload", default="sv", choices=["sv", "lv", "mc", "gemm", "batch", "surrogate"],
                     help="sv = the headline SV lattice solve; the others are secondary measurements")
     ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
     args = ap.parse_args()
     if args.workload != "sv" and args.impl == "b200":
-        fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "batch": run_batch}[args.workload]
+        fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "batch": run_batch, "surrogate": run_surrogate}[
+            args.workload]
         print(json.dumps(fn(args)))
         return 0
 

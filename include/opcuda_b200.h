@@ -235,6 +235,31 @@ int opb_batch_execute(opb_batch_plan *plan, double *quotes);
 int opb_batch_autotune(opb_batch_plan *plan, int reps, float *ms_out, int *best_cfg);
 int opb_batch_launches(const opb_batch_plan *plan);
 
+/* ------------------------------------------------------------------ surrogate pricer */
+/* new, no reference counterpart (closest: tests/bstest/BSPricer.cs:7-65): MLP 8 -> 256 x 4 -> 1
+ * (GELU) from (level, skew, width, kappa, rho, r, log-moneyness, T) to implied vol.  theta: FP32
+ * master parameters (layer l: W [out x in] row-major then b); training uses BF16-rounded
+ * working weights thb (FP32 storage), FP32 activations, Adam on theta.  loss receives the sum
+ * of squared errors. */
+int opb_mlp_param_count(void);
+long long opb_mlp_workspace_floats(int B);
+int opb_mlp_init(float *theta, unsigned long long seed);
+int opb_mlp_round(const float *theta, float *theta_bf, void *theta_b16);
+int opb_mlp_forward(const float *thb, const float *X, int B, float *ws, float *y);
+int opb_mlp_loss_grad(const float *thb, const float *X, const float *t, int B, float *ws, float *grad, double *loss);
+int opb_mlp_adam(float *theta, float *m, float *v, const float *grad, int step, float lr, float b1, float b2,
+                 float eps, float *theta_bf);
+/* implied volatilities of call prices with spots S0[i] (FP64 bisection); NaN without time value */
+int opb_implied_vol(long long n, const double *price, const double *K, const double *T, const double *r,
+                    const double *S0, double *iv);
+/* tensor-core ensemble inference: packed BF16 weights (opb_mlp_pack), members at packed +
+ * m * member_stride bytes; mean / spread (max - min) of the member outputs */
+long long opb_mlp_packed_bytes(void);
+int opb_mlp_pack(const float *theta, void *packed);
+long long opb_mlp_infer_workspace_bytes(long long n, int nmem);
+int opb_mlp_infer(const void *packed, int nmem, long long member_stride, const float *X, long long n, void *ws,
+                  long long ws_bytes, float *mean, float *spread);
+
 /* ------------------------------------------------------------------ cumulative rows, MC */
 /* replaces oplib/opcuda/sck.cu:88-93: nm column-major kernels -> cumulative normalised rows */
 int opcuda_sck(int d, int nm, uint64_t tpker_yy_m, uint64_t ctpker_yy_m);

@@ -104,6 +104,19 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_batch_execute": (i32, [vp, vp]),
     "opb_batch_autotune": (i32, [vp, i32, vp, vp]),
     "opb_batch_launches": (i32, [vp]),
+    # surrogate MLP
+    "opb_mlp_param_count": (i32, []),
+    "opb_mlp_workspace_floats": (i64, [i32]),
+    "opb_mlp_init": (i32, [vp, ull]),
+    "opb_mlp_round": (i32, [vp, vp, vp]),
+    "opb_mlp_forward": (i32, [vp, vp, i32, vp, vp]),
+    "opb_mlp_loss_grad": (i32, [vp, vp, vp, i32, vp, vp, vp]),
+    "opb_mlp_adam": (i32, [vp, vp, vp, vp, i32, f32, f32, f32, f32, vp]),
+    "opb_implied_vol": (i32, [i64, vp, vp, vp, vp, vp, vp]),
+    "opb_mlp_packed_bytes": (i64, []),
+    "opb_mlp_pack": (i32, [vp, vp]),
+    "opb_mlp_infer_workspace_bytes": (i64, [i64, i32]),
+    "opb_mlp_infer": (i32, [vp, i32, i64, vp, i64, vp, i64, vp, vp]),
     # cumulative rows / MC
     "opcuda_sck": (i32, [i32, i32, u64, u64]),
     "opb_sck_rm": (i32, [i32, i32, vp, vp]),

@@ -30,7 +30,10 @@ struct SgemmArgs {
     long long sA, sB, sC;
 };
 
-// Row-major C[M,N] = alpha * A[M,K] . B[K,N] + beta * C.  grid = (ceil(N/128), ceil(M/128), batch)
+// Row-major C[M,N] = alpha * op(A)[M,K] . op(B)[K,N] + beta * C; TA: A stored K x M
+// (element (m,k) at k*lda + m), TB: B stored N x K (element (k,n) at n*ldb + k).
+// grid = (ceil(N/128), ceil(M/128), batch)
+template <bool TA, bool TB>
 __global__ void __launch_bounds__(SG_THREADS, 2) k_sgemm_rm(SgemmArgs p) {
     __shared__ __align__(16) float As[2][SG_BK][SG_BM + SG_APAD];
     __shared__ __align__(16) float Bs[2][SG_BK][SG_BN];
@@ -54,13 +57,17 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_sgemm_rm(SgemmArgs p) {
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             int gk = k0 + a_k + j;
-            ra[j] = (gr < p.M && gk < p.K) ? __ldg(A + (long long)gr * p.lda + gk) : 0.f;
+            ra[j] = (gr < p.M && gk < p.K)
+                        ? __ldg(TA ? A + (long long)gk * p.lda + gr : A + (long long)gr * p.lda + gk)
+                        : 0.f;
         }
         int gk = k0 + b_k;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             int gc = n0 + b_col + j;
-            rb[j] = (gk < p.K && gc < p.N) ? __ldg(B + (long long)gk * p.ldb + gc) : 0.f;
+            rb[j] = (gk < p.K && gc < p.N)
+                        ? __ldg(TB ? B + (long long)gc * p.ldb + gk : B + (long long)gk * p.ldb + gc)
+                        : 0.f;
         }
     };
     auto store_tiles = [&](int buf) {
@@ -121,11 +128,23 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_sgemm_rm(SgemmArgs p) {
     }
 }
 
-int sgemm_rowmajor(const SgemmArgs &a, int batch, cudaStream_t s) {
+int sgemm_rowmajor(const SgemmArgs &a, int batch, cudaStream_t s, bool ta = false, bool tb = false) {
     if (a.M <= 0 || a.N <= 0 || batch <= 0) return OPB_OK;
     dim3 grid((a.N + SG_BN - 1) / SG_BN, (a.M + SG_BM - 1) / SG_BM, batch);
-    k_sgemm_rm<<<grid, SG_THREADS, 0, s>>>(a);
+    if (!ta && !tb) k_sgemm_rm<false, false><<<grid, SG_THREADS, 0, s>>>(a);
+    else if (ta && !tb) k_sgemm_rm<true, false><<<grid, SG_THREADS, 0, s>>>(a);
+    else if (!ta && tb) k_sgemm_rm<false, true><<<grid, SG_THREADS, 0, s>>>(a);
+    else k_sgemm_rm<true, true><<<grid, SG_THREADS, 0, s>>>(a);
     return static_cast<int>(cudaGetLastError());
+}
+
+// Row-major with transpose flags (see k_sgemm_rm).
+int sgemm_rm_t(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, int lda, const float *B, int ldb,
+               float beta, float *C, int ldc, cudaStream_t s) {
+    SgemmArgs a{};
+    a.M = M; a.N = N; a.K = K; a.lda = lda; a.ldb = ldb; a.ldc = ldc;
+    a.alpha = alpha; a.beta = beta; a.A = A; a.B = B; a.C = C;
+    return sgemm_rowmajor(a, 1, s, ta, tb);
 }
 
 // Convenience: row-major, unbatched.

@@ -135,11 +135,12 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, int NPROD = 3>
 struct TcCfg {
     static constexpr int A_BYTES = TC_BM * TC_BK * 2;  // one of Ahi/Alo
     static constexpr int B_BYTES = BN * TC_BK * 2;     // one of Bhi/Blo
-    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    static constexpr int NPARTS = NPROD == 1 ? 1 : 2;  // parts loaded per operand
+    static constexpr int STAGE_BYTES = NPARTS * (A_BYTES + B_BYTES);
     static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
     static constexpr int CPT = BN < 128 ? BN : 128;        // accumulator columns per epilogue thread
     static constexpr int HALVES = BN / CPT;                 // column groups per TMEM lane
@@ -156,6 +157,10 @@ struct TcParams {
     const float *Cin;
     float alpha, beta;
     double *rowsum;
+    // EPIMODE == 1 (network layer): H = GELU(alpha * acc + bias[col]) stored as BF16
+    const float *bias;
+    __nv_bfloat16 *H;
+    long long ldh;
 };
 
 // Batched launches read per-problem tensor maps (4 per problem: Ahi, Alo, Bhi, Blo) and
@@ -175,12 +180,12 @@ struct TcBatch {
 // into FP32 register sums (round to nearest) while the MMA warp fills the other
 // accumulator.  The tensor cores' truncating accumulation thus spans only 12*CHUNK MMA
 // instructions, and an item's final store overlaps the next item's MMAs.
-template <int BN, int STAGES, bool BATCHED, bool F16>
-__global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
+template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0>
+__global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
               const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p,
               TcBatch bt) {
-    using Cfg = TcCfg<BN, STAGES>;
+    using Cfg = TcCfg<BN, STAGES, NPROD>;
     constexpr int EPI = Cfg::EPI_WARPS;
     constexpr int CPT = Cfg::CPT;
     extern __shared__ uint8_t smem_raw[];
@@ -271,9 +276,13 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
                     mbar_expect_tx(full_bar(s), Cfg::STAGE_BYTES);
                     const int kx = kb * TC_BK;
                     tma_load_2d(st, mp[0], full_bar(s), kx, m0);
-                    tma_load_2d(st + Cfg::A_BYTES, mp[1], full_bar(s), kx, m0);
-                    tma_load_2d(st + 2 * Cfg::A_BYTES, mp[2], full_bar(s), kx, n0);
-                    tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, mp[3], full_bar(s), kx, n0);
+                    if constexpr (NPROD == 1) {
+                        tma_load_2d(st + Cfg::A_BYTES, mp[2], full_bar(s), kx, n0);
+                    } else {
+                        tma_load_2d(st + Cfg::A_BYTES, mp[1], full_bar(s), kx, m0);
+                        tma_load_2d(st + 2 * Cfg::A_BYTES, mp[2], full_bar(s), kx, n0);
+                        tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, mp[3], full_bar(s), kx, n0);
+                    }
                 }
             }
             if (!ok) {
@@ -315,15 +324,17 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
                         const uint32_t st = base + s * Cfg::STAGE_BYTES;
                         const uint64_t dAh = umma_desc_sw128(st);
                         const uint64_t dAl = umma_desc_sw128(st + Cfg::A_BYTES);
-                        const uint64_t dBh = umma_desc_sw128(st + 2 * Cfg::A_BYTES);
+                        const uint64_t dBh = umma_desc_sw128(st + Cfg::NPARTS * Cfg::A_BYTES);
                         const uint64_t dBl = umma_desc_sw128(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES);
 #pragma unroll
                         for (int k16 = 0; k16 < TC_BK / 16; k16++) {
                             const uint64_t adv = (uint64_t)((k16 * 32) >> 4);  // +32 bytes along K
                             const uint32_t acc0 = (kb > c * Cfg::CHUNK || k16 > 0) ? 1u : 0u;
                             umma_bf16(dacc, dAh + adv, dBh + adv, idesc, acc0);
-                            umma_bf16(dacc, dAh + adv, dBl + adv, idesc, 1u);
-                            umma_bf16(dacc, dAl + adv, dBh + adv, idesc, 1u);
+                            if constexpr (NPROD == 3) {
+                                umma_bf16(dacc, dAh + adv, dBl + adv, idesc, 1u);
+                                umma_bf16(dacc, dAl + adv, dBh + adv, idesc, 1u);
+                            }
                         }
                         umma_commit(empty_bar(s));
                     }
@@ -384,6 +395,25 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES>::THREADS, 1)
             }
             const int row = m0 + q * 32 + lane;
             const int col0 = n0 + h * CPT;
+            if constexpr (EPIMODE == 1) {
+                // network layer: BF16 GELU(alpha * acc + bias), 8 values per 16-byte store
+                __nv_bfloat16 *hrow = p.H + (long long)row * p.ldh + col0;
+#pragma unroll
+                for (int j = 0; j < CPT; j += 8) {
+                    uint32_t pk[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        float z0 = fmaf(alpha, sum[j + 2 * u], __ldg(p.bias + col0 + j + 2 * u));
+                        float z1 = fmaf(alpha, sum[j + 2 * u + 1], __ldg(p.bias + col0 + j + 2 * u + 1));
+                        z0 = 0.5f * z0 * (1.f + erff(z0 * 0.70710678118654752f));
+                        z1 = 0.5f * z1 * (1.f + erff(z1 * 0.70710678118654752f));
+                        pk[u] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(z0)) |
+                                ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(z1)) << 16);
+                    }
+                    *reinterpret_cast<uint4 *>(hrow + j) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                }
+                continue;
+            }
             float *crow = C + (long long)row * ldc + col0;
             const float *cin = Cin ? Cin + (long long)row * ldc + col0 : nullptr;
             double rs = 0.0;
@@ -473,14 +503,15 @@ int tc_gemm_check(const TcGemmArgs &a) {
     return OPB_OK;
 }
 
-template <int BN, int STAGES, bool BATCHED, bool F16>
+template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0>
 static int set_smem_attr() {
-    using Cfg = TcCfg<BN, STAGES>;
+    using Cfg = TcCfg<BN, STAGES, NPROD>;
     static bool attr_set[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED, F16, NPROD, EPIMODE>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              Cfg::SMEM);
         if (e != cudaSuccess) return (int)e;
         attr_set[dev] = true;
@@ -543,6 +574,29 @@ int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *pro
         case 129: return launch_batched_impl<64, 4, true>(maps, probs, work, nwork, grid, s);
         default: return OPB_E_UNSUPPORTED;
     }
+}
+
+// One network layer on the tensor cores: H[M, N] = GELU(alpha * A[M, K] . W[N, K]^T + bias)
+// with BF16 A, W and H (single product, FP32 accumulation); M % 128, N % 256, K % 64.
+int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, const __nv_bfloat16 *W,
+                    long long ldw, float alpha, const float *bias, __nv_bfloat16 *H, long long ldh, cudaStream_t s) {
+    constexpr int BN = 256, STAGES = 4;
+    using Cfg = TcCfg<BN, STAGES, 1>;
+    if (M <= 0 || M % TC_BM || N % BN || K % TC_BK) return OPB_E_UNSUPPORTED;
+    if (!A || !W || !bias || !H) return OPB_E_NULL;
+    int e0 = set_smem_attr<BN, STAGES, false, false, 1, 1>();
+    if (e0) return e0;
+    CUtensorMap mA, mW;
+    int r;
+    if ((r = make_map(&mA, A, M, K, lda, TC_BM)) != OPB_OK) return r;
+    if ((r = make_map(&mW, W, N, K, ldw, BN)) != OPB_OK) return r;
+    TcParams p{};
+    p.M = M; p.N = N; p.K = K; p.alpha = alpha; p.bias = bias; p.H = H; p.ldh = ldh;
+    const int ntiles = (M / TC_BM) * (N / BN);
+    const int grid = ntiles < num_sms() ? ntiles : num_sms();
+    TcBatch none{nullptr, nullptr, nullptr, 0};
+    k_tc_gemm<BN, STAGES, false, false, 1, 1><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mA, mA, mW, mW, p, none);
+    return (int)cudaGetLastError();
 }
 
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {

@@ -11,6 +11,8 @@ namespace opb {
 // gemm_simt.cu
 int sgemm_rm(int M, int N, int K, float alpha, const float *A, int lda, const float *B, int ldb, float beta,
              float *C, int ldc, cudaStream_t s);
+int sgemm_rm_t(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, int lda, const float *B, int ldb,
+               float beta, float *C, int ldc, cudaStream_t s);
 
 // lattice_kernels.cu
 int launch_ek_ell(int d, int w, const int *cols, const double *vals, double dt, int eform, float *out,
@@ -77,6 +79,8 @@ struct TcGemmArgs {
 int tc_gemm_tile_n(int N);                    // tile width chosen for N (0 if unsupported)
 int tc_gemm_check(const TcGemmArgs &a);       // argument/alignment check, OPB_* code
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s);
+int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, const __nv_bfloat16 *W,
+                    long long ldw, float alpha, const float *bias, __nv_bfloat16 *H, long long ldh, cudaStream_t s);
 int tc_gemm_nparts(int N);                    // number of row-sum partials written
 
 // Batched launches: problem descriptors and tensor maps live in device memory.

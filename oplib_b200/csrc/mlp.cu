@@ -1,0 +1,479 @@
+// Learned surrogate pricer: an MLP 8 -> 256 -> 256 -> 256 -> 256 -> 1 with GELU, from
+// (level, skew, width, kappa, rho, r, log-moneyness, T) to implied volatility, trained on
+// quotes that the batched lattice solver produces, with the lattice as fallback and judge.
+// The reference has no counterpart (its closest piece is the Black-Scholes pricer of its
+// known-answer test, tests/bstest/BSPricer.cs:7-65).
+//
+// Parameters live in one flat FP32 master vector theta (layer l: W_l [out x in] row-major,
+// then b_l [out]); training uses BF16-rounded working weights (kept as FP32 values), FP32
+// activations and gradients, and Adam on the FP32 master copy.  All kernels are this
+// project's: SIMT GEMMs (gemm_simt.cu, with transpose flags) plus the fused element-wise
+// kernels below.  Batched inference of the trained network runs through
+// opb_mlp_infer (BF16 weights and activations, FP32 accumulation).
+#include <cuda_bf16.h>
+
+#include <cmath>
+
+#include "common.cuh"
+#include "lattice.h"
+
+namespace opb {
+
+constexpr int MLP_IN = 8, MLP_H = 256, MLP_LAYERS = 5;  // 4 hidden + output
+constexpr int MLP_NPARAM = MLP_H * MLP_IN + MLP_H + 3 * (MLP_H * MLP_H + MLP_H) + MLP_H + 1;  // 199,937
+
+struct MlpLayout {
+    int in[MLP_LAYERS], out[MLP_LAYERS];
+    long long w[MLP_LAYERS], b[MLP_LAYERS];
+};
+
+__host__ __device__ inline MlpLayout mlp_layout() {
+    MlpLayout L{};
+    const int ins[MLP_LAYERS] = {MLP_IN, MLP_H, MLP_H, MLP_H, MLP_H};
+    const int outs[MLP_LAYERS] = {MLP_H, MLP_H, MLP_H, MLP_H, 1};
+    long long o = 0;
+    for (int l = 0; l < MLP_LAYERS; l++) {
+        L.in[l] = ins[l];
+        L.out[l] = outs[l];
+        L.w[l] = o;
+        o += (long long)ins[l] * outs[l];
+        L.b[l] = o;
+        o += outs[l];
+    }
+    return L;
+}
+
+__device__ __forceinline__ uint32_t hash32(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdULL;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ULL;
+    x ^= x >> 33;
+    return (uint32_t)x;
+}
+
+// Uniform(-a, a) weights with a = sqrt(6 / fan_in) (He-uniform), zero biases.
+__global__ void k_mlp_init(float *__restrict__ theta, uint64_t seed) {
+    const MlpLayout L = mlp_layout();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < MLP_NPARAM;
+         i += (long long)gridDim.x * blockDim.x) {
+        int l = 0;
+        while (l + 1 < MLP_LAYERS && i >= L.w[l + 1]) l++;
+        if (i >= L.b[l]) {
+            theta[i] = 0.f;
+        } else {
+            const float a = sqrtf(6.f / (float)L.in[l]);
+            const float u = (hash32(seed * 0x9E3779B97F4A7C15ULL + (uint64_t)i) >> 8) * (1.0f / 16777216.0f);
+            theta[i] = (2.f * u - 1.f) * a;
+        }
+    }
+}
+
+// BF16 working copy of the master weights (as FP32 values) and the BF16 storage used by
+// inference (same layout).
+__global__ void k_mlp_round(const float *__restrict__ theta, float *__restrict__ theta_bf,
+                            __nv_bfloat16 *__restrict__ theta_b16, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const __nv_bfloat16 b = __float2bfloat16_rn(theta[i]);
+        if (theta_bf) theta_bf[i] = __bfloat162float(b);
+        if (theta_b16) theta_b16[i] = b;
+    }
+}
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+    return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+// Z += b (per column), H = GELU(Z).  Z, H: [B x n] row-major.
+__global__ void k_bias_gelu(long long total, int n, float *__restrict__ Z, const float *__restrict__ b,
+                            float *__restrict__ H) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float z = Z[i] + b[i % n];
+        Z[i] = z;
+        H[i] = gelu(z);
+    }
+}
+
+// y[r] = H[r, :] . w + b0 (warp per row), and (optional) dy = 2 (y - t) / B, loss partials.
+__global__ void k_out_layer(int B, const float *__restrict__ H, const float *__restrict__ w, const float *__restrict__ b,
+                            float *__restrict__ y, const float *__restrict__ t, float *__restrict__ dy,
+                            double *__restrict__ loss_part) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    double se = 0.0;
+    if (warp < B) {
+        const float *h = H + (long long)warp * MLP_H;
+        float s = 0.f;
+        for (int j = lane; j < MLP_H; j += 32) s = fmaf(h[j], w[j], s);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        const float v = s + b[0];
+        if (lane == 0) {
+            y[warp] = v;
+            if (t) {
+                const float e = v - t[warp];
+                dy[warp] = 2.f * e / (float)B;
+                se = (double)e * (double)e;
+            }
+        }
+    }
+    if (loss_part && lane == 0) atomicAdd(loss_part, se);
+}
+
+// dZ = dH * GELU'(Z)
+__global__ void k_gelu_back(long long total, const float *__restrict__ Z, const float *__restrict__ dH,
+                            float *__restrict__ dZ) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x)
+        dZ[i] = dH[i] * gelu_grad(Z[i]);
+}
+
+// db[c] = sum_r dZ[r, c] (block per column group of 32, deterministic order)
+__global__ void k_colsum(int B, int n, const float *__restrict__ dZ, float *__restrict__ db) {
+    __shared__ float red[8][33];
+    const int c = blockIdx.x * 32 + (threadIdx.x & 31), rg = threadIdx.x >> 5;  // 8 row groups
+    float s = 0.f;
+    if (c < n)
+        for (int r = rg; r < B; r += 8) s += dZ[(long long)r * n + c];
+    red[rg][threadIdx.x & 31] = s;
+    __syncthreads();
+    if (rg == 0 && c < n) {
+        float t = 0.f;
+        for (int i = 0; i < 8; i++) t += red[i][threadIdx.x & 31];
+        db[c] = t;
+    }
+}
+
+// Output-layer weight gradient dw5[j] = sum_r dy[r] H4[r, j] and db5 = sum_r dy[r].
+__global__ void k_out_grad(int B, const float *__restrict__ H, const float *__restrict__ dy, float *__restrict__ dw,
+                           float *__restrict__ db) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > MLP_H) return;
+    float s = 0.f;
+    if (j < MLP_H)
+        for (int r = 0; r < B; r++) s = fmaf(dy[r], H[(long long)r * MLP_H + j], s);
+    else
+        for (int r = 0; r < B; r++) s += dy[r];
+    if (j < MLP_H) dw[j] = s;
+    else db[0] = s;
+}
+
+// dH4 = dy (outer) w5
+__global__ void k_out_back(int B, const float *__restrict__ dy, const float *__restrict__ w, float *__restrict__ dH) {
+    const long long total = (long long)B * MLP_H;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x)
+        dH[i] = dy[i / MLP_H] * w[i % MLP_H];
+}
+
+// Adam on the FP32 master weights; refreshes the BF16 working copy.
+__global__ void k_adam(int n, float *__restrict__ theta, float *__restrict__ m, float *__restrict__ v,
+                       const float *__restrict__ g, float lr, float b1, float b2, float eps, float c1, float c2,
+                       float *__restrict__ theta_bf) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float th = theta[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        theta[i] = th;
+        theta_bf[i] = __bfloat162float(__float2bfloat16_rn(th));
+    }
+}
+
+// ---- implied volatility of call prices (FP64 bisection on the Black-Scholes price)
+__device__ double bs_call(double s, double k, double r, double sig, double t) {
+    const double sq = sig * sqrt(t);
+    const double d1 = (log(s / k) + (r + 0.5 * sig * sig) * t) / sq;
+    return s * normcdf(d1) - k * exp(-r * t) * normcdf(d1 - sq);
+}
+
+__global__ void k_implied_vol(long long n, const double *__restrict__ price, const double *__restrict__ K,
+                              const double *__restrict__ T, const double *__restrict__ r,
+                              const double *__restrict__ S0, double *__restrict__ iv) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double p = price[i], k = K[i], t = T[i], rr = r[i], s0 = S0[i];
+        const double intrinsic = fmax(s0 - k * exp(-rr * t), 0.0);
+        double lo = 1e-4, hi = 4.0;
+        if (!(p > intrinsic) || p >= s0) {
+            iv[i] = nan("");
+            continue;
+        }
+        for (int it = 0; it < 80; it++) {
+            const double mid = 0.5 * (lo + hi);
+            if (bs_call(s0, k, rr, mid, t) > p) hi = mid; else lo = mid;
+        }
+        iv[i] = 0.5 * (lo + hi);
+    }
+}
+
+}  // namespace opb
+
+using namespace opb;
+
+namespace {
+
+struct MlpWs {  // training workspace carve (floats)
+    float *Z[4], *H[4], *dZ, *dH, *y, *dy;
+    double *loss;
+};
+
+MlpWs carve_mlp(float *ws, int B) {
+    MlpWs w{};
+    size_t o = 0;
+    for (int l = 0; l < 4; l++) {
+        w.Z[l] = ws + o; o += (size_t)B * MLP_H;
+        w.H[l] = ws + o; o += (size_t)B * MLP_H;
+    }
+    w.dZ = ws + o; o += (size_t)B * MLP_H;
+    w.dH = ws + o; o += (size_t)B * MLP_H;
+    w.y = ws + o; o += (size_t)B;
+    w.dy = ws + o; o += (size_t)B;
+    o = (o + 1) & ~size_t(1);
+    w.loss = reinterpret_cast<double *>(ws + o);
+    return w;
+}
+
+int grid_ew(long long n) {
+    long long b = (n + 255) / 256;
+    long long cap = 8LL * num_sms();
+    return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
+#define MT(expr)                          \
+    do {                                  \
+        int _r = (expr);                  \
+        if (_r) return set_status(_r);    \
+    } while (0)
+
+int mlp_forward(const float *thb, const float *X, int B, MlpWs &w, cudaStream_t s) {
+    const MlpLayout L = mlp_layout();
+    const float *in = X;
+    for (int l = 0; l < 4; l++) {
+        // Z = in . W^T  (W stored out x in: the TB form)
+        MT(sgemm_rm_t(false, true, B, L.out[l], L.in[l], 1.f, in, L.in[l], thb + L.w[l], L.in[l], 0.f, w.Z[l],
+                      L.out[l], s));
+        const long long tot = (long long)B * L.out[l];
+        k_bias_gelu<<<grid_ew(tot), 256, 0, s>>>(tot, L.out[l], w.Z[l], thb + L.b[l], w.H[l]);
+        in = w.H[l];
+    }
+    return (int)cudaGetLastError();
+}
+
+}  // namespace
+
+OPB_API int opb_mlp_param_count(void) { return MLP_NPARAM; }
+
+// floats of training workspace for batch B
+OPB_API long long opb_mlp_workspace_floats(int B) { return 10LL * B * MLP_H + 2LL * B + 8; }
+
+OPB_API int opb_mlp_init(float *theta, unsigned long long seed) {
+    OPB_REQUIRE(theta, OPB_E_NULL);
+    k_mlp_init<<<grid_ew(MLP_NPARAM), 256, 0, stream()>>>(theta, seed);
+    return launch_check();
+}
+
+// theta_bf: BF16-rounded FP32 working copy (optional); theta_b16: BF16 storage (optional)
+OPB_API int opb_mlp_round(const float *theta, float *theta_bf, void *theta_b16) {
+    OPB_REQUIRE(theta, OPB_E_NULL);
+    k_mlp_round<<<grid_ew(MLP_NPARAM), 256, 0, stream()>>>(theta, theta_bf, reinterpret_cast<__nv_bfloat16 *>(theta_b16),
+                                                            MLP_NPARAM);
+    return launch_check();
+}
+
+// Forward pass of B rows of X [B x 8] with the working weights thb; y [B].  The workspace
+// keeps the pre-activations for a following opb_mlp_backward.
+OPB_API int opb_mlp_forward(const float *thb, const float *X, int B, float *ws, float *y) {
+    OPB_REQUIRE(thb && X && ws && y, OPB_E_NULL);
+    OPB_REQUIRE(B > 0, OPB_E_ARG);
+    MlpWs w = carve_mlp(ws, B);
+    cudaStream_t s = stream();
+    MT(mlp_forward(thb, X, B, w, s));
+    const MlpLayout L = mlp_layout();
+    k_out_layer<<<(B * 32 + 255) / 256, 256, 0, s>>>(B, w.H[3], thb + L.w[4], thb + L.b[4], y, nullptr, nullptr,
+                                                      nullptr);
+    return launch_check();
+}
+
+// Loss (mean squared error against t) and its gradient with respect to the working weights,
+// written into grad [param count].  loss (device, 1 double, optional) receives the mean.
+OPB_API int opb_mlp_loss_grad(const float *thb, const float *X, const float *t, int B, float *ws, float *grad,
+                              double *loss) {
+    OPB_REQUIRE(thb && X && t && ws && grad, OPB_E_NULL);
+    OPB_REQUIRE(B > 0, OPB_E_ARG);
+    MlpWs w = carve_mlp(ws, B);
+    cudaStream_t s = stream();
+    const MlpLayout L = mlp_layout();
+    MT(mlp_forward(thb, X, B, w, s));
+    MT((int)cudaMemsetAsync(w.loss, 0, sizeof(double), s));
+    k_out_layer<<<(B * 32 + 255) / 256, 256, 0, s>>>(B, w.H[3], thb + L.w[4], thb + L.b[4], w.y, t, w.dy, w.loss);
+    // output layer
+    k_out_grad<<<(MLP_H + 1 + 255) / 256 * 1 + 1, 256, 0, s>>>(B, w.H[3], w.dy, grad + L.w[4], grad + L.b[4]);
+    k_out_back<<<grid_ew((long long)B * MLP_H), 256, 0, s>>>(B, w.dy, thb + L.w[4], w.dH);
+    for (int l = 3; l >= 0; l--) {
+        const long long tot = (long long)B * L.out[l];
+        k_gelu_back<<<grid_ew(tot), 256, 0, s>>>(tot, w.Z[l], w.dH, w.dZ);
+        // dW = dZ^T . in  (A = dZ stored B x out: the TA form)
+        const float *in = l > 0 ? w.H[l - 1] : X;
+        MT(sgemm_rm_t(true, false, L.out[l], L.in[l], B, 1.f, w.dZ, L.out[l], in, L.in[l], 0.f, grad + L.w[l],
+                      L.in[l], s));
+        k_colsum<<<(L.out[l] + 31) / 32, 256, 0, s>>>(B, L.out[l], w.dZ, grad + L.b[l]);
+        if (l > 0) MT(sgemm_rm_t(false, false, B, L.in[l], L.out[l], 1.f, w.dZ, L.out[l], thb + L.w[l], L.in[l], 0.f,
+                                 w.dH, L.in[l], s));
+    }
+    if (loss) {
+        // mean of the squared errors
+        MT((int)cudaMemcpyAsync(loss, w.loss, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    return launch_check();
+}
+
+OPB_API int opb_mlp_adam(float *theta, float *m, float *v, const float *grad, int step, float lr, float b1, float b2,
+                         float eps, float *theta_bf) {
+    OPB_REQUIRE(theta && m && v && grad && theta_bf, OPB_E_NULL);
+    OPB_REQUIRE(step >= 1 && lr > 0.f, OPB_E_ARG);
+    const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+    k_adam<<<grid_ew(MLP_NPARAM), 256, 0, stream()>>>(MLP_NPARAM, theta, m, v, grad, lr, b1, b2, eps, c1, c2, theta_bf);
+    return launch_check();
+}
+
+// Implied volatilities of n call prices with spots S0[i]; NaN where the price carries no
+// time value.
+OPB_API int opb_implied_vol(long long n, const double *price, const double *K, const double *T, const double *r,
+                            const double *S0, double *iv) {
+    OPB_REQUIRE(n >= 0, OPB_E_ARG);
+    if (n == 0) return set_status(OPB_OK);
+    OPB_REQUIRE(price && K && T && r && S0 && iv, OPB_E_NULL);
+    k_implied_vol<<<grid_ew(n), 256, 0, stream()>>>(n, price, K, T, r, S0, iv);
+    return launch_check();
+}
+
+// ---------------------------------------------------------------- tensor-core inference
+//
+// Packed inference weights of one network (bytes): W1 padded to [256 x 64] BF16 (input
+// features 8..63 zero), W2..W4 [256 x 256] BF16, then FP32 b1..b4 [4 x 256], w5 [256], b5.
+namespace opb {
+
+constexpr long long MLP_PACK_W1 = 256LL * 64 * 2, MLP_PACK_WH = 256LL * 256 * 2;
+constexpr long long MLP_PACK_BYTES = MLP_PACK_W1 + 3 * MLP_PACK_WH + (4 * 256 + 256 + 1) * 4;
+
+__global__ void k_mlp_pack(const float *__restrict__ theta, uint8_t *__restrict__ packed) {
+    const MlpLayout L = mlp_layout();
+    __nv_bfloat16 *w1 = reinterpret_cast<__nv_bfloat16 *>(packed);
+    __nv_bfloat16 *wh = reinterpret_cast<__nv_bfloat16 *>(packed + MLP_PACK_W1);
+    float *f = reinterpret_cast<float *>(packed + MLP_PACK_W1 + 3 * MLP_PACK_WH);
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x, nth = (long long)gridDim.x * blockDim.x;
+    for (long long i = tid; i < 256 * 64; i += nth) {
+        const int o = (int)(i / 64), c = (int)(i % 64);
+        w1[i] = __float2bfloat16_rn(c < MLP_IN ? theta[L.w[0] + (long long)o * MLP_IN + c] : 0.f);
+    }
+    for (long long i = tid; i < 3LL * 256 * 256; i += nth) {
+        const int l = 1 + (int)(i / (256 * 256));
+        wh[i] = __float2bfloat16_rn(theta[L.w[l] + i % (256 * 256)]);
+    }
+    for (long long i = tid; i < 4 * 256 + 256 + 1; i += nth) {
+        float v;
+        if (i < 4 * 256) v = __bfloat162float(__float2bfloat16_rn(theta[L.b[i / 256] + i % 256]));
+        else if (i < 4 * 256 + 256) v = __bfloat162float(__float2bfloat16_rn(theta[L.w[4] + (i - 1024)]));
+        else v = __bfloat162float(__float2bfloat16_rn(theta[L.b[4]]));
+        f[i] = v;
+    }
+}
+
+// X [n x 8] FP32 -> Xp [n x 64] BF16 (zero padded)
+__global__ void k_mlp_pad_input(long long n, const float *__restrict__ X, __nv_bfloat16 *__restrict__ Xp) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * 64;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / 64;
+        const int c = (int)(i % 64);
+        Xp[i] = __float2bfloat16_rn(c < MLP_IN ? X[r * MLP_IN + c] : 0.f);
+    }
+}
+
+// y[r] = H[r, :] . w5 + b5 with BF16 H (warp per row)
+__global__ void k_mlp_out_bf16(long long n, const __nv_bfloat16 *__restrict__ H, const float *__restrict__ w,
+                               const float *__restrict__ b, float *__restrict__ y) {
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const uint4 v = *reinterpret_cast<const uint4 *>(H + warp * 256 + lane * 8);
+    const uint32_t u[4] = {v.x, v.y, v.z, v.w};
+    float s = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        s = fmaf(__bfloat162float(__ushort_as_bfloat16((unsigned short)(u[j] & 0xffffu))), w[lane * 8 + 2 * j], s);
+        s = fmaf(__bfloat162float(__ushort_as_bfloat16((unsigned short)(u[j] >> 16))), w[lane * 8 + 2 * j + 1], s);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[warp] = s + b[0];
+}
+
+// ensemble mean and spread (max - min) over nmem member outputs y[m * n + r]
+__global__ void k_mlp_ensemble(long long n, int nmem, const float *__restrict__ y, float *__restrict__ mean,
+                               float *__restrict__ spread) {
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
+        float s = 0.f, lo = 3.4e38f, hi = -3.4e38f;
+        for (int m = 0; m < nmem; m++) {
+            const float v = y[(long long)m * n + r];
+            s += v;
+            lo = fminf(lo, v);
+            hi = fmaxf(hi, v);
+        }
+        mean[r] = s / (float)nmem;
+        if (spread) spread[r] = hi - lo;
+    }
+}
+
+}  // namespace opb
+
+OPB_API long long opb_mlp_packed_bytes(void) { return MLP_PACK_BYTES; }
+
+OPB_API int opb_mlp_pack(const float *theta, void *packed) {
+    OPB_REQUIRE(theta && packed, OPB_E_NULL);
+    OPB_REQUIRE(aligned(packed, 16), OPB_E_ALIGN);
+    k_mlp_pack<<<grid_ew(3LL * 256 * 256), 256, 0, stream()>>>(theta, reinterpret_cast<uint8_t *>(packed));
+    return launch_check();
+}
+
+// Inference workspace bytes for n rows (n padded to a multiple of 128 internally).
+OPB_API long long opb_mlp_infer_workspace_bytes(long long n, int nmem) {
+    const long long np = (n + 127) / 128 * 128;
+    return np * 64 * 2 + 2 * np * 256 * 2 + (long long)nmem * np * 4 + 1024;
+}
+
+// Ensemble inference on the tensor cores: members m = 0..nmem-1 with packed weights at
+// packed + m * member_stride bytes; X [n x 8] normalised features (FP32).  mean [n] and
+// spread [n] (optional) receive the ensemble mean and max - min of the member outputs.
+OPB_API int opb_mlp_infer(const void *packed, int nmem, long long member_stride, const float *X, long long n,
+                          void *ws, long long ws_bytes, float *mean, float *spread) {
+    OPB_REQUIRE(packed && X && ws && mean, OPB_E_NULL);
+    OPB_REQUIRE(nmem >= 1 && n >= 1 && member_stride >= MLP_PACK_BYTES, OPB_E_ARG);
+    OPB_REQUIRE(ws_bytes >= opb_mlp_infer_workspace_bytes(n, nmem), OPB_E_ARG);
+    OPB_REQUIRE(aligned(packed, 16) && member_stride % 16 == 0 && aligned(ws, 256), OPB_E_ALIGN);
+    cudaStream_t s = stream();
+    const long long np = (n + 127) / 128 * 128;
+    uint8_t *w8 = reinterpret_cast<uint8_t *>(ws);
+    __nv_bfloat16 *Xp = reinterpret_cast<__nv_bfloat16 *>(w8);
+    __nv_bfloat16 *Ha = reinterpret_cast<__nv_bfloat16 *>(w8 + np * 64 * 2);
+    __nv_bfloat16 *Hb = Ha + np * 256;
+    float *ym = reinterpret_cast<float *>(reinterpret_cast<uint8_t *>(Hb + np * 256));
+    MT((int)cudaMemsetAsync(Xp, 0, np * 64 * 2, s));
+    k_mlp_pad_input<<<grid_ew(n * 64), 256, 0, s>>>(n, X, Xp);
+    for (int m = 0; m < nmem; m++) {
+        const uint8_t *pk = reinterpret_cast<const uint8_t *>(packed) + (long long)m * member_stride;
+        const __nv_bfloat16 *W1 = reinterpret_cast<const __nv_bfloat16 *>(pk);
+        const __nv_bfloat16 *WH = reinterpret_cast<const __nv_bfloat16 *>(pk + MLP_PACK_W1);
+        const float *f = reinterpret_cast<const float *>(pk + MLP_PACK_W1 + 3 * MLP_PACK_WH);
+        MT(launch_tc_layer((int)np, 256, 64, Xp, 64, W1, 64, 1.f, f, Ha, 256, s));
+        MT(launch_tc_layer((int)np, 256, 256, Ha, 256, WH, 256, 1.f, f + 256, Hb, 256, s));
+        MT(launch_tc_layer((int)np, 256, 256, Hb, 256, WH + 65536, 256, 1.f, f + 512, Ha, 256, s));
+        MT(launch_tc_layer((int)np, 256, 256, Ha, 256, WH + 2 * 65536, 256, 1.f, f + 768, Hb, 256, s));
+        k_mlp_out_bf16<<<(int)((n * 32 + 255) / 256), 256, 0, s>>>(n, Hb, f + 1024, f + 1280, ym + (long long)m * n);
+    }
+    k_mlp_ensemble<<<grid_ew(n), 256, 0, s>>>(n, nmem, ym, mean, spread);
+    return launch_check();
+}

@@ -150,3 +150,21 @@ def test_mc_golden_fixture():
                               gold["paths"].shape[1], x=gold["x"], disc=float(gold["disc"]))
     assert np.array_equal(paths, gold["paths"])
     assert np.allclose(sums, gold["sums"], rtol=1e-12)
+
+
+def test_mlp_oracle_gradient_vs_finite_differences():
+    from oracle import mlp_oracle as M
+    _, n = M.layout()
+    assert n == 199937
+    rng = np.random.default_rng(0)
+    theta = rng.standard_normal(n) * 0.05
+    X = rng.uniform(-1, 1, (16, 8))
+    t = rng.standard_normal(16) * 0.1
+    _, g = M.loss_grad(theta, X, t)
+    for idx in rng.choice(n, 25, replace=False).tolist() + [n - 1, 0, 2048, 2048 + 256]:
+        h = 1e-6
+        tp, tm = theta.copy(), theta.copy()
+        tp[idx] += h
+        tm[idx] -= h
+        fd = (M.loss_grad(tp, X, t)[0] - M.loss_grad(tm, X, t)[0]) / (2 * h)
+        assert abs(fd - g[idx]) <= 1e-6 + 1e-5 * abs(fd), (idx, fd, g[idx])
