@@ -403,13 +403,17 @@ def run_mc(args):
     import torch
     from oplib_b200 import _lib
     from oplib_b200.model import Lattice, bind_stream, cumulative_rows, guide_table, mc_run
-    dev = torch.device("cuda", 0)
+    from oplib_b200.shard import allreduce_sums, path_range
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
     bind_stream(dev)
     stream = torch.cuda.current_stream(dev)
     lat = Lattice.local_vol(n=512, device=dev)
     plan = lat.plan(1 / 252, 2.0 ** -14)
-    npaths, nsteps = 1 << 20, 504
+    total_paths, nsteps = (1 << 20) * world, 504  # weak scaling: 2^20 paths per GPU
+    path0, npaths = path_range(total_paths, rank, world)
     disc = math.exp(-0.03 * nsteps / 252)
     nblk = _lib.load().opb_mc_scratch_blocks(npaths)
     scratch = torch.empty(2 * nblk, dtype=torch.float64, device=dev)
@@ -420,25 +424,33 @@ def run_mc(args):
             P = lat.kernel(1 / 252, 2.0 ** -14, mode="fp32", plan=plan)
             Cm = cumulative_rows(P)
             state["C"], state["g"] = Cm, guide_table(Cm, 64)
-        sums, _ = mc_run(state["C"], lat.y0, nsteps, 5489, npaths, guide=state["g"], x=lat.x, disc=disc,
-                         scratch=scratch)
-        state["sums"] = sums
+        sums, _ = mc_run(state["C"], lat.y0, nsteps, 5489, npaths, path0=path0, guide=state["g"], x=lat.x,
+                         disc=disc, scratch=scratch)
+        state["sums"] = allreduce_sums(sums)
 
     for _ in range(args.warmup):
         step()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
     ms = _time(step, args.steps, stream, torch)
     ms_mc = _time(lambda: step(False), args.steps, stream, torch)
-    sums = state["sums"].cpu().numpy() / npaths
-    samples = npaths * nsteps
+    if world > 1:
+        t = torch.tensor([ms, ms_mc], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_mc = float(t[0]), float(t[1])
+    sums = state["sums"].cpu().numpy() / total_paths
+    samples = total_paths * nsteps
     line = {"metric": "Monte Carlo path-steps/sec (MT19937 per path, inverse-CDF on FP32 cumulative rows)",
-            "value": round(samples / (ms * 1e-3), 1), "unit": "path-steps/s", "n_gpus": 1, "steps": args.steps,
+            "value": round(samples / (ms * 1e-3), 1), "unit": "path-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32 RNG + f32 compare", "data": "synthetic",
-            "config": {"workload": "LV(512) lattice, dt=1/252 step kernel, 2^20 paths x 504 steps, barrier 0.7 + "
-                                   "Asian, K=1", "paths": npaths, "steps_per_path": nsteps},
+            "config": {"workload": "LV(512) lattice, dt=1/252 step kernel, 2^20 paths per GPU x 504 steps, barrier "
+                                   "0.7 + Asian, K=1", "paths": total_paths, "steps_per_path": nsteps,
+                       "parallelism": f"path ranges x{world}, one all-reduce of 2 sums"},
             "mc_kernel_only": {"ms": round(ms_mc, 3), "path_steps_per_s": round(samples / (ms_mc * 1e-3), 1)},
             "prices": {"barrier_do_call": float(sums[0]), "asian_call": float(sums[1])}}
-    if args.cpu:
+    if args.cpu and rank == 0:
         from oracle import oracle_c as OC
         nth = os.cpu_count() or 1
         Cm = state["C"].cpu().numpy()
@@ -663,9 +675,24 @@ def main():
     ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
     args = ap.parse_args()
     if args.workload != "sv" and args.impl == "b200":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        if world > 1:
+            if args.workload != "mc":
+                raise SystemExit("only the sv and mc workloads run under torchrun")
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "batch": run_batch, "surrogate": run_surrogate}[
             args.workload]
-        print(json.dumps(fn(args)))
+        line = fn(args)
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps(line))
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
         return 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
