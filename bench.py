@@ -199,7 +199,7 @@ def run_b200(args, rank, world, local_rank):
         Ah = torch.empty(d, d, dtype=torch.bfloat16, device=dev).normal_(0, 1e-3)
         Al = torch.empty_like(Ah).normal_(0, 1e-6)
         X = torch.empty(d, d, dtype=torch.float32, device=dev).normal_()
-        rs = torch.empty(lib.opb_gemm_bf16x3_nparts(d) * d, dtype=torch.float64, device=dev)
+        rs = torch.empty(lib.opb_gemm_bf16x3_nparts(d, d) * d, dtype=torch.float64, device=dev)
         args_g = (d, d, d, Ah.data_ptr(), Al.data_ptr(), d, Ah.data_ptr(), Al.data_ptr(), d, 1.0, X.data_ptr(), 2.0,
                   X.data_ptr(), d, rs.data_ptr())
         for _ in range(3):
@@ -629,6 +629,35 @@ def run_surrogate(args):
             "final_train_mse": sur.history[-1][2]}
 
 
+def run_renorm(args):
+    """The FP64 row renormalisation + split kernel alone at size d (E-form with both
+    splits): algorithmic traffic 16 bytes per element (read 4, write 4 + 4 x 2) + the
+    row-sum partials."""
+    import torch
+    from oplib_b200 import _lib
+    from oplib_b200.model import bind_stream
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    bind_stream(dev)
+    d = args.d
+    X = torch.empty(d, d, dtype=torch.float32, device=dev).uniform_(0, 1e-3)
+    np_ = d // 128
+    part = torch.empty(np_ * d, dtype=torch.float64, device=dev).uniform_(0, 1e-3)
+    A = [torch.empty(d, d, dtype=torch.bfloat16, device=dev) for _ in range(4)]
+    f = lambda: _lib.call("opb_renorm_rows", d, X.data_ptr(), part.data_ptr(), np_, 0, *[a.data_ptr() for a in A], 0)
+    for _ in range(args.warmup):
+        f()
+    ms = _time(f, args.steps, torch.cuda.current_stream(dev), torch)
+    hbm, _, _, src = _peaks()
+    byts = 16.0 * d * d + 8.0 * np_ * d
+    gbs = byts / (ms * 1e-3) / 1e9
+    return {"metric": "FP64 renormalisation + split, achieved GB/s", "value": round(gbs, 1), "unit": "GB/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 -> bf16",
+            "data": "synthetic", "config": {"workload": f"k_renorm64 E-form with A and B splits, d={d}"},
+            "frac_of_peak": round(gbs / hbm, 4), "peak_source": src}
+
+
 def run_gemm(args):
     """The squaring GEMM alone (split-BF16, E-form: C = E.E + 2E in place) at size d."""
     import torch
@@ -642,7 +671,7 @@ def run_gemm(args):
     Ah = torch.empty(d, d, dtype=torch.bfloat16, device=dev).normal_(0, 1e-3)
     Al = torch.empty_like(Ah).normal_(0, 1e-6)
     X = torch.empty(d, d, dtype=torch.float32, device=dev).normal_()
-    rs = torch.empty(lib.opb_gemm_bf16x3_nparts(d) * d, dtype=torch.float64, device=dev)
+    rs = torch.empty(lib.opb_gemm_bf16x3_nparts(d, d) * d, dtype=torch.float64, device=dev)
     a = (d, d, d, Ah.data_ptr(), Al.data_ptr(), d, Ah.data_ptr(), Al.data_ptr(), d, 1.0, X.data_ptr(), 2.0,
          X.data_ptr(), d, rs.data_ptr())
     for _ in range(args.warmup):
@@ -670,7 +699,7 @@ def main():
     ap.add_argument("--train-lattices", type=int, default=2048)
     ap.add_argument("--members", type=int, default=4)
     ap.add_argument("--epochs", type=int, default=12)
-    ap.add_argument("--workload", default="sv", choices=["sv", "lv", "mc", "gemm", "batch", "surrogate"],
+    ap.add_argument("--workload", default="sv", choices=["sv", "lv", "mc", "gemm", "renorm", "batch", "surrogate"],
                     help="sv = the headline SV lattice solve; the others are secondary measurements")
     ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
     args = ap.parse_args()
@@ -685,7 +714,8 @@ def main():
             import torch.distributed as dist
             torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "batch": run_batch, "surrogate": run_surrogate}[
+        fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "renorm": run_renorm, "batch": run_batch,
+              "surrogate": run_surrogate}[
             args.workload]
         line = fn(args)
         if int(os.environ.get("RANK", "0")) == 0:

@@ -158,16 +158,24 @@ int opb_plan_interval(double maxdiag, double delta_t, double dt0, int *niter, do
 /* new: C = alpha*(Ahi*Bhi^T + Ahi*Blo^T + Alo*Bhi^T) + beta*Cin, row-major, K-major operands
  * (A: M x K, B: N x K), M % 128 == 0, N % 64 == 0, K % 64 == 0, 16-byte aligned; rowsum
  * (optional) receives FP64 row sums of C per N tile: rowsum[t*M + row],
- * t < opb_gemm_bf16x3_nparts(N).  Replaces the FP32 SIMT products of oplib/opcuda/ssqmm.cu. */
+ * t < opb_gemm_bf16x3_nparts(M, N).  Replaces the FP32 SIMT products of oplib/opcuda/ssqmm.cu. */
 typedef uint16_t opb_bf16; /* storage of one bfloat16 */
 int opb_gemm_bf16x3(int M, int N, int K, const opb_bf16 *Ahi, const opb_bf16 *Alo, long long lda,
                     const opb_bf16 *Bhi, const opb_bf16 *Blo, long long ldb, float alpha, const float *Cin,
                     float beta, float *C, long long ldc, double *rowsum);
-int opb_gemm_bf16x3_nparts(int N);
+int opb_gemm_bf16x3_nparts(int M, int N);
+/* new (tuning): force the output tile width (64, 128, 256) of single products; 0 = automatic */
+int opb_set_tile_n(int bn);
 /* new: the same product with FP16 parts (power-of-two-scaled splits; undo the scales in alpha) */
 int opb_gemm_f16x3(int M, int N, int K, const uint16_t *Ahi, const uint16_t *Alo, long long lda, const uint16_t *Bhi,
                    const uint16_t *Blo, long long ldb, float alpha, const float *Cin, float beta, float *C,
                    long long ldc, double *rowsum);
+/* new: FP64 row renormalisation of a source-major d x d FP32 matrix from row-sum partials
+ * partial[p*d + y] (p < nparts), with optional 16-bit splits (A row-major, B transposed);
+ * mode 0 E-form, 1 E-form in / P-form out, 2 P-form (no B); f16: FP16 parts of 2^15-scaled
+ * values instead of BF16; d % 64 == 0 (probability conservation, no reference counterpart) */
+int opb_renorm_rows(int d, float *X, const double *partial, int nparts, int mode, void *Ahi, void *Alo, void *Bhi,
+                    void *Blo, int f16);
 /* reads and clears the device error word of the tensor-core kernels (0 = none) */
 int opb_tc_error(void);
 

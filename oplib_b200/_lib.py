@@ -88,9 +88,11 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_plan_interval": (i32, [f64, f64, f64, C.POINTER(i32), C.POINTER(f64)]),
     # split-BF16 GEMM
     "opb_gemm_bf16x3": (i32, [i32, i32, i32, vp, vp, i64, vp, vp, i64, f32, vp, f32, vp, i64, vp]),
-    "opb_gemm_bf16x3_nparts": (i32, [i32]),
+    "opb_gemm_bf16x3_nparts": (i32, [i32, i32]),
+    "opb_set_tile_n": (i32, [i32]),
     "opb_gemm_f16x3": (i32, [i32, i32, i32, vp, vp, i64, vp, vp, i64, f32, vp, f32, vp, i64, vp]),
     "opb_tc_error": (i32, []),
+    "opb_renorm_rows": (i32, [i32, vp, vp, i32, i32, vp, vp, vp, vp, i32]),
     # lattice
     "opb_lattice_workspace_size": (ull, [i32, i32, i32]),
     "opb_lattice_solve": (i32, [C.POINTER(LatticeDesc), i32, vp, ull, vp, vp]),

@@ -477,16 +477,29 @@ static int make_map(CUtensorMap *m, const void *ptr, long long rows, long long K
     return r == CUDA_SUCCESS ? OPB_OK : OPB_E_ARG;
 }
 
+static int g_tile_override = 0;  // 0 = automatic
+
 int tc_gemm_tile_n(int N) {
+    if (g_tile_override && N % g_tile_override == 0) return g_tile_override;
     if (N % 256 == 0) return 256;
     if (N % 128 == 0) return 128;
     if (N % 64 == 0) return 64;
     return 0;
 }
 
-// Row-sum partials: one per 128-column group (64 for the 64-wide tile).
-int tc_gemm_nparts(int N) {
+// Tile width for a product of M rows: the widest that still gives every SM a tile,
+// else the narrowest that divides N (small-N products such as the pricing GEMM).
+static int tile_for(int M, int N) {
     int bn = tc_gemm_tile_n(N);
+    if (g_tile_override || !bn) return bn;
+    const int mt = M / TC_BM;
+    while (bn > 64 && (long long)mt * (N / bn) < num_sms() && N % (bn / 2) == 0) bn /= 2;
+    return bn;
+}
+
+// Row-sum partials: one per 128-column group (64 for the 64-wide tile).
+int tc_gemm_nparts(int M, int N) {
+    int bn = tile_for(M, N);
     if (!bn) return 0;
     return N / (bn < 128 ? bn : 128);
 }
@@ -602,7 +615,7 @@ int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, 
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
     int c = tc_gemm_check(a);
     if (c != OPB_OK) return c;
-    switch (tc_gemm_tile_n(a.N) * 2 + (a.f16 ? 1 : 0)) {
+    switch (tile_for(a.M, a.N) * 2 + (a.f16 ? 1 : 0)) {
         case 512: return launch_tc_impl<256, 2, false>(a, s);
         case 513: return launch_tc_impl<256, 2, true>(a, s);
         case 256: return launch_tc_impl<128, 3, false>(a, s);
@@ -641,7 +654,14 @@ OPB_API int opb_gemm_f16x3(int M, int N, int K, const uint16_t *Ahi, const uint1
     return set_status(launch_tc_gemm(a, stream()));
 }
 
-OPB_API int opb_gemm_bf16x3_nparts(int N) { return tc_gemm_nparts(N); }
+OPB_API int opb_gemm_bf16x3_nparts(int M, int N) { return tc_gemm_nparts(M, N); }
+
+// Tuning knob: force the output tile width (64, 128 or 256) of single products; 0 = automatic.
+OPB_API int opb_set_tile_n(int bn) {
+    OPB_REQUIRE(bn == 0 || bn == 64 || bn == 128 || bn == 256, OPB_E_ARG);
+    g_tile_override = bn;
+    return set_status(OPB_OK);
+}
 
 // Reads and clears the tensor-core kernels' device error word (0 = no bounded wait expired).
 OPB_API int opb_tc_error(void) {

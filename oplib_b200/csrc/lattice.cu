@@ -89,7 +89,7 @@ Bufs carve(Ws &w, int d, int nK, int mode) {
         b.Blo = w.take<__nv_bfloat16>(dd);
         b.GThi = w.take<__nv_bfloat16>((size_t)d * nK);
         b.GTlo = w.take<__nv_bfloat16>((size_t)d * nK);
-        int np = opb::tc_gemm_nparts(d);
+        int np = opb::tc_gemm_nparts(d, d);
         b.part = w.take<double>((size_t)(np > 0 ? np : 1) * d);
     } else {
         b.G = w.take<float>((size_t)d * nK);
@@ -175,7 +175,7 @@ int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s) {
 int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, cudaStream_t s, float *P_out,
              bool f16) {
     const int d = L.d, nK = L.nK;
-    const int np = opb::tc_gemm_nparts(d);
+    const int np = opb::tc_gemm_nparts(d, d);
     const float ss = f16 ? F16_SCALE : 0.f;                    // split scale of E / P parts
     const float unscale = f16 ? 1.f / (F16_SCALE * F16_SCALE) : 1.f;
     // E0 = dt*L in FP32 (FP64 arithmetic), then its splits

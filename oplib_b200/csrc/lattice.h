@@ -81,7 +81,7 @@ int tc_gemm_check(const TcGemmArgs &a);       // argument/alignment check, OPB_*
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s);
 int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, const __nv_bfloat16 *W,
                     long long ldw, float alpha, const float *bias, __nv_bfloat16 *H, long long ldh, cudaStream_t s);
-int tc_gemm_nparts(int N);                    // number of row-sum partials written
+int tc_gemm_nparts(int M, int N);             // number of row-sum partials written
 
 // Batched launches: problem descriptors and tensor maps live in device memory.
 struct TcProblem {

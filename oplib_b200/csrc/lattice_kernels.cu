@@ -578,3 +578,23 @@ OPB_API int opcuda_sekd_lambda(int d, uint64_t genPtr, float dt, uint64_t tpkerP
     OPB_REQUIRE(rPtr != 0 && lambdaPtr != 0, OPB_E_NULL);
     return sek_common(d, genPtr, dt, tpkerPtr, rPtr, lambdaPtr);
 }
+
+// Standalone FP64 row renormalisation (+ optional 16-bit splits) of a source-major d x d
+// FP32 matrix from row-sum partials partial[p * d + y], p < nparts.  mode: 0 = E-form,
+// 1 = E-form in / P-form out, 2 = P-form; f16: 0 BF16 parts, 1 FP16 parts of 2^15-scaled
+// values.  d % 64 == 0.
+OPB_API int opb_renorm_rows(int d, float *X, const double *partial, int nparts, int mode, void *Ahi, void *Alo,
+                            void *Bhi, void *Blo, int f16) {
+    OPB_REQUIRE(d > 0 && d % 64 == 0 && nparts >= 0 && mode >= 0 && mode <= 2, OPB_E_ARG);
+    OPB_REQUIRE(X && (nparts == 0 || partial), OPB_E_NULL);
+    OPB_REQUIRE((Ahi != nullptr) == (Alo != nullptr) && (Bhi != nullptr) == (Blo != nullptr), OPB_E_NULL);
+    OPB_REQUIRE(opb::aligned(X, 16) && (!Ahi || (opb::aligned(Ahi, 8) && opb::aligned(Alo, 8))) &&
+                    (!Bhi || (opb::aligned(Bhi, 8) && opb::aligned(Blo, 8))),
+                OPB_E_ALIGN);
+    dim3 g(d / 64, d / 64);
+    opb::k_renorm64<<<g, 256, 0, opb::stream()>>>(
+        d, X, partial, nparts, mode, reinterpret_cast<__nv_bfloat16 *>(Ahi), reinterpret_cast<__nv_bfloat16 *>(Alo),
+        mode == 2 ? nullptr : reinterpret_cast<__nv_bfloat16 *>(Bhi),
+        mode == 2 ? nullptr : reinterpret_cast<__nv_bfloat16 *>(Blo), f16 ? 32768.f : 0.f);
+    return opb::launch_check();
+}

@@ -115,8 +115,8 @@ def test_plan_interval_rule(lib):
 def test_workspace_sizes(lib):
     assert lib.opb_lattice_workspace_size(512, 64, 2) > 4 * 512 * 512 * 2
     assert lib.opb_lattice_workspace_size(0, 64, 2) == 0
-    assert lib.opb_gemm_bf16x3_nparts(6144) == 48  # one FP64 row-sum partial per 128 columns
-    assert lib.opb_gemm_bf16x3_nparts(384) == 3
+    assert lib.opb_gemm_bf16x3_nparts(6144, 6144) == 48  # one FP64 row-sum partial per 128 columns
+    assert lib.opb_gemm_bf16x3_nparts(384 * 128, 384) == 3
     assert lib.opb_sgemm4_task_size() == 48
     assert lib.opb_sgemv4_task_size() == 56
 

@@ -42,7 +42,7 @@ def test_bf16x3_gemm_matches_fp64_of_split(cuda, M, N, K):
     Bh, Bl, bh, bl = _split_dev(B, cuda)
     Cd = torch.from_numpy(Cin).to(cuda)
     Cout = torch.empty_like(Cd)
-    nparts = lib.opb_gemm_bf16x3_nparts(N)
+    nparts = lib.opb_gemm_bf16x3_nparts(M, N)
     rs = torch.empty(nparts * M, dtype=torch.float64, device=cuda)
     torch.cuda.synchronize()
     st = lib.opb_gemm_bf16x3(M, N, K, Ah.data_ptr(), Al.data_ptr(), K, Bh.data_ptr(), Bl.data_ptr(), K,

@@ -141,3 +141,51 @@ def test_workspace_too_small_is_rejected(cuda):
     q = torch.empty(2, 64, dtype=torch.float64, device=cuda)
     import ctypes as C
     assert _lib.load().opb_lattice_solve(C.byref(L), BF16X3, ws.data_ptr(), 1024, q.data_ptr(), None) == -1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode,f16", [(0, 0), (1, 0), (2, 0), (0, 1)])
+def test_renorm_rows_bit_exact(cuda, mode, f16):
+    """opb_renorm_rows against the same FP64 arithmetic on the host: sequential sum of the
+    partials, one reciprocal, (x - diag * sum) * inv (+1 on the diagonal for mode 1),
+    round to FP32, then the 16-bit splits (A row-major, B transposed)."""
+    from oplib_b200 import _lib
+    d, np_ = 192, 3
+    rng = np.random.default_rng(7 + mode + 10 * f16)
+    X0 = (rng.random((d, d)) * 1e-3).astype(np.float32)
+    part = rng.random((np_, d)) * (1e-2 if mode != 2 else 0.5)
+    X = torch.from_numpy(X0.copy()).cuda()
+    P = torch.from_numpy(part).cuda()
+    parts = [torch.zeros(d, d, dtype=torch.bfloat16, device="cuda") for _ in range(4)]
+    _lib.call("opb_renorm_rows", d, X.data_ptr(), P.data_ptr(), np_, mode, *[t.data_ptr() for t in parts], f16)
+    torch.cuda.synchronize()
+    s = np.zeros(d)
+    for p in range(np_):
+        s = s + part[p]
+    den = 1.0 + s if mode != 2 else s
+    inv = 1.0 / den
+    x = X0.astype(np.float64)
+    if mode != 2:
+        x = x - np.diag(s)
+    x = x * inv[:, None]
+    if mode == 1:
+        x = x + np.eye(d)
+    ref = x.astype(np.float32)
+    got = X.cpu().numpy()
+    assert np.array_equal(got, ref)
+    r = torch.from_numpy(ref)
+    if f16:
+        rs = r * 32768.0
+        hi = rs.to(torch.float16)
+        lo = (rs - hi.float()).to(torch.float16)
+        hi, lo = hi.view(torch.int16), lo.view(torch.int16)
+    else:
+        hi = r.to(torch.bfloat16)
+        lo = (r - hi.float()).to(torch.bfloat16)
+        hi, lo = hi.view(torch.int16), lo.view(torch.int16)
+    g = [t.view(torch.int16).cpu() for t in parts]
+    assert torch.equal(g[0], hi) and torch.equal(g[1], lo)
+    if mode != 2:
+        assert torch.equal(g[2], hi.T.contiguous()) and torch.equal(g[3], lo.T.contiguous())
+    else:
+        assert not g[2].any() and not g[3].any()
