@@ -166,6 +166,9 @@ int opb_gemm_bf16x3(int M, int N, int K, const opb_bf16 *Ahi, const opb_bf16 *Al
 int opb_gemm_bf16x3_nparts(int M, int N);
 /* new (tuning): force the output tile width (64, 128, 256) of single products; 0 = automatic */
 int opb_set_tile_n(int bn);
+/* new: tuning knob, K depth of a pipeline stage of 256-wide tiles: 64 (2 stages, 128-byte
+ * swizzle; default) or 32 (4 stages, 64-byte swizzle); results are identical */
+int opb_set_stage_k(int bk);
 /* new: the same product with FP16 parts (power-of-two-scaled splits; undo the scales in alpha) */
 int opb_gemm_f16x3(int M, int N, int K, const uint16_t *Ahi, const uint16_t *Alo, long long lda, const uint16_t *Bhi,
                    const uint16_t *Blo, long long ldb, float alpha, const float *Cin, float beta, float *C,

@@ -41,7 +41,7 @@ namespace opb {
 __device__ int g_tc_error = 0;
 
 constexpr int TC_BM = 128;
-constexpr int TC_BK = 64;  // 64 bf16 = 128 bytes = one swizzle row
+constexpr int TC_BK = 64;  // K granularity of the operands (64 bf16 = 128 bytes = one 128B swizzle row)
 constexpr unsigned long long TC_WAIT_NS = 4000000000ull;  // 4 s per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -89,15 +89,18 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// K-major, 128-byte swizzle UMMA shared-memory descriptor: 8-row core groups 1024 bytes
-// apart (SBO), LBO unused for swizzled K-major (1), descriptor version 1 (sm_100).
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+// K-major swizzled UMMA shared-memory descriptor for tiles whose rows are BK bf16 wide:
+// BK = 64 -> 128-byte swizzle (8-row core groups 1024 bytes apart), BK = 32 -> 64-byte
+// swizzle (512 bytes apart).  LBO is unused for swizzled K-major (1); version 1 (sm_100).
+template <int BK>
+__device__ __forceinline__ uint64_t umma_desc_sw(uint32_t saddr) {
+    static_assert(BK == 64 || BK == 32, "BK");
     uint64_t d = 0;
     d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
-    d |= (uint64_t)1 << 16;            // LBO
-    d |= (uint64_t)(1024 >> 4) << 32;  // SBO
-    d |= (uint64_t)1 << 46;            // version
-    d |= (uint64_t)2 << 61;            // SWIZZLE_128B
+    d |= (uint64_t)1 << 16;                   // LBO
+    d |= (uint64_t)((8 * BK * 2) >> 4) << 32;  // SBO: 8 rows of BK * 2 bytes
+    d |= (uint64_t)1 << 46;                   // version
+    d |= (uint64_t)(BK == 64 ? 2 : 4) << 61;  // SWIZZLE_128B / SWIZZLE_64B
     return d;
 }
 
@@ -135,10 +138,10 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-template <int BN, int STAGES, int NPROD = 3>
+template <int BN, int STAGES, int NPROD = 3, int BK = TC_BK>
 struct TcCfg {
-    static constexpr int A_BYTES = TC_BM * TC_BK * 2;  // one of Ahi/Alo
-    static constexpr int B_BYTES = BN * TC_BK * 2;     // one of Bhi/Blo
+    static constexpr int A_BYTES = TC_BM * BK * 2;  // one of Ahi/Alo
+    static constexpr int B_BYTES = BN * BK * 2;     // one of Bhi/Blo
     static constexpr int NPARTS = NPROD == 1 ? 1 : 2;  // parts loaded per operand
     static constexpr int STAGE_BYTES = NPARTS * (A_BYTES + B_BYTES);
     static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
@@ -147,7 +150,7 @@ struct TcCfg {
     static constexpr int EPI_WARPS = 4 * HALVES;            // epilogue warps (4 lane quadrants x groups)
     static constexpr int THREADS = 32 * (EPI_WARPS + 2);    // + TMA producer warp + MMA warp
     static constexpr int TMEM_COLS = 2 * BN;                // two accumulators (ping-pong chunks)
-    static constexpr int CHUNK = 2;                         // K-blocks accumulated in TMEM per chunk
+    static constexpr int CHUNK = 128 / BK;                  // K-blocks accumulated in TMEM per chunk (K = 128)
 };
 
 struct TcParams {
@@ -180,12 +183,12 @@ struct TcBatch {
 // into FP32 register sums (round to nearest) while the MMA warp fills the other
 // accumulator.  The tensor cores' truncating accumulation thus spans only 12*CHUNK MMA
 // instructions, and an item's final store overlaps the next item's MMAs.
-template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0>
-__global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD>::THREADS, 1)
+template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK>
+__global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
               const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p,
               TcBatch bt) {
-    using Cfg = TcCfg<BN, STAGES, NPROD>;
+    using Cfg = TcCfg<BN, STAGES, NPROD, BK>;
     constexpr int EPI = Cfg::EPI_WARPS;
     constexpr int CPT = Cfg::CPT;
     extern __shared__ uint8_t smem_raw[];
@@ -212,7 +215,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD>::THREADS, 1)
             prob = (int)(w >> 16);
             m0 = (int)((w >> 8) & 255u) * TC_BM;
             n0 = (int)(w & 255u) * BN;
-            nkb = bt.probs[prob].K / TC_BK;
+            nkb = bt.probs[prob].K / BK;
         } else {
             const int GM = 8;
             const int per_group = GM * ntiles_n;
@@ -223,7 +226,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD>::THREADS, 1)
             prob = 0;
             m0 = (first_m + r % gm) * TC_BM;
             n0 = (r / gm) * BN;
-            nkb = p.K / TC_BK;
+            nkb = p.K / BK;
         }
     };
 
@@ -274,7 +277,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD>::THREADS, 1)
                     }
                     const uint32_t st = base + s * Cfg::STAGE_BYTES;
                     mbar_expect_tx(full_bar(s), Cfg::STAGE_BYTES);
-                    const int kx = kb * TC_BK;
+                    const int kx = kb * BK;
                     tma_load_2d(st, mp[0], full_bar(s), kx, m0);
                     if constexpr (NPROD == 1) {
                         tma_load_2d(st + Cfg::A_BYTES, mp[2], full_bar(s), kx, n0);
@@ -322,12 +325,12 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD>::THREADS, 1)
                         }
                         tc_fence_after();
                         const uint32_t st = base + s * Cfg::STAGE_BYTES;
-                        const uint64_t dAh = umma_desc_sw128(st);
-                        const uint64_t dAl = umma_desc_sw128(st + Cfg::A_BYTES);
-                        const uint64_t dBh = umma_desc_sw128(st + Cfg::NPARTS * Cfg::A_BYTES);
-                        const uint64_t dBl = umma_desc_sw128(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES);
+                        const uint64_t dAh = umma_desc_sw<BK>(st);
+                        const uint64_t dAl = umma_desc_sw<BK>(st + Cfg::A_BYTES);
+                        const uint64_t dBh = umma_desc_sw<BK>(st + Cfg::NPARTS * Cfg::A_BYTES);
+                        const uint64_t dBl = umma_desc_sw<BK>(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES);
 #pragma unroll
-                        for (int k16 = 0; k16 < TC_BK / 16; k16++) {
+                        for (int k16 = 0; k16 < BK / 16; k16++) {
                             const uint64_t adv = (uint64_t)((k16 * 32) >> 4);  // +32 bytes along K
                             const uint32_t acc0 = (kb > c * Cfg::CHUNK || k16 > 0) ? 1u : 0u;
                             umma_bf16(dacc, dAh + adv, dBh + adv, idesc, acc0);
@@ -462,22 +465,25 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     return fn;
 }
 
-// rows x K bf16 row-major matrix (leading dimension ld elements), box = box_rows x 64.
+// rows x K bf16 row-major matrix (leading dimension ld elements), box = box_rows x bk
+// (bk = 64: 128-byte swizzle; bk = 32: 64-byte swizzle).
 static int make_map(CUtensorMap *m, const void *ptr, long long rows, long long K, long long ld, int box_rows,
-                    int f16 = 0) {
+                    int f16 = 0, int bk = TC_BK) {
     auto enc = get_encode();
     if (!enc) return OPB_E_UNSUPPORTED;
     cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
-    cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)bk, (cuuint32_t)box_rows};
     cuuint32_t es[2] = {1, 1};
     CUresult r = enc(m, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, es,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? OPB_OK : OPB_E_ARG;
 }
 
 static int g_tile_override = 0;  // 0 = automatic
+static int g_bk256 = 64;          // K depth of a pipeline stage for 256-wide tiles (32 or 64)
 
 int tc_gemm_tile_n(int N) {
     if (g_tile_override && N % g_tile_override == 0) return g_tile_override;
@@ -516,14 +522,14 @@ int tc_gemm_check(const TcGemmArgs &a) {
     return OPB_OK;
 }
 
-template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0>
+template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK>
 static int set_smem_attr() {
-    using Cfg = TcCfg<BN, STAGES, NPROD>;
+    using Cfg = TcCfg<BN, STAGES, NPROD, BK>;
     static bool attr_set[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED, F16, NPROD, EPIMODE>,
+        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED, F16, NPROD, EPIMODE, BK>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              Cfg::SMEM);
         if (e != cudaSuccess) return (int)e;
@@ -532,22 +538,22 @@ static int set_smem_attr() {
     return 0;
 }
 
-template <int BN, int STAGES, bool F16>
+template <int BN, int STAGES, bool F16, int BK = TC_BK>
 static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
-    using Cfg = TcCfg<BN, STAGES>;
-    int e0 = set_smem_attr<BN, STAGES, false, F16>();
+    using Cfg = TcCfg<BN, STAGES, 3, BK>;
+    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, BK>();
     if (e0) return e0;
     CUtensorMap mAh, mAl, mBh, mBl;
     int r;
-    if ((r = make_map(&mAh, a.Ahi, a.M, a.K, a.lda, TC_BM, F16)) != OPB_OK) return r;
-    if ((r = make_map(&mAl, a.Alo, a.M, a.K, a.lda, TC_BM, F16)) != OPB_OK) return r;
-    if ((r = make_map(&mBh, a.Bhi, a.N, a.K, a.ldb, BN, F16)) != OPB_OK) return r;
-    if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN, F16)) != OPB_OK) return r;
+    if ((r = make_map(&mAh, a.Ahi, a.M, a.K, a.lda, TC_BM, F16, BK)) != OPB_OK) return r;
+    if ((r = make_map(&mAl, a.Alo, a.M, a.K, a.lda, TC_BM, F16, BK)) != OPB_OK) return r;
+    if ((r = make_map(&mBh, a.Bhi, a.N, a.K, a.ldb, BN, F16, BK)) != OPB_OK) return r;
+    if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN, F16, BK)) != OPB_OK) return r;
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
     const int ntiles = (a.M / TC_BM) * (a.N / BN);
     const int grid = ntiles < num_sms() ? ntiles : num_sms();
     TcBatch none{nullptr, nullptr, nullptr, 0};
-    k_tc_gemm<BN, STAGES, false, F16><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl, p, none);
+    k_tc_gemm<BN, STAGES, false, F16, 3, 0, BK><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl, p, none);
     return (int)cudaGetLastError();
 }
 
@@ -616,8 +622,10 @@ int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
     int c = tc_gemm_check(a);
     if (c != OPB_OK) return c;
     switch (tile_for(a.M, a.N) * 2 + (a.f16 ? 1 : 0)) {
-        case 512: return launch_tc_impl<256, 2, false>(a, s);
-        case 513: return launch_tc_impl<256, 2, true>(a, s);
+        case 512:
+            return g_bk256 == 32 ? launch_tc_impl<256, 4, false, 32>(a, s) : launch_tc_impl<256, 2, false>(a, s);
+        case 513:
+            return g_bk256 == 32 ? launch_tc_impl<256, 4, true, 32>(a, s) : launch_tc_impl<256, 2, true>(a, s);
         case 256: return launch_tc_impl<128, 3, false>(a, s);
         case 257: return launch_tc_impl<128, 3, true>(a, s);
         case 128: return launch_tc_impl<64, 4, false>(a, s);
@@ -660,6 +668,14 @@ OPB_API int opb_gemm_bf16x3_nparts(int M, int N) { return tc_gemm_nparts(M, N); 
 OPB_API int opb_set_tile_n(int bn) {
     OPB_REQUIRE(bn == 0 || bn == 64 || bn == 128 || bn == 256, OPB_E_ARG);
     g_tile_override = bn;
+    return set_status(OPB_OK);
+}
+
+// Tuning knob: K depth of a pipeline stage of 256-wide tiles: 64 (2 stages of 96 KB,
+// 128-byte swizzle, the default) or 32 (4 stages of 48 KB, 64-byte swizzle).
+OPB_API int opb_set_stage_k(int bk) {
+    OPB_REQUIRE(bk == 32 || bk == 64, OPB_E_ARG);
+    g_bk256 = bk;
     return set_status(OPB_OK);
 }
 

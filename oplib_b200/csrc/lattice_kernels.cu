@@ -176,35 +176,53 @@ __global__ void k_renorm(int d, float *__restrict__ X, const double *__restrict_
     }
 }
 
-// Vectorised renormalisation of one 64 x 64 tile (d % 64 == 0), 256 threads: float4 loads
-// and stores of X, 8-byte stores of four BF16 parts, and the transposed parts staged
+// Vectorised renormalisation of 64 x 64 tiles (d % 64 == 0), 256 threads: float4 loads
+// and stores of X, 8-byte stores of four 16-bit parts, and the transposed parts staged
 // through shared memory so that every global access is a contiguous run per warp.
 // Modes: 0 = E-form in, E-form out; 1 = E-form in, P-form out (P = I + E_new: the last
 // squaring level); 2 = P-form in and out.  nparts = 0 skips the scaling (pure split).
+// Each (hi, lo) pair is one 32-bit shared word; the 65-word row stride keeps both the
+// row-wise stores and the column-wise reads of the transpose at most 2-way bank-conflicted.
 struct RenormSmem {
     double s_sum[64], s_inv[64];
-    __nv_bfloat16 th[64][72], tl[64][72];
+    uint32_t t[64][65];
 };
 
 __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) {
     return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
 }
 
-__device__ __forceinline__ void renorm64_tile(RenormSmem &sm, int d, float *__restrict__ X,
-                                              const double *__restrict__ partial, int nparts, int mode,
-                                              __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
-                                              __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo,
-                                              int r0, int c0, float sscale) {
+// FP64 row sums of rows r0..r0+63 over the nparts partials, summed in part order (the
+// loads are issued 8 at a time; the additions stay sequential), and their reciprocals.
+__device__ __forceinline__ void renorm64_sums(RenormSmem &sm, int d, const double *__restrict__ partial, int nparts,
+                                              int mode, int r0) {
     const int tid = threadIdx.x;
-    const bool eform = mode != 2;
     if (tid < 64) {
         double s = 0.0;
-        const int r = r0 + tid;
-        for (int p = 0; p < nparts; p++) s += partial[(long long)p * d + r];
+        const double *q = partial + r0 + tid;
+        int p = 0;
+        for (; p + 8 <= nparts; p += 8) {
+            double v[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) v[j] = q[(long long)(p + j) * d];
+#pragma unroll
+            for (int j = 0; j < 8; j++) s += v[j];
+        }
+        for (; p < nparts; p++) s += q[(long long)p * d];
         sm.s_sum[tid] = s;
-        const double den = nparts == 0 ? 1.0 : (eform ? 1.0 + s : s);
+        const double den = nparts == 0 ? 1.0 : (mode != 2 ? 1.0 + s : s);
         sm.s_inv[tid] = den != 0.0 ? 1.0 / den : 0.0;
     }
+}
+
+// One tile at (r0, c0), using the sums of renorm64_sums.  Starts with a barrier, so it can
+// follow renorm64_sums or a previous tile of the same rows directly.
+__device__ __forceinline__ void renorm64_apply(RenormSmem &sm, int d, float *__restrict__ X, int mode,
+                                               __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
+                                               __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo,
+                                               int r0, int c0, float sscale) {
+    const int tid = threadIdx.x;
+    const bool eform = mode != 2;
     __syncthreads();
     const int lc = (tid & 15) * 4;
 #pragma unroll
@@ -225,8 +243,7 @@ __device__ __forceinline__ void renorm64_tile(RenormSmem &sm, int d, float *__re
             if (mode == 1 && diag) x += 1.0;
             f[j] = (float)x;
             split2(f[j], h[j], l[j], sscale);
-            sm.th[lr][lc + j] = h[j];
-            sm.tl[lr][lc + j] = l[j];
+            sm.t[lr][lc + j] = pack_bf16(h[j], l[j]);
         }
         *reinterpret_cast<float4 *>(X + o) = make_float4(f[0], f[1], f[2], f[3]);
         if (Ahi) {
@@ -240,19 +257,33 @@ __device__ __forceinline__ void renorm64_tile(RenormSmem &sm, int d, float *__re
     for (int pass = 0; pass < 4; pass++) {
         const int orow = pass * 16 + (tid >> 4);
         const long long o = (long long)(c0 + orow) * d + r0 + lc;
-        *reinterpret_cast<uint2 *>(Bhi + o) = make_uint2(pack_bf16(sm.th[lc + 0][orow], sm.th[lc + 1][orow]),
-                                                         pack_bf16(sm.th[lc + 2][orow], sm.th[lc + 3][orow]));
-        *reinterpret_cast<uint2 *>(Blo + o) = make_uint2(pack_bf16(sm.tl[lc + 0][orow], sm.tl[lc + 1][orow]),
-                                                         pack_bf16(sm.tl[lc + 2][orow], sm.tl[lc + 3][orow]));
+        const uint32_t w0 = sm.t[lc + 0][orow], w1 = sm.t[lc + 1][orow], w2 = sm.t[lc + 2][orow],
+                       w3 = sm.t[lc + 3][orow];
+        *reinterpret_cast<uint2 *>(Bhi + o) = make_uint2(__byte_perm(w0, w1, 0x5410), __byte_perm(w2, w3, 0x5410));
+        *reinterpret_cast<uint2 *>(Blo + o) = make_uint2(__byte_perm(w0, w1, 0x7632), __byte_perm(w2, w3, 0x7632));
     }
 }
 
+// Grid (column chunks, d / 64): block (bx, by) renormalises rows 64*by.. over the column
+// tiles bx, bx + gridDim.x, ...; the row sums are formed once per block.
 __global__ void __launch_bounds__(256) k_renorm64(int d, float *__restrict__ X, const double *__restrict__ partial,
                                                   int nparts, int mode, __nv_bfloat16 *__restrict__ Ahi,
                                                   __nv_bfloat16 *__restrict__ Alo, __nv_bfloat16 *__restrict__ Bhi,
                                                   __nv_bfloat16 *__restrict__ Blo, float sscale) {
     __shared__ RenormSmem sm;
-    renorm64_tile(sm, d, X, partial, nparts, mode, Ahi, Alo, Bhi, Blo, blockIdx.y * 64, blockIdx.x * 64, sscale);
+    const int r0 = blockIdx.y * 64;
+    renorm64_sums(sm, d, partial, nparts, mode, r0);
+    for (int tc = blockIdx.x; tc < d / 64; tc += gridDim.x)
+        renorm64_apply(sm, d, X, mode, Ahi, Alo, Bhi, Blo, r0, tc * 64, sscale);
+}
+
+// Column chunks of a k_renorm64 launch: about 8 resident blocks per SM in total.
+static dim3 renorm64_grid(int d) {
+    const int nt = d / 64;
+    int chunks = (8 * num_sms() + nt - 1) / nt;
+    if (chunks > nt) chunks = nt;
+    if (chunks < 1) chunks = 1;
+    return dim3(chunks, nt);
 }
 
 // Batched: one block per work item (problem << 16 | mode << 14 | tile_r << 7 | tile_c);
@@ -265,8 +296,10 @@ __global__ void __launch_bounds__(256) k_renorm64_batched(const RenormProblem *_
     const RenormProblem &pr = probs[w >> 16];
     const int mode = (int)((w >> 14) & 3u);
     const int nparts = parts_div > 0 ? pr.d / parts_div : 0;
-    renorm64_tile(sm, pr.d, pr.X, pr.partial, nparts, mode, pr.Ahi, pr.Alo, mode == 2 ? nullptr : pr.Bhi,
-                  mode == 2 ? nullptr : pr.Blo, (int)((w >> 7) & 127u) * 64, (int)(w & 127u) * 64, sscale);
+    const int r0 = (int)((w >> 7) & 127u) * 64;
+    renorm64_sums(sm, pr.d, pr.partial, nparts, mode, r0);
+    renorm64_apply(sm, pr.d, pr.X, mode, pr.Ahi, pr.Alo, mode == 2 ? nullptr : pr.Bhi, mode == 2 ? nullptr : pr.Blo,
+                   r0, (int)(w & 127u) * 64, sscale);
 }
 
 // Batched ELL scatter into zeroed dense E-form matrices: thread per global ELL slot
@@ -403,8 +436,7 @@ int launch_rowsum(int d, const float *X, double *partial, cudaStream_t s) {
 int launch_renorm(int d, float *X, const double *partial, int nparts, int eform, __nv_bfloat16 *Ahi,
                   __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale) {
     if (d % 64 == 0 && (Ahi != nullptr) == (Alo != nullptr)) {
-        dim3 g(d / 64, d / 64);
-        k_renorm64<<<g, 256, 0, s>>>(d, X, partial, nparts, eform ? 0 : 2, Ahi, Alo, Bhi, Blo, sscale);
+        k_renorm64<<<renorm64_grid(d), 256, 0, s>>>(d, X, partial, nparts, eform ? 0 : 2, Ahi, Alo, Bhi, Blo, sscale);
         return (int)cudaGetLastError();
     }
     dim3 g((d + 31) / 32, (d + 31) / 32);
@@ -416,8 +448,7 @@ int launch_renorm(int d, float *X, const double *partial, int nparts, int eform,
 int launch_renorm_to_p(int d, float *X, const double *partial, int nparts, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
                        __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale) {
     if (d % 64) return OPB_E_UNSUPPORTED;
-    dim3 g(d / 64, d / 64);
-    k_renorm64<<<g, 256, 0, s>>>(d, X, partial, nparts, 1, Ahi, Alo, Bhi, Blo, sscale);
+    k_renorm64<<<renorm64_grid(d), 256, 0, s>>>(d, X, partial, nparts, 1, Ahi, Alo, Bhi, Blo, sscale);
     return (int)cudaGetLastError();
 }
 
@@ -591,8 +622,7 @@ OPB_API int opb_renorm_rows(int d, float *X, const double *partial, int nparts, 
     OPB_REQUIRE(opb::aligned(X, 16) && (!Ahi || (opb::aligned(Ahi, 8) && opb::aligned(Alo, 8))) &&
                     (!Bhi || (opb::aligned(Bhi, 8) && opb::aligned(Blo, 8))),
                 OPB_E_ALIGN);
-    dim3 g(d / 64, d / 64);
-    opb::k_renorm64<<<g, 256, 0, opb::stream()>>>(
+    opb::k_renorm64<<<opb::renorm64_grid(d), 256, 0, opb::stream()>>>(
         d, X, partial, nparts, mode, reinterpret_cast<__nv_bfloat16 *>(Ahi), reinterpret_cast<__nv_bfloat16 *>(Alo),
         mode == 2 ? nullptr : reinterpret_cast<__nv_bfloat16 *>(Bhi),
         mode == 2 ? nullptr : reinterpret_cast<__nv_bfloat16 *>(Blo), f16 ? 32768.f : 0.f);

@@ -62,6 +62,37 @@ def test_bf16x3_gemm_matches_fp64_of_split(cuda, M, N, K):
         assert np.allclose(parts[t], got[:, t * bn:(t + 1) * bn].sum(axis=1), rtol=1e-12, atol=1e-9)
 
 
+@pytest.mark.parametrize("M,N,K", [(256, 256, 512), (384, 768, 320), (1024, 512, 2048)])
+def test_stage_depth_gives_identical_results(cuda, M, N, K):
+    """256-wide tiles with 32-deep (4-stage, 64-byte swizzle) and 64-deep (2-stage,
+    128-byte swizzle) pipeline stages issue the same MMAs in the same order: the
+    outputs and row sums are bit-identical."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(K)
+    A = rng.random((M, K)).astype(np.float32)
+    B = rng.random((N, K)).astype(np.float32)
+    Ah, Al, _, _ = _split_dev(A, cuda)
+    Bh, Bl, _, _ = _split_dev(B, cuda)
+    Cd = torch.from_numpy(rng.standard_normal((M, N)).astype(np.float32)).to(cuda)
+    nparts = lib.opb_gemm_bf16x3_nparts(M, N)
+    outs = []
+    try:
+        for bk in (32, 64):
+            assert lib.opb_set_stage_k(bk) == 0
+            Cout = torch.empty_like(Cd)
+            rs = torch.empty(nparts * M, dtype=torch.float64, device=cuda)
+            assert lib.opb_gemm_bf16x3(M, N, K, Ah.data_ptr(), Al.data_ptr(), K, Bh.data_ptr(), Bl.data_ptr(), K,
+                                       1.0, Cd.data_ptr(), 1.0, Cout.data_ptr(), N, rs.data_ptr()) == 0
+            torch.cuda.synchronize()
+            outs.append((Cout.cpu(), rs.cpu()))
+    finally:
+        lib.opb_set_stage_k(64)
+    assert lib.opb_tc_error() == 0
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+    assert lib.opb_set_stage_k(48) != 0
+
+
 def _f16_dev(a32, dev):
     return torch.from_numpy(np.ascontiguousarray(a32, dtype=np.float16).view(np.int16)).to(dev)
 
