@@ -214,9 +214,15 @@ def run_b200(args, rank, world, local_rank):
         k_ms = e0.elapsed_time(e1) / n_rep
         mma_flops = 3 * 2.0 * d ** 3
         achieved = mma_flops / (k_ms * 1e-3) / 1e12
+        # DRAM bytes (read + write) of one launch of this kernel at d = 6144 from an ncu
+        # capture (dram__bytes_read.sum 930.5 MB + dram__bytes_write.sum 138.5 MB); the
+        # algorithmic traffic is 4 BF16 parts + Cin read, C written = 16 d^2 + 8 d^2 bytes.
+        traffic = 1069.0e6 if d == 6144 else None
         kern = {"bound": "tensor", "achieved": round(achieved, 1), "peak": bf16_burst, "unit": "TFLOP/s",
-                "frac": round(achieved / bf16_burst, 4), "traffic": None, "peak_source": f"{src} burst bf16",
-                "kernel": "k_tc_gemm<256,2> (E-form squaring, 6144^3 x 3 BF16 products)",
+                "frac": round(achieved / bf16_burst, 4), "traffic": traffic, "traffic_unit": "DRAM bytes per launch",
+                "algorithmic_bytes": 24.0 * d * d, "peak_source": f"{src} burst bf16",
+                "kernel": "k_tc_gemm<256,3,pair> (E-form squaring on 2-CTA clusters, cta_group::2, "
+                          f"{d}^3 x 3 BF16 products)",
                 "avg_launch_ms": round(k_ms, 4), "useful_tflops": round(achieved / 3, 1)}
         del Ah, Al, X, rs
     else:

@@ -169,6 +169,10 @@ int opb_set_tile_n(int bn);
 /* new: tuning knob, K depth of a pipeline stage of 256-wide tiles: 64 (2 stages, 128-byte
  * swizzle; default) or 32 (4 stages, 64-byte swizzle); results are identical */
 int opb_set_stage_k(int bk);
+/* new: tuning knob, 256 x 256 output tiles on 2-CTA clusters (cta_group::2 MMAs over both
+ * CTAs' shared memory) for products with M % 256 == 0: 1 = on (default), 0 = off;
+ * results are identical */
+int opb_set_cta_pair(int on);
 /* new: the same product with FP16 parts (power-of-two-scaled splits; undo the scales in alpha) */
 int opb_gemm_f16x3(int M, int N, int K, const uint16_t *Ahi, const uint16_t *Alo, long long lda, const uint16_t *Bhi,
                    const uint16_t *Blo, long long ldb, float alpha, const float *Cin, float beta, float *C,

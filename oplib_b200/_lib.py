@@ -93,6 +93,7 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_gemm_f16x3": (i32, [i32, i32, i32, vp, vp, i64, vp, vp, i64, f32, vp, f32, vp, i64, vp]),
     "opb_tc_error": (i32, []),
     "opb_set_stage_k": (i32, [i32]),
+    "opb_set_cta_pair": (i32, [i32]),
     "opb_renorm_rows": (i32, [i32, vp, vp, i32, i32, vp, vp, vp, vp, i32]),
     # lattice
     "opb_lattice_workspace_size": (ull, [i32, i32, i32]),

@@ -21,6 +21,12 @@
 //                        tile's last chunk, the alpha/beta update, FP32 stores and FP64
 //                        row sums of the stored values (rowsum[group * M + row], one per
 //                        128 columns, used by the row renormalisation).
+// CTA pairs (the default for M % 256 == 0 with 256-wide tiles): a 2-CTA cluster owns a
+// 256 x 256 output tile; each CTA loads its own 128 rows of A and 128 rows of B (3-stage
+// 64 KB ring per CTA, both CTAs' copies counted on the even CTA's full barrier), the even
+// CTA's MMA lane issues tcgen05.mma.cta_group::2 (M = 256) over both CTAs' shared memory
+// into each CTA's own TMEM, and its commits arrive on both CTAs' barriers.  Operand bytes
+// through shared memory per MMA flop drop by a third against one CTA per 128 x 256 tile.
 // The tensor cores truncate their FP32 accumulator (about half an ulp per MMA); chunked
 // accumulation bounds that bias by 24 MMAs instead of 3K/16.
 // Every mbarrier wait is bounded by a %globaltimer deadline; on expiry the kernel records
@@ -105,10 +111,10 @@ __device__ __forceinline__ uint64_t umma_desc_sw(uint32_t saddr) {
 }
 
 // kind::f16 instruction descriptor: D = F32, A = B = BF16 (format 1) or F16 (format 0),
-// both K-major, N, M = 128.
-__host__ __device__ constexpr uint32_t umma_idesc_16(int n, bool f16) {
+// both K-major, N, M (128 for one CTA, 256 for a CTA pair).
+__host__ __device__ constexpr uint32_t umma_idesc_16(int n, bool f16, int m = TC_BM) {
     return (1u << 4) | ((f16 ? 0u : 1u) << 7) | ((f16 ? 0u : 1u) << 10) | ((uint32_t)(n >> 3) << 17) |
-           ((uint32_t)(TC_BM >> 4) << 24);
+           ((uint32_t)(m >> 4) << 24);
 }
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -125,6 +131,53 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
+// ---- CTA-pair (cta_group::2) forms: one 256 x N MMA over the shared memory of both CTAs
+// of a 2-CTA cluster, issued by the even CTA; each CTA's tensor memory holds its 128 rows.
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// Address of the same shared variable in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t map_to_rank(uint32_t saddr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+// Tiled load into this CTA's shared memory whose completion is counted on an mbarrier
+// that may live in the peer CTA (the pair leader's).  No multicast.
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap *map, uint32_t bar_cluster, int x,
+                                                 int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_cluster), "r"(x), "r"(y)
+        : "memory");
+}
+__device__ __forceinline__ void umma_bf16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                               uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+// Arrive on the mbarrier at this offset in both CTAs of the pair once the pair's MMAs
+// issued so far have completed.
+__device__ __forceinline__ void umma_commit_pair(uint32_t bar) {
+    const uint16_t mask = 3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(bar),
+        "h"(mask)
+        : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -138,10 +191,12 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-template <int BN, int STAGES, int NPROD = 3, int BK = TC_BK>
+template <int BN, int STAGES, int NPROD = 3, int BK = TC_BK, bool PAIR = false>
 struct TcCfg {
-    static constexpr int A_BYTES = TC_BM * BK * 2;  // one of Ahi/Alo
-    static constexpr int B_BYTES = BN * BK * 2;     // one of Bhi/Blo
+    static constexpr int A_BYTES = TC_BM * BK * 2;                  // one of Ahi/Alo
+    static constexpr int B_ROWS = PAIR ? BN / 2 : BN;               // B rows held by this CTA
+    static constexpr int B_BYTES = B_ROWS * BK * 2;                 // one of Bhi/Blo
+    static constexpr int TILE_M = PAIR ? 2 * TC_BM : TC_BM;         // output rows per work item
     static constexpr int NPARTS = NPROD == 1 ? 1 : 2;  // parts loaded per operand
     static constexpr int STAGE_BYTES = NPARTS * (A_BYTES + B_BYTES);
     static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
@@ -183,12 +238,14 @@ struct TcBatch {
 // into FP32 register sums (round to nearest) while the MMA warp fills the other
 // accumulator.  The tensor cores' truncating accumulation thus spans only 12*CHUNK MMA
 // instructions, and an item's final store overlaps the next item's MMAs.
-template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK>
-__global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
+template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK,
+          bool PAIR = false>
+__global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
               const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p,
               TcBatch bt) {
-    using Cfg = TcCfg<BN, STAGES, NPROD, BK>;
+    using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR>;
+    static_assert(!(PAIR && BATCHED), "pair mode is for single products");
     constexpr int EPI = Cfg::EPI_WARPS;
     constexpr int CPT = Cfg::CPT;
     extern __shared__ uint8_t smem_raw[];
@@ -206,8 +263,12 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
     volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * STAGES + 6);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int mtiles = p.M / TC_BM, ntiles_n = p.N / BN;
+    const int mtiles = p.M / Cfg::TILE_M, ntiles_n = p.N / BN;
     const int nitems = BATCHED ? bt.nwork : mtiles * ntiles_n;
+    // pair mode: rank within the 2-CTA cluster, items walked per cluster
+    const uint32_t rank = PAIR ? cluster_rank() : 0u;
+    const int item0 = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    const int istep = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
     // item t -> (problem, m0, n0, K-blocks)
     auto get_item = [&](int t, int &prob, int &m0, int &n0, int &nkb) {
         if constexpr (BATCHED) {
@@ -224,7 +285,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
             const int gm = min(mtiles - first_m, GM);
             const int r = t - group * per_group;
             prob = 0;
-            m0 = (first_m + r % gm) * TC_BM;
+            m0 = (first_m + r % gm) * Cfg::TILE_M;
             n0 = (r / gm) * BN;
             nkb = p.K / BK;
         }
@@ -237,7 +298,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
         }
         for (int a = 0; a < 2; a++) {
             mbar_init(accf_bar(a), 1);
-            mbar_init(acce_bar(a), EPI * 32);
+            mbar_init(acce_bar(a), PAIR ? 2 * EPI : EPI * 32);  // pair: one lane per epilogue warp of both CTAs
         }
         mbar_init(drain_bar, 1);
         *abort_flag = 0;
@@ -246,13 +307,21 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
     }
     if (warp == 0) {
         const uint32_t slot = smem_u32(const_cast<uint32_t *>(tmem_slot));
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
-                     "r"(Cfg::TMEM_COLS)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        if constexpr (PAIR) {
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+                         "r"(Cfg::TMEM_COLS)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+                         "r"(Cfg::TMEM_COLS)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
     }
     tc_fence_before();
     __syncthreads();
+    if constexpr (PAIR) cluster_sync_all();  // both CTAs' barriers initialised before any cross-CTA signal
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
@@ -261,9 +330,11 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
             // ---------------- TMA producer
             long kbg = 0;  // K-blocks issued over the CTA's lifetime (stage ring position)
             bool ok = true;
-            for (int t = blockIdx.x; t < nitems && ok; t += gridDim.x) {
+            for (int t = item0; t < nitems && ok; t += istep) {
                 int prob, m0, n0, nkb;
                 get_item(t, prob, m0, n0, nkb);
+                const int ma = m0 + (int)rank * TC_BM;          // this CTA's A rows
+                const int nb = n0 + (int)rank * Cfg::B_ROWS;    // this CTA's B rows
                 const CUtensorMap *mp[4] = {&mAhi, &mAlo, &mBhi, &mBlo};
                 if constexpr (BATCHED) {
                     for (int i = 0; i < 4; i++) mp[i] = bt.maps + 4 * prob + i;
@@ -276,35 +347,49 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
                         break;
                     }
                     const uint32_t st = base + s * Cfg::STAGE_BYTES;
-                    mbar_expect_tx(full_bar(s), Cfg::STAGE_BYTES);
                     const int kx = kb * BK;
-                    tma_load_2d(st, mp[0], full_bar(s), kx, m0);
-                    if constexpr (NPROD == 1) {
-                        tma_load_2d(st + Cfg::A_BYTES, mp[2], full_bar(s), kx, n0);
+                    if constexpr (PAIR) {
+                        // both CTAs' copies complete on the leader's full barrier
+                        if (rank == 0) mbar_expect_tx(full_bar(s), 2 * Cfg::STAGE_BYTES);
+                        const uint32_t fb = map_to_rank(full_bar(s), 0);
+                        tma_load_2d_pair(st, mp[0], fb, kx, ma);
+                        tma_load_2d_pair(st + Cfg::A_BYTES, mp[1], fb, kx, ma);
+                        tma_load_2d_pair(st + 2 * Cfg::A_BYTES, mp[2], fb, kx, nb);
+                        tma_load_2d_pair(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, mp[3], fb, kx, nb);
                     } else {
-                        tma_load_2d(st + Cfg::A_BYTES, mp[1], full_bar(s), kx, m0);
-                        tma_load_2d(st + 2 * Cfg::A_BYTES, mp[2], full_bar(s), kx, n0);
-                        tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, mp[3], full_bar(s), kx, n0);
+                        mbar_expect_tx(full_bar(s), Cfg::STAGE_BYTES);
+                        tma_load_2d(st, mp[0], full_bar(s), kx, ma);
+                        if constexpr (NPROD == 1) {
+                            tma_load_2d(st + Cfg::A_BYTES, mp[2], full_bar(s), kx, nb);
+                        } else {
+                            tma_load_2d(st + Cfg::A_BYTES, mp[1], full_bar(s), kx, ma);
+                            tma_load_2d(st + 2 * Cfg::A_BYTES, mp[2], full_bar(s), kx, nb);
+                            tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, mp[3], full_bar(s), kx, nb);
+                        }
                     }
                 }
             }
             if (!ok) {
                 atomicExch(&g_tc_error, 1);
                 *abort_flag = 1;
+                // wait (bounded) for the copies in flight; in pair mode they complete on the
+                // leader's barriers, and the closing cluster barrier keeps this CTA resident
+                // until the leader has drained them
                 const long first = kbg > STAGES ? kbg - STAGES : 0;
-                for (long k = first; k < kbg; k++)
-                    (void)mbar_wait(full_bar((int)(k % STAGES)), (uint32_t)((k / STAGES) & 1), abort_flag,
-                                    100000000ull);
+                if (!PAIR || rank == 0)
+                    for (long k = first; k < kbg; k++)
+                        (void)mbar_wait(full_bar((int)(k % STAGES)), (uint32_t)((k / STAGES) & 1), abort_flag,
+                                        100000000ull);
             }
         }
         __syncwarp();
     } else if (warp == EPI + 1) {
-        if (lane == 0) {
-            // ---------------- MMA issuer
-            const uint32_t idesc = umma_idesc_16(BN, F16);
+        if (lane == 0 && rank == 0) {
+            // ---------------- MMA issuer (pair mode: the even CTA issues for both)
+            const uint32_t idesc = umma_idesc_16(BN, F16, Cfg::TILE_M);
             long kbg = 0, g = 0;  // K-blocks consumed, chunks issued
             bool ok = true;
-            for (int t = blockIdx.x; t < nitems && ok; t += gridDim.x) {
+            for (int t = item0; t < nitems && ok; t += istep) {
                 int prob, m0, n0, nkb;
                 get_item(t, prob, m0, n0, nkb);
                 const int nch = (nkb + Cfg::CHUNK - 1) / Cfg::CHUNK;
@@ -333,22 +418,34 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
                         for (int k16 = 0; k16 < BK / 16; k16++) {
                             const uint64_t adv = (uint64_t)((k16 * 32) >> 4);  // +32 bytes along K
                             const uint32_t acc0 = (kb > c * Cfg::CHUNK || k16 > 0) ? 1u : 0u;
-                            umma_bf16(dacc, dAh + adv, dBh + adv, idesc, acc0);
-                            if constexpr (NPROD == 3) {
-                                umma_bf16(dacc, dAh + adv, dBl + adv, idesc, 1u);
-                                umma_bf16(dacc, dAl + adv, dBh + adv, idesc, 1u);
+                            if constexpr (PAIR) {
+                                umma_bf16_pair(dacc, dAh + adv, dBh + adv, idesc, acc0);
+                                umma_bf16_pair(dacc, dAh + adv, dBl + adv, idesc, 1u);
+                                umma_bf16_pair(dacc, dAl + adv, dBh + adv, idesc, 1u);
+                            } else {
+                                umma_bf16(dacc, dAh + adv, dBh + adv, idesc, acc0);
+                                if constexpr (NPROD == 3) {
+                                    umma_bf16(dacc, dAh + adv, dBl + adv, idesc, 1u);
+                                    umma_bf16(dacc, dAl + adv, dBh + adv, idesc, 1u);
+                                }
                             }
                         }
-                        umma_commit(empty_bar(s));
+                        if constexpr (PAIR) umma_commit_pair(empty_bar(s));
+                        else umma_commit(empty_bar(s));
                     }
-                    if (ok) umma_commit(accf_bar(a));
+                    if (ok) {
+                        if constexpr (PAIR) umma_commit_pair(accf_bar(a));
+                        else umma_commit(accf_bar(a));
+                    }
                 }
             }
             if (!ok) {
                 atomicExch(&g_tc_error, 2);
                 *abort_flag = 1;
             }
-            umma_commit(drain_bar);  // arrives once every issued MMA has completed
+            // arrives once every issued MMA has completed
+            if constexpr (PAIR) umma_commit_pair(drain_bar);
+            else umma_commit(drain_bar);
             (void)mbar_wait(drain_bar, 0, abort_flag, TC_WAIT_NS);
         }
         __syncwarp();
@@ -359,7 +456,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
         float sum[CPT];
         long g = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < nitems && ok; t += gridDim.x) {
+        for (int t = item0; t < nitems && ok; t += istep) {
             int prob, m0, n0, nkb;
             get_item(t, prob, m0, n0, nkb);
             const int nch = (nkb + Cfg::CHUNK - 1) / Cfg::CHUNK;
@@ -381,7 +478,12 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
                     for (int i = 0; i < 32; i++) sum[32 * j + i] = __fadd_rn(sum[32 * j + i], __uint_as_float(v[i]));
                 }
                 tc_fence_before();
-                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acce_bar(a)) : "memory");
+                if constexpr (PAIR) {
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive_remote(map_to_rank(acce_bar(a), 0));
+                } else {
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acce_bar(a)) : "memory");
+                }
             }
             if (!ok || *abort_flag) break;
             float *C;
@@ -396,7 +498,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
             } else {
                 C = p.C; Cin = p.Cin; ldc = p.ldc; alpha = p.alpha; beta = p.beta; rowsum = p.rowsum; M = p.M;
             }
-            const int row = m0 + q * 32 + lane;
+            const int row = m0 + (int)rank * TC_BM + q * 32 + lane;
             const int col0 = n0 + h * CPT;
             if constexpr (EPIMODE == 1) {
                 // network layer: BF16 GELU(alpha * acc + bias), 8 values per 16-byte store
@@ -443,10 +545,15 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK>::THREADS, 1)
     }
     tc_fence_before();
     __syncthreads();
+    if constexpr (PAIR) cluster_sync_all();  // the leader's MMAs have drained before either CTA frees or exits
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS)
-                     : "memory");
+        if constexpr (PAIR)
+            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS)
+                         : "memory");
+        else
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cfg::TMEM_COLS)
+                         : "memory");
     }
 }
 
@@ -484,6 +591,7 @@ static int make_map(CUtensorMap *m, const void *ptr, long long rows, long long K
 
 static int g_tile_override = 0;  // 0 = automatic
 static int g_bk256 = 64;          // K depth of a pipeline stage for 256-wide tiles (32 or 64)
+static int g_pair = 1;            // 256 x 256 tiles on CTA pairs (cta_group::2) when M % 256 == 0
 
 int tc_gemm_tile_n(int N) {
     if (g_tile_override && N % g_tile_override == 0) return g_tile_override;
@@ -522,14 +630,15 @@ int tc_gemm_check(const TcGemmArgs &a) {
     return OPB_OK;
 }
 
-template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK>
+template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK,
+          bool PAIR = false>
 static int set_smem_attr() {
-    using Cfg = TcCfg<BN, STAGES, NPROD, BK>;
+    using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR>;
     static bool attr_set[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED, F16, NPROD, EPIMODE, BK>,
+        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED, F16, NPROD, EPIMODE, BK, PAIR>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              Cfg::SMEM);
         if (e != cudaSuccess) return (int)e;
@@ -555,6 +664,54 @@ static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
     TcBatch none{nullptr, nullptr, nullptr, 0};
     k_tc_gemm<BN, STAGES, false, F16, 3, 0, BK><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl, p, none);
     return (int)cudaGetLastError();
+}
+
+// 256 x 256 output tiles on 2-CTA clusters: each CTA loads its 128 rows of A and 128 rows
+// of B, the even CTA issues cta_group::2 MMAs over both CTAs' shared memory.  The grid is
+// as many clusters as can be resident at once (at most one per SM pair).
+template <bool F16>
+static int launch_tc_pair(const TcGemmArgs &a, cudaStream_t s) {
+    constexpr int BN = 256, STAGES = 3;
+    using Cfg = TcCfg<BN, STAGES, 3, TC_BK, true>;
+    auto kern = k_tc_gemm<BN, STAGES, false, F16, 3, 0, TC_BK, true>;
+    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, TC_BK, true>();
+    if (e0) return e0;
+    CUtensorMap mAh, mAl, mBh, mBl;
+    int r;
+    if ((r = make_map(&mAh, a.Ahi, a.M, a.K, a.lda, TC_BM, F16)) != OPB_OK) return r;
+    if ((r = make_map(&mAl, a.Alo, a.M, a.K, a.lda, TC_BM, F16)) != OPB_OK) return r;
+    if ((r = make_map(&mBh, a.Bhi, a.N, a.K, a.ldb, BN / 2, F16)) != OPB_OK) return r;
+    if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN / 2, F16)) != OPB_OK) return r;
+    TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
+    TcBatch none{nullptr, nullptr, nullptr, 0};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(Cfg::THREADS);
+    cfg.dynamicSmemBytes = Cfg::SMEM;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    static int max_clusters[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return OPB_E_UNSUPPORTED;
+    if (!max_clusters[dev]) {
+        cfg.gridDim = dim3(2 * (num_sms() / 2));
+        int n = 0;
+        cudaError_t e = cudaOccupancyMaxActiveClusters(&n, kern, &cfg);
+        if (e != cudaSuccess) return (int)e;
+        if (n <= 0) return OPB_E_UNSUPPORTED;
+        max_clusters[dev] = n;
+    }
+    const int ntiles = (a.M / (2 * TC_BM)) * (a.N / BN);
+    const int nclusters = ntiles < max_clusters[dev] ? ntiles : max_clusters[dev];
+    cfg.gridDim = dim3(2 * nclusters);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, mAh, mAl, mBh, mBl, p, none);
+    return e == cudaSuccess ? (int)cudaGetLastError() : (int)e;
 }
 
 int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo, long long M, long long lda,
@@ -623,8 +780,10 @@ int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
     if (c != OPB_OK) return c;
     switch (tile_for(a.M, a.N) * 2 + (a.f16 ? 1 : 0)) {
         case 512:
+            if (g_pair && a.M % (2 * TC_BM) == 0) return launch_tc_pair<false>(a, s);
             return g_bk256 == 32 ? launch_tc_impl<256, 4, false, 32>(a, s) : launch_tc_impl<256, 2, false>(a, s);
         case 513:
+            if (g_pair && a.M % (2 * TC_BM) == 0) return launch_tc_pair<true>(a, s);
             return g_bk256 == 32 ? launch_tc_impl<256, 4, true, 32>(a, s) : launch_tc_impl<256, 2, true>(a, s);
         case 256: return launch_tc_impl<128, 3, false>(a, s);
         case 257: return launch_tc_impl<128, 3, true>(a, s);
@@ -676,6 +835,14 @@ OPB_API int opb_set_tile_n(int bn) {
 OPB_API int opb_set_stage_k(int bk) {
     OPB_REQUIRE(bk == 32 || bk == 64, OPB_E_ARG);
     g_bk256 = bk;
+    return set_status(OPB_OK);
+}
+
+// Tuning knob: 256 x 256 tiles on CTA pairs (cta_group::2) for products with M % 256 == 0
+// and 256-wide tiles: 1 = on (default), 0 = off (one CTA per 128 x 256 tile).
+OPB_API int opb_set_cta_pair(int on) {
+    OPB_REQUIRE(on == 0 || on == 1, OPB_E_ARG);
+    g_pair = on;
     return set_status(OPB_OK);
 }
 

@@ -78,6 +78,7 @@ def test_stage_depth_gives_identical_results(cuda, M, N, K):
     nparts = lib.opb_gemm_bf16x3_nparts(M, N)
     outs = []
     try:
+        assert lib.opb_set_cta_pair(0) == 0  # stage depth applies to the one-CTA kernel
         for bk in (32, 64):
             assert lib.opb_set_stage_k(bk) == 0
             Cout = torch.empty_like(Cd)
@@ -88,9 +89,49 @@ def test_stage_depth_gives_identical_results(cuda, M, N, K):
             outs.append((Cout.cpu(), rs.cpu()))
     finally:
         lib.opb_set_stage_k(64)
+        lib.opb_set_cta_pair(1)
     assert lib.opb_tc_error() == 0
     assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
     assert lib.opb_set_stage_k(48) != 0
+
+
+@pytest.mark.parametrize("M,N,K", [(256, 256, 128), (512, 256, 512), (768, 512, 320), (1024, 1024, 2048)])
+def test_cta_pair_gemm_matches_fp64_of_split(cuda, M, N, K):
+    """256 x 256 tiles on 2-CTA clusters (cta_group::2): within the same FP32 bound as the
+    one-CTA kernel, and row sums of the stored values per 128 columns."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(M * 7 + K)
+    A = rng.random((M, K)).astype(np.float32)
+    B = rng.random((N, K)).astype(np.float32)
+    Cin = rng.standard_normal((M, N)).astype(np.float32)
+    Ah, Al, ah, al = _split_dev(A, cuda)
+    Bh, Bl, bh, bl = _split_dev(B, cuda)
+    Cd = torch.from_numpy(Cin).to(cuda)
+    nparts = lib.opb_gemm_bf16x3_nparts(M, N)
+    outs = []
+    try:
+        for pair in (1, 0):
+            assert lib.opb_set_cta_pair(pair) == 0
+            Cout = torch.empty_like(Cd)
+            rs = torch.empty(nparts * M, dtype=torch.float64, device=cuda)
+            assert lib.opb_gemm_bf16x3(M, N, K, Ah.data_ptr(), Al.data_ptr(), K, Bh.data_ptr(), Bl.data_ptr(), K,
+                                       0.5, Cd.data_ptr(), 2.0, Cout.data_ptr(), N, rs.data_ptr()) == 0
+            torch.cuda.synchronize()
+            assert lib.opb_tc_error() == 0
+            outs.append((Cout.cpu().numpy().astype(np.float64), rs.cpu().numpy().reshape(nparts, M)))
+    finally:
+        lib.opb_set_cta_pair(1)
+    ref = 0.5 * (ah @ bh.T + ah @ bl.T + al @ bh.T) + 2.0 * Cin.astype(np.float64)
+    scale = 0.5 * (np.abs(ah) + np.abs(al)) @ (np.abs(bh) + np.abs(bl)).T + 2 * np.abs(Cin)
+    bound = (3 * 128 / 16 + 8) * 2.0 ** -24
+    got, parts = outs[0]
+    assert np.all(np.abs(got - ref) <= bound * scale + 1e-30), np.max(np.abs(got - ref) / scale)
+    assert np.array_equal(got, outs[1][0])  # the same MMAs in the same order as one CTA per tile
+    bn = N // nparts
+    for t in range(nparts):
+        assert np.allclose(parts[t], got[:, t * bn:(t + 1) * bn].sum(axis=1), rtol=1e-12, atol=1e-9)
+    assert lib.opb_set_cta_pair(2) != 0
 
 
 def _f16_dev(a32, dev):
