@@ -147,6 +147,13 @@ int opcuda_sglvg(uint64_t gen_yy_i, int ni, int d, uint64_t invmat, uint64_t par
 int opb_lv_params(int d, double lo, double hi, double s0, double level, double skew, double width, double floor_,
                   double r, double *x, double *drift, double *vol);
 int opb_lv_generator_ell(int d, const double *x, const double *drift, const double *vol, int *cols, double *vals);
+/* new: LV generators of nlat lattices in one launch into concatenated ELL arrays (calibration
+ * loops); params = device array of nlat 56-byte records {int n, pad; long long row_off;
+ * double level, skew, width, floor, rate}; entries bit-identical to opb_lv_params +
+ * opb_lv_generator_ell per lattice (batched form of oplib/opcuda/sglvg.cu:42-99) */
+int opb_lv_generator_ell_batched(int nlat, const void *params, long long total_rows, double lo, double hi, double s0,
+                                 int *cols, double *vals);
+int opb_lv_param_size(void);
 int opb_sv_generator_ell(int nx, int nv, double x_lo, double x_hi, double v_lo, double v_hi, double r, double kappa,
                          double theta, double xi, double rho, int *cols, double *vals, double *x_y);
 int opb_ell_maxdiag(int d, int w, const int *cols, const double *vals, unsigned long long *dscratch,

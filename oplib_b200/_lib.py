@@ -92,6 +92,8 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_set_tile_n": (i32, [i32]),
     "opb_gemm_f16x3": (i32, [i32, i32, i32, vp, vp, i64, vp, vp, i64, f32, vp, f32, vp, i64, vp]),
     "opb_tc_error": (i32, []),
+    "opb_lv_generator_ell_batched": (i32, [i32, vp, i64, f64, f64, f64, vp, vp]),
+    "opb_lv_param_size": (i32, []),
     "opb_set_stage_k": (i32, [i32]),
     "opb_set_cta_pair": (i32, [i32]),
     "opb_renorm_rows": (i32, [i32, vp, vp, i32, i32, vp, vp, vp, vp, i32]),

@@ -23,17 +23,36 @@
 
 namespace opb {
 
+// The moment-matching solve of one interior node: rates pm (down) and pp (up) with
+// pm dm + pp dp = a and pm dm^2 + pp dp^2 = b.  Every operation is rounded explicitly
+// (no contraction into FMAs), so all kernels that build LV rows agree bit for bit.
+__device__ __forceinline__ void lv_rates(double dm, double dp, double a, double b, double &pm, double &pp) {
+    const double det = __dsub_rn(__dmul_rn(__dmul_rn(dm, dp), dp), __dmul_rn(__dmul_rn(dp, dm), dm));
+    pm = __ddiv_rn(__dsub_rn(__dmul_rn(__dmul_rn(dp, dp), a), __dmul_rn(dp, b)), det);
+    pp = __ddiv_rn(__dadd_rn(__dmul_rn(__dmul_rn(-dm, dm), a), __dmul_rn(dm, b)), det);
+}
+
+// sigma(x) = max(floor, level + skew*exp(-((x-1)/width)^2)), explicitly rounded.
+__device__ __forceinline__ double lv_sigma_at(double xv, double level, double skew, double width, double floor_) {
+    const double z = __ddiv_rn(__dsub_rn(xv, 1.0), width);
+    double sg = __dadd_rn(level, __dmul_rn(skew, exp(-__dmul_rn(z, z))));
+    return sg > floor_ ? sg : floor_;
+}
+
+// x_i = s0*lo*(hi/lo)^(i/(n-1)).
+__device__ __forceinline__ double lv_node(int n, double lo, double hi, double s0, int y) {
+    return __dmul_rn(__dmul_rn(s0, lo), pow(__ddiv_rn(hi, lo), __ddiv_rn((double)y, (double)(n - 1))));
+}
+
 __global__ void k_lv_ell(int d, const double *__restrict__ x, const double *__restrict__ drift,
                          const double *__restrict__ vol, int *__restrict__ cols, double *__restrict__ vals) {
     int y = blockIdx.x * blockDim.x + threadIdx.x;
     if (y >= d) return;
     double pm = 0.0, pp = 0.0;
     if (y > 0 && y < d - 1) {
-        const double dm = x[y - 1] - x[y], dp = x[y + 1] - x[y];
-        const double a = drift[y], v = vol[y], b = v * v;
-        const double det = dm * dp * dp - dp * dm * dm;
-        pm = (dp * dp * a - dp * b) / det;
-        pp = (-dm * dm * a + dm * b) / det;
+        const double dm = __dsub_rn(x[y - 1], x[y]), dp = __dsub_rn(x[y + 1], x[y]);
+        const double v = vol[y];
+        lv_rates(dm, dp, drift[y], __dmul_rn(v, v), pm, pp);
     }
     int *c = cols + 3LL * y;
     double *v = vals + 3LL * y;
@@ -52,13 +71,48 @@ __global__ void k_lv_params(int d, double lo, double hi, double s0, double level
                             double *__restrict__ vol) {
     int y = blockIdx.x * blockDim.x + threadIdx.x;
     if (y >= d) return;
-    double xv = s0 * lo * pow(hi / lo, (double)y / (double)(d - 1));
-    double z = (xv - 1.0) / width;
-    double sg = level + skew * exp(-z * z);
-    sg = sg > floor_ ? sg : floor_;
+    const double xv = lv_node(d, lo, hi, s0, y);
     x[y] = xv;
-    drift[y] = r * xv;
-    vol[y] = sg * xv;
+    drift[y] = __dmul_rn(r, xv);
+    vol[y] = __dmul_rn(lv_sigma_at(xv, level, skew, width, floor_), xv);
+}
+
+// Many LV lattices in one launch (calibration loops): thread per global row; lattice i
+// owns rows row_off .. row_off + n - 1 of the concatenated ELL arrays.  The arithmetic is
+// k_lv_params followed by k_lv_ell, node by node, so the entries are bit-identical.
+struct LvParam {
+    int n, pad;
+    long long row_off;
+    double level, skew, width, floor_, rate;
+};
+
+__global__ void k_lv_ell_batched(int nlat, const LvParam *__restrict__ P, long long total_rows, double lo, double hi,
+                                 double s0, int *__restrict__ cols, double *__restrict__ vals) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (g >= total_rows) return;
+    int a = 0, b = nlat - 1;
+    while (a < b) {  // last lattice with row_off <= g
+        const int mid = (a + b + 1) >> 1;
+        if (P[mid].row_off <= g) a = mid; else b = mid - 1;
+    }
+    const LvParam p = P[a];
+    const int d = p.n, y = (int)(g - p.row_off);
+    double pm = 0.0, pp = 0.0;
+    if (y > 0 && y < d - 1) {
+        const double xv = lv_node(d, lo, hi, s0, y);
+        const double v = __dmul_rn(lv_sigma_at(xv, p.level, p.skew, p.width, p.floor_), xv);
+        const double dm = __dsub_rn(lv_node(d, lo, hi, s0, y - 1), xv);
+        const double dp = __dsub_rn(lv_node(d, lo, hi, s0, y + 1), xv);
+        lv_rates(dm, dp, __dmul_rn(p.rate, xv), __dmul_rn(v, v), pm, pp);
+    }
+    int *c = cols + 3LL * g;
+    double *v = vals + 3LL * g;
+    c[0] = y > 0 ? y - 1 : -1;
+    v[0] = y > 0 ? pm : 0.0;
+    c[1] = y;
+    v[1] = -((y > 0 ? pm : 0.0) + (y < d - 1 ? pp : 0.0));
+    c[2] = y < d - 1 ? y + 1 : -1;
+    v[2] = y < d - 1 ? pp : 0.0;
 }
 
 struct SvArgs {
@@ -188,6 +242,22 @@ OPB_API int opb_lv_generator_ell(int d, const double *x, const double *drift, co
     k_lv_ell<<<(d + 255) / 256, 256, 0, stream()>>>(d, x, drift, vol, cols, vals);
     return launch_check();
 }
+
+// LV generators of nlat lattices in one launch, into concatenated ELL arrays (width 3).
+// params: device array of nlat records {int n, pad; int64 row_off; double level, skew,
+// width, floor, rate} (56 bytes), row_off ascending from 0; total_rows = sum of n.
+OPB_API int opb_lv_generator_ell_batched(int nlat, const void *params, long long total_rows, double lo, double hi,
+                                         double s0, int *cols, double *vals) {
+    OPB_REQUIRE(nlat > 0 && total_rows >= 3 && lo > 0.0 && hi > lo && s0 > 0.0, OPB_E_ARG);
+    OPB_REQUIRE(params && cols && vals, OPB_E_NULL);
+    OPB_REQUIRE(aligned(params, 8), OPB_E_ALIGN);
+    const long long g = (total_rows + 255) / 256;
+    k_lv_ell_batched<<<(unsigned)g, 256, 0, stream()>>>(nlat, reinterpret_cast<const LvParam *>(params), total_rows,
+                                                      lo, hi, s0, cols, vals);
+    return launch_check();
+}
+
+OPB_API int opb_lv_param_size(void) { return (int)sizeof(LvParam); }
 
 // SV generator in ELL form (width 7); x_y (optional) receives the spot value per state.
 OPB_API int opb_sv_generator_ell(int nx, int nv, double x_lo, double x_hi, double v_lo, double v_hi, double r,
