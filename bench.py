@@ -619,10 +619,11 @@ def run_batch(args):
 
 def run_surrogate(args):
     """Config 4: ensemble of MLP surrogates (8 -> 256 x 4 -> 1, GELU) trained by the
-    library's kernels on ~2^21 quotes that the batched lattice solver generates, then
-    inference on 2^20 held-out quotes on the tensor cores; quotes whose ensemble spread
-    exceeds 5 bp fall back to the lattice.  Reports surrogate quotes/s, the lattice's
-    quotes/s for the same family, fallback rate and errors against the lattice."""
+    library's kernels on ~2^21 quotes that the batched lattice solver generates (local-vol
+    lattices, n = 1024), then inference on 2^20 held-out quotes on the tensor cores;
+    quotes whose ensemble spread exceeds 5 bp fall back to the lattice.  Reports surrogate
+    quotes/s, the lattice's quotes/s for the same family, fallback rate and errors
+    against the lattice."""
     import torch
     from oplib_b200.model import Batch, bind_stream
     from oplib_b200.surrogate import NMAT, PERIOD, LM, Surrogate, lattice_quotes
@@ -655,8 +656,9 @@ def run_surrogate(args):
     # lattice throughput for the same family (one 512-lattice sweep of the test distribution)
     from oplib_b200.model import Lattice
     rng = np.random.default_rng(7)
-    lats = [Lattice.local_vol(n=int(rng.choice(np.arange(256, 1025, 128))), level=0.25, skew=0.1, width=0.5,
-                              rate=0.02, floor=0.01, device=dev) for _ in range(512)]
+    lats = [Lattice.local_vol(n=1024, level=float(rng.uniform(0.1, 0.4)), skew=float(rng.uniform(-0.3, 0.3)),
+                              width=float(rng.uniform(0.2, 1.0)), rate=float(rng.uniform(0.0, 0.05)), floor=0.01,
+                              device=dev) for _ in range(512)]
     bt = Batch(lats, np.exp(LM), NMAT, PERIOD, 2.0 ** -14, mode="fp16x3", autotune=True)
     qq = bt.execute()
     g = _graph(lambda: bt.execute(qq), dev, torch)
@@ -684,6 +686,7 @@ def run_surrogate(args):
             "all_err_bp": {"rms": round(float(err.pow(2).mean().sqrt().item()), 2), "p99": round(q(err, 0.99), 2)},
             "baseline_err_bp": {"rms": round(float(errb.pow(2).mean().sqrt().item()), 2), "p99": round(q(errb, 0.99), 2)},
             "effective_quotes_per_s_with_fallback": round(n_test / eff_s, 1),
+            "spread_threshold_bp": 5.0,
             "train_seconds": round(sur.train_seconds, 1), "data_seconds": round(t_data, 1),
             "final_train_mse": sur.history[-1][2]}
 
@@ -756,9 +759,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu", action="store_false")
     ap.add_argument("--nlat", type=int, default=None,
                     help="lattices for --workload batch (default 512), problems for --workload calibrate (default 64)")
-    ap.add_argument("--train-lattices", type=int, default=2048)
+    ap.add_argument("--train-lattices", type=int, default=2600, help="~2^21 training quotes after the vega filter")
     ap.add_argument("--members", type=int, default=4)
-    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--workload", default="sv",
                     choices=["sv", "lv", "mc", "gemm", "renorm", "batch", "surrogate", "calibrate"],
                     help="sv = the headline SV lattice solve; the others are secondary measurements")

@@ -147,6 +147,15 @@ int sgemm_rm_t(bool ta, bool tb, int M, int N, int K, float alpha, const float *
     return sgemm_rowmajor(a, 1, s, ta, tb);
 }
 
+int sgemm_rm_strided(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, int lda, long long sA,
+                     const float *B, int ldb, long long sB, float beta, float *C, int ldc, long long sC, int batch,
+                     cudaStream_t s) {
+    SgemmArgs a{};
+    a.M = M; a.N = N; a.K = K; a.lda = lda; a.ldb = ldb; a.ldc = ldc;
+    a.alpha = alpha; a.beta = beta; a.A = A; a.B = B; a.C = C; a.sA = sA; a.sB = sB; a.sC = sC;
+    return sgemm_rowmajor(a, batch, s, ta, tb);
+}
+
 // Convenience: row-major, unbatched.
 int sgemm_rm(int M, int N, int K, float alpha, const float *A, int lda, const float *B, int ldb,
              float beta, float *C, int ldc, cudaStream_t s) {

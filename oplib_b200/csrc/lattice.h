@@ -13,6 +13,11 @@ int sgemm_rm(int M, int N, int K, float alpha, const float *A, int lda, const fl
              float *C, int ldc, cudaStream_t s);
 int sgemm_rm_t(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, int lda, const float *B, int ldb,
                float beta, float *C, int ldc, cudaStream_t s);
+// Strided-batch form: batch entries z use A + z*sA, B + z*sB, C + z*sC (row-major roles as
+// in sgemm_rm_t); grid (N/128, M/128, batch).
+int sgemm_rm_strided(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, int lda, long long sA,
+                     const float *B, int ldb, long long sB, float beta, float *C, int ldc, long long sC, int batch,
+                     cudaStream_t s);
 
 // lattice_kernels.cu
 int launch_ek_ell(int d, int w, const int *cols, const double *vals, double dt, int eform, float *out,

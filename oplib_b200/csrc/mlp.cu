@@ -217,9 +217,16 @@ using namespace opb;
 namespace {
 
 struct MlpWs {  // training workspace carve (floats)
-    float *Z[4], *H[4], *dZ, *dH, *y, *dy;
+    float *Z[4], *H[4], *dZ, *dH, *y, *dy, *part;
     double *loss;
 };
+
+// Weight gradients reduce over the batch (K = B): split into at most MLP_KSPLIT chunks,
+// one batched SIMT launch over the chunks, then a fixed-order sum of the partials, so
+// that the reduction keeps every SM busy and stays deterministic.
+constexpr int MLP_KSPLIT = 32;
+
+int grid_ew(long long n);
 
 MlpWs carve_mlp(float *ws, int B) {
     MlpWs w{};
@@ -232,9 +239,42 @@ MlpWs carve_mlp(float *ws, int B) {
     w.dH = ws + o; o += (size_t)B * MLP_H;
     w.y = ws + o; o += (size_t)B;
     w.dy = ws + o; o += (size_t)B;
+    o = (o + 3) & ~size_t(3);
+    w.part = ws + o; o += (size_t)MLP_KSPLIT * MLP_H * MLP_H;
     o = (o + 1) & ~size_t(1);
     w.loss = reinterpret_cast<double *>(ws + o);
     return w;
+}
+
+__global__ void k_sum_parts(int nparts, long long n, const float *__restrict__ part, float *__restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float acc = 0.f;
+        for (int p = 0; p < nparts; p++) acc += part[p * n + i];
+        out[i] = acc;
+    }
+}
+
+// dW[out x in] = dZ[B x out]^T . in[B x in], split over the batch.
+int mlp_weight_grad(int out, int in, int B, const float *dZ, const float *X, float *dW, float *part,
+                    cudaStream_t s) {
+    int nch = (B + 63) / 64;
+    if (nch > MLP_KSPLIT) nch = MLP_KSPLIT;
+    const int kc = (B + nch - 1) / nch;
+    const int full = B / kc, rem = B - full * kc;
+    const long long n = (long long)out * in;
+    if (full > 0) {
+        int r = sgemm_rm_strided(true, false, out, in, kc, 1.f, dZ, out, (long long)kc * out, X, in,
+                                 (long long)kc * in, 0.f, part, in, n, full, s);
+        if (r) return r;
+    }
+    if (rem > 0) {
+        int r = sgemm_rm_t(true, false, out, in, rem, 1.f, dZ + (long long)full * kc * out, out,
+                           X + (long long)full * kc * in, in, 0.f, part + (long long)full * n, in, s);
+        if (r) return r;
+    }
+    const int np = full + (rem > 0 ? 1 : 0);
+    k_sum_parts<<<grid_ew(n), 256, 0, s>>>(np, n, part, dW);
+    return (int)cudaGetLastError();
 }
 
 int grid_ew(long long n) {
@@ -268,7 +308,9 @@ int mlp_forward(const float *thb, const float *X, int B, MlpWs &w, cudaStream_t 
 OPB_API int opb_mlp_param_count(void) { return MLP_NPARAM; }
 
 // floats of training workspace for batch B
-OPB_API long long opb_mlp_workspace_floats(int B) { return 10LL * B * MLP_H + 2LL * B + 8; }
+OPB_API long long opb_mlp_workspace_floats(int B) {
+    return 10LL * B * MLP_H + 2LL * B + 4 + (long long)MLP_KSPLIT * MLP_H * MLP_H + 8;
+}
 
 OPB_API int opb_mlp_init(float *theta, unsigned long long seed) {
     OPB_REQUIRE(theta, OPB_E_NULL);
@@ -318,8 +360,7 @@ OPB_API int opb_mlp_loss_grad(const float *thb, const float *X, const float *t, 
         k_gelu_back<<<grid_ew(tot), 256, 0, s>>>(tot, w.Z[l], w.dH, w.dZ);
         // dW = dZ^T . in  (A = dZ stored B x out: the TA form)
         const float *in = l > 0 ? w.H[l - 1] : X;
-        MT(sgemm_rm_t(true, false, L.out[l], L.in[l], B, 1.f, w.dZ, L.out[l], in, L.in[l], 0.f, grad + L.w[l],
-                      L.in[l], s));
+        MT(mlp_weight_grad(L.out[l], L.in[l], B, w.dZ, in, grad + L.w[l], w.part, s));
         k_colsum<<<(L.out[l] + 31) / 32, 256, 0, s>>>(B, L.out[l], w.dZ, grad + L.b[l]);
         if (l > 0) MT(sgemm_rm_t(false, false, B, L.in[l], L.out[l], 1.f, w.dZ, L.out[l], thb + L.w[l], L.in[l], 0.f,
                                  w.dH, L.in[l], s));
