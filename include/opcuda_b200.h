@@ -154,6 +154,13 @@ int opb_lv_generator_ell(int d, const double *x, const double *drift, const doub
 int opb_lv_generator_ell_batched(int nlat, const void *params, long long total_rows, double lo, double hi, double s0,
                                  int *cols, double *vals);
 int opb_lv_param_size(void);
+/* oplib/opcuda/sgsvg.cu:215 (opcuda_sgsvg): two-dimensional generator with jumps across
+ * volatility levels, dense column-major FP32 [ni][d][d] (d = nx*nr, caller zeroes it) from the
+ * per-node 4x4 moment inverses invmat[16 d] (S2DGrid.pregen) and par = {x[d], sdrift, svol,
+ * voldrift, volvol, jump_minus, jump_plus, each [ni][d]} (FP32); FP64 arithmetic; the upper
+ * jump size is the upper block (the reference kernel reads the lower one for both) */
+int opcuda_sgsvg(unsigned long long gen_yyi_ptr, int ni, int nx, int nr, unsigned long long invmat_ptr,
+                 unsigned long long parptr);
 int opb_sv_generator_ell(int nx, int nv, double x_lo, double x_hi, double v_lo, double v_hi, double r, double kappa,
                          double theta, double xi, double rho, int *cols, double *vals, double *x_y);
 int opb_ell_maxdiag(int d, int w, const int *cols, const double *vals, unsigned long long *dscratch,

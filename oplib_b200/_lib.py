@@ -94,6 +94,7 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_tc_error": (i32, []),
     "opb_lv_generator_ell_batched": (i32, [i32, vp, i64, f64, f64, f64, vp, vp]),
     "opb_lv_param_size": (i32, []),
+    "opcuda_sgsvg": (i32, [u64, i32, i32, i32, u64, u64]),
     "opb_set_stage_k": (i32, [i32]),
     "opb_set_cta_pair": (i32, [i32]),
     "opb_renorm_rows": (i32, [i32, vp, vp, i32, i32, vp, vp, vp, vp, i32]),

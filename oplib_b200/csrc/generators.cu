@@ -115,6 +115,94 @@ __global__ void k_lv_ell_batched(int nlat, const LvParam *__restrict__ P, long l
     v[2] = y < d - 1 ? pp : 0.0;
 }
 
+// The reference's two-dimensional generator with jumps across volatility levels (the
+// drop-in for oplib/opcuda/sgsvg.cu:40-236).  Thread per (interval i, source y0); the row
+// of y0 in interval i is built in place in the dense column-major FP32 output
+// (element y0 -> y1 at gen[i*d*d + y0 + d*y1]); arithmetic in FP64, entries stored in FP32:
+//   1. neighbour rates invm . (0, svol^2 [interior x], voldrift, volvol^2 [interior r]);
+//   2. for r1 > r0 with prob = sum of the row's level-r1 entries > 0: entries x1 < x0-1 and
+//      x1 > x0 of level r1 become prob * w / sum(w), w = exp(+-(x1 - x0) / (J x0)) with
+//      J = jump size below / above (the reference kernel reads the lower size for both,
+//      sgsvg.cu:111-112; the host model uses each side's own, CSVModel.cs:301-312);
+//   3. negative off-diagonal entries cleared, the drift corrected through one neighbour
+//      with the reference's formula (sgsvg.cu:166-207), diagonal = -(off-diagonal sum).
+// par: x [d], then sdrift, svol, voldrift, volvol, jump_minus, jump_plus, each [ni][d].
+__global__ void k_sgsvg(float *__restrict__ gen, int ni, int nx, int nr, const float *__restrict__ invm,
+                        const float *__restrict__ par) {
+    const int d = nx * nr;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)ni * d) return;
+    const int i = (int)(t / d), y0 = (int)(t - (long long)i * d);
+    const int r0 = y0 / nx, x0 = y0 - r0 * nx;
+    const float *xv = par;
+    const long long pi = (long long)d + (long long)i * d + y0;
+    const long long pstride = (long long)ni * d;
+    // blocks after x: sdrift, svol, voldrift, volvol, jump_minus, jump_plus (sgsvg.cu:223-229)
+    const double sdrift = par[pi], sv = par[pi + pstride], vd = par[pi + 2 * pstride], vv = par[pi + 3 * pstride];
+    const double jmin0 = par[pi + 4 * pstride], jplus0 = par[pi + 5 * pstride];
+    float *g = gen + (long long)i * d * d + y0;  // row y0: g[d * y1]
+    const double xo = xv[y0];
+    double rhs[4] = {0.0, (x0 > 0 && x0 < nx - 1) ? sv * sv : 0.0, vd, (r0 > 0 && r0 < nr - 1) ? vv * vv : 0.0};
+    double q[4];
+    for (int k = 0; k < 4; k++) {
+        double acc = 0.0;
+        for (int j = 0; j < 4; j++) acc += (double)invm[16LL * y0 + k + 4 * j] * rhs[j];
+        q[k] = acc;
+    }
+    if (x0 > 0) g[(long long)d * (y0 - 1)] = (float)q[0];
+    if (x0 < nx - 1) g[(long long)d * (y0 + 1)] = (float)q[1];
+    if (r0 > 0) g[(long long)d * (y0 - nx)] = (float)q[2];
+    if (r0 < nr - 1) g[(long long)d * (y0 + nx)] = (float)q[3];
+    // jumps to higher volatility levels
+    const double jmin = jmin0 * xo, jplus = jplus0 * xo;
+    for (int r1 = r0 + 1; r1 < nr; r1++) {
+        const int base = nx * r1;
+        double prob = 0.0;
+        for (int x1 = 0; x1 < nx; x1++) prob += (double)g[(long long)d * (base + x1)];
+        if (!(prob > 0.0)) continue;
+        double sum0 = 0.0;
+        if (jmin > 0.0)
+            for (int x1 = 0; x1 < x0 - 1; x1++) sum0 += exp(((double)xv[base + x1] - xo) / jmin);
+        if (jplus > 0.0)
+            for (int x1 = x0 + 1; x1 < nx; x1++) sum0 += exp(-((double)xv[base + x1] - xo) / jplus);
+        if (!(sum0 > 0.0)) continue;
+        const double ratio = prob / sum0;
+        if (jmin > 0.0)
+            for (int x1 = 0; x1 < x0 - 1; x1++)
+                g[(long long)d * (base + x1)] = (float)(ratio * exp(((double)xv[base + x1] - xo) / jmin));
+        if (jplus > 0.0)
+            for (int x1 = x0 + 1; x1 < nx; x1++)
+                g[(long long)d * (base + x1)] = (float)(ratio * exp(-((double)xv[base + x1] - xo) / jplus));
+    }
+    // sum rules: clear negatives, correct the drift, conserve probability
+    double drift = 0.0, tot = 0.0;
+    for (int y1 = 0; y1 < d; y1++) {
+        if (y1 == y0) continue;
+        float *e = g + (long long)d * y1;
+        const double v = *e;
+        if (v < 0.0) {
+            *e = 0.f;
+        } else {
+            drift += v * ((double)xv[y1] - xo);
+            tot += v;
+        }
+    }
+    if (drift > sdrift) {
+        if (x0 > 0) {
+            const double ratio = (drift - sdrift) / ((double)xv[y0 - 1] - xo);
+            float *e = g + (long long)d * (y0 - 1);
+            *e = (float)((double)*e + ratio);
+            tot += ratio;
+        }
+    } else if (x0 < nx - 1) {
+        const double ratio = (sdrift - drift) / ((double)xv[y0 + 1] - xo);
+        float *e = g + (long long)d * (y0 + 1);
+        *e = (float)((double)*e + ratio);
+        tot += ratio;
+    }
+    g[(long long)d * y0] = (float)(-tot);
+}
+
 struct SvArgs {
     int nx, nv;
     double x_lo, x_hi, v_lo, v_hi, r, kappa, theta, xi, rho;
@@ -258,6 +346,21 @@ OPB_API int opb_lv_generator_ell_batched(int nlat, const void *params, long long
 }
 
 OPB_API int opb_lv_param_size(void) { return (int)sizeof(LvParam); }
+
+// Drop-in for opcuda_sgsvg (oplib/opcuda/sgsvg.cu:215-236), 64-bit handles: ni intervals of
+// the dense column-major FP32 generator of an nx x nr grid from the per-node moment
+// inverses invmat [16 d] and the parameter block par (see k_sgsvg).  The caller zeroes
+// gen first, as the reference's caller does.
+OPB_API int opcuda_sgsvg(unsigned long long gen_yyi_ptr, int ni, int nx, int nr, unsigned long long invmat_ptr,
+                         unsigned long long parptr) {
+    OPB_REQUIRE(ni > 0 && nx >= 2 && nr >= 2, OPB_E_ARG);
+    OPB_REQUIRE(gen_yyi_ptr && invmat_ptr && parptr, OPB_E_NULL);
+    const long long n = (long long)ni * nx * nr;
+    k_sgsvg<<<(unsigned)((n + 127) / 128), 128, 0, stream()>>>(
+        reinterpret_cast<float *>(gen_yyi_ptr), ni, nx, nr, reinterpret_cast<const float *>(invmat_ptr),
+        reinterpret_cast<const float *>(parptr));
+    return launch_check();
+}
 
 // SV generator in ELL form (width 7); x_y (optional) receives the spot value per state.
 OPB_API int opb_sv_generator_ell(int nx, int nv, double x_lo, double x_hi, double v_lo, double v_hi, double r,

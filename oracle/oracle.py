@@ -386,6 +386,114 @@ def solve_lattice_fp64(L: np.ndarray, x: np.ndarray, strikes: np.ndarray, r: flo
 
 
 # ---------------------------------------------------------------------------------
+# The reference's two-dimensional generator with vol-level jumps (opcuda_sgsvg)
+# ---------------------------------------------------------------------------------
+
+
+def s2d_invm(xval: np.ndarray, rval: np.ndarray, nx: int, nr: int) -> np.ndarray:
+    """Per-node inverses of the 4 x 4 moment matrices, ``S2DGrid.pregen``
+    (``oplib/opmodel/types/S2DGrid.cs:123-245``).  Node y = x + nx*r; columns of the
+    moment matrix are the moves (x-1, x+1, r-1, r+1), rows the moments (dx, dx^2, dr,
+    dr^2), with identity-like rows at the boundaries.  Returns invm[16*d] with
+    invm[16*y + k + 4*i] = inverse[k, i] (column-major per node)."""
+    d = nx * nr
+    invm = np.zeros(16 * d)
+    for x0 in range(nx):
+        for a0 in range(nr):
+            y0 = x0 + nx * a0
+            m = np.zeros((4, 4))
+            m[0, 0] = xval[y0 - 1] - xval[y0] if x0 > 0 else 0.0
+            m[0, 1] = xval[y0 + 1] - xval[y0] if x0 < nx - 1 else 0.0
+            if 0 < x0 < nx - 1:
+                m[1, 0], m[1, 1] = m[0, 0] ** 2, m[0, 1] ** 2
+            elif x0 == 0:
+                m[1, 0], m[1, 1] = 1.0, 0.0
+            else:
+                m[1, 0], m[1, 1] = 0.0, 1.0
+            m[2, 2] = rval[y0 - nx] - rval[y0] if a0 > 0 else 0.0
+            m[2, 3] = rval[y0 + nx] - rval[y0] if a0 < nr - 1 else 0.0
+            if 0 < a0 < nr - 1:
+                m[3, 2], m[3, 3] = m[2, 2] ** 2, m[2, 3] ** 2
+            elif a0 == 0:
+                m[3, 2] = 1.0
+            else:
+                m[3, 3] = 1.0
+            inv = np.linalg.inv(m)
+            invm[16 * y0:16 * y0 + 16] = inv.T.reshape(-1)  # column-major
+    return invm
+
+
+def sgsvg_generator(invm, xval, sdrift, svol, voldrift, volvol, jm, jp, nx, nr, gen0=None):
+    """One interval of the two-dimensional generator with jumps across volatility levels,
+    row by row as ``global_sgsvg`` (``oplib/opcuda/sgsvg.cu:40-209``) and
+    ``CSVModel.host_d_gen`` (``oplib/opmodel/models/CSVModel.cs:187-379``) build it:
+
+    1. nearest-neighbour rates = invm . (0, svol^2 [interior x], voldrift, volvol^2
+       [interior r]) for the moves (x-1, x+1, r-1, r+1);
+    2. for every higher level r1 > r0 whose entries of the row sum to prob > 0, the
+       entries x1 < x0 - 1 and x1 > x0 of level r1 are set to prob * w / sum(w) with
+       w = exp(+-(x1 - x0) / (J x0)), J = jm below and jp above (the device kernel uses
+       jm on both sides, sgsvg.cu:111-112, a listed quirk not restated);
+    3. negative off-diagonal rates are cleared; the drift sum_y1 q (x1 - x0) is moved
+       toward sdrift through one neighbour with the reference's own formula (for drift
+       above target: (drift - sdrift) / (x_{x0-1} - x0) added to the x-1 rate, as both
+       reference versions do, sgsvg.cu:186-195, CSVModel.cs:343-352); the diagonal is
+       minus the off-diagonal sum.
+
+    ``gen0`` (optional [d, d]) is the buffer's prior content (the kernels add to what is
+    there only through step 2's sums, so a zeroed buffer is the normal case).  Returns
+    G[y0, y1] (row = source), FP64."""
+    d = nx * nr
+    G = np.zeros((d, d)) if gen0 is None else np.array(gen0, dtype=np.float64)
+    for y0 in range(d):
+        r0, x0 = divmod(y0, nx)
+        rhs = np.array([0.0, svol[y0] ** 2 if 0 < x0 < nx - 1 else 0.0, voldrift[y0],
+                        volvol[y0] ** 2 if 0 < r0 < nr - 1 else 0.0])
+        inv = invm[16 * y0:16 * y0 + 16].reshape(4, 4).T
+        q = inv @ rhs
+        if x0 > 0:
+            G[y0, y0 - 1] = q[0]
+        if x0 < nx - 1:
+            G[y0, y0 + 1] = q[1]
+        if r0 > 0:
+            G[y0, y0 - nx] = q[2]
+        if r0 < nr - 1:
+            G[y0, y0 + nx] = q[3]
+        jmin, jplus = jm[y0] * xval[y0], jp[y0] * xval[y0]
+        for r1 in range(r0 + 1, nr):
+            base = nx * r1
+            prob = G[y0, base:base + nx].sum()
+            if prob <= 0:
+                continue
+            lo_idx = [base + x1 for x1 in range(0, x0 - 1)] if jmin > 0 else []
+            hi_idx = [base + x1 for x1 in range(x0 + 1, nx)] if jplus > 0 else []
+            w_lo = np.exp((xval[lo_idx] - xval[y0]) / jmin) if lo_idx else np.zeros(0)
+            w_hi = np.exp(-(xval[hi_idx] - xval[y0]) / jplus) if hi_idx else np.zeros(0)
+            sum0 = w_lo.sum() + w_hi.sum()
+            if sum0 > 0:
+                ratio = prob / sum0
+                G[y0, lo_idx] = ratio * w_lo
+                G[y0, hi_idx] = ratio * w_hi
+        row = G[y0].copy()
+        row[y0] = 0.0
+        row[row < 0] = 0.0
+        G[y0] = row
+        drift = float(np.sum(row * (xval - xval[y0])))
+        tot = float(row.sum())
+        if drift > sdrift[y0]:
+            if x0 > 0:
+                ratio = (drift - sdrift[y0]) / (xval[y0 - 1] - xval[y0])
+                G[y0, y0 - 1] += ratio
+                tot += ratio
+        elif x0 < nx - 1:
+            ratio = (sdrift[y0] - drift) / (xval[y0 + 1] - xval[y0])
+            G[y0, y0 + 1] += ratio
+            tot += ratio
+        G[y0, y0] = -tot
+    return G
+
+
+# ---------------------------------------------------------------------------------
 # Cumulative rows and sampling
 # ---------------------------------------------------------------------------------
 

@@ -189,3 +189,54 @@ def test_renorm_rows_bit_exact(cuda, mode, f16):
         assert torch.equal(g[2], hi.T.contiguous()) and torch.equal(g[3], lo.T.contiguous())
     else:
         assert not g[2].any() and not g[3].any()
+
+
+@pytest.mark.gpu
+def test_opcuda_sgsvg_matches_oracle(cuda):
+    """The reference's two-dimensional generator with vol-level jumps (drop-in
+    opcuda_sgsvg) against the FP64 restatement, two intervals of a 12 x 5 grid; moment
+    inverses from the restated S2DGrid.pregen."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    nx, nr, ni = 12, 5, 2
+    d = nx * nr
+    xs = 0.05 * 100.0 ** (np.arange(nx) / (nx - 1))
+    rs = 0.1 * 8.0 ** (np.arange(nr) / (nr - 1))
+    xval = np.tile(xs, nr)
+    rval = np.repeat(rs, nx)
+    invm = O.s2d_invm(xval, rval, nx, nr).astype(np.float32)
+    rng = np.random.default_rng(3)
+    blocks = []
+    for name in ["sdrift", "svol", "voldrift", "volvol", "jm", "jp"]:
+        b = np.empty((ni, d))
+        for i in range(ni):
+            if name == "sdrift":
+                b[i] = 0.03 * xval
+            elif name == "svol":
+                b[i] = rval * xval
+            elif name == "voldrift":
+                b[i] = 2.0 * (0.3 - rval)
+            elif name == "volvol":
+                b[i] = 0.5 * rval
+            elif name == "jm":
+                b[i] = rng.uniform(0.05, 0.2, d)
+            else:
+                b[i] = rng.uniform(0.05, 0.2, d)
+        blocks.append(b.astype(np.float32))
+    par = np.concatenate([xval.astype(np.float32)] + [b.reshape(-1) for b in blocks])
+    d_par = torch.from_numpy(par).to(cuda)
+    d_inv = torch.from_numpy(invm).to(cuda)
+    gen = torch.zeros(ni * d * d, dtype=torch.float32, device=cuda)
+    assert lib.opcuda_sgsvg(gen.data_ptr(), ni, nx, nr, d_inv.data_ptr(), d_par.data_ptr()) == 0
+    torch.cuda.synchronize()
+    got = gen.cpu().numpy().reshape(ni, d, d)   # [i][y1][y0]: column-major rows = source
+    f64 = lambda a: np.asarray(a, dtype=np.float64)
+    for i in range(ni):
+        G = O.sgsvg_generator(f64(invm), f64(xval.astype(np.float32)), *[f64(b[i]) for b in blocks], nx, nr)
+        dev = got[i].T.astype(np.float64)       # -> [y0][y1]
+        scale = np.abs(G).max(axis=1, keepdims=True)
+        assert np.all(np.abs(dev - G) <= 2e-6 * scale + 1e-12), np.max(np.abs(dev - G) / scale)
+        assert np.abs(dev.sum(axis=1)).max() <= 1e-5 * scale.max()
+        # jumps reached levels above the neighbour
+        assert np.count_nonzero(dev) > 5 * d
+    assert lib.opcuda_sgsvg(gen.data_ptr(), 0, nx, nr, d_inv.data_ptr(), d_par.data_ptr()) != 0

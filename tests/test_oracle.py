@@ -168,3 +168,34 @@ def test_mlp_oracle_gradient_vs_finite_differences():
         tm[idx] -= h
         fd = (M.loss_grad(tp, X, t)[0] - M.loss_grad(tm, X, t)[0]) / (2 * h)
         assert abs(fd - g[idx]) <= 1e-6 + 1e-5 * abs(fd), (idx, fd, g[idx])
+
+
+def test_s2d_invm_solves_the_moment_equations():
+    nx, nr = 6, 4
+    xval = np.tile(0.5 * 2.0 ** (np.arange(nx) / 2.0), nr)
+    rval = np.repeat(0.1 * 2.0 ** np.arange(nr), nx)
+    invm = O.s2d_invm(xval, rval, nx, nr)
+    # interior node: rates from the moments reproduce them
+    y0 = 2 + nx * 1
+    inv = invm[16 * y0:16 * y0 + 16].reshape(4, 4).T
+    moments = np.array([0.01, 0.04, -0.02, 0.005])
+    q = inv @ moments
+    dxm, dxp = xval[y0 - 1] - xval[y0], xval[y0 + 1] - xval[y0]
+    drm, drp = rval[y0 - nx] - rval[y0], rval[y0 + nx] - rval[y0]
+    assert np.allclose([q[0] * dxm + q[1] * dxp, q[0] * dxm ** 2 + q[1] * dxp ** 2,
+                        q[2] * drm + q[3] * drp, q[2] * drm ** 2 + q[3] * drp ** 2], moments, rtol=1e-12)
+
+
+def test_sgsvg_oracle_row_sums_and_jumps():
+    nx, nr = 10, 4
+    d = nx * nr
+    xval = np.tile(0.2 * 1.3 ** np.arange(nx), nr)
+    rval = np.repeat(0.1 * 2.0 ** np.arange(nr), nx)
+    invm = O.s2d_invm(xval, rval, nx, nr)
+    G = O.sgsvg_generator(invm, xval, 0.03 * xval, rval * xval, 2.0 * (0.3 - rval), 0.5 * rval,
+                          np.full(d, 0.1), np.full(d, 0.15), nx, nr)
+    assert np.abs(G.sum(axis=1)).max() < 1e-12
+    off = G - np.diag(np.diag(G))
+    # the up-move of an interior node spreads over its next volatility level
+    y0 = 5 + nx * 1
+    assert np.count_nonzero(off[y0, nx * 2:nx * 3]) > 3
