@@ -617,6 +617,29 @@ def run_batch(args):
     return line
 
 
+def _surrogate_inference_only(args, dev, stream, torch):
+    """--epochs 0: inference timing alone (randomly initialised members, no data, no
+    training) on 2^20 seeded feature vectors -- the kernel-profiling case."""
+    from oplib_b200 import _lib
+    from oplib_b200.surrogate import RANGES, Surrogate
+    sur = Surrogate(members=args.members, device=dev)
+    for m in range(sur.members):
+        _lib.call("opb_mlp_pack", sur.theta[m].data_ptr(), sur.packed[m * sur.stride:].data_ptr())
+    n = 1 << 20
+    rng = np.random.default_rng(0)
+    feat = torch.from_numpy(np.column_stack([rng.uniform(lo, hi, n) for lo, hi in RANGES])).to(dev)
+    base = torch.zeros(n, dtype=torch.float64, device=dev)
+    ws = torch.empty(int(sur.lib.opb_mlp_infer_workspace_bytes(n, sur.members)), dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        sur.predict(feat, base, ws)
+    ms = _time(lambda: sur.predict(feat, base, ws), args.steps, stream, torch)
+    return {"metric": "surrogate quotes/sec (ensemble MLP on tensor cores), inference only", "value":
+            round(n / (ms * 1e-3), 1), "unit": "quotes/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 weights/activations, fp32 accumulate", "data": "synthetic (random weights)",
+            "config": {"workload": f"2^20 quotes, ensemble of {sur.members} MLPs 8-256x4-1, untrained"}}
+
+
 def run_surrogate(args):
     """Config 4: ensemble of MLP surrogates (8 -> 256 x 4 -> 1, GELU) trained by the
     library's kernels on ~2^21 quotes that the batched lattice solver generates (local-vol
@@ -631,6 +654,8 @@ def run_surrogate(args):
     torch.cuda.set_device(dev)
     bind_stream(dev)
     stream = torch.cuda.current_stream(dev)
+    if args.epochs == 0:
+        return _surrogate_inference_only(args, dev, stream, torch)
     t0 = time.perf_counter()
     train = lattice_quotes(args.train_lattices, seed=2026, device=dev)
     test = lattice_quotes(1024, seed=31337, device=dev)

@@ -191,7 +191,23 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-template <int BN, int STAGES, int NPROD = 3, int BK = TC_BK, bool PAIR = false>
+// GELU(z) = 0.5 z (1 + erf(z / sqrt 2)), with erf from Abramowitz & Stegun, Handbook of
+// Mathematical Functions, formula 7.1.26 (|error| <= 1.5e-7): for x >= 0,
+// erf(x) = 1 - q(t) exp(-x^2), t = 1 / (1 + p x), q(t) = a1 t + ... + a5 t^5.  For z < 0,
+// 1 + erf(z / sqrt 2) = q exp(-x^2) is used directly (no cancellation).  The error is far
+// below the BF16 rounding of the stored activations.
+__device__ __forceinline__ float gelu_as(float z) {
+    const float x = fabsf(z) * 0.70710678118654752f;
+    const float t = __fdividef(1.0f, fmaf(0.3275911f, x, 1.0f));
+    float q = fmaf(t, 1.061405429f, -1.453152027f);
+    q = fmaf(t, q, 1.421413741f);
+    q = fmaf(t, q, -0.284496736f);
+    q = fmaf(t, q, 0.254829592f);
+    const float e = q * t * __expf(-x * x);  // 1 - erf(|z| / sqrt 2)
+    return z >= 0.f ? fmaf(-0.5f * z, e, z) : 0.5f * z * e;
+}
+
+template <int BN, int STAGES, int NPROD = 3, int BK = TC_BK, bool PAIR = false, int CPT_MAX = 128>
 struct TcCfg {
     static constexpr int A_BYTES = TC_BM * BK * 2;                  // one of Ahi/Alo
     static constexpr int B_ROWS = PAIR ? BN / 2 : BN;               // B rows held by this CTA
@@ -200,12 +216,15 @@ struct TcCfg {
     static constexpr int NPARTS = NPROD == 1 ? 1 : 2;  // parts loaded per operand
     static constexpr int STAGE_BYTES = NPARTS * (A_BYTES + B_BYTES);
     static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
-    static constexpr int CPT = BN < 128 ? BN : 128;        // accumulator columns per epilogue thread
+    static constexpr int CPT = BN < CPT_MAX ? BN : CPT_MAX;  // accumulator columns per epilogue thread
     static constexpr int HALVES = BN / CPT;                 // column groups per TMEM lane
     static constexpr int EPI_WARPS = 4 * HALVES;            // epilogue warps (4 lane quadrants x groups)
     static constexpr int THREADS = 32 * (EPI_WARPS + 2);    // + TMA producer warp + MMA warp
     static constexpr int TMEM_COLS = 2 * BN;                // two accumulators (ping-pong chunks)
-    static constexpr int CHUNK = 128 / BK;                  // K-blocks accumulated in TMEM per chunk (K = 128)
+    // K-blocks accumulated in TMEM per chunk: K = 128 for the split products (bounds the
+    // tensor cores' truncation); the whole K for single BF16 products (network layers,
+    // whose BF16 outputs do not need it)
+    static constexpr int CHUNK = NPROD == 1 ? (1 << 20) : 128 / BK;
 };
 
 struct TcParams {
@@ -219,6 +238,10 @@ struct TcParams {
     const float *bias;
     __nv_bfloat16 *H;
     long long ldh;
+    // EPIMODE == 2 (last hidden layer + output layer): ypart[g * M + row] =
+    // sum over the columns of group g of bf16(GELU(alpha * acc + bias)) * w5[col]
+    const float *w5;
+    float *ypart;
 };
 
 // Batched launches read per-problem tensor maps (4 per problem: Ahi, Alo, Bhi, Blo) and
@@ -240,11 +263,13 @@ struct TcBatch {
 // instructions, and an item's final store overlaps the next item's MMAs.
 template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK,
           bool PAIR = false>
-__global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR>::THREADS, 1)
+__global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? TC_LAYER_CPT : 128)>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
               const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p,
               TcBatch bt) {
-    using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR>;
+    // network layers (EPIMODE >= 1) run twice the epilogue warps: their per-element GELU,
+    // not the MMAs, bounds a tile
+    using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? TC_LAYER_CPT : 128)>;
     static_assert(!(PAIR && BATCHED), "pair mode is for single products");
     constexpr int EPI = Cfg::EPI_WARPS;
     constexpr int CPT = Cfg::CPT;
@@ -503,20 +528,43 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR>::THREADS, 1
             if constexpr (EPIMODE == 1) {
                 // network layer: BF16 GELU(alpha * acc + bias), 8 values per 16-byte store
                 __nv_bfloat16 *hrow = p.H + (long long)row * p.ldh + col0;
+                const float4 *b4 = reinterpret_cast<const float4 *>(p.bias + col0);
 #pragma unroll
                 for (int j = 0; j < CPT; j += 8) {
+                    const float4 ba = __ldg(b4 + j / 4), bb = __ldg(b4 + j / 4 + 1);
+                    const float bv[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
                     uint32_t pk[4];
 #pragma unroll
                     for (int u = 0; u < 4; u++) {
-                        float z0 = fmaf(alpha, sum[j + 2 * u], __ldg(p.bias + col0 + j + 2 * u));
-                        float z1 = fmaf(alpha, sum[j + 2 * u + 1], __ldg(p.bias + col0 + j + 2 * u + 1));
-                        z0 = 0.5f * z0 * (1.f + erff(z0 * 0.70710678118654752f));
-                        z1 = 0.5f * z1 * (1.f + erff(z1 * 0.70710678118654752f));
-                        pk[u] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(z0)) |
-                                ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(z1)) << 16);
+                        const __nv_bfloat162 h2 =
+                            __floats2bfloat162_rn(gelu_as(fmaf(alpha, sum[j + 2 * u], bv[2 * u])),
+                                                  gelu_as(fmaf(alpha, sum[j + 2 * u + 1], bv[2 * u + 1])));
+                        pk[u] = *reinterpret_cast<const uint32_t *>(&h2);
                     }
                     *reinterpret_cast<uint4 *>(hrow + j) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
                 }
+                continue;
+            }
+            if constexpr (EPIMODE == 2) {
+                // last hidden layer fused with the output layer: partial dot over this
+                // thread's columns of the BF16-rounded activations
+                const float4 *b4 = reinterpret_cast<const float4 *>(p.bias + col0);
+                const float4 *w4 = reinterpret_cast<const float4 *>(p.w5 + col0);
+                float acc = 0.f;
+#pragma unroll
+                for (int j = 0; j < CPT; j += 4) {
+                    const float4 bv = __ldg(b4 + j / 4), wv = __ldg(w4 + j / 4);
+                    const __nv_bfloat162 h01 = __floats2bfloat162_rn(gelu_as(fmaf(alpha, sum[j], bv.x)),
+                                                                     gelu_as(fmaf(alpha, sum[j + 1], bv.y)));
+                    const __nv_bfloat162 h23 = __floats2bfloat162_rn(gelu_as(fmaf(alpha, sum[j + 2], bv.z)),
+                                                                     gelu_as(fmaf(alpha, sum[j + 3], bv.w)));
+                    const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+                    acc = fmaf(f01.x, wv.x, acc);
+                    acc = fmaf(f01.y, wv.y, acc);
+                    acc = fmaf(f23.x, wv.z, acc);
+                    acc = fmaf(f23.y, wv.w, acc);
+                }
+                p.ypart[(long long)(col0 / CPT) * p.M + row] = acc;
                 continue;
             }
             float *crow = C + (long long)row * ldc + col0;
@@ -754,24 +802,31 @@ int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *pro
 
 // One network layer on the tensor cores: H[M, N] = GELU(alpha * A[M, K] . W[N, K]^T + bias)
 // with BF16 A, W and H (single product, FP32 accumulation); M % 128, N % 256, K % 64.
+// With w5 and ypart (N = 256): no H; instead ypart[g * M + row], g < 256 / TC_LAYER_CPT, =
+// the dot of the BF16 activations of column group g with w5 (the output layer, fused).
 int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, const __nv_bfloat16 *W,
-                    long long ldw, float alpha, const float *bias, __nv_bfloat16 *H, long long ldh, cudaStream_t s) {
+                    long long ldw, float alpha, const float *bias, __nv_bfloat16 *H, long long ldh, cudaStream_t s,
+                    const float *w5, float *ypart) {
     constexpr int BN = 256, STAGES = 4;
-    using Cfg = TcCfg<BN, STAGES, 1>;
-    if (M <= 0 || M % TC_BM || N % BN || K % TC_BK) return OPB_E_UNSUPPORTED;
-    if (!A || !W || !bias || !H) return OPB_E_NULL;
-    int e0 = set_smem_attr<BN, STAGES, false, false, 1, 1>();
+    using Cfg = TcCfg<BN, STAGES, 1, TC_BK, false, TC_LAYER_CPT>;
+    const bool fused = w5 != nullptr;
+    if (M <= 0 || M % TC_BM || N % BN || K % TC_BK || (fused && N != BN)) return OPB_E_UNSUPPORTED;
+    if (!A || !W || !bias || (fused ? !ypart : !H)) return OPB_E_NULL;
+    int e0 = fused ? set_smem_attr<BN, STAGES, false, false, 1, 2>() : set_smem_attr<BN, STAGES, false, false, 1, 1>();
     if (e0) return e0;
     CUtensorMap mA, mW;
     int r;
     if ((r = make_map(&mA, A, M, K, lda, TC_BM)) != OPB_OK) return r;
     if ((r = make_map(&mW, W, N, K, ldw, BN)) != OPB_OK) return r;
     TcParams p{};
-    p.M = M; p.N = N; p.K = K; p.alpha = alpha; p.bias = bias; p.H = H; p.ldh = ldh;
+    p.M = M; p.N = N; p.K = K; p.alpha = alpha; p.bias = bias; p.H = H; p.ldh = ldh; p.w5 = w5; p.ypart = ypart;
     const int ntiles = (M / TC_BM) * (N / BN);
     const int grid = ntiles < num_sms() ? ntiles : num_sms();
     TcBatch none{nullptr, nullptr, nullptr, 0};
-    k_tc_gemm<BN, STAGES, false, false, 1, 1><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mA, mA, mW, mW, p, none);
+    if (fused)
+        k_tc_gemm<BN, STAGES, false, false, 1, 2><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mA, mA, mW, mW, p, none);
+    else
+        k_tc_gemm<BN, STAGES, false, false, 1, 1><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mA, mA, mW, mW, p, none);
     return (int)cudaGetLastError();
 }
 

@@ -84,8 +84,12 @@ struct TcGemmArgs {
 int tc_gemm_tile_n(int N);                    // tile width chosen for N (0 if unsupported)
 int tc_gemm_check(const TcGemmArgs &a);       // argument/alignment check, OPB_* code
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s);
+// Network layers: accumulator columns per epilogue thread; the fused output layer writes
+// N / TC_LAYER_CPT partial dots per row.
+constexpr int TC_LAYER_CPT = 64;
 int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, const __nv_bfloat16 *W,
-                    long long ldw, float alpha, const float *bias, __nv_bfloat16 *H, long long ldh, cudaStream_t s);
+                    long long ldw, float alpha, const float *bias, __nv_bfloat16 *H, long long ldh, cudaStream_t s,
+                    const float *w5 = nullptr, float *ypart = nullptr);
 int tc_gemm_nparts(int M, int N);             // number of row-sum partials written
 
 // Batched launches: problem descriptors and tensor maps live in device memory.

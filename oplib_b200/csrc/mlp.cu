@@ -434,32 +434,20 @@ __global__ void k_mlp_pad_input(long long n, const float *__restrict__ X, __nv_b
     }
 }
 
-// y[r] = H[r, :] . w5 + b5 with BF16 H (warp per row)
-__global__ void k_mlp_out_bf16(long long n, const __nv_bfloat16 *__restrict__ H, const float *__restrict__ w,
-                               const float *__restrict__ b, float *__restrict__ y) {
-    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    const uint4 v = *reinterpret_cast<const uint4 *>(H + warp * 256 + lane * 8);
-    const uint32_t u[4] = {v.x, v.y, v.z, v.w};
-    float s = 0.f;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        s = fmaf(__bfloat162float(__ushort_as_bfloat16((unsigned short)(u[j] & 0xffffu))), w[lane * 8 + 2 * j], s);
-        s = fmaf(__bfloat162float(__ushort_as_bfloat16((unsigned short)(u[j] >> 16))), w[lane * 8 + 2 * j + 1], s);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) y[warp] = s + b[0];
-}
-
-// ensemble mean and spread (max - min) over nmem member outputs y[m * n + r]
-__global__ void k_mlp_ensemble(long long n, int nmem, const float *__restrict__ y, float *__restrict__ mean,
-                               float *__restrict__ spread) {
+// Ensemble mean and spread (max - min): member m's output is its MLP_YPARTS column-group
+// partial dots yp[(MLP_YPARTS m + g) * np + r] (from the fused last layer) plus its bias b5
+// (the last float of its packed weights).
+constexpr int MLP_YPARTS = 256 / TC_LAYER_CPT;
+__global__ void k_mlp_ensemble(long long n, long long np, int nmem, const float *__restrict__ yp,
+                               const uint8_t *__restrict__ packed, long long stride, long long b5_off,
+                               float *__restrict__ mean, float *__restrict__ spread) {
     for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
         float s = 0.f, lo = 3.4e38f, hi = -3.4e38f;
         for (int m = 0; m < nmem; m++) {
-            const float v = y[(long long)m * n + r];
+            const float b5 = *reinterpret_cast<const float *>(packed + (long long)m * stride + b5_off);
+            float v = 0.f;
+            for (int g = 0; g < MLP_YPARTS; g++) v += yp[((long long)MLP_YPARTS * m + g) * np + r];
+            v += b5;
             s += v;
             lo = fminf(lo, v);
             hi = fmaxf(hi, v);
@@ -483,7 +471,7 @@ OPB_API int opb_mlp_pack(const float *theta, void *packed) {
 // Inference workspace bytes for n rows (n padded to a multiple of 128 internally).
 OPB_API long long opb_mlp_infer_workspace_bytes(long long n, int nmem) {
     const long long np = (n + 127) / 128 * 128;
-    return np * 64 * 2 + 2 * np * 256 * 2 + (long long)nmem * np * 4 + 1024;
+    return np * 64 * 2 + 2 * np * 256 * 2 + (long long)MLP_YPARTS * nmem * np * 4 + 1024;
 }
 
 // Ensemble inference on the tensor cores: members m = 0..nmem-1 with packed weights at
@@ -512,9 +500,11 @@ OPB_API int opb_mlp_infer(const void *packed, int nmem, long long member_stride,
         MT(launch_tc_layer((int)np, 256, 64, Xp, 64, W1, 64, 1.f, f, Ha, 256, s));
         MT(launch_tc_layer((int)np, 256, 256, Ha, 256, WH, 256, 1.f, f + 256, Hb, 256, s));
         MT(launch_tc_layer((int)np, 256, 256, Hb, 256, WH + 65536, 256, 1.f, f + 512, Ha, 256, s));
-        MT(launch_tc_layer((int)np, 256, 256, Ha, 256, WH + 2 * 65536, 256, 1.f, f + 768, Hb, 256, s));
-        k_mlp_out_bf16<<<(int)((n * 32 + 255) / 256), 256, 0, s>>>(n, Hb, f + 1024, f + 1280, ym + (long long)m * n);
+        // last hidden layer with the output layer fused into its epilogue
+        MT(launch_tc_layer((int)np, 256, 256, Ha, 256, WH + 2 * 65536, 256, 1.f, f + 768, nullptr, 256, s, f + 1024,
+                           ym + (long long)MLP_YPARTS * m * np));
     }
-    k_mlp_ensemble<<<grid_ew(n), 256, 0, s>>>(n, nmem, ym, mean, spread);
+    k_mlp_ensemble<<<grid_ew(n), 256, 0, s>>>(n, np, nmem, ym, reinterpret_cast<const uint8_t *>(packed),
+                                              member_stride, MLP_PACK_W1 + 3 * MLP_PACK_WH + 1280LL * 4, mean, spread);
     return launch_check();
 }

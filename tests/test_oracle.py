@@ -199,3 +199,19 @@ def test_sgsvg_oracle_row_sums_and_jumps():
     # the up-move of an interior node spreads over its next volatility level
     y0 = 5 + nx * 1
     assert np.count_nonzero(off[y0, nx * 2:nx * 3]) > 3
+
+
+def test_gelu_erf_approximation_bound():
+    """The tensor-core layers' GELU uses erf from Abramowitz & Stegun 7.1.26 (the constants
+    as written in the kernel); its published bound 1.5e-7 holds, so GELU is within
+    0.75e-7 |z| of the exact form."""
+    from scipy.special import erf
+    z = np.linspace(-12.0, 12.0, 200001)
+    x = np.abs(z) / math.sqrt(2.0)
+    t = 1.0 / (1.0 + 0.3275911 * x)
+    q = t * (0.254829592 + t * (-0.284496736 + t * (1.421413741 + t * (-1.453152027 + t * 1.061405429))))
+    e = q * np.exp(-x * x)
+    g = np.where(z >= 0, z - 0.5 * z * e, 0.5 * z * e)
+    exact = 0.5 * z * (1.0 + erf(z / math.sqrt(2.0)))
+    assert np.max(np.abs((1.0 - e) - erf(x))) <= 1.5e-7
+    assert np.all(np.abs(g - exact) <= 0.75e-7 * np.abs(z) + 1e-300)
