@@ -215,12 +215,23 @@ __device__ __forceinline__ void renorm64_sums(RenormSmem &sm, int d, const doubl
     }
 }
 
-// One tile at (r0, c0), using the sums of renorm64_sums.  Starts with a barrier, so it can
-// follow renorm64_sums or a previous tile of the same rows directly.
+// This thread's four float4 of the tile at (r0, c0).
+__device__ __forceinline__ void renorm64_load(int d, const float *__restrict__ X, int r0, int c0, float4 (&v)[4]) {
+    const int tid = threadIdx.x, lc = (tid & 15) * 4;
+#pragma unroll
+    for (int pass = 0; pass < 4; pass++)
+        v[pass] = *reinterpret_cast<const float4 *>(X + (long long)(r0 + pass * 16 + (tid >> 4)) * d + c0 + lc);
+}
+
+// One tile at (r0, c0), using the sums of renorm64_sums; vin holds the tile's values
+// (renorm64_load), and next (optional) is called after the row-major stores and before the
+// transposed ones, so that the next tile's loads overlap them.  Starts with a barrier, so
+// it can follow renorm64_sums or a previous tile of the same rows directly.
+template <class Next>
 __device__ __forceinline__ void renorm64_apply(RenormSmem &sm, int d, float *__restrict__ X, int mode,
                                                __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
                                                __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo,
-                                               int r0, int c0, float sscale) {
+                                               int r0, int c0, float sscale, const float4 (&vin)[4], Next &&next) {
     const int tid = threadIdx.x;
     const bool eform = mode != 2;
     __syncthreads();
@@ -230,7 +241,7 @@ __device__ __forceinline__ void renorm64_apply(RenormSmem &sm, int d, float *__r
         const int lr = pass * 16 + (tid >> 4);
         const int r = r0 + lr;
         const long long o = (long long)r * d + c0 + lc;
-        float4 v = *reinterpret_cast<const float4 *>(X + o);
+        const float4 v = vin[pass];
         const double su = sm.s_sum[lr], inv = sm.s_inv[lr];
         float f[4] = {v.x, v.y, v.z, v.w};
         __nv_bfloat16 h[4], l[4];
@@ -251,6 +262,7 @@ __device__ __forceinline__ void renorm64_apply(RenormSmem &sm, int d, float *__r
             *reinterpret_cast<uint2 *>(Alo + o) = make_uint2(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]));
         }
     }
+    next();
     if (!Bhi) return;
     __syncthreads();
 #pragma unroll
@@ -271,10 +283,18 @@ __global__ void __launch_bounds__(256) k_renorm64(int d, float *__restrict__ X, 
                                                   __nv_bfloat16 *__restrict__ Alo, __nv_bfloat16 *__restrict__ Bhi,
                                                   __nv_bfloat16 *__restrict__ Blo, float sscale) {
     __shared__ RenormSmem sm;
-    const int r0 = blockIdx.y * 64;
+    const int r0 = blockIdx.y * 64, nt = d / 64;
+    float4 cur[4], nxt[4];
+    if ((int)blockIdx.x < nt) renorm64_load(d, X, r0, blockIdx.x * 64, cur);
     renorm64_sums(sm, d, partial, nparts, mode, r0);
-    for (int tc = blockIdx.x; tc < d / 64; tc += gridDim.x)
-        renorm64_apply(sm, d, X, mode, Ahi, Alo, Bhi, Blo, r0, tc * 64, sscale);
+    for (int tc = blockIdx.x; tc < nt; tc += gridDim.x) {
+        const int tn = tc + gridDim.x;
+        renorm64_apply(sm, d, X, mode, Ahi, Alo, Bhi, Blo, r0, tc * 64, sscale, cur, [&] {
+            if (tn < nt) renorm64_load(d, X, r0, tn * 64, nxt);
+        });
+#pragma unroll
+        for (int j = 0; j < 4; j++) cur[j] = nxt[j];
+    }
 }
 
 // Column chunks of a k_renorm64 launch: about 8 resident blocks per SM in total.
@@ -296,10 +316,12 @@ __global__ void __launch_bounds__(256) k_renorm64_batched(const RenormProblem *_
     const RenormProblem &pr = probs[w >> 16];
     const int mode = (int)((w >> 14) & 3u);
     const int nparts = parts_div > 0 ? pr.d / parts_div : 0;
-    const int r0 = (int)((w >> 7) & 127u) * 64;
+    const int r0 = (int)((w >> 7) & 127u) * 64, c0 = (int)(w & 127u) * 64;
+    float4 v[4];
+    renorm64_load(pr.d, pr.X, r0, c0, v);
     renorm64_sums(sm, pr.d, pr.partial, nparts, mode, r0);
     renorm64_apply(sm, pr.d, pr.X, mode, pr.Ahi, pr.Alo, mode == 2 ? nullptr : pr.Bhi, mode == 2 ? nullptr : pr.Blo,
-                   r0, (int)(w & 127u) * 64, sscale);
+                   r0, c0, sscale, v, [] {});
 }
 
 // Batched ELL scatter into zeroed dense E-form matrices: thread per global ELL slot
