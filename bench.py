@@ -267,6 +267,25 @@ def run_b200(args, rank, world, local_rank):
                  "fp32_max_abs_err_vs_fp64": float((q32 - q_ref).abs().max().item()),
                  "speedup_vs_fp32": round(ms32 / ms, 2)}
         del ws32
+        # context for the comparison arm: the library's SIMT FP32 product against cuBLAS
+        # SGEMM (TF32 off) at the same size; the plain solve re-estimated with cuBLAS
+        # products in place of the 29 SIMT ones
+        A32 = torch.empty(d, d, dtype=torch.float32, device=dev).uniform_()
+        C32 = torch.empty_like(A32)
+        tf32 = torch.backends.cuda.matmul.allow_tf32
+        torch.backends.cuda.matmul.allow_tf32 = False
+        torch.mm(A32, A32, out=C32)
+        t_cu = _time(lambda: torch.mm(A32, A32, out=C32), 5, stream, torch)
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        t_si = _time(lambda: _lib.call("opb_sgemm_batched_rm", d, d, d, A32.data_ptr(), 0, A32.data_ptr(), 0,
+                                       C32.data_ptr(), 0, 1), 3, stream, torch)
+        nprod = plan.niter + NMAT - 1
+        ms32_cu = ms32 - nprod * (t_si - t_cu)
+        extra["fp32_gemm_context"] = {"simt_tflops": round(2.0 * d ** 3 / (t_si * 1e-3) / 1e12, 1),
+                                      "cublas_sgemm_tflops": round(2.0 * d ** 3 / (t_cu * 1e-3) / 1e12, 1),
+                                      "est_fp32_cublas_quotes_per_s": round(NMAT * NK * world / (ms32_cu * 1e-3), 1),
+                                      "est_speedup_vs_fp32_cublas": round(ms32_cu / ms, 2)}
+        del A32, C32
         m16 = MODES["fp16x3"]
         ws16 = lat.workspace(NK, m16)
         q16 = torch.empty_like(quotes)
