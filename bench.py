@@ -36,6 +36,16 @@ sys.path.insert(0, str(ROOT))
 
 SV = dict(nx=128, nv=48, x_lo=0.05, x_hi=5.0, v_lo=0.05, v_hi=1.0, rate=0.03, kappa=2.0, theta=0.04, xi=0.6, rho=-0.7)
 PERIOD, NMAT, NK, DT0 = 0.25, 16, 128, 2.0 ** -16
+NITER_SV = 14  # squarings to P(PERIOD) at dt0 (the plan rule; checked against the plan at run time)
+SV_METRIC = "priced quotes/sec at <=1e-5 abs err vs FP64 (split-BF16 tensor-core lattice vs plain FP32)"
+
+
+def sv_config(mode: str, world: int) -> dict:
+    """The headline workload's config, shared by both arms of the bench."""
+    return {"workload": "SV lattice 48 vol x 128 spot = 6144 states, dt0=2^-16, 14 squarings + 15 chains, "
+                        "128 strikes x 16 quarterly maturities (2048 quotes/solve)",
+            "d": SV["nx"] * SV["nv"], "niter": NITER_SV, "nmat": NMAT, "nK": NK, "mode": mode,
+            "parallelism": f"replicas x{world}", "l2": "operands 151-302 MB per matrix > 126 MB L2"}
 STRIKES = [0.5 + j / 127.0 for j in range(NK)]
 
 
@@ -129,6 +139,8 @@ def run_b200(args, rank, world, local_rank):
     sv["rho"] = SV["rho"] + 0.001 * rank  # independent replica per rank
     lat = Lattice.stoch_vol(**sv, device=dev)
     plan = lat.plan(PERIOD, DT0)
+    if plan.niter != NITER_SV:
+        raise SystemExit(f"plan gives {plan.niter} squarings, the workload states {NITER_SV}")
     strikes = torch.tensor(STRIKES, dtype=torch.float64, device=dev)
     ws = lat.workspace(NK, mode)
     quotes = torch.empty(NMAT, NK, dtype=torch.float64, device=dev)
@@ -310,14 +322,11 @@ def run_b200(args, rank, world, local_rank):
     else:
         launches = 1 + 2 + (3 if mode == 1 else 1) * plan.niter + 1 + 2 * NMAT + (3 if mode == 1 else 1) * (NMAT - 1)
     out = {
-        "metric": "priced quotes/sec at <=1e-5 abs err vs FP64 (split-BF16 tensor-core lattice vs plain FP32)",
+        "metric": SV_METRIC,
         "value": round(value, 1), "unit": "quotes/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "bf16x3->fp32 (fp64 renorm/discount)" if mode == 2 else "fp32", "data": "synthetic",
-        "config": {"workload": "SV lattice 48 vol x 128 spot = 6144 states, dt0=2^-16, 14 squarings + 15 chains, "
-                               "128 strikes x 16 quarterly maturities (2048 quotes/solve)",
-                   "d": d, "niter": plan.niter, "nmat": NMAT, "nK": NK, "mode": args.mode,
-                   "parallelism": f"replicas x{world}", "l2": "operands 151-302 MB per matrix > 126 MB L2"},
+        "config": sv_config(args.mode, world),
         "max_abs_err_vs_fp64": err,
         "e2e": {"value": round(quotes_per_step / (ms_e2e * 1e-3), 1), "unit": "quotes/s",
                 "h2d_bytes_per_step": NK * 8, "d2h_bytes_per_step": NMAT * NK * 8},
@@ -852,12 +861,11 @@ def main():
         v = statistics.median(x["value"] for x in vals)
         cb = dict(vals[0])
         cb["value"] = v
-        line = {"impl": "reference", "metric": "priced quotes/sec (FP64 oracle port on host cores)", "value": v,
+        line = {"impl": "reference", "metric": SV_METRIC, "value": v,
                 "unit": "quotes/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(NMAT * NK / v * 1e3, 1), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "SV lattice 6144 states, 29 products per solve, 2048 quotes",
-                           "parallelism": "host threads"},
+                "config": sv_config(args.mode, 1),
                 "cpu_baseline": cb, "e2e": {"value": v, "unit": "quotes/s", "h2d_bytes_per_step": 0,
                                             "d2h_bytes_per_step": 0},
                 "wall_s": round(time.perf_counter() - t0, 1)}
