@@ -231,7 +231,10 @@ OPB_API int opb_mc_mt19937(const float *C, long long row_stride, long long col_s
     OPB_REQUIRE(C != nullptr, OPB_E_NULL);
     if (guide) OPB_REQUIRE(nb >= 1 && nb <= 4096 && (nb & (nb - 1)) == 0 && col_stride == 1, OPB_E_ARG);
     if (x) OPB_REQUIRE(scratch != nullptr && sums != nullptr, OPB_E_NULL);
-    if (npaths == 0) return set_status(OPB_OK);
+    if (npaths == 0) {  // no paths: the payoff sums are zero
+        if (x) OPB_TRY(cudaMemsetAsync(sums, 0, 2 * sizeof(double), stream()));
+        return set_status(OPB_OK);
+    }
     McArgs a{};
     a.C = C; a.rs = row_stride; a.cs = col_stride; a.guide = guide; a.nb = nb;
     a.d = d; a.y0 = y0; a.nsteps = nsteps; a.seed = seed; a.path0 = path0; a.npaths = npaths;
