@@ -774,6 +774,42 @@ def run_renorm(args):
             "frac_of_peak": round(gbs / hbm, 4), "peak_source": src}
 
 
+def run_gemv(args):
+    """Backward-induction GEMV of the drop-in entry points on a d x d column-major FP32
+    matrix (the reference's layout; 151 MB at d = 6144, larger than L2): opcuda_sgemvT
+    (warp per column: the warp-per-row GEMV of a source-major kernel) and opcuda_sgemv
+    (column chunks + ordered reduction).  Algorithmic bytes: 4 d^2 + 12 d per call."""
+    import torch
+    from oplib_b200 import _lib
+    from oplib_b200.model import bind_stream
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    bind_stream(dev)
+    stream = torch.cuda.current_stream(dev)
+    d = args.d
+    A = torch.empty(d * d, dtype=torch.float32, device=dev).uniform_(0, 1.0 / d)
+    x = torch.empty(d, dtype=torch.float32, device=dev).uniform_()
+    y = torch.zeros(d, dtype=torch.float32, device=dev)
+    hbm, _, _, src = _peaks()
+    byts = 4.0 * d * d + 12.0 * d
+    res = {}
+    for name in ("opcuda_sgemvT", "opcuda_sgemv"):
+        f = lambda: _lib.call(name, d, d, 1.0, A.data_ptr(), d, x.data_ptr(), 1, 0.0, y.data_ptr(), 1)
+        for _ in range(max(3, args.warmup)):
+            f()
+        ms = _time(f, args.steps, stream, torch)
+        res[name] = {"ms": round(ms, 4), "GB_s": round(byts / (ms * 1e-3) / 1e9, 1),
+                     "frac": round(byts / (ms * 1e-3) / 1e9 / hbm, 4)}
+    v = res["opcuda_sgemvT"]
+    return {"metric": "backward-induction GEMV achieved GB/s (warp-per-row, source-major kernel)", "value": v["GB_s"],
+            "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"GEMV on a {d} x {d} FP32 matrix ({4 * d * d / 1e6:.0f} MB > L2)"},
+            "roofline": {"bound": "hbm", "achieved": v["GB_s"], "peak": hbm, "unit": "GB/s", "frac": v["frac"],
+                         "peak_source": src},
+            "column_major_N": res["opcuda_sgemv"]}
+
+
 def run_gemm(args):
     """The squaring GEMM alone (split-BF16, E-form: C = E.E + 2E in place) at size d."""
     import torch
@@ -817,7 +853,7 @@ def main():
     ap.add_argument("--members", type=int, default=4)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--workload", default="sv",
-                    choices=["sv", "lv", "mc", "gemm", "renorm", "batch", "surrogate", "calibrate"],
+                    choices=["sv", "lv", "mc", "gemm", "gemv", "renorm", "batch", "surrogate", "calibrate"],
                     help="sv = the headline SV lattice solve; the others are secondary measurements")
     ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
     args = ap.parse_args()
@@ -834,8 +870,8 @@ def main():
             import torch.distributed as dist
             torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "renorm": run_renorm, "batch": run_batch,
-              "surrogate": run_surrogate, "calibrate": run_calibrate}[
+        fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "gemv": run_gemv, "renorm": run_renorm,
+              "batch": run_batch, "surrogate": run_surrogate, "calibrate": run_calibrate}[
             args.workload]
         line = fn(args)
         if int(os.environ.get("RANK", "0")) == 0:

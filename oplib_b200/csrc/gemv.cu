@@ -14,29 +14,129 @@
 // Each kernel reads the matrix exactly once with coalesced accesses: consecutive threads
 // own consecutive rows of a column-major matrix, so every column step is one contiguous
 // 128-byte segment per warp.  Column lists are processed 16 at a time from one pass.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace opb {
 
-__global__ void k_sgemv_n(int m, int n, float alpha, const float *__restrict__ A, int lda,
-                          const float *__restrict__ x, int incx, float beta, float *__restrict__ y, int incy) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+// y = alpha * A x + beta * y, column-major A (m x n).  Block = 8 warps over one tile of
+// rows (128 rows, 4 per lane with float4 loads, when VEC; else 32 rows, one per lane) and
+// the column chunk [j0, j1): warp w takes the columns j0 + w, j0 + w + 8, ..., so every
+// warp load is one contiguous column segment; the 8 warp sums are combined in shared
+// memory in warp order.  With part != nullptr the chunk's sums go to part[chunk * m + row]
+// for k_sgemv_n_reduce; otherwise the block covers all columns and writes y.
+template <bool VEC>
+__global__ void __launch_bounds__(256) k_sgemv_n(int m, int n, int chunk, float alpha, const float *__restrict__ A,
+                                                 int lda, const float *__restrict__ x, int incx, float beta,
+                                                 float *__restrict__ y, int incy, float *__restrict__ part) {
+    constexpr int RPL = VEC ? 4 : 1;  // rows per lane
+    constexpr int TILE = 32 * RPL;
+    __shared__ float red[8][TILE];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * TILE + lane * RPL;
+    const int j0 = blockIdx.y * chunk, j1 = min(n, j0 + chunk);
+    float acc[RPL];
+#pragma unroll
+    for (int r = 0; r < RPL; r++) acc[r] = 0.f;
+    if (i < m) {
+        int j = j0 + warp;
+        if constexpr (VEC) {
+            for (; j + 24 < j1; j += 32) {  // four independent column loads in flight
+                float4 a[4];
+                float xv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    a[u] = __ldg(reinterpret_cast<const float4 *>(A + (long long)(j + 8 * u) * lda + i));
+                    xv[u] = __ldg(x + (long long)(j + 8 * u) * incx);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    acc[0] = fmaf(a[u].x, xv[u], acc[0]);
+                    acc[1] = fmaf(a[u].y, xv[u], acc[1]);
+                    acc[2] = fmaf(a[u].z, xv[u], acc[2]);
+                    acc[3] = fmaf(a[u].w, xv[u], acc[3]);
+                }
+            }
+            for (; j < j1; j += 8) {
+                const float4 a = __ldg(reinterpret_cast<const float4 *>(A + (long long)j * lda + i));
+                const float xv = __ldg(x + (long long)j * incx);
+                acc[0] = fmaf(a.x, xv, acc[0]);
+                acc[1] = fmaf(a.y, xv, acc[1]);
+                acc[2] = fmaf(a.z, xv, acc[2]);
+                acc[3] = fmaf(a.w, xv, acc[3]);
+            }
+        } else {
+            for (; j < j1; j += 8) acc[0] = fmaf(__ldg(A + (long long)j * lda + i), __ldg(x + (long long)j * incx), acc[0]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RPL; r++) red[warp][lane * RPL + r] = acc[r];
+    __syncthreads();
+    // combine the 8 warp sums of each row in warp order
+    for (int t = threadIdx.x; t < TILE; t += blockDim.x) {
+        const int row = blockIdx.x * TILE + t;
+        if (row >= m) continue;
+        float v = red[0][t];
+#pragma unroll
+        for (int w = 1; w < 8; w++) v += red[w][t];
+        if (part) {
+            part[(long long)blockIdx.y * m + row] = v;
+        } else {
+            float o = alpha * v;
+            if (beta != 0.f) o = fmaf(beta, y[(long long)row * incy], o);
+            y[(long long)row * incy] = o;
+        }
+    }
+}
+
+// y[i] = alpha * (sum over chunks in order of part[c * m + i]) + beta * y[i].
+__global__ void k_sgemv_n_reduce(int m, int nchunks, float alpha, const float *__restrict__ part, float beta,
+                                 float *__restrict__ y, int incy) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     float acc = 0.f;
-    for (int j = 0; j < n; j++) acc = fmaf(A[(long long)j * lda + i], x[(long long)j * incx], acc);
+    for (int c = 0; c < nchunks; c++) acc += part[(long long)c * m + i];
     float v = alpha * acc;
     if (beta != 0.f) v = fmaf(beta, y[(long long)i * incy], v);
     y[(long long)i * incy] = v;
 }
 
-__global__ void k_sgemv_t(int m, int n, float alpha, const float *__restrict__ A, int lda,
-                          const float *__restrict__ x, int incx, float beta, float *__restrict__ y, int incy) {
-    int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp per column
-    int lane = threadIdx.x & 31;
+// y = alpha * A^T x + beta * y, column-major A (m x n): warp per output, i.e. per column of
+// A (a contiguous run: the warp-per-row GEMV of a source-major matrix).  VEC: float4 loads
+// of the column and of x, two accumulators in a fixed order.
+template <bool VEC>
+__global__ void __launch_bounds__(256) k_sgemv_t(int m, int n, float alpha, const float *__restrict__ A, int lda,
+                                                 const float *__restrict__ x, int incx, float beta,
+                                                 float *__restrict__ y, int incy) {
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp per column
+    const int lane = threadIdx.x & 31;
     if (j >= n) return;
-    float acc = 0.f;
     const float *col = A + (long long)j * lda;
-    for (int i = lane; i < m; i += 32) acc = fmaf(col[i], x[(long long)i * incx], acc);
+    float acc0 = 0.f, acc1 = 0.f;
+    int tail = 0;
+    if constexpr (VEC) {
+        const int m4 = m >> 2;
+        const float4 *c4 = reinterpret_cast<const float4 *>(col);
+        const float4 *x4 = reinterpret_cast<const float4 *>(x);
+        int q = lane;
+        for (; q + 32 < m4; q += 64) {
+            const float4 a0 = __ldg(c4 + q), b0 = __ldg(x4 + q);
+            const float4 a1 = __ldg(c4 + q + 32), b1 = __ldg(x4 + q + 32);
+            acc0 = fmaf(a0.x, b0.x, acc0); acc0 = fmaf(a0.y, b0.y, acc0);
+            acc0 = fmaf(a0.z, b0.z, acc0); acc0 = fmaf(a0.w, b0.w, acc0);
+            acc1 = fmaf(a1.x, b1.x, acc1); acc1 = fmaf(a1.y, b1.y, acc1);
+            acc1 = fmaf(a1.z, b1.z, acc1); acc1 = fmaf(a1.w, b1.w, acc1);
+        }
+        if (q < m4) {
+            const float4 a0 = __ldg(c4 + q), b0 = __ldg(x4 + q);
+            acc0 = fmaf(a0.x, b0.x, acc0); acc0 = fmaf(a0.y, b0.y, acc0);
+            acc0 = fmaf(a0.z, b0.z, acc0); acc0 = fmaf(a0.w, b0.w, acc0);
+        }
+        tail = m4 << 2;
+    }
+    for (int i = tail + lane; i < m; i += 32) acc0 = fmaf(__ldg(col + i), __ldg(x + (long long)i * incx), acc0);
+    float acc = acc0 + acc1;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) {
@@ -44,6 +144,27 @@ __global__ void k_sgemv_t(int m, int n, float alpha, const float *__restrict__ A
         if (beta != 0.f) v = fmaf(beta, y[(long long)j * incy], v);
         y[(long long)j * incy] = v;
     }
+}
+
+// Per-device buffer for the column-chunk partials of opcuda_sgemv, grown on demand
+// (cudaMalloc on the first call that needs more, kept until exit).
+static float *g_gemv_part[64] = {nullptr};
+static size_t g_gemv_cap[64] = {0};
+static std::mutex g_gemv_mu;
+
+static int gemv_part_buffer(size_t floats, float **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return OPB_E_UNSUPPORTED;
+    std::lock_guard<std::mutex> lk(g_gemv_mu);
+    if (g_gemv_cap[dev] < floats) {
+        if (g_gemv_part[dev]) cudaFree(g_gemv_part[dev]);
+        g_gemv_part[dev] = nullptr;
+        g_gemv_cap[dev] = 0;
+        if (cudaMalloc(&g_gemv_part[dev], floats * sizeof(float)) != cudaSuccess) return OPB_E_NOMEM;
+        g_gemv_cap[dev] = floats;
+    }
+    *out = g_gemv_part[dev];
+    return OPB_OK;
 }
 
 // Multi-vector product for rows [row0, row0 + 128) and the 16 list entries starting at c0.
@@ -158,9 +279,30 @@ OPB_API int opcuda_sgemv(int m, int n, float alpha, uint64_t A, int lda, uint64_
     if (m == 0) return set_status(OPB_OK);
     OPB_REQUIRE(y != 0 && (n == 0 || (A != 0 && x != 0)), OPB_E_NULL);
     OPB_REQUIRE(lda >= (m > 1 ? m : 1) && incx > 0 && incy > 0, OPB_E_ARG);
-    k_sgemv_n<<<(m + 255) / 256, 256, 0, stream()>>>(m, n, alpha, reinterpret_cast<const float *>(A), lda,
-                                                      reinterpret_cast<const float *>(x), incx, beta,
-                                                      reinterpret_cast<float *>(y), incy);
+    const float *pA = reinterpret_cast<const float *>(A);
+    const float *px = reinterpret_cast<const float *>(x);
+    float *py = reinterpret_cast<float *>(y);
+    // float4 rows when every column starts 16-byte aligned and m is a multiple of 4
+    const bool vec = m % 4 == 0 && lda % 4 == 0 && aligned(pA, 16);
+    const int rows_per_block = vec ? 128 : 32;
+    const int tiles = (m + rows_per_block - 1) / rows_per_block;
+    // column chunks: about 8 blocks per SM in total
+    int nch = (8 * num_sms() + tiles - 1) / tiles;
+    if (nch > n) nch = n;
+    if (nch < 1) nch = 1;
+    const int chunk = n > 0 ? (n + nch - 1) / nch : 1;
+    nch = n > 0 ? (n + chunk - 1) / chunk : 1;
+    float *part = nullptr;
+    if (nch > 1) {
+        const int r = gemv_part_buffer((size_t)nch * m, &part);
+        if (r != OPB_OK) return set_status(r);
+    }
+    dim3 g(tiles, nch);
+    if (vec)
+        k_sgemv_n<true><<<g, 256, 0, stream()>>>(m, n, chunk, alpha, pA, lda, px, incx, beta, py, incy, part);
+    else
+        k_sgemv_n<false><<<g, 256, 0, stream()>>>(m, n, chunk, alpha, pA, lda, px, incx, beta, py, incy, part);
+    if (part) k_sgemv_n_reduce<<<(m + 255) / 256, 256, 0, stream()>>>(m, nch, alpha, part, beta, py, incy);
     return launch_check();
 }
 
@@ -171,9 +313,15 @@ OPB_API int opcuda_sgemvT(int m, int n, float alpha, uint64_t A, int lda, uint64
     OPB_REQUIRE(y != 0 && (m == 0 || (A != 0 && x != 0)), OPB_E_NULL);
     OPB_REQUIRE(lda >= (m > 1 ? m : 1) && incx > 0 && incy > 0, OPB_E_ARG);
     long long threads = 32LL * n;
-    k_sgemv_t<<<(int)((threads + 255) / 256), 256, 0, stream()>>>(m, n, alpha, reinterpret_cast<const float *>(A), lda,
-                                                                    reinterpret_cast<const float *>(x), incx, beta,
-                                                                    reinterpret_cast<float *>(y), incy);
+    const float *pA = reinterpret_cast<const float *>(A);
+    const float *px = reinterpret_cast<const float *>(x);
+    const bool vec = lda % 4 == 0 && incx == 1 && aligned(pA, 16) && aligned(px, 16);
+    if (vec)
+        k_sgemv_t<true><<<(int)((threads + 255) / 256), 256, 0, stream()>>>(m, n, alpha, pA, lda, px, incx, beta,
+                                                                         reinterpret_cast<float *>(y), incy);
+    else
+        k_sgemv_t<false><<<(int)((threads + 255) / 256), 256, 0, stream()>>>(m, n, alpha, pA, lda, px, incx, beta,
+                                                                          reinterpret_cast<float *>(y), incy);
     return launch_check();
 }
 

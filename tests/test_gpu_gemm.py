@@ -345,3 +345,36 @@ def test_opcuda_sglvg_matches_oracle_generator(cuda):
     got = dg.cpu().numpy().reshape(d, d).T  # column-major -> [source, target]
     ref = O.lv_generator(x, 0.03 * x, sig * x)
     assert np.allclose(got, ref, rtol=2e-4, atol=1e-3 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("m,n,lda,incx", [(2048, 1536, 2048, 1), (301, 77, 301, 1), (300, 500, 304, 2),
+                                          (6144, 6144, 6144, 1), (4, 1, 4, 1)])
+def test_opcuda_sgemv_paths(cuda, m, n, lda, incx):
+    """Both GEMV directions on every kernel path: float4 and scalar rows, column chunks
+    with the ordered partial reduction (large n), padded leading dimension and strided x
+    (scalar warp-per-column path); against FP64 within the FP32 bound."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(m + n)
+    A = rng.standard_normal((lda, n)).astype(np.float32)   # column-major storage, rows >= m used
+    dA = torch.from_numpy(np.asfortranarray(A).ravel(order="K").copy()).to(cuda)
+    Am = A[:m].astype(np.float64)
+    for trans in (False, True):
+        nx, ny = (n, m) if not trans else (m, n)
+        x = rng.standard_normal(nx * incx).astype(np.float32)
+        y0 = rng.standard_normal(ny).astype(np.float32)
+        dx, dy = torch.from_numpy(x).to(cuda), torch.from_numpy(y0.copy()).to(cuda)
+        f = lib.opcuda_sgemvT if trans else lib.opcuda_sgemv
+        assert f(m, n, 1.5, dA.data_ptr(), lda, dx.data_ptr(), incx, -0.5, dy.data_ptr(), 1) == 0
+        torch.cuda.synchronize()
+        xv = x[::incx].astype(np.float64)
+        M = Am.T if trans else Am
+        ref = 1.5 * (M @ xv) - 0.5 * y0
+        bound = 1.5 * (np.abs(M) @ np.abs(xv)) * (M.shape[1] + 8) * 2.0 ** -24 + 0.5 * np.abs(y0) * 2.0 ** -23
+        err = np.abs(dy.cpu().numpy() - ref)
+        assert np.all(err <= bound + 1e-6), (trans, float((err / (bound + 1e-30)).max()))
+        # deterministic: a second call gives the same bits
+        dy2 = torch.from_numpy(y0.copy()).to(cuda)
+        assert f(m, n, 1.5, dA.data_ptr(), lda, dx.data_ptr(), incx, -0.5, dy2.data_ptr(), 1) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(dy, dy2)
