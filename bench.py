@@ -610,8 +610,17 @@ def run_batch(args):
             sample = order[:8] + order[-4:]
             refs = {i: _fp64_lv_quotes(lats[i], b.plans[i], strikes, 8, 0.25, torch) for i in sample}
         errs = {int(i): float((q[i] - refs[i]).abs().max().item()) for i in sample}
+        # whole-sweep time of every configuration (the autotuner picks on level 0 alone)
+        sweep_ms = []
+        if mname == "fp16x3":
+            chosen = b.config
+            for cfg in range(_lib.load().opb_batch_num_configs()):
+                b.set_config(cfg)
+                b.execute(q)
+                sweep_ms.append(round(_time(lambda: b.execute(q), 2, stream, torch), 2))
+            b.set_config(chosen)
         res[mname] = dict(ms=ms, plan_s=t_plan, tune=b.tune_ms, cfg=b.config, launches=b.launches(), errs=errs,
-                          q=q, plans=b.plans)
+                          q=q, plans=b.plans, sweep_ms=sweep_ms)
         del g, b
     prim = res["fp16x3"]
     ms = prim["ms"]
@@ -626,6 +635,7 @@ def run_batch(args):
             "useful_tflops": round(useful / (ms * 1e-3) / 1e12, 1),
             "mma_tflops": round(3 * useful / (ms * 1e-3) / 1e12, 1),
             "autotune_ms_level0": [round(x, 3) for x in prim["tune"]], "config_chosen": prim["cfg"],
+            "sweep_ms_per_config": prim["sweep_ms"],
             "launches_per_sweep": prim["launches"], "plan_seconds": round(prim["plan_s"], 2),
             "max_abs_err_vs_fp64_sample": max(prim["errs"].values()), "sample_errs": prim["errs"],
             "bf16x3": {"quotes_per_s": round(nquotes / (res["bf16x3"]["ms"] * 1e-3), 1),

@@ -92,6 +92,7 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_set_tile_n": (i32, [i32]),
     "opb_gemm_f16x3": (i32, [i32, i32, i32, vp, vp, i64, vp, vp, i64, f32, vp, f32, vp, i64, vp]),
     "opb_tc_error": (i32, []),
+    "opb_batch_num_configs": (i32, []),
     "opb_lv_generator_ell_batched": (i32, [i32, vp, i64, f64, f64, f64, vp, vp]),
     "opb_lv_param_size": (i32, []),
     "opcuda_sgsvg": (i32, [u64, i32, i32, i32, u64, u64]),

@@ -51,8 +51,11 @@ struct opb_batch_desc {
 
 namespace {
 
-constexpr int NCFG = 4;  // (bn, order): (128, LPT), (64, LPT), (128, lattice), (64, lattice)
-constexpr int CFG_BN[NCFG] = {128, 64, 128, 64};
+// (bn, order): (128, LPT), (64, LPT), (128, lattice), (64, lattice), (256 mixed, LPT),
+// (256 mixed, lattice).  "256 mixed": 128 x 256 tiles for the lattices whose size is a
+// multiple of 256, 128 x 128 tiles for the rest (two launches per level).
+constexpr int NCFG = 6;
+constexpr int CFG_BN[NCFG] = {128, 64, 128, 64, 256, 256};
 
 // mirror of opb_lattice_desc (lattice.cu), used for the FP32 per-lattice path
 struct LatticeDescMirror {
@@ -87,7 +90,7 @@ struct opb_batch_plan {
     opb::BatchLattice *lats = nullptr;
     opb::TcProblem *sq = nullptr, *chain = nullptr, *price = nullptr;
     opb::RenormProblem *rn_sq = nullptr, *rn_chain = nullptr;
-    CUtensorMap *maps_sq[2] = {nullptr, nullptr};  // per bn (128, 64)
+    CUtensorMap *maps_sq[3] = {nullptr, nullptr, nullptr};  // per bn (128, 64, 256)
     CUtensorMap *maps_price = nullptr;
     uint32_t *work = nullptr;
     float *E_base = nullptr;
@@ -95,6 +98,8 @@ struct opb_batch_plan {
     // work lists (offsets into `work`)
     std::vector<ListRef> gemm_level[NCFG];
     ListRef gemm_chain[NCFG];
+    std::vector<ListRef> gemm_level_rest[NCFG];  // 256 mixed: the 128 x 128 items
+    ListRef gemm_chain_rest[NCFG];
     ListRef gemm_price;
     std::vector<ListRef> rn_level;
     ListRef rn_init, rn_chain_list;
@@ -164,6 +169,7 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     auto m128 = c.take<CUtensorMap>(4 * (size_t)n);
     auto m64 = c.take<CUtensorMap>(4 * (size_t)n);
     auto mp = c.take<CUtensorMap>(4 * (size_t)n);
+    auto m256 = c.take<CUtensorMap>(4 * (size_t)n);
     size_t Etot = 0;
     for (int i = 0; i < n; i++) Etot += (size_t)b->d[i] * b->d[i];
     float *E = c.take<float>(Etot);
@@ -185,10 +191,12 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     std::stable_sort(lpt.begin(), lpt.end(), [&](int a, int bb) { return b->d[a] > b->d[bb]; });
     int maxn = 0;
     for (int i = 0; i < n; i++) maxn = std::max(maxn, b->niter[i]);
-    auto gemm_list = [&](const std::vector<int> &order, int bn, int level, bool chain_or_all) {
+    // sel: 0 every lattice, 1 only sizes that are multiples of 256, 2 only the others
+    auto gemm_list = [&](const std::vector<int> &order, int bn, int level, bool chain_or_all, int sel = 0) {
         ListRef r{W.size(), 0};
         for (int i : order) {
             if (!chain_or_all && b->niter[i] <= level) continue;
+            if ((sel == 1 && b->d[i] % 256) || (sel == 2 && b->d[i] % 256 == 0)) continue;
             const int mt = b->d[i] / 128, nt = b->d[i] / bn;
             for (int a = 0; a < mt; a++)
                 for (int bb = 0; bb < nt; bb++) W.push_back(((uint32_t)i << 16) | ((uint32_t)a << 8) | (uint32_t)bb);
@@ -196,12 +204,25 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
         r.n = (int)(W.size() - r.off);
         return r;
     };
-    std::vector<ListRef> gl[NCFG];
-    ListRef gch[NCFG];
+    std::vector<ListRef> gl[NCFG], glr[NCFG];
+    ListRef gch[NCFG], gchr[NCFG];
     for (int cfg = 0; cfg < NCFG; cfg++) {
-        const auto &order = cfg < 2 ? lpt : nat;
-        for (int lv = 0; lv < maxn; lv++) gl[cfg].push_back(gemm_list(order, CFG_BN[cfg], lv, false));
-        gch[cfg] = gemm_list(order, CFG_BN[cfg], 0, true);
+        const auto &order = (cfg < 2 || cfg == 4) ? lpt : nat;
+        if (CFG_BN[cfg] == 256) {
+            for (int lv = 0; lv < maxn; lv++) {
+                gl[cfg].push_back(gemm_list(order, 256, lv, false, 1));
+                glr[cfg].push_back(gemm_list(order, 128, lv, false, 2));
+            }
+            gch[cfg] = gemm_list(order, 256, 0, true, 1);
+            gchr[cfg] = gemm_list(order, 128, 0, true, 2);
+        } else {
+            for (int lv = 0; lv < maxn; lv++) {
+                gl[cfg].push_back(gemm_list(order, CFG_BN[cfg], lv, false));
+                glr[cfg].push_back(ListRef{W.size(), 0});
+            }
+            gch[cfg] = gemm_list(order, CFG_BN[cfg], 0, true);
+            gchr[cfg] = ListRef{W.size(), 0};
+        }
     }
     ListRef gpr{W.size(), 0};
     for (int i : lpt)
@@ -238,9 +259,14 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     P->total_rows = off[n]; P->ell_width = b->ell_width; P->cols = b->gen_cols; P->vals = b->gen_vals;
     P->x = b->x; P->strikes = b->strikes; P->period = b->period;
     P->lats = lats; P->sq = sq; P->chain = ch; P->price = pr; P->rn_sq = rs; P->rn_chain = rc;
-    P->maps_sq[0] = m128; P->maps_sq[1] = m64; P->maps_price = mp; P->work = work;
+    P->maps_sq[0] = m128; P->maps_sq[1] = m64; P->maps_sq[2] = m256; P->maps_price = mp; P->work = work;
     P->E_base = E; P->E_bytes = Etot * sizeof(float);
-    for (int cfg = 0; cfg < NCFG; cfg++) { P->gemm_level[cfg] = gl[cfg]; P->gemm_chain[cfg] = gch[cfg]; }
+    for (int cfg = 0; cfg < NCFG; cfg++) {
+        P->gemm_level[cfg] = gl[cfg];
+        P->gemm_chain[cfg] = gch[cfg];
+        P->gemm_level_rest[cfg] = glr[cfg];
+        P->gemm_chain_rest[cfg] = gchr[cfg];
+    }
     P->gemm_price = gpr; P->rn_level = rl; P->rn_init = rinit; P->rn_chain_list = rch;
     if (work_out) *work_out = W;
     return total;
@@ -290,12 +316,13 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     std::vector<opb::BatchLattice> lats(n);
     std::vector<opb::TcProblem> sq(n), ch(n), pr(n);
     std::vector<opb::RenormProblem> rs(n), rc(n);
-    std::vector<CUtensorMap> m128(4 * (size_t)n), m64(4 * (size_t)n), mp(4 * (size_t)n);
+    std::vector<CUtensorMap> m128(4 * (size_t)n), m64(4 * (size_t)n), mp(4 * (size_t)n), m256(4 * (size_t)n);
     // recompute buffer pointers exactly as layout() carved them
     Carve cv{base, 0};
     cv.take<opb::BatchLattice>(n); cv.take<opb::TcProblem>(n); cv.take<opb::TcProblem>(n); cv.take<opb::TcProblem>(n);
     cv.take<opb::RenormProblem>(n); cv.take<opb::RenormProblem>(n);
     cv.take<CUtensorMap>(4 * (size_t)n); cv.take<CUtensorMap>(4 * (size_t)n); cv.take<CUtensorMap>(4 * (size_t)n);
+    cv.take<CUtensorMap>(4 * (size_t)n);
     size_t Etot = 0;
     for (int i = 0; i < n; i++) Etot += (size_t)b->d[i] * b->d[i];
     float *E = cv.take<float>(Etot), *Pa = cv.take<float>(Etot);
@@ -334,6 +361,9 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
         if (rc_status == OPB_OK)
             rc_status =
                 opb::tc_make_maps(&mp[4 * (size_t)i], Ah + eo, Al + eo, d, d, L.GThi, L.GTlo, P->ldk, d, d, 64, f16);
+        if (rc_status == OPB_OK && d % 256 == 0)  // 128 x 256 tiles only for sizes that are multiples of 256
+            rc_status =
+                opb::tc_make_maps(&m256[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 256, f16);
         eo += (size_t)d * d;
         po += (size_t)(d / 64) * d;
         ro += d;
@@ -355,6 +385,7 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     if (e == cudaSuccess) e = up(P->maps_sq[0], m128.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
     if (e == cudaSuccess) e = up(P->maps_sq[1], m64.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
     if (e == cudaSuccess) e = up(P->maps_price, mp.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
+    if (e == cudaSuccess) e = up(P->maps_sq[2], m256.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
     if (e == cudaSuccess) e = up(P->work, W.data(), sizeof(uint32_t) * W.size());
     if (e != cudaSuccess) {
         delete P;
@@ -366,13 +397,16 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     return set_status(OPB_OK);
 }
 
+OPB_API int opb_batch_num_configs(void) { return NCFG; }
+
 OPB_API int opb_batch_plan_destroy(opb_batch_plan *P) {
     delete P;
     return set_status(OPB_OK);
 }
 
-// Selects the launch configuration: cfg 0..3 = (BN 128, longest-K first), (64, longest
-// first), (128, lattice order), (64, lattice order); grid 0 = one CTA per SM.
+// Selects the launch configuration: cfg 0..5 = (BN 128, longest-K first), (64, longest
+// first), (128, lattice order), (64, lattice order), (256 mixed, longest first), (256
+// mixed, lattice order); grid 0 = one CTA per SM.
 OPB_API int opb_batch_set_config(opb_batch_plan *P, int cfg, int grid) {
     OPB_REQUIRE(P, OPB_E_NULL);
     OPB_REQUIRE(cfg >= 0 && cfg < NCFG && grid >= 0, OPB_E_ARG);
@@ -383,10 +417,22 @@ OPB_API int opb_batch_set_config(opb_batch_plan *P, int cfg, int grid) {
 
 namespace {
 
+int map_index(int bn) { return bn == 128 ? 0 : (bn == 64 ? 1 : 2); }
+
+// One squaring level (or, with chain, the chain product) under configuration cfg: one
+// launch, or two for the 256-mixed configurations (128 x 256 items, then 128 x 128 ones).
+int cfg_gemm(opb_batch_plan *P, int cfg, const opb::TcProblem *probs, const ListRef &l, const ListRef &rest,
+             cudaStream_t s) {
+    const int bn = CFG_BN[cfg];
+    int r = opb::launch_tc_gemm_batched(bn, P->maps_sq[map_index(bn)], probs, P->work + l.off, l.n, P->grid, s,
+                                        P->f16);
+    if (r == 0 && rest.n > 0)
+        r = opb::launch_tc_gemm_batched(128, P->maps_sq[0], probs, P->work + rest.off, rest.n, P->grid, s, P->f16);
+    return r;
+}
+
 int level_gemm(opb_batch_plan *P, int cfg, int level, cudaStream_t s) {
-    const ListRef &l = P->gemm_level[cfg][level];
-    const int bi = CFG_BN[cfg] == 128 ? 0 : 1;
-    return opb::launch_tc_gemm_batched(CFG_BN[cfg], P->maps_sq[bi], P->sq, P->work + l.off, l.n, P->grid, s, P->f16);
+    return cfg_gemm(P, cfg, P->sq, P->gemm_level[cfg][level], P->gemm_level_rest[cfg][level], s);
 }
 
 }  // namespace
@@ -419,11 +465,9 @@ OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
         BT(opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_level[lv].off, P->rn_level[lv].n, pdiv, s, ss));
     }
     BT(opb::launch_payoff_batched(P->lats, P->nlat, P->total_rows, P->nK, P->ldk, P->x, P->strikes, s, P->f16));
-    const int bi = bn == 128 ? 0 : 1;
     for (int m = 1; m <= P->nmat; m++) {
         if (m > 1) {
-            const ListRef &l = P->gemm_chain[cfg];
-            BT(opb::launch_tc_gemm_batched(bn, P->maps_sq[bi], P->chain, P->work + l.off, l.n, P->grid, s, P->f16));
+            BT(cfg_gemm(P, cfg, P->chain, P->gemm_chain[cfg], P->gemm_chain_rest[cfg], s));
             BT(opb::launch_renorm_batched(P->rn_chain, P->work + P->rn_chain_list.off, P->rn_chain_list.n, pdiv, s,
                                           ss));
         }
@@ -436,7 +480,8 @@ OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
 }
 
 // Times the level-0 squaring launch (all lattices active) for every configuration with
-// CUDA events and keeps the fastest; ms[cfg] (optional, 4 entries) receives the times.
+// CUDA events and keeps the fastest; ms[cfg] (optional, opb_batch_num_configs() entries)
+// receives the times.
 // Blocking; leaves the plan's buffers in an arbitrary state (run execute afterwards).
 OPB_API int opb_batch_autotune(opb_batch_plan *P, int reps, float *ms_out, int *best_cfg) {
     OPB_REQUIRE(P, OPB_E_NULL);

@@ -485,8 +485,10 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? 
             int prob, m0, n0, nkb;
             get_item(t, prob, m0, n0, nkb);
             const int nch = (nkb + Cfg::CHUNK - 1) / Cfg::CHUNK;
+            if constexpr (NPROD != 1) {  // single products have one chunk: its values are the sums
 #pragma unroll
-            for (int j = 0; j < CPT; j++) sum[j] = 0.f;
+                for (int j = 0; j < CPT; j++) sum[j] = 0.f;
+            }
             for (int c = 0; c < nch; c++, g++) {
                 const int a = (int)(g & 1);
                 if (!mbar_wait(accf_bar(a), (uint32_t)((g >> 1) & 1), abort_flag, TC_WAIT_NS)) {
@@ -500,7 +502,12 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? 
                     uint32_t v[32];
                     tmem_ld32(tacc + (uint32_t)(32 * j), v);
 #pragma unroll
-                    for (int i = 0; i < 32; i++) sum[32 * j + i] = __fadd_rn(sum[32 * j + i], __uint_as_float(v[i]));
+                    for (int i = 0; i < 32; i++) {
+                        if constexpr (NPROD == 1)
+                            sum[32 * j + i] = __uint_as_float(v[i]);
+                        else
+                            sum[32 * j + i] = __fadd_rn(sum[32 * j + i], __uint_as_float(v[i]));
+                    }
                 }
                 tc_fence_before();
                 if constexpr (PAIR) {
@@ -792,6 +799,8 @@ int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *pro
     if (nwork <= 0) return OPB_OK;
     if (grid <= 0 || grid > nwork) grid = nwork < num_sms() ? nwork : num_sms();
     switch (bn * 2 + (f16 ? 1 : 0)) {
+        case 512: return launch_batched_impl<256, 2, false>(maps, probs, work, nwork, grid, s);
+        case 513: return launch_batched_impl<256, 2, true>(maps, probs, work, nwork, grid, s);
         case 256: return launch_batched_impl<128, 3, false>(maps, probs, work, nwork, grid, s);
         case 257: return launch_batched_impl<128, 3, true>(maps, probs, work, nwork, grid, s);
         case 128: return launch_batched_impl<64, 4, false>(maps, probs, work, nwork, grid, s);

@@ -105,7 +105,7 @@ struct TcProblem {
 int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo, long long M, long long lda,
                  const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long N, long long ldb, long long K, int bn,
                  int f16 = 0);
-// work: packed (problem << 16 | m-tile << 8 | n-tile); bn in {64, 128}
+// work: packed (problem << 16 | m-tile << 8 | n-tile); bn in {64, 128, 256}
 int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
                            int grid, cudaStream_t s, int f16 = 0);
 

@@ -250,7 +250,7 @@ class Batch:
         call("opb_batch_plan_create", C.byref(bd), self.mode, _ptr(self.ws), self.ws.numel(), C.byref(self.plan))
         self.tune_ms = None
         if autotune and self.mode in (BF16X3, FP16X3):
-            ms = (C.c_float * 4)()
+            ms = (C.c_float * lib.opb_batch_num_configs())()
             best = C.c_int()
             call("opb_batch_autotune", self.plan, 2, ms, C.byref(best))
             self.tune_ms = list(ms)
