@@ -258,8 +258,8 @@ unsigned long long opb_batch_workspace_size(const opb_batch_desc *b, int mode);
 int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *workspace, unsigned long long ws_bytes,
                           opb_batch_plan **out);
 int opb_batch_plan_destroy(opb_batch_plan *plan);
-/* cfg < opb_batch_num_configs(): tile width x work order (128, 64 or 256-mixed; longest
- * first or lattice order); grid 0 = one CTA per SM */
+/* cfg < opb_batch_num_configs(): tile width x work order (128, 64, 256-mixed or 256 on
+ * CTA pairs mixed; longest first or lattice order); grid 0 = one CTA per SM */
 int opb_batch_set_config(opb_batch_plan *plan, int cfg, int grid);
 int opb_batch_num_configs(void);
 int opb_batch_execute(opb_batch_plan *plan, double *quotes);

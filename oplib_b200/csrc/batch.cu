@@ -52,10 +52,13 @@ struct opb_batch_desc {
 namespace {
 
 // (bn, order): (128, LPT), (64, LPT), (128, lattice), (64, lattice), (256 mixed, LPT),
-// (256 mixed, lattice).  "256 mixed": 128 x 256 tiles for the lattices whose size is a
-// multiple of 256, 128 x 128 tiles for the rest (two launches per level).
-constexpr int NCFG = 6;
-constexpr int CFG_BN[NCFG] = {128, 64, 128, 64, 256, 256};
+// (256 mixed, lattice), (256 pair mixed, LPT), (256 pair mixed, lattice).  "256 mixed":
+// 128 x 256 tiles for the lattices whose size is a multiple of 256, 128 x 128 tiles for
+// the rest (two launches per level); "256 pair mixed": 256 x 256 tiles on 2-CTA clusters
+// for those lattices instead.
+constexpr int NCFG = 8;
+constexpr int CFG_BN[NCFG] = {128, 64, 128, 64, 256, 256, 256, 256};
+constexpr bool CFG_PAIR[NCFG] = {false, false, false, false, false, false, true, true};
 
 // mirror of opb_lattice_desc (lattice.cu), used for the FP32 per-lattice path
 struct LatticeDescMirror {
@@ -192,12 +195,13 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     int maxn = 0;
     for (int i = 0; i < n; i++) maxn = std::max(maxn, b->niter[i]);
     // sel: 0 every lattice, 1 only sizes that are multiples of 256, 2 only the others
-    auto gemm_list = [&](const std::vector<int> &order, int bn, int level, bool chain_or_all, int sel = 0) {
+    auto gemm_list = [&](const std::vector<int> &order, int bn, int level, bool chain_or_all, int sel = 0,
+                         int tile_m = 128) {
         ListRef r{W.size(), 0};
         for (int i : order) {
             if (!chain_or_all && b->niter[i] <= level) continue;
             if ((sel == 1 && b->d[i] % 256) || (sel == 2 && b->d[i] % 256 == 0)) continue;
-            const int mt = b->d[i] / 128, nt = b->d[i] / bn;
+            const int mt = b->d[i] / tile_m, nt = b->d[i] / bn;
             for (int a = 0; a < mt; a++)
                 for (int bb = 0; bb < nt; bb++) W.push_back(((uint32_t)i << 16) | ((uint32_t)a << 8) | (uint32_t)bb);
         }
@@ -207,13 +211,14 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     std::vector<ListRef> gl[NCFG], glr[NCFG];
     ListRef gch[NCFG], gchr[NCFG];
     for (int cfg = 0; cfg < NCFG; cfg++) {
-        const auto &order = (cfg < 2 || cfg == 4) ? lpt : nat;
+        const auto &order = (cfg < 2 || cfg == 4 || cfg == 6) ? lpt : nat;
         if (CFG_BN[cfg] == 256) {
+            const int tm = CFG_PAIR[cfg] ? 256 : 128;
             for (int lv = 0; lv < maxn; lv++) {
-                gl[cfg].push_back(gemm_list(order, 256, lv, false, 1));
+                gl[cfg].push_back(gemm_list(order, 256, lv, false, 1, tm));
                 glr[cfg].push_back(gemm_list(order, 128, lv, false, 2));
             }
-            gch[cfg] = gemm_list(order, 256, 0, true, 1);
+            gch[cfg] = gemm_list(order, 256, 0, true, 1, tm);
             gchr[cfg] = gemm_list(order, 128, 0, true, 2);
         } else {
             for (int lv = 0; lv < maxn; lv++) {
@@ -404,9 +409,10 @@ OPB_API int opb_batch_plan_destroy(opb_batch_plan *P) {
     return set_status(OPB_OK);
 }
 
-// Selects the launch configuration: cfg 0..5 = (BN 128, longest-K first), (64, longest
+// Selects the launch configuration: cfg 0..7 = (BN 128, longest-K first), (64, longest
 // first), (128, lattice order), (64, lattice order), (256 mixed, longest first), (256
-// mixed, lattice order); grid 0 = one CTA per SM.
+// mixed, lattice order), (256 pair mixed, longest first), (256 pair mixed, lattice
+// order); grid 0 = one CTA per SM (the pair launches size their own grid).
 OPB_API int opb_batch_set_config(opb_batch_plan *P, int cfg, int grid) {
     OPB_REQUIRE(P, OPB_E_NULL);
     OPB_REQUIRE(cfg >= 0 && cfg < NCFG && grid >= 0, OPB_E_ARG);
@@ -424,8 +430,11 @@ int map_index(int bn) { return bn == 128 ? 0 : (bn == 64 ? 1 : 2); }
 int cfg_gemm(opb_batch_plan *P, int cfg, const opb::TcProblem *probs, const ListRef &l, const ListRef &rest,
              cudaStream_t s) {
     const int bn = CFG_BN[cfg];
-    int r = opb::launch_tc_gemm_batched(bn, P->maps_sq[map_index(bn)], probs, P->work + l.off, l.n, P->grid, s,
-                                        P->f16);
+    // pair items: each CTA loads 128 rows of A and of B, the 128-row maps
+    int r = CFG_PAIR[cfg]
+                ? opb::launch_tc_gemm_batched_pair(P->maps_sq[0], probs, P->work + l.off, l.n, s, P->f16)
+                : opb::launch_tc_gemm_batched(bn, P->maps_sq[map_index(bn)], probs, P->work + l.off, l.n, P->grid,
+                                              s, P->f16);
     if (r == 0 && rest.n > 0)
         r = opb::launch_tc_gemm_batched(128, P->maps_sq[0], probs, P->work + rest.off, rest.n, P->grid, s, P->f16);
     return r;
@@ -523,5 +532,8 @@ OPB_API int opb_batch_autotune(opb_batch_plan *P, int reps, float *ms_out, int *
 OPB_API int opb_batch_launches(const opb_batch_plan *P) {
     if (!P) return 0;
     if (!tc_mode_b(P->mode)) return -1;
-    return 3 + 2 * P->maxn + 1 + (P->f16 ? 1 : 0) + 2 * P->nmat + 2 * (P->nmat - 1);
+    int extra = 0;  // the 256-mixed configurations' second GEMM launch per level / chain
+    for (int lv = 0; lv < P->maxn; lv++) extra += P->gemm_level_rest[P->cfg][lv].n > 0 ? 1 : 0;
+    if (P->gemm_chain_rest[P->cfg].n > 0) extra += P->nmat - 1;
+    return 3 + 2 * P->maxn + 1 + (P->f16 ? 1 : 0) + 2 * P->nmat + 2 * (P->nmat - 1) + extra;
 }

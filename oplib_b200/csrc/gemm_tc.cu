@@ -270,7 +270,6 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? 
     // network layers (EPIMODE >= 1) run twice the epilogue warps: their per-element GELU,
     // not the MMAs, bounds a tile
     using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? TC_LAYER_CPT : 128)>;
-    static_assert(!(PAIR && BATCHED), "pair mode is for single products");
     constexpr int EPI = Cfg::EPI_WARPS;
     constexpr int CPT = Cfg::CPT;
     extern __shared__ uint8_t smem_raw[];
@@ -299,7 +298,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? 
         if constexpr (BATCHED) {
             const uint32_t w = bt.work[t];
             prob = (int)(w >> 16);
-            m0 = (int)((w >> 8) & 255u) * TC_BM;
+            m0 = (int)((w >> 8) & 255u) * Cfg::TILE_M;  // pair mode: 256-row items
             n0 = (int)(w & 255u) * BN;
             nkb = bt.probs[prob].K / BK;
         } else {
@@ -792,6 +791,57 @@ static int launch_batched_impl(const CUtensorMap *maps, const TcProblem *probs, 
     TcBatch bt{maps, probs, work, nwork};
     k_tc_gemm<BN, STAGES, true, F16><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(dummy, dummy, dummy, dummy, p, bt);
     return (int)cudaGetLastError();
+}
+
+// Batched 256 x 256 items on 2-CTA clusters: work items (problem << 16 | m-tile << 8 |
+// n-tile) in 256-row / 256-column units, maps with 128-row boxes for A and B (each CTA
+// loads its own half), problems with M % 256 == 0 and N % 256 == 0.
+template <bool F16>
+static int launch_batched_pair_impl(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
+                                    cudaStream_t s) {
+    constexpr int BN = 256, STAGES = 3;
+    using Cfg = TcCfg<BN, STAGES, 3, TC_BK, true>;
+    auto kern = k_tc_gemm<BN, STAGES, true, F16, 3, 0, TC_BK, true>;
+    int e0 = set_smem_attr<BN, STAGES, true, F16, 3, 0, TC_BK, true>();
+    if (e0) return e0;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(Cfg::THREADS);
+    cfg.dynamicSmemBytes = Cfg::SMEM;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    static int max_clusters[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return OPB_E_UNSUPPORTED;
+    if (!max_clusters[dev]) {
+        cfg.gridDim = dim3(2 * (num_sms() / 2));
+        int n = 0;
+        cudaError_t e = cudaOccupancyMaxActiveClusters(&n, kern, &cfg);
+        if (e != cudaSuccess) return (int)e;
+        if (n <= 0) return OPB_E_UNSUPPORTED;
+        max_clusters[dev] = n;
+    }
+    const int ncl = nwork < max_clusters[dev] ? nwork : max_clusters[dev];
+    cfg.gridDim = dim3(2 * ncl);
+    CUtensorMap dummy;
+    std::memset(&dummy, 0, sizeof(dummy));
+    TcParams p{};
+    TcBatch bt{maps, probs, work, nwork};
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, dummy, dummy, dummy, dummy, p, bt);
+    return e == cudaSuccess ? (int)cudaGetLastError() : (int)e;
+}
+
+int launch_tc_gemm_batched_pair(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
+                                cudaStream_t s, int f16) {
+    if (nwork <= 0) return OPB_OK;
+    return f16 ? launch_batched_pair_impl<true>(maps, probs, work, nwork, s)
+               : launch_batched_pair_impl<false>(maps, probs, work, nwork, s);
 }
 
 int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,

@@ -15,6 +15,7 @@
 // own consecutive rows of a column-major matrix, so every column step is one contiguous
 // 128-byte segment per warp.  Column lists are processed 16 at a time from one pass.
 #include <mutex>
+#include <unordered_map>
 
 #include "common.cuh"
 
@@ -146,24 +147,43 @@ __global__ void __launch_bounds__(256) k_sgemv_t(int m, int n, float alpha, cons
     }
 }
 
-// Per-device buffer for the column-chunk partials of opcuda_sgemv, grown on demand
-// (cudaMalloc on the first call that needs more, kept until exit).
-static float *g_gemv_part[64] = {nullptr};
-static size_t g_gemv_cap[64] = {0};
+// Buffers for the column-chunk partials of opcuda_sgemv, one per (device, stream) so that
+// calls on different streams never share one (calls on one stream run in order); grown on
+// demand (cudaMalloc on the first call that needs more) and kept until exit.
+struct GemvKey {
+    int dev;
+    cudaStream_t s;
+    bool operator==(const GemvKey &o) const { return dev == o.dev && s == o.s; }
+};
+struct GemvKeyHash {
+    size_t operator()(const GemvKey &k) const {
+        return std::hash<void *>()(reinterpret_cast<void *>(k.s)) ^ ((size_t)k.dev * 0x9E3779B97F4A7C15ull);
+    }
+};
+struct GemvBuf {
+    float *p = nullptr;
+    size_t cap = 0;
+};
+static std::unordered_map<GemvKey, GemvBuf, GemvKeyHash> g_gemv_bufs;
 static std::mutex g_gemv_mu;
 
-static int gemv_part_buffer(size_t floats, float **out) {
+static int gemv_part_buffer(cudaStream_t s, size_t floats, float **out) {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return OPB_E_UNSUPPORTED;
+    if (cudaGetDevice(&dev) != cudaSuccess) return OPB_E_UNSUPPORTED;
     std::lock_guard<std::mutex> lk(g_gemv_mu);
-    if (g_gemv_cap[dev] < floats) {
-        if (g_gemv_part[dev]) cudaFree(g_gemv_part[dev]);
-        g_gemv_part[dev] = nullptr;
-        g_gemv_cap[dev] = 0;
-        if (cudaMalloc(&g_gemv_part[dev], floats * sizeof(float)) != cudaSuccess) return OPB_E_NOMEM;
-        g_gemv_cap[dev] = floats;
+    GemvBuf &b = g_gemv_bufs[GemvKey{dev, s}];
+    if (b.cap < floats) {
+        if (b.p) {
+            // the stream's earlier calls may still read the old buffer
+            cudaStreamSynchronize(s);
+            cudaFree(b.p);
+        }
+        b.p = nullptr;
+        b.cap = 0;
+        if (cudaMalloc(&b.p, floats * sizeof(float)) != cudaSuccess) return OPB_E_NOMEM;
+        b.cap = floats;
     }
-    *out = g_gemv_part[dev];
+    *out = b.p;
     return OPB_OK;
 }
 
@@ -294,7 +314,7 @@ OPB_API int opcuda_sgemv(int m, int n, float alpha, uint64_t A, int lda, uint64_
     nch = n > 0 ? (n + chunk - 1) / chunk : 1;
     float *part = nullptr;
     if (nch > 1) {
-        const int r = gemv_part_buffer((size_t)nch * m, &part);
+        const int r = gemv_part_buffer(stream(), (size_t)nch * m, &part);
         if (r != OPB_OK) return set_status(r);
     }
     dim3 g(tiles, nch);

@@ -108,6 +108,10 @@ int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat1
 // work: packed (problem << 16 | m-tile << 8 | n-tile); bn in {64, 128, 256}
 int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
                            int grid, cudaStream_t s, int f16 = 0);
+// 256 x 256 items (256-row / 256-column units) on 2-CTA clusters; maps with 128-row boxes
+// for A and B (the bn = 128 maps); problems with M, N multiples of 256
+int launch_tc_gemm_batched_pair(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
+                                cudaStream_t s, int f16 = 0);
 
 // sck.cu
 int launch_sck_rm(int d, int nrows, const float *P, float *C, cudaStream_t s);

@@ -44,7 +44,7 @@ def test_batch_vs_fp64_and_single(batch_and_refs):
     assert _lib.load().opb_tc_error() == 0
     from oplib_b200 import _lib
     ncfg = _lib.load().opb_batch_num_configs()
-    assert ncfg == 6 and b.config in range(ncfg) and len(b.tune_ms) == ncfg
+    assert ncfg == 8 and b.config in range(ncfg) and len(b.tune_ms) == ncfg
     for i, lat in enumerate(lats):
         err = np.abs(q[i] - refs[i]).max()
         print(f"lattice {i} d={lat.d}: max abs err vs FP64 {err:.2e}")
@@ -62,9 +62,10 @@ def test_batch_configs_agree(batch_and_refs):
         outs.append(b.execute().cpu().numpy())
     for o in outs[1:]:
         assert np.abs(o - outs[0]).max() < 2e-7
-    # 128 x 256 tiles issue the same MMAs per element and the same 128-column row-sum
-    # partials as 128 x 128 ones: the 256-mixed configurations are bit-identical to them
+    # 128 x 256 tiles (one CTA or a CTA pair) issue the same MMAs per element and the same
+    # 128-column row-sum partials as 128 x 128 ones: bit-identical results
     assert np.array_equal(outs[4], outs[0]) and np.array_equal(outs[5], outs[2])
+    assert np.array_equal(outs[6], outs[0]) and np.array_equal(outs[7], outs[2])
     for i in range(len(lats)):
         assert np.abs(outs[1][i] - refs[i]).max() <= 1e-5
 
