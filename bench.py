@@ -124,6 +124,41 @@ def fp64_reference_quotes(lat, plan, torch):
     return torch.stack(out)
 
 
+def fp32_cublas_solve(lat, plan, strikes, torch, out):
+    """The plain-FP32 comparison arm on cuBLAS (TF32 off): U0 = I + dt L in FP32 from the
+    ELL generator, niter squarings and the chain products as cuBLAS SGEMMs, each followed by
+    the FP64 row renormalisation that the 1e-5 bar needs (FP64 row sums, FP32 scaling),
+    pricing P(T_m) G in FP32 and the FP64 discount.  Writes quotes [NMAT, NK] into out."""
+    d = lat.d
+    dev = lat.device
+    cols = lat.cols.view(d, -1).long()
+    vals = lat.vals.view(d, -1)
+    mask = cols >= 0
+    rows = torch.arange(d, device=dev).unsqueeze(1).expand_as(cols)
+    P = torch.zeros(d, d, dtype=torch.float32, device=dev)
+    P.index_put_((rows[mask], cols[mask]), (plan.dt * vals[mask]).float(), accumulate=True)
+    P.diagonal().add_(1.0)
+    T = torch.empty_like(P)
+
+    def renorm(X):
+        s = X.sum(dim=1, dtype=torch.float64)
+        X.mul_((1.0 / s).float().unsqueeze(1))
+
+    for _ in range(plan.niter):
+        torch.mm(P, P, out=T)
+        P, T = T, P
+        renorm(P)
+    G = torch.clamp(lat.x.unsqueeze(1) - strikes.unsqueeze(0), min=0.0).float()
+    Pm = P.clone()
+    for m in range(1, NMAT + 1):
+        if m > 1:
+            torch.mm(Pm, P, out=T)
+            Pm, T = T, Pm
+            renorm(Pm)
+        out[m - 1] = math.exp(-lat.rate * PERIOD * m) * (Pm[lat.y0] @ G).double()
+    return out
+
+
 def run_b200(args, rank, world, local_rank):
     import torch
     from oplib_b200 import _lib
@@ -291,13 +326,28 @@ def run_b200(args, rank, world, local_rank):
         torch.backends.cuda.matmul.allow_tf32 = tf32
         t_si = _time(lambda: _lib.call("opb_sgemm_batched_rm", d, d, d, A32.data_ptr(), 0, A32.data_ptr(), 0,
                                        C32.data_ptr(), 0, 1), 3, stream, torch)
-        nprod = plan.niter + NMAT - 1
-        ms32_cu = ms32 - nprod * (t_si - t_cu)
         extra["fp32_gemm_context"] = {"simt_tflops": round(2.0 * d ** 3 / (t_si * 1e-3) / 1e12, 1),
-                                      "cublas_sgemm_tflops": round(2.0 * d ** 3 / (t_cu * 1e-3) / 1e12, 1),
-                                      "est_fp32_cublas_quotes_per_s": round(NMAT * NK * world / (ms32_cu * 1e-3), 1),
-                                      "est_speedup_vs_fp32_cublas": round(ms32_cu / ms, 2)}
+                                      "cublas_sgemm_tflops": round(2.0 * d ** 3 / (t_cu * 1e-3) / 1e12, 1)}
         del A32, C32
+        # the cuBLAS plain-FP32 solve, measured; "plain FP32" is the faster of the two arms
+        qcu = torch.empty_like(quotes)
+        torch.backends.cuda.matmul.allow_tf32 = False
+        fp32_cublas_solve(lat, plan, strikes, torch, qcu)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fp32_cublas_solve(lat, plan, strikes, torch, qcu)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        ms_cu = e0.elapsed_time(e1)
+        extra["fp32_cublas_quotes_per_s"] = round(NMAT * NK * world / (ms_cu * 1e-3), 1)
+        extra["fp32_cublas_ms_per_solve"] = round(ms_cu, 2)
+        extra["fp32_cublas_max_abs_err_vs_fp64"] = float((qcu - q_ref).abs().max().item())
+        extra["speedup_vs_fp32_simt"] = extra["speedup_vs_fp32"]
+        extra["speedup_vs_fp32_cublas"] = round(ms_cu / ms, 2)
+        extra["speedup_vs_fp32"] = round(min(ms32, ms_cu) / ms, 2)
+        extra["fp32_arm"] = "cublas" if ms_cu < ms32 else "simt"
+        del qcu
         m16 = MODES["fp16x3"]
         ws16 = lat.workspace(NK, m16)
         q16 = torch.empty_like(quotes)
@@ -820,6 +870,170 @@ def run_gemv(args):
             "column_major_N": res["opcuda_sgemv"]}
 
 
+# OPBench figures published by the reference for its first box (Tesla "1060" GPU0 and its
+# host), docs/benchmarks/nehalem-tesla1060.jpg; context only (2009-era hardware).
+OPBENCH_PUBLISHED = {
+    "sgemm_576x100": (340.0, "GF/s"), "sgemm4_40x576": (368.6, "GF/s"), "sgemv_576x100": (2.5, "GF/s"),
+    "mt_uniforms": (1470.5, "M/s"), "mt_uniforms_with_copy": (510.5, "M/s"), "lv_kernels": (108.5, "GF/s"),
+    "lv_mc": (142.9, "M eval/s"), "sv_kernels": (256.5, "GF/s"), "sv_mc": (41.2, "M eval/s"),
+    "cpu_sgemm": (35.2, "GF/s"), "cpu_dgemm": (31.0, "GF/s"), "cpu_mt": (724.1, "M/s"), "cpu_lv_mc": (560.2, "M eval/s"),
+    "cpu_sv_mc": (485.5, "M eval/s"),
+}
+
+
+def run_refbench(args):
+    """The reference's own benchmark workloads (benchmarks/opbench/CBenchmarks.cs and the
+    benchmarks/*/Program.cs drivers) on this GPU through the drop-in entry points, and their
+    CPU counterparts on this host's cores in the same run:
+      SGEMM 576^3 x 100 (opcuda_sgemm), grouped SGEMM4 40 x 576^3 (opcuda_sgemm4 task table),
+      SGEMV 576 x 100 (opcuda_sgemv), MT uniforms 20 batches of 102,400 with and without the
+      copy to the host (opcuda_mt_benchmark), LV (128 states, sigma 0.25, r 0.05) and SV (64 x 8
+      states) step kernels for 7-day steps by squaring (GF/s = 2 d^3 per product / time) and
+      their Monte Carlo (opcuda_mc1f, 40 weekly steps; LV 20 x 102,400 paths, SV 4,096 paths;
+      M eval/s = path-steps / wall time including the per-batch copy of the int16 states, as
+      the reference times them); CPU: csgemm / cdgemm (torch-CPU), cmt (C MT19937 restatement,
+      all threads), clv / csv Monte Carlo (C restatement, all threads; 102,400 x 120 and
+      102,400 x 100 paths x 40 steps) on the same step kernels."""
+    import platform
+    import torch
+    from oplib_b200 import _lib
+    from oplib_b200.model import Lattice, bind_stream, cumulative_rows
+    from oracle import oracle_c as OC
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    bind_stream(dev)
+    stream = torch.cuda.current_stream(dev)
+    lib = _lib.load()
+    res = {}
+    ncpu = os.cpu_count() or 1
+
+    def put(name, value, unit, **kw):
+        pub = OPBENCH_PUBLISHED.get(name)
+        res[name] = dict(value=round(value, 2), unit=unit, **kw)
+        if pub:
+            res[name]["published_reference"] = pub[0]
+
+    # ---- SGEMM 576^3 x 100 (column-major drop-in, FP32 SIMT)
+    d = 576
+    A = torch.empty(d * d, device=dev).uniform_()
+    B = torch.empty(d * d, device=dev).uniform_()
+    Cc = torch.empty(d * d, device=dev)
+    f = lambda: lib.opcuda_sgemm(d, d, d, 1.0, A.data_ptr(), d, B.data_ptr(), d, 0.0, Cc.data_ptr(), d)
+    f()
+    ms = _time(f, 100, stream, torch)
+    put("sgemm_576x100", 2.0 * d ** 3 / (ms * 1e-3) / 1e9, "GF/s")
+    # ---- grouped SGEMM4: 40 products of 576^3 through one task table (64 x 16 C tiles)
+    mats = [(torch.empty(d * d, device=dev).uniform_(), torch.empty(d * d, device=dev).uniform_(),
+             torch.empty(d * d, device=dev)) for _ in range(40)]
+    sz = lib.opb_sgemm4_task_size()
+    tasks = []
+    for i, (a_, b_, c_) in enumerate(mats):
+        for bx in range(d // 64):
+            for by in range(d // 16):
+                tasks.append((i, bx, by, d, d, d, a_.data_ptr(), b_.data_ptr(), c_.data_ptr()))
+    rec = np.zeros((len(tasks), sz // 8), dtype=np.int64)
+    for t, (i, bx, by, m, n, k, a_, b_, c_) in enumerate(tasks):
+        rec[t, :3] = np.array([i, bx, by, m, n, k], dtype=np.int32).view(np.int64)
+        rec[t, 3:6] = [a_, b_, c_]
+    drec = torch.from_numpy(rec.ravel()).to(dev)
+    ptrs = torch.tensor([drec.data_ptr() + t * sz for t in range(len(tasks))], dtype=torch.int64, device=dev)
+    f = lambda: lib.opcuda_sgemm4(len(tasks), ptrs.data_ptr())
+    f()
+    ms = _time(f, 5, stream, torch)
+    put("sgemm4_40x576", 40 * 2.0 * d ** 3 / (ms * 1e-3) / 1e9, "GF/s")
+    del mats, drec, ptrs
+    # ---- SGEMV 576 x 100
+    x = torch.empty(d, device=dev).uniform_()
+    y = torch.empty(d, device=dev)
+    f = lambda: lib.opcuda_sgemv(d, d, 1.0, A.data_ptr(), d, x.data_ptr(), 1, 0.0, y.data_ptr(), 1)
+    f()
+    ms = _time(f, 100, stream, torch)
+    put("sgemv_576x100", 2.0 * d * d / (ms * 1e-3) / 1e9, "GF/s")
+    # ---- MT uniforms: 20 batches of 102,400 (25 per stream, 4096 streams)
+    nb, ns = 20, 4096 * 25
+    mt = torch.zeros(4, dtype=torch.int32, device=dev)
+    seed = np.array([5489], dtype=np.uint32)
+    assert lib.opcuda_mc_setseed(seed.ctypes.data, mt.data_ptr()) == 0
+    unif = torch.empty(ns, device=dev)
+    host = torch.empty(ns, dtype=torch.float32).pin_memory()
+    lib.opcuda_mt_benchmark(mt.data_ptr(), unif.data_ptr(), ns)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(nb):
+        lib.opcuda_mt_benchmark(mt.data_ptr(), unif.data_ptr(), ns)
+    torch.cuda.synchronize()
+    put("mt_uniforms", nb * ns / (time.perf_counter() - t0) / 1e6, "M/s")
+    t0 = time.perf_counter()
+    for _ in range(nb):
+        lib.opcuda_mt_benchmark(mt.data_ptr(), unif.data_ptr(), ns)
+        host.copy_(unif)
+    torch.cuda.synchronize()
+    put("mt_uniforms_with_copy", nb * ns / (time.perf_counter() - t0) / 1e6, "M/s")
+
+    # ---- LV and SV: 7-day step kernels by squaring, then Monte Carlo over 40 weekly steps
+    step, day = 7.0 / 365.25, 1.0 / 365.25
+    cpu_rows = {}
+    for name, lat, nbatch, nscen in [("lv", Lattice.local_vol(n=128, level=0.25, skew=0.0, width=1.0, rate=0.05,
+                                                                device=dev), 20, 4096 * 25),
+                                     ("sv", Lattice.stoch_vol(nx=64, nv=8, rate=0.05, device=dev), 1, 4096)]:
+        plan = lat.plan(step, day)
+        dd = lat.d
+        P = lat.kernel(step, day, mode="fp32", plan=plan)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(10):
+            P = lat.kernel(step, day, mode="fp32", plan=plan)
+        torch.cuda.synchronize()
+        sec = (time.perf_counter() - t0) / 10
+        put(f"{name}_kernels", 2.0 * dd ** 3 * plan.niter / sec / 1e9, "GF/s", d=dd, niter=plan.niter)
+        Cm = cumulative_rows(P)
+        Ccm = Cm.t().contiguous()  # the reference's column-major layout
+        mk = torch.zeros(40, dtype=torch.int32, device=dev)
+        ysk = torch.empty(nscen * 40, dtype=torch.int16, device=dev)
+        yh = torch.empty(nscen * 40, dtype=torch.int16).pin_memory()
+        assert lib.opcuda_mc_setseed(seed.ctypes.data, mt.data_ptr()) == 0
+        lib.opcuda_mc1f(mt.data_ptr(), lat.y0, ysk.data_ptr(), nscen, 40, dd, Ccm.data_ptr(), mk.data_ptr(),
+                        yh.data_ptr())
+        t0 = time.perf_counter()
+        for _ in range(nbatch):
+            assert lib.opcuda_mc1f(mt.data_ptr(), lat.y0, ysk.data_ptr(), nscen, 40, dd, Ccm.data_ptr(),
+                                   mk.data_ptr(), yh.data_ptr()) == 0
+        sec = time.perf_counter() - t0
+        put(f"{name}_mc", 40.0 * nbatch * nscen / sec / 1e6, "M eval/s", paths=nbatch * nscen, steps=40,
+            includes="copy of the int16 states to the host per batch")
+        cpu_rows[name] = (Cm.cpu().numpy(), lat.y0, dd, P.double().cpu(), plan)
+
+    # ---- CPU counterparts on this host's cores
+    for dt, name in [(torch.float32, "cpu_sgemm"), (torch.float64, "cpu_dgemm")]:
+        a_ = torch.rand(d, d, dtype=dt)
+        torch.mm(a_, a_)
+        t0 = time.perf_counter()
+        for _ in range(100):
+            torch.mm(a_, a_)
+        put(name, 100 * 2.0 * d ** 3 / (time.perf_counter() - t0) / 1e9, "GF/s", threads=torch.get_num_threads())
+    lo = OC.load()
+    per = (4096 * 25) // ncpu
+    t0 = time.perf_counter()
+    lo.oracle_mt_benchmark(per, 2000, ncpu, 5489)
+    put("cpu_mt", ncpu * per * 2000 / (time.perf_counter() - t0) / 1e6, "M/s", threads=ncpu,
+        note="MT19937 (the reference's CPU path used MKL MT2203)")
+    for name, npaths in [("lv", 4096 * 25 * 120), ("sv", 4096 * 25 * 100)]:
+        Cm, y0, dd, _, _ = cpu_rows[name]
+        t0 = time.perf_counter()
+        OC.mc_paths(Cm, y0, 5489, 0, npaths, 40, want_paths=False, nthreads=ncpu)
+        put(f"cpu_{name}_mc", 40.0 * npaths / (time.perf_counter() - t0) / 1e6, "M eval/s", threads=ncpu,
+            paths=npaths, steps=40)
+    lvmc = res["lv_mc"]["value"]
+    return {"metric": "reference benchmark suite (OPBench workloads): LV Monte Carlo M eval/s headline",
+            "value": lvmc, "unit": "M eval/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": round(lvmc / OPBENCH_PUBLISHED["lv_mc"][0], 1),
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "OPBench workloads (CBenchmarks.cs), drop-in entry points"},
+            "host": {"cpu": platform.processor() or platform.machine(), "nproc": ncpu},
+            "results": res,
+            "note": "published_reference = the reference's own OPBench figure on a 2009 Tesla box (context)"}
+
+
 def run_gemm(args):
     """The squaring GEMM alone (split-BF16, E-form: C = E.E + 2E in place) at size d."""
     import torch
@@ -863,7 +1077,8 @@ def main():
     ap.add_argument("--members", type=int, default=4)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--workload", default="sv",
-                    choices=["sv", "lv", "mc", "gemm", "gemv", "renorm", "batch", "surrogate", "calibrate"],
+                    choices=["sv", "lv", "mc", "gemm", "gemv", "renorm", "batch", "surrogate", "calibrate",
+                             "refbench"],
                     help="sv = the headline SV lattice solve; the others are secondary measurements")
     ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
     args = ap.parse_args()
@@ -881,7 +1096,8 @@ def main():
             torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "gemv": run_gemv, "renorm": run_renorm,
-              "batch": run_batch, "surrogate": run_surrogate, "calibrate": run_calibrate}[
+              "batch": run_batch, "surrogate": run_surrogate, "calibrate": run_calibrate,
+              "refbench": run_refbench}[
             args.workload]
         line = fn(args)
         if int(os.environ.get("RANK", "0")) == 0:
