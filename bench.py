@@ -783,6 +783,18 @@ def run_surrogate(args):
     # effective: surrogate for accepted quotes, lattice re-solve of every lattice holding a fallback
     n_test = test.feat.shape[0]
     eff_s = ms_inf * 1e-3 * n_test / n + (fb_lat / 512) * ms_lat * 1e-3
+    # a 2-member operating point (the first two members): half the inference work, the
+    # spread of a pair as the fallback test
+    ms2 = _time(lambda: sur.predict(feat, base, ws, members=2), args.steps, stream, torch)
+    iv2, sp2 = sur.predict(test.feat, test.base, ws, members=2)
+    err2 = (iv2 - test.iv).abs() * 1e4
+    acc2 = sp2 * 1e4 <= 5.0
+    two = {"quotes_per_s": round(n / (ms2 * 1e-3), 1), "ms": round(ms2, 3),
+           "speedup_vs_lattice": round(n / (ms2 * 1e-3) / (512 * NMAT * 64 / (ms_lat * 1e-3)), 1),
+           "fallback_rate": round(float((~acc2).float().mean().item()), 4),
+           "accepted_err_bp": {"rms": round(float(err2[acc2].pow(2).mean().sqrt().item()), 2),
+                               "p99": round(float(torch.quantile(err2[acc2].float(), 0.99).item()), 2)},
+           "all_err_bp": {"rms": round(float(err2.pow(2).mean().sqrt().item()), 2)}}
     q = lambda x, p: float(torch.quantile(x.float(), p).item()) if x.numel() else float("nan")
     return {"metric": "surrogate quotes/sec (ensemble MLP on tensor cores) vs lattice quotes/sec",
             "value": round(sur_qps, 1), "unit": "quotes/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -800,7 +812,7 @@ def run_surrogate(args):
             "all_err_bp": {"rms": round(float(err.pow(2).mean().sqrt().item()), 2), "p99": round(q(err, 0.99), 2)},
             "baseline_err_bp": {"rms": round(float(errb.pow(2).mean().sqrt().item()), 2), "p99": round(q(errb, 0.99), 2)},
             "effective_quotes_per_s_with_fallback": round(n_test / eff_s, 1),
-            "spread_threshold_bp": 5.0,
+            "spread_threshold_bp": 5.0, "two_members": two,
             "train_seconds": round(sur.train_seconds, 1), "data_seconds": round(t_data, 1),
             "final_train_mse": sur.history[-1][2]}
 

@@ -190,17 +190,22 @@ class Surrogate:
         self.train_seconds = time.perf_counter() - t0
         return self.history
 
-    def predict(self, feat: torch.Tensor, base: torch.Tensor, ws: torch.Tensor | None = None):
-        """Ensemble mean implied vol and spread (max - min) on the tensor cores."""
+    def predict(self, feat: torch.Tensor, base: torch.Tensor, ws: torch.Tensor | None = None,
+                members: int | None = None):
+        """Ensemble mean implied vol and spread (max - min) on the tensor cores, over the
+        first ``members`` members (default: all; at least 2 for a spread)."""
+        nmem = self.members if members is None else int(members)
+        if not 1 <= nmem <= self.members:
+            raise ValueError("members out of range")
         X = normalise(feat)
         n = X.shape[0]
-        need = int(self.lib.opb_mlp_infer_workspace_bytes(n, self.members))
+        need = int(self.lib.opb_mlp_infer_workspace_bytes(n, nmem))
         if ws is None or ws.numel() < need:
             ws = torch.empty(need, dtype=torch.uint8, device=self.device)
         mean = torch.empty(n, dtype=torch.float32, device=self.device)
         spread = torch.empty(n, dtype=torch.float32, device=self.device)
         bind_stream(self.device)
-        call("opb_mlp_infer", self.packed.data_ptr(), self.members, self.stride, X.data_ptr(), n, ws.data_ptr(),
+        call("opb_mlp_infer", self.packed.data_ptr(), nmem, self.stride, X.data_ptr(), n, ws.data_ptr(),
              ws.numel(), mean.data_ptr(), spread.data_ptr())
         return base + TARGET_SCALE * mean.double(), TARGET_SCALE * spread.double()
 
