@@ -187,6 +187,9 @@ int opb_set_stage_k(int bk);
  * CTAs' shared memory) for products with M % 256 == 0: 1 = on (default), 0 = off;
  * results are identical */
 int opb_set_cta_pair(int on);
+/* new: tuning knob, M-tiles per raster group of single products (L2 reuse of operand strips);
+ * 0 = 8; results are identical */
+int opb_set_group_m(int gm);
 /* new: the same product with FP16 parts (power-of-two-scaled splits; undo the scales in alpha) */
 int opb_gemm_f16x3(int M, int N, int K, const uint16_t *Ahi, const uint16_t *Alo, long long lda, const uint16_t *Bhi,
                    const uint16_t *Blo, long long ldb, float alpha, const float *Cin, float beta, float *C,

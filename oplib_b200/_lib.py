@@ -98,6 +98,7 @@ PROTOTYPES: dict[str, tuple] = {
     "opcuda_sgsvg": (i32, [u64, i32, i32, i32, u64, u64]),
     "opb_set_stage_k": (i32, [i32]),
     "opb_set_cta_pair": (i32, [i32]),
+    "opb_set_group_m": (i32, [i32]),
     "opb_renorm_rows": (i32, [i32, vp, vp, i32, i32, vp, vp, vp, vp, i32]),
     # lattice
     "opb_lattice_workspace_size": (ull, [i32, i32, i32]),

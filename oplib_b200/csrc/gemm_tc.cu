@@ -242,6 +242,7 @@ struct TcParams {
     // sum over the columns of group g of bf16(GELU(alpha * acc + bias)) * w5[col]
     const float *w5;
     float *ypart;
+    int group_m;  // M-tiles per raster group of a single product (0: 8)
 };
 
 // Batched launches read per-problem tensor maps (4 per problem: Ahi, Alo, Bhi, Blo) and
@@ -302,7 +303,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? 
             n0 = (int)(w & 255u) * BN;
             nkb = bt.probs[prob].K / BK;
         } else {
-            const int GM = 8;
+            const int GM = p.group_m > 0 ? p.group_m : 8;
             const int per_group = GM * ntiles_n;
             const int group = t / per_group;
             const int first_m = group * GM;
@@ -646,6 +647,7 @@ static int make_map(CUtensorMap *m, const void *ptr, long long rows, long long K
 static int g_tile_override = 0;  // 0 = automatic
 static int g_bk256 = 64;          // K depth of a pipeline stage for 256-wide tiles (32 or 64)
 static int g_pair = 1;            // 256 x 256 tiles on CTA pairs (cta_group::2) when M % 256 == 0
+static int g_group_m = 0;         // M-tiles per raster group of single products (0: 8)
 
 int tc_gemm_tile_n(int N) {
     if (g_tile_override && N % g_tile_override == 0) return g_tile_override;
@@ -713,6 +715,7 @@ static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
     if ((r = make_map(&mBh, a.Bhi, a.N, a.K, a.ldb, BN, F16, BK)) != OPB_OK) return r;
     if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN, F16, BK)) != OPB_OK) return r;
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
+    p.group_m = g_group_m;
     const int ntiles = (a.M / TC_BM) * (a.N / BN);
     const int grid = ntiles < num_sms() ? ntiles : num_sms();
     TcBatch none{nullptr, nullptr, nullptr, 0};
@@ -737,6 +740,7 @@ static int launch_tc_pair(const TcGemmArgs &a, cudaStream_t s) {
     if ((r = make_map(&mBh, a.Bhi, a.N, a.K, a.ldb, BN / 2, F16)) != OPB_OK) return r;
     if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN / 2, F16)) != OPB_OK) return r;
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
+    p.group_m = g_group_m;
     TcBatch none{nullptr, nullptr, nullptr, 0};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -957,6 +961,14 @@ OPB_API int opb_set_stage_k(int bk) {
 OPB_API int opb_set_cta_pair(int on) {
     OPB_REQUIRE(on == 0 || on == 1, OPB_E_ARG);
     g_pair = on;
+    return set_status(OPB_OK);
+}
+
+// Tuning knob: M-tiles per raster group of single products (operand-strip reuse in L2);
+// 0 = 8.  Results are identical.
+OPB_API int opb_set_group_m(int gm) {
+    OPB_REQUIRE(gm >= 0 && gm <= 64, OPB_E_ARG);
+    g_group_m = gm;
     return set_status(OPB_OK);
 }
 
