@@ -523,6 +523,19 @@ def run_mc(args):
         t = torch.tensor([ms, ms_mc], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_mc = float(t[0]), float(t[1])
+    # the same kernel writing every int16 state (the reference's y_sk output): 2 bytes per
+    # path-step to HBM, 1.06 GB for 2^20 x 504 -- its achieved write bandwidth
+    ypaths = torch.empty(nsteps, npaths, dtype=torch.int16, device=dev)
+
+    def step_paths():
+        _lib.call("opb_mc_mt19937", state["C"].data_ptr(), lat.d, 1, state["g"].data_ptr(), 64, lat.d, lat.y0,
+                  nsteps, 5489, path0, npaths, ypaths.data_ptr(), None, 1.0, 0.7, 1.0, None, None)
+
+    step_paths()
+    ms_paths = _time(step_paths, args.steps, stream, torch)
+    del ypaths
+    hbm, _, _, src = _peaks()
+    gbs = 2.0 * npaths * nsteps / (ms_paths * 1e-3) / 1e9
     sums = state["sums"].cpu().numpy() / total_paths
     samples = total_paths * nsteps
     line = {"metric": "Monte Carlo path-steps/sec (MT19937 per path, inverse-CDF on FP32 cumulative rows)",
@@ -533,6 +546,9 @@ def run_mc(args):
                                    "0.7 + Asian, K=1", "paths": total_paths, "steps_per_path": nsteps,
                        "parallelism": f"path ranges x{world}, one all-reduce of 2 sums"},
             "mc_kernel_only": {"ms": round(ms_mc, 3), "path_steps_per_s": round(samples / (ms_mc * 1e-3), 1)},
+            "with_state_output": {"ms": round(ms_paths, 3), "path_steps_per_s":
+                                  round(npaths * nsteps / (ms_paths * 1e-3), 1), "hbm_write_GB_s": round(gbs, 1),
+                                  "frac_of_hbm": round(gbs / hbm, 4), "peak_source": src},
             "prices": {"barrier_do_call": float(sums[0]), "asian_call": float(sums[1])}}
     if args.cpu and rank == 0:
         from oracle import oracle_c as OC
