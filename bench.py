@@ -507,7 +507,7 @@ def run_mc(args):
         if with_kernel:
             P = lat.kernel(1 / 252, 2.0 ** -14, mode="fp32", plan=plan)
             Cm = cumulative_rows(P)
-            state["C"], state["g"] = Cm, guide_table(Cm, 64)
+            state["C"], state["g"] = Cm, guide_table(Cm)
         sums, _ = mc_run(state["C"], lat.y0, nsteps, 5489, npaths, path0=path0, guide=state["g"], x=lat.x,
                          disc=disc, scratch=scratch)
         state["sums"] = allreduce_sums(sums)
@@ -528,7 +528,8 @@ def run_mc(args):
     ypaths = torch.empty(nsteps, npaths, dtype=torch.int16, device=dev)
 
     def step_paths():
-        _lib.call("opb_mc_mt19937", state["C"].data_ptr(), lat.d, 1, state["g"].data_ptr(), 64, lat.d, lat.y0,
+        _lib.call("opb_mc_mt19937", state["C"].data_ptr(), lat.d, 1, state["g"].data_ptr(), state["g"].shape[1],
+                  lat.d, lat.y0,
                   nsteps, 5489, path0, npaths, ypaths.data_ptr(), None, 1.0, 0.7, 1.0, None, None)
 
     step_paths()

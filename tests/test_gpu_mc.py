@@ -152,3 +152,19 @@ def test_mt_benchmark_uniforms(cuda):
     for s in [0, 5, 4095]:
         ref = (OC.mt_outputs(7 + s, 20).astype(np.float32) * np.float32(2.0 ** -32)).astype(np.float32)
         assert np.array_equal(got[:, s], ref)
+
+
+def test_mc_paths_bit_exact_with_default_guide_width(step_rows):
+    """The default guide table (two buckets per state: 1024 for 512 states) changes only
+    the search bracket: the paths stay those of the oracle."""
+    from oplib_b200.model import guide_buckets, guide_table, mc_run
+    lat, P, Cm, _ = step_rows
+    assert guide_buckets(512) == 1024 and guide_buckets(3000) == 4096 and guide_buckets(1) == 2
+    g = guide_table(Cm)
+    assert tuple(g.shape) == (512, 1024)
+    disc = math.exp(-0.03 * 2.0)
+    sums, paths = mc_run(Cm, lat.y0, 504, 5489, 2048, guide=g, x=lat.x, disc=disc, want_paths=True)
+    torch.cuda.synchronize()
+    ref_paths, ref_sums = OC.mc_paths(Cm.cpu().numpy(), lat.y0, 5489, 0, 2048, 504, x=lat.x.cpu().numpy(), disc=disc)
+    assert np.array_equal(paths.cpu().numpy().T, ref_paths)
+    assert np.allclose(sums.cpu().numpy(), ref_sums, rtol=1e-12)
