@@ -295,10 +295,11 @@ class Batch:
             pass
 
 
-def calibration_sweep(nlat=512, seed=20260, sizes=tuple(range(256, 2049, 128)), device="cuda"):
+def calibration_sweep(nlat=512, seed=20260, sizes=tuple(range(256, 2049, 128)), device="cuda", build=True):
     """Seeded local-vol lattices of the calibration sweep: n uniform over ``sizes``,
     level ~ U[0.1, 0.4], skew ~ U[-0.3, 0.3], width ~ U[0.2, 1.0], r ~ U[0, 0.05],
-    sigma(x) = max(0.01, level + skew * exp(-((x - 1)/width)^2))."""
+    sigma(x) = max(0.01, level + skew * exp(-((x - 1)/width)^2)).  build=False returns the
+    parameters only (None for the lattices)."""
     import numpy as np
     rng = np.random.default_rng(seed)
     n = rng.choice(np.array(sizes), size=nlat)
@@ -308,5 +309,5 @@ def calibration_sweep(nlat=512, seed=20260, sizes=tuple(range(256, 2049, 128)), 
     r = rng.uniform(0.0, 0.05, nlat)
     params = [dict(n=int(n[i]), level=float(level[i]), skew=float(skew[i]), width=float(width[i]), rate=float(r[i]),
                    floor=0.01) for i in range(nlat)]
-    lats = [Lattice.local_vol(device=device, **p) for p in params]
+    lats = [Lattice.local_vol(device=device, **p) for p in params] if build else None
     return lats, params
