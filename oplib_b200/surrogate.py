@@ -6,7 +6,7 @@ lattice solver (``model.Batch``) produces, converted to implied volatilities on 
 device; the networks are trained by the library's own forward/backward/Adam kernels
 (``opb_mlp_*``) and evaluated on the tensor cores (``opb_mlp_infer``).  A quote whose
 ensemble spread exceeds the tolerance (5 bp of volatility by default) falls back to the
-lattice, which is also the judge of the surrogate's error.
+lattice, which is also the reference for the surrogate's error.
 
 Local-volatility rows fix kappa = rho = 0 (the stochastic-volatility columns are inputs
 of the network but constant in the local-volatility training family).
