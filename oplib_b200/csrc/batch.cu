@@ -377,8 +377,11 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
         delete P;
         return set_status(rc_status);
     }
+    // uploads on the library stream (ordered after any earlier work on the workspace), then
+    // one synchronisation before the host staging vectors go out of scope
+    cudaStream_t ls = opb::stream();
     auto up = [&](void *dst, const void *src, size_t bytes) -> cudaError_t {
-        return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ls);
     };
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = up(P->lats, lats.data(), sizeof(opb::BatchLattice) * n);
@@ -392,6 +395,8 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     if (e == cudaSuccess) e = up(P->maps_price, mp.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
     if (e == cudaSuccess) e = up(P->maps_sq[2], m256.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
     if (e == cudaSuccess) e = up(P->work, W.data(), sizeof(uint32_t) * W.size());
+    const cudaError_t es = cudaStreamSynchronize(ls);
+    if (e == cudaSuccess) e = es;
     if (e != cudaSuccess) {
         delete P;
         return opb::set_cuda(e);

@@ -972,9 +972,12 @@ OPB_API int opb_set_group_m(int gm) {
     return set_status(OPB_OK);
 }
 
-// Reads and clears the tensor-core kernels' device error word (0 = no bounded wait expired).
+// Reads and clears the tensor-core kernels' device error word (0 = no bounded wait expired)
+// after the calling thread's library stream has drained (it may be a non-blocking stream,
+// which the symbol copies below would not wait for).
 OPB_API int opb_tc_error(void) {
     int v = 0, z = 0;
+    OPB_TRY(cudaStreamSynchronize(stream()));
     OPB_TRY(cudaMemcpyFromSymbol(&v, g_tc_error, sizeof(int)));
     OPB_TRY(cudaMemcpyToSymbol(g_tc_error, &z, sizeof(int)));
     set_status(OPB_OK);
