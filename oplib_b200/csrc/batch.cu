@@ -184,7 +184,8 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     size_t parts = 0;
     for (int i = 0; i < n; i++) parts += (size_t)(b->d[i] / 64) * b->d[i];
     double *part = c.take<double>(parts);
-    (void)c.take<float>(n);  // per-lattice FP16 payoff scales
+    (void)c.take<float>(n);          // per-lattice FP16 payoff scales
+    (void)c.take<double2>(off[n]);   // per-row fixes of the deferred E-form renormalisation
 
     // ---- work lists (host), appended into one blob
     std::vector<uint32_t> W;
@@ -243,10 +244,10 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
                 if (b->niter[i] <= level) continue;
                 mode_i = (level == b->niter[i] - 1) ? 1 : 0;
             }
-            const int t = b->d[i] / 64;
+            const int t = b->d[i] / 64, nch = opb::renorm_chunks(b->d[i]);
             for (int a = 0; a < t; a++)
-                for (int bb = 0; bb < t; bb++)
-                    W.push_back(((uint32_t)i << 16) | ((uint32_t)mode_i << 14) | ((uint32_t)a << 7) | (uint32_t)bb);
+                for (int c = 0; c < nch; c++)
+                    W.push_back(((uint32_t)i << 16) | ((uint32_t)mode_i << 14) | ((uint32_t)a << 7) | (uint32_t)c);
         }
         r.n = (int)(W.size() - r.off);
         return r;
@@ -340,6 +341,7 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     for (int i = 0; i < n; i++) parts += (size_t)(b->d[i] / 64) * b->d[i];
     double *part = cv.take<double>(parts);
     float *gsc = cv.take<float>(n);
+    double2 *fix = cv.take<double2>((size_t)P->total_rows);
     const int f16 = mode == OPB_FP16X3_B ? 1 : 0;
     P->f16 = f16;
     const float un2 = f16 ? 1.f / (F16S * F16S) : 1.f, un1 = f16 ? 1.f / F16S : 1.f;
@@ -354,11 +356,13 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
         L.GThi = Gh + (size_t)ro * P->ldk; L.GTlo = Gl + (size_t)ro * P->ldk;
         L.gscale = gsc + i;
         double *pi = part + po;
-        sq[i] = opb::TcProblem{d, d, d, 0, L.E, L.E, pi, d, un2, 2.f, 0};
-        ch[i] = opb::TcProblem{d, d, d, 0, L.Pa, nullptr, pi, d, un2, 0.f, 0};
-        pr[i] = opb::TcProblem{d, P->ldk, d, 0, L.V, nullptr, nullptr, P->ldk, un1, 0.f, 0};
-        rs[i] = opb::RenormProblem{d, 0, L.E, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo};
-        rc[i] = opb::RenormProblem{d, 0, L.Pa, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo};
+        // squaring reads E as the previous level's GEMM left it, renormalised on the fly by
+        // the row fixes of the previous level's (or the initial split's) renormalisation
+        sq[i] = opb::TcProblem{d, d, d, 0, L.E, L.E, pi, d, un2, 2.f, fix + ro};
+        ch[i] = opb::TcProblem{d, d, d, 0, L.Pa, nullptr, pi, d, un2, 0.f, nullptr};
+        pr[i] = opb::TcProblem{d, P->ldk, d, 0, L.V, nullptr, nullptr, P->ldk, un1, 0.f, nullptr};
+        rs[i] = opb::RenormProblem{d, 0, L.E, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo, fix + ro};
+        rc[i] = opb::RenormProblem{d, 0, L.Pa, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo, nullptr};
         rc_status = opb::tc_make_maps(&m128[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 128, f16);
         if (rc_status == OPB_OK)
             rc_status =

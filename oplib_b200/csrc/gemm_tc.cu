@@ -243,6 +243,7 @@ struct TcParams {
     const float *w5;
     float *ypart;
     int group_m;  // M-tiles per raster group of a single product (0: 8)
+    const double2 *cin_fix;  // as TcGemmArgs::cin_fix
 };
 
 // Batched launches read per-problem tensor maps (4 per problem: Ahi, Alo, Bhi, Blo) and
@@ -523,12 +524,15 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? 
             long long ldc;
             float alpha, beta;
             double *rowsum;
+            const double2 *fix;
             int M;
             if constexpr (BATCHED) {
                 const TcProblem &pr = bt.probs[prob];
                 C = pr.C; Cin = pr.Cin; ldc = pr.ldc; alpha = pr.alpha; beta = pr.beta; rowsum = pr.rowsum; M = pr.M;
+                fix = pr.cin_fix;
             } else {
                 C = p.C; Cin = p.Cin; ldc = p.ldc; alpha = p.alpha; beta = p.beta; rowsum = p.rowsum; M = p.M;
+                fix = p.cin_fix;
             }
             const int row = m0 + (int)rank * TC_BM + q * 32 + lane;
             const int col0 = n0 + h * CPT;
@@ -576,6 +580,10 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? 
             }
             float *crow = C + (long long)row * ldc + col0;
             const float *cin = Cin ? Cin + (long long)row * ldc + col0 : nullptr;
+            // deferred renormalisation of Cin (the arithmetic of the E-form renormalisation
+            // kernel, so Cin reads exactly as if that kernel had stored it)
+            const double2 fx = (cin && fix) ? fix[row] : make_double2(0.0, 1.0);
+            const int dcol = row - col0;  // this row's diagonal column within the group, if any
             double rs = 0.0;
 #pragma unroll
             for (int j = 0; j < CPT; j += 4) {
@@ -586,10 +594,19 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? 
                 o.w = alpha * sum[j + 3];
                 if (cin) {
                     const float4 ci = *reinterpret_cast<const float4 *>(cin + j);
-                    o.x = fmaf(beta, ci.x, o.x);
-                    o.y = fmaf(beta, ci.y, o.y);
-                    o.z = fmaf(beta, ci.z, o.z);
-                    o.w = fmaf(beta, ci.w, o.w);
+                    float c4[4] = {ci.x, ci.y, ci.z, ci.w};
+                    if (fix) {
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            double x = (double)c4[u];
+                            if (dcol == j + u) x -= fx.x;
+                            c4[u] = (float)(x * fx.y);
+                        }
+                    }
+                    o.x = fmaf(beta, c4[0], o.x);
+                    o.y = fmaf(beta, c4[1], o.y);
+                    o.z = fmaf(beta, c4[2], o.z);
+                    o.w = fmaf(beta, c4[3], o.w);
                 }
                 *reinterpret_cast<float4 *>(crow + j) = o;
                 rs += (double)o.x + (double)o.y + (double)o.z + (double)o.w;
@@ -683,6 +700,7 @@ int tc_gemm_check(const TcGemmArgs &a) {
     if (!aligned(a.Ahi, 16) || !aligned(a.Alo, 16) || !aligned(a.Bhi, 16) || !aligned(a.Blo, 16)) return OPB_E_ALIGN;
     if ((a.lda * 2) % 16 || (a.ldb * 2) % 16 || a.ldc % 4 || !aligned(a.C, 16)) return OPB_E_ALIGN;
     if (a.Cin && !aligned(a.Cin, 16)) return OPB_E_ALIGN;
+    if (a.cin_fix && !aligned(a.cin_fix, 16)) return OPB_E_ALIGN;
     return OPB_OK;
 }
 
@@ -716,6 +734,7 @@ static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
     if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN, F16, BK)) != OPB_OK) return r;
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
     p.group_m = g_group_m;
+    p.cin_fix = a.cin_fix;
     const int ntiles = (a.M / TC_BM) * (a.N / BN);
     const int grid = ntiles < num_sms() ? ntiles : num_sms();
     TcBatch none{nullptr, nullptr, nullptr, 0};
@@ -741,6 +760,7 @@ static int launch_tc_pair(const TcGemmArgs &a, cudaStream_t s) {
     if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN / 2, F16)) != OPB_OK) return r;
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
     p.group_m = g_group_m;
+    p.cin_fix = a.cin_fix;
     TcBatch none{nullptr, nullptr, nullptr, 0};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;

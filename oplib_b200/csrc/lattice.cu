@@ -69,6 +69,7 @@ struct Bufs {
     float *X, *Pa, *Pb, *G, *V, *gscale;
     __nv_bfloat16 *Ahi, *Alo, *Bhi, *Blo, *GThi, *GTlo;
     double *part;
+    double2 *fix;  // per-row (s, inv) of the last E-form renormalisation (deferred into the next Cin)
 };
 
 inline int padded_nk(int nK, int mode) { return tc_mode(mode) ? (nK + 63) / 64 * 64 : nK; }
@@ -91,6 +92,7 @@ Bufs carve(Ws &w, int d, int nK, int mode) {
         b.GTlo = w.take<__nv_bfloat16>((size_t)d * nK);
         int np = opb::tc_gemm_nparts(d, d);
         b.part = w.take<double>((size_t)(np > 0 ? np : 1) * d);
+        b.fix = w.take<double2>((size_t)d);
     } else {
         b.G = w.take<float>((size_t)d * nK);
         b.part = w.take<double>((size_t)d);
@@ -164,7 +166,7 @@ int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s) {
         t.Alo = a.Alo + (size_t)i * kslice;
         t.Bhi = a.Bhi + (size_t)i * kslice;
         t.Blo = a.Blo + (size_t)i * kslice;
-        if (i > 0) { t.Cin = a.C; t.beta = 1.f; }
+        if (i > 0) { t.Cin = a.C; t.beta = 1.f; t.cin_fix = nullptr; }
         if (i + 1 < S) t.rowsum = nullptr;
         int r = opb::launch_tc_gemm(t, s);
         if (r) return r;
@@ -186,14 +188,19 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
     g.M = d; g.N = d; g.K = d; g.lda = d; g.ldb = d; g.ldc = d; g.f16 = f16 ? 1 : 0;
     g.Ahi = b.Ahi; g.Alo = b.Alo; g.Bhi = b.Bhi; g.Blo = b.Blo;
     for (int r = 0; r < L.niter; r++) {
-        // D = 2E + E.E in place of E, with FP64 row-sum partials
+        // D = 2E + E.E in place of E, with FP64 row-sum partials.  From the second level on,
+        // X holds the previous product as it left the GEMM, and its renormalisation (b.fix)
+        // is applied as the epilogue reads it.
         g.C = b.X; g.Cin = b.X; g.alpha = unscale; g.beta = 2.f; g.rowsum = b.part;
+        g.cin_fix = r > 0 ? b.fix : nullptr;
         LT(tc_gemm_ksplit(g, s));
         // the last level emits P1 = I + E and its splits (row-major: A of the first chain and
-        // of pricing; transposed: B of every chain)
+        // of pricing; transposed: B of every chain); the others write only the splits and
+        // the row fixes
         if (r + 1 == L.niter) LT(opb::launch_renorm_to_p(d, b.X, b.part, np, b.Ahi, b.Alo, b.Bhi, b.Blo, s, ss));
-        else LT(opb::launch_renorm(d, b.X, b.part, np, 1, b.Ahi, b.Alo, b.Bhi, b.Blo, s, ss));
+        else LT(opb::launch_renorm(d, b.X, b.part, np, 1, b.Ahi, b.Alo, b.Bhi, b.Blo, s, ss, 0, b.fix));
     }
+    g.cin_fix = nullptr;
     if (L.niter == 0) {
         LT(opb::launch_add_identity(d, b.X, s));
         LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s, ss));
@@ -215,7 +222,7 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
             // P_m = P_{m-1} . P1 (A splits hold P_{m-1}), renormalise, split row-major into A
             g.C = b.Pa; g.Cin = nullptr; g.alpha = unscale; g.beta = 0.f; g.rowsum = b.part;
             LT(tc_gemm_ksplit(g, s));
-            LT(opb::launch_renorm(d, b.Pa, b.part, np, 0, b.Ahi, b.Alo, nullptr, nullptr, s, ss));
+            LT(opb::launch_renorm(d, b.Pa, b.part, np, 0, b.Ahi, b.Alo, nullptr, nullptr, s, ss, 0));
         }
         LT(tc_gemm_ksplit(pg, s));
         const double disc = std::exp(-L.rate * L.period * m);

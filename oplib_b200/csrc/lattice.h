@@ -26,8 +26,11 @@ int launch_ek_dense(int d, const double *L, double dt, int eform, float *out, cu
 int launch_split(int rows, int cols, const float *X, long long ld, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
                  __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, long long ldt, cudaStream_t s, float sscale = 0.f);
 int launch_rowsum(int d, const float *X, double *partial, cudaStream_t s);
+// write_x = 0 leaves X as it is (only the splits are written; d % 64 == 0); fix (optional,
+// E-form) receives the per-row (s, inv) that a following product applies to X as its Cin.
 int launch_renorm(int d, float *X, const double *partial, int nparts, int eform, __nv_bfloat16 *Ahi,
-                  __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale = 0.f);
+                  __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale = 0.f,
+                  int write_x = 1, double2 *fix = nullptr);
 int launch_add_identity(int d, float *X, cudaStream_t s);
 // dscale (device, optional): FP16 payoff split scale from launch_payoff_scale
 int launch_payoff_scale(int d, const double *x, int nK, const double *K, float *out, cudaStream_t s);
@@ -47,15 +50,22 @@ struct BatchLattice {
     __nv_bfloat16 *GThi, *GTlo;  // ldk x d payoff splits
     float *gscale;        // device scalar: FP16 payoff split scale
 };
+// Renormalisation staging: tiles in flight per block, and column tiles per batched work
+// item (a batched item renormalises the tiles chunk, chunk + renorm_chunks(d), ... of one
+// 64-row strip).
+constexpr int RN_RING = 3;
+constexpr int RN_TILES = 8;
+__host__ __device__ inline int renorm_chunks(int d) { return (d / 64 + RN_TILES - 1) / RN_TILES; }
 struct RenormProblem {
     int d, pad;
-    float *X;
+    float *X;  // read only
     const double *partial;
     __nv_bfloat16 *Ahi, *Alo, *Bhi, *Blo;
+    double2 *fix;  // mode-0 items: per-row (s, inv) for the next product's Cin (cin_fix)
 };
 int launch_renorm_to_p(int d, float *X, const double *partial, int nparts, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
                        __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale = 0.f);
-// work items: problem << 16 | mode << 14 | tile_r << 7 | tile_c (64 x 64 tiles)
+// work items: problem << 16 | mode << 14 | strip << 7 | chunk (see renorm_chunks)
 int launch_renorm_batched(const RenormProblem *probs, const uint32_t *work, int nwork, int parts_div, cudaStream_t s,
                           float sscale = 0.f);
 int launch_ek_batched(const BatchLattice *lats, int nlat, long long total_rows, int w, const int *cols,
@@ -80,6 +90,9 @@ struct TcGemmArgs {
     float alpha, beta;
     double *rowsum;       // optional
     int f16;              // 1: FP16 parts (kind::f16 with F16 inputs), 0: BF16 parts
+    // optional, with Cin: per-row (s, inv) of a deferred E-form renormalisation; the
+    // epilogue reads Cin[r][c] as (float)((Cin[r][c] - (r == c ? s : 0)) * inv)
+    const double2 *cin_fix;
 };
 int tc_gemm_tile_n(int N);                    // tile width chosen for N (0 if unsupported)
 int tc_gemm_check(const TcGemmArgs &a);       // argument/alignment check, OPB_* code
@@ -100,7 +113,7 @@ struct TcProblem {
     double *rowsum;       // partials rowsum[(col/min(bn,128)) * M + row]
     long long ldc;
     float alpha, beta;
-    long long pad2;
+    const double2 *cin_fix;  // as TcGemmArgs::cin_fix
 };
 int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo, long long M, long long lda,
                  const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long N, long long ldb, long long K, int bn,

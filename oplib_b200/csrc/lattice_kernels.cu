@@ -192,10 +192,39 @@ __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) 
     return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
 }
 
+// Input staging: a ring of RN_RING tiles in shared memory filled by cp.async (16 bytes per
+// thread and copy), so that RN_RING - 1 tiles are in flight per block while one is
+// processed.  Each thread copies and later reads back only its own four float4 of a tile,
+// so the ring needs no block barrier: cp.async.wait_group orders a thread's own copies.
+struct RenormRing {
+    float4 v[RN_RING][4][256];
+};
+constexpr int RN_SMEM = (int)(sizeof(RenormSmem) + sizeof(RenormRing));
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// This thread's four 16-byte copies of the tile at (r0, c0) into ring slot s.
+__device__ __forceinline__ void renorm64_issue(RenormRing &rg, int s, int d, const float *__restrict__ X, int r0,
+                                               int c0) {
+    const int tid = threadIdx.x, lc = (tid & 15) * 4;
+#pragma unroll
+    for (int pass = 0; pass < 4; pass++)
+        cp_async16(&rg.v[s][pass][tid], X + (long long)(r0 + pass * 16 + (tid >> 4)) * d + c0 + lc);
+}
+
 // FP64 row sums of rows r0..r0+63 over the nparts partials, summed in part order (the
 // loads are issued 8 at a time; the additions stay sequential), and their reciprocals.
 __device__ __forceinline__ void renorm64_sums(RenormSmem &sm, int d, const double *__restrict__ partial, int nparts,
-                                              int mode, int r0) {
+                                              int mode, int r0, double2 *__restrict__ fix = nullptr) {
     const int tid = threadIdx.x;
     if (tid < 64) {
         double s = 0.0;
@@ -211,27 +240,20 @@ __device__ __forceinline__ void renorm64_sums(RenormSmem &sm, int d, const doubl
         for (; p < nparts; p++) s += q[(long long)p * d];
         sm.s_sum[tid] = s;
         const double den = nparts == 0 ? 1.0 : (mode != 2 ? 1.0 + s : s);
-        sm.s_inv[tid] = den != 0.0 ? 1.0 / den : 0.0;
+        const double inv = den != 0.0 ? 1.0 / den : 0.0;
+        sm.s_inv[tid] = inv;
+        if (fix) fix[r0 + tid] = make_double2(s, inv);
     }
 }
 
-// This thread's four float4 of the tile at (r0, c0).
-__device__ __forceinline__ void renorm64_load(int d, const float *__restrict__ X, int r0, int c0, float4 (&v)[4]) {
-    const int tid = threadIdx.x, lc = (tid & 15) * 4;
-#pragma unroll
-    for (int pass = 0; pass < 4; pass++)
-        v[pass] = *reinterpret_cast<const float4 *>(X + (long long)(r0 + pass * 16 + (tid >> 4)) * d + c0 + lc);
-}
-
 // One tile at (r0, c0), using the sums of renorm64_sums; vin holds the tile's values
-// (renorm64_load), and next (optional) is called after the row-major stores and before the
-// transposed ones, so that the next tile's loads overlap them.  Starts with a barrier, so
-// it can follow renorm64_sums or a previous tile of the same rows directly.
-template <class Next>
+// (read back from the staging ring) and the renormalised values are stored back into X
+// unless it is null.  Starts with a barrier, so it can follow renorm64_sums or a previous
+// tile of the same rows directly.
 __device__ __forceinline__ void renorm64_apply(RenormSmem &sm, int d, float *__restrict__ X, int mode,
                                                __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
                                                __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo,
-                                               int r0, int c0, float sscale, const float4 (&vin)[4], Next &&next) {
+                                               int r0, int c0, float sscale, const float4 (&vin)[4]) {
     const int tid = threadIdx.x;
     const bool eform = mode != 2;
     __syncthreads();
@@ -256,13 +278,12 @@ __device__ __forceinline__ void renorm64_apply(RenormSmem &sm, int d, float *__r
             split2(f[j], h[j], l[j], sscale);
             sm.t[lr][lc + j] = pack_bf16(h[j], l[j]);
         }
-        *reinterpret_cast<float4 *>(X + o) = make_float4(f[0], f[1], f[2], f[3]);
+        if (X) *reinterpret_cast<float4 *>(X + o) = make_float4(f[0], f[1], f[2], f[3]);
         if (Ahi) {
             *reinterpret_cast<uint2 *>(Ahi + o) = make_uint2(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]));
             *reinterpret_cast<uint2 *>(Alo + o) = make_uint2(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]));
         }
     }
-    next();
     if (!Bhi) return;
     __syncthreads();
 #pragma unroll
@@ -278,26 +299,52 @@ __device__ __forceinline__ void renorm64_apply(RenormSmem &sm, int d, float *__r
 
 // Grid (column chunks, d / 64): block (bx, by) renormalises rows 64*by.. over the column
 // tiles bx, bx + gridDim.x, ...; the row sums are formed once per block.
-__global__ void __launch_bounds__(256) k_renorm64(int d, float *__restrict__ X, const double *__restrict__ partial,
-                                                  int nparts, int mode, __nv_bfloat16 *__restrict__ Ahi,
-                                                  __nv_bfloat16 *__restrict__ Alo, __nv_bfloat16 *__restrict__ Bhi,
-                                                  __nv_bfloat16 *__restrict__ Blo, float sscale) {
-    __shared__ RenormSmem sm;
-    const int r0 = blockIdx.y * 64, nt = d / 64;
-    float4 cur[4], nxt[4];
-    if ((int)blockIdx.x < nt) renorm64_load(d, X, r0, blockIdx.x * 64, cur);
-    renorm64_sums(sm, d, partial, nparts, mode, r0);
-    for (int tc = blockIdx.x; tc < nt; tc += gridDim.x) {
-        const int tn = tc + gridDim.x;
-        renorm64_apply(sm, d, X, mode, Ahi, Alo, Bhi, Blo, r0, tc * 64, sscale, cur, [&] {
-            if (tn < nt) renorm64_load(d, X, r0, tn * 64, nxt);
-        });
+// Column tiles first, first + step, ... of the 64-row strip at r0, through the cp.async
+// ring; the row sums are formed once, while the first tiles are in flight.  Xout (may be
+// null) receives the renormalised values; fix (optional) the per-row (s, inv).
+__device__ __forceinline__ void renorm64_strip(RenormSmem &sm, RenormRing &rg, int d, const float *__restrict__ X,
+                                               float *__restrict__ Xout, const double *__restrict__ partial,
+                                               int nparts, int mode, __nv_bfloat16 *__restrict__ Ahi,
+                                               __nv_bfloat16 *__restrict__ Alo, __nv_bfloat16 *__restrict__ Bhi,
+                                               __nv_bfloat16 *__restrict__ Blo, int r0, int first, int step,
+                                               float sscale, double2 *__restrict__ fix) {
+    const int nt = d / 64, tid = threadIdx.x;
+    const int cnt = first < nt ? (nt - 1 - first) / step + 1 : 0;
 #pragma unroll
-        for (int j = 0; j < 4; j++) cur[j] = nxt[j];
+    for (int k = 0; k < RN_RING - 1; k++) {
+        if (k < cnt) renorm64_issue(rg, k, d, X, r0, (first + k * step) * 64);
+        cp_async_commit();  // possibly empty: every iteration commits exactly one group
+    }
+    renorm64_sums(sm, d, partial, nparts, mode, r0, fix);
+    for (int k = 0; k < cnt; k++) {
+        // the slot refilled here was read (and its values used) in iteration k - 1
+        const int kn = k + RN_RING - 1;
+        if (kn < cnt) renorm64_issue(rg, kn % RN_RING, d, X, r0, (first + kn * step) * 64);
+        cp_async_commit();
+        cp_async_wait<RN_RING - 1>();  // this thread's copies of tile k have landed
+        const int sl = k % RN_RING;
+        const float4 v[4] = {rg.v[sl][0][tid], rg.v[sl][1][tid], rg.v[sl][2][tid], rg.v[sl][3][tid]};
+        renorm64_apply(sm, d, Xout, mode, Ahi, Alo, Bhi, Blo, r0, (first + k * step) * 64, sscale, v);
     }
 }
 
-// Column chunks of a k_renorm64 launch: about 8 resident blocks per SM in total.
+// Grid (column chunks, d / 64): block (bx, by) renormalises rows 64*by.. over the column
+// tiles bx, bx + gridDim.x, ...  write_x = 0: X is only read (its renormalised values go
+// to the splits alone); fix (optional) receives the per-row (s, inv), written by the
+// blocks of column chunk 0.  Dynamic shared memory RN_SMEM.
+__global__ void __launch_bounds__(256) k_renorm64(int d, float *__restrict__ X, const double *__restrict__ partial,
+                                                  int nparts, int mode, __nv_bfloat16 *__restrict__ Ahi,
+                                                  __nv_bfloat16 *__restrict__ Alo, __nv_bfloat16 *__restrict__ Bhi,
+                                                  __nv_bfloat16 *__restrict__ Blo, float sscale, int write_x = 1,
+                                                  double2 *__restrict__ fix = nullptr) {
+    extern __shared__ __align__(16) uint8_t rn_smem[];
+    RenormSmem &sm = *reinterpret_cast<RenormSmem *>(rn_smem);
+    RenormRing &rg = *reinterpret_cast<RenormRing *>(rn_smem + sizeof(RenormSmem));
+    renorm64_strip(sm, rg, d, X, write_x ? X : nullptr, partial, nparts, mode, Ahi, Alo, Bhi, Blo,
+                   (int)blockIdx.y * 64, (int)blockIdx.x, (int)gridDim.x, sscale, blockIdx.x == 0 ? fix : nullptr);
+}
+
+// Column chunks of a k_renorm64 launch: about 8 blocks per SM in total.
 static dim3 renorm64_grid(int d) {
     const int nt = d / 64;
     int chunks = (8 * num_sms() + nt - 1) / nt;
@@ -306,22 +353,42 @@ static dim3 renorm64_grid(int d) {
     return dim3(chunks, nt);
 }
 
-// Batched: one block per work item (problem << 16 | mode << 14 | tile_r << 7 | tile_c);
-// nparts of problem i is d_i / parts_div (0 when parts_div == 0: pure split).
+// Batched: one block per work item (problem << 16 | mode << 14 | strip << 7 | chunk): the
+// column tiles chunk, chunk + renorm_chunks(d), ... of one 64-row strip; nparts of problem
+// i is d_i / parts_div (0 when parts_div == 0: pure split).  X is only read: every later
+// product takes its operands from the splits, and a squaring's Cin gets this
+// renormalisation through the row fixes (mode-0 items, chunk 0).
 __global__ void __launch_bounds__(256) k_renorm64_batched(const RenormProblem *__restrict__ probs,
                                                           const uint32_t *__restrict__ work, int parts_div,
                                                           float sscale) {
-    __shared__ RenormSmem sm;
+    extern __shared__ __align__(16) uint8_t rn_smem[];
+    RenormSmem &sm = *reinterpret_cast<RenormSmem *>(rn_smem);
+    RenormRing &rg = *reinterpret_cast<RenormRing *>(rn_smem + sizeof(RenormSmem));
     const uint32_t w = work[blockIdx.x];
     const RenormProblem &pr = probs[w >> 16];
     const int mode = (int)((w >> 14) & 3u);
     const int nparts = parts_div > 0 ? pr.d / parts_div : 0;
-    const int r0 = (int)((w >> 7) & 127u) * 64, c0 = (int)(w & 127u) * 64;
-    float4 v[4];
-    renorm64_load(pr.d, pr.X, r0, c0, v);
-    renorm64_sums(sm, pr.d, pr.partial, nparts, mode, r0);
-    renorm64_apply(sm, pr.d, pr.X, mode, pr.Ahi, pr.Alo, mode == 2 ? nullptr : pr.Bhi, mode == 2 ? nullptr : pr.Blo,
-                   r0, c0, sscale, v, [] {});
+    const int r0 = (int)((w >> 7) & 127u) * 64, chunk = (int)(w & 127u);
+    renorm64_strip(sm, rg, pr.d, pr.X, nullptr, pr.partial, nparts, mode, pr.Ahi, pr.Alo,
+                   mode == 2 ? nullptr : pr.Bhi, mode == 2 ? nullptr : pr.Blo, r0, chunk, renorm_chunks(pr.d),
+                   sscale, mode == 0 && chunk == 0 ? pr.fix : nullptr);
+}
+
+// Opts both renormalisation kernels into RN_SMEM bytes of dynamic shared memory (once per
+// device).
+static int renorm64_prepare() {
+    static bool done[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return OPB_E_UNSUPPORTED;
+    if (!done[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(k_renorm64, cudaFuncAttributeMaxDynamicSharedMemorySize, RN_SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_renorm64_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, RN_SMEM);
+        if (e != cudaSuccess) return (int)e;
+        done[dev] = true;
+    }
+    return OPB_OK;
 }
 
 // Batched ELL scatter into zeroed dense E-form matrices: thread per global ELL slot
@@ -456,11 +523,15 @@ int launch_rowsum(int d, const float *X, double *partial, cudaStream_t s) {
 }
 
 int launch_renorm(int d, float *X, const double *partial, int nparts, int eform, __nv_bfloat16 *Ahi,
-                  __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale) {
+                  __nv_bfloat16 *Alo, __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale,
+                  int write_x, double2 *fix) {
     if (d % 64 == 0 && (Ahi != nullptr) == (Alo != nullptr)) {
-        k_renorm64<<<renorm64_grid(d), 256, 0, s>>>(d, X, partial, nparts, eform ? 0 : 2, Ahi, Alo, Bhi, Blo, sscale);
+        if (int r = renorm64_prepare()) return r;
+        k_renorm64<<<renorm64_grid(d), 256, RN_SMEM, s>>>(d, X, partial, nparts, eform ? 0 : 2, Ahi, Alo, Bhi, Blo,
+                                                          sscale, write_x, eform ? fix : nullptr);
         return (int)cudaGetLastError();
     }
+    if (!write_x || fix) return OPB_E_UNSUPPORTED;
     dim3 g((d + 31) / 32, (d + 31) / 32);
     k_renorm<<<g, 256, 0, s>>>(d, X, partial, nparts, eform, Ahi, Alo, Bhi, Blo, sscale);
     return (int)cudaGetLastError();
@@ -470,14 +541,16 @@ int launch_renorm(int d, float *X, const double *partial, int nparts, int eform,
 int launch_renorm_to_p(int d, float *X, const double *partial, int nparts, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
                        __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale) {
     if (d % 64) return OPB_E_UNSUPPORTED;
-    k_renorm64<<<renorm64_grid(d), 256, 0, s>>>(d, X, partial, nparts, 1, Ahi, Alo, Bhi, Blo, sscale);
+    if (int r = renorm64_prepare()) return r;
+    k_renorm64<<<renorm64_grid(d), 256, RN_SMEM, s>>>(d, X, partial, nparts, 1, Ahi, Alo, Bhi, Blo, sscale);
     return (int)cudaGetLastError();
 }
 
 int launch_renorm_batched(const RenormProblem *probs, const uint32_t *work, int nwork, int parts_div, cudaStream_t s,
                           float sscale) {
     if (nwork <= 0) return OPB_OK;
-    k_renorm64_batched<<<nwork, 256, 0, s>>>(probs, work, parts_div, sscale);
+    if (int r = renorm64_prepare()) return r;
+    k_renorm64_batched<<<nwork, 256, RN_SMEM, s>>>(probs, work, parts_div, sscale);
     return (int)cudaGetLastError();
 }
 
@@ -644,7 +717,8 @@ OPB_API int opb_renorm_rows(int d, float *X, const double *partial, int nparts, 
     OPB_REQUIRE(opb::aligned(X, 16) && (!Ahi || (opb::aligned(Ahi, 8) && opb::aligned(Alo, 8))) &&
                     (!Bhi || (opb::aligned(Bhi, 8) && opb::aligned(Blo, 8))),
                 OPB_E_ALIGN);
-    opb::k_renorm64<<<opb::renorm64_grid(d), 256, 0, opb::stream()>>>(
+    if (int r = opb::renorm64_prepare()) return opb::set_status(r);
+    opb::k_renorm64<<<opb::renorm64_grid(d), 256, opb::RN_SMEM, opb::stream()>>>(
         d, X, partial, nparts, mode, reinterpret_cast<__nv_bfloat16 *>(Ahi), reinterpret_cast<__nv_bfloat16 *>(Alo),
         mode == 2 ? nullptr : reinterpret_cast<__nv_bfloat16 *>(Bhi),
         mode == 2 ? nullptr : reinterpret_cast<__nv_bfloat16 *>(Blo), f16 ? 32768.f : 0.f);
