@@ -178,6 +178,21 @@ __device__ __forceinline__ void umma_commit_pair(uint32_t bar) {
         : "memory");
 }
 
+// Bulk prefetch of bytes (a multiple of 16) at a 16-byte aligned global address into L2.
+__device__ __forceinline__ void prefetch_l2(const void *ptr, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ptr), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -207,18 +222,22 @@ __device__ __forceinline__ float gelu_as(float z) {
     return z >= 0.f ? fmaf(-0.5f * z, e, z) : 0.5f * z * e;
 }
 
-template <int BN, int STAGES, int NPROD = 3, int BK = TC_BK, bool PAIR = false, int CPT_MAX = 128>
+template <int BN, int STAGES, int NPROD = 3, int BK = TC_BK, bool PAIR = false, int EPIMODE = 0>
 struct TcCfg {
+    static constexpr int CPT_MAX = EPIMODE ? TC_LAYER_CPT : 128;
     static constexpr int A_BYTES = TC_BM * BK * 2;                  // one of Ahi/Alo
     static constexpr int B_ROWS = PAIR ? BN / 2 : BN;               // B rows held by this CTA
     static constexpr int B_BYTES = B_ROWS * BK * 2;                 // one of Bhi/Blo
     static constexpr int TILE_M = PAIR ? 2 * TC_BM : TC_BM;         // output rows per work item
     static constexpr int NPARTS = NPROD == 1 ? 1 : 2;  // parts loaded per operand
     static constexpr int STAGE_BYTES = NPARTS * (A_BYTES + B_BYTES);
-    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
     static constexpr int CPT = BN < CPT_MAX ? BN : CPT_MAX;  // accumulator columns per epilogue thread
     static constexpr int HALVES = BN / CPT;                 // column groups per TMEM lane
     static constexpr int EPI_WARPS = 4 * HALVES;            // epilogue warps (4 lane quadrants x groups)
+    // FP32 output: each epilogue warp transposes 32 x 32 blocks through shared memory
+    // (row stride 33 words) so that Cin loads and C stores are whole 128-byte lines
+    static constexpr int OUT_BYTES = EPIMODE == 0 ? EPI_WARPS * 32 * 33 * 4 : 0;
+    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + OUT_BYTES;
     static constexpr int THREADS = 32 * (EPI_WARPS + 2);    // + TMA producer warp + MMA warp
     static constexpr int TMEM_COLS = 2 * BN;                // two accumulators (ping-pong chunks)
     // K-blocks accumulated in TMEM per chunk: K = 128 for the split products (bounds the
@@ -265,13 +284,13 @@ struct TcBatch {
 // instructions, and an item's final store overlaps the next item's MMAs.
 template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK,
           bool PAIR = false>
-__global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? TC_LAYER_CPT : 128)>::THREADS, 1)
+__global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
               const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p,
               TcBatch bt) {
     // network layers (EPIMODE >= 1) run twice the epilogue warps: their per-element GELU,
     // not the MMAs, bounds a tile
-    using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? TC_LAYER_CPT : 128)>;
+    using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>;
     constexpr int EPI = Cfg::EPI_WARPS;
     constexpr int CPT = Cfg::CPT;
     extern __shared__ uint8_t smem_raw[];
@@ -490,8 +509,25 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? 
 #pragma unroll
                 for (int j = 0; j < CPT; j++) sum[j] = 0.f;
             }
+            // this thread's Cin row segment is prefetched into L2 about three chunks before
+            // the output needs it
+            const float *pf = nullptr;
+            long long pf_ld = 0;
+            if constexpr (EPIMODE == 0) {
+                if constexpr (BATCHED) {
+                    pf = bt.probs[prob].Cin;
+                    pf_ld = bt.probs[prob].ldc;
+                } else {
+                    pf = p.Cin;
+                    pf_ld = p.ldc;
+                }
+            }
+            const int pf_chunk = nch > 3 ? nch - 3 : 0;
             for (int c = 0; c < nch; c++, g++) {
                 const int a = (int)(g & 1);
+                if (pf && c == pf_chunk)
+                    prefetch_l2(pf + (long long)(m0 + (int)rank * TC_BM + q * 32 + lane) * pf_ld + n0 + h * CPT,
+                                CPT * 4);
                 if (!mbar_wait(accf_bar(a), (uint32_t)((g >> 1) & 1), abort_flag, TC_WAIT_NS)) {
                     ok = false;
                     break;
@@ -499,15 +535,15 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? 
                 tc_fence_after();
                 const uint32_t tacc = tmem + lane_base + (uint32_t)(a * BN + h * CPT);
 #pragma unroll
-                for (int j = 0; j < CPT / 32; j++) {
-                    uint32_t v[32];
-                    tmem_ld32(tacc + (uint32_t)(32 * j), v);
+                for (int j = 0; j < CPT / 16; j++) {
+                    uint32_t v[16];
+                    tmem_ld16(tacc + (uint32_t)(16 * j), v);
 #pragma unroll
-                    for (int i = 0; i < 32; i++) {
+                    for (int i = 0; i < 16; i++) {
                         if constexpr (NPROD == 1)
-                            sum[32 * j + i] = __uint_as_float(v[i]);
+                            sum[16 * j + i] = __uint_as_float(v[i]);
                         else
-                            sum[32 * j + i] = __fadd_rn(sum[32 * j + i], __uint_as_float(v[i]));
+                            sum[16 * j + i] = __fadd_rn(sum[16 * j + i], __uint_as_float(v[i]));
                     }
                 }
                 tc_fence_before();
@@ -578,38 +614,74 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, (EPIMODE ? 
                 p.ypart[(long long)(col0 / CPT) * p.M + row] = acc;
                 continue;
             }
-            float *crow = C + (long long)row * ldc + col0;
-            const float *cin = Cin ? Cin + (long long)row * ldc + col0 : nullptr;
-            // deferred renormalisation of Cin (the arithmetic of the E-form renormalisation
-            // kernel, so Cin reads exactly as if that kernel had stored it)
-            const double2 fx = (cin && fix) ? fix[row] : make_double2(0.0, 1.0);
-            const int dcol = row - col0;  // this row's diagonal column within the group, if any
+            // FP32 output in 32 x 32 blocks: the warp's rows (lane = row while the values are
+            // in the accumulator layout) are staged in shared memory and read back so that
+            // lane l handles row 4i + l/8, columns 4(l%8)..+3 of the block: every Cin load and
+            // C store of the warp covers four whole 128-byte lines.  The FP64 row sum keeps
+            // its order (float4 groups in column order): each group sum is parked in the
+            // first two words of its group's slots (read by this lane alone) and the row's
+            // lane adds them up.
+            float *st = reinterpret_cast<float *>(gbase + STAGES * Cfg::STAGE_BYTES + 256) + warp * (32 * 33);
+            const int rbase = m0 + (int)rank * TC_BM + q * 32;
+            const int tr = lane >> 3, tc4 = (lane & 7) * 4;
             double rs = 0.0;
 #pragma unroll
-            for (int j = 0; j < CPT; j += 4) {
-                float4 o;
-                o.x = alpha * sum[j + 0];
-                o.y = alpha * sum[j + 1];
-                o.z = alpha * sum[j + 2];
-                o.w = alpha * sum[j + 3];
-                if (cin) {
-                    const float4 ci = *reinterpret_cast<const float4 *>(cin + j);
-                    float c4[4] = {ci.x, ci.y, ci.z, ci.w};
-                    if (fix) {
+            for (int j = 0; j < CPT / 32; j++) {
 #pragma unroll
-                        for (int u = 0; u < 4; u++) {
-                            double x = (double)c4[u];
-                            if (dcol == j + u) x -= fx.x;
-                            c4[u] = (float)(x * fx.y);
-                        }
+                for (int c = 0; c < 32; c++) st[lane * 33 + c] = sum[32 * j + c];
+                __syncwarp();
+                // each half block's Cin loads are issued before any of its stores (with Cin = C
+                // each element is read and then written by this lane alone), so that four
+                // line-sized loads per warp are in flight at once
+#pragma unroll
+                for (int hb = 0; hb < 2; hb++) {
+                    float4 cv[4];
+                    if (Cin) {
+#pragma unroll
+                        for (int i = 0; i < 4; i++)
+                            cv[i] = *reinterpret_cast<const float4 *>(
+                                Cin + (long long)(rbase + 4 * (4 * hb + i) + tr) * ldc + col0 + 32 * j + tc4);
                     }
-                    o.x = fmaf(beta, c4[0], o.x);
-                    o.y = fmaf(beta, c4[1], o.y);
-                    o.z = fmaf(beta, c4[2], o.z);
-                    o.w = fmaf(beta, c4[3], o.w);
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const int rr = 4 * (4 * hb + i) + tr;
+                        const int grow = rbase + rr, gcol = col0 + 32 * j + tc4;
+                        float4 o;
+                        o.x = alpha * st[rr * 33 + tc4 + 0];
+                        o.y = alpha * st[rr * 33 + tc4 + 1];
+                        o.z = alpha * st[rr * 33 + tc4 + 2];
+                        o.w = alpha * st[rr * 33 + tc4 + 3];
+                        if (Cin) {
+                            float c4[4] = {cv[i].x, cv[i].y, cv[i].z, cv[i].w};
+                            if (fix) {
+                                // deferred renormalisation of Cin (the arithmetic of the
+                                // E-form renormalisation kernel, so Cin reads exactly as if
+                                // that kernel had stored it)
+                                const double2 fx = fix[grow];
+#pragma unroll
+                                for (int u = 0; u < 4; u++) {
+                                    double x = (double)c4[u];
+                                    if (grow == gcol + u) x -= fx.x;
+                                    c4[u] = (float)(x * fx.y);
+                                }
+                            }
+                            o.x = fmaf(beta, c4[0], o.x);
+                            o.y = fmaf(beta, c4[1], o.y);
+                            o.z = fmaf(beta, c4[2], o.z);
+                            o.w = fmaf(beta, c4[3], o.w);
+                        }
+                        *reinterpret_cast<float4 *>(C + (long long)grow * ldc + gcol) = o;
+                        const double g = (double)o.x + (double)o.y + (double)o.z + (double)o.w;
+                        st[rr * 33 + tc4] = __int_as_float(__double2loint(g));
+                        st[rr * 33 + tc4 + 1] = __int_as_float(__double2hiint(g));
+                    }
                 }
-                *reinterpret_cast<float4 *>(crow + j) = o;
-                rs += (double)o.x + (double)o.y + (double)o.z + (double)o.w;
+                __syncwarp();
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    rs += __hiloint2double(__float_as_int(st[lane * 33 + 4 * k + 1]),
+                                           __float_as_int(st[lane * 33 + 4 * k]));
+                __syncwarp();  // before the next block overwrites the buffer
             }
             if (rowsum) rowsum[(long long)(col0 / CPT) * M + row] = rs;
         }
@@ -707,7 +779,7 @@ int tc_gemm_check(const TcGemmArgs &a) {
 template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK,
           bool PAIR = false>
 static int set_smem_attr() {
-    using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR>;
+    using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>;
     static bool attr_set[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -891,7 +963,7 @@ int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, 
                     long long ldw, float alpha, const float *bias, __nv_bfloat16 *H, long long ldh, cudaStream_t s,
                     const float *w5, float *ypart) {
     constexpr int BN = 256, STAGES = 4;
-    using Cfg = TcCfg<BN, STAGES, 1, TC_BK, false, TC_LAYER_CPT>;
+    using Cfg = TcCfg<BN, STAGES, 1, TC_BK, false, 1>;
     const bool fused = w5 != nullptr;
     if (M <= 0 || M % TC_BM || N % BN || K % TC_BK || (fused && N != BN)) return OPB_E_UNSUPPORTED;
     if (!A || !W || !bias || (fused ? !ypart : !H)) return OPB_E_NULL;
