@@ -262,11 +262,12 @@ def run_b200(args, rank, world, local_rank):
         mma_flops = 3 * 2.0 * d ** 3
         achieved = mma_flops / (k_ms * 1e-3) / 1e12
         # DRAM bytes (read + write) of one launch of this kernel at d = 6144 from an ncu
-        # capture (dram__bytes_read.sum 930.5 MB + dram__bytes_write.sum 138.5 MB); the
+        # capture (dram__bytes_read.sum 936.6 MB + dram__bytes_write.sum 142.1 MB); the
         # algorithmic traffic is 4 BF16 parts + Cin read, C written = 16 d^2 + 8 d^2 bytes.
-        traffic = 1069.0e6 if d == 6144 else None
+        traffic = 1078.7e6 if d == 6144 else None
         kern = {"bound": "tensor", "achieved": round(achieved, 1), "peak": bf16_burst, "unit": "TFLOP/s",
-                "frac": round(achieved / bf16_burst, 4), "traffic": traffic, "traffic_unit": "DRAM bytes per launch",
+                "frac": round(achieved / bf16_burst, 4), "frac_of_sustained": round(achieved / bf16_sus, 4),
+                "traffic": traffic, "traffic_unit": "DRAM bytes per launch",
                 "algorithmic_bytes": 24.0 * d * d, "peak_source": f"{src} burst bf16",
                 "kernel": "k_tc_gemm<256,3,pair> (E-form squaring on 2-CTA clusters, cta_group::2, "
                           f"{d}^3 x 3 BF16 products)",
