@@ -93,8 +93,10 @@ struct opb_batch_plan {
     opb::BatchLattice *lats = nullptr;
     opb::TcProblem *sq = nullptr, *chain = nullptr, *price = nullptr;
     opb::RenormProblem *rn_sq = nullptr, *rn_chain = nullptr;
-    CUtensorMap *maps_sq[3] = {nullptr, nullptr, nullptr};  // per bn (128, 64, 256)
-    CUtensorMap *maps_price = nullptr;
+    // 4 maps per lattice (Ahi, Alo, Bhi, Blo), the same for every tile width: squaring (B =
+    // E's row-major A parts, MN-major), chain (B = P1's row-major parts), pricing (K-major
+    // payoff parts)
+    CUtensorMap *maps_sq = nullptr, *maps_ch = nullptr, *maps_price = nullptr;
     uint32_t *work = nullptr;
     float *E_base = nullptr;
     size_t E_bytes = 0;
@@ -169,10 +171,9 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     auto pr = c.take<opb::TcProblem>(n);
     auto rs = c.take<opb::RenormProblem>(n);
     auto rc = c.take<opb::RenormProblem>(n);
-    auto m128 = c.take<CUtensorMap>(4 * (size_t)n);
-    auto m64 = c.take<CUtensorMap>(4 * (size_t)n);
+    auto msq = c.take<CUtensorMap>(4 * (size_t)n);
+    auto mch = c.take<CUtensorMap>(4 * (size_t)n);
     auto mp = c.take<CUtensorMap>(4 * (size_t)n);
-    auto m256 = c.take<CUtensorMap>(4 * (size_t)n);
     size_t Etot = 0;
     for (int i = 0; i < n; i++) Etot += (size_t)b->d[i] * b->d[i];
     float *E = c.take<float>(Etot);
@@ -265,7 +266,7 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     P->total_rows = off[n]; P->ell_width = b->ell_width; P->cols = b->gen_cols; P->vals = b->gen_vals;
     P->x = b->x; P->strikes = b->strikes; P->period = b->period;
     P->lats = lats; P->sq = sq; P->chain = ch; P->price = pr; P->rn_sq = rs; P->rn_chain = rc;
-    P->maps_sq[0] = m128; P->maps_sq[1] = m64; P->maps_sq[2] = m256; P->maps_price = mp; P->work = work;
+    P->maps_sq = msq; P->maps_ch = mch; P->maps_price = mp; P->work = work;
     P->E_base = E; P->E_bytes = Etot * sizeof(float);
     for (int cfg = 0; cfg < NCFG; cfg++) {
         P->gemm_level[cfg] = gl[cfg];
@@ -322,13 +323,12 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     std::vector<opb::BatchLattice> lats(n);
     std::vector<opb::TcProblem> sq(n), ch(n), pr(n);
     std::vector<opb::RenormProblem> rs(n), rc(n);
-    std::vector<CUtensorMap> m128(4 * (size_t)n), m64(4 * (size_t)n), mp(4 * (size_t)n), m256(4 * (size_t)n);
+    std::vector<CUtensorMap> msq(4 * (size_t)n), mch(4 * (size_t)n), mp(4 * (size_t)n);
     // recompute buffer pointers exactly as layout() carved them
     Carve cv{base, 0};
     cv.take<opb::BatchLattice>(n); cv.take<opb::TcProblem>(n); cv.take<opb::TcProblem>(n); cv.take<opb::TcProblem>(n);
     cv.take<opb::RenormProblem>(n); cv.take<opb::RenormProblem>(n);
     cv.take<CUtensorMap>(4 * (size_t)n); cv.take<CUtensorMap>(4 * (size_t)n); cv.take<CUtensorMap>(4 * (size_t)n);
-    cv.take<CUtensorMap>(4 * (size_t)n);
     size_t Etot = 0;
     for (int i = 0; i < n; i++) Etot += (size_t)b->d[i] * b->d[i];
     float *E = cv.take<float>(Etot), *Pa = cv.take<float>(Etot);
@@ -363,16 +363,14 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
         pr[i] = opb::TcProblem{d, P->ldk, d, 0, L.V, nullptr, nullptr, P->ldk, un1, 0.f, nullptr};
         rs[i] = opb::RenormProblem{d, 0, L.E, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo, fix + ro};
         rc[i] = opb::RenormProblem{d, 0, L.Pa, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo, nullptr};
-        rc_status = opb::tc_make_maps(&m128[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 128, f16);
+        rc_status = opb::tc_make_maps(&msq[4 * (size_t)i], Ah + eo, Al + eo, d, d, Ah + eo, Al + eo, d, d, d, 64,
+                                      f16, 1);
         if (rc_status == OPB_OK)
-            rc_status =
-                opb::tc_make_maps(&m64[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 64, f16);
+            rc_status = opb::tc_make_maps(&mch[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 64,
+                                          f16, 1);
         if (rc_status == OPB_OK)
             rc_status =
                 opb::tc_make_maps(&mp[4 * (size_t)i], Ah + eo, Al + eo, d, d, L.GThi, L.GTlo, P->ldk, d, d, 64, f16);
-        if (rc_status == OPB_OK && d % 256 == 0)  // 128 x 256 tiles only for sizes that are multiples of 256
-            rc_status =
-                opb::tc_make_maps(&m256[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 256, f16);
         eo += (size_t)d * d;
         po += (size_t)(d / 64) * d;
         ro += d;
@@ -394,10 +392,9 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     if (e == cudaSuccess) e = up(P->price, pr.data(), sizeof(opb::TcProblem) * n);
     if (e == cudaSuccess) e = up(P->rn_sq, rs.data(), sizeof(opb::RenormProblem) * n);
     if (e == cudaSuccess) e = up(P->rn_chain, rc.data(), sizeof(opb::RenormProblem) * n);
-    if (e == cudaSuccess) e = up(P->maps_sq[0], m128.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
-    if (e == cudaSuccess) e = up(P->maps_sq[1], m64.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
+    if (e == cudaSuccess) e = up(P->maps_sq, msq.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
+    if (e == cudaSuccess) e = up(P->maps_ch, mch.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
     if (e == cudaSuccess) e = up(P->maps_price, mp.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
-    if (e == cudaSuccess) e = up(P->maps_sq[2], m256.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
     if (e == cudaSuccess) e = up(P->work, W.data(), sizeof(uint32_t) * W.size());
     const cudaError_t es = cudaStreamSynchronize(ls);
     if (e == cudaSuccess) e = es;
@@ -432,25 +429,21 @@ OPB_API int opb_batch_set_config(opb_batch_plan *P, int cfg, int grid) {
 
 namespace {
 
-int map_index(int bn) { return bn == 128 ? 0 : (bn == 64 ? 1 : 2); }
-
-// One squaring level (or, with chain, the chain product) under configuration cfg: one
-// launch, or two for the 256-mixed configurations (128 x 256 items, then 128 x 128 ones).
-int cfg_gemm(opb_batch_plan *P, int cfg, const opb::TcProblem *probs, const ListRef &l, const ListRef &rest,
-             cudaStream_t s) {
+// One squaring level (or the chain product) under configuration cfg: one launch, or two
+// for the 256-mixed configurations (256-wide items, then 128 x 128 ones).  maps: the
+// squaring or the chain table (MN-major B).
+int cfg_gemm(opb_batch_plan *P, int cfg, const CUtensorMap *maps, const opb::TcProblem *probs, const ListRef &l,
+             const ListRef &rest, cudaStream_t s) {
     const int bn = CFG_BN[cfg];
-    // pair items: each CTA loads 128 rows of A and of B, the 128-row maps
-    int r = CFG_PAIR[cfg]
-                ? opb::launch_tc_gemm_batched_pair(P->maps_sq[0], probs, P->work + l.off, l.n, s, P->f16)
-                : opb::launch_tc_gemm_batched(bn, P->maps_sq[map_index(bn)], probs, P->work + l.off, l.n, P->grid,
-                                              s, P->f16);
+    int r = CFG_PAIR[cfg] ? opb::launch_tc_gemm_batched_pair(maps, probs, P->work + l.off, l.n, s, P->f16, 1)
+                          : opb::launch_tc_gemm_batched(bn, maps, probs, P->work + l.off, l.n, P->grid, s, P->f16, 1);
     if (r == 0 && rest.n > 0)
-        r = opb::launch_tc_gemm_batched(128, P->maps_sq[0], probs, P->work + rest.off, rest.n, P->grid, s, P->f16);
+        r = opb::launch_tc_gemm_batched(128, maps, probs, P->work + rest.off, rest.n, P->grid, s, P->f16, 1);
     return r;
 }
 
 int level_gemm(opb_batch_plan *P, int cfg, int level, cudaStream_t s) {
-    return cfg_gemm(P, cfg, P->sq, P->gemm_level[cfg][level], P->gemm_level_rest[cfg][level], s);
+    return cfg_gemm(P, cfg, P->maps_sq, P->sq, P->gemm_level[cfg][level], P->gemm_level_rest[cfg][level], s);
 }
 
 }  // namespace
@@ -485,12 +478,12 @@ OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
     BT(opb::launch_payoff_batched(P->lats, P->nlat, P->total_rows, P->nK, P->ldk, P->x, P->strikes, s, P->f16));
     for (int m = 1; m <= P->nmat; m++) {
         if (m > 1) {
-            BT(cfg_gemm(P, cfg, P->chain, P->gemm_chain[cfg], P->gemm_chain_rest[cfg], s));
+            BT(cfg_gemm(P, cfg, P->maps_ch, P->chain, P->gemm_chain[cfg], P->gemm_chain_rest[cfg], s));
             BT(opb::launch_renorm_batched(P->rn_chain, P->work + P->rn_chain_list.off, P->rn_chain_list.n, pdiv, s,
                                           ss));
         }
         BT(opb::launch_tc_gemm_batched(64, P->maps_price, P->price, P->work + P->gemm_price.off, P->gemm_price.n,
-                                       P->grid, s, P->f16));
+                                       P->grid, s, P->f16, 0));
         BT(opb::launch_quotes_batched(P->lats, P->nlat, P->nK, P->ldk, m, P->nmat, quotes, s, P->f16));
     }
 #undef BT

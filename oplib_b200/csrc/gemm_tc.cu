@@ -110,11 +110,24 @@ __device__ __forceinline__ uint64_t umma_desc_sw(uint32_t saddr) {
     return d;
 }
 
+// MN-major 128-byte-swizzled descriptor for a B tile stored K x N (N contiguous) as
+// 64-column boxes of BK = 64 rows: each box is 64 rows of 128 bytes (8-row swizzle atoms
+// 1024 bytes apart: SBO), and the boxes along N are 8192 bytes apart (LBO).
+__device__ __forceinline__ uint64_t umma_desc_mn(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)(8192 >> 4) << 16;  // LBO: next 64 columns
+    d |= (uint64_t)(1024 >> 4) << 32;  // SBO: next 8 rows of K
+    d |= (uint64_t)1 << 46;            // version
+    d |= (uint64_t)2 << 61;            // SWIZZLE_128B
+    return d;
+}
+
 // kind::f16 instruction descriptor: D = F32, A = B = BF16 (format 1) or F16 (format 0),
-// both K-major, N, M (128 for one CTA, 256 for a CTA pair).
-__host__ __device__ constexpr uint32_t umma_idesc_16(int n, bool f16, int m = TC_BM) {
-    return (1u << 4) | ((f16 ? 0u : 1u) << 7) | ((f16 ? 0u : 1u) << 10) | ((uint32_t)(n >> 3) << 17) |
-           ((uint32_t)(m >> 4) << 24);
+// A K-major, B K-major or (bmn) MN-major, N, M (128 for one CTA, 256 for a CTA pair).
+__host__ __device__ constexpr uint32_t umma_idesc_16(int n, bool f16, int m = TC_BM, bool bmn = false) {
+    return (1u << 4) | ((f16 ? 0u : 1u) << 7) | ((f16 ? 0u : 1u) << 10) | ((bmn ? 1u : 0u) << 16) |
+           ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -283,7 +296,7 @@ struct TcBatch {
 // accumulator.  The tensor cores' truncating accumulation thus spans only 12*CHUNK MMA
 // instructions, and an item's final store overlaps the next item's MMAs.
 template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK,
-          bool PAIR = false>
+          bool PAIR = false, bool BMN = false>
 __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
               const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p,
@@ -293,6 +306,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
     using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>;
     constexpr int EPI = Cfg::EPI_WARPS;
     constexpr int CPT = Cfg::CPT;
+    static_assert(!BMN || (BK == 64 && NPROD == 3 && Cfg::B_ROWS % 64 == 0), "MN-major B: split products, BK 64");
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -399,8 +413,17 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                         const uint32_t fb = map_to_rank(full_bar(s), 0);
                         tma_load_2d_pair(st, mp[0], fb, kx, ma);
                         tma_load_2d_pair(st + Cfg::A_BYTES, mp[1], fb, kx, ma);
-                        tma_load_2d_pair(st + 2 * Cfg::A_BYTES, mp[2], fb, kx, nb);
-                        tma_load_2d_pair(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, mp[3], fb, kx, nb);
+                        if constexpr (BMN) {
+#pragma unroll
+                            for (int i = 0; i < Cfg::B_ROWS / 64; i++) {
+                                tma_load_2d_pair(st + 2 * Cfg::A_BYTES + i * (BK * 128), mp[2], fb, nb + 64 * i, kx);
+                                tma_load_2d_pair(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES + i * (BK * 128), mp[3], fb,
+                                                 nb + 64 * i, kx);
+                            }
+                        } else {
+                            tma_load_2d_pair(st + 2 * Cfg::A_BYTES, mp[2], fb, kx, nb);
+                            tma_load_2d_pair(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, mp[3], fb, kx, nb);
+                        }
                     } else {
                         mbar_expect_tx(full_bar(s), Cfg::STAGE_BYTES);
                         tma_load_2d(st, mp[0], full_bar(s), kx, ma);
@@ -408,8 +431,18 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                             tma_load_2d(st + Cfg::A_BYTES, mp[2], full_bar(s), kx, nb);
                         } else {
                             tma_load_2d(st + Cfg::A_BYTES, mp[1], full_bar(s), kx, ma);
-                            tma_load_2d(st + 2 * Cfg::A_BYTES, mp[2], full_bar(s), kx, nb);
-                            tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, mp[3], full_bar(s), kx, nb);
+                            if constexpr (BMN) {
+#pragma unroll
+                                for (int i = 0; i < Cfg::B_ROWS / 64; i++) {
+                                    tma_load_2d(st + 2 * Cfg::A_BYTES + i * (BK * 128), mp[2], full_bar(s),
+                                                nb + 64 * i, kx);
+                                    tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES + i * (BK * 128), mp[3],
+                                                full_bar(s), nb + 64 * i, kx);
+                                }
+                            } else {
+                                tma_load_2d(st + 2 * Cfg::A_BYTES, mp[2], full_bar(s), kx, nb);
+                                tma_load_2d(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES, mp[3], full_bar(s), kx, nb);
+                            }
                         }
                     }
                 }
@@ -431,7 +464,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
     } else if (warp == EPI + 1) {
         if (lane == 0 && rank == 0) {
             // ---------------- MMA issuer (pair mode: the even CTA issues for both)
-            const uint32_t idesc = umma_idesc_16(BN, F16, Cfg::TILE_M);
+            const uint32_t idesc = umma_idesc_16(BN, F16, Cfg::TILE_M, BMN);
             long kbg = 0, g = 0;  // K-blocks consumed, chunks issued
             bool ok = true;
             for (int t = item0; t < nitems && ok; t += istep) {
@@ -457,21 +490,25 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                         const uint32_t st = base + s * Cfg::STAGE_BYTES;
                         const uint64_t dAh = umma_desc_sw<BK>(st);
                         const uint64_t dAl = umma_desc_sw<BK>(st + Cfg::A_BYTES);
-                        const uint64_t dBh = umma_desc_sw<BK>(st + Cfg::NPARTS * Cfg::A_BYTES);
-                        const uint64_t dBl = umma_desc_sw<BK>(st + 2 * Cfg::A_BYTES + Cfg::B_BYTES);
+                        const uint32_t sBh = st + Cfg::NPARTS * Cfg::A_BYTES;
+                        const uint32_t sBl = st + 2 * Cfg::A_BYTES + Cfg::B_BYTES;
+                        const uint64_t dBh = BMN ? umma_desc_mn(sBh) : umma_desc_sw<BK>(sBh);
+                        const uint64_t dBl = BMN ? umma_desc_mn(sBl) : umma_desc_sw<BK>(sBl);
 #pragma unroll
                         for (int k16 = 0; k16 < BK / 16; k16++) {
                             const uint64_t adv = (uint64_t)((k16 * 32) >> 4);  // +32 bytes along K
+                            // MN-major B: +16 rows of 128 bytes along K
+                            const uint64_t advb = BMN ? (uint64_t)((k16 * 16 * 128) >> 4) : adv;
                             const uint32_t acc0 = (kb > c * Cfg::CHUNK || k16 > 0) ? 1u : 0u;
                             if constexpr (PAIR) {
-                                umma_bf16_pair(dacc, dAh + adv, dBh + adv, idesc, acc0);
-                                umma_bf16_pair(dacc, dAh + adv, dBl + adv, idesc, 1u);
-                                umma_bf16_pair(dacc, dAl + adv, dBh + adv, idesc, 1u);
+                                umma_bf16_pair(dacc, dAh + adv, dBh + advb, idesc, acc0);
+                                umma_bf16_pair(dacc, dAh + adv, dBl + advb, idesc, 1u);
+                                umma_bf16_pair(dacc, dAl + adv, dBh + advb, idesc, 1u);
                             } else {
-                                umma_bf16(dacc, dAh + adv, dBh + adv, idesc, acc0);
+                                umma_bf16(dacc, dAh + adv, dBh + advb, idesc, acc0);
                                 if constexpr (NPROD == 3) {
-                                    umma_bf16(dacc, dAh + adv, dBl + adv, idesc, 1u);
-                                    umma_bf16(dacc, dAl + adv, dBh + adv, idesc, 1u);
+                                    umma_bf16(dacc, dAh + adv, dBl + advb, idesc, 1u);
+                                    umma_bf16(dacc, dAl + adv, dBh + advb, idesc, 1u);
                                 }
                             }
                         }
@@ -733,6 +770,32 @@ static int make_map(CUtensorMap *m, const void *ptr, long long rows, long long K
     return r == CUDA_SUCCESS ? OPB_OK : OPB_E_ARG;
 }
 
+// K x N bf16 row-major matrix (leading dimension ld elements) read as an MN-major B
+// operand: box = 64 columns x 64 rows, 128-byte swizzle.
+static int make_map_mn(CUtensorMap *m, const void *ptr, long long K, long long N, long long ld, int f16 = 0) {
+    auto enc = get_encode();
+    if (!enc) return OPB_E_UNSUPPORTED;
+    cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)K};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+    cuuint32_t box[2] = {64, 64};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(m, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                     const_cast<void *>(ptr), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? OPB_OK : OPB_E_ARG;
+}
+
+// The B maps of a product: K-major (N x K, box rows = brows) or MN-major (K x N).
+static int make_b_maps(CUtensorMap *hi, CUtensorMap *lo, const TcGemmArgs &a, int brows, int f16, int bk) {
+    int r;
+    if (a.b_kn) {
+        if ((r = make_map_mn(hi, a.Bhi, a.K, a.N, a.ldb, f16)) != OPB_OK) return r;
+        return make_map_mn(lo, a.Blo, a.K, a.N, a.ldb, f16);
+    }
+    if ((r = make_map(hi, a.Bhi, a.N, a.K, a.ldb, brows, f16, bk)) != OPB_OK) return r;
+    return make_map(lo, a.Blo, a.N, a.K, a.ldb, brows, f16, bk);
+}
+
 static int g_tile_override = 0;  // 0 = automatic
 static int g_bk256 = 64;          // K depth of a pipeline stage for 256-wide tiles (32 or 64)
 static int g_pair = 1;            // 256 x 256 tiles on CTA pairs (cta_group::2) when M % 256 == 0
@@ -767,7 +830,7 @@ int tc_gemm_check(const TcGemmArgs &a) {
     if (a.M <= 0 || a.N <= 0 || a.K <= 0) return OPB_E_ARG;
     if (a.M % TC_BM || a.K % TC_BK || !tc_gemm_tile_n(a.N)) return OPB_E_UNSUPPORTED;
     if (!a.Ahi || !a.Alo || !a.Bhi || !a.Blo || !a.C) return OPB_E_NULL;
-    if (a.lda < a.K || a.ldb < a.K || a.ldc < a.N) return OPB_E_ARG;
+    if (a.lda < a.K || a.ldb < (a.b_kn ? a.N : a.K) || a.ldc < a.N) return OPB_E_ARG;
     // TMA: 16-byte aligned bases and row strides; float4 epilogue: 16-byte aligned rows
     if (!aligned(a.Ahi, 16) || !aligned(a.Alo, 16) || !aligned(a.Bhi, 16) || !aligned(a.Blo, 16)) return OPB_E_ALIGN;
     if ((a.lda * 2) % 16 || (a.ldb * 2) % 16 || a.ldc % 4 || !aligned(a.C, 16)) return OPB_E_ALIGN;
@@ -777,14 +840,14 @@ int tc_gemm_check(const TcGemmArgs &a) {
 }
 
 template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK,
-          bool PAIR = false>
+          bool PAIR = false, bool BMN = false>
 static int set_smem_attr() {
     using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>;
     static bool attr_set[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED, F16, NPROD, EPIMODE, BK, PAIR>,
+        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED, F16, NPROD, EPIMODE, BK, PAIR, BMN>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              Cfg::SMEM);
         if (e != cudaSuccess) return (int)e;
@@ -793,43 +856,42 @@ static int set_smem_attr() {
     return 0;
 }
 
-template <int BN, int STAGES, bool F16, int BK = TC_BK>
+template <int BN, int STAGES, bool F16, int BK = TC_BK, bool BMN = false>
 static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
     using Cfg = TcCfg<BN, STAGES, 3, BK>;
-    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, BK>();
+    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, BK, false, BMN>();
     if (e0) return e0;
     CUtensorMap mAh, mAl, mBh, mBl;
     int r;
     if ((r = make_map(&mAh, a.Ahi, a.M, a.K, a.lda, TC_BM, F16, BK)) != OPB_OK) return r;
     if ((r = make_map(&mAl, a.Alo, a.M, a.K, a.lda, TC_BM, F16, BK)) != OPB_OK) return r;
-    if ((r = make_map(&mBh, a.Bhi, a.N, a.K, a.ldb, BN, F16, BK)) != OPB_OK) return r;
-    if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN, F16, BK)) != OPB_OK) return r;
+    if ((r = make_b_maps(&mBh, &mBl, a, BN, F16, BK)) != OPB_OK) return r;
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
     p.group_m = g_group_m;
     p.cin_fix = a.cin_fix;
     const int ntiles = (a.M / TC_BM) * (a.N / BN);
     const int grid = ntiles < num_sms() ? ntiles : num_sms();
     TcBatch none{nullptr, nullptr, nullptr, 0};
-    k_tc_gemm<BN, STAGES, false, F16, 3, 0, BK><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl, p, none);
+    k_tc_gemm<BN, STAGES, false, F16, 3, 0, BK, false, BMN><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl,
+                                                                                                  p, none);
     return (int)cudaGetLastError();
 }
 
 // 256 x 256 output tiles on 2-CTA clusters: each CTA loads its 128 rows of A and 128 rows
 // of B, the even CTA issues cta_group::2 MMAs over both CTAs' shared memory.  The grid is
 // as many clusters as can be resident at once (at most one per SM pair).
-template <bool F16>
+template <bool F16, bool BMN>
 static int launch_tc_pair(const TcGemmArgs &a, cudaStream_t s) {
     constexpr int BN = 256, STAGES = 3;
     using Cfg = TcCfg<BN, STAGES, 3, TC_BK, true>;
-    auto kern = k_tc_gemm<BN, STAGES, false, F16, 3, 0, TC_BK, true>;
-    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, TC_BK, true>();
+    auto kern = k_tc_gemm<BN, STAGES, false, F16, 3, 0, TC_BK, true, BMN>;
+    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, TC_BK, true, BMN>();
     if (e0) return e0;
     CUtensorMap mAh, mAl, mBh, mBl;
     int r;
     if ((r = make_map(&mAh, a.Ahi, a.M, a.K, a.lda, TC_BM, F16)) != OPB_OK) return r;
     if ((r = make_map(&mAl, a.Alo, a.M, a.K, a.lda, TC_BM, F16)) != OPB_OK) return r;
-    if ((r = make_map(&mBh, a.Bhi, a.N, a.K, a.ldb, BN / 2, F16)) != OPB_OK) return r;
-    if ((r = make_map(&mBl, a.Blo, a.N, a.K, a.ldb, BN / 2, F16)) != OPB_OK) return r;
+    if ((r = make_b_maps(&mBh, &mBl, a, BN / 2, F16, TC_BK)) != OPB_OK) return r;
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
     p.group_m = g_group_m;
     p.cin_fix = a.cin_fix;
@@ -866,39 +928,44 @@ static int launch_tc_pair(const TcGemmArgs &a, cudaStream_t s) {
 
 int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo, long long M, long long lda,
                  const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long N, long long ldb, long long K, int bn,
-                 int f16) {
+                 int f16, int b_kn) {
     int r;
     if ((r = make_map(&out4[0], Ahi, M, K, lda, TC_BM, f16)) != OPB_OK) return r;
     if ((r = make_map(&out4[1], Alo, M, K, lda, TC_BM, f16)) != OPB_OK) return r;
+    if (b_kn) {
+        if ((r = make_map_mn(&out4[2], Bhi, K, N, ldb, f16)) != OPB_OK) return r;
+        return make_map_mn(&out4[3], Blo, K, N, ldb, f16);
+    }
     if ((r = make_map(&out4[2], Bhi, N, K, ldb, bn, f16)) != OPB_OK) return r;
     if ((r = make_map(&out4[3], Blo, N, K, ldb, bn, f16)) != OPB_OK) return r;
     return OPB_OK;
 }
 
-template <int BN, int STAGES, bool F16>
+template <int BN, int STAGES, bool F16, bool BMN>
 static int launch_batched_impl(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
                                int grid, cudaStream_t s) {
     using Cfg = TcCfg<BN, STAGES>;
-    int e0 = set_smem_attr<BN, STAGES, true, F16>();
+    int e0 = set_smem_attr<BN, STAGES, true, F16, 3, 0, TC_BK, false, BMN>();
     if (e0) return e0;
     CUtensorMap dummy;
     std::memset(&dummy, 0, sizeof(dummy));
     TcParams p{};
     TcBatch bt{maps, probs, work, nwork};
-    k_tc_gemm<BN, STAGES, true, F16><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(dummy, dummy, dummy, dummy, p, bt);
+    k_tc_gemm<BN, STAGES, true, F16, 3, 0, TC_BK, false, BMN><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(
+        dummy, dummy, dummy, dummy, p, bt);
     return (int)cudaGetLastError();
 }
 
 // Batched 256 x 256 items on 2-CTA clusters: work items (problem << 16 | m-tile << 8 |
 // n-tile) in 256-row / 256-column units, maps with 128-row boxes for A and B (each CTA
 // loads its own half), problems with M % 256 == 0 and N % 256 == 0.
-template <bool F16>
+template <bool F16, bool BMN>
 static int launch_batched_pair_impl(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
                                     cudaStream_t s) {
     constexpr int BN = 256, STAGES = 3;
     using Cfg = TcCfg<BN, STAGES, 3, TC_BK, true>;
-    auto kern = k_tc_gemm<BN, STAGES, true, F16, 3, 0, TC_BK, true>;
-    int e0 = set_smem_attr<BN, STAGES, true, F16, 3, 0, TC_BK, true>();
+    auto kern = k_tc_gemm<BN, STAGES, true, F16, 3, 0, TC_BK, true, BMN>;
+    int e0 = set_smem_attr<BN, STAGES, true, F16, 3, 0, TC_BK, true, BMN>();
     if (e0) return e0;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -933,24 +1000,30 @@ static int launch_batched_pair_impl(const CUtensorMap *maps, const TcProblem *pr
     return e == cudaSuccess ? (int)cudaGetLastError() : (int)e;
 }
 
+// Batched squaring and chain products take MN-major B maps (b_kn = 1): pair and 256/128
+// tiles exist only in that form; 64-wide tiles in both (pricing is K-major).
 int launch_tc_gemm_batched_pair(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                                cudaStream_t s, int f16) {
+                                cudaStream_t s, int f16, int b_kn) {
     if (nwork <= 0) return OPB_OK;
-    return f16 ? launch_batched_pair_impl<true>(maps, probs, work, nwork, s)
-               : launch_batched_pair_impl<false>(maps, probs, work, nwork, s);
+    if (!b_kn) return OPB_E_UNSUPPORTED;
+    return f16 ? launch_batched_pair_impl<true, true>(maps, probs, work, nwork, s)
+               : launch_batched_pair_impl<false, true>(maps, probs, work, nwork, s);
 }
 
 int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                           int grid, cudaStream_t s, int f16) {
+                           int grid, cudaStream_t s, int f16, int b_kn) {
     if (nwork <= 0) return OPB_OK;
     if (grid <= 0 || grid > nwork) grid = nwork < num_sms() ? nwork : num_sms();
-    switch (bn * 2 + (f16 ? 1 : 0)) {
-        case 512: return launch_batched_impl<256, 2, false>(maps, probs, work, nwork, grid, s);
-        case 513: return launch_batched_impl<256, 2, true>(maps, probs, work, nwork, grid, s);
-        case 256: return launch_batched_impl<128, 3, false>(maps, probs, work, nwork, grid, s);
-        case 257: return launch_batched_impl<128, 3, true>(maps, probs, work, nwork, grid, s);
-        case 128: return launch_batched_impl<64, 4, false>(maps, probs, work, nwork, grid, s);
-        case 129: return launch_batched_impl<64, 4, true>(maps, probs, work, nwork, grid, s);
+    if (!b_kn && bn != 64) return OPB_E_UNSUPPORTED;
+    switch (bn * 4 + (f16 ? 2 : 0) + (b_kn ? 1 : 0)) {
+        case 1025: return launch_batched_impl<256, 2, false, true>(maps, probs, work, nwork, grid, s);
+        case 1027: return launch_batched_impl<256, 2, true, true>(maps, probs, work, nwork, grid, s);
+        case 513: return launch_batched_impl<128, 3, false, true>(maps, probs, work, nwork, grid, s);
+        case 515: return launch_batched_impl<128, 3, true, true>(maps, probs, work, nwork, grid, s);
+        case 256: return launch_batched_impl<64, 4, false, false>(maps, probs, work, nwork, grid, s);
+        case 257: return launch_batched_impl<64, 4, false, true>(maps, probs, work, nwork, grid, s);
+        case 258: return launch_batched_impl<64, 4, true, false>(maps, probs, work, nwork, grid, s);
+        case 259: return launch_batched_impl<64, 4, true, true>(maps, probs, work, nwork, grid, s);
         default: return OPB_E_UNSUPPORTED;
     }
 }
@@ -988,12 +1061,24 @@ int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, 
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
     int c = tc_gemm_check(a);
     if (c != OPB_OK) return c;
+    const bool pair = g_pair && a.M % (2 * TC_BM) == 0;
+    if (a.b_kn) {  // MN-major B (K x N): BK = 64 only
+        switch (tile_for(a.M, a.N) * 2 + (a.f16 ? 1 : 0)) {
+            case 512: return pair ? launch_tc_pair<false, true>(a, s) : launch_tc_impl<256, 2, false, 64, true>(a, s);
+            case 513: return pair ? launch_tc_pair<true, true>(a, s) : launch_tc_impl<256, 2, true, 64, true>(a, s);
+            case 256: return launch_tc_impl<128, 3, false, 64, true>(a, s);
+            case 257: return launch_tc_impl<128, 3, true, 64, true>(a, s);
+            case 128: return launch_tc_impl<64, 4, false, 64, true>(a, s);
+            case 129: return launch_tc_impl<64, 4, true, 64, true>(a, s);
+            default: return OPB_E_UNSUPPORTED;
+        }
+    }
     switch (tile_for(a.M, a.N) * 2 + (a.f16 ? 1 : 0)) {
         case 512:
-            if (g_pair && a.M % (2 * TC_BM) == 0) return launch_tc_pair<false>(a, s);
+            if (pair) return launch_tc_pair<false, false>(a, s);
             return g_bk256 == 32 ? launch_tc_impl<256, 4, false, 32>(a, s) : launch_tc_impl<256, 2, false>(a, s);
         case 513:
-            if (g_pair && a.M % (2 * TC_BM) == 0) return launch_tc_pair<true>(a, s);
+            if (pair) return launch_tc_pair<true, false>(a, s);
             return g_bk256 == 32 ? launch_tc_impl<256, 4, true, 32>(a, s) : launch_tc_impl<256, 2, true>(a, s);
         case 256: return launch_tc_impl<128, 3, false>(a, s);
         case 257: return launch_tc_impl<128, 3, true>(a, s);

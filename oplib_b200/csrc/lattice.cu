@@ -164,8 +164,9 @@ int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s) {
         t.K = kslice;
         t.Ahi = a.Ahi + (size_t)i * kslice;
         t.Alo = a.Alo + (size_t)i * kslice;
-        t.Bhi = a.Bhi + (size_t)i * kslice;
-        t.Blo = a.Blo + (size_t)i * kslice;
+        const size_t boff = a.b_kn ? (size_t)i * kslice * a.ldb : (size_t)i * kslice;  // K rows or K columns
+        t.Bhi = a.Bhi + boff;
+        t.Blo = a.Blo + boff;
         if (i > 0) { t.Cin = a.C; t.beta = 1.f; t.cin_fix = nullptr; }
         if (i + 1 < S) t.rowsum = nullptr;
         int r = opb::launch_tc_gemm(t, s);
@@ -183,10 +184,13 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
     // E0 = dt*L in FP32 (FP64 arithmetic), then its splits
     if (L.ell_width > 0) LT(opb::launch_ek_ell(d, L.ell_width, L.gen_cols, L.gen_vals, L.dt, 1, b.X, s));
     else LT(opb::launch_ek_dense(d, L.gen_dense, L.dt, 1, b.X, s));
-    LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s, ss));
+    LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, nullptr, nullptr, d, s, ss));
+    // every squaring and chain product reads its B operand K x N row-major (MN-major):
+    // a squaring's B is E's own row-major parts, a chain product's B the row-major parts of
+    // P1 kept in the B buffers
     opb::TcGemmArgs g{};
-    g.M = d; g.N = d; g.K = d; g.lda = d; g.ldb = d; g.ldc = d; g.f16 = f16 ? 1 : 0;
-    g.Ahi = b.Ahi; g.Alo = b.Alo; g.Bhi = b.Bhi; g.Blo = b.Blo;
+    g.M = d; g.N = d; g.K = d; g.lda = d; g.ldb = d; g.ldc = d; g.f16 = f16 ? 1 : 0; g.b_kn = 1;
+    g.Ahi = b.Ahi; g.Alo = b.Alo; g.Bhi = b.Ahi; g.Blo = b.Alo;
     for (int r = 0; r < L.niter; r++) {
         // D = 2E + E.E in place of E, with FP64 row-sum partials.  From the second level on,
         // X holds the previous product as it left the GEMM, and its renormalisation (b.fix)
@@ -194,17 +198,19 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
         g.C = b.X; g.Cin = b.X; g.alpha = unscale; g.beta = 2.f; g.rowsum = b.part;
         g.cin_fix = r > 0 ? b.fix : nullptr;
         LT(tc_gemm_ksplit(g, s));
-        // the last level emits P1 = I + E and its splits (row-major: A of the first chain and
-        // of pricing; transposed: B of every chain); the others write only the splits and
-        // the row fixes
+        // the last level emits P1 = I + E and its splits (row-major into A: the first
+        // chain's A and pricing's; row-major into B: every chain's B); the others write only
+        // the A splits and the row fixes
         if (r + 1 == L.niter) LT(opb::launch_renorm_to_p(d, b.X, b.part, np, b.Ahi, b.Alo, b.Bhi, b.Blo, s, ss));
-        else LT(opb::launch_renorm(d, b.X, b.part, np, 1, b.Ahi, b.Alo, b.Bhi, b.Blo, s, ss, 0, b.fix));
+        else LT(opb::launch_renorm(d, b.X, b.part, np, 1, b.Ahi, b.Alo, nullptr, nullptr, s, ss, 0, b.fix));
     }
     g.cin_fix = nullptr;
     if (L.niter == 0) {
         LT(opb::launch_add_identity(d, b.X, s));
-        LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, b.Bhi, b.Blo, d, s, ss));
+        LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, nullptr, nullptr, d, s, ss));
+        LT(opb::launch_split(d, d, b.X, d, b.Bhi, b.Blo, nullptr, nullptr, d, s, ss));
     }
+    g.Bhi = b.Bhi; g.Blo = b.Blo;
     if (P_out) return (int)cudaMemcpyAsync(P_out, b.X, sizeof(float) * (size_t)d * d, cudaMemcpyDeviceToDevice, s);
     const int nKp = padded_nk(nK, OPB_BF16X3);
     const float *gs = nullptr;
@@ -219,7 +225,8 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
     pg.alpha = f16 ? 1.f / F16_SCALE : 1.f;  // the payoff scale is undone in the FP64 discount
     for (int m = 1; m <= L.nmat; m++) {
         if (m > 1) {
-            // P_m = P_{m-1} . P1 (A splits hold P_{m-1}), renormalise, split row-major into A
+            // P_m = P_{m-1} . P1 (A splits hold P_{m-1}, B splits P1), renormalise, split
+            // row-major into A
             g.C = b.Pa; g.Cin = nullptr; g.alpha = unscale; g.beta = 0.f; g.rowsum = b.part;
             LT(tc_gemm_ksplit(g, s));
             LT(opb::launch_renorm(d, b.Pa, b.part, np, 0, b.Ahi, b.Alo, nullptr, nullptr, s, ss, 0));

@@ -93,6 +93,7 @@ struct TcGemmArgs {
     // optional, with Cin: per-row (s, inv) of a deferred E-form renormalisation; the
     // epilogue reads Cin[r][c] as (float)((Cin[r][c] - (r == c ? s : 0)) * inv)
     const double2 *cin_fix;
+    int b_kn;  // 1: B parts stored K x N row-major (ldb >= N; read as an MN-major operand)
 };
 int tc_gemm_tile_n(int N);                    // tile width chosen for N (0 if unsupported)
 int tc_gemm_check(const TcGemmArgs &a);       // argument/alignment check, OPB_* code
@@ -115,16 +116,20 @@ struct TcProblem {
     float alpha, beta;
     const double2 *cin_fix;  // as TcGemmArgs::cin_fix
 };
+// Four maps (Ahi, Alo, Bhi, Blo) of one problem: A with 128-row boxes; B K-major (N x K,
+// bn-row boxes) or, with b_kn, K x N row-major read as an MN-major operand (64 x 64
+// boxes, the same maps for every tile width).
 int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo, long long M, long long lda,
                  const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long N, long long ldb, long long K, int bn,
-                 int f16 = 0);
-// work: packed (problem << 16 | m-tile << 8 | n-tile); bn in {64, 128, 256}
+                 int f16 = 0, int b_kn = 0);
+// work: packed (problem << 16 | m-tile << 8 | n-tile); bn in {64, 128, 256}; K-major B
+// (b_kn = 0) only for bn = 64
 int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                           int grid, cudaStream_t s, int f16 = 0);
-// 256 x 256 items (256-row / 256-column units) on 2-CTA clusters; maps with 128-row boxes
-// for A and B (the bn = 128 maps); problems with M, N multiples of 256
+                           int grid, cudaStream_t s, int f16, int b_kn);
+// 256 x 256 items (256-row / 256-column units) on 2-CTA clusters, each CTA loading its
+// 128 rows of A and 128 columns of B; MN-major B maps; problems with M, N multiples of 256
 int launch_tc_gemm_batched_pair(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                                cudaStream_t s, int f16 = 0);
+                                cudaStream_t s, int f16, int b_kn);
 
 // sck.cu
 int launch_sck_rm(int d, int nrows, const float *P, float *C, cudaStream_t s);

@@ -248,12 +248,13 @@ __device__ __forceinline__ void renorm64_sums(RenormSmem &sm, int d, const doubl
 
 // One tile at (r0, c0), using the sums of renorm64_sums; vin holds the tile's values
 // (read back from the staging ring) and the renormalised values are stored back into X
-// unless it is null.  Starts with a barrier, so it can follow renorm64_sums or a previous
+// unless it is null.  B parts (optional) are stored transposed, or with b_rm row-major
+// like the A parts.  Starts with a barrier, so it can follow renorm64_sums or a previous
 // tile of the same rows directly.
 __device__ __forceinline__ void renorm64_apply(RenormSmem &sm, int d, float *__restrict__ X, int mode,
                                                __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
                                                __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo,
-                                               int r0, int c0, float sscale, const float4 (&vin)[4]) {
+                                               int r0, int c0, float sscale, const float4 (&vin)[4], bool b_rm) {
     const int tid = threadIdx.x;
     const bool eform = mode != 2;
     __syncthreads();
@@ -283,8 +284,12 @@ __device__ __forceinline__ void renorm64_apply(RenormSmem &sm, int d, float *__r
             *reinterpret_cast<uint2 *>(Ahi + o) = make_uint2(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]));
             *reinterpret_cast<uint2 *>(Alo + o) = make_uint2(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]));
         }
+        if (Bhi && b_rm) {
+            *reinterpret_cast<uint2 *>(Bhi + o) = make_uint2(pack_bf16(h[0], h[1]), pack_bf16(h[2], h[3]));
+            *reinterpret_cast<uint2 *>(Blo + o) = make_uint2(pack_bf16(l[0], l[1]), pack_bf16(l[2], l[3]));
+        }
     }
-    if (!Bhi) return;
+    if (!Bhi || b_rm) return;
     __syncthreads();
 #pragma unroll
     for (int pass = 0; pass < 4; pass++) {
@@ -307,7 +312,7 @@ __device__ __forceinline__ void renorm64_strip(RenormSmem &sm, RenormRing &rg, i
                                                int nparts, int mode, __nv_bfloat16 *__restrict__ Ahi,
                                                __nv_bfloat16 *__restrict__ Alo, __nv_bfloat16 *__restrict__ Bhi,
                                                __nv_bfloat16 *__restrict__ Blo, int r0, int first, int step,
-                                               float sscale, double2 *__restrict__ fix) {
+                                               float sscale, double2 *__restrict__ fix, bool b_rm) {
     const int nt = d / 64, tid = threadIdx.x;
     const int cnt = first < nt ? (nt - 1 - first) / step + 1 : 0;
 #pragma unroll
@@ -324,24 +329,26 @@ __device__ __forceinline__ void renorm64_strip(RenormSmem &sm, RenormRing &rg, i
         cp_async_wait<RN_RING - 1>();  // this thread's copies of tile k have landed
         const int sl = k % RN_RING;
         const float4 v[4] = {rg.v[sl][0][tid], rg.v[sl][1][tid], rg.v[sl][2][tid], rg.v[sl][3][tid]};
-        renorm64_apply(sm, d, Xout, mode, Ahi, Alo, Bhi, Blo, r0, (first + k * step) * 64, sscale, v);
+        renorm64_apply(sm, d, Xout, mode, Ahi, Alo, Bhi, Blo, r0, (first + k * step) * 64, sscale, v, b_rm);
     }
 }
 
 // Grid (column chunks, d / 64): block (bx, by) renormalises rows 64*by.. over the column
 // tiles bx, bx + gridDim.x, ...  write_x = 0: X is only read (its renormalised values go
 // to the splits alone); fix (optional) receives the per-row (s, inv), written by the
-// blocks of column chunk 0.  Dynamic shared memory RN_SMEM.
+// blocks of column chunk 0; b_rm: B parts row-major (else transposed).  Dynamic shared
+// memory RN_SMEM.
 __global__ void __launch_bounds__(256) k_renorm64(int d, float *__restrict__ X, const double *__restrict__ partial,
                                                   int nparts, int mode, __nv_bfloat16 *__restrict__ Ahi,
                                                   __nv_bfloat16 *__restrict__ Alo, __nv_bfloat16 *__restrict__ Bhi,
                                                   __nv_bfloat16 *__restrict__ Blo, float sscale, int write_x = 1,
-                                                  double2 *__restrict__ fix = nullptr) {
+                                                  double2 *__restrict__ fix = nullptr, int b_rm = 0) {
     extern __shared__ __align__(16) uint8_t rn_smem[];
     RenormSmem &sm = *reinterpret_cast<RenormSmem *>(rn_smem);
     RenormRing &rg = *reinterpret_cast<RenormRing *>(rn_smem + sizeof(RenormSmem));
     renorm64_strip(sm, rg, d, X, write_x ? X : nullptr, partial, nparts, mode, Ahi, Alo, Bhi, Blo,
-                   (int)blockIdx.y * 64, (int)blockIdx.x, (int)gridDim.x, sscale, blockIdx.x == 0 ? fix : nullptr);
+                   (int)blockIdx.y * 64, (int)blockIdx.x, (int)gridDim.x, sscale, blockIdx.x == 0 ? fix : nullptr,
+                   b_rm != 0);
 }
 
 // Column chunks of a k_renorm64 launch: about 8 blocks per SM in total.
@@ -357,7 +364,9 @@ static dim3 renorm64_grid(int d) {
 // column tiles chunk, chunk + renorm_chunks(d), ... of one 64-row strip; nparts of problem
 // i is d_i / parts_div (0 when parts_div == 0: pure split).  X is only read: every later
 // product takes its operands from the splits, and a squaring's Cin gets this
-// renormalisation through the row fixes (mode-0 items, chunk 0).
+// renormalisation through the row fixes (mode-0 items, chunk 0).  Only mode-1 items (P1,
+// the B operand of every chain product) write B parts, row-major; squarings read E's
+// row-major A parts as their B operand.
 __global__ void __launch_bounds__(256) k_renorm64_batched(const RenormProblem *__restrict__ probs,
                                                           const uint32_t *__restrict__ work, int parts_div,
                                                           float sscale) {
@@ -370,8 +379,8 @@ __global__ void __launch_bounds__(256) k_renorm64_batched(const RenormProblem *_
     const int nparts = parts_div > 0 ? pr.d / parts_div : 0;
     const int r0 = (int)((w >> 7) & 127u) * 64, chunk = (int)(w & 127u);
     renorm64_strip(sm, rg, pr.d, pr.X, nullptr, pr.partial, nparts, mode, pr.Ahi, pr.Alo,
-                   mode == 2 ? nullptr : pr.Bhi, mode == 2 ? nullptr : pr.Blo, r0, chunk, renorm_chunks(pr.d),
-                   sscale, mode == 0 && chunk == 0 ? pr.fix : nullptr);
+                   mode == 1 ? pr.Bhi : nullptr, mode == 1 ? pr.Blo : nullptr, r0, chunk, renorm_chunks(pr.d),
+                   sscale, mode == 0 && chunk == 0 ? pr.fix : nullptr, true);
 }
 
 // Opts both renormalisation kernels into RN_SMEM bytes of dynamic shared memory (once per
@@ -537,12 +546,15 @@ int launch_renorm(int d, float *X, const double *partial, int nparts, int eform,
     return (int)cudaGetLastError();
 }
 
-// E-form renorm whose output is P = I + E_new with both splits (the last squaring level).
+// E-form renorm whose output is P = I + E_new, with its splits row-major into both A and B
+// (the last squaring level: P1 is the A of the first chain product and of pricing, and
+// the B of every chain product).
 int launch_renorm_to_p(int d, float *X, const double *partial, int nparts, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
                        __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale) {
     if (d % 64) return OPB_E_UNSUPPORTED;
     if (int r = renorm64_prepare()) return r;
-    k_renorm64<<<renorm64_grid(d), 256, RN_SMEM, s>>>(d, X, partial, nparts, 1, Ahi, Alo, Bhi, Blo, sscale);
+    k_renorm64<<<renorm64_grid(d), 256, RN_SMEM, s>>>(d, X, partial, nparts, 1, Ahi, Alo, Bhi, Blo, sscale, 1,
+                                                      nullptr, 1);
     return (int)cudaGetLastError();
 }
 
