@@ -16,47 +16,74 @@
 
 namespace opb {
 
-// Row-major rows (row y contiguous).  One warp handles 32 rows; tiles of 32x32 are
-// staged through shared memory so global accesses are coalesced while each lane runs
-// the sequential sum of its own row.
+// Row-major rows (row y contiguous).  One warp handles 32 rows (lane = row while summing)
+// in two passes over the row block: the row totals, then the running sums again in the
+// same order, divided and clamped.  Each pass walks 32-column tiles staged through shared
+// memory (coalesced loads and stores), with the next tile's loads in flight while the
+// current one is summed; the outputs are written once.
 __global__ void k_sck_rm(int d, int nrows, const float *__restrict__ P, float *__restrict__ C) {
     __shared__ float t[32][33];
     const int lane = threadIdx.x;
     const int r0 = blockIdx.x * 32;
-    float acc = 0.f;
-    for (int c0 = 0; c0 < d; c0 += 32) {
+    float nxt[32];
+    auto load = [&](int c0) {
+#pragma unroll
         for (int i = 0; i < 32; i++) {
-            int r = r0 + i, c = c0 + lane;
-            t[i][lane] = (r < nrows && c < d) ? P[(long long)r * d + c] : 0.f;
+            const int r = r0 + i, c = c0 + lane;
+            nxt[i] = (r < nrows && c < d) ? P[(long long)r * d + c] : 0.f;
         }
-        __syncwarp();
-        int cmax = min(32, d - c0);
-        for (int j = 0; j < cmax; j++) {
-            float p = t[lane][j];
-            p = p > 0.f ? p : 0.f;
-            acc = (c0 + j == 0) ? p : __fadd_rn(acc, p);
-            t[lane][j] = acc;
+    };
+    float total = 0.f;
+    for (int pass = 0; pass < 2; pass++) {
+        float acc = 0.f;
+        load(0);
+        for (int c0 = 0; c0 < d; c0 += 32) {
+#pragma unroll
+            for (int i = 0; i < 32; i++) t[i][lane] = nxt[i];
+            __syncwarp();
+            if (c0 + 32 < d) load(c0 + 32);
+            const int cmax = min(32, d - c0);
+            if (cmax == 32) {
+                // whole tile: the row's 32 values into registers, the dependent additions,
+                // then the (independent) divisions
+                float pv[32];
+#pragma unroll
+                for (int j = 0; j < 32; j++) pv[j] = t[lane][j];
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    const float p = pv[j] > 0.f ? pv[j] : 0.f;
+                    acc = (c0 + j == 0) ? p : __fadd_rn(acc, p);
+                    pv[j] = acc;
+                }
+                if (pass == 1) {
+#pragma unroll
+                    for (int j = 0; j < 32; j++) {
+                        const float v = __fdiv_rn(pv[j], total);
+                        t[lane][j] = v < 1.0f ? v : 1.0f;
+                    }
+                }
+            } else {
+                for (int j = 0; j < cmax; j++) {
+                    float p = t[lane][j];
+                    p = p > 0.f ? p : 0.f;
+                    acc = (c0 + j == 0) ? p : __fadd_rn(acc, p);
+                    if (pass == 1) {
+                        const float v = __fdiv_rn(acc, total);
+                        t[lane][j] = v < 1.0f ? v : 1.0f;
+                    }
+                }
+            }
+            __syncwarp();
+            if (pass == 1) {
+#pragma unroll
+                for (int i = 0; i < 32; i++) {
+                    const int r = r0 + i, c = c0 + lane;
+                    if (r < nrows && c < d) C[(long long)r * d + c] = t[i][lane];
+                }
+            }
+            __syncwarp();
         }
-        __syncwarp();
-        for (int i = 0; i < 32; i++) {
-            int r = r0 + i, c = c0 + lane;
-            if (r < nrows && c < d) C[(long long)r * d + c] = t[i][lane];
-        }
-        __syncwarp();
-    }
-    // normalise: row total of lane's row is acc
-    __shared__ float tot[32];
-    tot[lane] = acc;
-    __syncwarp();
-    for (int i = 0; i < 32; i++) {
-        int r = r0 + i;
-        if (r >= nrows) break;
-        float s = tot[i];
-        for (int c = lane; c < d; c += 32) {
-            long long o = (long long)r * d + c;
-            float v = __fdiv_rn(C[o], s);
-            C[o] = v < 1.0f ? v : 1.0f;
-        }
+        total = acc;
     }
 }
 
