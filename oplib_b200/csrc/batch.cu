@@ -103,7 +103,7 @@ struct opb_batch_plan {
     // work lists (offsets into `work`)
     std::vector<ListRef> gemm_level[NCFG];
     ListRef gemm_chain[NCFG];
-    std::vector<ListRef> gemm_level_rest[NCFG];  // 256 mixed: the 128 x 128 items
+    std::vector<ListRef> gemm_level_rest[NCFG];  // pair configurations: the 128 x 256 items
     ListRef gemm_chain_rest[NCFG];
     ListRef gemm_price;
     std::vector<ListRef> rn_level;
@@ -196,14 +196,16 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     std::stable_sort(lpt.begin(), lpt.end(), [&](int a, int bb) { return b->d[a] > b->d[bb]; });
     int maxn = 0;
     for (int i = 0; i < n; i++) maxn = std::max(maxn, b->niter[i]);
-    // sel: 0 every lattice, 1 only sizes that are multiples of 256, 2 only the others
+    // sel: 0 every lattice, 1 only sizes that are multiples of 256, 2 only the others.  A
+    // size that is not a multiple of bn gets a last column tile that overhangs the matrix:
+    // its B columns beyond d load as zeros and its output groups beyond d are not stored.
     auto gemm_list = [&](const std::vector<int> &order, int bn, int level, bool chain_or_all, int sel = 0,
                          int tile_m = 128) {
         ListRef r{W.size(), 0};
         for (int i : order) {
             if (!chain_or_all && b->niter[i] <= level) continue;
             if ((sel == 1 && b->d[i] % 256) || (sel == 2 && b->d[i] % 256 == 0)) continue;
-            const int mt = b->d[i] / tile_m, nt = b->d[i] / bn;
+            const int mt = b->d[i] / tile_m, nt = (b->d[i] + bn - 1) / bn;
             for (int a = 0; a < mt; a++)
                 for (int bb = 0; bb < nt; bb++) W.push_back(((uint32_t)i << 16) | ((uint32_t)a << 8) | (uint32_t)bb);
         }
@@ -214,14 +216,15 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     ListRef gch[NCFG], gchr[NCFG];
     for (int cfg = 0; cfg < NCFG; cfg++) {
         const auto &order = (cfg < 2 || cfg == 4 || cfg == 6) ? lpt : nat;
-        if (CFG_BN[cfg] == 256) {
-            const int tm = CFG_PAIR[cfg] ? 256 : 128;
+        if (CFG_PAIR[cfg]) {
+            // 256 x 256 pair items for the multiples of 256, then 128 x 256 items (column
+            // overhang) for the other sizes
             for (int lv = 0; lv < maxn; lv++) {
-                gl[cfg].push_back(gemm_list(order, 256, lv, false, 1, tm));
-                glr[cfg].push_back(gemm_list(order, 128, lv, false, 2));
+                gl[cfg].push_back(gemm_list(order, 256, lv, false, 1, 256));
+                glr[cfg].push_back(gemm_list(order, 256, lv, false, 2, 128));
             }
-            gch[cfg] = gemm_list(order, 256, 0, true, 1, tm);
-            gchr[cfg] = gemm_list(order, 128, 0, true, 2);
+            gch[cfg] = gemm_list(order, 256, 0, true, 1, 256);
+            gchr[cfg] = gemm_list(order, 256, 0, true, 2, 128);
         } else {
             for (int lv = 0; lv < maxn; lv++) {
                 gl[cfg].push_back(gemm_list(order, CFG_BN[cfg], lv, false));
@@ -416,9 +419,10 @@ OPB_API int opb_batch_plan_destroy(opb_batch_plan *P) {
 }
 
 // Selects the launch configuration: cfg 0..7 = (BN 128, longest-K first), (64, longest
-// first), (128, lattice order), (64, lattice order), (256 mixed, longest first), (256
-// mixed, lattice order), (256 pair mixed, longest first), (256 pair mixed, lattice
-// order); grid 0 = one CTA per SM (the pair launches size their own grid).
+// first), (128, lattice order), (64, lattice order), (128 x 256 tiles for every size,
+// longest first), (the same, lattice order), (256 x 256 pair items for the multiples of
+// 256 and 128 x 256 tiles for the rest, longest first), (the same, lattice order); grid 0
+// = one CTA per SM (the pair launches size their own grid).
 OPB_API int opb_batch_set_config(opb_batch_plan *P, int cfg, int grid) {
     OPB_REQUIRE(P, OPB_E_NULL);
     OPB_REQUIRE(cfg >= 0 && cfg < NCFG && grid >= 0, OPB_E_ARG);
@@ -430,7 +434,7 @@ OPB_API int opb_batch_set_config(opb_batch_plan *P, int cfg, int grid) {
 namespace {
 
 // One squaring level (or the chain product) under configuration cfg: one launch, or two
-// for the 256-mixed configurations (256-wide items, then 128 x 128 ones).  maps: the
+// for the pair configurations (256 x 256 pair items, then 128 x 256 ones).  maps: the
 // squaring or the chain table (MN-major B).
 int cfg_gemm(opb_batch_plan *P, int cfg, const CUtensorMap *maps, const opb::TcProblem *probs, const ListRef &l,
              const ListRef &rest, cudaStream_t s) {
@@ -438,7 +442,7 @@ int cfg_gemm(opb_batch_plan *P, int cfg, const CUtensorMap *maps, const opb::TcP
     int r = CFG_PAIR[cfg] ? opb::launch_tc_gemm_batched_pair(maps, probs, P->work + l.off, l.n, s, P->f16, 1)
                           : opb::launch_tc_gemm_batched(bn, maps, probs, P->work + l.off, l.n, P->grid, s, P->f16, 1);
     if (r == 0 && rest.n > 0)
-        r = opb::launch_tc_gemm_batched(128, maps, probs, P->work + rest.off, rest.n, P->grid, s, P->f16, 1);
+        r = opb::launch_tc_gemm_batched(256, maps, probs, P->work + rest.off, rest.n, P->grid, s, P->f16, 1);
     return r;
 }
 
@@ -534,7 +538,7 @@ OPB_API int opb_batch_autotune(opb_batch_plan *P, int reps, float *ms_out, int *
 OPB_API int opb_batch_launches(const opb_batch_plan *P) {
     if (!P) return 0;
     if (!tc_mode_b(P->mode)) return -1;
-    int extra = 0;  // the 256-mixed configurations' second GEMM launch per level / chain
+    int extra = 0;  // the pair configurations' second GEMM launch per level / chain
     for (int lv = 0; lv < P->maxn; lv++) extra += P->gemm_level_rest[P->cfg][lv].n > 0 ? 1 : 0;
     if (P->gemm_chain_rest[P->cfg].n > 0) extra += P->nmat - 1;
     return 3 + 2 * P->maxn + 1 + (P->f16 ? 1 : 0) + 2 * P->nmat + 2 * (P->nmat - 1) + extra;

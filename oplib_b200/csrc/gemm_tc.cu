@@ -550,9 +550,12 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             // the output needs it
             const float *pf = nullptr;
             long long pf_ld = 0;
+            // a batched item's last column tile may overhang its matrix (zero B columns
+            // beyond N): this thread's column group then has nothing to store
+            const bool group_in = !BATCHED || n0 + h * CPT < bt.probs[prob].N;
             if constexpr (EPIMODE == 0) {
                 if constexpr (BATCHED) {
-                    pf = bt.probs[prob].Cin;
+                    pf = group_in ? bt.probs[prob].Cin : nullptr;
                     pf_ld = bt.probs[prob].ldc;
                 } else {
                     pf = p.Cin;
@@ -592,6 +595,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                 }
             }
             if (!ok || *abort_flag) break;
+            if (!group_in) continue;
             float *C;
             const float *Cin;
             long long ldc;
