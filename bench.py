@@ -250,27 +250,28 @@ def run_b200(args, rank, world, local_rank):
         args_g = (d, d, d, Ah.data_ptr(), Al.data_ptr(), d, Ah.data_ptr(), Al.data_ptr(), d, 1.0, X.data_ptr(), 2.0,
                   X.data_ptr(), d, rs.data_ptr())
         for _ in range(3):
-            _lib.call("opb_gemm_bf16x3", *args_g)
+            _lib.call("opb_gemm_bf16x3_kn", *args_g)
         torch.cuda.synchronize()
         n_rep = 20
         e0.record(stream)
         for _ in range(n_rep):
-            _lib.call("opb_gemm_bf16x3", *args_g)
+            _lib.call("opb_gemm_bf16x3_kn", *args_g)
         e1.record(stream)
         torch.cuda.synchronize()
         k_ms = e0.elapsed_time(e1) / n_rep
         mma_flops = 3 * 2.0 * d ** 3
         achieved = mma_flops / (k_ms * 1e-3) / 1e12
         # DRAM bytes (read + write) of one launch of this kernel at d = 6144 from an ncu
-        # capture (dram__bytes_read.sum 936.6 MB + dram__bytes_write.sum 142.1 MB); the
-        # algorithmic traffic is 4 BF16 parts + Cin read, C written = 16 d^2 + 8 d^2 bytes.
-        traffic = 1078.7e6 if d == 6144 else None
+        # capture (dram__bytes_read.sum 940.9 MB + dram__bytes_write.sum 148.3 MB); the
+        # algorithmic traffic is 4 BF16 operand reads + Cin read, C written = 16 d^2 + 8 d^2
+        # bytes.
+        traffic = 1089.2e6 if d == 6144 else None
         kern = {"bound": "tensor", "achieved": round(achieved, 1), "peak": bf16_burst, "unit": "TFLOP/s",
                 "frac": round(achieved / bf16_burst, 4), "frac_of_sustained": round(achieved / bf16_sus, 4),
                 "traffic": traffic, "traffic_unit": "DRAM bytes per launch",
                 "algorithmic_bytes": 24.0 * d * d, "peak_source": f"{src} burst bf16",
-                "kernel": "k_tc_gemm<256,3,pair> (E-form squaring on 2-CTA clusters, cta_group::2, "
-                          f"{d}^3 x 3 BF16 products)",
+                "kernel": "k_tc_gemm<256,3,pair,MN-major B> (E-form squaring on 2-CTA clusters, cta_group::2, "
+                          f"{d}^3 x 3 BF16 products, B = E's own row-major parts)",
                 "avg_launch_ms": round(k_ms, 4), "useful_tflops": round(achieved / 3, 1)}
         del Ah, Al, X, rs
     else:
@@ -1139,7 +1140,8 @@ def run_refbench(args):
 
 
 def run_gemm(args):
-    """The squaring GEMM alone (split-BF16, E-form: C = E.E + 2E in place) at size d."""
+    """The squaring GEMM alone (split-BF16, E-form: C = E.E + 2E in place) at size d, in the
+    solve's form: B is E's own row-major parts, read as an MN-major operand."""
     import torch
     from oplib_b200 import _lib
     from oplib_b200.model import bind_stream
@@ -1155,8 +1157,8 @@ def run_gemm(args):
     a = (d, d, d, Ah.data_ptr(), Al.data_ptr(), d, Ah.data_ptr(), Al.data_ptr(), d, 1.0, X.data_ptr(), 2.0,
          X.data_ptr(), d, rs.data_ptr())
     for _ in range(args.warmup):
-        _lib.call("opb_gemm_bf16x3", *a)
-    ms = _time(lambda: _lib.call("opb_gemm_bf16x3", *a), args.steps, torch.cuda.current_stream(dev), torch)
+        _lib.call("opb_gemm_bf16x3_kn", *a)
+    ms = _time(lambda: _lib.call("opb_gemm_bf16x3_kn", *a), args.steps, torch.cuda.current_stream(dev), torch)
     _, peak, _, src = _peaks()
     tf = 3 * 2.0 * d ** 3 / (ms * 1e-3) / 1e12
     return {"metric": "split-BF16 GEMM MMA TFLOP/s", "value": round(tf, 1), "unit": "TFLOP/s", "n_gpus": 1,

@@ -178,6 +178,12 @@ int opb_gemm_bf16x3(int M, int N, int K, const opb_bf16 *Ahi, const opb_bf16 *Al
                     const opb_bf16 *Bhi, const opb_bf16 *Blo, long long ldb, float alpha, const float *Cin,
                     float beta, float *C, long long ldc, double *rowsum);
 int opb_gemm_bf16x3_nparts(int M, int N);
+/* new: the same product with B given K x N row-major (ldb >= N), read by the tensor cores as
+ * an MN-major operand (the form of the lattice solve's squaring and chain products, whose B
+ * is a row-major split); results identical to opb_gemm_bf16x3 on the transposed B */
+int opb_gemm_bf16x3_kn(int M, int N, int K, const opb_bf16 *Ahi, const opb_bf16 *Alo, long long lda,
+                       const opb_bf16 *Bhi, const opb_bf16 *Blo, long long ldb, float alpha, const float *Cin,
+                       float beta, float *C, long long ldc, double *rowsum);
 /* new (tuning): force the output tile width (64, 128, 256) of single products; 0 = automatic */
 int opb_set_tile_n(int bn);
 /* new: tuning knob, K depth of a pipeline stage of 256-wide tiles: 64 (2 stages, 128-byte

@@ -1106,6 +1106,18 @@ OPB_API int opb_gemm_bf16x3(int M, int N, int K, const __nv_bfloat16 *Ahi, const
     return set_status(launch_tc_gemm(a, stream()));
 }
 
+// The same product with B given K x N row-major (ldb >= N), read as an MN-major operand:
+// the form the lattice solve uses (a squaring's B is E's own row-major parts).  Results are
+// identical to opb_gemm_bf16x3 on the transposed B.
+OPB_API int opb_gemm_bf16x3_kn(int M, int N, int K, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo,
+                               long long lda, const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long ldb,
+                               float alpha, const float *Cin, float beta, float *C, long long ldc, double *rowsum) {
+    TcGemmArgs a{};
+    a.M = M; a.N = N; a.K = K; a.Ahi = Ahi; a.Alo = Alo; a.Bhi = Bhi; a.Blo = Blo; a.lda = lda; a.ldb = ldb;
+    a.C = C; a.ldc = ldc; a.Cin = Cin; a.alpha = alpha; a.beta = beta; a.rowsum = rowsum; a.b_kn = 1;
+    return set_status(launch_tc_gemm(a, stream()));
+}
+
 // The same product with FP16 parts (e.g. of a power-of-two-scaled split; undo the scales
 // through alpha).
 OPB_API int opb_gemm_f16x3(int M, int N, int K, const uint16_t *Ahi, const uint16_t *Alo, long long lda,

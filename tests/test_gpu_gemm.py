@@ -62,6 +62,44 @@ def test_bf16x3_gemm_matches_fp64_of_split(cuda, M, N, K):
         assert np.allclose(parts[t], got[:, t * bn:(t + 1) * bn].sum(axis=1), rtol=1e-12, atol=1e-9)
 
 
+@pytest.mark.parametrize("M,N,K,tile,pair", [(128, 64, 64, 0, 1), (256, 128, 192, 128, 1), (384, 256, 512, 256, 1),
+                                             (512, 512, 1024, 256, 1), (512, 512, 1024, 256, 0),
+                                             (256, 768, 320, 256, 1), (512, 256, 640, 64, 1)])
+def test_kn_operand_matches_transposed_form(cuda, M, N, K, tile, pair):
+    """B given K x N row-major (read as an MN-major operand) gives the same bits as the
+    K-major product on B's transpose, for every tile width and with and without CTA pairs."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(7 * M + N + K)
+    A = rng.random((M, K)).astype(np.float32)
+    B = rng.random((K, N)).astype(np.float32)  # K x N row-major
+    Ah, Al, _, _ = _split_dev(A, cuda)
+    Bh, Bl, _, _ = _split_dev(B, cuda)
+    BhT, BlT = Bh.t().contiguous(), Bl.t().contiguous()
+    Cd = torch.from_numpy(rng.standard_normal((M, N)).astype(np.float32)).to(cuda)
+    outs = []
+    try:
+        assert lib.opb_set_cta_pair(pair) == 0 and lib.opb_set_tile_n(tile) == 0
+        nparts = lib.opb_gemm_bf16x3_nparts(M, N)  # under the forced tile width
+        for kn in (0, 1):
+            Cout = torch.empty_like(Cd)
+            rs = torch.empty(nparts * M, dtype=torch.float64, device=cuda)
+            if kn:
+                st = lib.opb_gemm_bf16x3_kn(M, N, K, Ah.data_ptr(), Al.data_ptr(), K, Bh.data_ptr(), Bl.data_ptr(), N,
+                                            0.5, Cd.data_ptr(), 2.0, Cout.data_ptr(), N, rs.data_ptr())
+            else:
+                st = lib.opb_gemm_bf16x3(M, N, K, Ah.data_ptr(), Al.data_ptr(), K, BhT.data_ptr(), BlT.data_ptr(), K,
+                                         0.5, Cd.data_ptr(), 2.0, Cout.data_ptr(), N, rs.data_ptr())
+            assert st == 0
+            torch.cuda.synchronize()
+            outs.append((Cout.cpu(), rs.cpu()))
+    finally:
+        lib.opb_set_cta_pair(1)
+        lib.opb_set_tile_n(0)
+    assert lib.opb_tc_error() == 0
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+
+
 @pytest.mark.parametrize("M,N,K", [(256, 256, 512), (384, 768, 320), (1024, 512, 2048)])
 def test_stage_depth_gives_identical_results(cuda, M, N, K):
     """256-wide tiles with 32-deep (4-stage, 64-byte swizzle) and 64-deep (2-stage,
