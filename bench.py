@@ -242,20 +242,22 @@ def run_b200(args, rank, world, local_rank):
     # ---- dominant kernel timed alone with CUDA events on the launching stream
     hbm, bf16_burst, bf16_sus, src = _peaks()
     kern = {}
-    if mode == MODES["bf16x3"]:
-        Ah = torch.empty(d, d, dtype=torch.bfloat16, device=dev).normal_(0, 1e-3)
+    if mode in (MODES["bf16x3"], MODES["fp16x3"]):
+        f16 = mode == MODES["fp16x3"]
+        Ah = torch.empty(d, d, dtype=torch.float16 if f16 else torch.bfloat16, device=dev).normal_(0, 1e-3)
         Al = torch.empty_like(Ah).normal_(0, 1e-6)
+        gemm_fn = "opb_gemm_f16x3_kn" if f16 else "opb_gemm_bf16x3_kn"
         X = torch.empty(d, d, dtype=torch.float32, device=dev).normal_()
         rs = torch.empty(lib.opb_gemm_bf16x3_nparts(d, d) * d, dtype=torch.float64, device=dev)
         args_g = (d, d, d, Ah.data_ptr(), Al.data_ptr(), d, Ah.data_ptr(), Al.data_ptr(), d, 1.0, X.data_ptr(), 2.0,
                   X.data_ptr(), d, rs.data_ptr())
         for _ in range(3):
-            _lib.call("opb_gemm_bf16x3_kn", *args_g)
+            _lib.call(gemm_fn, *args_g)
         torch.cuda.synchronize()
         n_rep = 20
         e0.record(stream)
         for _ in range(n_rep):
-            _lib.call("opb_gemm_bf16x3_kn", *args_g)
+            _lib.call(gemm_fn, *args_g)
         e1.record(stream)
         torch.cuda.synchronize()
         k_ms = e0.elapsed_time(e1) / n_rep
@@ -271,7 +273,7 @@ def run_b200(args, rank, world, local_rank):
                 "traffic": traffic, "traffic_unit": "DRAM bytes per launch",
                 "algorithmic_bytes": 24.0 * d * d, "peak_source": f"{src} burst bf16",
                 "kernel": "k_tc_gemm<256,3,pair,MN-major B> (E-form squaring on 2-CTA clusters, cta_group::2, "
-                          f"{d}^3 x 3 BF16 products, B = E's own row-major parts)",
+                          f"{d}^3 x 3 {'FP16' if f16 else 'BF16'} products, B = E's own row-major parts)",
                 "avg_launch_ms": round(k_ms, 4), "useful_tflops": round(achieved / 3, 1)}
         del Ah, Al, X, rs
     else:

@@ -200,6 +200,10 @@ int opb_set_group_m(int gm);
 int opb_gemm_f16x3(int M, int N, int K, const uint16_t *Ahi, const uint16_t *Alo, long long lda, const uint16_t *Bhi,
                    const uint16_t *Blo, long long ldb, float alpha, const float *Cin, float beta, float *C,
                    long long ldc, double *rowsum);
+/* new: the FP16-part product with B given K x N row-major (as opb_gemm_bf16x3_kn) */
+int opb_gemm_f16x3_kn(int M, int N, int K, const uint16_t *Ahi, const uint16_t *Alo, long long lda,
+                      const uint16_t *Bhi, const uint16_t *Blo, long long ldb, float alpha, const float *Cin,
+                      float beta, float *C, long long ldc, double *rowsum);
 /* new: FP64 row renormalisation of a source-major d x d FP32 matrix from row-sum partials
  * partial[p*d + y] (p < nparts), with optional 16-bit splits (A row-major, B transposed);
  * mode 0 E-form, 1 E-form in / P-form out, 2 P-form (no B); f16: FP16 parts of 2^15-scaled

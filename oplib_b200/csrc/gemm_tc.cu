@@ -1132,6 +1132,20 @@ OPB_API int opb_gemm_f16x3(int M, int N, int K, const uint16_t *Ahi, const uint1
     return set_status(launch_tc_gemm(a, stream()));
 }
 
+// The FP16-part product with B given K x N row-major (as opb_gemm_bf16x3_kn).
+OPB_API int opb_gemm_f16x3_kn(int M, int N, int K, const uint16_t *Ahi, const uint16_t *Alo, long long lda,
+                              const uint16_t *Bhi, const uint16_t *Blo, long long ldb, float alpha, const float *Cin,
+                              float beta, float *C, long long ldc, double *rowsum) {
+    TcGemmArgs a{};
+    a.M = M; a.N = N; a.K = K;
+    a.Ahi = reinterpret_cast<const __nv_bfloat16 *>(Ahi); a.Alo = reinterpret_cast<const __nv_bfloat16 *>(Alo);
+    a.Bhi = reinterpret_cast<const __nv_bfloat16 *>(Bhi); a.Blo = reinterpret_cast<const __nv_bfloat16 *>(Blo);
+    a.lda = lda; a.ldb = ldb; a.C = C; a.ldc = ldc; a.Cin = Cin; a.alpha = alpha; a.beta = beta; a.rowsum = rowsum;
+    a.f16 = 1;
+    a.b_kn = 1;
+    return set_status(launch_tc_gemm(a, stream()));
+}
+
 OPB_API int opb_gemm_bf16x3_nparts(int M, int N) { return tc_gemm_nparts(M, N); }
 
 // Tuning knob: force the output tile width (64, 128 or 256) of single products; 0 = automatic.
