@@ -186,8 +186,8 @@ int opb_gemm_bf16x3_kn(int M, int N, int K, const opb_bf16 *Ahi, const opb_bf16 
                        float beta, float *C, long long ldc, double *rowsum);
 /* new (tuning): force the output tile width (64, 128, 256) of single products; 0 = automatic */
 int opb_set_tile_n(int bn);
-/* new: tuning knob, K depth of a pipeline stage of 256-wide tiles: 64 (2 stages, 128-byte
- * swizzle; default) or 32 (4 stages, 64-byte swizzle); results are identical */
+/* new: tuning knob, K depth of a pipeline stage of 256-wide tiles: 64 (default) or 32 (twice
+ * the stages of half the size; 64-byte swizzle for A); results are identical */
 int opb_set_stage_k(int bk);
 /* new: tuning knob, 256 x 256 output tiles on 2-CTA clusters (cta_group::2 MMAs over both
  * CTAs' shared memory) for products with M % 256 == 0: 1 = on (default), 0 = off;

@@ -111,12 +111,14 @@ __device__ __forceinline__ uint64_t umma_desc_sw(uint32_t saddr) {
 }
 
 // MN-major 128-byte-swizzled descriptor for a B tile stored K x N (N contiguous) as
-// 64-column boxes of BK = 64 rows: each box is 64 rows of 128 bytes (8-row swizzle atoms
-// 1024 bytes apart: SBO), and the boxes along N are 8192 bytes apart (LBO).
+// 64-column boxes of BK rows: each box is BK rows of 128 bytes (8-row swizzle atoms 1024
+// bytes apart: SBO), and the boxes along N are BK * 128 bytes apart (LBO).
+template <int BK>
 __device__ __forceinline__ uint64_t umma_desc_mn(uint32_t saddr) {
+    static_assert(BK == 64 || BK == 32, "BK");
     uint64_t d = 0;
     d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
-    d |= (uint64_t)(8192 >> 4) << 16;  // LBO: next 64 columns
+    d |= (uint64_t)((BK * 128) >> 4) << 16;  // LBO: next 64 columns
     d |= (uint64_t)(1024 >> 4) << 32;  // SBO: next 8 rows of K
     d |= (uint64_t)1 << 46;            // version
     d |= (uint64_t)2 << 61;            // SWIZZLE_128B
@@ -306,7 +308,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
     using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>;
     constexpr int EPI = Cfg::EPI_WARPS;
     constexpr int CPT = Cfg::CPT;
-    static_assert(!BMN || (BK == 64 && NPROD == 3 && Cfg::B_ROWS % 64 == 0), "MN-major B: split products, BK 64");
+    static_assert(!BMN || (NPROD == 3 && Cfg::B_ROWS % 64 == 0), "MN-major B: split products");
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -492,8 +494,8 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                         const uint64_t dAl = umma_desc_sw<BK>(st + Cfg::A_BYTES);
                         const uint32_t sBh = st + Cfg::NPARTS * Cfg::A_BYTES;
                         const uint32_t sBl = st + 2 * Cfg::A_BYTES + Cfg::B_BYTES;
-                        const uint64_t dBh = BMN ? umma_desc_mn(sBh) : umma_desc_sw<BK>(sBh);
-                        const uint64_t dBl = BMN ? umma_desc_mn(sBl) : umma_desc_sw<BK>(sBl);
+                        const uint64_t dBh = BMN ? umma_desc_mn<BK>(sBh) : umma_desc_sw<BK>(sBh);
+                        const uint64_t dBl = BMN ? umma_desc_mn<BK>(sBl) : umma_desc_sw<BK>(sBl);
 #pragma unroll
                         for (int k16 = 0; k16 < BK / 16; k16++) {
                             const uint64_t adv = (uint64_t)((k16 * 32) >> 4);  // +32 bytes along K
@@ -775,13 +777,14 @@ static int make_map(CUtensorMap *m, const void *ptr, long long rows, long long K
 }
 
 // K x N bf16 row-major matrix (leading dimension ld elements) read as an MN-major B
-// operand: box = 64 columns x 64 rows, 128-byte swizzle.
-static int make_map_mn(CUtensorMap *m, const void *ptr, long long K, long long N, long long ld, int f16 = 0) {
+// operand: box = 64 columns x bk rows, 128-byte swizzle.
+static int make_map_mn(CUtensorMap *m, const void *ptr, long long K, long long N, long long ld, int f16 = 0,
+                       int bk = TC_BK) {
     auto enc = get_encode();
     if (!enc) return OPB_E_UNSUPPORTED;
     cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)K};
     cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
-    cuuint32_t box[2] = {64, 64};
+    cuuint32_t box[2] = {64, (cuuint32_t)bk};
     cuuint32_t es[2] = {1, 1};
     CUresult r = enc(m, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
                      const_cast<void *>(ptr), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -793,8 +796,8 @@ static int make_map_mn(CUtensorMap *m, const void *ptr, long long K, long long N
 static int make_b_maps(CUtensorMap *hi, CUtensorMap *lo, const TcGemmArgs &a, int brows, int f16, int bk) {
     int r;
     if (a.b_kn) {
-        if ((r = make_map_mn(hi, a.Bhi, a.K, a.N, a.ldb, f16)) != OPB_OK) return r;
-        return make_map_mn(lo, a.Blo, a.K, a.N, a.ldb, f16);
+        if ((r = make_map_mn(hi, a.Bhi, a.K, a.N, a.ldb, f16, bk)) != OPB_OK) return r;
+        return make_map_mn(lo, a.Blo, a.K, a.N, a.ldb, f16, bk);
     }
     if ((r = make_map(hi, a.Bhi, a.N, a.K, a.ldb, brows, f16, bk)) != OPB_OK) return r;
     return make_map(lo, a.Blo, a.N, a.K, a.ldb, brows, f16, bk);
@@ -884,18 +887,18 @@ static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
 // 256 x 256 output tiles on 2-CTA clusters: each CTA loads its 128 rows of A and 128 rows
 // of B, the even CTA issues cta_group::2 MMAs over both CTAs' shared memory.  The grid is
 // as many clusters as can be resident at once (at most one per SM pair).
-template <bool F16, bool BMN>
+template <bool F16, bool BMN, int STAGES = 3, int BK = TC_BK>
 static int launch_tc_pair(const TcGemmArgs &a, cudaStream_t s) {
-    constexpr int BN = 256, STAGES = 3;
-    using Cfg = TcCfg<BN, STAGES, 3, TC_BK, true>;
-    auto kern = k_tc_gemm<BN, STAGES, false, F16, 3, 0, TC_BK, true, BMN>;
-    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, TC_BK, true, BMN>();
+    constexpr int BN = 256;
+    using Cfg = TcCfg<BN, STAGES, 3, BK, true>;
+    auto kern = k_tc_gemm<BN, STAGES, false, F16, 3, 0, BK, true, BMN>;
+    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, BK, true, BMN>();
     if (e0) return e0;
     CUtensorMap mAh, mAl, mBh, mBl;
     int r;
-    if ((r = make_map(&mAh, a.Ahi, a.M, a.K, a.lda, TC_BM, F16)) != OPB_OK) return r;
-    if ((r = make_map(&mAl, a.Alo, a.M, a.K, a.lda, TC_BM, F16)) != OPB_OK) return r;
-    if ((r = make_b_maps(&mBh, &mBl, a, BN / 2, F16, TC_BK)) != OPB_OK) return r;
+    if ((r = make_map(&mAh, a.Ahi, a.M, a.K, a.lda, TC_BM, F16, BK)) != OPB_OK) return r;
+    if ((r = make_map(&mAl, a.Alo, a.M, a.K, a.lda, TC_BM, F16, BK)) != OPB_OK) return r;
+    if ((r = make_b_maps(&mBh, &mBl, a, BN / 2, F16, BK)) != OPB_OK) return r;
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
     p.group_m = g_group_m;
     p.cin_fix = a.cin_fix;
@@ -1068,8 +1071,14 @@ int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
     const bool pair = g_pair && a.M % (2 * TC_BM) == 0;
     if (a.b_kn) {  // MN-major B (K x N): BK = 64 only
         switch (tile_for(a.M, a.N) * 2 + (a.f16 ? 1 : 0)) {
-            case 512: return pair ? launch_tc_pair<false, true>(a, s) : launch_tc_impl<256, 2, false, 64, true>(a, s);
-            case 513: return pair ? launch_tc_pair<true, true>(a, s) : launch_tc_impl<256, 2, true, 64, true>(a, s);
+            case 512:
+                if (pair)
+                    return g_bk256 == 32 ? launch_tc_pair<false, true, 6, 32>(a, s) : launch_tc_pair<false, true>(a, s);
+                return launch_tc_impl<256, 2, false, 64, true>(a, s);
+            case 513:
+                if (pair)
+                    return g_bk256 == 32 ? launch_tc_pair<true, true, 6, 32>(a, s) : launch_tc_pair<true, true>(a, s);
+                return launch_tc_impl<256, 2, true, 64, true>(a, s);
             case 256: return launch_tc_impl<128, 3, false, 64, true>(a, s);
             case 257: return launch_tc_impl<128, 3, true, 64, true>(a, s);
             case 128: return launch_tc_impl<64, 4, false, 64, true>(a, s);
@@ -1155,8 +1164,10 @@ OPB_API int opb_set_tile_n(int bn) {
     return set_status(OPB_OK);
 }
 
-// Tuning knob: K depth of a pipeline stage of 256-wide tiles: 64 (2 stages of 96 KB,
-// 128-byte swizzle, the default) or 32 (4 stages of 48 KB, 64-byte swizzle).
+// Tuning knob: K depth of a pipeline stage of 256-wide tiles: 64 (the default: 2 stages of
+// 96 KB for one CTA, 3 of 64 KB per CTA of a pair) or 32 (4 stages of 48 KB, 6 of 32 KB for
+// a pair with B given K x N; A in 64-byte swizzle).  Results are identical; at d = 6144
+// the 64-deep stages are faster for both kernels.
 OPB_API int opb_set_stage_k(int bk) {
     OPB_REQUIRE(bk == 32 || bk == 64, OPB_E_ARG);
     g_bk256 = bk;

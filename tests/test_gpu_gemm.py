@@ -133,6 +133,37 @@ def test_stage_depth_gives_identical_results(cuda, M, N, K):
     assert lib.opb_set_stage_k(48) != 0
 
 
+@pytest.mark.parametrize("M,N,K", [(256, 256, 512), (512, 768, 320)])
+def test_pair_stage_depth_gives_identical_results(cuda, M, N, K):
+    """The CTA-pair kernel with B given K x N row-major: 32-deep (6 stages) and 64-deep (3
+    stages) pipeline stages give the same bits."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(M * K)
+    A = rng.random((M, K)).astype(np.float32)
+    B = rng.random((K, N)).astype(np.float32)
+    Ah, Al, _, _ = _split_dev(A, cuda)
+    Bh, Bl, _, _ = _split_dev(B, cuda)
+    Cd = torch.from_numpy(rng.standard_normal((M, N)).astype(np.float32)).to(cuda)
+    outs = []
+    try:
+        assert lib.opb_set_tile_n(256) == 0
+        nparts = lib.opb_gemm_bf16x3_nparts(M, N)
+        for bk in (32, 64):
+            assert lib.opb_set_stage_k(bk) == 0
+            Cout = torch.empty_like(Cd)
+            rs = torch.empty(nparts * M, dtype=torch.float64, device=cuda)
+            assert lib.opb_gemm_bf16x3_kn(M, N, K, Ah.data_ptr(), Al.data_ptr(), K, Bh.data_ptr(), Bl.data_ptr(), N,
+                                          1.0, Cd.data_ptr(), 2.0, Cout.data_ptr(), N, rs.data_ptr()) == 0
+            torch.cuda.synchronize()
+            outs.append((Cout.cpu(), rs.cpu()))
+    finally:
+        lib.opb_set_stage_k(64)
+        lib.opb_set_tile_n(0)
+    assert lib.opb_tc_error() == 0
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+
+
 @pytest.mark.parametrize("M,N,K", [(256, 256, 128), (512, 256, 512), (768, 512, 320), (1024, 1024, 2048)])
 def test_cta_pair_gemm_matches_fp64_of_split(cuda, M, N, K):
     """256 x 256 tiles on 2-CTA clusters (cta_group::2): within the same FP32 bound as the
@@ -198,6 +229,14 @@ def test_f16x3_gemm_matches_fp64_of_split(cuda, M, N, K):
     exact = A.astype(np.float64) @ B.astype(np.float64).T
     got = C.cpu().numpy().astype(np.float64)
     assert np.abs(got - ref).max() <= (3 * K / 16 + 8) * 2.0 ** -24 * exact.max()
+    # the same parts with B given K x N row-major: identical bits
+    C2 = torch.empty_like(C)
+    assert lib.opb_gemm_f16x3_kn(M, N, K, _f16_dev(ah, cuda).data_ptr(), _f16_dev(al, cuda).data_ptr(), K,
+                                 _f16_dev(bh.T, cuda).data_ptr(), _f16_dev(bl.T, cuda).data_ptr(), N, alpha, None,
+                                 0.0, C2.data_ptr(), N, None) == 0
+    torch.cuda.synchronize()
+    assert lib.opb_tc_error() == 0
+    assert torch.equal(C, C2)
     # 22-bit parts: the split product is within ~1e-6 relative of the exact product
     assert np.abs(ref - exact).max() <= 2e-6 * exact.max()
 
