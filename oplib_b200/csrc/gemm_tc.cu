@@ -5,8 +5,10 @@
 // A = Ahi + Alo and B = Bhi + Blo are FP32 matrices split into two BF16 parts
 // (hi = bf16(a), lo = bf16(a - hi)); the three products carry about 16 mantissa bits per
 // operand and accumulate in FP32 in tensor memory.  This replaces the FP32 SIMT squaring
-// of oplib/opcuda/ssqmm.cu:119-179 on the lattice path.  Operands are K-major (rows of A
-// and rows of B^T contiguous), M % 128 == 0, N % BN == 0, K % 64 == 0.
+// of oplib/opcuda/ssqmm.cu:119-179 on the lattice path.  A is K-major (rows contiguous);
+// B is K-major (rows of B^T contiguous) or, for the lattice's squaring and chain
+// products, K x N row-major and read as an MN-major operand (64-column TMA boxes), so a
+// squaring reads E's own row-major parts as B.  M % 128 == 0, N % BN == 0, K % 64 == 0.
 //
 // Structure (persistent: one CTA per SM over 128 x BN output tiles):
 //   TMA warp, one lane : 4 tiled bulk-tensor loads per K-block (Ahi, Alo, Bhi, Blo; 128B
@@ -18,11 +20,13 @@
 //                        each stage and hands each finished chunk to the epilogue.
 //   epilogue warps     : (4 lane quadrants x BN/128 column groups) tcgen05.ld of each
 //                        finished chunk into FP32 round-to-nearest register sums; after a
-//                        tile's last chunk, the alpha/beta update, FP32 stores and FP64
-//                        row sums of the stored values (rowsum[group * M + row], one per
-//                        128 columns, used by the row renormalisation).
+//                        tile's last chunk, the alpha/beta update (with the deferred
+//                        renormalisation of Cin, when given), FP32 stores staged through
+//                        shared memory in 32 x 32 blocks, and FP64 row sums of the
+//                        stored values (rowsum[group * M + row], one per 128 columns,
+//                        used by the row renormalisation).
 // CTA pairs (the default for M % 256 == 0 with 256-wide tiles): a 2-CTA cluster owns a
-// 256 x 256 output tile; each CTA loads its own 128 rows of A and 128 rows of B (3-stage
+// 256 x 256 output tile; each CTA loads its own 128 rows of A and 128 columns of B (3-stage
 // 64 KB ring per CTA, both CTAs' copies counted on the even CTA's full barrier), the even
 // CTA's MMA lane issues tcgen05.mma.cta_group::2 (M = 256) over both CTAs' shared memory
 // into each CTA's own TMEM, and its commits arrive on both CTAs' barriers.  Operand bytes

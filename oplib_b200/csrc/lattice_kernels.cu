@@ -10,10 +10,12 @@
 //              conservation after each squaring; no reference counterpart).  In E-form
 //              the identity is carried implicitly: with D = 2E + E.E and s = 1 + sum(D_y.),
 //              E_new[y,z] = (D[y,z] - [z==y]*sum(D_y.)) / s_y, which equals
-//              (I + D)/s - I exactly.
+//              (I + D)/s - I exactly.  Inside a lattice solve the FP32 matrix is not
+//              written back at intermediate levels: the per-row (sum, 1/s) go to a fix
+//              array that the next squaring's epilogue applies to its Cin.
 //   split    : a = hi + lo with hi = bf16(a), lo = bf16(a - hi), written row-major (the
-//              K-major A operand) and transposed (the K-major B operand) for the
-//              tensor-core GEMM.
+//              K-major A operand, and the MN-major B operand of the lattice products);
+//              the public forms can also write the transpose (a K-major B operand).
 //   payoff / discount : call payoffs G[z,k] = (x_z - K_k)^+ and the FP64 discounting of
 //              the backward-induction result.
 #include <cuda_bf16.h>
