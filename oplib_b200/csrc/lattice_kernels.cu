@@ -251,15 +251,17 @@ __device__ __forceinline__ void renorm64_sums(RenormSmem &sm, int d, const doubl
 // One tile at (r0, c0), using the sums of renorm64_sums; vin holds the tile's values
 // (read back from the staging ring) and the renormalised values are stored back into X
 // unless it is null.  B parts (optional) are stored transposed, or with b_rm row-major
-// like the A parts.  Starts with a barrier, so it can follow renorm64_sums or a previous
-// tile of the same rows directly.
+// like the A parts.  The sums must be visible to the block (a barrier after
+// renorm64_sums); the transposed form starts with its own barrier, for the shared tile
+// of the previous call.
 __device__ __forceinline__ void renorm64_apply(RenormSmem &sm, int d, float *__restrict__ X, int mode,
                                                __nv_bfloat16 *__restrict__ Ahi, __nv_bfloat16 *__restrict__ Alo,
                                                __nv_bfloat16 *__restrict__ Bhi, __nv_bfloat16 *__restrict__ Blo,
                                                int r0, int c0, float sscale, const float4 (&vin)[4], bool b_rm) {
     const int tid = threadIdx.x;
     const bool eform = mode != 2;
-    __syncthreads();
+    const bool transposed = Bhi && !b_rm;
+    if (transposed) __syncthreads();
     const int lc = (tid & 15) * 4;
 #pragma unroll
     for (int pass = 0; pass < 4; pass++) {
@@ -279,7 +281,7 @@ __device__ __forceinline__ void renorm64_apply(RenormSmem &sm, int d, float *__r
             if (mode == 1 && diag) x += 1.0;
             f[j] = (float)x;
             split2(f[j], h[j], l[j], sscale);
-            sm.t[lr][lc + j] = pack_bf16(h[j], l[j]);
+            if (transposed) sm.t[lr][lc + j] = pack_bf16(h[j], l[j]);
         }
         if (X) *reinterpret_cast<float4 *>(X + o) = make_float4(f[0], f[1], f[2], f[3]);
         if (Ahi) {
@@ -323,6 +325,7 @@ __device__ __forceinline__ void renorm64_strip(RenormSmem &sm, RenormRing &rg, i
         cp_async_commit();  // possibly empty: every iteration commits exactly one group
     }
     renorm64_sums(sm, d, partial, nparts, mode, r0, fix);
+    __syncthreads();  // the row sums are visible to every thread
     for (int k = 0; k < cnt; k++) {
         // the slot refilled here was read (and its values used) in iteration k - 1
         const int kn = k + RN_RING - 1;
