@@ -236,6 +236,15 @@ typedef struct opb_lattice_desc {
 unsigned long long opb_lattice_workspace_size(int d, int nK, int mode);
 int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
                       double *quotes, double *V_all);
+/* new (extension; the reference ships the induction kernels sgemv3/sgemv4 but no pricer on
+ * them): calls (put = 0) or puts (put = 1) of final maturity T = nmat * period by backward
+ * induction on P1 = P(period): V_nmat = e(x), V_m = exp(-rate*period) * P1 . V_{m+1},
+ * knocked out where x <= barrier (barrier > 0) and, with exercise = 1, floored by the
+ * exercise value, at every T_m, m = 1..nmat-1 (Bermudan / discretely monitored
+ * down-and-out); exercise = 0 and barrier = 0 give the European value at T.  quotes:
+ * device [nK] FP64 values at y0.  Split modes only; workspace as for opb_lattice_solve. */
+int opb_lattice_bermudan(const opb_lattice_desc *L, int mode, int put, int exercise, double barrier,
+                         void *workspace, unsigned long long ws_bytes, double *quotes);
 /* new: transition kernel P(period) only (device d x d FP32, source-major), e.g. the MC step
  * kernel; nmat, nK and strikes of L are ignored */
 int opb_lattice_kernel(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,

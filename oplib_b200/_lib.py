@@ -106,6 +106,7 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_lattice_workspace_size": (ull, [i32, i32, i32]),
     "opb_lattice_solve": (i32, [C.POINTER(LatticeDesc), i32, vp, ull, vp, vp]),
     "opb_lattice_kernel": (i32, [C.POINTER(LatticeDesc), i32, vp, ull, vp]),
+    "opb_lattice_bermudan": (i32, [C.POINTER(LatticeDesc), i32, i32, i32, f64, vp, ull, vp]),
     "opb_set_ksplit": (i32, [i32]),
     # batched lattices
     "opb_batch_workspace_size": (ull, [vp, i32]),

@@ -70,6 +70,7 @@ struct Bufs {
     __nv_bfloat16 *Ahi, *Alo, *Bhi, *Blo, *GThi, *GTlo;
     double *part;
     double2 *fix;  // per-row (s, inv) of the last E-form renormalisation (deferred into the next Cin)
+    double *Vd;    // FP64 option values of the backward induction, d x nKp
 };
 
 inline int padded_nk(int nK, int mode) { return tc_mode(mode) ? (nK + 63) / 64 * 64 : nK; }
@@ -93,6 +94,7 @@ Bufs carve(Ws &w, int d, int nK, int mode) {
         int np = opb::tc_gemm_nparts(d, d);
         b.part = w.take<double>((size_t)(np > 0 ? np : 1) * d);
         b.fix = w.take<double2>((size_t)d);
+        b.Vd = w.take<double>((size_t)d * nK);
     } else {
         b.G = w.take<float>((size_t)d * nK);
         b.part = w.take<double>((size_t)d);
@@ -175,9 +177,11 @@ int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s) {
     return 0;
 }
 
-int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, cudaStream_t s, float *P_out,
-             bool f16) {
-    const int d = L.d, nK = L.nK;
+// E0 = dt*L, niter split squarings with renormalisation: P1 = P(period) as row-major splits
+// in both the A and the B buffers and as FP32 in X.  g returns the product arguments of
+// the squarings (B read K x N row-major), with B set to P1's B parts.
+int square_tc(const opb_lattice_desc &L, Bufs &b, cudaStream_t s, bool f16, opb::TcGemmArgs &g) {
+    const int d = L.d;
     const int np = opb::tc_gemm_nparts(d, d);
     const float ss = f16 ? F16_SCALE : 0.f;                    // split scale of E / P parts
     const float unscale = f16 ? 1.f / (F16_SCALE * F16_SCALE) : 1.f;
@@ -188,7 +192,7 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
     // every squaring and chain product reads its B operand K x N row-major (MN-major):
     // a squaring's B is E's own row-major parts, a chain product's B the row-major parts of
     // P1 kept in the B buffers
-    opb::TcGemmArgs g{};
+    g = opb::TcGemmArgs{};
     g.M = d; g.N = d; g.K = d; g.lda = d; g.ldb = d; g.ldc = d; g.f16 = f16 ? 1 : 0; g.b_kn = 1;
     g.Ahi = b.Ahi; g.Alo = b.Alo; g.Bhi = b.Ahi; g.Blo = b.Alo;
     for (int r = 0; r < L.niter; r++) {
@@ -211,6 +215,17 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
         LT(opb::launch_split(d, d, b.X, d, b.Bhi, b.Blo, nullptr, nullptr, d, s, ss));
     }
     g.Bhi = b.Bhi; g.Blo = b.Blo;
+    return 0;
+}
+
+int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, cudaStream_t s, float *P_out,
+             bool f16) {
+    const int d = L.d, nK = L.nK;
+    const int np = opb::tc_gemm_nparts(d, d);
+    const float ss = f16 ? F16_SCALE : 0.f;                    // split scale of E / P parts
+    const float unscale = f16 ? 1.f / (F16_SCALE * F16_SCALE) : 1.f;
+    opb::TcGemmArgs g{};
+    LT(square_tc(L, b, s, f16, g));
     if (P_out) return (int)cudaMemcpyAsync(P_out, b.X, sizeof(float) * (size_t)d * d, cudaMemcpyDeviceToDevice, s);
     const int nKp = padded_nk(nK, OPB_BF16X3);
     const float *gs = nullptr;
@@ -235,6 +250,37 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
         const double disc = std::exp(-L.rate * L.period * m);
         LT(opb::launch_discount(d, nK, nKp, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d * nK : nullptr, L.y0,
                                 quotes + (size_t)(m - 1) * nK, s, gs));
+    }
+    return 0;
+}
+
+// Backward induction on the period kernel: V_nmat = e(x), then for m = nmat-1 .. 0
+// V_m = e^{-r period} P1 . V_{m+1}, knocked out below the barrier at the dates m >= 1 and,
+// with exercise, floored by the exercise value there.  Each product runs on the tensor
+// cores with V's split parts as a K x N row-major B operand.
+int bermudan_tc(const opb_lattice_desc &L, Bufs &b, int put, int exercise, double barrier, double *quotes,
+                cudaStream_t s, bool f16) {
+    const int d = L.d, nK = L.nK, nKp = padded_nk(nK, OPB_BF16X3);
+    opb::TcGemmArgs g{};
+    LT(square_tc(L, b, s, f16, g));
+    const float *gs = nullptr;
+    if (f16) {
+        LT(opb::launch_berm_scale(d, L.x, nK, L.strikes, put, b.gscale, s));
+        gs = b.gscale;
+    }
+    // V's parts live in the payoff-part buffers (d x nKp each)
+    LT(opb::launch_berm_init(d, nK, nKp, L.x, L.strikes, put, barrier, b.Vd, b.GThi, b.GTlo, gs, s));
+    opb::TcGemmArgs pg{};
+    pg.M = d; pg.N = nKp; pg.K = d; pg.lda = d; pg.ldb = nKp; pg.ldc = nKp; pg.f16 = f16 ? 1 : 0; pg.b_kn = 1;
+    pg.Ahi = b.Ahi; pg.Alo = b.Alo; pg.Bhi = b.GThi; pg.Blo = b.GTlo; pg.C = b.V; pg.beta = 0.f;
+    pg.alpha = f16 ? 1.f / F16_SCALE : 1.f;  // the P1 part scale; V's scale is undone in the step
+    const double disc = std::exp(-L.rate * L.period);
+    for (int m = L.nmat - 1; m >= 0; m--) {
+        LT(tc_gemm_ksplit(pg, s));
+        const bool last = m == 0;
+        LT(opb::launch_berm_step(d, nK, nKp, b.V, disc, L.x, L.strikes, put, last ? 0.0 : barrier,
+                                 last ? 0 : exercise, b.Vd, last ? nullptr : b.GThi, last ? nullptr : b.GTlo, gs,
+                                 L.y0, last ? quotes : nullptr, s));
     }
     return 0;
 }
@@ -292,6 +338,30 @@ OPB_API int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspa
     int r = tc_mode(mode) ? solve_tc(*L, b, quotes, V_all, s, nullptr, mode == OPB_FP16X3)
                           : solve_fp32(*L, mode, b, quotes, V_all, s, nullptr);
     return opb::set_status(r);
+}
+
+// Bermudan or barrier options on one lattice by backward induction on the period kernel
+// P1 = P(period) (an extension: the reference ships the induction kernels, sgemv3/sgemv4,
+// but no pricer on them).  Calls (put = 0) or puts (put = 1) with strikes L->strikes and
+// final maturity T = nmat * period; exercise = 1: exercisable at T_m = m * period for m =
+// 1..nmat (Bermudan), 0: at T only; barrier > 0: knocked out when the spot is at or below
+// the barrier on any date T_m (m >= 1).  exercise = 0 with barrier = 0 gives the European
+// value at T.  quotes: device [nK] FP64, the values at state y0.  Split modes only (the
+// induction products run on the tensor cores); workspace as for opb_lattice_solve.
+OPB_API int opb_lattice_bermudan(const opb_lattice_desc *L, int mode, int put, int exercise, double barrier,
+                                 void *workspace, unsigned long long ws_bytes, double *quotes) {
+    int c = check_desc(L, mode);
+    if (c == OPB_OK && !quotes) c = OPB_E_NULL;
+    if (c == OPB_OK && !tc_mode(mode)) c = OPB_E_UNSUPPORTED;
+    if (c == OPB_OK && (put < 0 || put > 1 || exercise < 0 || exercise > 1 || !(barrier >= 0.0))) c = OPB_E_ARG;
+    if (c != OPB_OK) return opb::set_status(c);
+    OPB_REQUIRE(workspace, OPB_E_NULL);
+    OPB_REQUIRE(ws_bytes >= opb_lattice_workspace_size(L->d, L->nK, mode), OPB_E_ARG);
+    Ws w{reinterpret_cast<char *>(workspace), 0};
+    size_t off = (256 - (reinterpret_cast<uintptr_t>(workspace) & 255)) & 255;
+    w.p += off;
+    Bufs b = carve(w, L->d, L->nK, mode);
+    return opb::set_status(bermudan_tc(*L, b, put, exercise, barrier, quotes, opb::stream(), mode == OPB_FP16X3));
 }
 
 // Transition kernel only: P_out (device, d x d FP32, source-major) = P(period) after

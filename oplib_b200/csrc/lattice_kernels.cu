@@ -502,6 +502,98 @@ __global__ void k_discount(int d, int nK, int ldk, const float *__restrict__ V32
     if (quotes && y == y0) quotes[k] = v;
 }
 
+// ------------------------------------------------------------------ backward induction
+// Bermudan / barrier induction on the period kernel (an extension: the reference exposes
+// only the multi-vector GEMV kernels, oplib/opcuda/sgemv3.cu and sgemv4.cu, for it).
+// Values V[z, k] are FP64, d x ldk row-major; columns nK..ldk-1 are padding (zero).  The
+// exercise value is (x_z - K_k)^+ for calls, (K_k - x_z)^+ for puts; with barrier > 0 a
+// state with x_z <= barrier is knocked out (value 0) at every monitoring date.
+
+__device__ __forceinline__ double berm_exercise(double x, double K, int put) {
+    const double g = put ? K - x : x - K;
+    return g > 0.0 ? g : 0.0;
+}
+
+// Power-of-two FP16 split scale of the option values: every value is bounded by the
+// largest exercise value (max x - min K for calls, max K - min x for puts).
+__global__ void k_berm_scale(int d, const double *__restrict__ x, int nK, const double *__restrict__ K, int put,
+                             float *__restrict__ out) {
+    __shared__ double s0[256], s1[256];
+    double a = -1e300, b = 1e300;  // calls: max x, min K; puts: max K, min x
+    for (int i = threadIdx.x; i < d; i += blockDim.x) {
+        if (put) b = fmin(b, x[i]);
+        else a = fmax(a, x[i]);
+    }
+    for (int i = threadIdx.x; i < nK; i += blockDim.x) {
+        if (put) a = fmax(a, K[i]);
+        else b = fmin(b, K[i]);
+    }
+    s0[threadIdx.x] = a;
+    s1[threadIdx.x] = b;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            s0[threadIdx.x] = fmax(s0[threadIdx.x], s0[threadIdx.x + o]);
+            s1[threadIdx.x] = fmin(s1[threadIdx.x], s1[threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double g = s0[0] - s1[0];
+        int e = g > 0.0 ? (int)floor(log2(16384.0 / g)) : 0;
+        e = e < 0 ? 0 : (e > 60 ? 60 : e);
+        *out = (float)ldexp(1.0, e);
+    }
+}
+
+// Terminal values V = e(x) (knocked out below the barrier) and their split parts, stored
+// K x N row-major: the B operand of the next induction product.
+__global__ void k_berm_init(int d, int nK, int ldk, const double *__restrict__ x, const double *__restrict__ K,
+                            int put, double barrier, double *__restrict__ V, __nv_bfloat16 *__restrict__ Vhi,
+                            __nv_bfloat16 *__restrict__ Vlo, const float *__restrict__ dscale) {
+    const float sscale = dscale ? *dscale : 0.f;
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)d * ldk) return;
+    const int z = (int)(t / ldk), k = (int)(t - (long long)z * ldk);
+    double v = k < nK ? berm_exercise(x[z], K[k], put) : 0.0;
+    if (barrier > 0.0 && x[z] <= barrier) v = 0.0;
+    V[t] = v;
+    __nv_bfloat16 h, l;
+    split2((float)v, h, l, sscale);
+    Vhi[t] = h;
+    Vlo[t] = l;
+}
+
+// One induction date from the product C = P1 . V_next (FP32, times the split scale when
+// there is one): V = disc * C, then knocked out below the barrier, or (exercise) the larger
+// of it and the exercise value; the split parts for the next product (Vhi non-null) and
+// the quotes at state y0 (quotes non-null).
+__global__ void k_berm_step(int d, int nK, int ldk, const float *__restrict__ C, double disc,
+                            const double *__restrict__ x, const double *__restrict__ K, int put, double barrier,
+                            int exercise, double *__restrict__ V, __nv_bfloat16 *__restrict__ Vhi,
+                            __nv_bfloat16 *__restrict__ Vlo, const float *__restrict__ dscale, int y0,
+                            double *__restrict__ quotes) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)d * ldk) return;
+    const int z = (int)(t / ldk), k = (int)(t - (long long)z * ldk);
+    const float sscale = dscale ? *dscale : 0.f;
+    double v = 0.0;
+    if (k < nK) {
+        v = disc * (double)C[t];
+        if (dscale) v /= (double)sscale;
+        if (barrier > 0.0 && x[z] <= barrier) v = 0.0;
+        else if (exercise) v = fmax(v, berm_exercise(x[z], K[k], put));
+    }
+    V[t] = v;
+    if (Vhi) {
+        __nv_bfloat16 h, l;
+        split2((float)v, h, l, sscale);
+        Vhi[t] = h;
+        Vlo[t] = l;
+    }
+    if (quotes && z == y0 && k < nK) quotes[k] = v;
+}
+
 // ------------------------------------------------------------------ host launchers
 
 static inline int blocks_for(long long n, int threads) { return (int)((n + threads - 1) / threads); }
@@ -661,6 +753,27 @@ int launch_payoff(int d, int nK, int ldk, const double *x, const double *K, floa
                   __nv_bfloat16 *GTlo, cudaStream_t s, const float *dscale) {
     long long n = (long long)d * ldk;
     k_payoff<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, x, K, G, GThi, GTlo, dscale);
+    return (int)cudaGetLastError();
+}
+
+int launch_berm_scale(int d, const double *x, int nK, const double *K, int put, float *out, cudaStream_t s) {
+    k_berm_scale<<<1, 256, 0, s>>>(d, x, nK, K, put, out);
+    return (int)cudaGetLastError();
+}
+
+int launch_berm_init(int d, int nK, int ldk, const double *x, const double *K, int put, double barrier, double *V,
+                     __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo, const float *dscale, cudaStream_t s) {
+    const long long n = (long long)d * ldk;
+    k_berm_init<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, x, K, put, barrier, V, Vhi, Vlo, dscale);
+    return (int)cudaGetLastError();
+}
+
+int launch_berm_step(int d, int nK, int ldk, const float *C, double disc, const double *x, const double *K, int put,
+                     double barrier, int exercise, double *V, __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo,
+                     const float *dscale, int y0, double *quotes, cudaStream_t s) {
+    const long long n = (long long)d * ldk;
+    k_berm_step<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, C, disc, x, K, put, barrier, exercise, V, Vhi, Vlo,
+                                                   dscale, y0, quotes);
     return (int)cudaGetLastError();
 }
 

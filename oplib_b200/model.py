@@ -140,6 +140,23 @@ class Lattice:
         call("opb_lattice_solve", C.byref(L), mode, _ptr(ws), ws.numel(), _ptr(quotes), _ptr(V))
         return quotes, V
 
+    def bermudan(self, strikes, nmat: int, period: float, dt0: float, mode="bf16x3", put: bool = False,
+                 exercise: bool = True, barrier: float = 0.0, plan: Plan | None = None,
+                 workspace: torch.Tensor | None = None) -> torch.Tensor:
+        """Values at y0 [nK] (FP64) of calls or puts of maturity nmat*period by backward
+        induction on P(period), exercisable at every m*period (``exercise``) and knocked
+        out where the spot is at or below ``barrier`` on those dates (barrier > 0)."""
+        mode = MODES[mode] if isinstance(mode, str) else mode
+        strikes = torch.as_tensor(strikes, dtype=torch.float64, device=self.device)
+        plan = plan or self.plan(period, dt0)
+        ws = workspace if workspace is not None else self.workspace(strikes.numel(), mode)
+        quotes = torch.empty(strikes.numel(), dtype=torch.float64, device=self.device)
+        L = self.desc(plan, period, nmat, strikes)
+        bind_stream(self.device)
+        call("opb_lattice_bermudan", C.byref(L), mode, int(put), int(exercise), float(barrier), _ptr(ws), ws.numel(),
+             _ptr(quotes))
+        return quotes
+
     def kernel(self, period: float, dt0: float, mode="fp32", plan: Plan | None = None) -> torch.Tensor:
         """Transition kernel P(period) as a d x d FP32 source-major matrix."""
         mode = MODES[mode] if isinstance(mode, str) else mode

@@ -385,6 +385,34 @@ def solve_lattice_fp64(L: np.ndarray, x: np.ndarray, strikes: np.ndarray, r: flo
     return price_from_kernels(Ps, x, strikes, r, mats), niter, dt
 
 
+def bermudan_fp64(L: np.ndarray, x: np.ndarray, strikes: np.ndarray, r: float, period: float, nmat: int,
+                  dt0: float, put: bool = False, exercise: bool = True, barrier: float = 0.0) -> np.ndarray:
+    """FP64 backward induction on the period kernel P1 = P(period) (the same plan,
+    squarings and row renormalisation as ``solve_lattice_fp64``): V_nmat = e(x), then for
+    m = nmat-1 .. 0, V_m = exp(-r period) P1 . V_{m+1}, set to 0 where x <= barrier
+    (barrier > 0) and otherwise floored by the exercise value (exercise) at the dates
+    m >= 1.  e(x) = (x - K)^+ for calls, (K - x)^+ for puts.  This is the multi-vector
+    induction the reference's ``opcuda_sgemv3``/``sgemv4`` kernels perform
+    (``oplib/opcuda/sgemv3.cu:92-159``), with the exercise and barrier rules of a
+    Bermudan / discretely monitored down-and-out contract (no reference counterpart).
+    Returns V_0[y, k]."""
+    niter, dt = plan_niter(L, period, dt0)
+    P1 = square(ek(L, dt), niter, renorm=True)
+    K = np.asarray(strikes, dtype=np.float64)[None, :]
+    xs = np.asarray(x, dtype=np.float64)[:, None]
+    ex = np.maximum(K - xs, 0.0) if put else np.maximum(xs - K, 0.0)
+    out = (xs <= barrier) if barrier > 0.0 else np.zeros_like(xs, dtype=bool)
+    V = np.where(out, 0.0, ex)
+    disc = math.exp(-r * period)
+    for m in range(nmat - 1, -1, -1):
+        V = disc * (P1 @ V)
+        if m >= 1:
+            if exercise:
+                V = np.maximum(V, ex)
+            V = np.where(out, 0.0, V)
+    return V
+
+
 # ---------------------------------------------------------------------------------
 # The reference's two-dimensional generator with vol-level jumps (opcuda_sgsvg)
 # ---------------------------------------------------------------------------------

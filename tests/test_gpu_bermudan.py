@@ -1,0 +1,73 @@
+"""GPU parity of the backward-induction pricer (Bermudan and discretely monitored
+down-and-out options on the period kernel, ``opb_lattice_bermudan``) against the FP64
+induction oracle.  Tolerance: 1e-5 absolute price error (S0 = 1), the target accuracy of
+the lattice path."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+CASES = [  # (put, exercise, barrier)
+    (True, True, 0.0),    # Bermudan put
+    (False, True, 0.0),   # Bermudan call
+    (True, False, 0.0),   # European put by induction
+    (False, False, 0.8),  # down-and-out call, barrier 0.8
+    (True, True, 0.7),    # Bermudan down-and-out put
+]
+
+
+@pytest.mark.parametrize("mode", ["bf16x3", "fp16x3"])
+def test_bermudan_lv_matches_oracle(cuda, mode):
+    """The config-0 local-vol lattice (512 nodes, quarterly dates to 2 years, 64 strikes)."""
+    from oplib_b200.model import Lattice
+    cfg = O.LVLattice(n=512, nmat=8)
+    L, x = cfg.generator()
+    lat = Lattice.local_vol(n=512, level=cfg.level, skew=cfg.skew, width=cfg.width, rate=cfg.r, device=cuda)
+    y0 = O.nearest_node(x)
+    assert lat.y0 == y0
+    for put, ex, bar in CASES:
+        ref = O.bermudan_fp64(L, x, cfg.strikes, cfg.r, cfg.period, cfg.nmat, cfg.dt0, put=put, exercise=ex,
+                              barrier=bar)[y0]
+        q = lat.bermudan(cfg.strikes, cfg.nmat, cfg.period, cfg.dt0, mode=mode, put=put, exercise=ex, barrier=bar)
+        err = np.abs(q.cpu().numpy() - ref).max()
+        print(f"lv512 {mode} put={put} exercise={ex} barrier={bar}: {err:.3e}")
+        assert err <= TOL, (put, ex, bar, err)
+
+
+def test_european_by_induction_matches_the_chained_solve(cuda):
+    """exercise = 0, barrier = 0: the induction on P1 gives the chained solve's value at the
+    last maturity (two device paths through different products)."""
+    from oplib_b200.model import Lattice
+    cfg = O.LVLattice(n=512, nmat=8)
+    lat = Lattice.local_vol(n=512, level=cfg.level, skew=cfg.skew, width=cfg.width, rate=cfg.r, device=cuda)
+    q_ind = lat.bermudan(cfg.strikes, cfg.nmat, cfg.period, cfg.dt0, mode="fp16x3", put=False, exercise=False)
+    q_chain, _ = lat.solve(cfg.strikes, cfg.nmat, cfg.period, cfg.dt0, mode="fp16x3")
+    assert np.abs(q_ind.cpu().numpy() - q_chain[-1].cpu().numpy()).max() <= TOL
+
+
+def test_bermudan_sv_matches_oracle(cuda):
+    """A reduced stochastic-vol lattice (32 x 8 = 256 states), Bermudan puts."""
+    from oplib_b200.model import Lattice
+    spec = O.SVSpec(nx=32, nv=8)
+    L, xy, _ = O.sv_generator(spec)
+    strikes = 0.7 + np.arange(64) / 100
+    lat = Lattice.stoch_vol(nx=32, nv=8, device=cuda)
+    ref = O.bermudan_fp64(L, xy, strikes, spec.r, 0.25, 4, 2.0 ** -16, put=True, exercise=True)[lat.y0]
+    for mode in ("bf16x3", "fp16x3"):
+        q = lat.bermudan(strikes, 4, 0.25, 2.0 ** -16, mode=mode, put=True, exercise=True)
+        err = np.abs(q.cpu().numpy() - ref).max()
+        print(f"sv256 bermudan put {mode}: {err:.3e}")
+        assert err <= TOL, (mode, err)
+
+
+def test_bermudan_rejects_fp32_modes_and_bad_flags(cuda):
+    from oplib_b200._lib import OpcudaError
+    from oplib_b200.model import Lattice
+    lat = Lattice.local_vol(n=256, device=cuda)
+    with pytest.raises(OpcudaError):
+        lat.bermudan([1.0], 2, 0.25, 2.0 ** -14, mode="fp32")
+    with pytest.raises(OpcudaError):
+        lat.bermudan([1.0], 2, 0.25, 2.0 ** -14, mode="bf16x3", barrier=-1.0)

@@ -215,3 +215,33 @@ def test_gelu_erf_approximation_bound():
     exact = 0.5 * z * (1.0 + erf(z / math.sqrt(2.0)))
     assert np.max(np.abs((1.0 - e) - erf(x))) <= 1.5e-7
     assert np.all(np.abs(g - exact) <= 0.75e-7 * np.abs(z) + 1e-300)
+
+
+def test_bermudan_oracle_identities():
+    """The induction oracle against the chained European solve and the textbook ordering
+    of contract values: on a 128-node local-vol lattice (r > 0, no dividends) the European
+    value by induction equals the chained solve's value at the last maturity; a Bermudan
+    call is never exercised early away from the grid's upper edge (where the truncated
+    lattice is no longer a martingale), so it equals the European call there; a Bermudan
+    put is worth at least the European put (strictly more near the spot); a down-and-out
+    call is worth less than the vanilla call (strictly less at the spot).  Exercise and the
+    barrier apply at the dates m * period, m >= 1, not at time 0."""
+    cfg = O.LVLattice(n=128, nmat=6)
+    L, x = cfg.generator()
+    K = cfg.strikes[::8]
+    V, _, _ = O.solve_lattice_fp64(L, x, K, cfg.r, cfg.period, cfg.nmat, cfg.dt0)
+    args = (L, x, K, cfg.r, cfg.period, cfg.nmat, cfg.dt0)
+    euro_call = O.bermudan_fp64(*args, put=False, exercise=False)
+    assert np.abs(euro_call - V[-1]).max() < 1e-12
+    berm_call = O.bermudan_fp64(*args, put=False, exercise=True)
+    inner = x <= 1.25  # the edge's influence decays inward: 2e-11 at the spot, 1.6e-5 at x = 2.2
+    assert np.abs(berm_call - euro_call)[inner].max() < 1e-9
+    assert np.all(berm_call >= euro_call - 1e-14)
+    euro_put = O.bermudan_fp64(*args, put=True, exercise=False)
+    berm_put = O.bermudan_fp64(*args, put=True, exercise=True)
+    assert np.all(berm_put >= euro_put - 1e-14)
+    assert berm_put.max() - (berm_put - euro_put).max() > 0 and (berm_put - euro_put).max() > 1e-4
+    dao = O.bermudan_fp64(*args, put=False, exercise=False, barrier=0.8)
+    assert np.all(dao <= euro_call + 1e-14)
+    y0 = O.nearest_node(x)
+    assert np.all(dao[y0] < euro_call[y0] - 1e-4)
