@@ -1141,6 +1141,98 @@ def run_refbench(args):
             "note": "published_reference = the reference's own OPBench figure on a 2009 Tesla box (context)"}
 
 
+def run_bermudan(args):
+    """Bermudan puts on the SV lattice of the headline (d = 6144, 128 strikes, exercisable
+    every 0.25 y to 4 y) by backward induction on the period kernel: 14 split squarings,
+    then 16 induction products P1 . V (6144 x 6144 x 128) with the FP64 exercise step.  The
+    plain-FP32 arm squares on cuBLAS SGEMM (TF32 off) with the same FP64 row
+    renormalisation and runs the induction products in FP32 with the same FP64 step; the
+    FP64 reference does everything in FP64 with torch on the device."""
+    import torch
+    from oplib_b200 import _lib
+    from oplib_b200.model import MODES, Lattice, bind_stream
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    bind_stream(dev)
+    stream = torch.cuda.current_stream(dev)
+    lat = Lattice.stoch_vol(**SV, device=dev)
+    plan = lat.plan(PERIOD, DT0)
+    strikes = torch.tensor(STRIKES, dtype=torch.float64, device=dev)
+    desc = lat.desc(plan, PERIOD, NMAT, strikes)
+    disc = math.exp(-lat.rate * PERIOD)
+    x = lat.x
+    ex = torch.clamp(strikes.unsqueeze(0) - x.unsqueeze(1), min=0.0)  # put exercise values [d, nK]
+
+    def induction(P1, dtype):
+        V = ex.clone()
+        for m in range(NMAT - 1, -1, -1):
+            V = disc * (P1 @ V.to(dtype)).double()
+            if m >= 1:
+                V = torch.maximum(V, ex)
+        return V[lat.y0]
+
+    out = {}
+    for mode in ("bf16x3", "fp16x3"):
+        md = MODES[mode]
+        ws = lat.workspace(NK, md)
+        q = torch.empty(NK, dtype=torch.float64, device=dev)
+        f = lambda: _lib.call("opb_lattice_bermudan", C.byref(desc), md, 1, 1, 0.0, ws.data_ptr(), ws.numel(),
+                              q.data_ptr())
+        for _ in range(args.warmup):
+            f()
+        ms = _time(f, args.steps, stream, torch)
+        out[mode] = {"ms_per_solve": round(ms, 3), "quotes_per_s": round(NK / (ms * 1e-3), 1), "q": q.clone()}
+        del ws
+    # FP64 reference (outside the timed regions)
+    d = lat.d
+    cols = lat.cols.view(d, -1).long()
+    vals = lat.vals.view(d, -1)
+    mask = cols >= 0
+    rows = torch.arange(d, device=dev).unsqueeze(1).expand_as(cols)
+    Ld = torch.zeros(d, d, dtype=torch.float64, device=dev)
+    Ld.index_put_((rows[mask], cols[mask]), vals[mask], accumulate=True)
+    P = torch.eye(d, dtype=torch.float64, device=dev) + plan.dt * Ld
+    del Ld
+    for _ in range(plan.niter):
+        P = P @ P
+        P /= P.sum(dim=1, keepdim=True)
+    ref = induction(P, torch.float64)
+    del P
+    for mode in out:
+        out[mode]["max_abs_err_vs_fp64"] = float((out[mode].pop("q") - ref).abs().max().item())
+    # plain FP32 arm: cuBLAS squaring with FP64 row renormalisation, FP32 induction products
+    prev_tf32 = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+
+    def fp32_arm():
+        P = torch.zeros(d, d, dtype=torch.float32, device=dev)
+        P.index_put_((rows[mask], cols[mask]), (plan.dt * vals[mask]).float(), accumulate=True)
+        P.diagonal().add_(1.0)
+        T = torch.empty_like(P)
+        for _ in range(plan.niter):
+            torch.mm(P, P, out=T)
+            P, T = T, P
+            P.mul_((1.0 / P.sum(dim=1, dtype=torch.float64)).float().unsqueeze(1))
+        return induction(P, torch.float32)
+
+    fp32_arm()
+    torch.cuda.synchronize()
+    ms32 = _time(fp32_arm, max(2, args.steps // 3), stream, torch)
+    err32 = float((fp32_arm() - ref).abs().max().item())
+    torch.backends.cuda.matmul.allow_tf32 = prev_tf32
+    best = out["bf16x3"]
+    return {"metric": "Bermudan put quotes/sec (backward induction on the SV d=6144 period kernel)",
+            "value": best["quotes_per_s"], "unit": "quotes/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": best["ms_per_solve"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic",
+            "config": {"workload": f"SV lattice d={d}, {NK} strikes, Bermudan puts exercisable every {PERIOD} y "
+                                   f"to {PERIOD * NMAT} y", "niter": plan.niter, "products": NMAT},
+            "max_abs_err_vs_fp64": best["max_abs_err_vs_fp64"], "modes": out,
+            "fp32_cublas": {"quotes_per_s": round(NK / (ms32 * 1e-3), 1), "ms_per_solve": round(ms32, 3),
+                            "max_abs_err_vs_fp64": err32},
+            "speedup_vs_fp32_cublas": round(ms32 / best["ms_per_solve"], 2)}
+
+
 def run_gemm(args):
     """The squaring GEMM alone (split-BF16, E-form: C = E.E + 2E in place) at size d, in the
     solve's form: B is E's own row-major parts, read as an MN-major operand."""
@@ -1186,7 +1278,7 @@ def main():
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--workload", default="sv",
                     choices=["sv", "lv", "mc", "gemm", "gemv", "renorm", "batch", "surrogate", "calibrate",
-                             "refbench"],
+                             "refbench", "bermudan"],
                     help="sv = the headline SV lattice solve; the others are secondary measurements")
     ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
     args = ap.parse_args()
@@ -1206,7 +1298,7 @@ def main():
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "gemv": run_gemv, "renorm": run_renorm,
               "batch": run_batch_sharded if launched else run_batch, "surrogate": run_surrogate,
-              "calibrate": run_calibrate, "refbench": run_refbench}[args.workload]
+              "calibrate": run_calibrate, "refbench": run_refbench, "bermudan": run_bermudan}[args.workload]
         line = fn(args)
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps(line))
