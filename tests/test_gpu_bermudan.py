@@ -71,3 +71,17 @@ def test_bermudan_rejects_fp32_modes_and_bad_flags(cuda):
         lat.bermudan([1.0], 2, 0.25, 2.0 ** -14, mode="fp32")
     with pytest.raises(OpcudaError):
         lat.bermudan([1.0], 2, 0.25, 2.0 ** -14, mode="bf16x3", barrier=-1.0)
+
+
+def test_bermudan_ragged_strike_count(cuda):
+    """Five strikes (padded to the 64-column tile inside): the padding columns stay zero and
+    the five values match the oracle."""
+    from oplib_b200.model import Lattice
+    cfg = O.LVLattice(n=256, nmat=3)
+    L, x = cfg.generator()
+    K = np.array([0.8, 0.95, 1.0, 1.1, 1.3])
+    lat = Lattice.local_vol(n=256, level=cfg.level, skew=cfg.skew, width=cfg.width, rate=cfg.r, device=cuda)
+    ref = O.bermudan_fp64(L, x, K, cfg.r, cfg.period, cfg.nmat, cfg.dt0, put=True, exercise=True)[lat.y0]
+    q = lat.bermudan(K, cfg.nmat, cfg.period, cfg.dt0, mode="bf16x3", put=True, exercise=True)
+    assert q.shape == (5,)
+    assert np.abs(q.cpu().numpy() - ref).max() <= TOL
