@@ -1144,10 +1144,11 @@ def run_refbench(args):
 def run_bermudan(args):
     """Bermudan puts on the SV lattice of the headline (d = 6144, 128 strikes, exercisable
     every 0.25 y to 4 y) by backward induction on the period kernel: 14 split squarings,
-    then 16 induction products P1 . V (6144 x 6144 x 128) with the FP64 exercise step.  The
-    plain-FP32 arm squares on cuBLAS SGEMM (TF32 off) with the same FP64 row
-    renormalisation and runs the induction products in FP32 with the same FP64 step; the
-    FP64 reference does everything in FP64 with torch on the device."""
+    then 16 induction products P1 . V (6144 x 6144 x 128) with the FP64 exercise step.  Two
+    plain-FP32 arms: the library's SIMT path (`opb_lattice_bermudan` in OPB_FP32_RENORM) and
+    cuBLAS SGEMM (TF32 off) with the same FP64 row renormalisation and FP64 step, the
+    faster one being `speedup_vs_fp32`; the FP64 reference does everything in FP64 with
+    torch on the device."""
     import torch
     from oplib_b200 import _lib
     from oplib_b200.model import MODES, Lattice, bind_stream
@@ -1172,15 +1173,15 @@ def run_bermudan(args):
         return V[lat.y0]
 
     out = {}
-    for mode in ("bf16x3", "fp16x3"):
+    for mode in ("bf16x3", "fp16x3", "fp32"):  # fp32: the library's SIMT path with FP64 renormalisation
         md = MODES[mode]
         ws = lat.workspace(NK, md)
         q = torch.empty(NK, dtype=torch.float64, device=dev)
         f = lambda: _lib.call("opb_lattice_bermudan", C.byref(desc), md, 1, 1, 0.0, ws.data_ptr(), ws.numel(),
                               q.data_ptr())
-        for _ in range(args.warmup):
+        for _ in range(args.warmup if mode != "fp32" else 1):
             f()
-        ms = _time(f, args.steps, stream, torch)
+        ms = _time(f, args.steps if mode != "fp32" else 2, stream, torch)
         out[mode] = {"ms_per_solve": round(ms, 3), "quotes_per_s": round(NK / (ms * 1e-3), 1), "q": q.clone()}
         del ws
     # FP64 reference (outside the timed regions)
@@ -1230,7 +1231,9 @@ def run_bermudan(args):
             "max_abs_err_vs_fp64": best["max_abs_err_vs_fp64"], "modes": out,
             "fp32_cublas": {"quotes_per_s": round(NK / (ms32 * 1e-3), 1), "ms_per_solve": round(ms32, 3),
                             "max_abs_err_vs_fp64": err32},
-            "speedup_vs_fp32_cublas": round(ms32 / best["ms_per_solve"], 2)}
+            "speedup_vs_fp32_cublas": round(ms32 / best["ms_per_solve"], 2),
+            "speedup_vs_fp32_simt": round(out["fp32"]["ms_per_solve"] / best["ms_per_solve"], 2),
+            "speedup_vs_fp32": round(min(ms32, out["fp32"]["ms_per_solve"]) / best["ms_per_solve"], 2)}
 
 
 def run_gemm(args):

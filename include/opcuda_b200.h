@@ -242,7 +242,8 @@ int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspace, unsi
  * knocked out where x <= barrier (barrier > 0) and, with exercise = 1, floored by the
  * exercise value, at every T_m, m = 1..nmat-1 (Bermudan / discretely monitored
  * down-and-out); exercise = 0 and barrier = 0 give the European value at T.  quotes:
- * device [nK] FP64 values at y0.  Split modes only; workspace as for opb_lattice_solve. */
+ * device [nK] FP64 values at y0.  Induction products on the tensor cores in the split modes,
+ * on the FP32 SIMT GEMM in the FP32 modes; workspace as for opb_lattice_solve. */
 int opb_lattice_bermudan(const opb_lattice_desc *L, int mode, int put, int exercise, double barrier,
                          void *workspace, unsigned long long ws_bytes, double *quotes);
 /* new: transition kernel P(period) only (device d x d FP32, source-major), e.g. the MC step

@@ -98,6 +98,7 @@ Bufs carve(Ws &w, int d, int nK, int mode) {
     } else {
         b.G = w.take<float>((size_t)d * nK);
         b.part = w.take<double>((size_t)d);
+        b.Vd = w.take<double>((size_t)d * nK);
     }
     return b;
 }
@@ -108,9 +109,10 @@ Bufs carve(Ws &w, int d, int nK, int mode) {
         if (_r != 0) return _r;          \
     } while (0)
 
-int solve_fp32(const opb_lattice_desc &L, int mode, Bufs &b, double *quotes, double *V_all, cudaStream_t s,
-               float *P_out) {
-    const int d = L.d, nK = L.nK;
+// U0 = I + dt*L in FP32, niter FP32 squarings (with FP64 row renormalisation in
+// OPB_FP32_RENORM) ping-ponging through X, Pa, Pb; *cur receives the index of P1.
+int square_fp32(const opb_lattice_desc &L, int mode, Bufs &b, cudaStream_t s, int *cur_out) {
+    const int d = L.d;
     // U0 in FP32 from FP64 arithmetic
     if (L.ell_width > 0) LT(opb::launch_ek_ell(d, L.ell_width, L.gen_cols, L.gen_vals, L.dt, 0, b.X, s));
     else LT(opb::launch_ek_dense(d, L.gen_dense, L.dt, 0, b.X, s));
@@ -124,6 +126,16 @@ int solve_fp32(const opb_lattice_desc &L, int mode, Bufs &b, double *quotes, dou
         }
         int t = cur; cur = nxt; nxt = t;
     }
+    *cur_out = cur;
+    return 0;
+}
+
+int solve_fp32(const opb_lattice_desc &L, int mode, Bufs &b, double *quotes, double *V_all, cudaStream_t s,
+               float *P_out) {
+    const int d = L.d, nK = L.nK;
+    int cur = 0;
+    LT(square_fp32(L, mode, b, s, &cur));
+    float *buf[3] = {b.X, b.Pa, b.Pb};
     // buf[cur] = P(period); the chain alternates between the two other buffers
     float *P1 = buf[cur];
     if (P_out) return (int)cudaMemcpyAsync(P_out, P1, sizeof(float) * (size_t)d * d, cudaMemcpyDeviceToDevice, s);
@@ -269,7 +281,7 @@ int bermudan_tc(const opb_lattice_desc &L, Bufs &b, int put, int exercise, doubl
         gs = b.gscale;
     }
     // V's parts live in the payoff-part buffers (d x nKp each)
-    LT(opb::launch_berm_init(d, nK, nKp, L.x, L.strikes, put, barrier, b.Vd, b.GThi, b.GTlo, gs, s));
+    LT(opb::launch_berm_init(d, nK, nKp, L.x, L.strikes, put, barrier, b.Vd, b.GThi, b.GTlo, nullptr, gs, s));
     opb::TcGemmArgs pg{};
     pg.M = d; pg.N = nKp; pg.K = d; pg.lda = d; pg.ldb = nKp; pg.ldc = nKp; pg.f16 = f16 ? 1 : 0; pg.b_kn = 1;
     pg.Ahi = b.Ahi; pg.Alo = b.Alo; pg.Bhi = b.GThi; pg.Blo = b.GTlo; pg.C = b.V; pg.beta = 0.f;
@@ -279,8 +291,29 @@ int bermudan_tc(const opb_lattice_desc &L, Bufs &b, int put, int exercise, doubl
         LT(tc_gemm_ksplit(pg, s));
         const bool last = m == 0;
         LT(opb::launch_berm_step(d, nK, nKp, b.V, disc, L.x, L.strikes, put, last ? 0.0 : barrier,
-                                 last ? 0 : exercise, b.Vd, last ? nullptr : b.GThi, last ? nullptr : b.GTlo, gs,
-                                 L.y0, last ? quotes : nullptr, s));
+                                 last ? 0 : exercise, b.Vd, last ? nullptr : b.GThi, last ? nullptr : b.GTlo, nullptr,
+                                 gs, L.y0, last ? quotes : nullptr, s));
+    }
+    return 0;
+}
+
+// The same induction with FP32 SIMT products (the reference's FP32 arithmetic; with
+// OPB_FP32_RENORM the squarings are renormalised in FP64).
+int bermudan_fp32(const opb_lattice_desc &L, int mode, Bufs &b, int put, int exercise, double barrier,
+                  double *quotes, cudaStream_t s) {
+    const int d = L.d, nK = L.nK;
+    int cur = 0;
+    LT(square_fp32(L, mode, b, s, &cur));
+    float *buf[3] = {b.X, b.Pa, b.Pb};
+    const float *P1 = buf[cur];
+    LT(opb::launch_berm_init(d, nK, nK, L.x, L.strikes, put, barrier, b.Vd, nullptr, nullptr, b.G, nullptr, s));
+    const double disc = std::exp(-L.rate * L.period);
+    for (int m = L.nmat - 1; m >= 0; m--) {
+        LT(opb::sgemm_rm(d, nK, d, 1.f, P1, d, b.G, nK, 0.f, b.V, nK, s));
+        const bool last = m == 0;
+        LT(opb::launch_berm_step(d, nK, nK, b.V, disc, L.x, L.strikes, put, last ? 0.0 : barrier,
+                                 last ? 0 : exercise, b.Vd, nullptr, nullptr, last ? nullptr : b.G, nullptr, L.y0,
+                                 last ? quotes : nullptr, s));
     }
     return 0;
 }
@@ -346,13 +379,13 @@ OPB_API int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspa
 // final maturity T = nmat * period; exercise = 1: exercisable at T_m = m * period for m =
 // 1..nmat (Bermudan), 0: at T only; barrier > 0: knocked out when the spot is at or below
 // the barrier on any date T_m (m >= 1).  exercise = 0 with barrier = 0 gives the European
-// value at T.  quotes: device [nK] FP64, the values at state y0.  Split modes only (the
-// induction products run on the tensor cores); workspace as for opb_lattice_solve.
+// value at T.  quotes: device [nK] FP64, the values at state y0.  In the split modes the
+// induction products run on the tensor cores, in the FP32 modes on the SIMT GEMM;
+// workspace as for opb_lattice_solve.
 OPB_API int opb_lattice_bermudan(const opb_lattice_desc *L, int mode, int put, int exercise, double barrier,
                                  void *workspace, unsigned long long ws_bytes, double *quotes) {
     int c = check_desc(L, mode);
     if (c == OPB_OK && !quotes) c = OPB_E_NULL;
-    if (c == OPB_OK && !tc_mode(mode)) c = OPB_E_UNSUPPORTED;
     if (c == OPB_OK && (put < 0 || put > 1 || exercise < 0 || exercise > 1 || !(barrier >= 0.0))) c = OPB_E_ARG;
     if (c != OPB_OK) return opb::set_status(c);
     OPB_REQUIRE(workspace, OPB_E_NULL);
@@ -361,7 +394,9 @@ OPB_API int opb_lattice_bermudan(const opb_lattice_desc *L, int mode, int put, i
     size_t off = (256 - (reinterpret_cast<uintptr_t>(workspace) & 255)) & 255;
     w.p += off;
     Bufs b = carve(w, L->d, L->nK, mode);
-    return opb::set_status(bermudan_tc(*L, b, put, exercise, barrier, quotes, opb::stream(), mode == OPB_FP16X3));
+    cudaStream_t s = opb::stream();
+    return opb::set_status(tc_mode(mode) ? bermudan_tc(*L, b, put, exercise, barrier, quotes, s, mode == OPB_FP16X3)
+                                         : bermudan_fp32(*L, mode, b, put, exercise, barrier, quotes, s));
 }
 
 // Transition kernel only: P_out (device, d x d FP32, source-major) = P(period) after

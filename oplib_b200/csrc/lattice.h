@@ -66,9 +66,9 @@ struct RenormProblem {
 // Bermudan / barrier backward induction (lattice_kernels.cu)
 int launch_berm_scale(int d, const double *x, int nK, const double *K, int put, float *out, cudaStream_t s);
 int launch_berm_init(int d, int nK, int ldk, const double *x, const double *K, int put, double barrier, double *V,
-                     __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo, const float *dscale, cudaStream_t s);
+                     __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo, float *Vf, const float *dscale, cudaStream_t s);
 int launch_berm_step(int d, int nK, int ldk, const float *C, double disc, const double *x, const double *K, int put,
-                     double barrier, int exercise, double *V, __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo,
+                     double barrier, int exercise, double *V, __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo, float *Vf,
                      const float *dscale, int y0, double *quotes, cudaStream_t s);
 int launch_renorm_to_p(int d, float *X, const double *partial, int nparts, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
                        __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale = 0.f);

@@ -546,11 +546,11 @@ __global__ void k_berm_scale(int d, const double *__restrict__ x, int nK, const 
     }
 }
 
-// Terminal values V = e(x) (knocked out below the barrier) and their split parts, stored
-// K x N row-major: the B operand of the next induction product.
+// Terminal values V = e(x) (knocked out below the barrier) and the next induction
+// product's B operand, K x N row-major: the split parts (Vhi non-null) or FP32 values (Vf).
 __global__ void k_berm_init(int d, int nK, int ldk, const double *__restrict__ x, const double *__restrict__ K,
                             int put, double barrier, double *__restrict__ V, __nv_bfloat16 *__restrict__ Vhi,
-                            __nv_bfloat16 *__restrict__ Vlo, const float *__restrict__ dscale) {
+                            __nv_bfloat16 *__restrict__ Vlo, float *__restrict__ Vf, const float *__restrict__ dscale) {
     const float sscale = dscale ? *dscale : 0.f;
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)d * ldk) return;
@@ -558,21 +558,24 @@ __global__ void k_berm_init(int d, int nK, int ldk, const double *__restrict__ x
     double v = k < nK ? berm_exercise(x[z], K[k], put) : 0.0;
     if (barrier > 0.0 && x[z] <= barrier) v = 0.0;
     V[t] = v;
-    __nv_bfloat16 h, l;
-    split2((float)v, h, l, sscale);
-    Vhi[t] = h;
-    Vlo[t] = l;
+    if (Vhi) {
+        __nv_bfloat16 h, l;
+        split2((float)v, h, l, sscale);
+        Vhi[t] = h;
+        Vlo[t] = l;
+    }
+    if (Vf) Vf[t] = (float)v;
 }
 
 // One induction date from the product C = P1 . V_next (FP32, times the split scale when
 // there is one): V = disc * C, then knocked out below the barrier, or (exercise) the larger
-// of it and the exercise value; the split parts for the next product (Vhi non-null) and
-// the quotes at state y0 (quotes non-null).
+// of it and the exercise value; the next product's operand (split parts when Vhi is
+// non-null, FP32 values when Vf is) and the quotes at state y0 (quotes non-null).
 __global__ void k_berm_step(int d, int nK, int ldk, const float *__restrict__ C, double disc,
                             const double *__restrict__ x, const double *__restrict__ K, int put, double barrier,
                             int exercise, double *__restrict__ V, __nv_bfloat16 *__restrict__ Vhi,
-                            __nv_bfloat16 *__restrict__ Vlo, const float *__restrict__ dscale, int y0,
-                            double *__restrict__ quotes) {
+                            __nv_bfloat16 *__restrict__ Vlo, float *__restrict__ Vf, const float *__restrict__ dscale,
+                            int y0, double *__restrict__ quotes) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)d * ldk) return;
     const int z = (int)(t / ldk), k = (int)(t - (long long)z * ldk);
@@ -591,6 +594,7 @@ __global__ void k_berm_step(int d, int nK, int ldk, const float *__restrict__ C,
         Vhi[t] = h;
         Vlo[t] = l;
     }
+    if (Vf) Vf[t] = (float)v;
     if (quotes && z == y0 && k < nK) quotes[k] = v;
 }
 
@@ -762,18 +766,18 @@ int launch_berm_scale(int d, const double *x, int nK, const double *K, int put, 
 }
 
 int launch_berm_init(int d, int nK, int ldk, const double *x, const double *K, int put, double barrier, double *V,
-                     __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo, const float *dscale, cudaStream_t s) {
+                     __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo, float *Vf, const float *dscale, cudaStream_t s) {
     const long long n = (long long)d * ldk;
-    k_berm_init<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, x, K, put, barrier, V, Vhi, Vlo, dscale);
+    k_berm_init<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, x, K, put, barrier, V, Vhi, Vlo, Vf, dscale);
     return (int)cudaGetLastError();
 }
 
 int launch_berm_step(int d, int nK, int ldk, const float *C, double disc, const double *x, const double *K, int put,
-                     double barrier, int exercise, double *V, __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo,
+                     double barrier, int exercise, double *V, __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo, float *Vf,
                      const float *dscale, int y0, double *quotes, cudaStream_t s) {
     const long long n = (long long)d * ldk;
     k_berm_step<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, C, disc, x, K, put, barrier, exercise, V, Vhi, Vlo,
-                                                   dscale, y0, quotes);
+                                                   Vf, dscale, y0, quotes);
     return (int)cudaGetLastError();
 }
 

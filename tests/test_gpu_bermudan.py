@@ -63,14 +63,29 @@ def test_bermudan_sv_matches_oracle(cuda):
         assert err <= TOL, (mode, err)
 
 
-def test_bermudan_rejects_fp32_modes_and_bad_flags(cuda):
+def test_bermudan_fp32_modes(cuda):
+    """The FP32 SIMT induction: with the FP64 row renormalisation within the 1e-5 bar; the
+    reference's plain FP32 squaring within 5e-4 (its error is what renormalisation removes)."""
+    from oplib_b200.model import Lattice
+    cfg = O.LVLattice(n=256, nmat=4)
+    L, x = cfg.generator()
+    lat = Lattice.local_vol(n=256, level=cfg.level, skew=cfg.skew, width=cfg.width, rate=cfg.r, device=cuda)
+    ref = O.bermudan_fp64(L, x, cfg.strikes, cfg.r, cfg.period, cfg.nmat, cfg.dt0, put=True, exercise=True)[lat.y0]
+    for mode, tol in (("fp32", TOL), ("fp32_plain", 5e-4)):
+        q = lat.bermudan(cfg.strikes, cfg.nmat, cfg.period, cfg.dt0, mode=mode, put=True, exercise=True)
+        err = np.abs(q.cpu().numpy() - ref).max()
+        print(f"lv256 bermudan put {mode}: {err:.3e}")
+        assert err <= tol, (mode, err)
+
+
+def test_bermudan_rejects_bad_flags(cuda):
     from oplib_b200._lib import OpcudaError
     from oplib_b200.model import Lattice
     lat = Lattice.local_vol(n=256, device=cuda)
     with pytest.raises(OpcudaError):
-        lat.bermudan([1.0], 2, 0.25, 2.0 ** -14, mode="fp32")
-    with pytest.raises(OpcudaError):
         lat.bermudan([1.0], 2, 0.25, 2.0 ** -14, mode="bf16x3", barrier=-1.0)
+    with pytest.raises(OpcudaError):
+        lat.bermudan([1.0], 2, 0.25, 2.0 ** -14, mode="bf16x3", put=2)
 
 
 def test_bermudan_ragged_strike_count(cuda):
