@@ -286,6 +286,11 @@ int opb_batch_plan_destroy(opb_batch_plan *plan);
 int opb_batch_set_config(opb_batch_plan *plan, int cfg, int grid);
 int opb_batch_num_configs(void);
 int opb_batch_execute(opb_batch_plan *plan, double *quotes);
+/* new (extension, as opb_lattice_bermudan): Bermudan or down-and-out calls/puts of maturity
+ * nmat * period on every lattice of the plan by backward induction on its period kernel,
+ * one batched tensor-core product per date over all lattices; quotes: device [nlat][nK]
+ * FP64 values at each lattice's y0 */
+int opb_batch_execute_bermudan(opb_batch_plan *plan, int put, int exercise, double barrier, double *quotes);
 /* times the level-0 launch for every configuration (ms_out: opb_batch_num_configs() floats)
  * and keeps the fastest */
 int opb_batch_autotune(opb_batch_plan *plan, int reps, float *ms_out, int *best_cfg);

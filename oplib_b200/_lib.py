@@ -114,6 +114,7 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_batch_plan_destroy": (i32, [vp]),
     "opb_batch_set_config": (i32, [vp, i32, i32]),
     "opb_batch_execute": (i32, [vp, vp]),
+    "opb_batch_execute_bermudan": (i32, [vp, i32, i32, f64, vp]),
     "opb_batch_autotune": (i32, [vp, i32, vp, vp]),
     "opb_batch_launches": (i32, [vp]),
     # surrogate MLP

@@ -31,6 +31,8 @@ struct opb_lattice_desc;  // lattice.cu
 extern "C" int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
                                  double *quotes, double *V_all);
 extern "C" unsigned long long opb_lattice_workspace_size(int d, int nK, int mode);
+extern "C" int opb_lattice_bermudan(const opb_lattice_desc *L, int mode, int put, int exercise, double barrier,
+                                    void *workspace, unsigned long long ws_bytes, double *quotes);
 
 struct opb_batch_desc {
     int nlat;
@@ -97,6 +99,8 @@ struct opb_batch_plan {
     // E's row-major A parts, MN-major), chain (B = P1's row-major parts), pricing (K-major
     // payoff parts)
     CUtensorMap *maps_sq = nullptr, *maps_ch = nullptr, *maps_price = nullptr;
+    // backward induction: A = P1's parts, B = the option values' parts read d x ldk row-major
+    CUtensorMap *maps_berm = nullptr;
     uint32_t *work = nullptr;
     float *E_base = nullptr;
     size_t E_bytes = 0;
@@ -187,6 +191,8 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     double *part = c.take<double>(parts);
     (void)c.take<float>(n);          // per-lattice FP16 payoff scales
     (void)c.take<double2>(off[n]);   // per-row fixes of the deferred E-form renormalisation
+    auto mbm = c.take<CUtensorMap>(4 * (size_t)n);  // backward-induction maps
+    (void)c.take<double>((size_t)off[n] * ldk);     // FP64 option values of the backward induction
 
     // ---- work lists (host), appended into one blob
     std::vector<uint32_t> W;
@@ -269,7 +275,7 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     P->total_rows = off[n]; P->ell_width = b->ell_width; P->cols = b->gen_cols; P->vals = b->gen_vals;
     P->x = b->x; P->strikes = b->strikes; P->period = b->period;
     P->lats = lats; P->sq = sq; P->chain = ch; P->price = pr; P->rn_sq = rs; P->rn_chain = rc;
-    P->maps_sq = msq; P->maps_ch = mch; P->maps_price = mp; P->work = work;
+    P->maps_sq = msq; P->maps_ch = mch; P->maps_price = mp; P->maps_berm = mbm; P->work = work;
     P->E_base = E; P->E_bytes = Etot * sizeof(float);
     for (int cfg = 0; cfg < NCFG; cfg++) {
         P->gemm_level[cfg] = gl[cfg];
@@ -326,7 +332,7 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     std::vector<opb::BatchLattice> lats(n);
     std::vector<opb::TcProblem> sq(n), ch(n), pr(n);
     std::vector<opb::RenormProblem> rs(n), rc(n);
-    std::vector<CUtensorMap> msq(4 * (size_t)n), mch(4 * (size_t)n), mp(4 * (size_t)n);
+    std::vector<CUtensorMap> msq(4 * (size_t)n), mch(4 * (size_t)n), mp(4 * (size_t)n), mbm(4 * (size_t)n);
     // recompute buffer pointers exactly as layout() carved them
     Carve cv{base, 0};
     cv.take<opb::BatchLattice>(n); cv.take<opb::TcProblem>(n); cv.take<opb::TcProblem>(n); cv.take<opb::TcProblem>(n);
@@ -345,6 +351,8 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     double *part = cv.take<double>(parts);
     float *gsc = cv.take<float>(n);
     double2 *fix = cv.take<double2>((size_t)P->total_rows);
+    (void)cv.take<CUtensorMap>(4 * (size_t)n);
+    double *vd = cv.take<double>((size_t)P->total_rows * P->ldk);
     const int f16 = mode == OPB_FP16X3_B ? 1 : 0;
     P->f16 = f16;
     const float un2 = f16 ? 1.f / (F16S * F16S) : 1.f, un1 = f16 ? 1.f / F16S : 1.f;
@@ -358,6 +366,7 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
         L.E = E + eo; L.Pa = Pa + eo; L.V = V + (size_t)ro * P->ldk;
         L.GThi = Gh + (size_t)ro * P->ldk; L.GTlo = Gl + (size_t)ro * P->ldk;
         L.gscale = gsc + i;
+        L.Vd = vd + (size_t)ro * P->ldk;
         double *pi = part + po;
         // squaring reads E as the previous level's GEMM left it, renormalised on the fly by
         // the row fixes of the previous level's (or the initial split's) renormalisation
@@ -374,6 +383,9 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
         if (rc_status == OPB_OK)
             rc_status =
                 opb::tc_make_maps(&mp[4 * (size_t)i], Ah + eo, Al + eo, d, d, L.GThi, L.GTlo, P->ldk, d, d, 64, f16);
+        if (rc_status == OPB_OK)  // the same buffers, the value parts read d x ldk row-major
+            rc_status = opb::tc_make_maps(&mbm[4 * (size_t)i], Ah + eo, Al + eo, d, d, L.GThi, L.GTlo, P->ldk,
+                                          P->ldk, d, 64, f16, 1);
         eo += (size_t)d * d;
         po += (size_t)(d / 64) * d;
         ro += d;
@@ -398,6 +410,7 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     if (e == cudaSuccess) e = up(P->maps_sq, msq.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
     if (e == cudaSuccess) e = up(P->maps_ch, mch.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
     if (e == cudaSuccess) e = up(P->maps_price, mp.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
+    if (e == cudaSuccess) e = up(P->maps_berm, mbm.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
     if (e == cudaSuccess) e = up(P->work, W.data(), sizeof(uint32_t) * W.size());
     const cudaError_t es = cudaStreamSynchronize(ls);
     if (e == cudaSuccess) e = es;
@@ -450,6 +463,22 @@ int level_gemm(opb_batch_plan *P, int cfg, int level, cudaStream_t s) {
     return cfg_gemm(P, cfg, P->maps_sq, P->sq, P->gemm_level[cfg][level], P->gemm_level_rest[cfg][level], s);
 }
 
+// E0 build and every squaring level (one GEMM + one renormalisation launch each): P1 of
+// every lattice as row-major parts in its A and B buffers.
+int batch_square(opb_batch_plan *P, cudaStream_t s) {
+    const int cfg = P->cfg, bn = CFG_BN[cfg], pdiv = bn < 128 ? bn : 128;
+    const float ss = P->f16 ? F16S : 0.f;
+    int r = (int)cudaMemsetAsync(P->E_base, 0, P->E_bytes, s);
+    if (r == 0) r = opb::launch_ek_batched(P->lats, P->nlat, P->total_rows, P->ell_width, P->cols, P->vals, s);
+    if (r == 0) r = opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_init.off, P->rn_init.n, 0, s, ss);
+    for (int lv = 0; lv < P->maxn && r == 0; lv++) {
+        r = level_gemm(P, cfg, lv, s);
+        if (r == 0)
+            r = opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_level[lv].off, P->rn_level[lv].n, pdiv, s, ss);
+    }
+    return r;
+}
+
 }  // namespace
 
 // Executes the plan on the library stream: E0 build, every squaring level (one GEMM +
@@ -472,13 +501,7 @@ OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
     }
     const int cfg = P->cfg, bn = CFG_BN[cfg], pdiv = bn < 128 ? bn : 128;
     const float ss = P->f16 ? F16S : 0.f;
-    BT((int)cudaMemsetAsync(P->E_base, 0, P->E_bytes, s));
-    BT(opb::launch_ek_batched(P->lats, P->nlat, P->total_rows, P->ell_width, P->cols, P->vals, s));
-    BT(opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_init.off, P->rn_init.n, 0, s, ss));
-    for (int lv = 0; lv < P->maxn; lv++) {
-        BT(level_gemm(P, cfg, lv, s));
-        BT(opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_level[lv].off, P->rn_level[lv].n, pdiv, s, ss));
-    }
+    BT(batch_square(P, s));
     BT(opb::launch_payoff_batched(P->lats, P->nlat, P->total_rows, P->nK, P->ldk, P->x, P->strikes, s, P->f16));
     for (int m = 1; m <= P->nmat; m++) {
         if (m > 1) {
@@ -489,6 +512,41 @@ OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
         BT(opb::launch_tc_gemm_batched(64, P->maps_price, P->price, P->work + P->gemm_price.off, P->gemm_price.n,
                                        P->grid, s, P->f16, 0));
         BT(opb::launch_quotes_batched(P->lats, P->nlat, P->nK, P->ldk, m, P->nmat, quotes, s, P->f16));
+    }
+#undef BT
+    return set_status(OPB_OK);
+}
+
+// Bermudan or barrier calls/puts on every lattice of the plan by backward induction on its
+// period kernel (as opb_lattice_bermudan): maturity nmat * period, exercisable at every
+// m * period (exercise = 1), knocked out at or below barrier on those dates (barrier >
+// 0).  The squarings run as in opb_batch_execute; then per date one batched tensor-core
+// product P1_i . V_i over all lattices and one FP64 step.  quotes: device [nlat][nK] FP64,
+// the values at each lattice's y0.  No host synchronisation, no allocation.
+OPB_API int opb_batch_execute_bermudan(opb_batch_plan *P, int put, int exercise, double barrier, double *quotes) {
+    OPB_REQUIRE(P && quotes, OPB_E_NULL);
+    OPB_REQUIRE(put >= 0 && put <= 1 && exercise >= 0 && exercise <= 1 && barrier >= 0.0, OPB_E_ARG);
+    cudaStream_t s = opb::stream();
+    int r = 0;
+#define BT(expr)                                  \
+    do {                                          \
+        r = (expr);                               \
+        if (r != 0) return set_status(r);         \
+    } while (0)
+    if (!tc_mode_b(P->mode)) {
+        for (int i = 0; i < P->nlat; i++)
+            BT(opb_lattice_bermudan(reinterpret_cast<const opb_lattice_desc *>(&P->fp32_desc[i]), P->mode, put,
+                                    exercise, barrier, P->fp32_ws[0], P->fp32_ws_bytes, quotes + (size_t)i * P->nK));
+        return set_status(OPB_OK);
+    }
+    BT(batch_square(P, s));
+    BT(opb::launch_berm_batched_init(P->lats, P->nlat, P->total_rows, P->nK, P->ldk, P->x, P->strikes, put, barrier,
+                                     P->f16, s));
+    for (int m = P->nmat - 1; m >= 0; m--) {
+        BT(opb::launch_tc_gemm_batched(64, P->maps_berm, P->price, P->work + P->gemm_price.off, P->gemm_price.n,
+                                       P->grid, s, P->f16, 1));
+        BT(opb::launch_berm_batched_step(P->lats, P->nlat, P->total_rows, P->nK, P->ldk, P->x, P->strikes, put,
+                                         barrier, exercise, m == 0, P->f16, quotes, s));
     }
 #undef BT
     return set_status(OPB_OK);

@@ -47,8 +47,9 @@ struct BatchLattice {
     float *E;             // d x d FP32 (E-form, then P1)
     float *Pa;            // d x d FP32 chain product
     float *V;             // d x ldk FP32 pricing result
-    __nv_bfloat16 *GThi, *GTlo;  // ldk x d payoff splits
+    __nv_bfloat16 *GThi, *GTlo;  // ldk x d payoff splits (or, in the induction, d x ldk value splits)
     float *gscale;        // device scalar: FP16 payoff split scale
+    double *Vd;           // d x ldk FP64 option values of the backward induction
 };
 // Renormalisation staging: tiles in flight per block, and column tiles per batched work
 // item (a batched item renormalises the tiles chunk, chunk + renorm_chunks(d), ... of one
@@ -63,6 +64,14 @@ struct RenormProblem {
     __nv_bfloat16 *Ahi, *Alo, *Bhi, *Blo;
     double2 *fix;  // mode-0 items: per-row (s, inv) for the next product's Cin (cin_fix)
 };
+// Batched backward induction over all lattices of a sweep (lattice_kernels.cu): per-lattice
+// split scales, terminal values and one induction date (quotes [nlat][nK] at the last)
+int launch_berm_batched_init(const BatchLattice *lats, int nlat, long long total_rows, int nK, int ldk,
+                             const double *x, const double *strikes, int put, double barrier, int f16,
+                             cudaStream_t s);
+int launch_berm_batched_step(const BatchLattice *lats, int nlat, long long total_rows, int nK, int ldk,
+                             const double *x, const double *strikes, int put, double barrier, int exercise,
+                             int last, int f16, double *quotes, cudaStream_t s);
 // Bermudan / barrier backward induction (lattice_kernels.cu)
 int launch_berm_scale(int d, const double *x, int nK, const double *K, int put, float *out, cudaStream_t s);
 int launch_berm_init(int d, int nK, int ldk, const double *x, const double *K, int put, double barrier, double *V,

@@ -701,6 +701,129 @@ __global__ void k_payoff_scale_batched(const BatchLattice *__restrict__ lats, co
     }
 }
 
+// ---- batched backward induction: lattice i's values live at rows row_off_i .. + d_i of
+// the concatenated row space; V_i = Vd_i (FP64, d x ldk), its split parts in GThi/GTlo
+// read as d x ldk row-major (the K x N operand of the induction product)
+
+__device__ __forceinline__ int lattice_of_row(const BatchLattice *__restrict__ lats, int nlat, long long grow) {
+    int lo = 0, hi = nlat - 1;
+    while (lo < hi) {  // last lattice with row_off <= grow
+        int mid = (lo + hi + 1) >> 1;
+        if (lats[mid].row_off <= grow) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Per-lattice FP16 split scales of the option values (one block per lattice): a power of
+// two from the largest exercise value, as k_berm_scale.
+__global__ void k_berm_scale_batched(const BatchLattice *__restrict__ lats, const double *__restrict__ x, int nK,
+                                     const double *__restrict__ strikes, int put) {
+    const BatchLattice &L = lats[blockIdx.x];
+    __shared__ double s0[256], s1[256];
+    double a = -1e300, b = 1e300;  // calls: max x, min K; puts: max K, min x
+    for (int i = threadIdx.x; i < L.d; i += blockDim.x) {
+        if (put) b = fmin(b, x[L.row_off + i]);
+        else a = fmax(a, x[L.row_off + i]);
+    }
+    for (int i = threadIdx.x; i < nK; i += blockDim.x) {
+        const double k = strikes[(long long)blockIdx.x * nK + i];
+        if (put) a = fmax(a, k);
+        else b = fmin(b, k);
+    }
+    s0[threadIdx.x] = a;
+    s1[threadIdx.x] = b;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            s0[threadIdx.x] = fmax(s0[threadIdx.x], s0[threadIdx.x + o]);
+            s1[threadIdx.x] = fmin(s1[threadIdx.x], s1[threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double g = s0[0] - s1[0];
+        int e = g > 0.0 ? (int)floor(log2(16384.0 / g)) : 0;
+        e = e < 0 ? 0 : (e > 60 ? 60 : e);
+        L.gscale[0] = (float)ldexp(1.0, e);
+    }
+}
+
+// Terminal values of every lattice (as k_berm_init).
+__global__ void k_berm_init_batched(const BatchLattice *__restrict__ lats, int nlat, long long total_rows, int nK,
+                                    int ldk, const double *__restrict__ x, const double *__restrict__ strikes, int put,
+                                    double barrier, int f16) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= total_rows * ldk) return;
+    const long long grow = t / ldk;
+    const int k = (int)(t - grow * ldk);
+    const int i = lattice_of_row(lats, nlat, grow);
+    const BatchLattice &L = lats[i];
+    const long long o = (grow - L.row_off) * ldk + k;
+    double v = k < nK ? berm_exercise(x[grow], strikes[(long long)i * nK + k], put) : 0.0;
+    if (barrier > 0.0 && x[grow] <= barrier) v = 0.0;
+    L.Vd[o] = v;
+    __nv_bfloat16 h, l;
+    split2((float)v, h, l, f16 ? L.gscale[0] : 0.f);
+    L.GThi[o] = h;
+    L.GTlo[o] = l;
+}
+
+// One induction date of every lattice from its product C_i = P1_i . V_i in L.V (as
+// k_berm_step); at the last date (t = 0) quotes[i*nK + k] = V_i[y0_i, k] and no parts.
+__global__ void k_berm_step_batched(const BatchLattice *__restrict__ lats, int nlat, long long total_rows, int nK,
+                                    int ldk, const double *__restrict__ x, const double *__restrict__ strikes,
+                                    int put, double barrier, int exercise, int last, int f16,
+                                    double *__restrict__ quotes) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= total_rows * ldk) return;
+    const long long grow = t / ldk;
+    const int k = (int)(t - grow * ldk);
+    const int i = lattice_of_row(lats, nlat, grow);
+    const BatchLattice &L = lats[i];
+    const int z = (int)(grow - L.row_off);
+    const long long o = (long long)z * ldk + k;
+    const float sscale = f16 ? L.gscale[0] : 0.f;
+    double v = 0.0;
+    if (k < nK) {
+        v = exp(-L.rate * L.period) * (double)L.V[o];
+        if (f16) v /= (double)sscale;
+        if (!last) {
+            if (barrier > 0.0 && x[grow] <= barrier) v = 0.0;
+            else if (exercise) v = fmax(v, berm_exercise(x[grow], strikes[(long long)i * nK + k], put));
+        }
+    }
+    L.Vd[o] = v;
+    if (!last) {
+        __nv_bfloat16 h, l;
+        split2((float)v, h, l, sscale);
+        L.GThi[o] = h;
+        L.GTlo[o] = l;
+    } else if (z == L.y0 && k < nK) {
+        quotes[(long long)i * nK + k] = v;
+    }
+}
+
+int launch_berm_batched_init(const BatchLattice *lats, int nlat, long long total_rows, int nK, int ldk,
+                             const double *x, const double *strikes, int put, double barrier, int f16,
+                             cudaStream_t s) {
+    const long long n = total_rows * ldk;
+    if (n <= 0) return OPB_OK;
+    if (f16) k_berm_scale_batched<<<nlat, 256, 0, s>>>(lats, x, nK, strikes, put);
+    k_berm_init_batched<<<blocks_for(n, 256), 256, 0, s>>>(lats, nlat, total_rows, nK, ldk, x, strikes, put, barrier,
+                                                          f16);
+    return (int)cudaGetLastError();
+}
+
+int launch_berm_batched_step(const BatchLattice *lats, int nlat, long long total_rows, int nK, int ldk,
+                             const double *x, const double *strikes, int put, double barrier, int exercise,
+                             int last, int f16, double *quotes, cudaStream_t s) {
+    const long long n = total_rows * ldk;
+    if (n <= 0) return OPB_OK;
+    k_berm_step_batched<<<blocks_for(n, 256), 256, 0, s>>>(lats, nlat, total_rows, nK, ldk, x, strikes, put, barrier,
+                                                          exercise, last, f16, quotes);
+    return (int)cudaGetLastError();
+}
+
 int launch_payoff_batched(const BatchLattice *lats, int nlat, long long total_rows, int nK, int ldk, const double *x,
                           const double *strikes, cudaStream_t s, int f16) {
     long long n = total_rows * ldk;

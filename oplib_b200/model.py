@@ -300,6 +300,17 @@ class Batch:
         call("opb_batch_execute", self.plan, _ptr(quotes))
         return quotes
 
+    def execute_bermudan(self, put: bool = True, exercise: bool = True, barrier: float = 0.0,
+                         quotes: torch.Tensor | None = None) -> torch.Tensor:
+        """Values [nlat, nK] (FP64) at each lattice's y0 of calls or puts of maturity
+        nmat*period by backward induction on the period kernels, exercisable at every
+        m*period (``exercise``) and knocked out at or below ``barrier`` on those dates."""
+        if quotes is None:
+            quotes = torch.empty(self.nlat, self.nK, dtype=torch.float64, device=self.device)
+        bind_stream(self.device)
+        call("opb_batch_execute_bermudan", self.plan, int(put), int(exercise), float(barrier), _ptr(quotes))
+        return quotes
+
     def launches(self) -> int:
         return _lib.load().opb_batch_launches(self.plan)
 

@@ -100,3 +100,38 @@ def test_bermudan_ragged_strike_count(cuda):
     q = lat.bermudan(K, cfg.nmat, cfg.period, cfg.dt0, mode="bf16x3", put=True, exercise=True)
     assert q.shape == (5,)
     assert np.abs(q.cpu().numpy() - ref).max() <= TOL
+
+
+@pytest.mark.parametrize("mode", ["fp16x3", "bf16x3", "fp32"])
+def test_batched_bermudan_matches_single_lattices(cuda, mode):
+    """Seven uneven local-vol lattices (sizes 256..1024, three of them odd multiples of 128)
+    priced together by opb_batch_execute_bermudan against one opb_lattice_bermudan per
+    lattice, under every launch configuration of the squarings; and one lattice against
+    the FP64 induction oracle."""
+    from oplib_b200.model import Batch, Lattice
+    rng = np.random.default_rng(11)
+    sizes = [256, 384, 512, 640, 768, 1024, 896]
+    params = [dict(level=float(rng.uniform(0.15, 0.35)), skew=float(rng.uniform(-0.2, 0.2)),
+                   width=float(rng.uniform(0.3, 0.9)), rate=float(rng.uniform(0.0, 0.05))) for _ in sizes]
+    lats = [Lattice.local_vol(n=n, floor=0.01, device=cuda, **p) for n, p in zip(sizes, params)]
+    K = np.linspace(0.8, 1.25, 12)
+    nmat, period, dt0 = 4, 0.25, 2.0 ** -14
+    bt = Batch(lats, K, nmat, period, dt0, mode=mode, autotune=False)
+    for put, ex, bar in ((True, True, 0.0), (False, False, 0.85)):
+        single = np.stack([lat.bermudan(K, nmat, period, dt0, mode=mode, put=put, exercise=ex, barrier=bar)
+                           .cpu().numpy() for lat in lats])
+        for cfg in (range(8) if mode != "fp32" else [0]):
+            if mode != "fp32":
+                bt.set_config(cfg)
+            q = bt.execute_bermudan(put=put, exercise=ex, barrier=bar).cpu().numpy()
+            assert q.shape == (len(lats), len(K))
+            assert np.abs(q - single).max() <= 1e-7, (mode, cfg, put, np.abs(q - single).max())
+    # the 512-node lattice against the oracle
+    i = 2
+    x = lats[i].x.cpu().numpy()
+    p = params[i]
+    sig = O.lv_sigma(x, p["level"], p["skew"], p["width"], 0.01)
+    L = O.lv_generator_fast(x, p["rate"] * x, sig * x)
+    ref = O.bermudan_fp64(L, x, K, p["rate"], period, nmat, dt0, put=True, exercise=True)[lats[i].y0]
+    q = bt.execute_bermudan(put=True, exercise=True).cpu().numpy()[i]
+    assert np.abs(q - ref).max() <= TOL
