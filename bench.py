@@ -704,7 +704,16 @@ def run_batch(args):
         errs = {int(i): float((q[i] - refs[i]).abs().max().item()) for i in sample}
         # whole-sweep time of every configuration (the autotuner picks on level 0 alone)
         sweep_ms = []
+        berm = None
         if mname == "fp16x3":
+            # Bermudan puts on every lattice (32 strikes, 8 quarterly exercise dates) by
+            # backward induction on the same plan: squarings plus 8 batched induction products
+            qb = torch.empty(nlat, 32, dtype=torch.float64, device=dev)
+            b.execute_bermudan(put=True, exercise=True, quotes=qb)
+            ms_b = _time(lambda: b.execute_bermudan(put=True, exercise=True, quotes=qb), max(2, args.steps), stream,
+                         torch)
+            berm = {"quotes_per_s": round(nlat * 32 / (ms_b * 1e-3), 1), "ms_per_sweep": round(ms_b, 3),
+                    "quotes_per_sweep": nlat * 32}
             chosen = b.config
             for cfg in range(_lib.load().opb_batch_num_configs()):
                 b.set_config(cfg)
@@ -712,7 +721,7 @@ def run_batch(args):
                 sweep_ms.append(round(_time(lambda: b.execute(q), 2, stream, torch), 2))
             b.set_config(chosen)
         res[mname] = dict(ms=ms, plan_s=t_plan, tune=b.tune_ms, cfg=b.config, launches=b.launches(), errs=errs,
-                          q=q, plans=b.plans, sweep_ms=sweep_ms)
+                          q=q, plans=b.plans, sweep_ms=sweep_ms, berm=berm)
         del g, b
     prim = res["fp16x3"]
     ms = prim["ms"]
@@ -731,7 +740,8 @@ def run_batch(args):
             "launches_per_sweep": prim["launches"], "plan_seconds": round(prim["plan_s"], 2),
             "max_abs_err_vs_fp64_sample": max(prim["errs"].values()), "sample_errs": prim["errs"],
             "bf16x3": {"quotes_per_s": round(nquotes / (res["bf16x3"]["ms"] * 1e-3), 1),
-                       "max_abs_err_vs_fp64_sample": max(res["bf16x3"]["errs"].values())}}
+                       "max_abs_err_vs_fp64_sample": max(res["bf16x3"]["errs"].values())},
+            "bermudan_puts_fp16x3": prim["berm"]}
     q = prim["q"]
     b = type("P", (), {"plans": prim["plans"]})
     if args.compare:
