@@ -282,6 +282,8 @@ struct TcParams {
     float *ypart;
     int group_m;  // M-tiles per raster group of a single product (0: 8)
     const double2 *cin_fix;  // as TcGemmArgs::cin_fix
+    int ksplit;              // as TcGemmArgs::ksplit (single products; 0 or 1: none)
+    long long c_slice;       // elements between the K-slices' partial outputs
 };
 
 // Batched launches read per-problem tensor maps (4 per problem: Ahi, Alo, Bhi, Blo) and
@@ -329,20 +331,26 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mtiles = p.M / Cfg::TILE_M, ntiles_n = p.N / BN;
-    const int nitems = BATCHED ? bt.nwork : mtiles * ntiles_n;
+    const int nsplit = (!BATCHED && p.ksplit > 1) ? p.ksplit : 1;  // K-slices of a single product
+    const int nitems = BATCHED ? bt.nwork : mtiles * ntiles_n * nsplit;
     // pair mode: rank within the 2-CTA cluster, items walked per cluster
     const uint32_t rank = PAIR ? cluster_rank() : 0u;
     const int item0 = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
     const int istep = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
-    // item t -> (problem, m0, n0, K-blocks)
-    auto get_item = [&](int t, int &prob, int &m0, int &n0, int &nkb) {
+    // item t -> (problem, m0, n0, K-blocks, first K-block, K-slice); a single product split
+    // into nsplit K-slices has nsplit consecutive items per output tile
+    auto get_item = [&](int t, int &prob, int &m0, int &n0, int &nkb, int &kb0, int &slice) {
         if constexpr (BATCHED) {
             const uint32_t w = bt.work[t];
             prob = (int)(w >> 16);
             m0 = (int)((w >> 8) & 255u) * Cfg::TILE_M;  // pair mode: 256-row items
             n0 = (int)(w & 255u) * BN;
             nkb = bt.probs[prob].K / BK;
+            kb0 = 0;
+            slice = 0;
         } else {
+            slice = t % nsplit;
+            t /= nsplit;
             const int GM = p.group_m > 0 ? p.group_m : 8;
             const int per_group = GM * ntiles_n;
             const int group = t / per_group;
@@ -352,7 +360,8 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             prob = 0;
             m0 = (first_m + r % gm) * Cfg::TILE_M;
             n0 = (r / gm) * BN;
-            nkb = p.K / BK;
+            nkb = p.K / BK / nsplit;
+            kb0 = slice * nkb;
         }
     };
 
@@ -396,8 +405,8 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             long kbg = 0;  // K-blocks issued over the CTA's lifetime (stage ring position)
             bool ok = true;
             for (int t = item0; t < nitems && ok; t += istep) {
-                int prob, m0, n0, nkb;
-                get_item(t, prob, m0, n0, nkb);
+                int prob, m0, n0, nkb, kb0, slice;
+                get_item(t, prob, m0, n0, nkb, kb0, slice);
                 const int ma = m0 + (int)rank * TC_BM;          // this CTA's A rows
                 const int nb = n0 + (int)rank * Cfg::B_ROWS;    // this CTA's B rows
                 const CUtensorMap *mp[4] = {&mAhi, &mAlo, &mBhi, &mBlo};
@@ -412,7 +421,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                         break;
                     }
                     const uint32_t st = base + s * Cfg::STAGE_BYTES;
-                    const int kx = kb * BK;
+                    const int kx = (kb0 + kb) * BK;
                     if constexpr (PAIR) {
                         // both CTAs' copies complete on the leader's full barrier
                         if (rank == 0) mbar_expect_tx(full_bar(s), 2 * Cfg::STAGE_BYTES);
@@ -474,8 +483,8 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             long kbg = 0, g = 0;  // K-blocks consumed, chunks issued
             bool ok = true;
             for (int t = item0; t < nitems && ok; t += istep) {
-                int prob, m0, n0, nkb;
-                get_item(t, prob, m0, n0, nkb);
+                int prob, m0, n0, nkb, kb0, slice;
+                get_item(t, prob, m0, n0, nkb, kb0, slice);
                 const int nch = (nkb + Cfg::CHUNK - 1) / Cfg::CHUNK;
                 for (int c = 0; c < nch && ok; c++, g++) {
                     const int a = (int)(g & 1);
@@ -545,8 +554,8 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
         long g = 0;
         bool ok = true;
         for (int t = item0; t < nitems && ok; t += istep) {
-            int prob, m0, n0, nkb;
-            get_item(t, prob, m0, n0, nkb);
+            int prob, m0, n0, nkb, kb0, slice;
+            get_item(t, prob, m0, n0, nkb, kb0, slice);
             const int nch = (nkb + Cfg::CHUNK - 1) / Cfg::CHUNK;
             if constexpr (NPROD != 1) {  // single products have one chunk: its values are the sums
 #pragma unroll
@@ -614,7 +623,8 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                 C = pr.C; Cin = pr.Cin; ldc = pr.ldc; alpha = pr.alpha; beta = pr.beta; rowsum = pr.rowsum; M = pr.M;
                 fix = pr.cin_fix;
             } else {
-                C = p.C; Cin = p.Cin; ldc = p.ldc; alpha = p.alpha; beta = p.beta; rowsum = p.rowsum; M = p.M;
+                C = p.C + (long long)slice * p.c_slice;  // K-slices write separate partial outputs
+                Cin = p.Cin; ldc = p.ldc; alpha = p.alpha; beta = p.beta; rowsum = p.rowsum; M = p.M;
                 fix = p.cin_fix;
             }
             const int row = m0 + (int)rank * TC_BM + q * 32 + lane;
@@ -830,6 +840,16 @@ static int tile_for(int M, int N) {
     return bn;
 }
 
+int tc_gemm_split_for(int M, int N, int K) {
+    const int bn = tile_for(M, N);
+    if (!bn || M % TC_BM) return 1;
+    const long long tiles = (long long)(M / TC_BM) * (N / bn);
+    int sp = (int)(2LL * num_sms() / (tiles > 0 ? tiles : 1));
+    sp = sp < 1 ? 1 : (sp > 4 ? 4 : sp);
+    while (sp > 1 && (K / TC_BK) % sp) sp--;
+    return sp;
+}
+
 // Row-sum partials: one per 128-column group (64 for the 64-wide tile).
 int tc_gemm_nparts(int M, int N) {
     int bn = tile_for(M, N);
@@ -847,6 +867,10 @@ int tc_gemm_check(const TcGemmArgs &a) {
     if ((a.lda * 2) % 16 || (a.ldb * 2) % 16 || a.ldc % 4 || !aligned(a.C, 16)) return OPB_E_ALIGN;
     if (a.Cin && !aligned(a.Cin, 16)) return OPB_E_ALIGN;
     if (a.cin_fix && !aligned(a.cin_fix, 16)) return OPB_E_ALIGN;
+    if (a.ksplit > 1) {
+        if (a.Cin || a.rowsum || a.ksplit > 64 || (a.K / TC_BK) % a.ksplit) return OPB_E_ARG;
+        if (a.c_slice < (long long)a.M * a.ldc || a.c_slice % 4) return OPB_E_ARG;
+    }
     return OPB_OK;
 }
 
@@ -880,7 +904,9 @@ static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
     p.group_m = g_group_m;
     p.cin_fix = a.cin_fix;
-    const int ntiles = (a.M / TC_BM) * (a.N / BN);
+    p.ksplit = a.ksplit > 1 ? a.ksplit : 1;
+    p.c_slice = a.c_slice;
+    const int ntiles = (a.M / TC_BM) * (a.N / BN) * p.ksplit;
     const int grid = ntiles < num_sms() ? ntiles : num_sms();
     TcBatch none{nullptr, nullptr, nullptr, 0};
     k_tc_gemm<BN, STAGES, false, F16, 3, 0, BK, false, BMN><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl,
@@ -1072,7 +1098,7 @@ int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, 
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
     int c = tc_gemm_check(a);
     if (c != OPB_OK) return c;
-    const bool pair = g_pair && a.M % (2 * TC_BM) == 0;
+    const bool pair = g_pair && a.M % (2 * TC_BM) == 0 && a.ksplit <= 1;
     if (a.b_kn) {  // MN-major B (K x N): BK = 64 only
         switch (tile_for(a.M, a.N) * 2 + (a.f16 ? 1 : 0)) {
             case 512:

@@ -82,7 +82,8 @@ Bufs carve(Ws &w, int d, int nK, int mode) {
     b.X = w.take<float>(dd);
     b.Pa = w.take<float>(dd);
     if (!tc_mode(mode)) b.Pb = w.take<float>(dd);
-    b.V = w.take<float>((size_t)d * nK);
+    // the small-N products (pricing, induction) may run as up to 4 K-slices
+    b.V = w.take<float>((size_t)d * nK * (tc_mode(mode) ? 4 : 1));
     b.gscale = w.take<float>(64);
     if (tc_mode(mode)) {
         b.Ahi = w.take<__nv_bfloat16>(dd);
@@ -171,7 +172,7 @@ int g_ksplit = 0;
 int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s) {
     int S = g_ksplit > 0 ? g_ksplit : 1;
     int kb = a.K / 64;
-    if (S <= 1 || kb < S || kb % S) return opb::launch_tc_gemm(a, s);
+    if (S <= 1 || kb < S || kb % S || a.ksplit > 1) return opb::launch_tc_gemm(a, s);
     const int kslice = a.K / S;
     for (int i = 0; i < S; i++) {
         opb::TcGemmArgs t = a;
@@ -250,6 +251,9 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
     pg.M = d; pg.N = nKp; pg.K = d; pg.lda = d; pg.ldb = d; pg.ldc = nKp; pg.f16 = g.f16;
     pg.Ahi = b.Ahi; pg.Alo = b.Alo; pg.Bhi = b.GThi; pg.Blo = b.GTlo; pg.C = b.V; pg.beta = 0.f;
     pg.alpha = f16 ? 1.f / F16_SCALE : 1.f;  // the payoff scale is undone in the FP64 discount
+    // K-slices fill the GPU with this small-N product's tiles; the discount sums them
+    pg.ksplit = opb::tc_gemm_split_for(d, nKp, d);
+    pg.c_slice = (long long)d * nKp;
     for (int m = 1; m <= L.nmat; m++) {
         if (m > 1) {
             // P_m = P_{m-1} . P1 (A splits hold P_{m-1}, B splits P1), renormalise, split
@@ -261,7 +265,7 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
         LT(tc_gemm_ksplit(pg, s));
         const double disc = std::exp(-L.rate * L.period * m);
         LT(opb::launch_discount(d, nK, nKp, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d * nK : nullptr, L.y0,
-                                quotes + (size_t)(m - 1) * nK, s, gs));
+                                quotes + (size_t)(m - 1) * nK, s, gs, pg.ksplit, pg.c_slice));
     }
     return 0;
 }
@@ -286,13 +290,15 @@ int bermudan_tc(const opb_lattice_desc &L, Bufs &b, int put, int exercise, doubl
     pg.M = d; pg.N = nKp; pg.K = d; pg.lda = d; pg.ldb = nKp; pg.ldc = nKp; pg.f16 = f16 ? 1 : 0; pg.b_kn = 1;
     pg.Ahi = b.Ahi; pg.Alo = b.Alo; pg.Bhi = b.GThi; pg.Blo = b.GTlo; pg.C = b.V; pg.beta = 0.f;
     pg.alpha = f16 ? 1.f / F16_SCALE : 1.f;  // the P1 part scale; V's scale is undone in the step
+    pg.ksplit = opb::tc_gemm_split_for(d, nKp, d);  // K-slices, summed by the step
+    pg.c_slice = (long long)d * nKp;
     const double disc = std::exp(-L.rate * L.period);
     for (int m = L.nmat - 1; m >= 0; m--) {
         LT(tc_gemm_ksplit(pg, s));
         const bool last = m == 0;
         LT(opb::launch_berm_step(d, nK, nKp, b.V, disc, L.x, L.strikes, put, last ? 0.0 : barrier,
                                  last ? 0 : exercise, b.Vd, last ? nullptr : b.GThi, last ? nullptr : b.GTlo, nullptr,
-                                 gs, L.y0, last ? quotes : nullptr, s));
+                                 gs, L.y0, last ? quotes : nullptr, s, pg.ksplit, pg.c_slice));
     }
     return 0;
 }

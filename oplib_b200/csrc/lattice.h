@@ -36,8 +36,10 @@ int launch_add_identity(int d, float *X, cudaStream_t s);
 int launch_payoff_scale(int d, const double *x, int nK, const double *K, float *out, cudaStream_t s);
 int launch_payoff(int d, int nK, int ldk, const double *x, const double *K, float *G, __nv_bfloat16 *GThi,
                   __nv_bfloat16 *GTlo, cudaStream_t s, const float *dscale = nullptr);
+// V32 may hold nslice K-slices' partial products slice_stride elements apart, summed in
+// FP64 in slice order
 int launch_discount(int d, int nK, int ldk, const float *V32, double disc, double *V64, int y0, double *quotes,
-                    cudaStream_t s, const float *dscale = nullptr);
+                    cudaStream_t s, const float *dscale = nullptr, int nslice = 1, long long slice_stride = 0);
 
 // Batched lattice tables (device memory).
 struct BatchLattice {
@@ -78,7 +80,8 @@ int launch_berm_init(int d, int nK, int ldk, const double *x, const double *K, i
                      __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo, float *Vf, const float *dscale, cudaStream_t s);
 int launch_berm_step(int d, int nK, int ldk, const float *C, double disc, const double *x, const double *K, int put,
                      double barrier, int exercise, double *V, __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo, float *Vf,
-                     const float *dscale, int y0, double *quotes, cudaStream_t s);
+                     const float *dscale, int y0, double *quotes, cudaStream_t s, int nslice = 1,
+                     long long slice_stride = 0);
 int launch_renorm_to_p(int d, float *X, const double *partial, int nparts, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
                        __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, cudaStream_t s, float sscale = 0.f);
 // work items: problem << 16 | mode << 14 | strip << 7 | chunk (see renorm_chunks)
@@ -110,7 +113,13 @@ struct TcGemmArgs {
     // epilogue reads Cin[r][c] as (float)((Cin[r][c] - (r == c ? s : 0)) * inv)
     const double2 *cin_fix;
     int b_kn;  // 1: B parts stored K x N row-major (ldb >= N; read as an MN-major operand)
+    // > 1: the product runs as ksplit K-slices written to C + s * c_slice (s < ksplit) for the
+    // caller to sum; needs no Cin and no rowsum, (K / 64) % ksplit == 0, c_slice >= M * ldc
+    int ksplit;
+    long long c_slice;
 };
+// K-slices that fill the GPU with the tiles of a small-N product (1 = none), at most 4
+int tc_gemm_split_for(int M, int N, int K);
 int tc_gemm_tile_n(int N);                    // tile width chosen for N (0 if unsupported)
 int tc_gemm_check(const TcGemmArgs &a);       // argument/alignment check, OPB_* code
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s);

@@ -489,15 +489,23 @@ __global__ void k_payoff(int d, int nK, int ldk, const double *__restrict__ x, c
     }
 }
 
-// V64[y, k] = disc * V32[y, k] / gscale (V32 leading dimension ldk >= nK; gscale = the
-// payoff split scale, 1 without one); quotes[k] = V64[y0, k].
+// FP64 sum of the K-slices' partial products at offset o (slice order).
+__device__ __forceinline__ double sum_slices(const float *__restrict__ P, long long o, int nslice, long long stride) {
+    double v = (double)P[o];
+    for (int sl = 1; sl < nslice; sl++) v += (double)P[o + sl * stride];
+    return v;
+}
+
+// V64[y, k] = disc * V32[y, k] / gscale (V32 leading dimension ldk >= nK, summed over its
+// nslice K-slices; gscale = the payoff split scale, 1 without one); quotes[k] = V64[y0, k].
 __global__ void k_discount(int d, int nK, int ldk, const float *__restrict__ V32, double disc,
-                           double *__restrict__ V64, int y0, double *__restrict__ quotes, const float *__restrict__ dscale) {
+                           double *__restrict__ V64, int y0, double *__restrict__ quotes, const float *__restrict__ dscale,
+                           int nslice, long long slice_stride) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)d * nK) return;
     int y = (int)(t / nK), k = (int)(t - (long long)y * nK);
     if (dscale) disc /= (double)*dscale;
-    double v = disc * (double)V32[(long long)y * ldk + k];
+    double v = disc * sum_slices(V32, (long long)y * ldk + k, nslice, slice_stride);
     if (V64) V64[t] = v;
     if (quotes && y == y0) quotes[k] = v;
 }
@@ -575,14 +583,14 @@ __global__ void k_berm_step(int d, int nK, int ldk, const float *__restrict__ C,
                             const double *__restrict__ x, const double *__restrict__ K, int put, double barrier,
                             int exercise, double *__restrict__ V, __nv_bfloat16 *__restrict__ Vhi,
                             __nv_bfloat16 *__restrict__ Vlo, float *__restrict__ Vf, const float *__restrict__ dscale,
-                            int y0, double *__restrict__ quotes) {
+                            int y0, double *__restrict__ quotes, int nslice, long long slice_stride) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)d * ldk) return;
     const int z = (int)(t / ldk), k = (int)(t - (long long)z * ldk);
     const float sscale = dscale ? *dscale : 0.f;
     double v = 0.0;
     if (k < nK) {
-        v = disc * (double)C[t];
+        v = disc * sum_slices(C, t, nslice, slice_stride);
         if (dscale) v /= (double)sscale;
         if (barrier > 0.0 && x[z] <= barrier) v = 0.0;
         else if (exercise) v = fmax(v, berm_exercise(x[z], K[k], put));
@@ -897,17 +905,19 @@ int launch_berm_init(int d, int nK, int ldk, const double *x, const double *K, i
 
 int launch_berm_step(int d, int nK, int ldk, const float *C, double disc, const double *x, const double *K, int put,
                      double barrier, int exercise, double *V, __nv_bfloat16 *Vhi, __nv_bfloat16 *Vlo, float *Vf,
-                     const float *dscale, int y0, double *quotes, cudaStream_t s) {
+                     const float *dscale, int y0, double *quotes, cudaStream_t s, int nslice,
+                     long long slice_stride) {
     const long long n = (long long)d * ldk;
     k_berm_step<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, C, disc, x, K, put, barrier, exercise, V, Vhi, Vlo,
-                                                   Vf, dscale, y0, quotes);
+                                                   Vf, dscale, y0, quotes, nslice > 1 ? nslice : 1, slice_stride);
     return (int)cudaGetLastError();
 }
 
 int launch_discount(int d, int nK, int ldk, const float *V32, double disc, double *V64, int y0, double *quotes,
-                    cudaStream_t s, const float *dscale) {
+                    cudaStream_t s, const float *dscale, int nslice, long long slice_stride) {
     long long n = (long long)d * nK;
-    k_discount<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, V32, disc, V64, y0, quotes, dscale);
+    k_discount<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, V32, disc, V64, y0, quotes, dscale,
+                                                  nslice > 1 ? nslice : 1, slice_stride);
     return (int)cudaGetLastError();
 }
 

@@ -50,7 +50,9 @@ def test_batch_vs_fp64_and_single(batch_and_refs):
         print(f"lattice {i} d={lat.d}: max abs err vs FP64 {err:.2e}")
         assert err <= 1e-5, (i, err)
         qs, _ = lat.solve(STRIKES, NMAT, PERIOD, DT0, mode="bf16x3")
-        assert np.abs(q[i] - qs.cpu().numpy()).max() < 2e-7
+        # the single solve's pricing products run as K-slices summed in FP64 (they have too
+        # few tiles to fill the GPU), the batch's in one pass: FP32 rounding differences only
+        assert np.abs(q[i] - qs.cpu().numpy()).max() < 1e-6
 
 
 def test_batch_configs_agree(batch_and_refs):

@@ -125,7 +125,9 @@ def test_batched_bermudan_matches_single_lattices(cuda, mode):
                 bt.set_config(cfg)
             q = bt.execute_bermudan(put=put, exercise=ex, barrier=bar).cpu().numpy()
             assert q.shape == (len(lats), len(K))
-            assert np.abs(q - single).max() <= 1e-7, (mode, cfg, put, np.abs(q - single).max())
+            # the single-lattice induction products run as K-slices summed in FP64, the
+            # batched ones in one pass: the two differ by FP32 rounding only
+            assert np.abs(q - single).max() <= 1e-6, (mode, cfg, put, np.abs(q - single).max())
     # the 512-node lattice against the oracle
     i = 2
     x = lats[i].x.cpu().numpy()
