@@ -14,6 +14,10 @@ iteration:
 3. per problem, on the host in FP64: accepts or rejects the trial, forms J^T J and J^T r
    from the bumped prices, and solves the damped 3 x 3 system for the next trial.
 
+The targets are European calls (one batched ``opb_batch_execute`` per iteration) or, with
+``contract="bermudan"``, Bermudan / down-and-out contracts priced by the batched backward
+induction (``opb_batch_execute_bermudan``).
+
 The reference lays out buffers for this loop but leaves it unwritten
 (oplib/opmodel/types/SCalBuffers.cs:9-31: the discounted kernels at lambda = 1 +- eps,
 kept for sensitivities).  Here the sensitivities come from bumped generators instead.
@@ -149,11 +153,17 @@ def best_of_starts(out, M: int):
 class LVBatchPricer:
     """Device pricer for ``lm_calibrate``: ``slots`` local-vol lattices per problem (the
     trial point and its bumps; 7 for central differences) in one batch whose generators
-    are rewritten in place per call."""
+    are rewritten in place per call.  ``contract`` selects the quotes: "european" (calls
+    at the nmat maturities m * period, nmat * nK per problem) or "bermudan" (one value per
+    strike of the contract maturing at nmat * period: calls or puts (``put``) exercisable
+    at every m * period, knocked out at or below ``barrier`` when it is positive)."""
 
     def __init__(self, n, rate, strikes, nmat: int, period: float, dt0: float = 2.0 ** -14, mode="fp16x3",
                  floor: float = 0.01, lo: float = 0.05, hi: float = 5.0, s0: float = 1.0, slots: int = 7,
-                 device="cuda"):
+                 device="cuda", contract: str = "european", put: bool = True, barrier: float = 0.0):
+        if contract not in ("european", "bermudan"):
+            raise ValueError(f"contract must be 'european' or 'bermudan', not {contract!r}")
+        self.contract, self.put, self.barrier = contract, bool(put), float(barrier)
         self.n = [int(v) for v in n]
         self.rate = [float(v) for v in rate]
         self.M = len(self.n)
@@ -167,7 +177,7 @@ class LVBatchPricer:
                                   lo=lo, hi=hi, s0=s0, device=self.device)
                 for i in range(self.M) for _ in range(self.S)]
         self.batch = Batch(lats, strikes, nmat, period, dt0, mode=mode, autotune=False)
-        self.K = nmat * self.batch.nK
+        self.K = (nmat if contract == "european" else 1) * self.batch.nK
         # one 56-byte record per lattice for opb_lv_generator_ell_batched
         nlat = self.M * self.S
         self.rec = np.zeros(nlat, dtype=LV_PARAM)
@@ -189,7 +199,10 @@ class LVBatchPricer:
         self.d_rec.copy_(self.h_rec, non_blocking=True)
         call("opb_lv_generator_ell_batched", self.M * self.S, self.d_rec.data_ptr(), self.total_rows, self.lo,
              self.hi, self.s0, self.batch.cols.data_ptr(), self.batch.vals.data_ptr())
-        q = self.batch.execute()
+        if self.contract == "european":
+            q = self.batch.execute()
+        else:
+            q = self.batch.execute_bermudan(put=self.put, exercise=True, barrier=self.barrier)
         self.calls += 1
         return q.reshape(self.M, self.S, self.K).cpu().numpy()
 
