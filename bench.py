@@ -1248,7 +1248,8 @@ def run_bermudan(args):
 
 def run_gemm(args):
     """The squaring GEMM alone (split-BF16, E-form: C = E.E + 2E in place) at size d, in the
-    solve's form: B is E's own row-major parts, read as an MN-major operand."""
+    solve's form: B is E's own row-major parts, read as an MN-major operand.  --cta-pair 0
+    runs the one-CTA 128 x 256 kernel instead of the 2-CTA pair kernel."""
     import torch
     from oplib_b200 import _lib
     from oplib_b200.model import bind_stream
@@ -1257,6 +1258,7 @@ def run_gemm(args):
     bind_stream(dev)
     lib = _lib.load()
     d = args.d
+    lib.opb_set_cta_pair(args.cta_pair)
     Ah = torch.empty(d, d, dtype=torch.bfloat16, device=dev).normal_(0, 1e-3)
     Al = torch.empty_like(Ah).normal_(0, 1e-6)
     X = torch.empty(d, d, dtype=torch.float32, device=dev).normal_()
@@ -1271,7 +1273,8 @@ def run_gemm(args):
     return {"metric": "split-BF16 GEMM MMA TFLOP/s", "value": round(tf, 1), "unit": "TFLOP/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic",
-            "config": {"workload": f"E-form squaring GEMM d={d}"}, "frac_of_peak": round(tf / peak, 4),
+            "config": {"workload": f"E-form squaring GEMM d={d}", "cta_pair": args.cta_pair},
+            "frac_of_peak": round(tf / peak, 4),
             "peak_source": src}
 
 
@@ -1294,6 +1297,8 @@ def main():
                              "refbench", "bermudan"],
                     help="sv = the headline SV lattice solve; the others are secondary measurements")
     ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
+    ap.add_argument("--cta-pair", type=int, default=1, choices=[0, 1],
+                    help="--workload gemm: 2-CTA pair kernel (1, the default) or one CTA per tile (0)")
     args = ap.parse_args()
     if args.nlat is None:
         args.nlat = 64 if args.workload == "calibrate" else 512
