@@ -335,12 +335,15 @@ int opcuda_mc_status_sz(void);
 /* replaces oplib/opcuda/smc.cu:137-156: first uint32 at host_seedptr is the base seed;
  * mtptr is the device continuation record (opcuda_mc_status_sz() words) */
 int opcuda_mc_setseed(uint64_t host_seedptr, uint64_t mtptr);
-/* replaces oplib/opcuda/smc.cu:610-656 (per-path MT19937 streams; nk <= 623, d <= 32767) */
+/* replaces oplib/opcuda/smc.cu:610-656 (per-path MT19937 streams; any nk >= 1, d <= 32767) */
 int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk, int d, uint64_t ctpker_m_yy, uint64_t m_k,
                 uint64_t yhostptr);
-/* replaces oplib/opcuda/smc.cu:731-736 (nscen % 4096 == 0, nscen/4096 <= 623) */
+/* replaces oplib/opcuda/smc.cu:731-736 (nscen % 4096 == 0) */
 int opcuda_mt_benchmark(uint64_t mtptr, uint64_t unif_ptr, int nscen);
-/* new: MT19937 Monte Carlo, path p seeded init_genrand(seed + path0 + p); see mc.cu */
+/* new: MT19937 Monte Carlo, path p seeded init_genrand(seed + path0 + p); see mc.cu.
+ * Runs of up to 623 steps keep the generator in registers; longer runs hold the
+ * 624-word state in per-thread local memory (2496 bytes a thread), which the CUDA
+ * driver may provision on the first such launch. */
 int opb_mc_scratch_blocks(long long npaths);
 int opb_mc_mt19937(const float *C, long long row_stride, long long col_stride, const uint32_t *guide, int nb, int d,
                    int y0, int nsteps, uint32_t seed, unsigned long long path0, long long npaths, short *ypaths,
@@ -351,7 +354,8 @@ int opb_mc_mt19937(const float *C, long long row_stride, long long col_stride, c
  * synchronisation).  The payoff partial sums use a fixed 64 KiB device array inside the
  * library (held by every GPU that loads it until exit); results are bit-identical to
  * opb_mc_mt19937.  Grids above 4096 blocks (devices with more than 512 SMs) return
- * OPB_E_UNSUPPORTED.  The first call on a device looks up the array's device address (make
+ * OPB_E_UNSUPPORTED, and so do runs longer than 623 steps (they would need the driver's
+ * local-memory reservation to grow).  The first call on a device looks up the array's device address (make
  * it before any stream capture); calls that overlap on the GPU share the array and race. */
 int opb_mc_mt19937_noalloc(const float *C, long long row_stride, long long col_stride, const uint32_t *guide, int nb,
                            int d, int y0, int nsteps, uint32_t seed, unsigned long long path0, long long npaths,

@@ -7,16 +7,11 @@
 // u = ((float)x + 1.0f) * 2^-32 in (0, 1] (oplib/opcuda/smc.cu:329) and moves to the
 // smallest state z with u < C[y, z], capped at d-1 (oplib/opcuda/smc.cu:336-350).
 //
-// B200 design: one thread per path with the whole generator in registers.  The first
-// n <= 623 outputs of a freshly seeded MT19937 only need one regeneration of the state,
-// and every regenerated word is an XOR of tw() terms of initial words mt[j], each of
-// which is a forward recurrence from the seed.  The kernel walks that recurrence with a
-// few cursors (and one saved word, mt[397]) instead of storing 624 words per path, so
-// no local or shared memory is used for RNG state:
-//   i <  227 : mt'[i] = mt[i+397] ^ tw(mt[i], mt[i+1])
-//   i <  454 : mt'[i] = mt[i+170] ^ tw(mt[i-227], mt[i-226]) ^ tw(mt[i], mt[i+1])
-//   i <  623 : mt'[i] = mt[i-57] ^ tw(mt[i-454], mt[i-453]) ^ tw(mt[i-227], mt[i-226])
-//                       ^ tw(mt[i], mt[i+1])
+// B200 design: one thread per path with the whole generator in registers for runs of up
+// to 623 steps (mt19937_first in mt19937.cuh walks the seeding recurrence with a few
+// cursors, no state array); longer runs keep the 624-word state in a per-thread
+// local-memory array (mt19937_any), a separate instantiation of the same kernels, so the
+// register-only form is unchanged.
 // The inverse-CDF search starts from the guide-table bracket of the previous state's row
 // (about one probe per step) and falls back to the full row without a guide table.
 // Payoffs (discretely monitored down-and-out call, arithmetic-Asian call) are reduced per
@@ -26,68 +21,9 @@
 
 #include "common.cuh"
 #include "lattice.h"
+#include "mt19937.cuh"
 
 namespace opb {
-
-__device__ __forceinline__ uint32_t mt_init_next(uint32_t v, uint32_t i) {
-    return 1812433253u * (v ^ (v >> 30)) + i;
-}
-__device__ __forceinline__ uint32_t mt_tw(uint32_t a, uint32_t b) {
-    uint32_t y = (a & 0x80000000u) | (b & 0x7fffffffu);
-    return (y >> 1) ^ ((b & 1u) ? 0x9908b0dfu : 0u);
-}
-__device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
-    y ^= (y >> 11);
-    y ^= (y << 7) & 0x9d2c5680u;
-    y ^= (y << 15) & 0xefc60000u;
-    y ^= (y >> 18);
-    return y;
-}
-
-// Calls f(k, x_k) for the first n (<= 623) outputs of MT19937 seeded with `seed`.
-template <class F>
-__device__ __forceinline__ void mt19937_first(uint32_t seed, int n, F &&f) {
-    // cursor A at i: (a0, a1) = (mt[i], mt[i+1])
-    uint32_t a0 = seed, a1 = mt_init_next(seed, 1u);
-    // cursor B at i + 397
-    uint32_t b = seed;
-#pragma unroll 1
-    for (uint32_t j = 1; j <= 397; j++) b = mt_init_next(b, j);
-    const uint32_t m397 = b;
-    uint32_t bi = 397;
-    int i = 0;
-    const int n1 = n < 227 ? n : 227;
-#pragma unroll 1
-    for (; i < n1; i++) {
-        f(i, mt_temper(b ^ mt_tw(a0, a1)));
-        a0 = a1; a1 = mt_init_next(a1, (uint32_t)i + 2u);
-        bi++; b = mt_init_next(b, bi);
-    }
-    if (i >= n) return;
-    // phase 2: cursor C at i-227 from the seed, cursor B restarted at 397
-    uint32_t c0 = seed, c1 = mt_init_next(seed, 1u);
-    b = m397; bi = 397;
-    const int n2 = n < 454 ? n : 454;
-#pragma unroll 1
-    for (; i < n2; i++) {
-        f(i, mt_temper(b ^ mt_tw(c0, c1) ^ mt_tw(a0, a1)));
-        a0 = a1; a1 = mt_init_next(a1, (uint32_t)i + 2u);
-        c0 = c1; c1 = mt_init_next(c1, (uint32_t)(i - 227) + 2u);
-        bi++; b = mt_init_next(b, bi);
-    }
-    if (i >= n) return;
-    // phase 3: cursor D at i-454 from the seed, B restarted at 397 (= i-57 at i = 454)
-    uint32_t d0 = seed, d1 = mt_init_next(seed, 1u);
-    b = m397; bi = 397;
-#pragma unroll 1
-    for (; i < n; i++) {
-        f(i, mt_temper(b ^ mt_tw(d0, d1) ^ mt_tw(c0, c1) ^ mt_tw(a0, a1)));
-        a0 = a1; a1 = mt_init_next(a1, (uint32_t)i + 2u);
-        c0 = c1; c1 = mt_init_next(c1, (uint32_t)(i - 227) + 2u);
-        d0 = d1; d1 = mt_init_next(d1, (uint32_t)(i - 454) + 2u);
-        bi++; b = mt_init_next(b, bi);
-    }
-}
 
 __device__ __forceinline__ float mt_uniform_open0(uint32_t x) {
     float f = __uint2float_rn(x);
@@ -112,6 +48,7 @@ struct McArgs {
     double *block_sums;      // [gridDim.x * 2]
 };
 
+template <bool ANY_LENGTH>
 __global__ void __launch_bounds__(256) k_mc(McArgs a) {
     double s_bar = 0.0, s_asi = 0.0;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -120,7 +57,7 @@ __global__ void __launch_bounds__(256) k_mc(McArgs a) {
         const uint32_t seed = a.seed + (uint32_t)(a.path0 + (unsigned long long)p);
         int y = a.y0;
         double xmin = 1e300, xsum = 0.0, xlast = 0.0;
-        mt19937_first(seed, a.nsteps, [&](int k, uint32_t bits) {
+        mt19937_stream<ANY_LENGTH>(seed, a.nsteps, [&](int k, uint32_t bits) {
             const float u = mt_uniform_open0(bits);
             const float *row = a.C + (long long)y * a.rs + (a.m_k ? (long long)__ldg(a.m_k + k) * a.ms : 0LL);
             int lo = 0, hi = a.d - 1;
@@ -186,19 +123,31 @@ __global__ void k_reduce_pairs(int n, const double *__restrict__ in, double *__r
 // Uniform-generation throughput kernel (the gmt workload): stream s of nstreams writes
 // its first nper uniforms u = x * 2^-32 (oplib/opcuda/smc.cu:711-714) to
 // unif[s + nstreams*j].
+template <bool ANY_LENGTH>
 __global__ void __launch_bounds__(256) k_mt_bench(uint32_t seed, long long nstreams, int nper, float *__restrict__ unif) {
     long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (s >= nstreams) return;
-    mt19937_first(seed + (uint32_t)s, nper, [&](int j, uint32_t bits) {
+    mt19937_stream<ANY_LENGTH>(seed + (uint32_t)s, nper, [&](int j, uint32_t bits) {
         unif[s + nstreams * (long long)j] = __fmul_rn(__uint2float_rn(bits), 2.3283064365386963e-10f);
     });
 }
 
 // Raw outputs, for parity tests of the generator itself: out[s*n + j].
+template <bool ANY_LENGTH>
 __global__ void k_mt_raw(uint32_t seed, long long nstreams, int n, uint32_t *__restrict__ out) {
     long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (s >= nstreams) return;
-    mt19937_first(seed + (uint32_t)s, n, [&](int j, uint32_t bits) { out[s * n + j] = bits; });
+    mt19937_stream<ANY_LENGTH>(seed + (uint32_t)s, n, [&](int j, uint32_t bits) { out[s * n + j] = bits; });
+}
+
+// The register-only generator up to 623 steps, the state-array one beyond.
+void launch_mc(int grid, const McArgs &a) {
+    if (a.nsteps <= kMtCursorMax) k_mc<false><<<grid, 256, 0, stream()>>>(a);
+    else k_mc<true><<<grid, 256, 0, stream()>>>(a);
+}
+void launch_mt_bench(int grid, uint32_t seed, long long nstreams, int nper, float *unif) {
+    if (nper <= kMtCursorMax) k_mt_bench<false><<<grid, 256, 0, stream()>>>(seed, nstreams, nper, unif);
+    else k_mt_bench<true><<<grid, 256, 0, stream()>>>(seed, nstreams, nper, unif);
 }
 
 int mc_grid(long long npaths) {
@@ -226,8 +175,7 @@ OPB_API int opb_mc_mt19937(const float *C, long long row_stride, long long col_s
                            long long npaths, short *ypaths, const double *x, double strike, double barrier,
                            double disc, double *scratch, double *sums) {
     OPB_REQUIRE(d > 0 && d <= 32767 && y0 >= 0 && y0 < d, OPB_E_ARG);
-    OPB_REQUIRE(nsteps >= 1 && nsteps <= 623, OPB_E_UNSUPPORTED);
-    OPB_REQUIRE(npaths >= 0, OPB_E_ARG);
+    OPB_REQUIRE(nsteps >= 1 && npaths >= 0, OPB_E_ARG);
     OPB_REQUIRE(C != nullptr, OPB_E_NULL);
     if (guide) OPB_REQUIRE(nb >= 1 && nb <= 4096 && (nb & (nb - 1)) == 0 && col_stride == 1, OPB_E_ARG);
     if (x) OPB_REQUIRE(scratch != nullptr && sums != nullptr, OPB_E_NULL);
@@ -241,16 +189,18 @@ OPB_API int opb_mc_mt19937(const float *C, long long row_stride, long long col_s
     a.ypaths = ypaths; a.x = x; a.strike = strike; a.barrier = barrier; a.disc = disc;
     a.block_sums = x ? scratch : nullptr;
     int grid = mc_grid(npaths);
-    k_mc<<<grid, 256, 0, stream()>>>(a);
+    launch_mc(grid, a);
     if (x) k_reduce_pairs<<<1, 256, 0, stream()>>>(grid, scratch, sums);
     return launch_check();
 }
 
 OPB_API int opb_mt19937_raw(uint32_t seed, long long nstreams, int n, uint32_t *out) {
-    OPB_REQUIRE(nstreams >= 0 && n >= 1 && n <= 623, OPB_E_ARG);
+    OPB_REQUIRE(nstreams >= 0 && n >= 1, OPB_E_ARG);
     if (nstreams == 0) return set_status(OPB_OK);
     OPB_REQUIRE(out != nullptr, OPB_E_NULL);
-    k_mt_raw<<<(int)((nstreams + 255) / 256), 256, 0, stream()>>>(seed, nstreams, n, out);
+    const int grid = (int)((nstreams + 255) / 256);
+    if (n <= kMtCursorMax) k_mt_raw<false><<<grid, 256, 0, stream()>>>(seed, nstreams, n, out);
+    else k_mt_raw<true><<<grid, 256, 0, stream()>>>(seed, nstreams, n, out);
     return launch_check();
 }
 
@@ -289,12 +239,12 @@ OPB_API int opcuda_mc_setseed(uint64_t host_seedptr, uint64_t mtptr) {
 // steps from state y0 over the column-major cumulative kernels ctpker_m_yy (kernel m_k[k]
 // at step k), writing int16 states y_sk[p + nscen*k] and copying them to yhostptr
 // (blocking, as the reference does).  Unlike the reference (d < 1024 only,
-// smc.cu:622) any d <= 32767 is accepted; nk <= 623.
+// smc.cu:622) any d <= 32767 is accepted, and any nk >= 1.
 OPB_API int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk, int d, uint64_t ctpker_m_yy,
                         uint64_t m_k, uint64_t yhostptr) {
     OPB_REQUIRE(mtptr != 0 && y_sk != 0 && ctpker_m_yy != 0 && m_k != 0, OPB_E_NULL);
     OPB_REQUIRE(d > 0 && d <= 32767 && y0 >= 0 && y0 < d && nscen >= 0, OPB_E_ARG);
-    OPB_REQUIRE(nk >= 1 && nk <= 623, OPB_E_UNSUPPORTED);
+    OPB_REQUIRE(nk >= 1, OPB_E_ARG);
     uint32_t rec[4];
     OPB_TRY(cudaMemcpyAsync(rec, reinterpret_cast<const void *>(mtptr), sizeof(rec), cudaMemcpyDeviceToHost, stream()));
     OPB_TRY(cudaStreamSynchronize(stream()));
@@ -305,7 +255,7 @@ OPB_API int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk
         a.rs = 1; a.cs = d; a.m_k = reinterpret_cast<const int *>(m_k); a.ms = (long long)d * d;
         a.d = d; a.y0 = y0; a.nsteps = nk; a.seed = rec[0]; a.path0 = path0; a.npaths = nscen;
         a.ypaths = reinterpret_cast<short *>(y_sk);
-        k_mc<<<mc_grid(nscen), 256, 0, stream()>>>(a);
+        launch_mc(mc_grid(nscen), a);
         OPB_TRY(cudaGetLastError());
     }
     path0 += (unsigned long long)nscen;
@@ -321,26 +271,25 @@ OPB_API int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk
 
 // Uniform throughput benchmark (oplib/opcuda/smc.cu:664-736): nscen uniforms from
 // opcuda_mc_nrng-independent per-stream MT19937 generators -- 4096 streams of nscen/4096
-// values each (nscen/4096 <= 623), stream s seeded with base seed + s.
+// values each, stream s seeded with base seed + s.
 OPB_API int opcuda_mt_benchmark(uint64_t mtptr, uint64_t unif_ptr, int nscen) {
     OPB_REQUIRE(mtptr != 0 && unif_ptr != 0, OPB_E_NULL);
     OPB_REQUIRE(nscen >= 0 && nscen % 4096 == 0, OPB_E_ARG);
     int nper = nscen / 4096;
-    OPB_REQUIRE(nper <= 623, OPB_E_UNSUPPORTED);
     if (nper == 0) return set_status(OPB_OK);
     uint32_t rec[4];
     OPB_TRY(cudaMemcpyAsync(rec, reinterpret_cast<const void *>(mtptr), sizeof(rec), cudaMemcpyDeviceToHost, stream()));
     OPB_TRY(cudaStreamSynchronize(stream()));
-    k_mt_bench<<<4096 / 256, 256, 0, stream()>>>(rec[0], 4096, nper, reinterpret_cast<float *>(unif_ptr));
+    launch_mt_bench(4096 / 256, rec[0], 4096, nper, reinterpret_cast<float *>(unif_ptr));
     return launch_check();
 }
 
 // Uniform generation with typed pointers: nstreams streams (seed + s) x nper values.
 OPB_API int opb_mt_uniforms(uint32_t seed, long long nstreams, int nper, float *unif) {
-    OPB_REQUIRE(nstreams >= 0 && nper >= 1 && nper <= 623, OPB_E_ARG);
+    OPB_REQUIRE(nstreams >= 0 && nper >= 1, OPB_E_ARG);
     if (nstreams == 0) return set_status(OPB_OK);
     OPB_REQUIRE(unif != nullptr, OPB_E_NULL);
-    k_mt_bench<<<(int)((nstreams + 255) / 256), 256, 0, stream()>>>(seed, nstreams, nper, unif);
+    launch_mt_bench((int)((nstreams + 255) / 256), seed, nstreams, nper, unif);
     return launch_check();
 }
 
@@ -356,7 +305,10 @@ OPB_API int opb_mt_uniforms(uint32_t seed, long long nstreams, int nper, float *
 // keeps until the process exits.  The grid is the one opb_mc_mt19937 uses for the same
 // npaths (at most 8 blocks per SM), so results are bit-identical to it; a grid larger than
 // the array -- only possible on a device with more than 512 SMs -- is rejected with
-// OPB_E_UNSUPPORTED.  All calls share the array and it keeps the last call's contents (each
+// OPB_E_UNSUPPORTED.  Runs longer than 623 steps are rejected with OPB_E_UNSUPPORTED too:
+// opb_mc_mt19937 serves them with a per-thread local-memory state array, and the CUDA
+// driver may grow its local-memory reservation for that kernel on first use, an allocation
+// this entry point exists to avoid.  All calls share the array and it keeps the last call's contents (each
 // call overwrites the partials of the blocks it launches before reading them), so calls
 // that overlap on the GPU -- concurrent streams, or several host threads -- race on it and
 // must be serialised by the caller.
@@ -396,6 +348,7 @@ OPB_API int opb_mc_mt19937_noalloc(const float *C, long long row_stride, long lo
                                    const uint32_t *guide, int nb, int d, int y0, int nsteps, uint32_t seed,
                                    unsigned long long path0, long long npaths, short *ypaths, const double *x,
                                    double strike, double barrier, double disc, double *sums) {
+    OPB_REQUIRE(nsteps <= kMtCursorMax, OPB_E_UNSUPPORTED);
     OPB_REQUIRE(npaths >= 0, OPB_E_ARG);
     OPB_REQUIRE(mc_grid(npaths) <= OPB_MC_NOALLOC_MAX_BLOCKS, OPB_E_UNSUPPORTED);
     double *scratch = nullptr;

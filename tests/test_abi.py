@@ -70,12 +70,16 @@ def test_version_and_status_strings(lib):
     (lambda L: L.opcuda_ssqmm(8, 1, 0, 1, 1), -2),
     (lambda L: L.opcuda_sck(-1, 1, 1, 1), -1),
     (lambda L: L.opcuda_sek(8, 0, 0.1, 1), -2),
-    (lambda L: L.opcuda_mc1f(1, 0, 1, 4096, 700, 64, 1, 1, 0), -4),  # nk > 623
+    (lambda L: L.opcuda_mc1f(1, 0, 1, 4096, 0, 64, 1, 1, 0), -1),  # no steps
     (lambda L: L.opcuda_mc1f(1, 70, 1, 4096, 10, 64, 1, 1, 0), -1),  # y0 >= d
     (lambda L: L.opcuda_mt_benchmark(1, 1, 4097), -1),
     (lambda L: L.opb_guide_table(64, 4, 48, 1, 1), -1),  # nb not a power of two
-    (lambda L: L.opb_mc_mt19937(1, 64, 1, None, 0, 64, 0, 624, 1, 0, 10, None, None, 1.0, 0.7, 1.0, None, None), -4),
-    (lambda L: L.opb_mt19937_raw(1, 4, 700, 1), -1),
+    (lambda L: L.opb_mc_mt19937(1, 64, 1, None, 0, 64, 0, 0, 1, 0, 10, None, None, 1.0, 0.7, 1.0, None, None), -1),
+    # runs past the register-only generator would grow the driver's local memory
+    (lambda L: L.opb_mc_mt19937_noalloc(1, 64, 1, None, 0, 64, 0, 624, 1, 0, 10, None, None, 1.0, 0.7, 1.0, None),
+     -4),
+    (lambda L: L.opb_mt19937_raw(1, 4, 0, 1), -1),
+    (lambda L: L.opb_mt_uniforms(1, 4, 0, 1), -1),
     (lambda L: L.opb_sv_generator_ell(2, 8, 0.05, 5.0, 0.05, 1.0, 0.03, 2.0, 0.04, 0.6, -0.7, 1, 1, None), -1),
     (lambda L: L.opb_lv_generator_ell(2, 1, 1, 1, 1, 1), -1),
     (lambda L: L.opcuda_sgemv(4, 4, 1.0, 0, 4, 1, 1, 0.0, 1, 1), -2),

@@ -1,6 +1,6 @@
-"""Edge cases of the device path against the oracle: empty and single inputs, the largest
-supported step count, ragged sizes, degenerate guide tables and pricing grids, and the
-rejections that guard the supported range."""
+"""Edge cases of the device path against the oracle: empty and single inputs, the step
+counts on either side of the register-only generator's limit, ragged sizes, degenerate
+guide tables and pricing grids, and the rejections that guard the supported range."""
 import math
 
 import numpy as np
@@ -33,8 +33,8 @@ def test_mc_no_paths_gives_zero_sums(rows):
 
 
 def test_mc_single_path_longest_run_bit_exact(rows):
-    """One path of 623 steps, the most a fresh MT19937 state serves without a second
-    regeneration."""
+    """One path of 623 steps, the longest run of the register-only generator (a fresh
+    MT19937 state serves 623 outputs without a second regeneration)."""
     from oplib_b200.model import mc_run
     lat, Cm = rows
     disc = math.exp(-0.03)
@@ -59,13 +59,28 @@ def test_mc_ragged_paths_with_extreme_guide_tables(rows, nb):
     assert np.array_equal(paths.cpu().numpy().T, ref_paths)
 
 
-def test_mc_rejects_steps_beyond_one_regeneration(rows):
+@pytest.mark.parametrize("nsteps,use_guide", [(624, False), (1400, True)])
+def test_mc_long_paths_bit_exact(rows, nsteps, use_guide):
+    """Runs past the register-only generator (the per-thread state-array form): 624 steps
+    (the first output of the second regeneration) and 1400 (two regenerations), 300 paths
+    whose seeds wrap past 2^32, with the fused payoffs."""
+    from oplib_b200.model import guide_table, mc_run
+    lat, Cm = rows
+    g = guide_table(Cm, 64) if use_guide else None
+    disc = math.exp(-0.03 * nsteps / 252)
+    seed = 4294967000
+    sums, paths = mc_run(Cm, lat.y0, nsteps, seed, 300, guide=g, x=lat.x, disc=disc, want_paths=True)
+    torch.cuda.synchronize()
+    ref_paths, ref_sums = OC.mc_paths(Cm.cpu().numpy(), lat.y0, seed, 0, 300, nsteps, x=lat.x.cpu().numpy(),
+                                      disc=disc)
+    assert np.array_equal(paths.cpu().numpy().T, ref_paths)
+    assert np.allclose(sums.cpu().numpy(), ref_sums, rtol=1e-12, atol=0)
+
+
+def test_mc_rejects_out_of_range_start_state(rows):
     from oplib_b200 import _lib
     lat, Cm = rows
     d = Cm.shape[1]
-    r = _lib.load().opb_mc_mt19937(Cm.data_ptr(), d, 1, None, 0, d, lat.y0, 624, 1, 0, 16, None, None, 1.0, 0.7,
-                                   1.0, None, None)
-    assert r == -4
     r = _lib.load().opb_mc_mt19937(Cm.data_ptr(), d, 1, None, 0, d, d, 10, 1, 0, 16, None, None, 1.0, 0.7, 1.0,
                                    None, None)
     assert r == -1

@@ -15,7 +15,8 @@ pytestmark = pytest.mark.gpu
 def test_mt19937_streams_bit_exact(cuda):
     from oplib_b200 import _lib
     lib = _lib.load()
-    for seed, n in [(5489, 623), (0, 504), (4294967200, 300), (20260, 17)]:
+    # 623: the register-only generator's longest stream; 2000: the state-array form
+    for seed, n in [(5489, 623), (0, 504), (4294967200, 300), (20260, 17), (5489, 2000), (4294967200, 624)]:
         ns = 300
         out = torch.empty(ns * n, dtype=torch.int32, device=cuda)
         assert lib.opb_mt19937_raw(seed, ns, n, out.data_ptr()) == 0
@@ -124,7 +125,12 @@ def test_opcuda_mc1f_reference_layout_and_continuation(cuda):
     niter, dt = O.plan_niter(L, 1 / 52, cfg.dt0)
     P = O.square(O.ek(L, dt), niter)
     Cr = O.cumrows_f32(P)  # source-major
-    d, nk, nscen, y0 = 128, 40, 4096, O.nearest_node(x)
+    d, nscen, y0 = 128, 4096, O.nearest_node(x)
+    for nk in (40, 700):  # 700: past the register-only generator's 623 steps
+        _mc1f_batches(lib, cuda, Cr, d, nk, nscen, y0)
+
+
+def _mc1f_batches(lib, cuda, Cr, d, nk, nscen, y0):
     ccm = torch.from_numpy(np.asfortranarray(Cr).ravel(order="K").copy()).to(cuda)
     mk = torch.zeros(nk, dtype=torch.int32, device=cuda)
     st = torch.zeros(lib.opcuda_mc_status_sz(), dtype=torch.int32, device=cuda)
@@ -139,18 +145,19 @@ def test_opcuda_mc1f_reference_layout_and_continuation(cuda):
         assert np.array_equal(yh.reshape(nk, nscen).T, ref)
 
 
-def test_mt_benchmark_uniforms(cuda):
+@pytest.mark.parametrize("nper", [20, 700])
+def test_mt_benchmark_uniforms(cuda, nper):
     from oplib_b200 import _lib
     lib = _lib.load()
     st = torch.zeros(4, dtype=torch.int32, device=cuda)
     seed = np.array([7], dtype=np.uint32)
     assert lib.opcuda_mc_setseed(seed.ctypes.data, st.data_ptr()) == 0
-    n = 4096 * 20
+    n = 4096 * nper
     u = torch.empty(n, device=cuda)
     assert lib.opcuda_mt_benchmark(st.data_ptr(), u.data_ptr(), n) == 0
-    got = u.cpu().numpy().reshape(20, 4096)
+    got = u.cpu().numpy().reshape(nper, 4096)
     for s in [0, 5, 4095]:
-        ref = (OC.mt_outputs(7 + s, 20).astype(np.float32) * np.float32(2.0 ** -32)).astype(np.float32)
+        ref = (OC.mt_outputs(7 + s, nper).astype(np.float32) * np.float32(2.0 ** -32)).astype(np.float32)
         assert np.array_equal(got[:, s], ref)
 
 

@@ -1,0 +1,77 @@
+"""The device MT19937 generator's two forms (oplib_b200/csrc/mt19937.cuh) compiled for the
+host and checked against the oracle's MT19937, itself pinned to libstdc++ std::mt19937:
+the register-cursor form up to its 623-output limit, and the state-array form that the
+kernels use for longer runs across several regenerations of the state (no GPU)."""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle_c as OC
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER_DIR = ROOT / "oplib_b200" / "csrc"
+
+DRIVER = r"""
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+#include "mt19937.cuh"
+
+int main(int argc, char **argv) {
+    const unsigned seed = (unsigned)strtoul(argv[1], 0, 10);
+    const int n = atoi(argv[2]);
+    const bool any = strcmp(argv[3], "any") == 0;
+    std::vector<uint32_t> out(n, 0u);
+    int calls = 0;
+    auto f = [&](int k, uint32_t x) { out[k] = x; calls++; };
+    if (any) opb::mt19937_stream<true>(seed, n, f);
+    else opb::mt19937_stream<false>(seed, n, f);
+    if (calls != n) return 2;
+    fwrite(out.data(), 4, n, stdout);
+    return 0;
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def exe(tmp_path_factory):
+    d = tmp_path_factory.mktemp("mtgen")
+    src = d / "mtgen.cpp"
+    src.write_text(DRIVER)
+    binary = d / "mtgen"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-Wall", "-Wno-unknown-pragmas", "-I", str(HEADER_DIR),
+                    str(src), "-o", str(binary)], check=True)
+    return binary
+
+
+def run(exe, seed, n, form):
+    out = subprocess.run([str(exe), str(seed), str(n), form], capture_output=True, check=True).stdout
+    return np.frombuffer(out, dtype=np.uint32)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 5489, 20260, 4294967295])
+def test_cursor_form_matches_mt19937(exe, seed):
+    for n in (1, 226, 227, 453, 454, 623):
+        assert np.array_equal(run(exe, seed, n, "first"), OC.mt_outputs(seed, n)), (seed, n)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 5489, 20260, 4294967295])
+def test_state_array_form_matches_mt19937(exe, seed):
+    # 3 * 624 + 5 outputs: three full regenerations and the words on either side of each
+    n = 3 * 624 + 5
+    got = run(exe, seed, n, "any")
+    assert np.array_equal(got, OC.mt_outputs(seed, n)), seed
+    assert np.array_equal(got[:623], run(exe, seed, 623, "first"))
+
+
+def test_state_array_form_reaches_the_standard_value(exe):
+    # C++11 [rand.predef]: the 10000th output of mt19937 seeded 5489 is 4123659995
+    assert int(run(exe, 5489, 10000, "any")[-1]) == 4123659995
+
+
+def test_zero_outputs(exe):
+    assert run(exe, 7, 0, "any").size == 0
+    assert run(exe, 7, 0, "first").size == 0
