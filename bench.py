@@ -503,7 +503,8 @@ def run_mc(args):
     stream = torch.cuda.current_stream(dev)
     lat = Lattice.local_vol(n=512, device=dev)
     plan = lat.plan(1 / 252, 2.0 ** -14)
-    total_paths, nsteps = (1 << 20) * world, 504  # weak scaling: 2^20 paths per GPU
+    # weak scaling: 2^20 paths per GPU; runs past 623 steps use the state-array generator
+    total_paths, nsteps = (1 << 20) * world, args.mc_steps
     path0, npaths = path_range(total_paths, rank, world)
     disc = math.exp(-0.03 * nsteps / 252)
     nblk = _lib.load().opb_mc_scratch_blocks(npaths)
@@ -567,8 +568,9 @@ def run_mc(args):
             "value": round(samples / (ms * 1e-3), 1), "unit": "path-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32 RNG + f32 compare", "data": "synthetic",
-            "config": {"workload": "LV(512) lattice, dt=1/252 step kernel, 2^20 paths per GPU x 504 steps, barrier "
-                                   "0.7 + Asian, K=1", "paths": total_paths, "steps_per_path": nsteps,
+            "config": {"workload": f"LV(512) lattice, dt=1/252 step kernel, 2^20 paths per GPU x {nsteps} steps, "
+                                   "barrier 0.7 + Asian, K=1", "paths": total_paths, "steps_per_path": nsteps,
+                       "generator": "register cursors" if nsteps <= 623 else "624-word state in local memory",
                        "parallelism": f"path ranges x{world}, one all-reduce of 2 sums",
                        "step": "step-kernel build + cumulative rows + guide table (one CUDA graph) + MC kernel"},
             "mc_kernel_only": {"ms": round(ms_mc, 3), "path_steps_per_s": round(samples / (ms_mc * 1e-3), 1)},
@@ -1297,6 +1299,8 @@ def main():
                              "refbench", "bermudan"],
                     help="sv = the headline SV lattice solve; the others are secondary measurements")
     ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
+    ap.add_argument("--mc-steps", type=int, default=504,
+                    help="--workload mc: steps per path (504 = two years of daily steps)")
     ap.add_argument("--cta-pair", type=int, default=1, choices=[0, 1],
                     help="--workload gemm: 2-CTA pair kernel (1, the default) or one CTA per tile (0)")
     args = ap.parse_args()
