@@ -5,7 +5,6 @@ Tolerances (absolute price error, S0 = 1):
 - OPB_FP32_PLAIN (the reference's FP32 semantics, no renormalisation) is reported and
   bounded by 5e-4; its error is what the FP64 renormalisation removes.
 """
-import math
 
 import numpy as np
 import pytest
