@@ -1,0 +1,248 @@
+"""CPU tests of the restated ``opc`` library (``oracle/opc.c``): the reference's CPU
+entry points under their own names and argument order, checked against numpy/scipy, the
+MT19937 pins, and the reference's own call sequences (S1DGrid.pregen's dgesv solves, the
+host bracket table and opc_dmc1's sampler with its payoff callback).  No GPU."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import scipy.linalg
+import scipy.special
+
+from oracle import opc
+from oracle import oracle as O
+from oracle import oracle_c as OC
+
+F32_EPS, F64_EPS = np.finfo(np.float32).eps, np.finfo(np.float64).eps
+
+
+def p(a):
+    return a.ctypes.data
+
+
+@pytest.fixture(scope="module")
+def lib():
+    return opc.load()
+
+
+def colmajor(m, ld):
+    """Column-major buffer of m with leading dimension ld >= rows (padding = NaN, which a
+    correct routine never reads)."""
+    rows, cols = m.shape
+    buf = np.full((cols, ld), np.nan, dtype=m.dtype)
+    buf[:, :rows] = m.T
+    return buf
+
+
+@pytest.mark.parametrize("dt,fn", [(np.float32, "opc_sgemm"), (np.float64, "opc_dgemm")])
+def test_gemm(lib, dt, fn):
+    rng = np.random.default_rng(1)
+    for m, n, k in [(7, 5, 3), (64, 33, 100), (1, 1, 1), (5, 4, 0)]:
+        A = rng.standard_normal((m, k)).astype(dt)
+        B = rng.standard_normal((k, n)).astype(dt)
+        a, b = colmajor(A, m + 3), colmajor(B, k + 1)
+        c = colmajor(np.full((m, n), 7, dtype=dt), m + 2)
+        getattr(lib, fn)(p(a), p(b), p(c), m + 3, max(k + 1, 1), m + 2, m, n, k)
+        got = c[:, :m].T
+        ref = A.astype(np.float64) @ B.astype(np.float64)
+        bound = (k + 1) * (F32_EPS if dt == np.float32 else F64_EPS) * (np.abs(A) @ np.abs(B)) + 1e-300
+        assert np.all(np.abs(got - ref) <= bound), (m, n, k)
+        assert np.isnan(c[:, m:]).all()  # nothing written past m in any column
+
+
+@pytest.mark.parametrize("dt,fn", [(np.float32, "opc_sgemv"), (np.float64, "opc_dgemv")])
+def test_gemv_increments_alpha_beta(lib, dt, fn):
+    rng = np.random.default_rng(2)
+    m, n = 37, 23
+    A = rng.standard_normal((m, n)).astype(dt)
+    a = colmajor(A, m + 5)
+    for incx, incy, alpha, beta in [(1, 1, 1.0, 0.0), (2, -1, 0.5, 2.0), (-3, 2, -1.0, 1.0), (1, 1, 0.0, 3.0)]:
+        x = rng.standard_normal(n * abs(incx)).astype(dt)
+        y = rng.standard_normal(m * abs(incy)).astype(dt)
+        if beta == 0.0:
+            y[:] = np.nan  # BLAS: beta = 0 overwrites y without reading it
+        xv = x[:: abs(incx)][:n] if incx > 0 else x[:: abs(incx)][:n][::-1]
+        yv = y[:: abs(incy)][:m] if incy > 0 else y[:: abs(incy)][:m][::-1]
+        ref = alpha * (A.astype(np.float64) @ xv.astype(np.float64)) + (0.0 if beta == 0.0 else beta * yv)
+        getattr(lib, fn)(m, n, alpha, p(a), m + 5, p(x), incx, beta, p(y), incy)
+        got = y[:: abs(incy)][:m] if incy > 0 else y[:: abs(incy)][:m][::-1]
+        eps = F32_EPS if dt == np.float32 else F64_EPS
+        bound = (n + 2) * eps * (abs(alpha) * (np.abs(A) @ np.abs(xv)) + abs(beta) * np.abs(np.nan_to_num(yv)))
+        assert np.all(np.abs(got - ref) <= bound + 1e-300), (incx, incy, alpha, beta)
+
+
+def test_dcopy(lib):
+    src = np.arange(10, dtype=np.float64)
+    dst = np.full(12, -1.0)
+    lib.opc_dcopy(10, p(dst), p(src))
+    assert np.array_equal(dst[:10], src) and np.all(dst[10:] == -1)
+
+
+@pytest.mark.parametrize("n,nrhs", [(2, 2), (4, 4), (50, 3)])
+def test_dgesv_matches_lapack_getrf(lib, n, nrhs):
+    rng = np.random.default_rng(n)
+    A = rng.standard_normal((n, n))
+    B = rng.standard_normal((n, nrhs))
+    a, b = colmajor(A, n + 1), colmajor(B, n + 2)
+    ipiv = np.zeros(n, dtype=np.int32)
+    assert lib.opc_dgesv(n, nrhs, p(a), n, n, n + 1, p(ipiv), p(b), n + 2) == 0
+    lu, piv = scipy.linalg.lu_factor(A)
+    assert np.array_equal(ipiv, piv + 1)  # 1-based LAPACK pivots
+    assert np.allclose(a[:, :n].T, lu, rtol=0, atol=1e-12 * n)
+    assert np.allclose(b[:, :n].T, np.linalg.solve(A, B), rtol=1e-10, atol=1e-12)
+
+
+def test_sgesv_and_singular_info(lib):
+    A = np.array([[2.0, 1.0, 1.0], [4.0, 2.0, 2.0], [1.0, 0.0, 3.0]], dtype=np.float32)  # rank 2
+    a, b = colmajor(A, 3), colmajor(np.eye(3, dtype=np.float32), 3)
+    ipiv, info = np.zeros(3, dtype=np.int32), np.zeros(1, dtype=np.int32)
+    r = lib.opc_sgesv(3, 3, p(a), 3, 3, 3, p(ipiv), p(b), 3, p(info))
+    assert r == info[0] == 3  # U(3,3) is exactly zero
+    assert np.array_equal(b, np.eye(3, dtype=np.float32).T)  # no solve after a zero pivot
+    A = np.array([[3.0, 1.0], [1.0, 2.0]], dtype=np.float32)
+    a, b = colmajor(A, 2), colmajor(np.eye(2, dtype=np.float32), 2)
+    assert lib.opc_sgesv(2, 2, p(a), 2, 2, 2, p(ipiv), p(b), 2, p(info)) == 0
+    assert np.allclose(b.T, np.linalg.inv(A.astype(np.float64)), rtol=2e-7)
+    assert lib.opc_dgesv(-1, 1, None, 0, 0, 1, None, None, 1) == -1
+    assert lib.opc_dgesv(3, 1, None, 3, 3, 2, None, None, 3) == -4
+
+
+def test_s1dgrid_pregen_through_dgesv_matches_oracle_invm(lib):
+    """S1DGrid.pregen (oplib/opmodel/types/S1DGrid.cs:78-147) step for step: identity
+    blocks in invm, the 2x2 moment matrix per node, opc_dgesv(2, 2, mat, 2, 2, 2, ipiv,
+    invm + 4*x0, 2).  The oracle's lv_invm must be the same inverses."""
+    x = 0.05 * 100.0 ** (np.arange(512) / 511.0)
+    d = x.size
+    invm = np.zeros(4 * d)
+    for xx in range(d):
+        for z in range(2):
+            invm[4 * xx + z + 2 * z] = 1.0
+    ipiv = np.zeros(20, dtype=np.int32)
+    for x0 in range(d):
+        mat = np.zeros(4)
+        mat[0] = x[x0 - 1] - x[x0] if x0 > 0 else 1.0
+        mat[2] = x[x0 + 1] - x[x0] if x0 < d - 1 else 1.0
+        if 0 < x0 < d:
+            mat[1], mat[3] = mat[0] ** 2, mat[2] ** 2
+        if x0 == 0:
+            mat[1], mat[3] = 0.0, 1.0
+        if x0 == d - 1:
+            mat[1], mat[3] = 1.0, 0.0
+        blk = invm[4 * x0:4 * x0 + 4].copy()
+        assert lib.opc_dgesv(2, 2, p(mat), 2, 2, 2, p(ipiv), p(blk), 2) == 0
+        invm[4 * x0:4 * x0 + 4] = blk
+    ref = O.lv_invm(x)  # (d, 2, 2) row-major
+    got = invm.reshape(d, 2, 2).transpose(0, 2, 1)  # column-major blocks
+    assert np.allclose(got, ref, rtol=1e-12, atol=0)
+
+
+def test_rangen_streams(lib):
+    seeds = np.array([5489, 7, 4294967295], dtype=np.uint32)
+    lib.opc_rangen_init_seed(p(seeds), 3)
+    assert lib.opc_rangen_getstatus() == 0
+    r = np.empty(1000)
+    lib.opc_genunif(p(r), 1000, -1.0, 3.0, 1)
+    assert lib.opc_rangen_getstatus() == 0
+    assert np.array_equal(r, -1.0 + 4.0 * (OC.mt_outputs(7, 1000).astype(np.float64) * 2.0 ** -32))
+    # a stream continues across calls; other threads' streams are untouched
+    r2 = np.empty(10)
+    lib.opc_genunif(p(r2), 10, 0.0, 1.0, 1)
+    assert np.array_equal(r2, OC.mt_outputs(7, 1010)[1000:] * 2.0 ** -32)
+    lib.opc_genunif(p(r2), 10, 0.0, 1.0, 2)
+    assert np.array_equal(r2, OC.mt_outputs(4294967295, 10) * 2.0 ** -32)
+    u = np.empty(4096, dtype=np.float32)
+    assert lib.opc_mt_benchmark(4096, p(u), 0) == 0
+    bits = OC.mt_outputs(5489, 4096)
+    assert np.array_equal(u, bits.astype(np.float32) / np.float32(2.0 ** 32))
+    lib.opc_genunif(p(r2), 10, 0.0, 1.0, 3)  # no such thread
+    assert lib.opc_rangen_getstatus() < 0
+    lib.opc_rangen_finalize()
+    lib.opc_genunif(p(r2), 10, 0.0, 1.0, 0)
+    assert lib.opc_rangen_getstatus() < 0
+
+
+def test_gennor_inverts_the_normal_cdf(lib):
+    seeds = np.array([20260], dtype=np.uint32)
+    lib.opc_rangen_init_seed(p(seeds), 1)
+    n = 1 << 16
+    r = np.empty(n)
+    lib.opc_gennor(p(r), n, 0.25, 2.0, 0)
+    u = (OC.mt_outputs(20260, n).astype(np.float64) + 0.5) * 2.0 ** -32
+    z = scipy.special.ndtri(u)
+    assert np.all(np.abs((r - 0.25) / 2.0 - z) <= 8 * F64_EPS * np.maximum(1.0, np.abs(z)))
+    assert abs(r.mean() - 0.25) < 4 * 2.0 / np.sqrt(n) and abs(r.std() / 2.0 - 1.0) < 0.02
+    lib.opc_rangen_finalize()
+
+
+@pytest.fixture(scope="module")
+def lv64():
+    cfg = O.LVLattice(n=64)
+    L, x = cfg.generator()
+    niter, dt = O.plan_niter(L, 1 / 52, cfg.dt0)
+    P = O.square(O.ek(L, dt), niter)  # source-major rows
+    return P, O.nearest_node(x)
+
+
+def test_host_bracket_table(lib, lv64):
+    """opc_host_mc_hash against a numpy restatement of host_d_mc_hash: cumulative rows
+    normalised from the second column on (the first keeps the raw entry), brackets that
+    contain the inverse-CDF answer of every bucket."""
+    P, _ = lv64
+    d = P.shape[0]
+    mats = (P, P @ P)
+    tpk_cm = np.concatenate([np.asfortranarray(m).ravel(order="K") for m in mats])
+    ctpk = np.empty(2 * d * d)
+    hash_ = np.empty(2 * d * d, dtype=np.int32)
+    lib.opc_host_mc_hash(p(tpk_cm), d, 2, p(ctpk), p(hash_))
+    for m, Pm in enumerate(mats):
+        cs = np.cumsum(Pm, axis=1)
+        ref = np.minimum(cs / cs[:, -1:], 1.0)
+        ref[:, 0] = Pm[:, 0]
+        Cm = ctpk[m * d * d:(m + 1) * d * d].reshape(d, d).T  # [y1, y2]
+        assert np.allclose(Cm, ref, rtol=1e-15, atol=1e-17)
+        H = hash_[m * d * d:(m + 1) * d * d].reshape(d, d).T  # [y1, bucket]
+        lb, ub = H & 0xFFFF, H >> 16
+        assert np.all(lb <= ub) and np.all(ub < d)
+        rng = np.random.default_rng(m)
+        for y in rng.integers(0, d, 16):
+            u = rng.random(500)
+            ans = np.minimum(np.argmax(u[:, None] < Cm[y][None, :], axis=1), d - 1)
+            s = (u * d).astype(np.int64)
+            assert np.all((lb[y, s] <= ans) & (ans <= ub[y, s]))
+
+
+def test_dmc1_sampler_and_payoff_callback(lib, lv64):
+    """opc_dmc1 (oplib/opc/rangen.cpp:97-153): each state is the smallest y with
+    u < C[yprev, y] on the bracket table's cumulative rows, u = x / 2^32 from the thread's
+    stream (step-major), and the payoff callback sees the batch once."""
+    P, y0 = lv64
+    d = P.shape[0]
+    tpk = np.asfortranarray(P).ravel(order="K").copy()
+    ctpk = np.empty(d * d)
+    hash_ = np.empty(d * d, dtype=np.int32)
+    lib.opc_host_mc_hash(p(tpk), d, 1, p(ctpk), p(hash_))
+    nscen, nk = 512, 30
+    seeds = np.array([11, 4242], dtype=np.uint32)
+    lib.opc_rangen_init_seed(p(seeds), 2)
+    unif = np.empty(nscen, dtype=np.uint32)
+    y_sk = np.full(nscen * nk, -1, dtype=np.int16)
+    m_k = np.zeros(nk, dtype=np.int32)
+    seen = []
+
+    def cb(yp, th, b):
+        seen.append((th, b, int(yp[0]), int(yp[nscen * nk - 1])))
+
+    fn = opc.PAYOFF_EVAL(cb)
+    addr = C.cast(fn, C.c_void_p).value
+    assert lib.opc_dmc1(p(ctpk), p(hash_), d, nscen, nk, y0, p(unif), p(y_sk), p(m_k), addr, 1, 9) == 0
+    lib.opc_rangen_finalize()
+    assert seen == [(1, 9, int(y_sk[0]), int(y_sk[-1]))]
+    Cm = ctpk.reshape(d, d).T
+    u = OC.mt_outputs(4242, nscen * nk).reshape(nk, nscen).astype(np.float64) / 2.0 ** 32
+    Y = y_sk.reshape(nk, nscen)
+    prev = np.full(nscen, y0)
+    for k in range(nk):
+        ans = np.minimum(np.argmax(u[k][:, None] < Cm[prev], axis=1), d - 1)
+        assert np.array_equal(Y[k], ans), k
+        prev = Y[k].astype(np.int64)
+    assert len(np.unique(Y[-1])) > 5  # the chain moved
