@@ -17,8 +17,12 @@
 // Output 623 would need mt'[0] as the second operand of its tw(), i.e. a word of the
 // regenerated state, which is where the cursor form stops.
 //
-// mt19937_any (any n): the 624-word state in a per-thread array (local memory on the
-// device, 2496 bytes a thread), regenerated one word per output:
+// mt19937_any (any n): the first 623 outputs come from the same cursors, and each
+// regenerated word is also stored in a per-thread 624-word array (local memory on the
+// device, 2496 bytes a thread), so no separate initialisation pass is needed.  Output 623
+// closes the first regeneration (mt'[623] = mt'[396] ^ tw(mt[623], mt'[0]), with the
+// initial word mt[623] taken from the cursor), and every later output regenerates one word
+// of the array:
 //   mt[i] = mt[(i+397) mod 624] ^ tw(mt[i], mt[(i+1) mod 624]);  output temper(mt[i])
 // Word i of a generation reads mt[i+397] before it is regenerated (i < 227) and after
 // (i >= 227), and word 623 reads the regenerated mt[0], exactly as genrand_int32's block
@@ -56,9 +60,10 @@ OPB_MT_FN uint32_t mt_temper(uint32_t y) {
     return y;
 }
 
-// Calls f(k, x_k) for the first n (<= 623) outputs of MT19937 seeded with `seed`.
+// Calls f(k, w_k) with the regenerated (untempered) state word w_k = mt'[k] for the first
+// n (<= 623) words of MT19937 seeded with `seed`; returns the initial word mt[n].
 template <class F>
-OPB_MT_FN void mt19937_first(uint32_t seed, int n, F &&f) {
+OPB_MT_FN uint32_t mt19937_cursor_words(uint32_t seed, int n, F &&f) {
     // cursor A at i: (a0, a1) = (mt[i], mt[i+1])
     uint32_t a0 = seed, a1 = mt_init_next(seed, 1u);
     // cursor B at i + 397
@@ -71,47 +76,59 @@ OPB_MT_FN void mt19937_first(uint32_t seed, int n, F &&f) {
     const int n1 = n < 227 ? n : 227;
 #pragma unroll 1
     for (; i < n1; i++) {
-        f(i, mt_temper(b ^ mt_tw(a0, a1)));
+        f(i, b ^ mt_tw(a0, a1));
         a0 = a1; a1 = mt_init_next(a1, (uint32_t)i + 2u);
         bi++; b = mt_init_next(b, bi);
     }
-    if (i >= n) return;
+    if (i >= n) return a0;
     // phase 2: cursor C at i-227 from the seed, cursor B restarted at 397
     uint32_t c0 = seed, c1 = mt_init_next(seed, 1u);
     b = m397; bi = 397;
     const int n2 = n < 454 ? n : 454;
 #pragma unroll 1
     for (; i < n2; i++) {
-        f(i, mt_temper(b ^ mt_tw(c0, c1) ^ mt_tw(a0, a1)));
+        f(i, b ^ mt_tw(c0, c1) ^ mt_tw(a0, a1));
         a0 = a1; a1 = mt_init_next(a1, (uint32_t)i + 2u);
         c0 = c1; c1 = mt_init_next(c1, (uint32_t)(i - 227) + 2u);
         bi++; b = mt_init_next(b, bi);
     }
-    if (i >= n) return;
+    if (i >= n) return a0;
     // phase 3: cursor D at i-454 from the seed, B restarted at 397 (= i-57 at i = 454)
     uint32_t d0 = seed, d1 = mt_init_next(seed, 1u);
     b = m397; bi = 397;
 #pragma unroll 1
     for (; i < n; i++) {
-        f(i, mt_temper(b ^ mt_tw(d0, d1) ^ mt_tw(c0, c1) ^ mt_tw(a0, a1)));
+        f(i, b ^ mt_tw(d0, d1) ^ mt_tw(c0, c1) ^ mt_tw(a0, a1));
         a0 = a1; a1 = mt_init_next(a1, (uint32_t)i + 2u);
         c0 = c1; c1 = mt_init_next(c1, (uint32_t)(i - 227) + 2u);
         d0 = d1; d1 = mt_init_next(d1, (uint32_t)(i - 454) + 2u);
         bi++; b = mt_init_next(b, bi);
     }
+    return a0;
+}
+
+// Calls f(k, x_k) for the first n (<= 623) outputs of MT19937 seeded with `seed`.
+template <class F>
+OPB_MT_FN void mt19937_first(uint32_t seed, int n, F &&f) {
+    mt19937_cursor_words(seed, n, [&](int i, uint32_t w) { f(i, mt_temper(w)); });
 }
 
 // Calls f(k, x_k) for the first n outputs of MT19937 seeded with `seed`, any n >= 0.
 template <class F>
 OPB_MT_FN void mt19937_any(uint32_t seed, int n, F &&f) {
     uint32_t mt[624];
-    mt[0] = seed;
-#pragma unroll 1
-    for (uint32_t j = 1; j < 624; j++) mt[j] = mt_init_next(mt[j - 1], j);
+    const int n1 = n < kMtCursorMax ? n : kMtCursorMax;
+    const uint32_t init623 = mt19937_cursor_words(seed, n1, [&](int k, uint32_t w) {
+        mt[k] = w;
+        f(k, mt_temper(w));
+    });
+    if (n <= kMtCursorMax) return;
+    mt[623] = mt[396] ^ mt_tw(init623, mt[0]);
+    f(623, mt_temper(mt[623]));
     int i = 0, im = 397;  // im = (i + 397) mod 624
     uint32_t cur = mt[0]; // mt[i], carried from the previous output's mt[i+1] load
 #pragma unroll 1
-    for (int k = 0; k < n; k++) {
+    for (int k = 624; k < n; k++) {
         const int i1 = i == 623 ? 0 : i + 1;
         const uint32_t nxt = mt[i1];
         const uint32_t y = mt[im] ^ mt_tw(cur, nxt);

@@ -1,7 +1,7 @@
 """The device MT19937 generator's two forms (oplib_b200/csrc/mt19937.cuh) compiled for the
 host and checked against the oracle's MT19937, itself pinned to libstdc++ std::mt19937:
-the register-cursor form up to its 623-output limit, and the state-array form that the
-kernels use for longer runs across several regenerations of the state (no GPU)."""
+the register-cursor form up to its 623-output limit, and the cursor/state-array form that
+the kernels use for longer runs across several regenerations of the state (no GPU)."""
 import subprocess
 from pathlib import Path
 
@@ -65,6 +65,8 @@ def test_state_array_form_matches_mt19937(exe, seed):
     got = run(exe, seed, n, "any")
     assert np.array_equal(got, OC.mt_outputs(seed, n)), seed
     assert np.array_equal(got[:623], run(exe, seed, 623, "first"))
+    for m in (1, 622, 623, 624, 625, 1247, 1248, 1249):  # each side of the cursor/array hand-over
+        assert np.array_equal(run(exe, seed, m, "any"), got[:m]), (seed, m)
 
 
 def test_state_array_form_reaches_the_standard_value(exe):
