@@ -9,9 +9,10 @@
 //
 // B200 design: one thread per path with the whole generator in registers for runs of up
 // to 623 steps (mt19937_first in mt19937.cuh walks the seeding recurrence with a few
-// cursors, no state array); longer runs keep the 624-word state in a per-thread
-// local-memory array (mt19937_any) in a separate instantiation of the same kernels, so the
-// register-only instantiation carries no stack frame.
+// cursors, no state array); longer runs (mt19937_any) take their first 623 outputs from
+// the same cursors while storing the regenerated words in a per-thread 624-word
+// local-memory array, which serves every later output.  They run in a separate
+// instantiation of the same kernels, so the register-only one carries no stack frame.
 // The inverse-CDF search starts from the guide-table bracket of the previous state's row
 // (about one probe per step) and falls back to the full row without a guide table.
 // Payoffs (discretely monitored down-and-out call, arithmetic-Asian call) are reduced per
