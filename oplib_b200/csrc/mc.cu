@@ -141,7 +141,7 @@ __global__ void k_mt_raw(uint32_t seed, long long nstreams, int n, uint32_t *__r
     mt19937_stream<ANY_LENGTH>(seed + (uint32_t)s, n, [&](int j, uint32_t bits) { out[s * n + j] = bits; });
 }
 
-// The register-only generator up to 623 steps, the state-array one beyond.
+// The register-only generator up to 623 steps, the cursor/state-array one beyond.
 void launch_mc(int grid, const McArgs &a) {
     if (a.nsteps <= kMtCursorMax) k_mc<false><<<grid, 256, 0, stream()>>>(a);
     else k_mc<true><<<grid, 256, 0, stream()>>>(a);
