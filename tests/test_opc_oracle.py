@@ -246,3 +246,34 @@ def test_dmc1_sampler_and_payoff_callback(lib, lv64):
         assert np.array_equal(Y[k], ans), k
         prev = Y[k].astype(np.int64)
     assert len(np.unique(Y[-1])) > 5  # the chain moved
+
+
+def test_dmc1_first_state_bracket(lib):
+    """Rows with heavy mass on state 0 and on the last state: the sampler's bracket-at-0
+    rule (oplib/opc/rangen.cpp:131-133) and the d-1 cap still give the inverse-CDF answer."""
+    rng = np.random.default_rng(5)
+    d = 8
+    P = rng.random((d, d)) ** 3
+    P[:, 0] += 2.0
+    P[:, -1] += 1.0
+    P /= P.sum(axis=1, keepdims=True)
+    tpk = np.asfortranarray(P).ravel(order="K").copy()
+    ctpk = np.empty(d * d)
+    hash_ = np.empty(d * d, dtype=np.int32)
+    lib.opc_host_mc_hash(p(tpk), d, 1, p(ctpk), p(hash_))
+    nscen, nk = 4096, 6
+    lib.opc_rangen_init_seed(p(np.array([99], dtype=np.uint32)), 1)
+    unif = np.empty(nscen, dtype=np.uint32)
+    y_sk = np.empty(nscen * nk, dtype=np.int16)
+    m_k = np.zeros(nk, dtype=np.int32)
+    assert lib.opc_dmc1(p(ctpk), p(hash_), d, nscen, nk, 3, p(unif), p(y_sk), p(m_k), 0, 0, 0) == 0
+    lib.opc_rangen_finalize()
+    Cm = ctpk.reshape(d, d).T
+    u = OC.mt_outputs(99, nscen * nk).reshape(nk, nscen).astype(np.float64) / 2.0 ** 32
+    Y = y_sk.reshape(nk, nscen)
+    prev = np.full(nscen, 3)
+    for k in range(nk):
+        ans = np.minimum(np.argmax(u[k][:, None] < Cm[prev], axis=1), d - 1)
+        assert np.array_equal(Y[k], ans), k
+        prev = Y[k].astype(np.int64)
+    assert (Y == 0).mean() > 0.3 and (Y == d - 1).mean() > 0.05
