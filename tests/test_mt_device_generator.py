@@ -77,3 +77,13 @@ def test_state_array_form_reaches_the_standard_value(exe):
 def test_zero_outputs(exe):
     assert run(exe, 7, 0, "any").size == 0
     assert run(exe, 7, 0, "first").size == 0
+
+
+def test_random_seeds_and_lengths(exe):
+    rng = np.random.default_rng(20260)
+    for seed, n in zip(rng.integers(0, 2**32, 40), rng.integers(0, 2600, 40)):
+        seed, n = int(seed), int(n)
+        ref = OC.mt_outputs(seed, n) if n else np.empty(0, dtype=np.uint32)
+        assert np.array_equal(run(exe, seed, n, "any"), ref), (seed, n)
+        m = min(n, 623)
+        assert np.array_equal(run(exe, seed, m, "first"), ref[:m]), (seed, m)
