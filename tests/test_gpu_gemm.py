@@ -14,6 +14,7 @@ import numpy as np
 import pytest
 import torch
 
+from oracle import opc
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -338,6 +339,17 @@ def test_opcuda_sgemm4_task_table(cuda):
         got = dC.cpu().numpy().reshape(n, m).T
         ref = A.astype(np.float64) @ B
         assert np.abs(got - ref).max() / (1 + np.abs(ref).max()) < 2e-3 * 1e-2
+    # the reference's own check (benchmarks/gsgemm4/Program.cs:229-291): the inputs come
+    # back unchanged, and every C agrees with the CPU library's
+    # opc_sgemm(A, B, C, m, k, m, m, n, k) within |C - C'| / (1 + |C'|) <= 2e-3
+    L = opc.load()
+    for (A, B, dA, dB), dC in zip(mats, outs):
+        (m, k), n = A.shape, B.shape[1]
+        a, b = np.asfortranarray(A).ravel(order="K").copy(), np.asfortranarray(B).ravel(order="K").copy()
+        assert np.array_equal(dA.cpu().numpy(), a) and np.array_equal(dB.cpu().numpy(), b)
+        c = np.empty(m * n, dtype=np.float32)
+        L.opc_sgemm(a.ctypes.data, b.ctypes.data, c.ctypes.data, m, k, m, m, n, k)
+        assert (np.abs(dC.cpu().numpy() - c) / (1 + np.abs(c))).max() <= 2e-3
 
 
 def test_opcuda_sgemv_family(cuda):
@@ -389,6 +401,17 @@ def test_opcuda_sgemv3_columns_and_sentinel(cuda):
     for j in range(nz):
         assert np.allclose(got[nz + j], A.astype(np.float64) @ Z[j], rtol=1e-5, atol=1e-5)
         assert np.array_equal(got[j], Z[j])
+    # the reference's own check (benchmarks/gsgemv4/Program.cs:329-391): the same column
+    # list through opc_sgemv(d, d, 1, A, d, Z + col0, 1, 0, Z + col1, 1) on the host, then
+    # |Z - Z'| / (1 + |Z'|) <= 1e-3
+    L = opc.load()
+    ah = np.asfortranarray(A).ravel(order="K").copy()
+    zh = Z.ravel().copy()
+    for a0, a1 in zip(col0, col1):
+        if a1 != 2 * nz:  # the sentinel entry writes nothing
+            L.opc_sgemv(d, d, 1.0, ah.ctypes.data, d, zh.ctypes.data + 4 * a0 * d, 1, 0.0,
+                        zh.ctypes.data + 4 * a1 * d, 1)
+    assert (np.abs(got.ravel() - zh) / (1 + np.abs(zh))).max() <= 1e-3
 
 
 def test_opcuda_sek_fp64_sum(cuda):
