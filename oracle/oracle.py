@@ -45,6 +45,69 @@ def log_grid(n: int, lo: float = 0.05, hi: float = 5.0, s0: float = 1.0) -> np.n
     return s0 * lo * (hi / lo) ** (i / (n - 1))
 
 
+def pivot_grid(nx: int, pivots, spacings, xval0: float) -> tuple[np.ndarray, int]:
+    """The reference's pivot/spacing spot grid and its spot node (``SGrid.xgrid`` and
+    ``grid_iterate``, ``oplib/opmodel/types/SGrid.cs:492-593``).
+
+    Node 0 sits on the first pivot; node x adds scale * (current spacing), and the spacing
+    switches to the next pivot's once a node passes that pivot.  The scale is bracketed in
+    steps of 0.1 (up from 1 while the last node falls short of the last pivot, down
+    otherwise), bisected 10 times, and the grid of the last bisection step is kept; the
+    node nearest to ``xval0`` (first on ties) becomes the spot node x0 and the whole grid is
+    scaled so that node is exactly ``xval0``.  Returns (nodes, x0)."""
+    pivots = [float(p) for p in pivots]
+    spacings = [float(s) for s in spacings]
+    npv = len(pivots)
+    if npv <= 2 or len(spacings) != npv:
+        raise ValueError("pivot_grid needs more than two pivots, one spacing each")
+    x = np.zeros(nx)
+
+    def iterate(scale):
+        x[0] = pivots[0]
+        step, p = spacings[0], 1
+        nextp = pivots[p] if p < npv else 0.0
+        for i in range(1, nx):
+            x[i] = x[i - 1] + scale * step
+            if p < npv and x[i] > nextp:
+                step = spacings[p]
+                p += 1
+                if p < npv:
+                    nextp = pivots[p]
+        return x[nx - 1]
+
+    scale0 = scale1 = 1.0
+    f0 = pivots[-1] / iterate(1.0)
+    if f0 > 1:
+        it = 1
+        while True:
+            scale0 = 1 + 0.1 * it
+            if pivots[-1] / iterate(scale0) < 1:
+                break
+            scale1 = scale0
+            it += 1
+    else:
+        it = 1
+        while True:
+            scale1 = 1 / (1 + 0.1 * it)
+            if pivots[-1] / iterate(scale1) > 1:
+                break
+            scale0 = scale1
+            it += 1
+    for _ in range(10):
+        mid = 0.5 * (scale0 + scale1)
+        f2 = pivots[-1] / iterate(mid)
+        if f2 > 1:
+            scale1 = mid
+        if f2 <= 1:
+            scale0 = mid
+    x0, best = 0, abs(x[0] - xval0)
+    for i in range(1, nx):
+        e = abs(x[i] - xval0)
+        if e < best:
+            x0, best = i, e
+    return x * (xval0 / x[x0]), x0
+
+
 def nearest_node(x: np.ndarray, s0: float = 1.0) -> int:
     """Index of the node nearest to the spot (the reference's ``grid.y0``)."""
     return int(np.argmin(np.abs(x - s0)))

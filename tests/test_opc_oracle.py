@@ -3,6 +3,7 @@ entry points under their own names and argument order, checked against numpy/sci
 MT19937 pins, and the reference's own call sequences (S1DGrid.pregen's dgesv solves, the
 host bracket table and opc_dmc1's sampler with its payoff callback).  No GPU."""
 import ctypes as C
+import math
 
 import numpy as np
 import pytest
@@ -277,3 +278,71 @@ def test_dmc1_first_state_bracket(lib):
         assert np.array_equal(Y[k], ans), k
         prev = Y[k].astype(np.int64)
     assert (Y == 0).mean() > 0.3 and (Y == d - 1).mean() > 0.05
+
+
+BSTEST_PIVOTS = [1.0, 70.0, 90.0, 110.0, 140.0, 200.0, 300.0]  # tests/bstest/OPPricer.cs:72-79
+BSTEST_SPACINGS = [5.0, 2.5, 1.0, 2.5, 5.0, 7.5, 10.0]
+
+
+def test_pivot_grid_of_bstest():
+    x, y0 = O.pivot_grid(256, BSTEST_PIVOTS, BSTEST_SPACINGS, 100.0)
+    dx = np.diff(x)
+    assert x[y0] == 100.0 and np.all(dx > 0)
+    # one common scale on the pivot spacings, the finest (1) around the spot; the last node
+    # lands on the last pivot, so its spacing (10) is never used
+    s = dx[y0]
+    assert dx.min() == s and set(np.round(dx / s, 9)) == {1.0, 2.5, 5.0, 7.5}
+    assert abs(x[-1] - 300.0) < 7.5 * s and abs(x[0] - 1.0) < 0.01
+
+
+def test_bstest_through_the_restated_cpu_path(lib):
+    """The reference's integration test (tests/bstest/Program.cs:11-37, OPPricer.cs:67-148)
+    on its host-FP64 path, call for call: the 256-node pivot grid around S = 100,
+    S1DGrid.pregen's opc_dgesv solves, the LV generator with drift r x and vol sigma x,
+    one 365-day step planned by the niter rule with dt0 = 1 day, I + dt L squared niter
+    times through opc_dgemm, the bracket table, opc_dmc1 with the vanilla payoff evaluator
+    as its callback, and discounting over 365 / 365.25 years.  The reference prints the
+    price beside the closed form and checks nothing; here the Monte Carlo price must agree
+    with the lattice's own expectation within 4 standard errors, and that with the closed
+    form within the grid's discretisation error."""
+    S, K, r, sig = 100.0, 100.0, 0.05, 0.25
+    T, dt0 = 365 / 365.25, 1 / 365.25
+    x, y0 = O.pivot_grid(256, BSTEST_PIVOTS, BSTEST_SPACINGS, S)
+    d = x.size
+    L = O.lv_generator(x, r * x, sig * x)
+    niter, dt = O.plan_niter(L, T, dt0)
+    a = np.asfortranarray(O.ek(L, dt)).ravel(order="K").copy()
+    c = np.empty_like(a)
+    for _ in range(niter):  # host_d_mc_sq: ping-pong through opc_dgemm
+        lib.opc_dgemm(p(a), p(a), p(c), d, d, d, d, d, d)
+        a, c = c, a
+    P = a.reshape(d, d).T
+    ctpk = np.empty(d * d)
+    hash_ = np.empty(d * d, dtype=np.int32)
+    lib.opc_host_mc_hash(p(a), d, 1, p(ctpk), p(hash_))
+    nscen, nbatch = 4096 * 25, 12
+    lib.opc_rangen_init_seed(p(np.array([12345], dtype=np.uint32)), 1)
+    unif = np.empty(nscen, dtype=np.uint32)
+    y_sk = np.empty(nscen, dtype=np.int16)
+    m_k = np.zeros(1, dtype=np.int32)
+    sums = np.zeros(2)
+
+    def evaluate(yp, th, batch):  # VanillaPayoffEvaluator.mc_eval_implementation
+        pay = np.maximum(x[np.ctypeslib.as_array(yp, shape=(nscen,))] - K, 0.0)
+        sums[0] += pay.sum()
+        sums[1] += (pay * pay).sum()
+
+    fn = opc.PAYOFF_EVAL(evaluate)
+    addr = C.cast(fn, C.c_void_p).value
+    for b in range(nbatch):
+        assert lib.opc_dmc1(p(ctpk), p(hash_), d, nscen, 1, y0, p(unif), p(y_sk), p(m_k), addr, 0, b) == 0
+    lib.opc_rangen_finalize()
+    n = nscen * nbatch
+    disc = math.exp(-r * T)
+    mean = sums[0] / n
+    se = disc * math.sqrt((sums[1] / n - mean * mean) / n)
+    price_mc = disc * mean
+    price_lattice = disc * (P[y0] @ np.maximum(x - K, 0.0))
+    assert abs(price_mc - price_lattice) < 4 * se, (price_mc, price_lattice, se)
+    # 12.3301 against 12.3310 (the closed form at T = 365 / 365.25; 12.33600 at T = 1)
+    assert abs(price_lattice - float(O.bs_call(S, K, r, sig, T))) < 5e-3, price_lattice
