@@ -39,10 +39,15 @@ import numpy as np
 def log_grid(n: int, lo: float = 0.05, hi: float = 5.0, s0: float = 1.0) -> np.ndarray:
     """Log-spaced spot nodes x_i = s0*lo*(hi/lo)**(i/(n-1)), i = 0..n-1.
 
-    Replaces the pivot/spacing grid of ``oplib/opmodel/types/SGrid.cs:492-593`` (the
-    lattice configurations are defined on log-spaced nodes)."""
+    The lattice configurations are defined on log-spaced nodes; the reference's own
+    pivot/spacing grid (``oplib/opmodel/types/SGrid.cs:492-593``) is :func:`pivot_grid`."""
     i = np.arange(n, dtype=np.float64)
     return s0 * lo * (hi / lo) ** (i / (n - 1))
+
+
+# The pivot grid of the reference's integration test (tests/bstest/OPPricer.cs:72-79).
+BSTEST_PIVOTS = (1.0, 70.0, 90.0, 110.0, 140.0, 200.0, 300.0)
+BSTEST_SPACINGS = (5.0, 2.5, 1.0, 2.5, 5.0, 7.5, 10.0)
 
 
 def pivot_grid(nx: int, pivots, spacings, xval0: float) -> tuple[np.ndarray, int]:

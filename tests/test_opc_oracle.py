@@ -280,12 +280,8 @@ def test_dmc1_first_state_bracket(lib):
     assert (Y == 0).mean() > 0.3 and (Y == d - 1).mean() > 0.05
 
 
-BSTEST_PIVOTS = [1.0, 70.0, 90.0, 110.0, 140.0, 200.0, 300.0]  # tests/bstest/OPPricer.cs:72-79
-BSTEST_SPACINGS = [5.0, 2.5, 1.0, 2.5, 5.0, 7.5, 10.0]
-
-
 def test_pivot_grid_of_bstest():
-    x, y0 = O.pivot_grid(256, BSTEST_PIVOTS, BSTEST_SPACINGS, 100.0)
+    x, y0 = O.pivot_grid(256, O.BSTEST_PIVOTS, O.BSTEST_SPACINGS, 100.0)
     dx = np.diff(x)
     assert x[y0] == 100.0 and np.all(dx > 0)
     # one common scale on the pivot spacings, the finest (1) around the spot; the last node
@@ -307,7 +303,7 @@ def test_bstest_through_the_restated_cpu_path(lib):
     form within the grid's discretisation error."""
     S, K, r, sig = 100.0, 100.0, 0.05, 0.25
     T, dt0 = 365 / 365.25, 1 / 365.25
-    x, y0 = O.pivot_grid(256, BSTEST_PIVOTS, BSTEST_SPACINGS, S)
+    x, y0 = O.pivot_grid(256, O.BSTEST_PIVOTS, O.BSTEST_SPACINGS, S)
     d = x.size
     L = O.lv_generator(x, r * x, sig * x)
     niter, dt = O.plan_niter(L, T, dt0)
