@@ -137,6 +137,56 @@ def test_s1dgrid_pregen_through_dgesv_matches_oracle_invm(lib):
     assert np.allclose(got, ref, rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("xs,rs", [((0.05, 5.0), (0.05, 1.0)), ((10.0, 300.0), (0.5, 40.0))])
+def test_s2dgrid_pregen_through_dgesv_matches_oracle_invm(lib, xs, rs):
+    """S2DGrid.pregen (oplib/opmodel/types/S2DGrid.cs:123-245) literally: identity blocks
+    in invm, one 4 x 4 buffer reused for every node (opc_dgesv overwrites it with its LU
+    factors and the loop never resets entries (1, 2) and (1, 3); they stay zero because
+    the x and r blocks never mix), opc_dgesv(4, 4, mat, 4, 4, 4, ipiv, invm + 16*y0, 4).
+    The oracle's s2d_invm must be the same inverses -- on grids with spacings below and
+    above 1, so both pivot orders of the 2 x 2 blocks occur."""
+    nx, nr = 12, 5
+    xg = xs[0] * (xs[1] / xs[0]) ** (np.arange(nx) / (nx - 1))
+    rg = rs[0] * (rs[1] / rs[0]) ** (np.arange(nr) / (nr - 1))
+    d = nx * nr
+    xval = np.tile(xg, nr)
+    rval = np.repeat(rg, nx)
+    invm = np.zeros(16 * d)
+    for y in range(d):
+        for i in range(4):
+            invm[16 * y + i + 4 * i] = 1.0
+    mat = np.zeros(16)
+    ipiv = np.zeros(4, dtype=np.int32)
+    ld = 4
+    for x0 in range(nx):
+        for a0 in range(nr):
+            y0 = x0 + nx * a0
+            mat[0 + ld * 0] = xval[y0 - 1] - xval[y0] if x0 > 0 else 0.0
+            mat[0 + ld * 1] = xval[y0 + 1] - xval[y0] if x0 < nx - 1 else 0.0
+            mat[0 + ld * 2] = mat[0 + ld * 3] = 0.0
+            if 0 < x0 < nx - 1:
+                mat[1 + ld * 0], mat[1 + ld * 1] = mat[0] ** 2, mat[0 + ld * 1] ** 2
+            if x0 == 0:
+                mat[1 + ld * 0], mat[1 + ld * 1] = 1.0, 0.0
+            if x0 == nx - 1:
+                mat[1 + ld * 0], mat[1 + ld * 1] = 0.0, 1.0
+            mat[2 + ld * 0] = mat[2 + ld * 1] = 0.0
+            mat[2 + ld * 2] = rval[y0 - nx] - rval[y0] if a0 > 0 else 0.0
+            mat[2 + ld * 3] = rval[y0 + nx] - rval[y0] if a0 < nr - 1 else 0.0
+            mat[3 + ld * 0] = mat[3 + ld * 1] = 0.0
+            if 0 < a0 < nr - 1:
+                mat[3 + ld * 2], mat[3 + ld * 3] = mat[2 + ld * 2] ** 2, mat[2 + ld * 3] ** 2
+            if a0 == 0:
+                mat[3 + ld * 2], mat[3 + ld * 3] = 1.0, 0.0
+            if a0 == nr - 1:
+                mat[3 + ld * 2], mat[3 + ld * 3] = 0.0, 1.0
+            blk = invm[16 * y0:16 * y0 + 16].copy()
+            assert lib.opc_dgesv(4, 4, p(mat), 4, 4, 4, p(ipiv), p(blk), 4) == 0
+            invm[16 * y0:16 * y0 + 16] = blk
+            assert mat[1 + ld * 2] == 0.0 and mat[1 + ld * 3] == 0.0
+    assert np.allclose(invm, O.s2d_invm(xval, rval, nx, nr), rtol=1e-12, atol=1e-12 * np.abs(invm).max())
+
+
 def test_rangen_streams(lib):
     seeds = np.array([5489, 7, 4294967295], dtype=np.uint32)
     lib.opc_rangen_init_seed(p(seeds), 3)
