@@ -56,6 +56,37 @@ def test_header_compiles_as_c(tmp_path):
                     str(tmp_path / "t")], check=True)
 
 
+def test_c_host_program_links_and_calls(tmp_path):
+    """A plain C host, as a P/Invoke or cgo binding would be, links the library by name and
+    calls its host-side entry points: version, status strings, the niter rule, workspace
+    sizes and a host-side argument rejection read back through opcuda_get_status."""
+    from oplib_b200 import _lib
+    src = tmp_path / "host.c"
+    src.write_text(r"""
+#include <stdio.h>
+#include <string.h>
+#include "opcuda_b200.h"
+int main(void) {
+    int n = 0;
+    double dt = 0.0;
+    if (!strstr(opb_version(), "sm_100a")) return 1;
+    if (opb_plan_interval(1108.0573710154804, 0.25, 0.00006103515625, &n, &dt) != OPB_OK || n != 12) return 2;
+    if (opb_lattice_workspace_size(512, 64, 2) == 0) return 3;
+    if (opb_sgemm4_task_size() != 48) return 4;
+    if (opcuda_ssqmm(-3, 1, 1, 1, 1) != OPB_E_ARG || opcuda_get_status() != OPB_E_ARG) return 5;
+    printf("%s|%s\n", opb_status_string(OPB_E_ARG), opb_status_string(OPB_E_NULL));
+    return 0;
+}
+""")
+    libdir = str(_lib.LIB_PATH.parent)
+    exe = tmp_path / "host"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", str(ROOT / "include"), str(src), "-o", str(exe),
+                    "-L", libdir, "-lopcuda_b200", "-Wl,-rpath," + libdir], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out
+    assert out.stdout.strip() == "invalid size or count|null pointer"
+
+
 def test_version_and_status_strings(lib):
     assert b"sm_100a" in lib.opb_version()
     assert lib.opb_status_string(-1) == b"invalid size or count"
