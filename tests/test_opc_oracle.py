@@ -392,3 +392,35 @@ def test_bstest_through_the_restated_cpu_path(lib):
     assert abs(price_mc - price_lattice) < 4 * se, (price_mc, price_lattice, se)
     # 12.3301 against 12.3310 (the closed form at T = 365 / 365.25; 12.33600 at T = 1)
     assert abs(price_lattice - float(O.bs_call(S, K, r, sig, T))) < 5e-3, price_lattice
+
+
+def test_reference_cpu_sampler_and_device_definition_sample_the_same_law(lib, lv64):
+    """The reference's CPU Monte Carlo (opc_dmc1: FP64 rows, bracket table, u = x / 2^32)
+    and this project's sampling definition (FP32 cumulative rows, u = (x + 1) / 2^32, the
+    device kernel's bit-exact oracle) draw from different streams, so they can only agree in
+    law: the terminal-state histograms of 2^17 paths x 10 steps each pass a chi-square test
+    against the lattice's exact 10-step distribution."""
+    import scipy.stats
+    P, y0 = lv64
+    d = P.shape[0]
+    nscen, nk = 1 << 17, 10
+    tpk = np.asfortranarray(P).ravel(order="K").copy()
+    ctpk = np.empty(d * d)
+    hash_ = np.empty(d * d, dtype=np.int32)
+    lib.opc_host_mc_hash(p(tpk), d, 1, p(ctpk), p(hash_))
+    lib.opc_rangen_init_seed(p(np.array([777], dtype=np.uint32)), 1)
+    unif = np.empty(nscen, dtype=np.uint32)
+    y_sk = np.empty(nscen * nk, dtype=np.int16)
+    m_k = np.zeros(nk, dtype=np.int32)
+    assert lib.opc_dmc1(p(ctpk), p(hash_), d, nscen, nk, y0, p(unif), p(y_sk), p(m_k), 0, 0, 0) == 0
+    lib.opc_rangen_finalize()
+    ref_final = y_sk.reshape(nk, nscen)[-1]
+    own_paths, _ = OC.mc_paths(O.cumrows_f32(P), y0, 777, 0, nscen, nk)
+    own_final = own_paths[:, -1]
+    exact = np.linalg.matrix_power(P, nk)[y0]
+    keep = exact * nscen >= 20  # chi-square cells with enough expected counts
+    for final in (ref_final, own_final):
+        counts = np.bincount(final, minlength=d).astype(np.float64)
+        obs = np.append(counts[keep], counts[~keep].sum())
+        exp = np.append(exact[keep], exact[~keep].sum()) * nscen
+        assert scipy.stats.chisquare(obs, exp).pvalue > 1e-4
