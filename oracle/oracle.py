@@ -397,6 +397,22 @@ def chain(P1: np.ndarray, nmat: int) -> list[np.ndarray]:
     return out
 
 
+def mc_plan_kernels(plan, generators) -> list[np.ndarray]:
+    """Step kernels of a Monte Carlo plan in FP64: elementary kernels
+    X_j = (I + dt_j L_{i_j})^(2^niter_j) (``CModel Host Double.cs:125-197``) and step
+    kernels X_{f0} . X_{f1} . ... over each step's factors in time order.  ``plan`` has the
+    planner's ``i_j``, ``dt_j``, ``niter_j`` and ``jfactor_ms``; ``generators[i]`` is the
+    dense generator that holds on generator interval i."""
+    X = [square(ek(generators[i], dt), n) for i, dt, n in zip(plan.i_j, plan.dt_j, plan.niter_j)]
+    out = []
+    for factors in plan.jfactor_ms:
+        P = X[factors[0]].copy()
+        for j in factors[1:]:
+            P = P @ X[j]
+        out.append(P)
+    return out
+
+
 def payoff_calls(x: np.ndarray, strikes: np.ndarray) -> np.ndarray:
     """G[y, k] = (x_y - K_k)^+."""
     return np.maximum(x[:, None] - strikes[None, :], 0.0)
