@@ -156,6 +156,19 @@ def test_workspace_sizes(lib):
     assert lib.opb_sgemv4_task_size() == 56
 
 
+def test_wall_clock_timers(lib):
+    """opcuda_create/reset/stop_timer and opcuda_get_timer_value (oplib/opmodel/types/
+    CStopWatch.cs:44-54 binds them): seconds between the last reset and the last stop."""
+    import time
+    lib.opcuda_create_timer()
+    time.sleep(0.02)
+    lib.opcuda_stop_timer()
+    v = lib.opcuda_get_timer_value()
+    assert 0.015 < v < 5.0
+    lib.opcuda_reset_timer()
+    assert lib.opcuda_get_timer_value() == 0.0
+
+
 def test_injected_alloc_failure(lib):
     # the hook fails the next allocation on the host side, before any CUDA call
     assert lib.opb_test_fail_next_alloc(1) == 0
