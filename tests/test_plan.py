@@ -82,3 +82,104 @@ def test_step_ending_on_a_generator_date_keeps_its_own_kernel():
 def test_plan_rejections(t_k, t_i, dt0):
     with pytest.raises(ValueError):
         make_mc_plan(t_k, t_i, dt0, [1.0] * len(t_i))
+
+
+def _literal_plan(t_k, t_i):
+    """A line-by-line transcription of make_mc_plan's index loops
+    (CModel Common.cs:187-259, 323-475), dates in days after today (= 0)."""
+    nk, ni = len(t_k), len(t_i)
+    t_q = sorted(t_k + t_i)
+    q0 = 0
+    for q in range(1, len(t_q)):
+        if t_q[q] > t_q[q0] and t_q[q] <= t_k[nk - 1]:
+            q0 += 1
+            t_q[q0] = t_q[q]
+    nq = q0 + 1
+    t_q = t_q[:nq]
+    i_q = [0] * nq
+    i = 0
+    for q in range(nq):
+        if t_q[q] <= t_i[i]:
+            i_q[q] = i
+        else:
+            i += 1
+            i_q[q] = i
+    todo_q = [True] * nq
+    for q2 in range(1, nq):
+        if t_q[q2] - t_q[q2 - 1] == t_q[0] - 0 and i_q[0] == i_q[q2]:
+            todo_q[q2] = False
+    for q1 in range(1, nq):
+        for q2 in range(q1 + 1, nq):
+            if t_q[q2] - t_q[q2 - 1] == t_q[q1] - t_q[q1 - 1] and i_q[q1] == i_q[q2]:
+                todo_q[q2] = False
+    j_q = [0] * nq
+    nj = 0
+    for q1 in range(nq):
+        if todo_q[q1]:
+            j_q[q1] = nj
+            nj += 1
+            for q2 in range(q1 + 1, nq):
+                if i_q[q1] == i_q[q2]:
+                    if q1 == 0:
+                        if t_q[q2] - t_q[q2 - 1] == t_q[q1] - 0:
+                            j_q[q2] = j_q[q1]
+                    elif t_q[q2] - t_q[q2 - 1] == t_q[q1] - t_q[q1 - 1]:
+                        j_q[q2] = j_q[q1]
+
+    def first_ge(t):
+        ii = 0
+        while ii < ni and t_i[ii] < t:
+            ii += 1
+        return ii
+
+    def key(k):
+        i1 = first_ge(t_k[k])
+        if k == 0:
+            return i1, 0, t_k[k] - 0
+        return i1, first_ge(t_k[k - 1]), t_k[k] - t_k[k - 1]
+
+    todo_k = [True] * nk
+    for k1 in range(nk):
+        i1, ii1, dt1 = key(k1)
+        if i1 == ii1:
+            for k2 in range(k1 + 1, nk):
+                i2, ii2, dt2 = key(k2)
+                if i2 == ii2 and i1 == i2 and dt1 == dt2:
+                    todo_k[k2] = False
+    m_k = [0] * nk
+    nm = 0
+    for k in range(nk):
+        if todo_k[k]:
+            m_k[k] = nm
+            nm += 1
+    for k1 in range(nk):
+        if todo_k[k1]:
+            i1, ii1, dt1 = key(k1)
+            if i1 == ii1:
+                for k2 in range(k1 + 1, nk):
+                    i2, ii2, dt2 = key(k2)
+                    if i2 == ii2 and i1 == i2 and dt1 == dt2:
+                        m_k[k2] = m_k[k1]
+    jf = [None] * nm
+    for k in range(nk):
+        t0 = t_k[k - 1] if k > 0 else 0
+        fs = [j_q[q] for q in range(nq) if (t_q[q - 1] if q > 0 else 0) >= t0 and t_q[q] <= t_k[k]]
+        if jf[m_k[k]] is None:
+            jf[m_k[k]] = fs
+    return t_q, i_q, j_q, m_k, jf
+
+
+def test_planner_matches_a_literal_transcription_on_random_schedules():
+    rng = np.random.default_rng(20260)
+    for _ in range(300):
+        nk = int(rng.integers(1, 12))
+        t_k = sorted(set(int(v) for v in rng.integers(1, 200, nk)))
+        ni = int(rng.integers(1, 5))
+        t_i = sorted(set(int(v) for v in rng.integers(1, 200, ni - 1)) | {t_k[-1] + int(rng.integers(0, 30))})
+        plan = make_mc_plan(t_k, t_i, 1, [1000.0] * len(t_i))
+        t_q, i_q, j_q, m_k, jf = _literal_plan(t_k, t_i)
+        assert (plan.t_q, plan.i_q, plan.j_q, plan.m_k, plan.jfactor_ms) == (t_q, i_q, j_q, m_k, jf)
+        # every step's factors tile its interval, and each factor lies under one generator
+        for k, m in enumerate(plan.m_k):
+            span = sum(plan.t1_j[j] - plan.t0_j[j] for j in plan.jfactor_ms[m])
+            assert span == t_k[k] - (t_k[k - 1] if k else 0)
