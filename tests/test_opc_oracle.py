@@ -424,3 +424,46 @@ def test_reference_cpu_sampler_and_device_definition_sample_the_same_law(lib, lv
         obs = np.append(counts[keep], counts[~keep].sum())
         exp = np.append(exact[keep], exact[~keep].sum()) * nscen
         assert scipy.stats.chisquare(obs, exp).pvalue > 1e-4
+
+
+def test_dmc1_threads_run_their_own_streams(lib, lv64):
+    """host_d_mc_run1f (CModel Host Double.cs:319-377) runs opc_dmc1 on every core at once,
+    thread th on stream th: four concurrent threads produce the paths that the same calls
+    produce one after another."""
+    import threading
+    P, y0 = lv64
+    d = P.shape[0]
+    tpk = np.asfortranarray(P).ravel(order="K").copy()
+    ctpk = np.empty(d * d)
+    hash_ = np.empty(d * d, dtype=np.int32)
+    lib.opc_host_mc_hash(p(tpk), d, 1, p(ctpk), p(hash_))
+    nth, nscen, nk = 4, 8192, 12
+    seeds = np.array([101, 202, 303, 404], dtype=np.uint32)
+    m_k = np.zeros(nk, dtype=np.int32)
+
+    def run(concurrent):
+        lib.opc_rangen_init_seed(p(seeds), nth)
+        unif = [np.empty(nscen, dtype=np.uint32) for _ in range(nth)]
+        ys = [np.empty(nscen * nk, dtype=np.int16) for _ in range(nth)]
+        rc = [None] * nth
+
+        def work(th):
+            rc[th] = lib.opc_dmc1(p(ctpk), p(hash_), d, nscen, nk, y0, p(unif[th]), p(ys[th]), p(m_k), 0, th, 0)
+
+        if concurrent:
+            workers = [threading.Thread(target=work, args=(th,)) for th in range(nth)]
+            for w in workers:
+                w.start()
+            for w in workers:
+                w.join()
+        else:
+            for th in range(nth):
+                work(th)
+        lib.opc_rangen_finalize()
+        assert rc == [0] * nth
+        return ys
+
+    together, alone = run(True), run(False)
+    for a, b in zip(together, alone):
+        assert np.array_equal(a, b)
+    assert not np.array_equal(together[0], together[1])
