@@ -43,7 +43,8 @@ def load():
     global _lib
     if _lib is not None:
         return _lib
-    if not LIB.exists():
+    sources = [HERE / "opc.c", HERE / "opc.h"]
+    if not LIB.exists() or LIB.stat().st_mtime < max(s.stat().st_mtime for s in sources):
         subprocess.run(["make", "-C", str(HERE), "-s"], check=True)
     lib = C.CDLL(str(LIB))
     for name, (res, args) in PROTOTYPES.items():
