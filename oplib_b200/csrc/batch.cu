@@ -485,6 +485,7 @@ int batch_square(opb_batch_plan *P, cudaStream_t s) {
 // one renormalisation launch each), chaining and pricing.  quotes: device
 // [nlat][nmat][nK] FP64.  No host synchronisation, no allocation (graph-capturable).
 OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
+    OPB_NVTX("opb_batch_execute");
     OPB_REQUIRE(P && quotes, OPB_E_NULL);
     cudaStream_t s = opb::stream();
     int r = 0;
@@ -524,6 +525,7 @@ OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
 // product P1_i . V_i over all lattices and one FP64 step.  quotes: device [nlat][nK] FP64,
 // the values at each lattice's y0.  No host synchronisation, no allocation.
 OPB_API int opb_batch_execute_bermudan(opb_batch_plan *P, int put, int exercise, double barrier, double *quotes) {
+    OPB_NVTX("opb_batch_execute_bermudan");
     OPB_REQUIRE(P && quotes, OPB_E_NULL);
     OPB_REQUIRE(put >= 0 && put <= 1 && exercise >= 0 && exercise <= 1 && barrier >= 0.0, OPB_E_ARG);
     cudaStream_t s = opb::stream();

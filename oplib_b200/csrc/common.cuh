@@ -8,6 +8,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #define OPB_API extern "C" __attribute__((visibility("default")))
@@ -33,7 +34,18 @@ int launch_check();               // cudaGetLastError -> status
 
 inline bool aligned(const void *p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
 
+// Profiler range over one library call (NVTX; a no-op unless a profiler is attached), so
+// that a capture can select a call's kernels by name.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
 }  // namespace opb
+
+#define OPB_NVTX(name) opb::NvtxRange opb_nvtx_range_(name)
 
 #define OPB_TRY(expr)                                  \
     do {                                               \

@@ -364,6 +364,7 @@ OPB_API unsigned long long opb_lattice_workspace_size(int d, int nK, int mode) {
 // opb_lattice_workspace_size(d, nK, mode) bytes.
 OPB_API int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
                               double *quotes, double *V_all) {
+    OPB_NVTX("opb_lattice_solve");
     int c = check_desc(L, mode);
     if (c == OPB_OK && !quotes) c = OPB_E_NULL;
     if (c != OPB_OK) return opb::set_status(c);
@@ -390,6 +391,7 @@ OPB_API int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspa
 // workspace as for opb_lattice_solve.
 OPB_API int opb_lattice_bermudan(const opb_lattice_desc *L, int mode, int put, int exercise, double barrier,
                                  void *workspace, unsigned long long ws_bytes, double *quotes) {
+    OPB_NVTX("opb_lattice_bermudan");
     int c = check_desc(L, mode);
     if (c == OPB_OK && !quotes) c = OPB_E_NULL;
     if (c == OPB_OK && (put < 0 || put > 1 || exercise < 0 || exercise > 1 || !(barrier >= 0.0))) c = OPB_E_ARG;

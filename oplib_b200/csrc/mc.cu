@@ -175,6 +175,7 @@ OPB_API int opb_mc_mt19937(const float *C, long long row_stride, long long col_s
                            int nb, int d, int y0, int nsteps, uint32_t seed, unsigned long long path0,
                            long long npaths, short *ypaths, const double *x, double strike, double barrier,
                            double disc, double *scratch, double *sums) {
+    OPB_NVTX("opb_mc_mt19937");
     OPB_REQUIRE(d > 0 && d <= 32767 && y0 >= 0 && y0 < d, OPB_E_ARG);
     OPB_REQUIRE(nsteps >= 1 && npaths >= 0, OPB_E_ARG);
     OPB_REQUIRE(C != nullptr, OPB_E_NULL);
@@ -243,6 +244,7 @@ OPB_API int opcuda_mc_setseed(uint64_t host_seedptr, uint64_t mtptr) {
 // smc.cu:622) any d <= 32767 is accepted, and any nk >= 1.
 OPB_API int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk, int d, uint64_t ctpker_m_yy,
                         uint64_t m_k, uint64_t yhostptr) {
+    OPB_NVTX("opcuda_mc1f");
     OPB_REQUIRE(mtptr != 0 && y_sk != 0 && ctpker_m_yy != 0 && m_k != 0, OPB_E_NULL);
     OPB_REQUIRE(d > 0 && d <= 32767 && y0 >= 0 && y0 < d && nscen >= 0, OPB_E_ARG);
     OPB_REQUIRE(nk >= 1, OPB_E_ARG);

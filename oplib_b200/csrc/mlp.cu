@@ -479,6 +479,7 @@ OPB_API long long opb_mlp_infer_workspace_bytes(long long n, int nmem) {
 // spread [n] (optional) receive the ensemble mean and max - min of the member outputs.
 OPB_API int opb_mlp_infer(const void *packed, int nmem, long long member_stride, const float *X, long long n,
                           void *ws, long long ws_bytes, float *mean, float *spread) {
+    OPB_NVTX("opb_mlp_infer");
     OPB_REQUIRE(packed && X && ws && mean, OPB_E_NULL);
     OPB_REQUIRE(nmem >= 1 && n >= 1 && member_stride >= MLP_PACK_BYTES, OPB_E_ARG);
     OPB_REQUIRE(ws_bytes >= opb_mlp_infer_workspace_bytes(n, nmem), OPB_E_ARG);
