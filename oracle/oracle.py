@@ -15,9 +15,13 @@ are pinned as follows (see ``tests/test_oracle.py``):
 * Lattice pricing: against the Black-Scholes closed form (the reference's only known-
   answer test, ``tests/bstest/Program.cs:11-37``), against ``scipy.linalg.expm``, and
   by probability conservation / semigroup identities.
-* The reference implementation itself cannot be built here: its CPU path needs Intel
-  MKL (``oplib/opc/rangen.cpp:36``), its model layer needs .NET, and its CUDA path
-  passes 32-bit device pointers (``oplib/opcuda/util.cu:170-175``).
+* The reference's own CUDA kernels for cumulative rows, kernels from generators, strided
+  dot products, multi-vector induction, the jump generator and fills are compiled from its
+  unchanged sources (``oracle/Makefile`` -> ``oracle/_ref``) and launched directly by
+  ``oracle/ref_opcuda.cu`` (its exported wrappers pass 32-bit device pointers,
+  ``oplib/opcuda/util.cu:170-175``); ``tests/test_gpu_ref_kernels.py`` compares the drop-in
+  entry points with them.  The rest of the reference cannot be built here: its CPU path
+  needs Intel MKL (``oplib/opc/rangen.cpp:36``) and its model layer needs .NET.
 
 Layout convention.  The reference stores the transition element (source y1 -> target
 y2) at ``y1 + d*y2`` (column-major with rows = source; ``oplib/opmodel/models/
@@ -135,21 +139,24 @@ def lv_invm(x: np.ndarray) -> np.ndarray:
     """Per-node inverse of the 2x2 moment matrix [[dm, dp], [dm^2, dp^2]].
 
     Follows ``oplib/opmodel/types/S1DGrid.cs:78-147`` (``pregen``): dm = x[i-1]-x[i],
-    dp = x[i+1]-x[i]; the first and last nodes get the boundary rows of
-    S1DGrid.cs:95-128.  Returns an array (d, 2, 2) of inverses (row-major 2x2)."""
+    dp = x[i+1]-x[i], with 1 in place of the missing spacing at either end
+    (S1DGrid.cs:95-110).  The second row is [dm^2, dp^2] for every node but the first,
+    which gets [0, 1]: the reference's test ``x0 > 0 && x0 < d`` (S1DGrid.cs:111) also holds
+    for the last node, so the last node's row is [dm^2, 1] and the ``x0 == d - 1`` branch
+    (S1DGrid.cs:123-127) is never reached.  The boundary inverses are unused: the generator
+    zeroes the boundary nodes' rates (CLVModel.cs:99-114).  Returns an array (d, 2, 2) of
+    inverses (row-major 2x2)."""
     d = x.shape[0]
     inv = np.zeros((d, 2, 2))
     for i in range(d):
         m = np.zeros((2, 2))
         m[0, 0] = x[i - 1] - x[i] if i > 0 else 1.0
         m[0, 1] = x[i + 1] - x[i] if i < d - 1 else 1.0
-        if 0 < i < d - 1:
+        if i > 0:
             m[1, 0] = m[0, 0] ** 2
             m[1, 1] = m[0, 1] ** 2
-        elif i == 0:
-            m[1, 0], m[1, 1] = 0.0, 1.0
         else:
-            m[1, 0], m[1, 1] = 1.0, 0.0
+            m[1, 0], m[1, 1] = 0.0, 1.0
         inv[i] = np.linalg.inv(m)
     return inv
 
@@ -424,6 +431,40 @@ def price_from_kernels(Ps: list[np.ndarray], x: np.ndarray, strikes: np.ndarray,
     discounting exp(-r T).  Returns V[m, y, k]."""
     G = payoff_calls(x, strikes)
     return np.stack([math.exp(-r * T) * (P @ G) for P, T in zip(Ps, mats)])
+
+
+def host_solve_stages(L, x, strikes, r: float, period: float, nmat: int, niter: int, dt: float):
+    """The reference's host FP64 solve, one product at a time, on torch-CPU FP64 tensors
+    (the matrix products are MKL DGEMMs, the library family of ``opc_dgemm``,
+    ``oplib/opc/linalg.c:93-101``):
+
+    * U0 = I + dt L (``host_d_mc_ek``, ``CModel Host Double.cs:89-121``);
+    * niter squarings U <- U.U (``host_d_mc_sq``, ``CModel Host Double.cs:125-197``);
+    * chaining P_m = P_{m-1}.P1, m = 2..nmat (``host_d_mc_mk``, ``CModel Host Double.cs:227-277``);
+    * the payoff product V_m = exp(-r m period) P_m.G for every source state once P_m is
+      formed (the backward induction the reference exports as ``sgemv``/``sdot2`` kernels).
+
+    No renormalisation: the reference's host path has none (row sums stay 1 to FP64
+    rounding).  A generator that yields once per product, niter + nmat - 1 times (U0 is built
+    in the first stage, each payoff product in the stage that forms its P_m): None, and at the
+    last stage V [nmat, d, nK].  niter >= 1.  L: torch FP64 [d, d] (row = source)."""
+    import torch
+    xs = torch.as_tensor(np.asarray(x, dtype=np.float64))
+    K = torch.as_tensor(np.asarray(strikes, dtype=np.float64))
+    G = torch.clamp(xs[:, None] - K[None, :], min=0.0)
+    V = []
+    U = L * dt
+    U.diagonal().add_(1.0)
+    for lev in range(niter):
+        U = U @ U
+        if lev == niter - 1:
+            V.append(math.exp(-r * period) * (U @ G))
+        yield torch.stack(V) if (lev == niter - 1 and nmat == 1) else None
+    P1 = Pm = U
+    for m in range(2, nmat + 1):
+        Pm = Pm @ P1
+        V.append(math.exp(-r * period * m) * (Pm @ G))
+        yield torch.stack(V) if m == nmat else None
 
 
 # ---------------------------------------------------------------------------------

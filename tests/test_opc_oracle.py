@@ -111,7 +111,10 @@ def test_sgesv_and_singular_info(lib):
 def test_s1dgrid_pregen_through_dgesv_matches_oracle_invm(lib):
     """S1DGrid.pregen (oplib/opmodel/types/S1DGrid.cs:78-147) step for step: identity
     blocks in invm, the 2x2 moment matrix per node, opc_dgesv(2, 2, mat, 2, 2, 2, ipiv,
-    invm + 4*x0, 2).  The oracle's lv_invm must be the same inverses."""
+    invm + 4*x0, 2).  The branch structure is the reference's: the second row is
+    [dm^2, dp^2] whenever 0 < x0 < d, so also for the last node (dp = 1 there), and the
+    boundary rows [0, 1] / [1, 0] sit in the else branch, of which only x0 == 0 is ever
+    taken.  The oracle's lv_invm must be the same inverses."""
     x = 0.05 * 100.0 ** (np.arange(512) / 511.0)
     d = x.size
     invm = np.zeros(4 * d)
@@ -125,16 +128,20 @@ def test_s1dgrid_pregen_through_dgesv_matches_oracle_invm(lib):
         mat[2] = x[x0 + 1] - x[x0] if x0 < d - 1 else 1.0
         if 0 < x0 < d:
             mat[1], mat[3] = mat[0] ** 2, mat[2] ** 2
-        if x0 == 0:
-            mat[1], mat[3] = 0.0, 1.0
-        if x0 == d - 1:
-            mat[1], mat[3] = 1.0, 0.0
+        else:
+            if x0 == 0:
+                mat[1], mat[3] = 0.0, 1.0
+            if x0 == d - 1:
+                mat[1], mat[3] = 1.0, 0.0
         blk = invm[4 * x0:4 * x0 + 4].copy()
         assert lib.opc_dgesv(2, 2, p(mat), 2, 2, 2, p(ipiv), p(blk), 2) == 0
         invm[4 * x0:4 * x0 + 4] = blk
     ref = O.lv_invm(x)  # (d, 2, 2) row-major
     got = invm.reshape(d, 2, 2).transpose(0, 2, 1)  # column-major blocks
     assert np.allclose(got, ref, rtol=1e-12, atol=0)
+    # the last node's moment matrix is [[dm, 1], [dm^2, 1]]
+    dm = x[-2] - x[-1]
+    assert np.allclose(got[-1], np.linalg.inv([[dm, 1.0], [dm * dm, 1.0]]), rtol=1e-12, atol=0)
 
 
 @pytest.mark.parametrize("xs,rs", [((0.05, 5.0), (0.05, 1.0)), ((10.0, 300.0), (0.5, 40.0))])

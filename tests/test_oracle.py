@@ -245,3 +245,20 @@ def test_bermudan_oracle_identities():
     assert np.all(dao <= euro_call + 1e-14)
     y0 = O.nearest_node(x)
     assert np.all(dao[y0] < euro_call[y0] - 1e-4)
+
+
+def test_host_solve_stages_matches_the_fp64_solve():
+    """The staged host solve (the bench's reference arm: U0, squarings, chain products and
+    payoff products one product per stage) is the oracle's FP64 solve without
+    renormalisation, and yields once per product with the values at the last stage."""
+    import torch
+    cfg = O.LVLattice(n=256, nmat=5)
+    L, x = cfg.generator()
+    niter, dt = O.plan_niter(L, cfg.period, cfg.dt0)
+    outs = list(O.host_solve_stages(torch.from_numpy(L.copy()), x, cfg.strikes, cfg.r, cfg.period, cfg.nmat,
+                                    niter, dt))
+    assert len(outs) == niter + cfg.nmat - 1 and all(o is None for o in outs[:-1])
+    V, _, _ = O.solve_lattice_fp64(L, x, cfg.strikes, cfg.r, cfg.period, cfg.nmat, cfg.dt0, renorm=False)
+    assert np.allclose(outs[-1].numpy(), V, rtol=1e-12, atol=1e-14)
+    one = list(O.host_solve_stages(torch.from_numpy(L.copy()), x, cfg.strikes, cfg.r, cfg.period, 1, niter, dt))
+    assert len(one) == niter and np.allclose(one[-1].numpy()[0], V[0], rtol=1e-12, atol=1e-14)
