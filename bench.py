@@ -124,11 +124,11 @@ def fp64_reference_quotes(lat, plan, torch):
     return torch.stack(out)
 
 
-def fp32_cublas_solve(lat, plan, strikes, torch, out):
+def fp32_cublas_solve(lat, plan, strikes, torch, out, nmat=NMAT, period=PERIOD):
     """The plain-FP32 comparison arm on cuBLAS (TF32 off): U0 = I + dt L in FP32 from the
     ELL generator, niter squarings and the chain products as cuBLAS SGEMMs, each followed by
     the FP64 row renormalisation that the 1e-5 bar needs (FP64 row sums, FP32 scaling),
-    pricing P(T_m) G in FP32 and the FP64 discount.  Writes quotes [NMAT, NK] into out."""
+    pricing P(T_m) G in FP32 and the FP64 discount.  Writes quotes [nmat, nK] into out."""
     d = lat.d
     dev = lat.device
     cols = lat.cols.view(d, -1).long()
@@ -150,12 +150,12 @@ def fp32_cublas_solve(lat, plan, strikes, torch, out):
         renorm(P)
     G = torch.clamp(lat.x.unsqueeze(1) - strikes.unsqueeze(0), min=0.0).float()
     Pm = P.clone()
-    for m in range(1, NMAT + 1):
+    for m in range(1, nmat + 1):
         if m > 1:
             torch.mm(Pm, P, out=T)
             Pm, T = T, Pm
             renorm(Pm)
-        out[m - 1] = math.exp(-lat.rate * PERIOD * m) * (Pm[lat.y0] @ G).double()
+        out[m - 1] = math.exp(-lat.rate * period * m) * (Pm[lat.y0] @ G).double()
     return out
 
 
@@ -372,7 +372,8 @@ def run_b200(args, rank, world, local_rank):
     # gpu launches per step (library kernels): generator, E0 scatter, split, niter*(gemm+renorm),
     # add_identity, split, payoff, nmat*(price gemm + discount), (nmat-1)*(chain gemm + renorm)
     if mode == MODES["bf16x3"]:
-        launches = 1 + 1 + 1 + 2 * plan.niter + 1 + 1 + 1 + 2 * NMAT + 2 * (NMAT - 1)
+        # ... + the generator's band (one block)
+        launches = 1 + 1 + 1 + 1 + 2 * plan.niter + 1 + 1 + 1 + 2 * NMAT + 2 * (NMAT - 1)
     else:
         launches = 1 + 2 + (3 if mode == 1 else 1) * plan.niter + 1 + 2 * NMAT + (3 if mode == 1 else 1) * (NMAT - 1)
     out = {
@@ -390,6 +391,104 @@ def run_b200(args, rank, world, local_rank):
     }
     out.update(extra)
     return out
+
+
+SWEEP_METRIC = "priced quotes/sec, calibration sweep (512 LV lattices, one tensor-core launch per level)"
+
+
+def sweep_summary(args):
+    """Config 3 beside the headline: the 512 seeded local-vol lattices (seed 20260, n in
+    256..2048 step 128, 32 strikes x 8 quarterly maturities = 131,072 quotes) solved by the
+    batched split path in bf16x3 and fp16x3 (every squaring level of all lattices one
+    persistent launch, the sweep replayed from a CUDA graph, autotuned tiles), each lattice's
+    quotes against an FP64 solve of it (all 512), and the two plain-FP32 arms on the same
+    lattices: cuBLAS SGEMM (TF32 off) with FP64 renormalisation, per lattice, and the
+    library's SIMT FP32 solve per lattice.  The speed-up is against the faster FP32 arm."""
+    import torch
+    from oplib_b200.model import Batch, bind_stream, calibration_sweep
+    dev = torch.device("cuda", 0)
+    bind_stream(dev)
+    stream = torch.cuda.current_stream(dev)
+    nlat, nmat, period, dt0 = 512, 8, 0.25, 2.0 ** -14
+    strikes = [0.5 + j / 31.0 for j in range(32)]
+    nq = nlat * nmat * len(strikes)
+    t_all = time.perf_counter()
+    lats, _ = calibration_sweep(nlat=nlat, device=dev)
+    out, plans = {}, None
+    for mode in ("bf16x3", "fp16x3"):
+        b = Batch(lats, strikes, nmat, period, dt0, mode=mode, autotune=True)
+        plans = b.plans
+        q = torch.empty(nlat, nmat, len(strikes), dtype=torch.float64, device=dev)
+        for _ in range(max(1, args.warmup)):
+            b.execute(q)
+        g = _graph(lambda: b.execute(q), dev, torch)
+        g.replay()
+        ms = _time(g.replay, max(3, args.steps), stream, torch)
+        out[mode] = {"quotes_per_s": round(nq / (ms * 1e-3), 1), "ms_per_sweep": round(ms, 3),
+                     "config_chosen": b.config, "launches_per_sweep": b.launches(), "q": q.clone()}
+        del g, b, q
+    K = torch.tensor(strikes, dtype=torch.float64, device=dev)
+    ref = torch.stack([_fp64_lv_quotes(lat, pl, strikes, nmat, period, torch) for lat, pl in zip(lats, plans)])
+    tf32 = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    qcu = torch.empty(nlat, nmat, len(strikes), dtype=torch.float64, device=dev)
+
+    def cublas_sweep():
+        for i, (lat, pl) in enumerate(zip(lats, plans)):
+            fp32_cublas_solve(lat, pl, K, torch, qcu[i], nmat=nmat, period=period)
+
+    cublas_sweep()
+    ms_cu = _time(cublas_sweep, 1, stream, torch)
+    torch.backends.cuda.matmul.allow_tf32 = tf32
+    b32 = Batch(lats, strikes, nmat, period, dt0, mode="fp32", autotune=False)
+    q32 = b32.execute()
+    ms_si = _time(lambda: b32.execute(q32), 1, stream, torch)
+    torch.cuda.synchronize()
+    res = {"metric": SWEEP_METRIC, "unit": "quotes/s", "quotes_per_sweep": nq,
+           "workload": f"{nlat} LV lattices (seed 20260), n in 256..2048 step 128, niter "
+                       f"{min(p.niter for p in plans)}..{max(p.niter for p in plans)}, 32 strikes x {nmat} maturities; "
+                       "CUDA-graph replay; error over every lattice against its FP64 solve"}
+    for mode in ("bf16x3", "fp16x3"):
+        o = out[mode]
+        e = (o.pop("q") - ref).abs().amax(dim=(1, 2))
+        o["max_abs_err_vs_fp64"] = float(e.max().item())
+        o["lattices_above_1e-5"] = int((e > 1e-5).sum().item())
+        res[mode] = o
+    res["fp32_cublas"] = {"quotes_per_s": round(nq / (ms_cu * 1e-3), 1), "ms_per_sweep": round(ms_cu, 1),
+                          "max_abs_err_vs_fp64": float((qcu - ref).abs().max().item())}
+    res["fp32_simt"] = {"quotes_per_s": round(nq / (ms_si * 1e-3), 1), "ms_per_sweep": round(ms_si, 1),
+                        "max_abs_err_vs_fp64": float((q32 - ref).abs().max().item())}
+    fastest32 = min(ms_cu, ms_si)
+    res["fp32_arm"] = "cublas" if ms_cu <= ms_si else "simt"
+    for mode in ("bf16x3", "fp16x3"):
+        res[mode]["speedup_vs_fp32"] = round(fastest32 / res[mode]["ms_per_sweep"], 2)
+    res["wall_s"] = round(time.perf_counter() - t_all, 1)
+    del b32, q32, qcu, ref
+    torch.cuda.empty_cache()
+    return res
+
+
+def surrogate_summary(args):
+    """Config 4 beside the headline: the ensemble surrogate trained in this run by the
+    library's kernels on ~2^21 lattice quotes (2600 seeded local-vol lattices, n = 1024,
+    solved by the batched split path), then 2^20 quotes inferred on the tensor cores with 4
+    and with 2 members: quotes/s, the lattice's quotes/s for the same family, the fallback
+    rate (ensemble spread > 5 bp), the accepted quotes' error against the lattice in bp, and
+    the quotes/s with the fallback quotes' lattices re-solved by the batched sweep."""
+    a = argparse.Namespace(**vars(args))
+    a.epochs, a.members, a.train_lattices = 40, 4, 2600
+    a.steps, a.warmup = max(3, args.steps), max(3, args.warmup)
+    t0 = time.perf_counter()
+    line = run_surrogate(a)
+    keep = ["value", "ms_per_step", "lattice_quotes_per_s", "speedup_vs_lattice", "fallback_rate", "fallback_lattices",
+            "test_quotes", "accepted_err_bp", "all_err_bp", "baseline_err_bp", "effective_quotes_per_s_with_fallback",
+            "two_members", "train_seconds", "data_seconds"]
+    res = {"metric": "surrogate quotes/s (ensemble of 4 MLPs on tensor cores), 2^20 quotes", "unit": "quotes/s",
+           "config": line["config"]}
+    res.update({k: line[k] for k in keep if k in line})
+    res["quotes_per_s"] = res.pop("value")
+    res["wall_s"] = round(time.perf_counter() - t0, 1)
+    return res
 
 
 def _host_info():
@@ -1430,6 +1529,15 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     out = run_b200(args, rank, world, local_rank)
     if rank == 0:
+        if args.compare and world == 1:
+            try:
+                out["config3_sweep"] = sweep_summary(args)
+            except Exception as e:  # a secondary figure must not cost the headline line
+                out["config3_sweep"] = {"error": f"{type(e).__name__}: {e}"[:300]}
+            try:
+                out["config4_surrogate"] = surrogate_summary(args)
+            except Exception as e:
+                out["config4_surrogate"] = {"error": f"{type(e).__name__}: {e}"[:300]}
         if args.cpu:
             out["cpu_baseline"] = cpu_baseline()
         print(json.dumps(out))

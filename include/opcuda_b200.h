@@ -136,7 +136,7 @@ int opcuda_sdot2(uint64_t aptr, uint64_t bptr, uint64_t cptr, int m, int n);
 
 /* ------------------------------------------------------------------ kernels from generators */
 /* replace oplib/opcuda/sek.cu:106-137: column-major U = (I + dt*gen) [/(1 + dt*r*lambda)],
- * formed in FP64 and rounded once */
+ * in the reference kernels' FP32 arithmetic (fused numerator, FP32 division), bit for bit */
 int opcuda_sek(int d, uint64_t genPtr, float dt, uint64_t tpkerPtr);
 int opcuda_sekd(int d, uint64_t genPtr, float dt, uint64_t tpkerPtr, uint64_t rPtr);
 int opcuda_sekd_lambda(int d, uint64_t genPtr, float dt, uint64_t tpkerPtr, uint64_t rPtr, uint64_t lambdaPtr);
@@ -232,7 +232,9 @@ typedef struct opb_lattice_desc {
 } opb_lattice_desc;
 /* new: the device branch of CModel.exe_mc_plan (oplib/opmodel/models/CModel Common.cs:651-669)
  * plus payoff backward induction: quotes[(m-1)*nK + k] = exp(-rate*T_m) * (P(T_m) G)[y0, k],
- * G[z, k] = (x_z - K_k)^+; V_all (optional) receives all states [nmat][d][nK]. */
+ * G[z, k] = (x_z - K_k)^+; V_all (optional) receives all states [nmat][d][nK].  Any d in every
+ * mode: the split modes solve a d that is no multiple of 128 as the lattice padded with
+ * absorbing states up to the next multiple (the workspace size accounts for it). */
 unsigned long long opb_lattice_workspace_size(int d, int nK, int mode);
 int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
                       double *quotes, double *V_all);
@@ -250,9 +252,27 @@ int opb_lattice_bermudan(const opb_lattice_desc *L, int mode, int put, int exerc
  * kernel; nmat, nK and strikes of L are ignored */
 int opb_lattice_kernel(const opb_lattice_desc *L, int mode, void *workspace, unsigned long long ws_bytes,
                        float *P_out);
+/* new: step kernel of a Monte Carlo step that spans several elementary intervals (a generator
+ * date inside the step): out = X_0 . X_1 ... X_{nf-1} of row-major d x d FP32 kernels (factors:
+ * host array of nf device pointers, in time order), FP32 products each renormalised to unit
+ * row sums in FP64.  Replaces the reference's device chaining of the planned factor lists
+ * (oplib/opmodel/models/CModel Device.cs:252-295 over CModel Common.cs:431-486's jfactor_ms) */
+unsigned long long opb_chain_workspace_size(int d);
+int opb_chain_kernels(int d, int nf, const float *const *factors, float *out, void *workspace,
+                      unsigned long long ws_bytes);
 /* new: issue every tensor-core product of the solve as s K-slices summed in the FP32
  * epilogue (shorter in-TMEM accumulation chains); 0 (default) = automatic */
 int opb_set_ksplit(int s);
+/* new: split-BF16 squarings (single and batched solves) add the fourth product lo.lo on their
+ * first n levels; default 8, 0..64.  Leaving lo.lo out everywhere (n = 0) gives the plain
+ * three-product form, whose error reaches 1.4e-5 on the highest-niter lattices of the
+ * calibration sweep; with the default every sweep price is within 2e-6 of FP64 */
+int opb_set_lolo_levels(int n);
+/* new: 1 (default): squarings of an ELL generator's E_r = P(2^r dt) - I skip the K-blocks and
+ * output tiles outside twice E_r's band (h0 * 2^r for the generator's half-bandwidth h0),
+ * whose products are exact zeros; 0: every squaring runs the full product.  Results are
+ * bit-identical either way */
+int opb_set_band_skip(int on);
 
 /* ------------------------------------------------------------------ batched lattices */
 typedef struct opb_batch_desc {
@@ -310,6 +330,11 @@ int opb_mlp_forward(const float *thb, const float *X, int B, float *ws, float *y
 int opb_mlp_loss_grad(const float *thb, const float *X, const float *t, int B, float *ws, float *grad, double *loss);
 int opb_mlp_adam(float *theta, float *m, float *v, const float *grad, int step, float lr, float b1, float b2,
                  float eps, float *theta_bf);
+/* new: opb_mlp_adam with the step count (device int, advanced by the call) and a learning-rate
+ * table (device, lr_table[step - 1]) in device memory: every epoch of a training loop is then
+ * the same launches, captured once in a CUDA graph and replayed */
+int opb_mlp_adam_sched(float *theta, float *m, float *v, const float *grad, int *step, const float *lr_table, float b1,
+                       float b2, float eps, float *theta_bf);
 /* implied volatilities of call prices with spots S0[i] (FP64 bisection); NaN without time value */
 int opb_implied_vol(long long n, const double *price, const double *K, const double *T, const double *r,
                     const double *S0, double *iv);
@@ -338,6 +363,14 @@ int opcuda_mc_setseed(uint64_t host_seedptr, uint64_t mtptr);
 /* replaces oplib/opcuda/smc.cu:610-656 (per-path MT19937 streams; any nk >= 1, d <= 32767) */
 int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk, int d, uint64_t ctpker_m_yy, uint64_t m_k,
                 uint64_t yhostptr);
+/* new, the device side of the reference's opcuda_mc1f + CMCEvaluator.eval pair
+ * (oplib/opmodel/models/CModel Device.cs:343-364, oplib/opmodel/interfaces/CMCEvaluator.cs:41-67):
+ * the paths of opcuda_mc1f (continuing the status record), each valued on the device by a
+ * cashflow table -- results[p] = sum_k cashflow[k*d + y_k] over the steps before the first
+ * state with knockout[k*d + y_k] != 0 (knockout optional, 0) -- so the states need not be
+ * copied to the host; y_sk optional (0).  Blocking, as opcuda_mc1f. */
+int opcuda_mc1f_eval(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk, int d, uint64_t ctpker_m_yy,
+                     uint64_t m_k, uint64_t cashflow, uint64_t knockout, uint64_t results);
 /* replaces oplib/opcuda/smc.cu:731-736 (nscen % 4096 == 0) */
 int opcuda_mt_benchmark(uint64_t mtptr, uint64_t unif_ptr, int nscen);
 /* new: MT19937 Monte Carlo, path p seeded init_genrand(seed + path0 + p); see mc.cu.
@@ -348,6 +381,14 @@ int opb_mc_scratch_blocks(long long npaths);
 int opb_mc_mt19937(const float *C, long long row_stride, long long col_stride, const uint32_t *guide, int nb, int d,
                    int y0, int nsteps, uint32_t seed, unsigned long long path0, long long npaths, short *ypaths,
                    const double *x, double strike, double barrier, double disc, double *scratch, double *sums);
+/* new: opb_mc_mt19937's paths valued by a device-side evaluator instead of the fused payoffs:
+ * v_p = sum_k cashflow[k*d + y_k] (FP64 [nsteps][d], discounting folded in) over the steps
+ * before the first knocked-out state (knockout [nsteps][d] bytes, optional); path_values
+ * (optional) [npaths]; sums[0] = sum v_p, sums[1] = sum v_p^2; scratch as opb_mc_mt19937 */
+int opb_mc_mt19937_eval(const float *C, long long row_stride, long long col_stride, const uint32_t *guide, int nb,
+                        int d, int y0, int nsteps, uint32_t seed, unsigned long long path0, long long npaths,
+                        short *ypaths, const double *cashflow, const unsigned char *knockout, double *path_values,
+                        double *scratch, double *sums);
 /* new, no counterpart in the reference: opb_mc_mt19937 without the scratch argument, for
  * callers that must not let the library allocate device memory (a host framework that owns
  * the device-memory budget, or a loop that cannot afford cudaMalloc's implicit device
@@ -355,8 +396,10 @@ int opb_mc_mt19937(const float *C, long long row_stride, long long col_stride, c
  * library (held by every GPU that loads it until exit); results are bit-identical to
  * opb_mc_mt19937.  Grids above 4096 blocks (devices with more than 512 SMs) return
  * OPB_E_UNSUPPORTED, and so do runs longer than 623 steps (they would need the driver's
- * local-memory reservation to grow).  The first call on a device looks up the array's device address (make
- * it before any stream capture); calls that overlap on the GPU share the array and race. */
+ * local-memory reservation to grow).  The first call on a device, whatever its arguments, looks up
+ * the array's device address (make it before any stream capture); the address is kept for the
+ * process, so the entry point must not be used on a device after cudaDeviceReset.  Calls that
+ * overlap on the GPU share the array and race. */
 int opb_mc_mt19937_noalloc(const float *C, long long row_stride, long long col_stride, const uint32_t *guide, int nb,
                            int d, int y0, int nsteps, uint32_t seed, unsigned long long path0, long long npaths,
                            short *ypaths, const double *x, double strike, double barrier, double disc, double *sums);

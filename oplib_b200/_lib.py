@@ -108,6 +108,10 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_lattice_kernel": (i32, [C.POINTER(LatticeDesc), i32, vp, ull, vp]),
     "opb_lattice_bermudan": (i32, [C.POINTER(LatticeDesc), i32, i32, i32, f64, vp, ull, vp]),
     "opb_set_ksplit": (i32, [i32]),
+    "opb_set_lolo_levels": (i32, [i32]),
+    "opb_chain_workspace_size": (ull, [i32]),
+    "opb_chain_kernels": (i32, [i32, i32, vp, vp, vp, ull]),
+    "opb_set_band_skip": (i32, [i32]),
     # batched lattices
     "opb_batch_workspace_size": (ull, [vp, i32]),
     "opb_batch_plan_create": (i32, [vp, i32, vp, ull, vp]),
@@ -125,6 +129,7 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_mlp_forward": (i32, [vp, vp, i32, vp, vp]),
     "opb_mlp_loss_grad": (i32, [vp, vp, vp, i32, vp, vp, vp]),
     "opb_mlp_adam": (i32, [vp, vp, vp, vp, i32, f32, f32, f32, f32, vp]),
+    "opb_mlp_adam_sched": (i32, [vp, vp, vp, vp, vp, vp, f32, f32, f32, vp]),
     "opb_implied_vol": (i32, [i64, vp, vp, vp, vp, vp, vp]),
     "opb_mlp_packed_bytes": (i64, []),
     "opb_mlp_pack": (i32, [vp, vp]),
@@ -139,9 +144,11 @@ PROTOTYPES: dict[str, tuple] = {
     "opcuda_mc_status_sz": (i32, []),
     "opcuda_mc_setseed": (i32, [u64, u64]),
     "opcuda_mc1f": (i32, [u64, i32, u64, i32, i32, i32, u64, u64, u64]),
+    "opcuda_mc1f_eval": (i32, [u64, i32, u64, i32, i32, i32, u64, u64, u64, u64, u64]),
     "opcuda_mt_benchmark": (i32, [u64, u64, i32]),
     "opb_mc_scratch_blocks": (i32, [i64]),
     "opb_mc_mt19937": (i32, [vp, i64, i64, vp, i32, i32, i32, i32, u32, ull, i64, vp, vp, f64, f64, f64, vp, vp]),
+    "opb_mc_mt19937_eval": (i32, [vp, i64, i64, vp, i32, i32, i32, i32, u32, ull, i64, vp, vp, vp, vp, vp, vp]),
     "opb_mc_mt19937_noalloc": (i32, [vp, i64, i64, vp, i32, i32, i32, i32, u32, ull, i64, vp, vp, f64, f64, f64,
                                      vp]),
     "opb_mt19937_raw": (i32, [u32, i64, i32, vp]),

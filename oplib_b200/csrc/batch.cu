@@ -148,7 +148,25 @@ int check_batch(const opb_batch_desc *b, int mode) {
 }
 
 // Layout of all device buffers and tables; with base == nullptr it only measures.
-size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, std::vector<uint32_t> *work_out) {
+// K-blocks of 64 that a squaring tile (rows [m0, m0 + tm), columns [n0, n0 + tn)) issues at
+// `level` when the generator's half-bandwidth is h0 (0: unknown, dense): the host mirror of
+// the kernel's band_kblocks with its 128-wide accumulation chunks, used to order the work.
+int host_band_kblocks(int h0, int level, int m0, int tm, int n0, int tn, int K) {
+    const int all = K / 64;
+    if (h0 <= 0) return all;
+    const long long h = level >= 40 ? (1LL << 40) : (long long)h0 << level;
+    if (h >= K) return all;
+    const long long lo = (long long)std::max(m0, n0) - h, hi = (long long)std::min(m0 + tm, n0 + tn) - 1 + h;
+    if (lo > hi || hi < 0 || lo >= K) return 0;
+    const int c_lo = (int)(std::max(lo, 0LL) / 128), c_hi = (int)(std::min(hi, (long long)K - 1) / 128) + 1;
+    return std::min(2 * c_hi, all) - 2 * c_lo;
+}
+
+// bands: the generators' half-bandwidths (nullptr when only measuring): the squaring levels'
+// work lists of the longest-first configurations are then ordered by the K-blocks each item
+// issues at that level, longest first.
+size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, std::vector<uint32_t> *work_out,
+              const std::vector<int> *bands = nullptr) {
     Carve c{base, 0};
     const int n = b->nlat;
     std::vector<long long> off(n + 1, 0);
@@ -206,7 +224,7 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     // size that is not a multiple of bn gets a last column tile that overhangs the matrix:
     // its B columns beyond d load as zeros and its output groups beyond d are not stored.
     auto gemm_list = [&](const std::vector<int> &order, int bn, int level, bool chain_or_all, int sel = 0,
-                         int tile_m = 128) {
+                         int tile_m = 128, bool by_work = false) {
         ListRef r{W.size(), 0};
         for (int i : order) {
             if (!chain_or_all && b->niter[i] <= level) continue;
@@ -216,24 +234,33 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
                 for (int bb = 0; bb < nt; bb++) W.push_back(((uint32_t)i << 16) | ((uint32_t)a << 8) | (uint32_t)bb);
         }
         r.n = (int)(W.size() - r.off);
+        if (by_work && bands && !chain_or_all) {
+            auto kb = [&](uint32_t w) {
+                const int i = (int)(w >> 16);
+                return host_band_kblocks((*bands)[i], level, (int)((w >> 8) & 255u) * tile_m, tile_m,
+                                         (int)(w & 255u) * bn, bn, b->d[i]);
+            };
+            std::stable_sort(W.begin() + r.off, W.end(), [&](uint32_t x, uint32_t y) { return kb(x) > kb(y); });
+        }
         return r;
     };
     std::vector<ListRef> gl[NCFG], glr[NCFG];
     ListRef gch[NCFG], gchr[NCFG];
     for (int cfg = 0; cfg < NCFG; cfg++) {
-        const auto &order = (cfg < 2 || cfg == 4 || cfg == 6) ? lpt : nat;
+        const bool longest = cfg < 2 || cfg == 4 || cfg == 6;
+        const auto &order = longest ? lpt : nat;
         if (CFG_PAIR[cfg]) {
             // 256 x 256 pair items for the multiples of 256, then 128 x 256 items (column
             // overhang) for the other sizes
             for (int lv = 0; lv < maxn; lv++) {
-                gl[cfg].push_back(gemm_list(order, 256, lv, false, 1, 256));
-                glr[cfg].push_back(gemm_list(order, 256, lv, false, 2, 128));
+                gl[cfg].push_back(gemm_list(order, 256, lv, false, 1, 256, longest));
+                glr[cfg].push_back(gemm_list(order, 256, lv, false, 2, 128, longest));
             }
             gch[cfg] = gemm_list(order, 256, 0, true, 1, 256);
             gchr[cfg] = gemm_list(order, 256, 0, true, 2, 128);
         } else {
             for (int lv = 0; lv < maxn; lv++) {
-                gl[cfg].push_back(gemm_list(order, CFG_BN[cfg], lv, false));
+                gl[cfg].push_back(gemm_list(order, CFG_BN[cfg], lv, false, 0, 128, longest));
                 glr[cfg].push_back(ListRef{W.size(), 0});
             }
             gch[cfg] = gemm_list(order, CFG_BN[cfg], 0, true);
@@ -310,9 +337,35 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     base += (256 - (reinterpret_cast<uintptr_t>(base) & 255)) & 255;
     opb_batch_plan *P = new opb_batch_plan();
     P->mode = mode;
-    std::vector<uint32_t> W;
-    layout(b, mode, P, base, &W);
     const int n = b->nlat;
+    // the generators' half-bandwidths, from their column pattern (read once: the plan stays
+    // valid while the generators' values change, not their columns)
+    std::vector<int> bands(n, 0);
+    if (tc_mode_b(mode)) {
+        long long rows = 0;
+        for (int i = 0; i < n; i++) rows += b->d[i];
+        std::vector<int> cols((size_t)rows * b->ell_width);
+        cudaError_t e = cudaMemcpyAsync(cols.data(), b->gen_cols, sizeof(int) * cols.size(), cudaMemcpyDeviceToHost,
+                                        opb::stream());
+        if (e == cudaSuccess) e = cudaStreamSynchronize(opb::stream());
+        if (e != cudaSuccess) {
+            delete P;
+            return opb::set_cuda(e);
+        }
+        long long ro = 0;
+        for (int i = 0; i < n; i++) {
+            int h = 0;
+            for (int y = 0; y < b->d[i]; y++)
+                for (int k = 0; k < b->ell_width; k++) {
+                    const int z = cols[(size_t)(ro + y) * b->ell_width + k];
+                    if (z >= 0 && z < b->d[i]) h = std::max(h, std::abs(z - y));
+                }
+            bands[i] = h;
+            ro += b->d[i];
+        }
+    }
+    std::vector<uint32_t> W;
+    layout(b, mode, P, base, &W, &bands);
     if (!tc_mode_b(mode)) {
         P->nlat = n; P->nmat = b->nmat; P->nK = b->nK;
         long long roff = 0;
@@ -370,7 +423,7 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
         double *pi = part + po;
         // squaring reads E as the previous level's GEMM left it, renormalised on the fly by
         // the row fixes of the previous level's (or the initial split's) renormalisation
-        sq[i] = opb::TcProblem{d, d, d, 0, L.E, L.E, pi, d, un2, 2.f, fix + ro};
+        sq[i] = opb::TcProblem{d, d, d, bands[i], L.E, L.E, pi, d, un2, 2.f, fix + ro};
         ch[i] = opb::TcProblem{d, d, d, 0, L.Pa, nullptr, pi, d, un2, 0.f, nullptr};
         pr[i] = opb::TcProblem{d, P->ldk, d, 0, L.V, nullptr, nullptr, P->ldk, un1, 0.f, nullptr};
         rs[i] = opb::RenormProblem{d, 0, L.E, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo, fix + ro};
@@ -450,17 +503,30 @@ namespace {
 // for the pair configurations (256 x 256 pair items, then 128 x 256 ones).  maps: the
 // squaring or the chain table (MN-major B).
 int cfg_gemm(opb_batch_plan *P, int cfg, const CUtensorMap *maps, const opb::TcProblem *probs, const ListRef &l,
-             const ListRef &rest, cudaStream_t s) {
+             const ListRef &rest, cudaStream_t s, int level = 0, int lolo = 0, int skip = 0) {
     const int bn = CFG_BN[cfg];
-    int r = CFG_PAIR[cfg] ? opb::launch_tc_gemm_batched_pair(maps, probs, P->work + l.off, l.n, s, P->f16, 1)
-                          : opb::launch_tc_gemm_batched(bn, maps, probs, P->work + l.off, l.n, P->grid, s, P->f16, 1);
+    int r = CFG_PAIR[cfg] ? opb::launch_tc_gemm_batched_pair(maps, probs, P->work + l.off, l.n, s, P->f16, 1, level,
+                                                             lolo, skip)
+                          : opb::launch_tc_gemm_batched(bn, maps, probs, P->work + l.off, l.n, P->grid, s, P->f16, 1,
+                                                        level, lolo, skip);
     if (r == 0 && rest.n > 0)
-        r = opb::launch_tc_gemm_batched(256, maps, probs, P->work + rest.off, rest.n, P->grid, s, P->f16, 1);
+        r = opb::launch_tc_gemm_batched(256, maps, probs, P->work + rest.off, rest.n, P->grid, s, P->f16, 1, level,
+                                        lolo, skip);
     return r;
 }
 
+// Squaring level `level` of every lattice still squaring; each lattice's operands are
+// banded by its generator (TcProblem::band), and BF16 parts add the lo.lo product on the
+// first OPB_LOLO_LEVELS levels, as in the single-lattice solve.
 int level_gemm(opb_batch_plan *P, int cfg, int level, cudaStream_t s) {
-    return cfg_gemm(P, cfg, P->maps_sq, P->sq, P->gemm_level[cfg][level], P->gemm_level_rest[cfg][level], s);
+    const int lolo = (!P->f16 && level < opb::g_lolo_levels) ? 1 : 0;
+    return cfg_gemm(P, cfg, P->maps_sq, P->sq, P->gemm_level[cfg][level], P->gemm_level_rest[cfg][level], s, level,
+                    lolo, opb::g_band_skip);
+}
+
+// The chain product of every lattice (dense, all lattices active): what the autotuner times.
+int chain_gemm(opb_batch_plan *P, int cfg, cudaStream_t s) {
+    return cfg_gemm(P, cfg, P->maps_ch, P->chain, P->gemm_chain[cfg], P->gemm_chain_rest[cfg], s);
 }
 
 // E0 build and every squaring level (one GEMM + one renormalisation launch each): P1 of
@@ -506,7 +572,7 @@ OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
     BT(opb::launch_payoff_batched(P->lats, P->nlat, P->total_rows, P->nK, P->ldk, P->x, P->strikes, s, P->f16));
     for (int m = 1; m <= P->nmat; m++) {
         if (m > 1) {
-            BT(cfg_gemm(P, cfg, P->maps_ch, P->chain, P->gemm_chain[cfg], P->gemm_chain_rest[cfg], s));
+            BT(chain_gemm(P, cfg, s));
             BT(opb::launch_renorm_batched(P->rn_chain, P->work + P->rn_chain_list.off, P->rn_chain_list.n, pdiv, s,
                                           ss));
         }
@@ -554,9 +620,9 @@ OPB_API int opb_batch_execute_bermudan(opb_batch_plan *P, int put, int exercise,
     return set_status(OPB_OK);
 }
 
-// Times the level-0 squaring launch (all lattices active) for every configuration with
-// CUDA events and keeps the fastest; ms[cfg] (optional, opb_batch_num_configs() entries)
-// receives the times.
+// Times the chain product (dense, all lattices active: the shape of every squaring level
+// once the operands have filled in) for every configuration with CUDA events and keeps the
+// fastest; ms[cfg] (optional, opb_batch_num_configs() entries) receives the times.
 // Blocking; leaves the plan's buffers in an arbitrary state (run execute afterwards).
 OPB_API int opb_batch_autotune(opb_batch_plan *P, int reps, float *ms_out, int *best_cfg) {
     OPB_REQUIRE(P, OPB_E_NULL);
@@ -572,11 +638,11 @@ OPB_API int opb_batch_autotune(opb_batch_plan *P, int reps, float *ms_out, int *
     float best = 1e30f;
     int bc = 0;
     for (int cfg = 0; cfg < NCFG; cfg++) {
-        int r = level_gemm(P, cfg, 0, s);  // warm-up (also sets the smem attribute)
+        int r = chain_gemm(P, cfg, s);  // warm-up (also sets the smem attribute)
         if (r) return set_status(r);
         OPB_TRY(cudaEventRecord(e0, s));
         for (int i = 0; i < reps; i++) {
-            r = level_gemm(P, cfg, 0, s);
+            r = chain_gemm(P, cfg, s);
             if (r) return set_status(r);
         }
         OPB_TRY(cudaEventRecord(e1, s));

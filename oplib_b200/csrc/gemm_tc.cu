@@ -225,20 +225,36 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// GELU(z) = 0.5 z (1 + erf(z / sqrt 2)), with erf from Abramowitz & Stegun, Handbook of
-// Mathematical Functions, formula 7.1.26 (|error| <= 1.5e-7): for x >= 0,
-// erf(x) = 1 - q(t) exp(-x^2), t = 1 / (1 + p x), q(t) = a1 t + ... + a5 t^5.  For z < 0,
-// 1 + erf(z / sqrt 2) = q exp(-x^2) is used directly (no cancellation).  The error is far
-// below the BF16 rounding of the stored activations.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// GELU(z) = z Phi(z), Phi(z) = 0.5 (1 + erf(z / sqrt 2)), with erf from Abramowitz & Stegun,
+// Handbook of Mathematical Functions, formula 7.1.26 (|error| <= 1.5e-7): for x >= 0,
+// erf(x) = 1 - q(t) exp(-x^2), t = 1 / (1 + p x), q(t) = a1 t + ... + a5 t^5.  With
+// h = q(t) exp(-x^2) / 2 at x = |z| / sqrt 2, Phi(z) = 1 - h for z >= 0 and h for z < 0 (no
+// cancellation in the negative tail).  Folded for the epilogue's instruction count: 1/sqrt 2
+// into p, the halving into the a_i, exp(-x^2) = 2^(z^2 (-log2(e) / 2)); one reciprocal and
+// one exponential on the XU pipe, nine FMA-pipe instructions.  The error is far below the
+// BF16 rounding of the stored activations.
 __device__ __forceinline__ float gelu_as(float z) {
-    const float x = fabsf(z) * 0.70710678118654752f;
-    const float t = __fdividef(1.0f, fmaf(0.3275911f, x, 1.0f));
-    float q = fmaf(t, 1.061405429f, -1.453152027f);
-    q = fmaf(t, q, 1.421413741f);
-    q = fmaf(t, q, -0.284496736f);
-    q = fmaf(t, q, 0.254829592f);
-    const float e = q * t * __expf(-x * x);  // 1 - erf(|z| / sqrt 2)
-    return z >= 0.f ? fmaf(-0.5f * z, e, z) : 0.5f * z * e;
+    constexpr float P = 0.3275911f * 0.70710678118654752f;
+    constexpr float A1 = 0.5f * 0.254829592f, A2 = 0.5f * -0.284496736f, A3 = 0.5f * 1.421413741f,
+                    A4 = 0.5f * -1.453152027f, A5 = 0.5f * 1.061405429f;
+    const float t = rcp_approx(fmaf(P, fabsf(z), 1.0f));
+    float q = fmaf(t, A5, A4);
+    q = fmaf(t, q, A3);
+    q = fmaf(t, q, A2);
+    q = fmaf(t, q, A1);
+    const float h = q * t * ex2_approx(z * z * -0.72134752044448170f);  // -log2(e) / 2
+    return z * (z >= 0.f ? 1.f - h : h);
 }
 
 template <int BN, int STAGES, int NPROD = 3, int BK = TC_BK, bool PAIR = false, int EPIMODE = 0>
@@ -284,7 +300,47 @@ struct TcParams {
     const double2 *cin_fix;  // as TcGemmArgs::cin_fix
     int ksplit;              // as TcGemmArgs::ksplit (single products; 0 or 1: none)
     long long c_slice;       // elements between the K-slices' partial outputs
+    const int *band;         // as TcGemmArgs::band (single products; batched: TcProblem::band)
+    int level;               // as TcGemmArgs::level
+    int lolo;                // as TcGemmArgs::lolo
+    int band_skip;           // as TcGemmArgs::band_skip
 };
+
+// K-blocks [kb_lo, kb_lo + nkb) that can contribute to the output tile rows [m0, m0 + tm),
+// columns [n0, n0 + tn) of A.B when A and B are both zero outside the band |row - col| <= h:
+// k must lie within h of some row and of some column.  The range is widened to whole
+// accumulation chunks (chunk K-blocks each, counted from K = 0), so every chunk that is
+// issued holds the same K-blocks as in the full product and the sums are bit-identical;
+// the chunks left out hold only exact-zero products.  h < 0: the whole K range.
+__device__ __forceinline__ void band_kblocks(long long h, int m0, int tm, int n0, int tn, int K, int bk, int chunk,
+                                             int &kb_lo, int &nkb) {
+    const int nkb_all = K / bk;
+    if (h < 0 || h >= K) {
+        kb_lo = 0;
+        nkb = nkb_all;
+        return;
+    }
+    const long long lo = (long long)max(m0, n0) - h;
+    const long long hi = (long long)min(m0 + tm - 1, n0 + tn - 1) + h;
+    if (lo > hi || hi < 0 || lo >= K) {
+        kb_lo = 0;
+        nkb = 0;
+        return;
+    }
+    const int span = bk * chunk;
+    const int c_lo = (int)(max(lo, 0LL) / span);
+    const int c_hi = (int)(min(hi, (long long)K - 1) / span) + 1;
+    kb_lo = c_lo * chunk;
+    nkb = min(c_hi * chunk, nkb_all) - kb_lo;
+}
+
+// Half-bandwidth of the operands at squaring level `level` when the generator's is h0
+// (E_0 = dt L has L's band; each squaring at most doubles it); -1: no band (dense).
+__device__ __forceinline__ long long level_band(int h0, int level) {
+    if (h0 < 0) return -1;
+    if (level >= 40) return 1LL << 40;
+    return (long long)h0 << level;
+}
 
 // Batched launches read per-problem tensor maps (4 per problem: Ahi, Alo, Bhi, Blo) and
 // parameters from device tables and walk a work list of packed items
@@ -345,8 +401,9 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             prob = (int)(w >> 16);
             m0 = (int)((w >> 8) & 255u) * Cfg::TILE_M;  // pair mode: 256-row items
             n0 = (int)(w & 255u) * BN;
-            nkb = bt.probs[prob].K / BK;
-            kb0 = 0;
+            const TcProblem &pr = bt.probs[prob];
+            const long long h = (pr.band > 0 && p.band_skip) ? level_band(pr.band, p.level) : -1;
+            band_kblocks(h, m0, Cfg::TILE_M, n0, BN, pr.K, BK, Cfg::CHUNK, kb0, nkb);
             slice = 0;
         } else {
             slice = t % nsplit;
@@ -362,7 +419,26 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             n0 = (r / gm) * BN;
             nkb = p.K / BK / nsplit;
             kb0 = slice * nkb;
+            if (p.band && p.band_skip && nsplit == 1) {
+                const int h0 = *p.band;
+                band_kblocks(h0 > 0 ? level_band(h0, p.level) : -1, m0, Cfg::TILE_M, n0, BN, p.K, BK, Cfg::CHUNK,
+                             kb0, nkb);
+            }
         }
+    };
+    // the fourth split product lo.lo, on the launches that ask for it (p.lolo), and there
+    // only while the operands are still banded (twice the band below the size), when the
+    // band is known; the batched launches decide per problem
+    auto item_lolo = [&](int prob) -> bool {
+        if (NPROD != 3 || !p.lolo) return false;
+        int h0 = -1, K = p.K;
+        if constexpr (BATCHED) {
+            h0 = bt.probs[prob].band;
+            K = bt.probs[prob].K;
+        } else if (p.band) {
+            h0 = *p.band;
+        }
+        return h0 <= 0 || 2 * level_band(h0, p.level) < K;
     };
 
     if (threadIdx.x == 0) {
@@ -485,6 +561,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             for (int t = item0; t < nitems && ok; t += istep) {
                 int prob, m0, n0, nkb, kb0, slice;
                 get_item(t, prob, m0, n0, nkb, kb0, slice);
+                const bool lolo = item_lolo(prob);
                 const int nch = (nkb + Cfg::CHUNK - 1) / Cfg::CHUNK;
                 for (int c = 0; c < nch && ok; c++, g++) {
                     const int a = (int)(g & 1);
@@ -519,11 +596,13 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                                 umma_bf16_pair(dacc, dAh + adv, dBh + advb, idesc, acc0);
                                 umma_bf16_pair(dacc, dAh + adv, dBl + advb, idesc, 1u);
                                 umma_bf16_pair(dacc, dAl + adv, dBh + advb, idesc, 1u);
+                                if (lolo) umma_bf16_pair(dacc, dAl + adv, dBl + advb, idesc, 1u);
                             } else {
                                 umma_bf16(dacc, dAh + adv, dBh + advb, idesc, acc0);
                                 if constexpr (NPROD == 3) {
                                     umma_bf16(dacc, dAh + adv, dBl + advb, idesc, 1u);
                                     umma_bf16(dacc, dAl + adv, dBh + advb, idesc, 1u);
+                                    if (lolo) umma_bf16(dacc, dAl + adv, dBl + advb, idesc, 1u);
                                 }
                             }
                         }
@@ -629,6 +708,15 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             }
             const int row = m0 + (int)rank * TC_BM + q * 32 + lane;
             const int col0 = n0 + h * CPT;
+            if constexpr (EPIMODE == 0) {
+                if (nch == 0 && Cin == C) {
+                    // a tile that no K-block reaches (outside twice the operands' band): the
+                    // product is zero there, and C, updated in place, is zero there too and
+                    // keeps its values; only the row-sum partial is written
+                    if (rowsum) rowsum[(long long)(col0 / CPT) * M + row] = 0.0;
+                    continue;
+                }
+            }
             if constexpr (EPIMODE == 1) {
                 // network layer: BF16 GELU(alpha * acc + bias), 8 values per 16-byte store
                 __nv_bfloat16 *hrow = p.H + (long long)row * p.ldh + col0;
@@ -832,19 +920,23 @@ int tc_gemm_tile_n(int N) {
 
 // Tile width for a product of M rows: the widest that still gives every SM a tile,
 // else the narrowest that divides N (small-N products such as the pricing GEMM).
-static int tile_for(int M, int N) {
+// A product that runs as K-slices keeps the widest tile, so that A, the large operand of a
+// small-N product, is read from memory once; without K-slices narrower tiles give every SM
+// a tile.
+static int tile_for(int M, int N, int ksplit = 1) {
     int bn = tc_gemm_tile_n(N);
-    if (g_tile_override || !bn) return bn;
+    if (g_tile_override || !bn || ksplit > 1) return bn;
     const int mt = M / TC_BM;
     while (bn > 64 && (long long)mt * (N / bn) < num_sms() && N % (bn / 2) == 0) bn /= 2;
     return bn;
 }
 
+// K-slices (at most 4) that bring a small-N product's widest tiles up to about one per SM.
 int tc_gemm_split_for(int M, int N, int K) {
-    const int bn = tile_for(M, N);
+    const int bn = tc_gemm_tile_n(N);
     if (!bn || M % TC_BM) return 1;
     const long long tiles = (long long)(M / TC_BM) * (N / bn);
-    int sp = (int)(2LL * num_sms() / (tiles > 0 ? tiles : 1));
+    int sp = (int)(num_sms() / (tiles > 0 ? tiles : 1));
     sp = sp < 1 ? 1 : (sp > 4 ? 4 : sp);
     while (sp > 1 && (K / TC_BK) % sp) sp--;
     return sp;
@@ -871,6 +963,9 @@ int tc_gemm_check(const TcGemmArgs &a) {
         if (a.Cin || a.rowsum || a.ksplit > 64 || (a.K / TC_BK) % a.ksplit) return OPB_E_ARG;
         if (a.c_slice < (long long)a.M * a.ldc || a.c_slice % 4) return OPB_E_ARG;
     }
+    // band-limited squaring: in place, square, one pass over K
+    if (a.band && (a.Cin != a.C || a.M != a.N || a.N != a.K || a.ksplit > 1 || a.level < 0 || a.level > 62))
+        return OPB_E_ARG;
     return OPB_OK;
 }
 
@@ -906,6 +1001,10 @@ static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
     p.cin_fix = a.cin_fix;
     p.ksplit = a.ksplit > 1 ? a.ksplit : 1;
     p.c_slice = a.c_slice;
+    p.band = a.band;
+    p.level = a.level;
+    p.lolo = a.lolo;
+    p.band_skip = a.band_skip;
     const int ntiles = (a.M / TC_BM) * (a.N / BN) * p.ksplit;
     const int grid = ntiles < num_sms() ? ntiles : num_sms();
     TcBatch none{nullptr, nullptr, nullptr, 0};
@@ -932,6 +1031,10 @@ static int launch_tc_pair(const TcGemmArgs &a, cudaStream_t s) {
     TcParams p{a.M, a.N, a.K, a.C, a.ldc, a.Cin, a.alpha, a.beta, a.rowsum};
     p.group_m = g_group_m;
     p.cin_fix = a.cin_fix;
+    p.band = a.band;
+    p.level = a.level;
+    p.lolo = a.lolo;
+    p.band_skip = a.band_skip;
     TcBatch none{nullptr, nullptr, nullptr, 0};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -980,13 +1083,16 @@ int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat1
 
 template <int BN, int STAGES, bool F16, bool BMN>
 static int launch_batched_impl(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                               int grid, cudaStream_t s) {
+                               int grid, cudaStream_t s, int level, int lolo, int band_skip) {
     using Cfg = TcCfg<BN, STAGES>;
     int e0 = set_smem_attr<BN, STAGES, true, F16, 3, 0, TC_BK, false, BMN>();
     if (e0) return e0;
     CUtensorMap dummy;
     std::memset(&dummy, 0, sizeof(dummy));
     TcParams p{};
+    p.level = level;
+    p.lolo = lolo;
+    p.band_skip = band_skip;
     TcBatch bt{maps, probs, work, nwork};
     k_tc_gemm<BN, STAGES, true, F16, 3, 0, TC_BK, false, BMN><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(
         dummy, dummy, dummy, dummy, p, bt);
@@ -998,7 +1104,7 @@ static int launch_batched_impl(const CUtensorMap *maps, const TcProblem *probs, 
 // loads its own half), problems with M % 256 == 0 and N % 256 == 0.
 template <bool F16, bool BMN>
 static int launch_batched_pair_impl(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                                    cudaStream_t s) {
+                                    cudaStream_t s, int level, int lolo, int band_skip) {
     constexpr int BN = 256, STAGES = 3;
     using Cfg = TcCfg<BN, STAGES, 3, TC_BK, true>;
     auto kern = k_tc_gemm<BN, STAGES, true, F16, 3, 0, TC_BK, true, BMN>;
@@ -1032,6 +1138,9 @@ static int launch_batched_pair_impl(const CUtensorMap *maps, const TcProblem *pr
     CUtensorMap dummy;
     std::memset(&dummy, 0, sizeof(dummy));
     TcParams p{};
+    p.level = level;
+    p.lolo = lolo;
+    p.band_skip = band_skip;
     TcBatch bt{maps, probs, work, nwork};
     cudaError_t e = cudaLaunchKernelEx(&cfg, kern, dummy, dummy, dummy, dummy, p, bt);
     return e == cudaSuccess ? (int)cudaGetLastError() : (int)e;
@@ -1040,27 +1149,35 @@ static int launch_batched_pair_impl(const CUtensorMap *maps, const TcProblem *pr
 // Batched squaring and chain products take MN-major B maps (b_kn = 1): pair and 256/128
 // tiles exist only in that form; 64-wide tiles in both (pricing is K-major).
 int launch_tc_gemm_batched_pair(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                                cudaStream_t s, int f16, int b_kn) {
+                                cudaStream_t s, int f16, int b_kn, int level, int lolo, int band_skip) {
     if (nwork <= 0) return OPB_OK;
     if (!b_kn) return OPB_E_UNSUPPORTED;
-    return f16 ? launch_batched_pair_impl<true, true>(maps, probs, work, nwork, s)
-               : launch_batched_pair_impl<false, true>(maps, probs, work, nwork, s);
+    return f16 ? launch_batched_pair_impl<true, true>(maps, probs, work, nwork, s, level, lolo, band_skip)
+               : launch_batched_pair_impl<false, true>(maps, probs, work, nwork, s, level, lolo, band_skip);
 }
 
 int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                           int grid, cudaStream_t s, int f16, int b_kn) {
+                           int grid, cudaStream_t s, int f16, int b_kn, int level, int lolo, int band_skip) {
     if (nwork <= 0) return OPB_OK;
     if (grid <= 0 || grid > nwork) grid = nwork < num_sms() ? nwork : num_sms();
     if (!b_kn && bn != 64) return OPB_E_UNSUPPORTED;
     switch (bn * 4 + (f16 ? 2 : 0) + (b_kn ? 1 : 0)) {
-        case 1025: return launch_batched_impl<256, 2, false, true>(maps, probs, work, nwork, grid, s);
-        case 1027: return launch_batched_impl<256, 2, true, true>(maps, probs, work, nwork, grid, s);
-        case 513: return launch_batched_impl<128, 3, false, true>(maps, probs, work, nwork, grid, s);
-        case 515: return launch_batched_impl<128, 3, true, true>(maps, probs, work, nwork, grid, s);
-        case 256: return launch_batched_impl<64, 4, false, false>(maps, probs, work, nwork, grid, s);
-        case 257: return launch_batched_impl<64, 4, false, true>(maps, probs, work, nwork, grid, s);
-        case 258: return launch_batched_impl<64, 4, true, false>(maps, probs, work, nwork, grid, s);
-        case 259: return launch_batched_impl<64, 4, true, true>(maps, probs, work, nwork, grid, s);
+        case 1025:
+            return launch_batched_impl<256, 2, false, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
+        case 1027:
+            return launch_batched_impl<256, 2, true, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
+        case 513:
+            return launch_batched_impl<128, 3, false, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
+        case 515:
+            return launch_batched_impl<128, 3, true, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
+        case 256:
+            return launch_batched_impl<64, 4, false, false>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
+        case 257:
+            return launch_batched_impl<64, 4, false, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
+        case 258:
+            return launch_batched_impl<64, 4, true, false>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
+        case 259:
+            return launch_batched_impl<64, 4, true, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
         default: return OPB_E_UNSUPPORTED;
     }
 }
@@ -1100,7 +1217,7 @@ int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
     if (c != OPB_OK) return c;
     const bool pair = g_pair && a.M % (2 * TC_BM) == 0 && a.ksplit <= 1;
     if (a.b_kn) {  // MN-major B (K x N): BK = 64 only
-        switch (tile_for(a.M, a.N) * 2 + (a.f16 ? 1 : 0)) {
+        switch (tile_for(a.M, a.N, a.ksplit) * 2 + (a.f16 ? 1 : 0)) {
             case 512:
                 if (pair)
                     return g_bk256 == 32 ? launch_tc_pair<false, true, 6, 32>(a, s) : launch_tc_pair<false, true>(a, s);
@@ -1116,7 +1233,7 @@ int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
             default: return OPB_E_UNSUPPORTED;
         }
     }
-    switch (tile_for(a.M, a.N) * 2 + (a.f16 ? 1 : 0)) {
+    switch (tile_for(a.M, a.N, a.ksplit) * 2 + (a.f16 ? 1 : 0)) {
         case 512:
             if (pair) return launch_tc_pair<false, false>(a, s);
             return g_bk256 == 32 ? launch_tc_impl<256, 4, false, 32>(a, s) : launch_tc_impl<256, 2, false>(a, s);

@@ -71,11 +71,19 @@ struct Bufs {
     double *part;
     double2 *fix;  // per-row (s, inv) of the last E-form renormalisation (deferred into the next Cin)
     double *Vd;    // FP64 option values of the backward induction, d x nKp
+    int *band;     // the ELL generator's half-bandwidth, found on the device per solve
+    double *xpad;  // spot values of the padded lattice (split modes, d % 128 != 0)
 };
 
 inline int padded_nk(int nK, int mode) { return tc_mode(mode) ? (nK + 63) / 64 * 64 : nK; }
 
-Bufs carve(Ws &w, int d, int nK, int mode) {
+// The split modes run on multiples of 128 states: a lattice of another size is solved as one
+// padded with absorbing states (zero generator rows and columns).  No state of the lattice
+// reaches a padding state, so P(t) is block diagonal, [[P_lattice(t), 0], [0, I]], and the
+// lattice's rows of every product, renormalisation and price are the unpadded ones.
+inline int padded_d(int d, int mode) { return tc_mode(mode) ? (d + 127) / 128 * 128 : d; }
+
+Bufs carve(Ws &w, int d, int nK, int mode, bool pad = false) {
     Bufs b{};
     size_t dd = (size_t)d * d;
     nK = padded_nk(nK, mode);
@@ -96,6 +104,8 @@ Bufs carve(Ws &w, int d, int nK, int mode) {
         b.part = w.take<double>((size_t)(np > 0 ? np : 1) * d);
         b.fix = w.take<double2>((size_t)d);
         b.Vd = w.take<double>((size_t)d * nK);
+        b.band = w.take<int>(1);
+        if (pad) b.xpad = w.take<double>((size_t)d);
     } else {
         b.G = w.take<float>((size_t)d * nK);
         b.part = w.take<double>((size_t)d);
@@ -172,7 +182,7 @@ int g_ksplit = 0;
 int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s) {
     int S = g_ksplit > 0 ? g_ksplit : 1;
     int kb = a.K / 64;
-    if (S <= 1 || kb < S || kb % S || a.ksplit > 1) return opb::launch_tc_gemm(a, s);
+    if (S <= 1 || kb < S || kb % S || a.ksplit > 1 || a.band) return opb::launch_tc_gemm(a, s);
     const int kslice = a.K / S;
     for (int i = 0; i < S; i++) {
         opb::TcGemmArgs t = a;
@@ -193,14 +203,22 @@ int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s) {
 // E0 = dt*L, niter split squarings with renormalisation: P1 = P(period) as row-major splits
 // in both the A and the B buffers and as FP32 in X.  g returns the product arguments of
 // the squarings (B read K x N row-major), with B set to P1's B parts.
-int square_tc(const opb_lattice_desc &L, Bufs &b, cudaStream_t s, bool f16, opb::TcGemmArgs &g) {
+int square_tc(const opb_lattice_desc &L, Bufs &b, cudaStream_t s, bool f16, opb::TcGemmArgs &g, int d_gen) {
     const int d = L.d;
     const int np = opb::tc_gemm_nparts(d, d);
     const float ss = f16 ? F16_SCALE : 0.f;                    // split scale of E / P parts
     const float unscale = f16 ? 1.f / (F16_SCALE * F16_SCALE) : 1.f;
-    // E0 = dt*L in FP32 (FP64 arithmetic), then its splits
-    if (L.ell_width > 0) LT(opb::launch_ek_ell(d, L.ell_width, L.gen_cols, L.gen_vals, L.dt, 1, b.X, s));
-    else LT(opb::launch_ek_dense(d, L.gen_dense, L.dt, 1, b.X, s));
+    // E0 = dt*L in FP32 (FP64 arithmetic), then its splits.  An ELL generator's band h0
+    // bounds E_r's to h0 * 2^r: the squarings skip the K-blocks (and whole output tiles) that
+    // only multiply zeros, with bit-identical results.
+    // (d_gen < d: the generator's d_gen states, then absorbing padding states)
+    if (d_gen != d) LT(opb::launch_ek_padded(d_gen, d, L.ell_width, L.gen_cols, L.gen_vals, L.gen_dense, L.dt, b.X, s));
+    if (L.ell_width > 0) {
+        if (d_gen == d) LT(opb::launch_ek_ell(d, L.ell_width, L.gen_cols, L.gen_vals, L.dt, 1, b.X, s));
+        LT(opb::launch_ell_band(d_gen, L.ell_width, L.gen_cols, b.band, s));
+    } else if (d_gen == d) {
+        LT(opb::launch_ek_dense(d, L.gen_dense, L.dt, 1, b.X, s));
+    }
     LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, nullptr, nullptr, d, s, ss));
     // every squaring and chain product reads its B operand K x N row-major (MN-major):
     // a squaring's B is E's own row-major parts, a chain product's B the row-major parts of
@@ -214,6 +232,11 @@ int square_tc(const opb_lattice_desc &L, Bufs &b, cudaStream_t s, bool f16, opb:
         // is applied as the epilogue reads it.
         g.C = b.X; g.Cin = b.X; g.alpha = unscale; g.beta = 2.f; g.rowsum = b.part;
         g.cin_fix = r > 0 ? b.fix : nullptr;
+        g.band = L.ell_width > 0 ? b.band : nullptr;
+        g.band_skip = opb::g_band_skip;
+        g.level = r;
+        // BF16 parts: the lo.lo product on the first levels (see OPB_LOLO_LEVELS)
+        g.lolo = (!f16 && r < opb::g_lolo_levels) ? 1 : 0;
         LT(tc_gemm_ksplit(g, s));
         // the last level emits P1 = I + E and its splits (row-major into A: the first
         // chain's A and pricing's; row-major into B: every chain's B); the others write only
@@ -222,6 +245,10 @@ int square_tc(const opb_lattice_desc &L, Bufs &b, cudaStream_t s, bool f16, opb:
         else LT(opb::launch_renorm(d, b.X, b.part, np, 1, b.Ahi, b.Alo, nullptr, nullptr, s, ss, 0, b.fix));
     }
     g.cin_fix = nullptr;
+    g.band = nullptr;
+    g.band_skip = 0;
+    g.level = 0;
+    g.lolo = 0;
     if (L.niter == 0) {
         LT(opb::launch_add_identity(d, b.X, s));
         LT(opb::launch_split(d, d, b.X, d, b.Ahi, b.Alo, nullptr, nullptr, d, s, ss));
@@ -231,15 +258,18 @@ int square_tc(const opb_lattice_desc &L, Bufs &b, cudaStream_t s, bool f16, opb:
     return 0;
 }
 
+// d_gen: the lattice's own states (L.d when unpadded); V_all and P_out hold only those.
 int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, cudaStream_t s, float *P_out,
-             bool f16) {
+             bool f16, int d_gen) {
     const int d = L.d, nK = L.nK;
     const int np = opb::tc_gemm_nparts(d, d);
     const float ss = f16 ? F16_SCALE : 0.f;                    // split scale of E / P parts
     const float unscale = f16 ? 1.f / (F16_SCALE * F16_SCALE) : 1.f;
     opb::TcGemmArgs g{};
-    LT(square_tc(L, b, s, f16, g));
-    if (P_out) return (int)cudaMemcpyAsync(P_out, b.X, sizeof(float) * (size_t)d * d, cudaMemcpyDeviceToDevice, s);
+    LT(square_tc(L, b, s, f16, g, d_gen));
+    if (P_out)
+        return (int)cudaMemcpy2DAsync(P_out, sizeof(float) * d_gen, b.X, sizeof(float) * d, sizeof(float) * d_gen, d_gen,
+                                      cudaMemcpyDeviceToDevice, s);
     const int nKp = padded_nk(nK, OPB_BF16X3);
     const float *gs = nullptr;
     if (f16) {
@@ -264,8 +294,8 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
         }
         LT(tc_gemm_ksplit(pg, s));
         const double disc = std::exp(-L.rate * L.period * m);
-        LT(opb::launch_discount(d, nK, nKp, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d * nK : nullptr, L.y0,
-                                quotes + (size_t)(m - 1) * nK, s, gs, pg.ksplit, pg.c_slice));
+        LT(opb::launch_discount(d_gen, nK, nKp, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d_gen * nK : nullptr,
+                                L.y0, quotes + (size_t)(m - 1) * nK, s, gs, pg.ksplit, pg.c_slice));
     }
     return 0;
 }
@@ -275,10 +305,10 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
 // with exercise, floored by the exercise value there.  Each product runs on the tensor
 // cores with V's split parts as a K x N row-major B operand.
 int bermudan_tc(const opb_lattice_desc &L, Bufs &b, int put, int exercise, double barrier, double *quotes,
-                cudaStream_t s, bool f16) {
+                cudaStream_t s, bool f16, int d_gen) {
     const int d = L.d, nK = L.nK, nKp = padded_nk(nK, OPB_BF16X3);
     opb::TcGemmArgs g{};
-    LT(square_tc(L, b, s, f16, g));
+    LT(square_tc(L, b, s, f16, g, d_gen));
     const float *gs = nullptr;
     if (f16) {
         LT(opb::launch_berm_scale(d, L.x, nK, L.strikes, put, b.gscale, s));
@@ -335,14 +365,39 @@ int check_desc(const opb_lattice_desc *L, int mode) {
         return OPB_E_NULL;
     }
     if (mode < OPB_FP32_PLAIN || mode > OPB_FP16X3) return OPB_E_ARG;
-    if (tc_mode(mode)) {
-        if (L->d % 128 != 0) return OPB_E_UNSUPPORTED;
-        if (opb::tc_gemm_tile_n(L->d) == 0) return OPB_E_UNSUPPORTED;
-    }
+    if (tc_mode(mode) && opb::tc_gemm_tile_n(padded_d(L->d, mode)) == 0) return OPB_E_UNSUPPORTED;
     return OPB_OK;
 }
 
+// The lattice the split modes solve: L itself, or L padded with absorbing states (its spot
+// values extended into b.xpad).
+int prepare_padded(const opb_lattice_desc &L, int mode, Bufs &b, opb_lattice_desc &out, cudaStream_t s) {
+    out = L;
+    const int dp = padded_d(L.d, mode);
+    if (dp == L.d) return 0;
+    out.d = dp;
+    out.x = b.xpad;
+    return opb::launch_pad_x(L.d, dp, L.x, b.xpad, s);
+}
+
 }  // namespace
+
+namespace opb {
+int g_lolo_levels = OPB_LOLO_LEVELS;
+int g_band_skip = 1;
+}  // namespace opb
+
+OPB_API int opb_set_lolo_levels(int n) {
+    OPB_REQUIRE(n >= 0 && n <= 64, OPB_E_ARG);
+    opb::g_lolo_levels = n;
+    return opb::set_status(OPB_OK);
+}
+
+OPB_API int opb_set_band_skip(int on) {
+    OPB_REQUIRE(on == 0 || on == 1, OPB_E_ARG);
+    opb::g_band_skip = on;
+    return opb::set_status(OPB_OK);
+}
 
 OPB_API int opb_set_ksplit(int s) {
     OPB_REQUIRE(s >= 0 && s <= 64, OPB_E_ARG);
@@ -354,7 +409,8 @@ OPB_API int opb_set_ksplit(int s) {
 OPB_API unsigned long long opb_lattice_workspace_size(int d, int nK, int mode) {
     if (d <= 0 || nK <= 0) return 0;
     Ws w{nullptr, 0};
-    (void)carve(w, d, nK, mode);
+    const int dp = padded_d(d, mode);
+    (void)carve(w, dp, nK, mode, dp != d);
     return (unsigned long long)w.used + 256;
 }
 
@@ -373,10 +429,17 @@ OPB_API int opb_lattice_solve(const opb_lattice_desc *L, int mode, void *workspa
     Ws w{reinterpret_cast<char *>(workspace), 0};
     size_t off = (256 - (reinterpret_cast<uintptr_t>(workspace) & 255)) & 255;
     w.p += off;
-    Bufs b = carve(w, L->d, L->nK, mode);
+    const int dp = padded_d(L->d, mode);
+    Bufs b = carve(w, dp, L->nK, mode, dp != L->d);
     cudaStream_t s = opb::stream();
-    int r = tc_mode(mode) ? solve_tc(*L, b, quotes, V_all, s, nullptr, mode == OPB_FP16X3)
-                          : solve_fp32(*L, mode, b, quotes, V_all, s, nullptr);
+    int r;
+    if (tc_mode(mode)) {
+        opb_lattice_desc Lp;
+        r = prepare_padded(*L, mode, b, Lp, s);
+        if (r == 0) r = solve_tc(Lp, b, quotes, V_all, s, nullptr, mode == OPB_FP16X3, L->d);
+    } else {
+        r = solve_fp32(*L, mode, b, quotes, V_all, s, nullptr);
+    }
     return opb::set_status(r);
 }
 
@@ -401,10 +464,14 @@ OPB_API int opb_lattice_bermudan(const opb_lattice_desc *L, int mode, int put, i
     Ws w{reinterpret_cast<char *>(workspace), 0};
     size_t off = (256 - (reinterpret_cast<uintptr_t>(workspace) & 255)) & 255;
     w.p += off;
-    Bufs b = carve(w, L->d, L->nK, mode);
+    const int dp = padded_d(L->d, mode);
+    Bufs b = carve(w, dp, L->nK, mode, dp != L->d);
     cudaStream_t s = opb::stream();
-    return opb::set_status(tc_mode(mode) ? bermudan_tc(*L, b, put, exercise, barrier, quotes, s, mode == OPB_FP16X3)
-                                         : bermudan_fp32(*L, mode, b, put, exercise, barrier, quotes, s));
+    if (!tc_mode(mode)) return opb::set_status(bermudan_fp32(*L, mode, b, put, exercise, barrier, quotes, s));
+    opb_lattice_desc Lp;
+    int r = prepare_padded(*L, mode, b, Lp, s);
+    if (r == 0) r = bermudan_tc(Lp, b, put, exercise, barrier, quotes, s, mode == OPB_FP16X3, L->d);
+    return opb::set_status(r);
 }
 
 // Transition kernel only: P_out (device, d x d FP32, source-major) = P(period) after
@@ -423,11 +490,65 @@ OPB_API int opb_lattice_kernel(const opb_lattice_desc *L, int mode, void *worksp
     Ws w{reinterpret_cast<char *>(workspace), 0};
     size_t off = (256 - (reinterpret_cast<uintptr_t>(workspace) & 255)) & 255;
     w.p += off;
-    Bufs b = carve(w, L2.d, L2.nK, mode);
+    const int dp = padded_d(L2.d, mode);
+    Bufs b = carve(w, dp, L2.nK, mode, dp != L2.d);
     cudaStream_t s = opb::stream();
-    int r = tc_mode(mode) ? solve_tc(L2, b, nullptr, nullptr, s, P_out, mode == OPB_FP16X3)
-                          : solve_fp32(L2, mode, b, nullptr, nullptr, s, P_out);
+    int r;
+    if (tc_mode(mode)) {
+        opb_lattice_desc Lp;
+        r = prepare_padded(L2, mode, b, Lp, s);
+        if (r == 0) r = solve_tc(Lp, b, nullptr, nullptr, s, P_out, mode == OPB_FP16X3, L2.d);
+    } else {
+        r = solve_fp32(L2, mode, b, nullptr, nullptr, s, P_out);
+    }
     return opb::set_status(r);
+}
+
+// Step kernels of a Monte Carlo plan whose steps span several elementary intervals (a
+// generator date inside a step): the kernel of such a step is the product of its elementary
+// kernels in time order.  The reference plans the factor lists (jfactor_ms,
+// oplib/opmodel/models/CModel Common.cs:431-486) and chains them on the device with FP32
+// products (device_mc_sminit / smk / smcopy, CModel Device.cs:252-295); here each product is
+// an FP32 GEMM followed by the FP64 row renormalisation of the lattice solve.  factors: host
+// array of nf device pointers to row-major (source-major) d x d FP32 kernels; out must not
+// alias them.  workspace: opb_chain_workspace_size(d) bytes.
+OPB_API unsigned long long opb_chain_workspace_size(int d) {
+    if (d <= 0) return 0;
+    Ws w{nullptr, 0};
+    (void)w.take<float>((size_t)d * d);
+    (void)w.take<double>((size_t)d);
+    return (unsigned long long)w.used + 256;
+}
+
+OPB_API int opb_chain_kernels(int d, int nf, const float *const *factors, float *out, void *workspace,
+                              unsigned long long ws_bytes) {
+    OPB_NVTX("opb_chain_kernels");
+    OPB_REQUIRE(d > 0 && nf >= 1, OPB_E_ARG);
+    OPB_REQUIRE(factors && out, OPB_E_NULL);
+    for (int i = 0; i < nf; i++) {
+        OPB_REQUIRE(factors[i] != nullptr, OPB_E_NULL);
+        OPB_REQUIRE(factors[i] != out, OPB_E_ARG);
+    }
+    cudaStream_t s = opb::stream();
+    const size_t bytes = sizeof(float) * (size_t)d * d;
+    if (nf == 1) return opb::set_status((int)cudaMemcpyAsync(out, factors[0], bytes, cudaMemcpyDeviceToDevice, s));
+    OPB_REQUIRE(workspace, OPB_E_NULL);
+    OPB_REQUIRE(ws_bytes >= opb_chain_workspace_size(d), OPB_E_ARG);
+    Ws w{reinterpret_cast<char *>(workspace), 0};
+    w.p += (256 - (reinterpret_cast<uintptr_t>(workspace) & 255)) & 255;
+    float *tmp = w.take<float>((size_t)d * d);
+    double *part = w.take<double>((size_t)d);
+    // the products alternate between out and tmp so that the last one lands in out
+    const float *cur = factors[0];
+    for (int i = 1; i < nf; i++) {
+        float *dst = ((nf - 1 - i) % 2 == 0) ? out : tmp;
+        int r = opb::sgemm_rm(d, d, d, 1.f, cur, d, factors[i], d, 0.f, dst, d, s);
+        if (r == 0) r = opb::launch_rowsum(d, dst, part, s);
+        if (r == 0) r = opb::launch_renorm(d, dst, part, 1, 0, nullptr, nullptr, nullptr, nullptr, s);
+        if (r != 0) return opb::set_status(r);
+        cur = dst;
+    }
+    return opb::set_status(OPB_OK);
 }
 
 // The reference's plan rule for one interval (oplib/opmodel/models/CModel Common.cs:289-307):

@@ -20,8 +20,16 @@ int sgemm_rm_strided(bool ta, bool tb, int M, int N, int K, float alpha, const f
                      cudaStream_t s);
 
 // lattice_kernels.cu
+// *out = max |col - row| over the ELL entries (the generator's half-bandwidth)
+int launch_ell_band(int d, int w, const int *cols, int *out, cudaStream_t s);
 int launch_ek_ell(int d, int w, const int *cols, const double *vals, double dt, int eform, float *out,
                   cudaStream_t s);
+// E0 = dt L (E-form) of a d-state generator (ELL when w > 0, else dense) into a dpad x dpad
+// matrix whose states d..dpad-1 are absorbing (zero rows and columns)
+int launch_ek_padded(int d, int dpad, int w, const int *cols, const double *vals, const double *dense, double dt,
+                     float *out, cudaStream_t s);
+// xpad[i] = x[min(i, d - 1)], i < dpad
+int launch_pad_x(int d, int dpad, const double *x, double *xpad, cudaStream_t s);
 int launch_ek_dense(int d, const double *L, double dt, int eform, float *out, cudaStream_t s);
 int launch_split(int rows, int cols, const float *X, long long ld, __nv_bfloat16 *Ahi, __nv_bfloat16 *Alo,
                  __nv_bfloat16 *Bhi, __nv_bfloat16 *Blo, long long ldt, cudaStream_t s, float sscale = 0.f);
@@ -117,7 +125,29 @@ struct TcGemmArgs {
     // caller to sum; needs no Cin and no rowsum, (K / 64) % ksplit == 0, c_slice >= M * ldc
     int ksplit;
     long long c_slice;
+    // optional (device int h0 > 0): A and B are both zero outside the band |row - col| <=
+    // h0 << level.  With band_skip, each output tile issues only the K-blocks within reach
+    // of its rows and columns, in whole accumulation chunks (bit-identical to the full
+    // product), and a tile that no K-block reaches writes only its zero row-sum partials:
+    // such tiles must be zero in C already, with C == Cin.  Single products without K-slices.
+    const int *band;
+    int level;
+    int band_skip;
+    // 1: also issue the fourth split product lo.lo (split modes); where the band is known,
+    // only while the operands are banded (2 * (h0 << level) < K)
+    int lolo;
 };
+// Split-BF16 squarings add the fourth product lo.lo on their first OPB_LOLO_LEVELS levels,
+// as long as the operands are still banded (twice the band below the size; every level up
+// to OPB_LOLO_LEVELS when the band is not known).  hi.hi + hi.lo + lo.hi leaves out lo.lo,
+// a term of 2^-16 relative size that does not average out on the early, banded levels: on
+// the 512 lattices of the calibration sweep (n up to 2048, up to 16 squarings) leaving it
+// out everywhere costs up to 1.4e-5 in price, adding it on the first 8 levels brings every
+// price within 2e-6 of FP64.  Those levels are banded, so the extra product costs little.
+constexpr int OPB_LOLO_LEVELS = 8;
+// knobs shared by the single and batched solves (opb_set_lolo_levels, opb_set_band_skip)
+extern int g_lolo_levels;  // leading squaring levels with the lo.lo product (BF16 parts)
+extern int g_band_skip;    // 1: squarings leave out the K-blocks outside the operands' band
 // K-slices that fill the GPU with the tiles of a small-N product (1 = none), at most 4
 int tc_gemm_split_for(int M, int N, int K);
 int tc_gemm_tile_n(int N);                    // tile width chosen for N (0 if unsupported)
@@ -133,7 +163,8 @@ int tc_gemm_nparts(int M, int N);             // number of row-sum partials writ
 
 // Batched launches: problem descriptors and tensor maps live in device memory.
 struct TcProblem {
-    int M, N, K, pad;
+    // band > 0: squaring operands zero outside |row - col| <= band << level (TcGemmArgs::band)
+    int M, N, K, band;
     float *C;
     const float *Cin;
     double *rowsum;       // partials rowsum[(col/min(bn,128)) * M + row]
@@ -149,12 +180,15 @@ int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat1
                  int f16 = 0, int b_kn = 0);
 // work: packed (problem << 16 | m-tile << 8 | n-tile); bn in {64, 128, 256}; K-major B
 // (b_kn = 0) only for bn = 64
+// level, lolo: as TcGemmArgs (band per problem in TcProblem::band)
 int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                           int grid, cudaStream_t s, int f16, int b_kn);
+                           int grid, cudaStream_t s, int f16, int b_kn, int level = 0, int lolo = 0,
+                           int band_skip = 0);
 // 256 x 256 items (256-row / 256-column units) on 2-CTA clusters, each CTA loading its
 // 128 rows of A and 128 columns of B; MN-major B maps; problems with M, N multiples of 256
 int launch_tc_gemm_batched_pair(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                                cudaStream_t s, int f16, int b_kn);
+                                cudaStream_t s, int f16, int b_kn, int level = 0,
+                                int lolo = 0, int band_skip = 0);
 
 // sck.cu
 int launch_sck_rm(int d, int nrows, const float *P, float *C, cudaStream_t s);

@@ -44,16 +44,45 @@ __global__ void k_ek_scatter_ell(int d, int w, const int *__restrict__ cols, con
     out[(long long)y * ld + z] = (float)v;
 }
 
-// Dense FP64 generator, row-major (source-major).
-__global__ void k_ek_dense(int d, const double *__restrict__ L, double dt, int eform, float *__restrict__ out) {
+// Half-bandwidth of an ELL generator: max |col - row| over its entries (padding excluded),
+// by one block.  The squarings read it to leave out the K-blocks that multiply zeros.
+__global__ void __launch_bounds__(1024) k_ell_band(int d, int w, const int *__restrict__ cols, int *__restrict__ out) {
+    __shared__ int wmax[32];
+    int m = 0;
+    const long long n = (long long)d * w;
+    for (long long t = threadIdx.x; t < n; t += blockDim.x) {
+        const int z = cols[t];
+        if (z >= 0 && z < d) m = max(m, abs(z - (int)(t / w)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? wmax[threadIdx.x] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) *out = m;
+    }
+}
+
+// Dense FP64 generator, row-major (source-major), into rows of leading dimension ld.
+__global__ void k_ek_dense(int d, const double *__restrict__ L, double dt, int eform, float *__restrict__ out,
+                           long long ld) {
     long long n = (long long)d * d;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
         int y = (int)(t / d), z = (int)(t - (long long)y * d);
         double v = dt * L[t];
         if (!eform && z == y) v += 1.0;
-        out[t] = (float)v;
+        out[(long long)y * ld + z] = (float)v;
     }
+}
+
+// Spot values of a lattice padded with absorbing states: xpad[i] = x[min(i, d - 1)].
+__global__ void k_pad_x(int d, int dpad, const double *__restrict__ x, double *__restrict__ xpad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < dpad) xpad[i] = x[i < d ? i : d - 1];
 }
 
 // Two-part split of an FP32 value into 16-bit storage.  sscale == 0: BF16 parts,
@@ -620,11 +649,36 @@ int launch_ek_ell(int d, int w, const int *cols, const double *vals, double dt, 
     return (int)cudaGetLastError();
 }
 
+int launch_ell_band(int d, int w, const int *cols, int *out, cudaStream_t s) {
+    k_ell_band<<<1, 1024, 0, s>>>(d, w, cols, out);
+    return (int)cudaGetLastError();
+}
+
 int launch_ek_dense(int d, const double *L, double dt, int eform, float *out, cudaStream_t s) {
     long long n = (long long)d * d;
     int b = blocks_for(n, 256);
     int cap = 16 * num_sms();
-    k_ek_dense<<<b < cap ? b : cap, 256, 0, s>>>(d, L, dt, eform, out);
+    k_ek_dense<<<b < cap ? b : cap, 256, 0, s>>>(d, L, dt, eform, out, d);
+    return (int)cudaGetLastError();
+}
+
+int launch_ek_padded(int d, int dpad, int w, const int *cols, const double *vals, const double *dense, double dt,
+                     float *out, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float) * (size_t)dpad * dpad, s);
+    if (e != cudaSuccess) return (int)e;
+    if (w > 0) {
+        long long n = (long long)d * w;
+        if (n > 0) k_ek_scatter_ell<<<blocks_for(n, 256), 256, 0, s>>>(d, w, cols, vals, dt, 1, out, dpad);
+    } else {
+        long long n = (long long)d * d;
+        int b = blocks_for(n, 256), cap = 16 * num_sms();
+        k_ek_dense<<<b < cap ? b : cap, 256, 0, s>>>(d, dense, dt, 1, out, dpad);
+    }
+    return (int)cudaGetLastError();
+}
+
+int launch_pad_x(int d, int dpad, const double *x, double *xpad, cudaStream_t s) {
+    k_pad_x<<<blocks_for(dpad, 256), 256, 0, s>>>(d, dpad, x, xpad);
     return (int)cudaGetLastError();
 }
 
@@ -925,21 +979,24 @@ int launch_discount(int d, int nK, int ldk, const float *V32, double disc, doubl
 
 // ------------------------------------------------------------------ reference ek entry points
 
-// U = I + dt*gen for a column-major d x d FP32 generator (oplib/opcuda/sek.cu:40-59,106-115).
-// The sum is formed in FP64 and rounded once.
+// U = I + dt*gen for a column-major d x d FP32 generator (oplib/opcuda/sek.cu:40-59,106-115),
+// in the reference kernels' FP32 arithmetic so that the drop-ins reproduce them bit for bit:
+// the numerator id + dt*gen is one fused multiply-add (nvcc contracts the reference's
+// expression), the discount denominator 1 + dt*r[y1] (sek.cu:78) or 1 + (dt*r[y1])*lambda
+// (sek.cu:100) rounds the inner product and fuses the last one, and the quotient is the
+// IEEE FP32 division.  The lattice path builds its U0 in FP64 elsewhere; this is the drop-in.
 __global__ void k_sek(int d, const float *__restrict__ gen, float dt, float *__restrict__ out,
                       const float *__restrict__ r, const float *__restrict__ lambda) {
     long long n = (long long)d * d;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
         int y1 = (int)(t % d), y2 = (int)(t / d);  // column-major: t = y1 + d*y2
-        double v = (double)dt * (double)gen[t] + (y1 == y2 ? 1.0 : 0.0);
+        float v = __fmaf_rn(dt, gen[t], y1 == y2 ? 1.f : 0.f);
         if (r) {
-            double rr = (double)r[y1];
-            if (lambda) rr *= (double)lambda[0];
-            v /= 1.0 + (double)dt * rr;  // oplib/opcuda/sek.cu:78,100
+            float den = lambda ? __fmaf_rn(__fmul_rn(dt, r[y1]), lambda[0], 1.f) : __fmaf_rn(dt, r[y1], 1.f);
+            v = __fdiv_rn(v, den);
         }
-        out[t] = (float)v;
+        out[t] = v;
     }
 }
 

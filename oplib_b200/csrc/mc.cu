@@ -47,9 +47,16 @@ struct McArgs {
     const double *x;         // optional node values (payoffs)
     double strike, barrier, disc;
     double *block_sums;      // [gridDim.x * 2]
+    // device-side evaluator (EVAL): path value v = sum over steps k of cf[k*d + y_k] up to,
+    // not including, the first step whose state is knocked out (ko[k*d + y_k] != 0)
+    const double *cf;        // [nsteps][d] cashflow per step and state (discounting folded in)
+    const unsigned char *ko; // optional [nsteps][d] knock-out flags
+    double *pv;              // optional [npaths] path values
 };
 
-template <bool ANY_LENGTH>
+// EVAL: block sums are (sum v, sum v^2) of the evaluator's path values instead of the
+// fused barrier / Asian payoffs.
+template <bool ANY_LENGTH, bool EVAL = false>
 __global__ void __launch_bounds__(256) k_mc(McArgs a) {
     double s_bar = 0.0, s_asi = 0.0;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -58,6 +65,8 @@ __global__ void __launch_bounds__(256) k_mc(McArgs a) {
         const uint32_t seed = a.seed + (uint32_t)(a.path0 + (unsigned long long)p);
         int y = a.y0;
         double xmin = 1e300, xsum = 0.0, xlast = 0.0;
+        double v = 0.0;
+        bool alive = true;
         mt19937_stream<ANY_LENGTH>(seed, a.nsteps, [&](int k, uint32_t bits) {
             const float u = mt_uniform_open0(bits);
             const float *row = a.C + (long long)y * a.rs + (a.m_k ? (long long)__ldg(a.m_k + k) * a.ms : 0LL);
@@ -75,14 +84,24 @@ __global__ void __launch_bounds__(256) k_mc(McArgs a) {
             }
             y = lo;
             if (a.ypaths) a.ypaths[p + a.npaths * (long long)k] = (short)y;
-            if (a.x) {
+            if constexpr (EVAL) {
+                const long long o = (long long)k * a.d + y;
+                if (alive) {
+                    if (a.ko && __ldg(a.ko + o)) alive = false;
+                    else v += __ldg(a.cf + o);
+                }
+            } else if (a.x) {
                 double xv = __ldg(a.x + y);
                 xmin = xv < xmin ? xv : xmin;
                 xsum += xv;
                 xlast = xv;
             }
         });
-        if (a.x) {
+        if constexpr (EVAL) {
+            if (a.pv) a.pv[p] = v;
+            s_bar += v;
+            s_asi += v * v;
+        } else if (a.x) {
             double pay = xlast - a.strike;
             if (xmin > a.barrier && pay > 0.0) s_bar += a.disc * pay;
             double avg = xsum / (double)a.nsteps - a.strike;
@@ -141,10 +160,17 @@ __global__ void k_mt_raw(uint32_t seed, long long nstreams, int n, uint32_t *__r
     mt19937_stream<ANY_LENGTH>(seed + (uint32_t)s, n, [&](int j, uint32_t bits) { out[s * n + j] = bits; });
 }
 
-// The register-only generator up to 623 steps, the cursor/state-array one beyond.
+// The register-only generator up to 623 steps, the cursor/state-array one beyond; the
+// evaluator form when a cashflow table is given.
 void launch_mc(int grid, const McArgs &a) {
-    if (a.nsteps <= kMtCursorMax) k_mc<false><<<grid, 256, 0, stream()>>>(a);
-    else k_mc<true><<<grid, 256, 0, stream()>>>(a);
+    if (a.cf) {
+        if (a.nsteps <= kMtCursorMax) k_mc<false, true><<<grid, 256, 0, stream()>>>(a);
+        else k_mc<true, true><<<grid, 256, 0, stream()>>>(a);
+    } else if (a.nsteps <= kMtCursorMax) {
+        k_mc<false><<<grid, 256, 0, stream()>>>(a);
+    } else {
+        k_mc<true><<<grid, 256, 0, stream()>>>(a);
+    }
 }
 void launch_mt_bench(int grid, uint32_t seed, long long nstreams, int nper, float *unif) {
     if (nper <= kMtCursorMax) k_mt_bench<false><<<grid, 256, 0, stream()>>>(seed, nstreams, nper, unif);
@@ -193,6 +219,37 @@ OPB_API int opb_mc_mt19937(const float *C, long long row_stride, long long col_s
     int grid = mc_grid(npaths);
     launch_mc(grid, a);
     if (x) k_reduce_pairs<<<1, 256, 0, stream()>>>(grid, scratch, sums);
+    return launch_check();
+}
+
+// The same paths as opb_mc_mt19937 evaluated on the device by a cashflow table instead of
+// the fused payoffs: path value v_p = sum_k cashflow[k*d + y_k] over the steps before the
+// first knocked-out state (knockout[k*d + y_k] != 0; knockout optional).  path_values
+// (optional) receives v_p for each path, sums[0] / sums[1] the sum of v_p and of v_p^2
+// (fixed-order FP64 reductions).  This replaces the host round trip of the reference's
+// evaluator callback (oplib/opmodel/models/CModel Device.cs:352-364,
+// oplib/opmodel/interfaces/CMCEvaluator.cs:41-67) for payoffs that are sums of per-date
+// cashflows with discrete knock-out.  scratch: 2*opb_mc_scratch_blocks(npaths) doubles.
+OPB_API int opb_mc_mt19937_eval(const float *C, long long row_stride, long long col_stride, const uint32_t *guide,
+                                int nb, int d, int y0, int nsteps, uint32_t seed, unsigned long long path0,
+                                long long npaths, short *ypaths, const double *cashflow,
+                                const unsigned char *knockout, double *path_values, double *scratch, double *sums) {
+    OPB_NVTX("opb_mc_mt19937_eval");
+    OPB_REQUIRE(d > 0 && d <= 32767 && y0 >= 0 && y0 < d, OPB_E_ARG);
+    OPB_REQUIRE(nsteps >= 1 && npaths >= 0, OPB_E_ARG);
+    OPB_REQUIRE(C != nullptr && cashflow != nullptr && scratch != nullptr && sums != nullptr, OPB_E_NULL);
+    if (guide) OPB_REQUIRE(nb >= 1 && nb <= 4096 && (nb & (nb - 1)) == 0 && col_stride == 1, OPB_E_ARG);
+    if (npaths == 0) {
+        OPB_TRY(cudaMemsetAsync(sums, 0, 2 * sizeof(double), stream()));
+        return set_status(OPB_OK);
+    }
+    McArgs a{};
+    a.C = C; a.rs = row_stride; a.cs = col_stride; a.guide = guide; a.nb = nb;
+    a.d = d; a.y0 = y0; a.nsteps = nsteps; a.seed = seed; a.path0 = path0; a.npaths = npaths;
+    a.ypaths = ypaths; a.cf = cashflow; a.ko = knockout; a.pv = path_values; a.block_sums = scratch;
+    const int grid = mc_grid(npaths);
+    launch_mc(grid, a);
+    k_reduce_pairs<<<1, 256, 0, stream()>>>(grid, scratch, sums);
     return launch_check();
 }
 
@@ -272,6 +329,42 @@ OPB_API int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk
     return set_status(OPB_OK);
 }
 
+// opcuda_mc1f with the evaluator on the device: the same paths (continuing the status
+// record), each valued by the cashflow table as in opb_mc_mt19937_eval, results[p] the
+// value of path p of this call.  y_sk (optional, 0 for none) still receives the states; no
+// host copy of them is made.  Blocking, as opcuda_mc1f is.  It stands for the
+// reference's opcuda_mc1f + evaluator.eval(y_host) pair (oplib/opmodel/models/CModel
+// Device.cs:343-364): the evaluator becomes a table, the states need not leave the device.
+OPB_API int opcuda_mc1f_eval(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk, int d, uint64_t ctpker_m_yy,
+                             uint64_t m_k, uint64_t cashflow, uint64_t knockout, uint64_t results) {
+    OPB_NVTX("opcuda_mc1f_eval");
+    OPB_REQUIRE(mtptr != 0 && ctpker_m_yy != 0 && m_k != 0 && cashflow != 0 && results != 0, OPB_E_NULL);
+    OPB_REQUIRE(d > 0 && d <= 32767 && y0 >= 0 && y0 < d && nscen >= 0, OPB_E_ARG);
+    OPB_REQUIRE(nk >= 1, OPB_E_ARG);
+    uint32_t rec[4];
+    OPB_TRY(cudaMemcpyAsync(rec, reinterpret_cast<const void *>(mtptr), sizeof(rec), cudaMemcpyDeviceToHost, stream()));
+    OPB_TRY(cudaStreamSynchronize(stream()));
+    unsigned long long path0 = (unsigned long long)rec[1] | ((unsigned long long)rec[2] << 32);
+    if (nscen > 0) {
+        McArgs a{};
+        a.C = reinterpret_cast<const float *>(ctpker_m_yy);
+        a.rs = 1; a.cs = d; a.m_k = reinterpret_cast<const int *>(m_k); a.ms = (long long)d * d;
+        a.d = d; a.y0 = y0; a.nsteps = nk; a.seed = rec[0]; a.path0 = path0; a.npaths = nscen;
+        a.ypaths = reinterpret_cast<short *>(y_sk);
+        a.cf = reinterpret_cast<const double *>(cashflow);
+        a.ko = reinterpret_cast<const unsigned char *>(knockout);
+        a.pv = reinterpret_cast<double *>(results);
+        launch_mc(mc_grid(nscen), a);
+        OPB_TRY(cudaGetLastError());
+    }
+    path0 += (unsigned long long)nscen;
+    rec[1] = (uint32_t)(path0 & 0xffffffffull);
+    rec[2] = (uint32_t)(path0 >> 32);
+    OPB_TRY(cudaMemcpyAsync(reinterpret_cast<void *>(mtptr), rec, sizeof(rec), cudaMemcpyHostToDevice, stream()));
+    OPB_TRY(cudaStreamSynchronize(stream()));
+    return set_status(OPB_OK);
+}
+
 // Uniform throughput benchmark (oplib/opcuda/smc.cu:664-736): nscen uniforms from
 // opcuda_mc_nrng-independent per-stream MT19937 generators -- 4096 streams of nscen/4096
 // values each, stream s seeded with base seed + s.
@@ -318,7 +411,10 @@ OPB_API int opb_mt_uniforms(uint32_t seed, long long nstreams, int nper, float *
 //
 // Host code cannot use the array's name as a device address, so the device address is
 // looked up with cudaGetSymbolAddress once per device, with that device current, by the
-// first call made on that device; make that first call before any stream capture.
+// first call made on that device (whatever its arguments); make that first call before any
+// stream capture.  The address is kept for the life of the process: after cudaDeviceReset
+// (a new primary context) it no longer belongs to the array, so this entry point must not
+// be used on a device after that device has been reset.
 
 #define OPB_MC_NOALLOC_MAX_BLOCKS 4096
 
@@ -351,14 +447,16 @@ OPB_API int opb_mc_mt19937_noalloc(const float *C, long long row_stride, long lo
                                    const uint32_t *guide, int nb, int d, int y0, int nsteps, uint32_t seed,
                                    unsigned long long path0, long long npaths, short *ypaths, const double *x,
                                    double strike, double barrier, double disc, double *sums) {
+    OPB_NVTX("opb_mc_mt19937_noalloc");
     OPB_REQUIRE(nsteps <= kMtCursorMax, OPB_E_UNSUPPORTED);
     OPB_REQUIRE(npaths >= 0, OPB_E_ARG);
     OPB_REQUIRE(mc_grid(npaths) <= OPB_MC_NOALLOC_MAX_BLOCKS, OPB_E_UNSUPPORTED);
+    // the address is looked up on the first call on a device even when this call needs no
+    // partial sums (x == NULL), so that the lookup never falls inside a later stream capture
     double *scratch = nullptr;
-    if (x) {
-        int r = noalloc_scratch(&scratch);
-        if (r != OPB_OK) return set_status(r);
-    }
+    int r = noalloc_scratch(&scratch);
+    if (r != OPB_OK) return set_status(r);
+    if (!x) scratch = nullptr;
     return opb_mc_mt19937(C, row_stride, col_stride, guide, nb, d, y0, nsteps, seed, path0, npaths, ypaths, x,
                           strike, barrier, disc, scratch, sums);
 }

@@ -183,6 +183,31 @@ __global__ void k_adam(int n, float *__restrict__ theta, float *__restrict__ m, 
     }
 }
 
+// The same step with the step count and learning rate on the device: step s = *step + 1,
+// lr = lr_table[s - 1] (a schedule), bias corrections 1 - b^s; a following k_step_inc
+// advances *step.  A training loop of these launches can be captured in a CUDA graph once
+// and replayed every epoch.
+__global__ void k_adam_sched(int n, float *__restrict__ theta, float *__restrict__ m, float *__restrict__ v,
+                             const float *__restrict__ g, const float *__restrict__ lr_table,
+                             const int *__restrict__ step, float b1, float b2, float eps,
+                             float *__restrict__ theta_bf) {
+    const int s = *step + 1;
+    const float c1 = 1.f - powf(b1, (float)s), c2 = 1.f - powf(b2, (float)s);
+    const float lr = lr_table[s - 1];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float th = theta[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        theta[i] = th;
+        theta_bf[i] = __bfloat162float(__float2bfloat16_rn(th));
+    }
+}
+
+__global__ void k_step_inc(int *step) { *step += 1; }
+
 // ---- implied volatility of call prices (FP64 bisection on the Black-Scholes price)
 __device__ double bs_call(double s, double k, double r, double sig, double t) {
     const double sq = sig * sqrt(t);
@@ -378,6 +403,19 @@ OPB_API int opb_mlp_adam(float *theta, float *m, float *v, const float *grad, in
     OPB_REQUIRE(step >= 1 && lr > 0.f, OPB_E_ARG);
     const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
     k_adam<<<grid_ew(MLP_NPARAM), 256, 0, stream()>>>(MLP_NPARAM, theta, m, v, grad, lr, b1, b2, eps, c1, c2, theta_bf);
+    return launch_check();
+}
+
+// Adam with the step counter (device int, advanced by the call) and the learning-rate
+// schedule (device lr_table[step - 1]) in device memory, so that a training loop of
+// opb_mlp_loss_grad / opb_mlp_adam_sched calls is the same work every epoch and can be
+// captured in a CUDA graph.  Same update as opb_mlp_adam.
+OPB_API int opb_mlp_adam_sched(float *theta, float *m, float *v, const float *grad, int *step, const float *lr_table,
+                               float b1, float b2, float eps, float *theta_bf) {
+    OPB_REQUIRE(theta && m && v && grad && step && lr_table && theta_bf, OPB_E_NULL);
+    k_adam_sched<<<grid_ew(MLP_NPARAM), 256, 0, stream()>>>(MLP_NPARAM, theta, m, v, grad, lr_table, step, b1, b2,
+                                                             eps, theta_bf);
+    k_step_inc<<<1, 1, 0, stream()>>>(step);
     return launch_check();
 }
 

@@ -228,6 +228,31 @@ def mc_run(Cm: torch.Tensor, y0: int, nsteps: int, seed: int, npaths: int, path0
 
 # -------------------------------------------------------------------- batched lattices
 
+def mc_plan_kernels(plan, lattices: list, mode="fp32") -> torch.Tensor:
+    """Step kernels [nm, d, d] (FP32, source-major) of a Monte Carlo plan (``plan.McPlan``)
+    on the device: each elementary kernel X_j = (I + dt_j L)^(2^niter_j) by the lattice
+    solve's squarings under its generator ``lattices[plan.i_j[j]]``, then each step kernel
+    the product of its elementary factors in time order (``opb_chain_kernels``), so a step
+    that spans a generator date chains kernels of different generators."""
+    dev = lattices[0].device
+    d = lattices[0].d
+    if any(lat.d != d for lat in lattices):
+        raise ValueError("every generator of a plan lives on the same states")
+    X = []
+    for j in range(plan.nj):
+        lat = lattices[plan.i_j[j]]
+        delta_t = (plan.t1_j[j] - plan.t0_j[j]) / 365.25
+        X.append(lat.kernel(delta_t, plan.dt_j[j], mode=mode, plan=Plan(plan.niter_j[j], plan.dt_j[j], 0.0)))
+    lib = _lib.load()
+    out = torch.empty(plan.nm, d, d, dtype=torch.float32, device=dev)
+    ws = torch.empty(int(lib.opb_chain_workspace_size(d)), dtype=torch.uint8, device=dev)
+    bind_stream(dev)
+    for m, factors in enumerate(plan.jfactor_ms):
+        ptrs = (C.c_void_p * len(factors))(*[X[j].data_ptr() for j in factors])
+        call("opb_chain_kernels", d, len(factors), ptrs, out[m].data_ptr(), ws.data_ptr(), ws.numel())
+    return out
+
+
 class BatchDesc(C.Structure):
     """Mirror of ``opb_batch_desc``."""
 

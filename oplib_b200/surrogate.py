@@ -150,43 +150,81 @@ class Surrogate:
 
     def train(self, data: QuoteSet, epochs: int = 10, batch: int = 4096, lr: float = 1e-3, seed: int = 0,
               lr_final: float = 1e-5):
+        """Adam with a cosine learning-rate decay from lr to lr_final over all steps; each
+        member draws its own batch order (seed + 101 m).  One epoch of a member (batch
+        gathers, opb_mlp_loss_grad, opb_mlp_adam_sched) is captured once in a CUDA graph
+        and replayed every epoch after a fresh permutation, the members' graphs on their own
+        streams so that their small kernels overlap."""
         X = normalise(data.feat)
         t = ((data.iv - data.base) / TARGET_SCALE).to(torch.float32).contiguous()
         n = X.shape[0]
         steps = n // batch
-        ws = torch.empty(int(self.lib.opb_mlp_workspace_floats(batch)), dtype=torch.float32, device=self.device)
-        grad = torch.empty(self.nparam, dtype=torch.float32, device=self.device)
-        loss = torch.zeros(1, dtype=torch.float64, device=self.device)
-        g = torch.Generator(device=self.device)
+        if steps < 1:
+            raise ValueError("fewer quotes than one batch")
+        total = epochs * steps
+        k = torch.arange(1, total + 1, dtype=torch.float64)
+        lr_tab = (lr_final + 0.5 * (lr - lr_final) * (1 + torch.cos(math.pi * k / total))).float().to(self.device)
         t0 = time.perf_counter()
+        dev = self.device
+        main = torch.cuda.current_stream(dev)
+        members = []
         for m in range(self.members):
-            g.manual_seed(seed + 101 * m)
-            theta = self.theta[m]
-            thb = torch.empty_like(theta)
-            mom = torch.zeros_like(theta)
-            var = torch.zeros_like(theta)
-            bind_stream(self.device)
-            call("opb_mlp_round", theta.data_ptr(), thb.data_ptr(), None)
-            step = 0
-            total = epochs * steps
-            for ep in range(epochs):
-                perm = torch.randperm(n, device=self.device, generator=g)
-                ep_loss = torch.zeros((), dtype=torch.float64, device=self.device)
-                for s in range(steps):
-                    idx = perm[s * batch:(s + 1) * batch]
-                    xb = X.index_select(0, idx).contiguous()
-                    tb = t.index_select(0, idx).contiguous()
-                    step += 1
-                    # cosine decay from lr to lr_final
-                    lr_s = lr_final + 0.5 * (lr - lr_final) * (1 + math.cos(math.pi * step / total))
-                    call("opb_mlp_loss_grad", thb.data_ptr(), xb.data_ptr(), tb.data_ptr(), batch, ws.data_ptr(),
-                         grad.data_ptr(), loss.data_ptr())
-                    call("opb_mlp_adam", theta.data_ptr(), mom.data_ptr(), var.data_ptr(), grad.data_ptr(), step,
-                         lr_s, 0.9, 0.999, 1e-8, thb.data_ptr())
-                    ep_loss += loss[0]
-                self.history.append((m, ep, float(ep_loss.item()) / (steps * batch)))
-            call("opb_mlp_pack", theta.data_ptr(), self.packed[m * self.stride:].data_ptr())
-        torch.cuda.synchronize()
+            st = dict(
+                theta=self.theta[m], thb=torch.empty_like(self.theta[m]), mom=torch.zeros_like(self.theta[m]),
+                var=torch.zeros_like(self.theta[m]), step=torch.zeros(1, dtype=torch.int32, device=dev),
+                perm=torch.empty(n, dtype=torch.int64, device=dev),
+                xb=torch.empty(batch, X.shape[1], dtype=torch.float32, device=dev),
+                tb=torch.empty(batch, dtype=torch.float32, device=dev),
+                ws=torch.empty(int(self.lib.opb_mlp_workspace_floats(batch)), dtype=torch.float32, device=dev),
+                grad=torch.empty(self.nparam, dtype=torch.float32, device=dev),
+                loss=torch.zeros(1, dtype=torch.float64, device=dev),
+                ep_loss=torch.zeros(1, dtype=torch.float64, device=dev),
+                gen=torch.Generator(device=dev), stream=torch.cuda.Stream(dev))
+            st["gen"].manual_seed(seed + 101 * m)
+            bind_stream(dev)
+            call("opb_mlp_round", st["theta"].data_ptr(), st["thb"].data_ptr(), None)
+            members.append(st)
+        torch.cuda.synchronize(dev)
+
+        def epoch(st):
+            for s in range(steps):
+                idx = st["perm"][s * batch:(s + 1) * batch]
+                torch.index_select(X, 0, idx, out=st["xb"])
+                torch.index_select(t, 0, idx, out=st["tb"])
+                call("opb_mlp_loss_grad", st["thb"].data_ptr(), st["xb"].data_ptr(), st["tb"].data_ptr(), batch,
+                     st["ws"].data_ptr(), st["grad"].data_ptr(), st["loss"].data_ptr())
+                call("opb_mlp_adam_sched", st["theta"].data_ptr(), st["mom"].data_ptr(), st["var"].data_ptr(),
+                     st["grad"].data_ptr(), st["step"].data_ptr(), lr_tab.data_ptr(), 0.9, 0.999, 1e-8,
+                     st["thb"].data_ptr())
+                st["ep_loss"].add_(st["loss"])
+
+        for st in members:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(st["stream"]):
+                bind_stream(dev)
+                g.capture_begin()
+                epoch(st)
+                g.capture_end()
+            st["graph"] = g
+        bind_stream(dev)
+        for ep in range(epochs):
+            for st in members:
+                st["stream"].wait_stream(main)
+                with torch.cuda.stream(st["stream"]):
+                    st["perm"].copy_(torch.randperm(n, device=dev, generator=st["gen"]))
+                    st["ep_loss"].zero_()
+                    st["graph"].replay()
+            for m, st in enumerate(members):
+                main.wait_stream(st["stream"])
+                self.history.append((m, ep, st["ep_loss"].clone()))
+        torch.cuda.synchronize(dev)
+        self.history = [(m, ep, float(v.item()) / (steps * batch)) if torch.is_tensor(v) else (m, ep, v)
+                        for m, ep, v in self.history]
+        bind_stream(dev)
+        for m, st in enumerate(members):
+            call("opb_mlp_pack", st["theta"].data_ptr(), self.packed[m * self.stride:].data_ptr())
+            st["graph"].reset()
+        torch.cuda.synchronize(dev)
         self.train_seconds = time.perf_counter() - t0
         return self.history
 

@@ -53,6 +53,27 @@ def forward(theta, X):
     return (h @ W.T + b)[:, 0], cache, h
 
 
+def bf16_round(a):
+    """Round to the nearest BF16 value (ties to even), returned as FP64."""
+    a32 = np.ascontiguousarray(a, dtype=np.float32)
+    u = a32.view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return (u & 0xFFFFFFFF).astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def forward_inference(theta, X):
+    """The numerics of the library's tensor-core inference (opb_mlp_infer), in FP64: every
+    parameter and the input rounded to BF16 (the packed weights), products summed exactly,
+    the exact-erf GELU, each hidden layer's activations rounded to BF16 (they are stored as
+    BF16 between layers), then y = w5 . h4 + b5.  Returns y [n]."""
+    layers = [(bf16_round(W), bf16_round(b)) for W, b in unpack(np.asarray(theta, dtype=np.float64))]
+    h = bf16_round(X)
+    for W, b in layers[:-1]:
+        h = bf16_round(gelu(h @ W.T + b))
+    W, b = layers[-1]
+    return (h @ W.T + b)[:, 0]
+
+
 def loss_grad(theta, X, t):
     """Sum of squared errors and its gradient; the library's kernels use the gradient of
     the mean (the 1/B factor), so compare with grad / B."""

@@ -433,6 +433,24 @@ def price_from_kernels(Ps: list[np.ndarray], x: np.ndarray, strikes: np.ndarray,
     return np.stack([math.exp(-r * T) * (P @ G) for P, T in zip(Ps, mats)])
 
 
+def mc_cashflow_values(paths: np.ndarray, cashflow: np.ndarray, knockout: np.ndarray | None = None) -> np.ndarray:
+    """Per-path values of the cashflow-table evaluator: v_p = sum_k cashflow[k, y_pk] over the
+    steps k before the first one whose state is knocked out (knockout[k, y_pk] != 0), added
+    in step order in FP64.  It generalises the reference's vanilla evaluator
+    (``tests/bstest/OPPricer.cs:8-63``: the payoff (x_T - K)^+ of the last step's state,
+    called back on host copies of the states, ``oplib/opmodel/interfaces/CMCEvaluator.cs:41-67``)
+    to cashflows at every step with discrete knock-out.  paths: [npaths, nsteps] states."""
+    npaths, nsteps = paths.shape
+    v = np.zeros(npaths)
+    alive = np.ones(npaths, dtype=bool)
+    for k in range(nsteps):
+        y = paths[:, k].astype(np.int64)
+        if knockout is not None:
+            alive &= knockout[k, y] == 0
+        v = np.where(alive, v + cashflow[k, y], v)
+    return v
+
+
 def host_solve_stages(L, x, strikes, r: float, period: float, nmat: int, niter: int, dt: float):
     """The reference's host FP64 solve, one product at a time, on torch-CPU FP64 tensors
     (the matrix products are MKL DGEMMs, the library family of ``opc_dgemm``,

@@ -1,0 +1,130 @@
+"""Band-limited squarings and the fourth split product (lo.lo) on the GPU.
+
+- An ELL generator's half-bandwidth h0 bounds E_r = P(2^r dt) - I to |row - col| <= h0 2^r,
+  so the squarings issue only the K-blocks within reach of each output tile and skip the tiles
+  no K-block reaches.  The skipped products are exact zeros and the issued chunks are the
+  full product's, so quotes, all-state values and the period kernel are bit-identical with
+  the skipping switched off (``opb_set_band_skip``), in both split modes, single and batched.
+- Split-BF16 squarings add lo.lo on their first 8 levels (``opb_set_lolo_levels``).  The
+  calibration sweep's extreme lattices (seed 20260: the stiffest generator, hence the most
+  squarings, at n = 2048, 1920 and 1792, and the two stiffest at n = 256) then price within
+  1e-5 of the FP64 oracle in bf16x3, as in fp16x3; the three-product form (n = 0) misses the
+  bar on them (1.4e-5 on the n = 1792 lattice).
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+STRIKES = 0.5 + np.arange(32) / 31.0
+NMAT, PERIOD, DT0 = 8, 0.25, 2.0 ** -14
+
+
+@pytest.fixture()
+def knobs(cuda):
+    """Restores the library's defaults after a test that changes them."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    yield lib
+    assert lib.opb_set_band_skip(1) == 0
+    assert lib.opb_set_lolo_levels(8) == 0
+
+
+def _equal(a, b):
+    return np.array_equal(a.cpu().numpy(), b.cpu().numpy())
+
+
+@pytest.mark.parametrize("mode", ["bf16x3", "fp16x3"])
+@pytest.mark.parametrize("kind", ["lv1024", "sv64x16"])
+def test_band_skip_is_bit_identical_single(knobs, cuda, mode, kind):
+    from oplib_b200.model import Lattice
+    lat = (Lattice.local_vol(n=1024, level=0.3, skew=0.2, width=0.3, rate=0.02) if kind == "lv1024"
+           else Lattice.stoch_vol(nx=64, nv=16))
+    out = {}
+    for on in (1, 0):
+        assert knobs.opb_set_band_skip(on) == 0
+        q, V = lat.solve(STRIKES, 4, PERIOD, DT0, mode=mode, all_states=True)
+        P = lat.kernel(PERIOD, DT0, mode=mode)
+        torch.cuda.synchronize()
+        out[on] = (q, V, P)
+    assert knobs.opb_tc_error() == 0
+    for a, b in zip(out[1], out[0]):
+        assert _equal(a, b)
+
+
+def test_band_skip_is_bit_identical_batched(knobs, cuda):
+    from oplib_b200.model import Batch, Lattice
+    specs = [dict(n=128, level=0.25, skew=0.1, width=0.5, rate=0.02, floor=0.01),
+             dict(n=640, level=0.15, skew=-0.2, width=0.3, rate=0.04, floor=0.01),
+             dict(n=1024, level=0.35, skew=0.25, width=0.9, rate=0.0, floor=0.01),
+             dict(n=256, level=0.1, skew=-0.3, width=0.2, rate=0.05, floor=0.01)]
+    lats = [Lattice.local_vol(device=cuda, **s) for s in specs]
+    for mode in ("bf16x3", "fp16x3"):
+        b = Batch(lats, STRIKES, 4, PERIOD, DT0, mode=mode, autotune=False)
+        from oplib_b200 import _lib
+        for cfg in (0, 4, 6):
+            b.set_config(cfg)
+            res = {}
+            for on in (1, 0):
+                assert knobs.opb_set_band_skip(on) == 0
+                res[on] = (b.execute().clone(), b.execute_bermudan(put=True).clone())
+            torch.cuda.synchronize()
+            assert _equal(res[1][0], res[0][0]) and _equal(res[1][1], res[0][1]), (mode, cfg)
+        assert _lib.load().opb_tc_error() == 0
+
+
+def _extremes():
+    """Indices into the seed-20260 sweep: the stiffest lattice at n = 2048, 1920, 1792 and the
+    two stiffest at n = 256 (the plan's niter grows with max |L_yy|)."""
+    from oplib_b200.model import calibration_sweep
+    _, params = calibration_sweep(build=False)
+    stiff = []
+    for i, p in enumerate(params):
+        x = O.log_grid(p["n"])
+        L = O.lv_generator_fast(x, p["rate"] * x, O.lv_sigma(x, p["level"], p["skew"], p["width"], p["floor"]) * x)
+        stiff.append(float(np.abs(np.diag(L)).max()))
+    pick = []
+    for n, k in ((2048, 1), (1920, 1), (1792, 1), (256, 2)):
+        idx = [i for i, p in enumerate(params) if p["n"] == n]
+        pick += sorted(idx, key=lambda i: -stiff[i])[:k]
+    return params, pick
+
+
+@pytest.fixture(scope="module")
+def sweep_extremes(cuda):
+    params, pick = _extremes()
+    refs = {}
+    for i in pick:
+        p = params[i]
+        x = O.log_grid(p["n"])
+        L = O.lv_generator_fast(x, p["rate"] * x, O.lv_sigma(x, p["level"], p["skew"], p["width"], p["floor"]) * x)
+        V, niter, _ = O.solve_lattice_fp64(L, x, STRIKES, p["rate"], PERIOD, NMAT, DT0)
+        refs[i] = (V[:, O.nearest_node(x), :], niter)
+    return params, pick, refs
+
+
+def test_sweep_extremes_within_1e5(knobs, sweep_extremes):
+    from oplib_b200.model import Batch, Lattice
+    params, pick, refs = sweep_extremes
+    lats = [Lattice.local_vol(**params[i]) for i in pick]
+    assert max(refs[i][1] for i in pick) == 16  # the sweep's deepest plan is among them
+    errs = {}
+    for mode, lolo in (("bf16x3", 8), ("fp16x3", 8), ("bf16x3", 0)):
+        assert knobs.opb_set_lolo_levels(lolo) == 0
+        b = Batch(lats, STRIKES, NMAT, PERIOD, DT0, mode=mode, autotune=True)
+        q = b.execute().cpu().numpy()
+        errs[(mode, lolo)] = [float(np.abs(q[j] - refs[i][0]).max()) for j, i in enumerate(pick)]
+        # the single-lattice solve applies the same rule
+        qs, _ = lats[0].solve(STRIKES, NMAT, PERIOD, DT0, mode=mode)
+        assert np.abs(qs.cpu().numpy() - q[0]).max() < 1e-6
+    from oplib_b200 import _lib
+    assert _lib.load().opb_tc_error() == 0
+    for key, e in errs.items():
+        print(key, " ".join(f"n={params[i]['n']}/niter={refs[i][1]}:{v:.2e}" for i, v in zip(pick, e)))
+    assert max(errs[("bf16x3", 8)]) <= 1e-5
+    assert max(errs[("fp16x3", 8)]) <= 1e-5
+    # lo.lo on the first levels is what brings split-BF16 within the bar on the stiff lattices
+    assert max(errs[("bf16x3", 8)]) < 0.5 * max(errs[("bf16x3", 0)])

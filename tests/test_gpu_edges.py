@@ -124,12 +124,30 @@ def test_fp32_path_on_a_size_not_multiple_of_64(cuda):
     assert np.abs(Vall.cpu().numpy() - V).max() < 1e-5 * max(1.0, np.abs(V).max())
 
 
-def test_split_modes_reject_sizes_off_the_tile_grid(cuda):
-    from oplib_b200._lib import OpcudaError
+@pytest.mark.parametrize("mode", ["bf16x3", "fp16x3"])
+@pytest.mark.parametrize("n", [100, 300])
+def test_split_modes_on_sizes_off_the_tile_grid(cuda, mode, n):
+    """The split modes solve a lattice whose size is no multiple of 128 as one padded with
+    absorbing states: quotes, all-state values and the period kernel against the FP64
+    oracle, and a Bermudan put against the oracle's induction."""
     from oplib_b200.model import Lattice
-    lat = Lattice.local_vol(n=100)
-    with pytest.raises(OpcudaError):
-        lat.solve([1.0], 1, 0.25, 2.0 ** -14, mode="bf16x3")
+    cfg = O.LVLattice(n=n, nmat=3)
+    L, x = cfg.generator()
+    K = cfg.strikes[::8]
+    V, niter, dt = O.solve_lattice_fp64(L, x, K, cfg.r, cfg.period, cfg.nmat, cfg.dt0)
+    lat = Lattice.local_vol(n=n, level=cfg.level, skew=cfg.skew, width=cfg.width, rate=cfg.r)
+    q, Vall = lat.solve(K, cfg.nmat, cfg.period, cfg.dt0, mode=mode, all_states=True)
+    P = lat.kernel(cfg.period, cfg.dt0, mode=mode)
+    torch.cuda.synchronize()
+    assert q.shape == (cfg.nmat, K.size) and Vall.shape == (cfg.nmat, n, K.size) and P.shape == (n, n)
+    assert np.abs(q.cpu().numpy() - V[:, O.nearest_node(x), :]).max() < 1e-5
+    assert np.abs(Vall.cpu().numpy() - V).max() < 5e-5 * max(1.0, np.abs(V).max())
+    P1 = O.square(O.ek(L, dt), niter, renorm=True)
+    assert np.abs(P.cpu().numpy() - P1).max() < 2e-5
+    assert np.allclose(P.double().sum(1).cpu().numpy(), 1.0, atol=1e-6)
+    Vb = O.bermudan_fp64(L, x, K, cfg.r, cfg.period, cfg.nmat, cfg.dt0, put=True)
+    qb = lat.bermudan(K, cfg.nmat, cfg.period, cfg.dt0, put=True, mode=mode)
+    assert np.abs(qb.cpu().numpy() - Vb[O.nearest_node(x)]).max() < 1e-5
 
 
 def test_batch_of_one_lattice_matches_its_single_solve(cuda):

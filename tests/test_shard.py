@@ -65,7 +65,7 @@ def test_mc_shards_reproduce_single_process():
     from oracle import oracle as O
     from oracle import oracle_c as OC
     world = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_mc_worker, args=(world, _free_port(), out), nprocs=world, join=True)
     cfg = O.LVLattice(n=128)
@@ -101,7 +101,7 @@ def _batch_worker(rank, world, port, out):
 def test_batch_shards_gather_all_quotes():
     from oracle import oracle as O
     world = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_batch_worker, args=(world, _free_port(), out), nprocs=world, join=True)
     sizes = [64, 96, 128, 64, 160, 32, 96]

@@ -55,3 +55,13 @@ def test_noalloc_mc_matches_regular_entry_point_twice():
         assert torch.equal(paths, paths_ref), f"call {call}: state paths differ"
         s, sr = sums.cpu().numpy(), sums_ref.cpu().numpy()
         assert np.all(np.isfinite(s)) and np.allclose(s, sr, rtol=1e-12, atol=0.0), (call, s, sr)
+
+    # once set up, a call allocates no device memory: the device's free memory is the same
+    # before and after it (torch's caching allocator idle in between)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(dev)
+    assert lib.opb_mc_mt19937_noalloc(Cm.data_ptr(), d, 1, g.data_ptr(), 64, d, lat.y0, nsteps, 5489, 0, npaths,
+                                      paths.data_ptr(), lat.x.data_ptr(), 1.0, 0.7, disc, sums.data_ptr()) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0, (free0, free1)
