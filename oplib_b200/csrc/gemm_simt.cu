@@ -128,8 +128,144 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_sgemm_rm(SgemmArgs p) {
     }
 }
 
+// ---- the pipelined form for whole tiles (row-major A and B, M and N multiples of 128, K of
+// 16, 16-byte aligned rows, no pointer tables): K in steps of 16 through a 3-stage
+// cp.async ring (A rows padded to 20 floats, so the two row groups of a warp fall on
+// different banks), each thread 8 x 8 outputs from 128-bit shared loads of A along k and of
+// B along n.  Every output still sums its products in k order, so the results are
+// bit-identical to k_sgemm_rm's.
+constexpr int SF_BK = 16, SF_STAGES = 3, SF_APITCH = SF_BK + 4;
+constexpr int SF_A_FLOATS = SG_BM * SF_APITCH, SF_B_FLOATS = SF_BK * SG_BN;
+constexpr int SF_SMEM = SF_STAGES * (SF_A_FLOATS + SF_B_FLOATS) * 4;
+
+__device__ __forceinline__ void sf_cp16(float *dst, const float *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void sf_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void sf_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(SG_THREADS, 2) k_sgemm_pipe(SgemmArgs p) {
+    extern __shared__ __align__(16) float sm[];
+    const int z = blockIdx.z;
+    const float *A = p.A + z * p.sA;
+    const float *B = p.B + z * p.sB;
+    float *C = p.C + z * p.sC;
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    const int m0 = blockIdx.y * SG_BM, n0 = blockIdx.x * SG_BN;
+    const float *Ab = A + (long long)m0 * p.lda;
+    const float *Bb = B + n0;
+
+    auto issue = [&](int stage, int k0) {
+        float *As = sm + stage * (SF_A_FLOATS + SF_B_FLOATS);
+        float *Bs = As + SF_A_FLOATS;
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const int c = tid + SG_THREADS * i;
+            const int row = c >> 2, kq = (c & 3) * 4;  // 128 rows x 4 chunks of 4 floats
+            sf_cp16(As + row * SF_APITCH + kq, Ab + (long long)row * p.lda + k0 + kq);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const int c = tid + SG_THREADS * i;
+            const int kr = c >> 5, col = (c & 31) * 4;  // 16 rows x 32 chunks of 4 floats
+            sf_cp16(Bs + kr * SG_BN + col, Bb + (long long)(k0 + kr) * p.ldb + col);
+        }
+        sf_commit();
+    };
+
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+
+    const int nk = p.K / SF_BK;
+#pragma unroll
+    for (int st = 0; st < SF_STAGES - 1; st++) {
+        if (st < nk) issue(st, st * SF_BK);
+        else sf_commit();
+    }
+    for (int kt = 0; kt < nk; kt++) {
+        sf_wait<SF_STAGES - 2>();
+        __syncthreads();  // stage kt landed for every thread; stage kt - 1 is free to refill
+        const int nt = kt + SF_STAGES - 1;
+        if (nt < nk) issue(nt % SF_STAGES, nt * SF_BK);
+        else sf_commit();
+        const float *As = sm + (kt % SF_STAGES) * (SF_A_FLOATS + SF_B_FLOATS);
+        const float *Bs = As + SF_A_FLOATS;
+#pragma unroll
+        for (int kk = 0; kk < SF_BK; kk += 4) {
+            float4 a4[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int row = i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4);
+                a4[i] = *reinterpret_cast<const float4 *>(As + row * SF_APITCH + kk);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const float4 b0 = *reinterpret_cast<const float4 *>(Bs + (kk + u) * SG_BN + tx * 4);
+                const float4 b1 = *reinterpret_cast<const float4 *>(Bs + (kk + u) * SG_BN + 64 + tx * 4);
+                const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const float a = u == 0 ? a4[i].x : u == 1 ? a4[i].y : u == 2 ? a4[i].z : a4[i].w;
+#pragma unroll
+                    for (int j = 0; j < 8; j++) acc[i][j] = fmaf(a, b[j], acc[i][j]);
+                }
+            }
+        }
+    }
+    sf_wait<0>();
+
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int r = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+        float *crow = C + (long long)r * p.ldc + n0;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            float4 *cp = reinterpret_cast<float4 *>(crow + h * 64 + tx * 4);
+            float4 v = make_float4(p.alpha * acc[i][4 * h], p.alpha * acc[i][4 * h + 1], p.alpha * acc[i][4 * h + 2],
+                                   p.alpha * acc[i][4 * h + 3]);
+            if (p.beta != 0.f) {
+                const float4 c = *cp;
+                v.x = fmaf(p.beta, c.x, v.x);
+                v.y = fmaf(p.beta, c.y, v.y);
+                v.z = fmaf(p.beta, c.z, v.z);
+                v.w = fmaf(p.beta, c.w, v.w);
+            }
+            *cp = v;
+        }
+    }
+}
+
+static bool sgemm_pipe_ok(const SgemmArgs &a, int batch) {
+    auto al = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 15) == 0; };
+    return !a.A_tab && !a.B_tab && !a.C_tab && a.M % SG_BM == 0 && a.N % SG_BN == 0 && a.K % SF_BK == 0 &&
+           a.K > 0 && a.lda % 4 == 0 && a.ldb % 4 == 0 && a.ldc % 4 == 0 && al(a.A) && al(a.B) && al(a.C) &&
+           (batch == 1 || (a.sA % 4 == 0 && a.sB % 4 == 0 && a.sC % 4 == 0));
+}
+
 int sgemm_rowmajor(const SgemmArgs &a, int batch, cudaStream_t s, bool ta = false, bool tb = false) {
     if (a.M <= 0 || a.N <= 0 || batch <= 0) return OPB_OK;
+    if (!ta && !tb && sgemm_pipe_ok(a, batch)) {
+        static bool attr[64] = {false};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev >= 0 && dev < 64 && !attr[dev]) {
+            cudaError_t e = cudaFuncSetAttribute(k_sgemm_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, SF_SMEM);
+            if (e != cudaSuccess) return (int)e;
+            attr[dev] = true;
+        }
+        dim3 grid(a.N / SG_BN, a.M / SG_BM, batch);
+        k_sgemm_pipe<<<grid, SG_THREADS, SF_SMEM, s>>>(a);
+        return static_cast<int>(cudaGetLastError());
+    }
     dim3 grid((a.N + SG_BN - 1) / SG_BN, (a.M + SG_BM - 1) / SG_BM, batch);
     if (!ta && !tb) k_sgemm_rm<false, false><<<grid, SG_THREADS, 0, s>>>(a);
     else if (ta && !tb) k_sgemm_rm<true, false><<<grid, SG_THREADS, 0, s>>>(a);

@@ -198,6 +198,14 @@ class Surrogate:
                      st["thb"].data_ptr())
                 st["ep_loss"].add_(st["loss"])
 
+        # one gradient evaluation per member outside the capture (it changes no weights), so
+        # that every kernel's one-time set-up has run before the capture
+        for st in members:
+            torch.index_select(X, 0, st["perm"][:batch].copy_(torch.arange(batch, device=dev)), out=st["xb"])
+            torch.index_select(t, 0, st["perm"][:batch], out=st["tb"])
+            call("opb_mlp_loss_grad", st["thb"].data_ptr(), st["xb"].data_ptr(), st["tb"].data_ptr(), batch,
+                 st["ws"].data_ptr(), st["grad"].data_ptr(), st["loss"].data_ptr())
+        torch.cuda.synchronize(dev)
         for st in members:
             g = torch.cuda.CUDAGraph()
             with torch.cuda.stream(st["stream"]):

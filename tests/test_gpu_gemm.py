@@ -505,3 +505,31 @@ def test_opcuda_sgemv_on_two_streams(cuda):
         ref = A.astype(np.float64) @ xs[k]
         bound = (np.abs(A) @ np.abs(xs[k])) * (n + 8) * 2.0 ** -24
         assert np.all(np.abs(ys[k].cpu().numpy() - ref) <= bound + 1e-6)
+
+
+@pytest.mark.parametrize("M,N,K,batch", [(256, 384, 272, 1), (128, 128, 16, 3), (512, 256, 1024, 2)])
+def test_sgemm_pipelined_bit_identical_to_tiled(cuda, M, N, K, batch):
+    """Whole-tile shapes with 16-byte aligned operands take the cp.async-pipelined SIMT kernel;
+    the same operands one float off alignment take the register-staged one.  Both sum each
+    output's products in k order with fused multiply-adds: bit-identical results, and within
+    the FP32 bound of the FP64 product."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(M + N + K)
+    A = rng.standard_normal((batch, M, K)).astype(np.float32)
+    B = rng.standard_normal((batch, K, N)).astype(np.float32)
+    outs = []
+    for off in (0, 1):
+        dA = torch.zeros(batch * M * K + 4, device=cuda)
+        dB = torch.zeros(batch * K * N + 4, device=cuda)
+        dC = torch.zeros(batch * M * N + 4, device=cuda)
+        dA[off:off + A.size] = torch.from_numpy(A.ravel()).to(cuda)
+        dB[off:off + B.size] = torch.from_numpy(B.ravel()).to(cuda)
+        assert lib.opb_sgemm_batched_rm(M, N, K, dA.data_ptr() + 4 * off, M * K, dB.data_ptr() + 4 * off, K * N,
+                                        dC.data_ptr() + 4 * off, M * N, batch) == 0
+        torch.cuda.synchronize()
+        outs.append(dC[off:off + batch * M * N].cpu().numpy().reshape(batch, M, N))
+    assert np.array_equal(outs[0], outs[1])
+    ref = np.einsum("bmk,bkn->bmn", A.astype(np.float64), B.astype(np.float64))
+    bound = K * 2.0 ** -23 * np.einsum("bmk,bkn->bmn", np.abs(A).astype(np.float64), np.abs(B).astype(np.float64))
+    assert np.all(np.abs(outs[0] - ref) <= bound)
