@@ -505,47 +505,50 @@ def _host_info():
 
 
 class HostSolve:
-    """The reference's host FP64 solve of the headline SV lattice (``oracle.host_solve_stages``:
+    """The reference's host FP64 solve of the headline SV lattice (``oracle.HostSolveFP64``:
     U0 = I + dt L, 14 squarings and 15 chain products as torch-CPU/MKL DGEMMs, the payoff
-    product after each P_m) on all host threads, driven one product ("stage") at a time.  A
-    solve is 29 stages; the generator (dense FP64, 302 MB) is built once, outside every
-    timed stage, like the strikes.  When a solve ends the next one starts over."""
+    product with each P_m) on all host threads, one product ("stage") at a time; a solve is
+    29 stages.  The generator (dense FP64, 302 MB) is built once, outside every timing,
+    like the strikes.  Denormal operands are flushed to zero (torch.set_flush_denormal): the
+    far corners of the middle squarings' operands underflow, and FP64 products with
+    denormal operands run several times slower on x86; flushing them changes no price and
+    makes this CPU baseline faster, not slower."""
 
     def __init__(self):
         import torch
 
         from oracle import oracle as O
-        self.torch = torch
         self.nth, self.model = _host_info()
         torch.set_num_threads(self.nth)
+        self.ftz = bool(torch.set_flush_denormal(True))
         spec = O.SVSpec(nx=SV["nx"], nv=SV["nv"], x_lo=SV["x_lo"], x_hi=SV["x_hi"], v_lo=SV["v_lo"], v_hi=SV["v_hi"],
                         r=SV["rate"], kappa=SV["kappa"], theta=SV["theta"], xi=SV["xi"], rho=SV["rho"])
-        L, self.x, _ = O.sv_generator(spec)
-        self.niter, self.dt = O.plan_niter(L, PERIOD, DT0)
-        self.L = torch.from_numpy(L)
-        self.O = O
-        self.stages = self.niter + NMAT - 1
-        self.solves_done = 0
-        self.V = None
-        self._gen = None
+        L, x, _ = O.sv_generator(spec)
+        niter, dt = O.plan_niter(L, PERIOD, DT0)
+        self.hs = O.HostSolveFP64(torch.from_numpy(L), x, STRIKES, SV["rate"], PERIOD, NMAT, niter, dt)
+        self.niter, self.stages, self.d = niter, self.hs.stages, L.shape[0]
 
-    def stage(self):
-        """Runs the next product of the current solve (starting a new solve if needed)."""
-        if self._gen is None:
-            self._gen = self.O.host_solve_stages(self.L.clone(), self.x, STRIKES, SV["rate"], PERIOD, NMAT,
-                                                 self.niter, self.dt)
-            self._left = self.stages
-        out = next(self._gen)
-        self._left -= 1
-        if self._left == 0:
-            self.V, self._gen = out, None
-            self.solves_done += 1
-
-    def solve(self):
-        """One whole solve, timed: seconds."""
+    def solve(self, keep=()):
+        """One whole solve; returns (seconds, values, {stage: its input state} for the stages in
+        ``keep``)."""
+        inputs, state = {}, {}
         t0 = time.perf_counter()
-        for _ in range(self.stages):
-            self.stage()
+        for p in range(self.stages):
+            if p in keep:
+                inputs[p] = state
+            state = self.hs.run(p, state)
+        t = time.perf_counter() - t0
+        return t, self.hs.values(state), inputs
+
+    def positions(self, k: int):
+        """k stage positions spread evenly over a solve (all of them, cyclically, if k > 29), so
+        that a sample of k stages weighs the solve's cheap and dear products as the solve does."""
+        return [int((i + 0.5) * self.stages / k) % self.stages if k < self.stages else i % self.stages
+                for i in range(k)]
+
+    def run_stage(self, p, state):
+        t0 = time.perf_counter()
+        self.hs.run(p, state)
         return time.perf_counter() - t0
 
 
@@ -553,16 +556,14 @@ def cpu_baseline():
     """The reference's host FP64 solve (``HostSolve``): one whole config-1 solve (29 DGEMM
     products of 6144^3 with the O(d^2) work) timed on all host threads."""
     hs = HostSolve()
-    hs.stage()  # warm the BLAS threads (one product, not timed)
-    hs._gen = None
-    t = hs.solve()
-    assert hs.V is not None and hs.V.shape == (NMAT, hs.L.shape[0], NK)
-    assert hs.solves_done == 1
+    hs.hs.run(0, {})  # warm the BLAS threads (one product, not timed)
+    t, V, _ = hs.solve()
+    assert V.shape == (NMAT, hs.d, NK)
     return {"value": round(NMAT * NK / t, 3), "unit": "quotes/s", "cores": hs.nth, "kind": "port",
             "cpu_model": hs.model,
             "sample": f"one whole FP64 solve of the SV lattice (U0 = I + dt L, {hs.niter} squarings, {NMAT - 1} "
-                      f"chain products, payoff products; torch-CPU/MKL DGEMM, {hs.nth} threads) = {t:.2f} s; "
-                      "generator built once outside the timing"}
+                      f"chain products, payoff products; torch-CPU/MKL DGEMM, {hs.nth} threads, denormals "
+                      f"flushed: {hs.ftz}) = {t:.2f} s; generator built once outside the timing"}
 
 
 # ----------------------------------------------------------------------------------------
@@ -1485,28 +1486,28 @@ def main():
 
     if args.impl == "reference":
         # The reference's own host FP64 path on the host cores (rank 0 only).  A step is one
-        # product of the solve (a bounded sample of it: 1/29 of a solve), the solve running on
-        # from step to step and starting over when it ends; value = quotes per solve times the
-        # solves the timed steps complete per second.
+        # product of the solve, a bounded sample of it (1/29 of a solve).  One whole solve runs
+        # first, untimed (it also warms the BLAS threads); it keeps the inputs of the stages
+        # the timed steps run, spread evenly over the solve, so that the sample weighs cheap
+        # and dear products as a solve does.  value = quotes per solve x (timed products / 29)
+        # / timed seconds.
         if rank != 0:
             return 0
         t0 = time.perf_counter()
         hs = HostSolve()
-        for _ in range(args.warmup):
-            hs.stage()
-        ts = []
-        for _ in range(args.steps):
-            t1 = time.perf_counter()
-            hs.stage()
-            ts.append(time.perf_counter() - t1)
+        pos = hs.positions(args.steps)
+        t_full, _, inputs = hs.solve(keep=set(pos))
+        for i in range(args.warmup):
+            hs.run_stage(pos[i % len(pos)], inputs[pos[i % len(pos)]])
+        ts = [hs.run_stage(p, inputs[p]) for p in pos]
         timed = sum(ts)
         v = round(NMAT * NK * (args.steps / hs.stages) / timed, 3)
         cb = {"value": v, "unit": "quotes/s", "cores": hs.nth, "kind": "port", "cpu_model": hs.model,
-              "sample": f"{args.steps} timed products (after {args.warmup} untimed) of the reference's host FP64 "
-                        f"solve of the SV lattice, {hs.stages} products per solve (U0 = I + dt L, {hs.niter} "
-                        f"squarings, {NMAT - 1} chain products; payoff products with their P_m); torch-CPU/MKL "
-                        f"DGEMM, {hs.nth} threads; value = {NMAT * NK} quotes x (timed products / {hs.stages}) / "
-                        "timed seconds"}
+              "sample": f"{args.steps} timed products of the reference's host FP64 solve of the SV lattice at stage "
+                        f"positions spread over the {hs.stages} of a solve (U0 = I + dt L, {hs.niter} squarings, "
+                        f"{NMAT - 1} chain products; payoff products with their P_m), inputs from one untimed "
+                        f"whole solve; torch-CPU/MKL DGEMM, {hs.nth} threads, denormals flushed: {hs.ftz}; "
+                        f"value = {NMAT * NK} quotes x (timed products / {hs.stages}) / timed seconds"}
         line = {"impl": "reference", "metric": SV_METRIC, "value": v,
                 "unit": "quotes/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": round(timed / args.steps * 1e3, 1), "higher_is_better": True, "scaling": "weak",
@@ -1515,7 +1516,7 @@ def main():
                 "cpu_baseline": cb, "e2e": {"value": v, "unit": "quotes/s", "h2d_bytes_per_step": 0,
                                             "d2h_bytes_per_step": 0},
                 "step_s_min_max": [round(min(ts), 3), round(max(ts), 3)],
-                "solves_completed": hs.solves_done,
+                "untimed_whole_solve_s": round(t_full, 2),
                 "wall_s": round(time.perf_counter() - t0, 1)}
         print(json.dumps(line))
         return 0

@@ -451,38 +451,64 @@ def mc_cashflow_values(paths: np.ndarray, cashflow: np.ndarray, knockout: np.nda
     return v
 
 
-def host_solve_stages(L, x, strikes, r: float, period: float, nmat: int, niter: int, dt: float):
-    """The reference's host FP64 solve, one product at a time, on torch-CPU FP64 tensors
-    (the matrix products are MKL DGEMMs, the library family of ``opc_dgemm``,
+class HostSolveFP64:
+    """The reference's host FP64 solve, one product ("stage") at a time, on torch-CPU FP64
+    tensors (the matrix products are MKL DGEMMs, the library family of ``opc_dgemm``,
     ``oplib/opc/linalg.c:93-101``):
 
-    * U0 = I + dt L (``host_d_mc_ek``, ``CModel Host Double.cs:89-121``);
-    * niter squarings U <- U.U (``host_d_mc_sq``, ``CModel Host Double.cs:125-197``);
-    * chaining P_m = P_{m-1}.P1, m = 2..nmat (``host_d_mc_mk``, ``CModel Host Double.cs:227-277``);
-    * the payoff product V_m = exp(-r m period) P_m.G for every source state once P_m is
-      formed (the backward induction the reference exports as ``sgemv``/``sdot2`` kernels).
+    * U0 = I + dt L (``host_d_mc_ek``, ``CModel Host Double.cs:89-121``), built in stage 0;
+    * stages 0..niter-1: squarings U <- U.U (``host_d_mc_sq``, ``CModel Host Double.cs:125-197``);
+    * stages niter..niter+nmat-2: chaining P_m = P_{m-1}.P1, m = 2..nmat (``host_d_mc_mk``,
+      ``CModel Host Double.cs:227-277``);
+    * the payoff product V_m = exp(-r m period) P_m.G for every source state in the stage
+      that forms P_m (the backward induction the reference exports as ``sgemv``/``sdot2``).
 
     No renormalisation: the reference's host path has none (row sums stay 1 to FP64
-    rounding).  A generator that yields once per product, niter + nmat - 1 times (U0 is built
-    in the first stage, each payoff product in the stage that forms its P_m): None, and at the
-    last stage V [nmat, d, nK].  niter >= 1.  L: torch FP64 [d, d] (row = source)."""
-    import torch
-    xs = torch.as_tensor(np.asarray(x, dtype=np.float64))
-    K = torch.as_tensor(np.asarray(strikes, dtype=np.float64))
-    G = torch.clamp(xs[:, None] - K[None, :], min=0.0)
-    V = []
-    U = L * dt
-    U.diagonal().add_(1.0)
-    for lev in range(niter):
-        U = U @ U
-        if lev == niter - 1:
-            V.append(math.exp(-r * period) * (U @ G))
-        yield torch.stack(V) if (lev == niter - 1 and nmat == 1) else None
-    P1 = Pm = U
-    for m in range(2, nmat + 1):
-        Pm = Pm @ P1
-        V.append(math.exp(-r * period * m) * (Pm @ G))
-        yield torch.stack(V) if m == nmat else None
+    rounding).  ``state`` holds the stage's inputs (``U``, or ``Pm`` and ``P1``) and the
+    values so far; ``run`` leaves its inputs untouched, so a stage can be run again on the
+    same inputs.  niter >= 1.  L: torch FP64 [d, d] (row = source)."""
+
+    def __init__(self, L, x, strikes, r: float, period: float, nmat: int, niter: int, dt: float):
+        import torch
+        self.torch = torch
+        self.L, self.r, self.period, self.nmat, self.niter, self.dt = L, r, period, nmat, niter, dt
+        xs = torch.as_tensor(np.asarray(x, dtype=np.float64))
+        K = torch.as_tensor(np.asarray(strikes, dtype=np.float64))
+        self.G = torch.clamp(xs[:, None] - K[None, :], min=0.0)
+        self.stages = niter + nmat - 1
+
+    def run(self, p: int, state: dict) -> dict:
+        """Stage p on the inputs in ``state``; returns the next stage's state."""
+        if p < self.niter:
+            if p == 0:
+                U = self.L * self.dt
+                U.diagonal().add_(1.0)
+            else:
+                U = state["U"]
+            U = U @ U
+            V = list(state.get("V", []))
+            if p == self.niter - 1:
+                V.append(math.exp(-self.r * self.period) * (U @ self.G))
+                return {"Pm": U, "P1": U, "V": V}
+            return {"U": U, "V": V}
+        m = p - self.niter + 2
+        Pm = state["Pm"] @ state["P1"]
+        V = list(state["V"]) + [math.exp(-self.r * self.period * m) * (Pm @ self.G)]
+        return {"Pm": Pm, "P1": state["P1"], "V": V}
+
+    def values(self, state: dict):
+        """V [nmat, d, nK] after the last stage."""
+        return self.torch.stack(state["V"])
+
+
+def host_solve_stages(L, x, strikes, r: float, period: float, nmat: int, niter: int, dt: float):
+    """``HostSolveFP64`` as a generator that yields once per stage, niter + nmat - 1 times:
+    None, and at the last stage V [nmat, d, nK]."""
+    hs = HostSolveFP64(L, x, strikes, r, period, nmat, niter, dt)
+    state = {}
+    for p in range(hs.stages):
+        state = hs.run(p, state)
+        yield hs.values(state) if p == hs.stages - 1 else None
 
 
 # ---------------------------------------------------------------------------------

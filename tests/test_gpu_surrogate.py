@@ -146,14 +146,15 @@ def test_tensor_core_inference_matches_the_fp64_oracle(cuda):
 
 @pytest.mark.timeout(900)
 def test_surrogate_meets_the_5bp_bar_on_accepted_quotes(cuda):
-    """A fixed, seeded training run (512 lattices, two members): on quotes of 64 held-out
-    lattices, the quotes the ensemble accepts (spread <= 5 bp) are within 5 bp of the
-    lattice's implied vol at the 99th percentile; the rest fall back to the lattice."""
+    """The seeded training run of the benchmark (2600 lattices, about 2^21 quotes after the
+    vega filter, four members, 40 epochs): on quotes of 128 held-out lattices, the quotes
+    the ensemble accepts (spread <= 5 bp) are within 5 bp of the lattice's implied vol at
+    the 99th percentile, and at most 10% of the quotes fall back to the lattice."""
     from oplib_b200.surrogate import Surrogate, lattice_quotes
-    train = lattice_quotes(512, seed=11, device=cuda)
-    test = lattice_quotes(64, seed=99, device=cuda)
-    s = Surrogate(members=2, device=cuda)
-    s.train(train, epochs=30, batch=4096, lr=2e-3)
+    train = lattice_quotes(2600, seed=2026, device=cuda)
+    test = lattice_quotes(128, seed=99, device=cuda)
+    s = Surrogate(members=4, device=cuda)
+    s.train(train, epochs=40, batch=4096, lr=2e-3)
     iv, spread = s.predict(test.feat, test.base)
     err = ((iv - test.iv).abs() * 1e4).cpu().numpy()
     acc = (spread * 1e4 <= 5.0).cpu().numpy()
@@ -163,4 +164,4 @@ def test_surrogate_meets_the_5bp_bar_on_accepted_quotes(cuda):
           f"{p99:.2f} bp, RMS {np.sqrt((err[acc] ** 2).mean()):.2f} bp, fallback {100 * fb:.2f}%, all-quote p99 "
           f"{np.quantile(err, 0.99):.2f} bp")
     assert p99 <= 5.0
-    assert fb <= 0.25
+    assert fb <= 0.10
