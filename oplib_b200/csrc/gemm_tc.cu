@@ -272,7 +272,9 @@ struct TcCfg {
     // FP32 output: each epilogue warp transposes 32 x 32 blocks through shared memory
     // (row stride 33 words) so that Cin loads and C stores are whole 128-byte lines
     static constexpr int OUT_BYTES = EPIMODE == 0 ? EPI_WARPS * 32 * 33 * 4 : 0;
-    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + OUT_BYTES;
+    // network layers: the tile's bias (and output weights) staged in shared memory once
+    static constexpr int VEC_BYTES = EPIMODE ? 2 * BN * 4 : 0;
+    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + OUT_BYTES + VEC_BYTES;
     static constexpr int THREADS = 32 * (EPI_WARPS + 2);    // + TMA producer warp + MMA warp
     static constexpr int TMEM_COLS = 2 * BN;                // two accumulators (ping-pong chunks)
     // K-blocks accumulated in TMEM per chunk: K = 128 for the split products (bounds the
@@ -467,6 +469,17 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                          "r"(Cfg::TMEM_COLS)
                          : "memory");
             asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
+    }
+    // network layers with one column tile (N == BN, every layer of the surrogate): the bias
+    // and output weights are read from shared memory in the epilogue, not from L1/L2 on the
+    // dependent path of every element
+    float *svec = reinterpret_cast<float *>(gbase + STAGES * Cfg::STAGE_BYTES + 256 + Cfg::OUT_BYTES);
+    const bool vec_smem = EPIMODE != 0 && p.N == BN;
+    if (vec_smem) {
+        for (int i = threadIdx.x; i < BN; i += blockDim.x) {
+            svec[i] = p.bias[i];
+            if (EPIMODE == 2) svec[BN + i] = p.w5[i];
         }
     }
     tc_fence_before();
@@ -720,10 +733,10 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             if constexpr (EPIMODE == 1) {
                 // network layer: BF16 GELU(alpha * acc + bias), 8 values per 16-byte store
                 __nv_bfloat16 *hrow = p.H + (long long)row * p.ldh + col0;
-                const float4 *b4 = reinterpret_cast<const float4 *>(p.bias + col0);
+                const float4 *b4 = reinterpret_cast<const float4 *>((vec_smem ? svec - n0 : p.bias) + col0);
 #pragma unroll
                 for (int j = 0; j < CPT; j += 8) {
-                    const float4 ba = __ldg(b4 + j / 4), bb = __ldg(b4 + j / 4 + 1);
+                    const float4 ba = b4[j / 4], bb = b4[j / 4 + 1];
                     const float bv[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
                     uint32_t pk[4];
 #pragma unroll
@@ -740,12 +753,12 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             if constexpr (EPIMODE == 2) {
                 // last hidden layer fused with the output layer: partial dot over this
                 // thread's columns of the BF16-rounded activations
-                const float4 *b4 = reinterpret_cast<const float4 *>(p.bias + col0);
-                const float4 *w4 = reinterpret_cast<const float4 *>(p.w5 + col0);
+                const float4 *b4 = reinterpret_cast<const float4 *>((vec_smem ? svec - n0 : p.bias) + col0);
+                const float4 *w4 = reinterpret_cast<const float4 *>((vec_smem ? svec + BN - n0 : p.w5) + col0);
                 float acc = 0.f;
 #pragma unroll
                 for (int j = 0; j < CPT; j += 4) {
-                    const float4 bv = __ldg(b4 + j / 4), wv = __ldg(w4 + j / 4);
+                    const float4 bv = b4[j / 4], wv = w4[j / 4];
                     const __nv_bfloat162 h01 = __floats2bfloat162_rn(gelu_as(fmaf(alpha, sum[j], bv.x)),
                                                                      gelu_as(fmaf(alpha, sum[j + 1], bv.y)));
                     const __nv_bfloat162 h23 = __floats2bfloat162_rn(gelu_as(fmaf(alpha, sum[j + 2], bv.z)),
