@@ -888,7 +888,7 @@ def run_batch(args):
                        "niter_range": [min(p.niter for p in prim["plans"]), max(p.niter for p in prim["plans"])]},
             "useful_tflops": round(useful / (ms * 1e-3) / 1e12, 1),
             "mma_tflops": round(3 * useful / (ms * 1e-3) / 1e12, 1),
-            "autotune_ms_level0": [round(x, 3) for x in prim["tune"]], "config_chosen": prim["cfg"],
+            "autotune_ms_chain_product": [round(x, 3) for x in prim["tune"]], "config_chosen": prim["cfg"],
             "sweep_ms_per_config": prim["sweep_ms"],
             "launches_per_sweep": prim["launches"], "plan_seconds": round(prim["plan_s"], 2),
             "max_abs_err_vs_fp64_sample": max(prim["errs"].values()), "sample_errs": prim["errs"],

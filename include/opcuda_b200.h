@@ -311,8 +311,8 @@ int opb_batch_execute(opb_batch_plan *plan, double *quotes);
  * one batched tensor-core product per date over all lattices; quotes: device [nlat][nK]
  * FP64 values at each lattice's y0 */
 int opb_batch_execute_bermudan(opb_batch_plan *plan, int put, int exercise, double barrier, double *quotes);
-/* times the level-0 launch for every configuration (ms_out: opb_batch_num_configs() floats)
- * and keeps the fastest */
+/* times the chain product (all lattices, dense operands) for every configuration
+ * (ms_out: opb_batch_num_configs() floats) and keeps the fastest */
 int opb_batch_autotune(opb_batch_plan *plan, int reps, float *ms_out, int *best_cfg);
 int opb_batch_launches(const opb_batch_plan *plan);
 
