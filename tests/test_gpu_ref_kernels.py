@@ -165,3 +165,111 @@ def test_sset_bit_exact_vs_reference_kernel(lib, ref, cuda):
         torch.cuda.synchronize()
         assert ref.ref_ssetone(theirs.data_ptr(), n, -2.5, i) == 0
     assert np.array_equal(_bits(mine), _bits(theirs))
+
+
+# ---- the reference's kernels that read device tables of 32-bit pointers (ssqmm, sgemm4,
+# sgemv4), run on memory placed below 4 GB of device address space
+
+@pytest.fixture(scope="module")
+def low(ref):
+    import ctypes as C
+    p = C.c_ulonglong()
+    size = 96 << 20
+    r = ref.ref_low_alloc(size, C.byref(p))
+    if r != 0:
+        pytest.skip(f"no device memory below 4 GB of address space here (ref_low_alloc: {r})")
+    assert 0 < p.value and p.value + size <= 1 << 32
+    yield ref_opcuda.LowArena(ref, p.value, size)
+    ref.ref_low_free_all()
+
+
+def _colmajor(a):
+    return np.asfortranarray(a).ravel(order="K").copy()
+
+
+def test_ssqmm_bit_exact_vs_reference_kernel(lib, ref, low, cuda):
+    """The FP32 squaring drop-in (64-bit pointer tables) against global_ssqmm (32-bit tables)
+    on the same column-major matrices, three products at d = 256, one of them a square."""
+    d, ni = 256, 3
+    rng = np.random.default_rng(4)
+    A = [rng.random((d, d)).astype(np.float32) / d for _ in range(ni)]
+    B = [A[0]] + [rng.random((d, d)).astype(np.float32) / d for _ in range(ni - 1)]
+    a_low = [low.put(_colmajor(a)) for a in A]
+    b_low = [low.put(_colmajor(b)) for b in B]
+    c_low = [low.alloc(d * d * 4) for _ in range(ni)]
+    tabs = [low.put(np.array(t, dtype=np.uint32)) for t in (a_low, b_low, c_low)]
+    assert ref.ref_ssqmm(d, ni, *tabs) == 0
+    mine = [torch.empty(d * d, device=cuda) for _ in range(ni)]
+    t64 = [torch.tensor(t, dtype=torch.int64, device=cuda) for t in (a_low, b_low, [m.data_ptr() for m in mine])]
+    assert lib.opcuda_ssqmm(d, ni, *[t.data_ptr() for t in t64]) == 0
+    torch.cuda.synchronize()
+    for i in range(ni):
+        theirs = low.get(c_low[i], d * d, np.float32)
+        assert np.array_equal(mine[i].cpu().numpy().view(np.uint32), theirs.view(np.uint32)), i
+        ref64 = A[i].astype(np.float64) @ B[i].astype(np.float64)
+        assert np.abs(theirs.reshape(d, d).T - ref64).max() < 1e-5 * np.abs(ref64).max()
+
+
+def test_sgemm4_bit_exact_vs_reference_kernel(lib, ref, low, cuda):
+    """Grouped column-major products through task tables: the drop-in's widened records
+    (64-bit pointers) against global_sgemm4's 9-word records (32-bit), same tiles."""
+    rng = np.random.default_rng(5)
+    shapes = [(128, 32, 64), (64, 48, 80), (192, 16, 128)]
+    mats, ref_tasks, my_tasks, outs = [], [], [], []
+    for i, (m, n, k) in enumerate(shapes):
+        A = rng.standard_normal((m, k)).astype(np.float32)
+        B = rng.standard_normal((k, n)).astype(np.float32)
+        a, b, c = low.put(_colmajor(A)), low.put(_colmajor(B)), low.alloc(m * n * 4)
+        dC = torch.zeros(m * n, device=cuda)
+        mats.append((m, n, c))
+        outs.append(dC)
+        for bx in range(m // 64):
+            for by in range(n // 16):
+                ref_tasks.append([i, bx, by, m, n, k, a, b, c])
+                my_tasks.append((i, bx, by, m, n, k, a, b, dC.data_ptr()))
+    recs = [low.put(np.array(t, dtype=np.uint32)) for t in ref_tasks]
+    assert ref.ref_sgemm4(len(recs), low.put(np.array(recs, dtype=np.uint32))) == 0
+    sz = lib.opb_sgemm4_task_size()
+    rec = np.zeros((len(my_tasks), sz // 8), dtype=np.int64)
+    for t, (i, bx, by, m, n, k, a, b, c) in enumerate(my_tasks):
+        rec[t, :3] = np.array([i, bx, by, m, n, k], dtype=np.int32).view(np.int64)
+        rec[t, 3:6] = [a, b, c]
+    drec = torch.from_numpy(rec.ravel()).to(cuda)
+    ptrs = torch.tensor([drec.data_ptr() + t * sz for t in range(len(my_tasks))], dtype=torch.int64, device=cuda)
+    assert lib.opcuda_sgemm4(len(my_tasks), ptrs.data_ptr()) == 0
+    torch.cuda.synchronize()
+    for (m, n, c), dC in zip(mats, outs):
+        assert np.array_equal(dC.cpu().numpy().view(np.uint32), low.get(c, m * n, np.float32).view(np.uint32))
+
+
+def test_sgemv4_bit_exact_vs_reference_kernel(lib, ref, low, cuda):
+    """Multi-vector induction through task tables (global_sgemv4's 64-row blocks against the
+    drop-in's 128-row blocks) on two matrices, with a sentinel in one column list."""
+    rng = np.random.default_rng(6)
+    d, nz = 256, 6
+    ref_tasks, my_tasks, zs = [], [], []
+    for i in range(2):
+        A = (rng.standard_normal((d, d)) / np.sqrt(d)).astype(np.float32)
+        Z0 = rng.standard_normal(2 * nz * d).astype(np.float32)
+        col0 = np.array([(c % nz) * d for c in range(16)], dtype=np.int32)
+        col1 = np.array([(nz + c % nz) * d for c in range(16)], dtype=np.int32)
+        if i == 1:
+            col1[9] = 2 * nz * d
+        a, z, c0, c1 = low.put(_colmajor(A)), low.put(Z0), low.put(col0), low.put(col1)
+        mz = torch.from_numpy(Z0.copy()).to(cuda)
+        zs.append((z, mz))
+        ref_tasks += [[i, bx, 0, d, nz, 16, a, z, c0, c1] for bx in range(d // 64)]
+        my_tasks += [(i, bx, 0, d, nz, 16, a, mz.data_ptr(), c0, c1) for bx in range(d // 128)]
+    recs = [low.put(np.array(t, dtype=np.uint32)) for t in ref_tasks]
+    assert ref.ref_sgemv4(len(recs), low.put(np.array(recs, dtype=np.uint32))) == 0
+    sz = lib.opb_sgemv4_task_size()
+    rec = np.zeros((len(my_tasks), sz // 8), dtype=np.int64)
+    for t, (i, bx, by, dd, z, ncol, a, zp, c0, c1) in enumerate(my_tasks):
+        rec[t, :3] = np.array([i, bx, by, dd, z, ncol], dtype=np.int32).view(np.int64)
+        rec[t, 3:7] = [a, zp, c0, c1]
+    drec = torch.from_numpy(rec.ravel()).to(cuda)
+    ptrs = torch.tensor([drec.data_ptr() + t * sz for t in range(len(my_tasks))], dtype=torch.int64, device=cuda)
+    assert lib.opcuda_sgemv4(len(my_tasks), ptrs.data_ptr()) == 0
+    torch.cuda.synchronize()
+    for z, mz in zs:
+        assert np.array_equal(mz.cpu().numpy().view(np.uint32), low.get(z, 2 * nz * d, np.float32).view(np.uint32))
