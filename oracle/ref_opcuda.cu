@@ -20,8 +20,9 @@
 //   global_sgsvg     (sgsvg.cu:40-209, launch sgsvg.cu:215-234)      nx*nr % 32 == 0, output
 //                    zeroed by the caller
 //   global_ssetall/ssetone (sset.cu:41-75)                           any n
-// Not wrapped: global_sglvg (a __syncthreads inside a divergent branch), global_ssqmm and
-// global_sgemm4/sgemv4 (device tables of 32-bit pointers), and the Monte Carlo kernels (their
+// Wrapped in ref_tables.cu instead: global_ssqmm and global_sgemm4/sgemv4, whose device
+// tables hold 32-bit pointers (run on memory below 4 GB, ref_lowmem.cu).  Not wrapped:
+// global_sglvg (a __syncthreads inside a divergent branch) and the Monte Carlo kernels (their
 // MT607 parameter file is not shipped).
 //
 // Every entry synchronises the device and returns the CUDA error code (0 = success).
