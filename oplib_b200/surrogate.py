@@ -8,10 +8,8 @@ device; the networks are trained by the library's own forward/backward/Adam kern
 ensemble spread exceeds the tolerance (5 bp of volatility by default) falls back to the
 lattice, which is also the reference for the surrogate's error.
 
-Two lattice families feed it: local-volatility lattices (``lattice_quotes``; kappa = rho =
-0, the level / skew / width of sigma(x)) and stochastic-volatility lattices
-(``sv_lattice_quotes``; sqrt(theta), skew 0, the vol of variance, kappa, rho), both solved by
-the batched split solver.
+Local-volatility rows fix kappa = rho = 0 (the stochastic-volatility columns are inputs
+of the network but constant in the local-volatility training family).
 
 The network predicts a correction to a closed-form baseline: the implied volatility is
 approximated by the root-mean-square local volatility sigma(x) over the log-spot path
@@ -131,80 +129,6 @@ def lattice_quotes(nlat: int, seed: int, device, mode: str = "fp16x3", batch: in
         lidx.append((torch.arange(nb, device=device) + b0).repeat_interleave(NMAT * 64)[ok])
         del bt
     return QuoteSet(torch.cat(feats), torch.cat(ivs), torch.cat(bases), torch.cat(lidx))
-
-
-SV_GRID = dict(nx=64, nv=16, x_lo=0.05, x_hi=5.0, v_lo=0.05, v_hi=1.0)  # the SV training family's lattice
-
-
-def sv_baseline_iv(v0, theta, kappa, T):
-    """The SV family's closed-form baseline: the root of the expected mean variance over
-    [0, T] of the variance process dV = kappa (theta - V) dt + ..., started at v0."""
-    kt = kappa * T
-    return torch.sqrt(theta + (v0 - theta) * (1.0 - torch.exp(-kt)) / kt)
-
-
-def sv_lattice_quotes(nlat: int, seed: int, device, mode: str = "fp16x3", batch: int = 256) -> QuoteSet:
-    """Quotes of seeded stochastic-volatility lattices, a reduced configuration-1 family (64
-    spot x 16 vol states, spot-variance correlation), as implied volatilities with the same
-    64 strikes exp(LM) and 16 maturities as ``lattice_quotes``: sqrt(theta) ~ U[0.1, 0.4]
-    (the level feature), the vol of variance xi ~ U[0.2, 1.0] (the width-or-vol-of-vol
-    feature), kappa ~ U[0.5, 4.0], rho ~ U[-0.9, 0.3], r ~ U[0, 0.05]; the skew feature is 0.
-    The quoted state is the spot node nearest 1 at the vol state nearest sqrt(theta), whose
-    variance starts the baseline."""
-    rng = np.random.default_rng(seed)
-    g = SV_GRID
-    strikes = np.exp(LM)
-    feats, ivs, bases, lidx = [], [], [], []
-    for b0 in range(0, nlat, batch):
-        nb = min(batch, nlat - b0)
-        level = rng.uniform(0.1, 0.4, nb)
-        xi = rng.uniform(0.2, 1.0, nb)
-        kappa = rng.uniform(0.5, 4.0, nb)
-        rho = rng.uniform(-0.9, 0.3, nb)
-        r = rng.uniform(0.0, 0.05, nb)
-        lats = [Lattice.stoch_vol(rate=float(r[i]), kappa=float(kappa[i]), theta=float(level[i]) ** 2, xi=float(xi[i]),
-                                  rho=float(rho[i]), device=device, **g) for i in range(nb)]
-        bt = Batch(lats, strikes, NMAT, PERIOD, 2.0 ** -14, mode=mode, autotune=False)
-        q = bt.execute()
-        T = torch.arange(1, NMAT + 1, dtype=torch.float64, device=device) * PERIOD
-        Kt = torch.as_tensor(strikes, dtype=torch.float64, device=device)
-        rr = torch.as_tensor(r, dtype=torch.float64, device=device)
-        s0 = torch.stack([lat.x[lat.y0] for lat in lats])
-        vols = g["v_lo"] * (g["v_hi"] / g["v_lo"]) ** (np.array([lat.y0 // g["nx"] for lat in lats]) / (g["nv"] - 1))
-        price = q.reshape(-1).contiguous()
-        Kf = Kt.repeat(nb * NMAT)
-        Tf = T.repeat_interleave(64).repeat(nb)
-        rf = rr.repeat_interleave(NMAT * 64)
-        s0f = s0.repeat_interleave(NMAT * 64).contiguous()
-        iv = torch.empty_like(price)
-        bind_stream(device)
-        call("opb_implied_vol", price.numel(), price.data_ptr(), Kf.data_ptr(), Tf.data_ptr(), rf.data_ptr(),
-             s0f.data_ptr(), iv.data_ptr())
-        lm = torch.log(Kf / s0f)
-        P = lambda a: torch.as_tensor(a, dtype=torch.float64, device=device).repeat_interleave(NMAT * 64)
-        lev, xif, kf, rhof, v0 = P(level), P(xi), P(kappa), P(rho), P(vols ** 2)
-        feat = torch.stack([lev, torch.zeros_like(lev), xif, kf, rhof, rf, lm, Tf], dim=1)
-        sq = iv * torch.sqrt(Tf)
-        d1 = (-lm + (rf + 0.5 * iv * iv) * Tf) / sq
-        vega = torch.exp(-0.5 * d1 * d1) / math.sqrt(2 * math.pi) * torch.sqrt(Tf)
-        ok = torch.isfinite(iv) & (vega * 5e-4 > 2e-7)
-        feats.append(feat[ok])
-        ivs.append(iv[ok])
-        bases.append(sv_baseline_iv(v0[ok], lev[ok] ** 2, kf[ok], Tf[ok]))
-        lidx.append((torch.arange(nb, device=device) + b0).repeat_interleave(NMAT * 64)[ok])
-        del bt
-    return QuoteSet(torch.cat(feats), torch.cat(ivs), torch.cat(bases), torch.cat(lidx))
-
-
-def join_quotes(*sets: QuoteSet) -> QuoteSet:
-    """One quote set from several (lattice indices kept distinct: each set's are offset past
-    the previous sets')."""
-    off, lidx = 0, []
-    for q in sets:
-        lidx.append(q.lattice + off)
-        off += int(q.lattice.max().item()) + 1 if q.lattice.numel() else 0
-    return QuoteSet(torch.cat([q.feat for q in sets]), torch.cat([q.iv for q in sets]),
-                    torch.cat([q.base for q in sets]), torch.cat(lidx))
 
 
 class Surrogate:
