@@ -1431,6 +1431,58 @@ def run_gemm(args):
             "peak_source": src}
 
 
+def run_price(args):
+    """The pricing / induction product alone at size d: V = P.G with P's two BF16 parts (d x d)
+    against 128 payoff columns (two parts), three split products as K-slices whose FP32
+    partials the caller sums (the form of the SV solve's 16 pricing products and of the
+    Bermudan induction).  Algorithmic bytes: P's parts read once (4 d^2), the payoff parts
+    (4 * 128 d) and the partials written (4 * 128 d per slice).  Beside it, a device copy
+    moving the same number of bytes (read + write), timed the same way, as the bandwidth a
+    transfer of this size reaches.  Inputs larger than L2 (151 MB)."""
+    import ctypes
+
+    import torch
+    from oplib_b200 import _lib
+    from oplib_b200.model import bind_stream
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    bind_stream(dev)
+    lib = _lib.load()
+    d, n = args.d, 128
+    Ph = torch.empty(d, d, dtype=torch.bfloat16, device=dev).uniform_(0, 2.0 / d)
+    Pl = (torch.empty(d, d, dtype=torch.float32, device=dev).uniform_(-1, 1) * 2.0 ** -9 / d).to(torch.bfloat16)
+    Gh = torch.empty(n, d, dtype=torch.bfloat16, device=dev).uniform_(0, 1)
+    Gl = (torch.empty(n, d, dtype=torch.float32, device=dev).uniform_(-1, 1) * 2.0 ** -9).to(torch.bfloat16)
+    used = ctypes.c_int(0)
+    C = torch.empty(4 * d * n, dtype=torch.float32, device=dev)
+    call = lambda: _lib.call("opb_gemm_bf16x3_ksliced", d, n, d, Ph.data_ptr(), Pl.data_ptr(), d, Gh.data_ptr(),
+                             Gl.data_ptr(), d, C.data_ptr(), n, 0, d * n, ctypes.byref(used))
+    stream = torch.cuda.current_stream(dev)
+    res = {}
+    for _ in range(args.warmup):
+        call()
+    ms = _time(call, args.steps, stream, torch)
+    nbytes = 4.0 * d * d + 4.0 * n * d + 4.0 * n * d * used.value
+    src_b = torch.empty(int(nbytes) // 2, dtype=torch.uint8, device=dev)
+    dst_b = torch.empty_like(src_b)
+    for _ in range(args.warmup):
+        dst_b.copy_(src_b)
+    ms_copy = _time(lambda: dst_b.copy_(src_b), args.steps, stream, torch)
+    hbm, _, _, src = _peaks()
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    gbs_copy = 2 * src_b.numel() / (ms_copy * 1e-3) / 1e9
+    return {"metric": "pricing product GB/s (P read once)", "value": round(gbs, 1), "unit": "GB/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3",
+            "data": "synthetic (inputs larger than L2)",
+            "config": {"workload": f"V = P.G, d={d}, 128 columns, {used.value} K-slices"},
+            "frac_of_hbm": round(gbs / hbm, 4), "peak_source": src,
+            "copy_same_bytes": {"GB/s": round(gbs_copy, 1), "us": round(ms_copy * 1e3, 2),
+                                "frac_of_hbm": round(gbs_copy / hbm, 4)},
+            "frac_of_copy_same_bytes": round(gbs / gbs_copy, 4),
+            "us_per_launch": round(ms * 1e3, 2), "algorithmic_bytes": nbytes}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1447,7 +1499,7 @@ def main():
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--workload", default="sv",
                     choices=["sv", "lv", "mc", "gemm", "gemv", "renorm", "batch", "surrogate", "calibrate",
-                             "refbench", "bermudan"],
+                             "refbench", "bermudan", "price"],
                     help="sv = the headline SV lattice solve; the others are secondary measurements")
     ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
     ap.add_argument("--mc-steps", type=int, default=504,
@@ -1471,7 +1523,8 @@ def main():
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "gemv": run_gemv, "renorm": run_renorm,
               "batch": run_batch_sharded if launched else run_batch, "surrogate": run_surrogate,
-              "calibrate": run_calibrate, "refbench": run_refbench, "bermudan": run_bermudan}[args.workload]
+              "calibrate": run_calibrate, "refbench": run_refbench, "bermudan": run_bermudan,
+              "price": run_price}[args.workload]
         line = fn(args)
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps(line))

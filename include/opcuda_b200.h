@@ -184,6 +184,15 @@ int opb_gemm_bf16x3_nparts(int M, int N);
 int opb_gemm_bf16x3_kn(int M, int N, int K, const opb_bf16 *Ahi, const opb_bf16 *Alo, long long lda,
                        const opb_bf16 *Bhi, const opb_bf16 *Blo, long long ldb, float alpha, const float *Cin,
                        float beta, float *C, long long ldc, double *rowsum);
+/* new: the product of a skinny B (N <= 128: payoff or option-value columns, B N x K row-major)
+ * as ksplit K-slices, slice s writing its FP32 partial product to C + s * c_slice (c_slice >=
+ * M * ldc) for the caller to sum; ksplit = 0 picks the count that brings the tiles to about
+ * one per SM (at most 4), as the lattice solve's pricing and induction products do, and
+ * returns it through ksplit_used (optional).  The memory-bound form of the product: A is read
+ * from memory once. */
+int opb_gemm_bf16x3_ksliced(int M, int N, int K, const opb_bf16 *Ahi, const opb_bf16 *Alo, long long lda,
+                            const opb_bf16 *Bhi, const opb_bf16 *Blo, long long ldb, float *C, long long ldc,
+                            int ksplit, long long c_slice, int *ksplit_used);
 /* new (tuning): force the output tile width (64, 128, 256) of single products; 0 = automatic */
 int opb_set_tile_n(int bn);
 /* new: tuning knob, K depth of a pipeline stage of 256-wide tiles: 64 (default) or 32 (twice

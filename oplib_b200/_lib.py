@@ -92,6 +92,7 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_gemm_bf16x3_kn": (i32, [i32, i32, i32, vp, vp, i64, vp, vp, i64, f32, vp, f32, vp, i64, vp]),
     "opb_gemm_f16x3_kn": (i32, [i32, i32, i32, vp, vp, i64, vp, vp, i64, f32, vp, f32, vp, i64, vp]),
     "opb_set_tile_n": (i32, [i32]),
+    "opb_gemm_bf16x3_ksliced": (i32, [i32, i32, i32, vp, vp, i64, vp, vp, i64, vp, i64, i32, i64, C.POINTER(i32)]),
     "opb_gemm_f16x3": (i32, [i32, i32, i32, vp, vp, i64, vp, vp, i64, f32, vp, f32, vp, i64, vp]),
     "opb_tc_error": (i32, []),
     "opb_batch_num_configs": (i32, []),

@@ -944,15 +944,32 @@ static int tile_for(int M, int N, int ksplit = 1) {
     return bn;
 }
 
-// K-slices (at most 4) that bring a small-N product's widest tiles up to about one per SM.
+// K-slices (at most 4, dividing K / 64) for a small-N product's widest tiles: the count
+// whose items fill the SMs' waves best (items / (waves x SMs)); among equal fills, one that
+// gives every SM an item, then the fewest slices.  A CTA streams A at a bounded rate
+// (about 20-28 GB/s of BF16 parts through its 3-stage ring), so an idle SM is bandwidth lost:
+// at d = 12288 one slice leaves 52 of 148 SMs idle (0.30 of HBM), three fill them.
 int tc_gemm_split_for(int M, int N, int K) {
     const int bn = tc_gemm_tile_n(N);
     if (!bn || M % TC_BM) return 1;
     const long long tiles = (long long)(M / TC_BM) * (N / bn);
-    int sp = (int)(num_sms() / (tiles > 0 ? tiles : 1));
-    sp = sp < 1 ? 1 : (sp > 4 ? 4 : sp);
-    while (sp > 1 && (K / TC_BK) % sp) sp--;
-    return sp;
+    const long long sms = num_sms();
+    int best = 1;
+    double best_fill = -1.0;
+    bool best_all = false;
+    for (int sp = 1; sp <= 4; sp++) {
+        if ((K / TC_BK) % sp) continue;
+        const long long items = tiles * sp;
+        const long long waves = (items + sms - 1) / sms;
+        const double fill = (double)items / (double)(waves * sms);
+        const bool all = items >= sms;
+        if (fill > best_fill + 0.02 || (fill > best_fill - 0.02 && all && !best_all)) {
+            best = sp;
+            best_fill = fill;
+            best_all = all;
+        }
+    }
+    return best;
 }
 
 // Row-sum partials: one per 128-column group (64 for the 64-wide tile).
@@ -1228,6 +1245,8 @@ int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, 
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
     int c = tc_gemm_check(a);
     if (c != OPB_OK) return c;
+    // K-sliced products (pricing, induction) stay on one CTA per tile: on CTA pairs, which
+    // share the B tile and so hold four stages of A instead of three, they ran 6% slower
     const bool pair = g_pair && a.M % (2 * TC_BM) == 0 && a.ksplit <= 1;
     if (a.b_kn) {  // MN-major B (K x N): BK = 64 only
         switch (tile_for(a.M, a.N, a.ksplit) * 2 + (a.f16 ? 1 : 0)) {
@@ -1316,6 +1335,24 @@ OPB_API int opb_gemm_f16x3_kn(int M, int N, int K, const uint16_t *Ahi, const ui
 }
 
 OPB_API int opb_gemm_bf16x3_nparts(int M, int N) { return tc_gemm_nparts(M, N); }
+
+// The product of a skinny B (N <= 128 columns: payoffs, option values) as ksplit K-slices:
+// slice s (of K / ksplit) writes its FP32 partial product to C + s * c_slice (c_slice >=
+// M * ldc), for the caller to sum.  B is N x K row-major (K-major).  ksplit = 0 picks the
+// slice count that brings the tiles to about one per SM (at most 4), as the lattice solve's
+// pricing products do; the count used is returned through ksplit_used (optional).
+OPB_API int opb_gemm_bf16x3_ksliced(int M, int N, int K, const __nv_bfloat16 *Ahi, const __nv_bfloat16 *Alo,
+                                    long long lda, const __nv_bfloat16 *Bhi, const __nv_bfloat16 *Blo, long long ldb,
+                                    float *C, long long ldc, int ksplit, long long c_slice, int *ksplit_used) {
+    OPB_REQUIRE(ksplit >= 0 && ksplit <= 64 && N > 0 && N <= 128, OPB_E_ARG);
+    TcGemmArgs a{};
+    a.M = M; a.N = N; a.K = K; a.Ahi = Ahi; a.Alo = Alo; a.Bhi = Bhi; a.Blo = Blo; a.lda = lda; a.ldb = ldb;
+    a.C = C; a.ldc = ldc; a.alpha = 1.f; a.beta = 0.f;
+    a.ksplit = ksplit > 0 ? ksplit : tc_gemm_split_for(M, N, K);
+    a.c_slice = c_slice;
+    if (ksplit_used) *ksplit_used = a.ksplit;
+    return set_status(launch_tc_gemm(a, stream()));
+}
 
 // Tuning knob: force the output tile width (64, 128 or 256) of single products; 0 = automatic.
 OPB_API int opb_set_tile_n(int bn) {

@@ -259,6 +259,53 @@ def test_bf16x3_gemm_in_place(cuda):
     assert np.abs(X.cpu().numpy() - ref).max() < 1e-7
 
 
+@pytest.mark.parametrize("M,N,K,ksplit", [(6144, 128, 6144, 0), (1024, 64, 2048, 4), (512, 128, 1024, 2),
+                                          (384, 128, 512, 2)])
+def test_ksliced_product_matches_fp64(cuda, M, N, K, ksplit):
+    """opb_gemm_bf16x3_ksliced: the K-slices' partials sum to the FP64 product of the same
+    parts (each slice within the tensor cores' FP32 bound over its own K range), and every
+    slice is written."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(M + N + K)
+    A = (rng.random((M, K)) * (2.0 / K)).astype(np.float32)
+    B = rng.random((N, K)).astype(np.float32)
+    Ah, Al, ah, al = _split_dev(A, cuda)
+    Bh, Bl, bh, bl = _split_dev(B, cuda)
+    used = C.c_int(0)
+    Cs = torch.full((4 * M * N,), float("nan"), dtype=torch.float32, device=cuda)
+    assert lib.opb_gemm_bf16x3_ksliced(M, N, K, Ah.data_ptr(), Al.data_ptr(), K, Bh.data_ptr(), Bl.data_ptr(), K,
+                                       Cs.data_ptr(), N, ksplit, M * N, C.byref(used)) == 0
+    torch.cuda.synchronize()
+    assert lib.opb_tc_error() == 0
+    assert used.value == (ksplit if ksplit else lib_split_expected(M, N, K))
+    out = Cs[: used.value * M * N].cpu().numpy().reshape(used.value, M, N)
+    assert np.isfinite(out).all()
+    got = out.astype(np.float64).sum(axis=0)
+    ref = ah @ bh.T + ah @ bl.T + al @ bh.T
+    scale = (np.abs(ah) + np.abs(al)) @ (np.abs(bh) + np.abs(bl)).T
+    bound = (3 * K / 16 + 8) * 2.0 ** -24
+    assert np.all(np.abs(got - ref) <= bound * scale + 1e-30)
+
+
+def lib_split_expected(M, N, K):
+    """The automatic slice count: at most 4, dividing K / 64, the one whose items (tiles x
+    slices) fill the SMs' waves best; among fills within 0.02, one that reaches every SM, then
+    the fewest slices."""
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    tiles = (M // 128) * max(1, N // 128)
+    best, best_fill, best_all = 1, -1.0, False
+    for sp in range(1, 5):
+        if (K // 64) % sp:
+            continue
+        items = tiles * sp
+        fill = items / (-(-items // sms) * sms)
+        every = items >= sms
+        if fill > best_fill + 0.02 or (fill > best_fill - 0.02 and every and not best_all):
+            best, best_fill, best_all = sp, fill, every
+    return best
+
+
 def test_bf16x3_rejects_unsupported_shapes(cuda):
     from oplib_b200 import _lib
     lib = _lib.load()
