@@ -1431,6 +1431,43 @@ def run_gemm(args):
             "peak_source": src}
 
 
+def run_solve(args):
+    """One SV lattice solve of a chosen grid (--sv-nx x --sv-nv states, config 1's parameters
+    otherwise: 16 maturities x 128 strikes), CUDA-graph replay, in --mode; with
+    --fused-max-d the row normalisation's form (fused into the epilogues up to that many
+    states, a kernel after every product above)."""
+    import torch
+    from oplib_b200 import _lib
+    from oplib_b200.model import MODES, Lattice, bind_stream
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    bind_stream(dev)
+    stream = torch.cuda.current_stream(dev)
+    sv = dict(SV, nx=args.sv_nx, nv=args.sv_nv)
+    lat = Lattice.stoch_vol(**sv, device=dev)
+    plan = lat.plan(PERIOD, DT0)
+    strikes = torch.tensor(STRIKES, dtype=torch.float64, device=dev)
+    mode = MODES[args.mode]
+    ws = lat.workspace(NK, mode)
+    q = torch.empty(NMAT, NK, dtype=torch.float64, device=dev)
+    desc = lat.desc(plan, PERIOD, NMAT, strikes)
+
+    def step():
+        _lib.call("opb_lattice_solve", C.byref(desc), mode, ws.data_ptr(), ws.numel(), q.data_ptr(), None)
+    for _ in range(args.warmup):
+        step()
+    g = _graph(step, dev, torch)
+    g.replay()
+    ms = _time(g.replay, args.steps, stream, torch)
+    return {"metric": "priced quotes/sec, SV lattice solve (CUDA-graph replay)",
+            "value": round(NMAT * NK / (ms * 1e-3), 1), "unit": "quotes/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.mode, "data": "synthetic",
+            "config": {"workload": f"SV lattice {args.sv_nv} vol x {args.sv_nx} spot = {lat.d} states, "
+                                   f"{plan.niter} squarings + {NMAT - 1} chains, {NK} strikes x {NMAT} maturities",
+                       "fused_max_d": args.fused_max_d}}
+
+
 def run_price(args):
     """The pricing / induction product alone at size d: V = P.G with P's two BF16 parts (d x d)
     against 128 payoff columns (two parts), three split products as K-slices whose FP32
@@ -1499,16 +1536,24 @@ def main():
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--workload", default="sv",
                     choices=["sv", "lv", "mc", "gemm", "gemv", "renorm", "batch", "surrogate", "calibrate",
-                             "refbench", "bermudan", "price"],
+                             "refbench", "bermudan", "price", "solve"],
                     help="sv = the headline SV lattice solve; the others are secondary measurements")
     ap.add_argument("--d", type=int, default=4096, help="matrix size for --workload gemm")
     ap.add_argument("--mc-steps", type=int, default=504,
                     help="--workload mc: steps per path (504 = two years of daily steps)")
+    ap.add_argument("--sv-nx", type=int, default=128, help="--workload solve: spot states")
+    ap.add_argument("--sv-nv", type=int, default=48, help="--workload solve: vol states")
+    ap.add_argument("--fused-max-d", type=int, default=-1,
+                    help="largest single lattice whose row normalisation is fused into the products' epilogues "
+                         "(-1: the library's default)")
     ap.add_argument("--cta-pair", type=int, default=1, choices=[0, 1],
                     help="--workload gemm: 2-CTA pair kernel (1, the default) or one CTA per tile (0)")
     args = ap.parse_args()
     if args.nlat is None:
         args.nlat = 64 if args.workload == "calibrate" else 512
+    if args.fused_max_d >= 0 and args.impl == "b200":
+        from oplib_b200 import _lib
+        _lib.call("opb_set_fused_normalisation", args.fused_max_d)
     if args.workload != "sv" and args.impl == "b200":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         launched = "LOCAL_RANK" in os.environ  # under torchrun (any world size)
@@ -1524,7 +1569,7 @@ def main():
         fn = {"lv": run_lv, "mc": run_mc, "gemm": run_gemm, "gemv": run_gemv, "renorm": run_renorm,
               "batch": run_batch_sharded if launched else run_batch, "surrogate": run_surrogate,
               "calibrate": run_calibrate, "refbench": run_refbench, "bermudan": run_bermudan,
-              "price": run_price}[args.workload]
+              "price": run_price, "solve": run_solve}[args.workload]
         line = fn(args)
         if int(os.environ.get("RANK", "0")) == 0:
             print(json.dumps(line))

@@ -282,6 +282,14 @@ int opb_set_lolo_levels(int n);
  * whose products are exact zeros; 0: every squaring runs the full product.  Results are
  * bit-identical either way */
 int opb_set_band_skip(int on);
+/* new: the split-mode solves defer each product's FP64 row normalisation into the next
+ * product's epilogue, which also writes that product's 16-bit operand parts, so no
+ * renormalisation kernel runs between products (squarings: the next level applies
+ * D [E'.E' - S E' - E' S + S^2] + 2 D (E' - S) with D = diag(1/(1+s)), S = diag(s), the D
+ * between the factors left out; chain products: the row scaling, exact).  The batched
+ * sweep always does; a single-lattice solve does up to max_d states (default 0: a
+ * renormalisation kernel after every product, which costs about the same for one lattice). */
+int opb_set_fused_normalisation(int max_d);
 
 /* ------------------------------------------------------------------ batched lattices */
 typedef struct opb_batch_desc {

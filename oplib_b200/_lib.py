@@ -113,6 +113,7 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_chain_workspace_size": (ull, [i32]),
     "opb_chain_kernels": (i32, [i32, i32, vp, vp, vp, ull]),
     "opb_set_band_skip": (i32, [i32]),
+    "opb_set_fused_normalisation": (i32, [i32]),
     # batched lattices
     "opb_batch_workspace_size": (ull, [vp, i32]),
     "opb_batch_plan_create": (i32, [vp, i32, vp, ull, vp]),

@@ -5,15 +5,17 @@
 // batches every interval that still needs squaring at level r into one call
 // (oplib/opmodel/models/CModel Common.cs:508-545, CModel Device.cs:216-228).  Here every
 // squaring level of all lattices is ONE persistent tcgen05 launch over a work list of
-// (lattice, m-tile, n-tile) items, followed by ONE batched FP64 renormalisation launch;
-// chaining and pricing are batched the same way.  The plan (tables, tensor maps, work
+// (lattice, m-tile, n-tile) items.  Its epilogue writes the next level's 16-bit parts and
+// applies the previous level's deferred FP64 row normalisation, so between levels only a
+// small row-fix launch runs (plus a renormalisation of the lattices whose last level it
+// was); chaining and pricing are batched the same way.  The plan (tables, tensor maps, work
 // lists) is built once on the host and uploaded into the caller's workspace; execute()
-// then issues ~4 launches per level with no host synchronisation and no allocation, so a
+// then issues 2-4 launches per level with no host synchronisation and no allocation, so a
 // whole sweep can be captured in a CUDA graph and replayed.
 //
-// Tile shape and work order are chosen by opb_batch_autotune, which times the level-0
-// launch for each candidate (BN 128 or 64; items ordered longest-K first or by lattice)
-// with CUDA events and keeps the fastest.
+// Tile shape and work order are chosen by opb_batch_autotune, which times the chain
+// product for each candidate (tile width 64, 128, 256 or 256 on CTA pairs; items ordered
+// longest-K first or by lattice) with CUDA events and keeps the fastest.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -93,12 +95,17 @@ struct opb_batch_plan {
     double period = 0.0;
     // device tables
     opb::BatchLattice *lats = nullptr;
-    opb::TcProblem *sq = nullptr, *chain = nullptr, *price = nullptr;
-    opb::RenormProblem *rn_sq = nullptr, *rn_chain = nullptr;
+    // the squaring and chain problems and maps come in two sets, [0] reading the parts in
+    // the A buffers and [1] those in the other buffer (squarings: B; chains: the pair carved
+    // from the FP32 chain buffer), each product writing its output's parts into the other
+    opb::TcProblem *sq[2] = {nullptr, nullptr}, *chain[2] = {nullptr, nullptr}, *price = nullptr;
+    opb::RenormProblem *rn_sq = nullptr;
     // 4 maps per lattice (Ahi, Alo, Bhi, Blo), the same for every tile width: squaring (B =
-    // E's row-major A parts, MN-major), chain (B = P1's row-major parts), pricing (K-major
-    // payoff parts)
-    CUtensorMap *maps_sq = nullptr, *maps_ch = nullptr, *maps_price = nullptr;
+    // E's row-major parts, MN-major), chain (B = P1's row-major parts), pricing (K-major
+    // payoff parts), per part set
+    CUtensorMap *maps_sq[2] = {nullptr, nullptr}, *maps_ch[2] = {nullptr, nullptr}, *maps_price[2] = {nullptr, nullptr};
+    __nv_bfloat16 *B_hi = nullptr, *B_lo = nullptr;  // the B part buffers of all lattices
+    size_t B_bytes = 0;                                 // of each
     // backward induction: A = P1's parts, B = the option values' parts read d x ldk row-major
     CUtensorMap *maps_berm = nullptr;
     uint32_t *work = nullptr;
@@ -110,8 +117,9 @@ struct opb_batch_plan {
     std::vector<ListRef> gemm_level_rest[NCFG];  // pair configurations: the 128 x 256 items
     ListRef gemm_chain_rest[NCFG];
     ListRef gemm_price;
-    std::vector<ListRef> rn_level;
-    ListRef rn_init, rn_chain_list;
+    std::vector<ListRef> rn_level;     // per level: the lattices whose last level it is (P1)
+    std::vector<char> level_inter;     // per level: some lattice squares on after it
+    ListRef rn_init;
     // FP32 path
     std::vector<LatticeDescMirror> fp32_desc;
     std::vector<char *> fp32_ws;
@@ -188,14 +196,13 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     }
     const int ldk = 64;
     auto lats = c.take<opb::BatchLattice>(n);
-    auto sq = c.take<opb::TcProblem>(n);
-    auto ch = c.take<opb::TcProblem>(n);
+    auto sq = c.take<opb::TcProblem>(2 * (size_t)n);
+    auto ch = c.take<opb::TcProblem>(2 * (size_t)n);
     auto pr = c.take<opb::TcProblem>(n);
     auto rs = c.take<opb::RenormProblem>(n);
-    auto rc = c.take<opb::RenormProblem>(n);
-    auto msq = c.take<CUtensorMap>(4 * (size_t)n);
-    auto mch = c.take<CUtensorMap>(4 * (size_t)n);
-    auto mp = c.take<CUtensorMap>(4 * (size_t)n);
+    auto msq = c.take<CUtensorMap>(8 * (size_t)n);
+    auto mch = c.take<CUtensorMap>(8 * (size_t)n);
+    auto mp = c.take<CUtensorMap>(8 * (size_t)n);
     size_t Etot = 0;
     for (int i = 0; i < n; i++) Etot += (size_t)b->d[i] * b->d[i];
     float *E = c.take<float>(Etot);
@@ -271,15 +278,13 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     for (int i : lpt)
         for (int a = 0; a < b->d[i] / 128; a++) W.push_back(((uint32_t)i << 16) | ((uint32_t)a << 8));
     gpr.n = (int)(W.size() - gpr.off);
-    auto rn_list = [&](int level, int kind) {  // kind: 0 init split, 1 squaring level, 2 chain
+    auto rn_list = [&](int level, int kind) {  // kind: 0 init split, 1 the lattices ending at `level`
         ListRef r{W.size(), 0};
         for (int i : lpt) {
-            int mode_i;
-            if (kind == 0) mode_i = 0;
-            else if (kind == 2) mode_i = 2;
-            else {
-                if (b->niter[i] <= level) continue;
-                mode_i = (level == b->niter[i] - 1) ? 1 : 0;
+            int mode_i = 0;
+            if (kind == 1) {
+                if (b->niter[i] != level + 1) continue;
+                mode_i = 1;
             }
             const int t = b->d[i] / 64, nch = opb::renorm_chunks(b->d[i]);
             for (int a = 0; a < t; a++)
@@ -291,8 +296,11 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     };
     ListRef rinit = rn_list(0, 0);
     std::vector<ListRef> rl;
-    for (int lv = 0; lv < maxn; lv++) rl.push_back(rn_list(lv, 1));
-    ListRef rch = rn_list(0, 2);
+    std::vector<char> inter(maxn, 0);
+    for (int lv = 0; lv < maxn; lv++) {
+        rl.push_back(rn_list(lv, 1));
+        for (int i = 0; i < n; i++) inter[lv] |= b->niter[i] > lv + 1 ? 1 : 0;
+    }
     uint32_t *work = c.take<uint32_t>(W.size());
     size_t total = c.used + 256;
     if (!P) return total;
@@ -301,8 +309,15 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
     P->nlat = n; P->nmat = b->nmat; P->nK = b->nK; P->ldk = ldk; P->maxn = maxn;
     P->total_rows = off[n]; P->ell_width = b->ell_width; P->cols = b->gen_cols; P->vals = b->gen_vals;
     P->x = b->x; P->strikes = b->strikes; P->period = b->period;
-    P->lats = lats; P->sq = sq; P->chain = ch; P->price = pr; P->rn_sq = rs; P->rn_chain = rc;
-    P->maps_sq = msq; P->maps_ch = mch; P->maps_price = mp; P->maps_berm = mbm; P->work = work;
+    P->lats = lats; P->sq[0] = sq; P->sq[1] = sq + n; P->chain[0] = ch; P->chain[1] = ch + n; P->price = pr;
+    P->rn_sq = rs;
+    for (int k = 0; k < 2; k++) {
+        P->maps_sq[k] = msq + 4 * (size_t)n * k;
+        P->maps_ch[k] = mch + 4 * (size_t)n * k;
+        P->maps_price[k] = mp + 4 * (size_t)n * k;
+    }
+    P->maps_berm = mbm; P->work = work;
+    P->B_hi = Bh; P->B_lo = Bl; P->B_bytes = sizeof(__nv_bfloat16) * Etot;
     P->E_base = E; P->E_bytes = Etot * sizeof(float);
     for (int cfg = 0; cfg < NCFG; cfg++) {
         P->gemm_level[cfg] = gl[cfg];
@@ -310,7 +325,7 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
         P->gemm_level_rest[cfg] = glr[cfg];
         P->gemm_chain_rest[cfg] = gchr[cfg];
     }
-    P->gemm_price = gpr; P->rn_level = rl; P->rn_init = rinit; P->rn_chain_list = rch;
+    P->gemm_price = gpr; P->rn_level = rl; P->level_inter = inter; P->rn_init = rinit;
     if (work_out) *work_out = W;
     return total;
 }
@@ -383,14 +398,14 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     }
     // host images of the device tables
     std::vector<opb::BatchLattice> lats(n);
-    std::vector<opb::TcProblem> sq(n), ch(n), pr(n);
-    std::vector<opb::RenormProblem> rs(n), rc(n);
-    std::vector<CUtensorMap> msq(4 * (size_t)n), mch(4 * (size_t)n), mp(4 * (size_t)n), mbm(4 * (size_t)n);
+    std::vector<opb::TcProblem> sq(2 * (size_t)n), ch(2 * (size_t)n), pr(n);
+    std::vector<opb::RenormProblem> rs(n);
+    std::vector<CUtensorMap> msq(8 * (size_t)n), mch(8 * (size_t)n), mp(8 * (size_t)n), mbm(4 * (size_t)n);
     // recompute buffer pointers exactly as layout() carved them
     Carve cv{base, 0};
-    cv.take<opb::BatchLattice>(n); cv.take<opb::TcProblem>(n); cv.take<opb::TcProblem>(n); cv.take<opb::TcProblem>(n);
-    cv.take<opb::RenormProblem>(n); cv.take<opb::RenormProblem>(n);
-    cv.take<CUtensorMap>(4 * (size_t)n); cv.take<CUtensorMap>(4 * (size_t)n); cv.take<CUtensorMap>(4 * (size_t)n);
+    cv.take<opb::BatchLattice>(n); cv.take<opb::TcProblem>(2 * (size_t)n); cv.take<opb::TcProblem>(2 * (size_t)n);
+    cv.take<opb::TcProblem>(n); cv.take<opb::RenormProblem>(n);
+    cv.take<CUtensorMap>(8 * (size_t)n); cv.take<CUtensorMap>(8 * (size_t)n); cv.take<CUtensorMap>(8 * (size_t)n);
     size_t Etot = 0;
     for (int i = 0; i < n; i++) Etot += (size_t)b->d[i] * b->d[i];
     float *E = cv.take<float>(Etot), *Pa = cv.take<float>(Etot);
@@ -414,6 +429,7 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     int rc_status = OPB_OK;
     for (int i = 0; i < n && rc_status == OPB_OK; i++) {
         const int d = b->d[i];
+        const size_t dd = (size_t)d * d;
         opb::BatchLattice &L = lats[i];
         L.d = d; L.y0 = b->y0[i]; L.row_off = ro; L.dt = b->dt[i]; L.rate = b->rate[i]; L.period = b->period;
         L.E = E + eo; L.Pa = Pa + eo; L.V = V + (size_t)ro * P->ldk;
@@ -421,25 +437,36 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
         L.gscale = gsc + i;
         L.Vd = vd + (size_t)ro * P->ldk;
         double *pi = part + po;
-        // squaring reads E as the previous level's GEMM left it, renormalised on the fly by
-        // the row fixes of the previous level's (or the initial split's) renormalisation
-        sq[i] = opb::TcProblem{d, d, d, bands[i], L.E, L.E, pi, d, un2, 2.f, fix + ro};
-        ch[i] = opb::TcProblem{d, d, d, 0, L.Pa, nullptr, pi, d, un2, 0.f, nullptr};
+        L.niter = b->niter[i]; L.partial = pi; L.fix = fix + ro;
+        // part sets: squarings between A and B, chains between A and a pair carved from the
+        // FP32 chain buffer (2 d^2 BF16 values in its d^2 floats)
+        __nv_bfloat16 *sh[2] = {Ah + eo, Bh + eo}, *sl[2] = {Al + eo, Bl + eo};
+        __nv_bfloat16 *c2 = reinterpret_cast<__nv_bfloat16 *>(Pa + eo);
+        __nv_bfloat16 *chh[2] = {Ah + eo, c2}, *chl[2] = {Al + eo, c2 + dd};
+        for (int k = 0; k < 2 && rc_status == OPB_OK; k++) {
+            // squaring: E' = 2E + E.E in place of E (as the previous level's GEMM left it, its
+            // normalisation deferred into this epilogue through the row fixes), the output's
+            // parts into the other set
+            sq[k * n + i] = opb::TcProblem{d, d, d, bands[i], L.E, L.E, pi, d, un2, 2.f, fix + ro, sh[k ^ 1],
+                                           sl[k ^ 1]};
+            // chain: parts only, P_{m-1}'s row fix applied in the epilogue
+            ch[k * n + i] = opb::TcProblem{d, d, d, 0, nullptr, nullptr, pi, d, un2, 0.f, fix + ro, chh[k ^ 1],
+                                           chl[k ^ 1]};
+            rc_status = opb::tc_make_maps(&msq[4 * ((size_t)k * n + i)], sh[k], sl[k], d, d, sh[k], sl[k], d, d, d,
+                                          64, f16, 1);
+            if (rc_status == OPB_OK)
+                rc_status = opb::tc_make_maps(&mch[4 * ((size_t)k * n + i)], chh[k], chl[k], d, d, Bh + eo, Bl + eo, d,
+                                              d, d, 64, f16, 1);
+            if (rc_status == OPB_OK)
+                rc_status = opb::tc_make_maps(&mp[4 * ((size_t)k * n + i)], chh[k], chl[k], d, d, L.GThi, L.GTlo,
+                                              P->ldk, d, d, 64, f16);
+        }
         pr[i] = opb::TcProblem{d, P->ldk, d, 0, L.V, nullptr, nullptr, P->ldk, un1, 0.f, nullptr};
         rs[i] = opb::RenormProblem{d, 0, L.E, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo, fix + ro};
-        rc[i] = opb::RenormProblem{d, 0, L.Pa, pi, Ah + eo, Al + eo, Bh + eo, Bl + eo, nullptr};
-        rc_status = opb::tc_make_maps(&msq[4 * (size_t)i], Ah + eo, Al + eo, d, d, Ah + eo, Al + eo, d, d, d, 64,
-                                      f16, 1);
-        if (rc_status == OPB_OK)
-            rc_status = opb::tc_make_maps(&mch[4 * (size_t)i], Ah + eo, Al + eo, d, d, Bh + eo, Bl + eo, d, d, d, 64,
-                                          f16, 1);
-        if (rc_status == OPB_OK)
-            rc_status =
-                opb::tc_make_maps(&mp[4 * (size_t)i], Ah + eo, Al + eo, d, d, L.GThi, L.GTlo, P->ldk, d, d, 64, f16);
         if (rc_status == OPB_OK)  // the same buffers, the value parts read d x ldk row-major
             rc_status = opb::tc_make_maps(&mbm[4 * (size_t)i], Ah + eo, Al + eo, d, d, L.GThi, L.GTlo, P->ldk,
                                           P->ldk, d, 64, f16, 1);
-        eo += (size_t)d * d;
+        eo += dd;
         po += (size_t)(d / 64) * d;
         ro += d;
     }
@@ -455,14 +482,13 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     };
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = up(P->lats, lats.data(), sizeof(opb::BatchLattice) * n);
-    if (e == cudaSuccess) e = up(P->sq, sq.data(), sizeof(opb::TcProblem) * n);
-    if (e == cudaSuccess) e = up(P->chain, ch.data(), sizeof(opb::TcProblem) * n);
+    if (e == cudaSuccess) e = up(P->sq[0], sq.data(), sizeof(opb::TcProblem) * 2 * (size_t)n);
+    if (e == cudaSuccess) e = up(P->chain[0], ch.data(), sizeof(opb::TcProblem) * 2 * (size_t)n);
     if (e == cudaSuccess) e = up(P->price, pr.data(), sizeof(opb::TcProblem) * n);
     if (e == cudaSuccess) e = up(P->rn_sq, rs.data(), sizeof(opb::RenormProblem) * n);
-    if (e == cudaSuccess) e = up(P->rn_chain, rc.data(), sizeof(opb::RenormProblem) * n);
-    if (e == cudaSuccess) e = up(P->maps_sq, msq.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
-    if (e == cudaSuccess) e = up(P->maps_ch, mch.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
-    if (e == cudaSuccess) e = up(P->maps_price, mp.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
+    if (e == cudaSuccess) e = up(P->maps_sq[0], msq.data(), sizeof(CUtensorMap) * 8 * (size_t)n);
+    if (e == cudaSuccess) e = up(P->maps_ch[0], mch.data(), sizeof(CUtensorMap) * 8 * (size_t)n);
+    if (e == cudaSuccess) e = up(P->maps_price[0], mp.data(), sizeof(CUtensorMap) * 8 * (size_t)n);
     if (e == cudaSuccess) e = up(P->maps_berm, mbm.data(), sizeof(CUtensorMap) * 4 * (size_t)n);
     if (e == cudaSuccess) e = up(P->work, W.data(), sizeof(uint32_t) * W.size());
     const cudaError_t es = cudaStreamSynchronize(ls);
@@ -501,45 +527,59 @@ namespace {
 
 // One squaring level (or the chain product) under configuration cfg: one launch, or two
 // for the pair configurations (256 x 256 pair items, then 128 x 256 ones).  maps: the
-// squaring or the chain table (MN-major B).
+// squaring or the chain table (MN-major B); fixmode: how the problems' row fixes apply.
 int cfg_gemm(opb_batch_plan *P, int cfg, const CUtensorMap *maps, const opb::TcProblem *probs, const ListRef &l,
-             const ListRef &rest, cudaStream_t s, int level = 0, int lolo = 0, int skip = 0) {
+             const ListRef &rest, cudaStream_t s, int level, int lolo, int skip, int fixmode, int fuse) {
     const int bn = CFG_BN[cfg];
+    const float ss = P->f16 ? F16S : 0.f;
     int r = CFG_PAIR[cfg] ? opb::launch_tc_gemm_batched_pair(maps, probs, P->work + l.off, l.n, s, P->f16, 1, level,
-                                                             lolo, skip)
+                                                             lolo, skip, fixmode, ss, fuse)
                           : opb::launch_tc_gemm_batched(bn, maps, probs, P->work + l.off, l.n, P->grid, s, P->f16, 1,
-                                                        level, lolo, skip);
+                                                        level, lolo, skip, fixmode, ss, fuse);
     if (r == 0 && rest.n > 0)
         r = opb::launch_tc_gemm_batched(256, maps, probs, P->work + rest.off, rest.n, P->grid, s, P->f16, 1, level,
-                                        lolo, skip);
+                                        lolo, skip, fixmode, ss, fuse);
     return r;
 }
 
 // Squaring level `level` of every lattice still squaring; each lattice's operands are
 // banded by its generator (TcProblem::band), and BF16 parts add the lo.lo product on the
-// first OPB_LOLO_LEVELS levels, as in the single-lattice solve.
+// first OPB_LOLO_LEVELS levels, as in the single-lattice solve.  The level reads the part
+// set level % 2 and writes the other; from level 1 on, the previous level's normalisation
+// is deferred into this epilogue.
 int level_gemm(opb_batch_plan *P, int cfg, int level, cudaStream_t s) {
     const int lolo = (!P->f16 && level < opb::g_lolo_levels) ? 1 : 0;
-    return cfg_gemm(P, cfg, P->maps_sq, P->sq, P->gemm_level[cfg][level], P->gemm_level_rest[cfg][level], s, level,
-                    lolo, opb::g_band_skip);
+    const int k = level & 1;
+    return cfg_gemm(P, cfg, P->maps_sq[k], P->sq[k], P->gemm_level[cfg][level], P->gemm_level_rest[cfg][level], s,
+                    level, lolo, opb::g_band_skip, level > 0 ? opb::OPB_FIX_SQUARE : opb::OPB_FIX_NONE, 1);
 }
 
 // The chain product of every lattice (dense, all lattices active): what the autotuner times.
-int chain_gemm(opb_batch_plan *P, int cfg, cudaStream_t s) {
-    return cfg_gemm(P, cfg, P->maps_ch, P->chain, P->gemm_chain[cfg], P->gemm_chain_rest[cfg], s);
+// set: the part set holding P_{m-1}; scaled: apply P_{m-1}'s row fixes (every chain but the
+// first, whose A is the normalised P1).
+int chain_gemm(opb_batch_plan *P, int cfg, cudaStream_t s, int set = 0, bool scaled = false) {
+    return cfg_gemm(P, cfg, P->maps_ch[set], P->chain[set], P->gemm_chain[cfg], P->gemm_chain_rest[cfg], s, 0, 0, 0,
+                    scaled ? opb::OPB_FIX_ROWSCALE : opb::OPB_FIX_NONE, 2);
 }
 
-// E0 build and every squaring level (one GEMM + one renormalisation launch each): P1 of
-// every lattice as row-major parts in its A and B buffers.
+// E0 build and every squaring level: P1 of every lattice as row-major parts in its A and B
+// buffers.  Per level one GEMM, then the row fixes of the lattices that square on and the
+// renormalisation (to P1) of those whose last level it was.
 int batch_square(opb_batch_plan *P, cudaStream_t s) {
     const int cfg = P->cfg, bn = CFG_BN[cfg], pdiv = bn < 128 ? bn : 128;
     const float ss = P->f16 ? F16S : 0.f;
     int r = (int)cudaMemsetAsync(P->E_base, 0, P->E_bytes, s);
+    // the B part set starts zeroed: a level skips the output tiles outside its operands'
+    // band, which must read as zeros when the next level issues their K-blocks
+    if (r == 0) r = (int)cudaMemsetAsync(P->B_hi, 0, P->B_bytes, s);
+    if (r == 0) r = (int)cudaMemsetAsync(P->B_lo, 0, P->B_bytes, s);
     if (r == 0) r = opb::launch_ek_batched(P->lats, P->nlat, P->total_rows, P->ell_width, P->cols, P->vals, s);
     if (r == 0) r = opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_init.off, P->rn_init.n, 0, s, ss);
     for (int lv = 0; lv < P->maxn && r == 0; lv++) {
         r = level_gemm(P, cfg, lv, s);
-        if (r == 0)
+        if (r == 0 && P->level_inter[lv])
+            r = opb::launch_rowfix_batched(P->lats, P->nlat, P->total_rows, pdiv, lv, 1, s);
+        if (r == 0 && P->rn_level[lv].n > 0)
             r = opb::launch_renorm_batched(P->rn_sq, P->work + P->rn_level[lv].off, P->rn_level[lv].n, pdiv, s, ss);
     }
     return r;
@@ -567,18 +607,20 @@ OPB_API int opb_batch_execute(opb_batch_plan *P, double *quotes) {
         return set_status(OPB_OK);
     }
     const int cfg = P->cfg, bn = CFG_BN[cfg], pdiv = bn < 128 ? bn : 128;
-    const float ss = P->f16 ? F16S : 0.f;
     BT(batch_square(P, s));
     BT(opb::launch_payoff_batched(P->lats, P->nlat, P->total_rows, P->nK, P->ldk, P->x, P->strikes, s, P->f16));
+    // chains: P_m = P_{m-1} . P1 writes only its parts (into the other part set) and its row
+    // sums; its row fixes scale the next chain's epilogue and this maturity's quotes
+    int set = 0;
     for (int m = 1; m <= P->nmat; m++) {
         if (m > 1) {
-            BT(chain_gemm(P, cfg, s));
-            BT(opb::launch_renorm_batched(P->rn_chain, P->work + P->rn_chain_list.off, P->rn_chain_list.n, pdiv, s,
-                                          ss));
+            BT(chain_gemm(P, cfg, s, set, m > 2));
+            BT(opb::launch_rowfix_batched(P->lats, P->nlat, P->total_rows, pdiv, -1, 0, s));
+            set ^= 1;
         }
-        BT(opb::launch_tc_gemm_batched(64, P->maps_price, P->price, P->work + P->gemm_price.off, P->gemm_price.n,
-                                       P->grid, s, P->f16, 0));
-        BT(opb::launch_quotes_batched(P->lats, P->nlat, P->nK, P->ldk, m, P->nmat, quotes, s, P->f16));
+        BT(opb::launch_tc_gemm_batched(64, P->maps_price[set], P->price, P->work + P->gemm_price.off,
+                                       P->gemm_price.n, P->grid, s, P->f16, 0));
+        BT(opb::launch_quotes_batched(P->lats, P->nlat, P->nK, P->ldk, m, P->nmat, quotes, s, P->f16, m > 1));
     }
 #undef BT
     return set_status(OPB_OK);
@@ -667,5 +709,8 @@ OPB_API int opb_batch_launches(const opb_batch_plan *P) {
     int extra = 0;  // the pair configurations' second GEMM launch per level / chain
     for (int lv = 0; lv < P->maxn; lv++) extra += P->gemm_level_rest[P->cfg][lv].n > 0 ? 1 : 0;
     if (P->gemm_chain_rest[P->cfg].n > 0) extra += P->nmat - 1;
-    return 3 + 2 * P->maxn + 1 + (P->f16 ? 1 : 0) + 2 * P->nmat + 2 * (P->nmat - 1) + extra;
+    int per_level = 0;  // GEMM, row fixes (some lattice squares on), renormalisation (some ends)
+    for (int lv = 0; lv < P->maxn; lv++)
+        per_level += 1 + (P->level_inter[lv] ? 1 : 0) + (P->rn_level[lv].n > 0 ? 1 : 0);
+    return 5 + per_level + 1 + (P->f16 ? 1 : 0) + 2 * P->nmat + 2 * (P->nmat - 1) + extra;
 }

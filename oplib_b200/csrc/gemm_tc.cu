@@ -166,8 +166,12 @@ __device__ __forceinline__ uint32_t map_to_rank(uint32_t saddr, uint32_t rank) {
 __device__ __forceinline__ void cluster_sync_all() {
     asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
-__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+// Arrive without release semantics: for signals that order only tcgen05 work the arriving
+// thread has already waited for (TMEM loads completed by tcgen05.wait::ld and fenced by
+// tcgen05.fence::before_thread_sync), so that the arrive does not wait for the thread's
+// outstanding global stores (the output phase of the previous tile).
+__device__ __forceinline__ void mbar_arrive_remote_relaxed(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.relaxed.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
 }
 // Tiled load into this CTA's shared memory whose completion is counted on an mbarrier
 // that may live in the peer CTA (the pair leader's).  No multicast.
@@ -306,6 +310,9 @@ struct TcParams {
     int level;               // as TcGemmArgs::level
     int lolo;                // as TcGemmArgs::lolo
     int band_skip;           // as TcGemmArgs::band_skip
+    int fixmode;             // as TcGemmArgs::fixmode
+    __nv_bfloat16 *Shi, *Slo;  // as TcGemmArgs::Shi / Slo (single products; batched: TcProblem)
+    float sscale;            // as TcGemmArgs::sscale
 };
 
 // K-blocks [kb_lo, kb_lo + nkb) that can contribute to the output tile rows [m0, m0 + tm),
@@ -361,8 +368,11 @@ struct TcBatch {
 // into FP32 register sums (round to nearest) while the MMA warp fills the other
 // accumulator.  The tensor cores' truncating accumulation thus spans only 12*CHUNK MMA
 // instructions, and an item's final store overlaps the next item's MMAs.
+// FUSE (split products, EPIMODE 0): 0 = FP32 output (+ Cin, OPB_FIX_CIN); 1 = squaring with
+// its output's parts (Shi / Slo) and OPB_FIX_SQUARE; 2 = parts only (C optional), no Cin,
+// OPB_FIX_ROWSCALE.  Separate instantiations keep each epilogue's registers to its own work.
 template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK,
-          bool PAIR = false, bool BMN = false>
+          bool PAIR = false, bool BMN = false, int FUSE = 0>
 __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
               const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, TcParams p,
@@ -696,9 +706,9 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                 tc_fence_before();
                 if constexpr (PAIR) {
                     __syncwarp();
-                    if (lane == 0) mbar_arrive_remote(map_to_rank(acce_bar(a), 0));
+                    if (lane == 0) mbar_arrive_remote_relaxed(map_to_rank(acce_bar(a), 0));
                 } else {
-                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(acce_bar(a)) : "memory");
+                    asm volatile("mbarrier.arrive.relaxed.cta.shared::cta.b64 _, [%0];" ::"r"(acce_bar(a)) : "memory");
                 }
             }
             if (!ok || *abort_flag) break;
@@ -709,20 +719,22 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             float alpha, beta;
             double *rowsum;
             const double2 *fix;
+            __nv_bfloat16 *Shi, *Slo;  // optional 16-bit parts of the stored values
             int M;
             if constexpr (BATCHED) {
                 const TcProblem &pr = bt.probs[prob];
                 C = pr.C; Cin = pr.Cin; ldc = pr.ldc; alpha = pr.alpha; beta = pr.beta; rowsum = pr.rowsum; M = pr.M;
-                fix = pr.cin_fix;
+                fix = pr.cin_fix; Shi = pr.Shi; Slo = pr.Slo;
             } else {
-                C = p.C + (long long)slice * p.c_slice;  // K-slices write separate partial outputs
+                C = p.C ? p.C + (long long)slice * p.c_slice : nullptr;  // K-slices write separate partials
                 Cin = p.Cin; ldc = p.ldc; alpha = p.alpha; beta = p.beta; rowsum = p.rowsum; M = p.M;
-                fix = p.cin_fix;
+                fix = p.cin_fix; Shi = p.Shi; Slo = p.Slo;
             }
+            const int fm = fix ? (p.fixmode ? p.fixmode : OPB_FIX_CIN) : OPB_FIX_NONE;
             const int row = m0 + (int)rank * TC_BM + q * 32 + lane;
             const int col0 = n0 + h * CPT;
             if constexpr (EPIMODE == 0) {
-                if (nch == 0 && Cin == C) {
+                if (nch == 0 && C && Cin == C) {
                     // a tile that no K-block reaches (outside twice the operands' band): the
                     // product is zero there, and C, updated in place, is zero there too and
                     // keeps its values; only the row-sum partial is written
@@ -787,6 +799,14 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             for (int j = 0; j < CPT / 32; j++) {
 #pragma unroll
                 for (int c = 0; c < 32; c++) st[lane * 33 + c] = sum[32 * j + c];
+                // deferred squaring: the column terms s_j of this lane's four columns
+                float sj[4] = {0.f, 0.f, 0.f, 0.f};
+                if constexpr (FUSE == 1) {
+                    if (fm == OPB_FIX_SQUARE) {
+#pragma unroll
+                        for (int u = 0; u < 4; u++) sj[u] = (float)fix[col0 + 32 * j + tc4 + u].x;
+                    }
+                }
                 __syncwarp();
                 // each half block's Cin loads are issued before any of its stores (with Cin = C
                 // each element is read and then written by this lane alone), so that four
@@ -794,7 +814,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
 #pragma unroll
                 for (int hb = 0; hb < 2; hb++) {
                     float4 cv[4];
-                    if (Cin) {
+                    if (FUSE != 2 && Cin) {
 #pragma unroll
                         for (int i = 0; i < 4; i++)
                             cv[i] = *reinterpret_cast<const float4 *>(
@@ -804,14 +824,41 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                     for (int i = 0; i < 4; i++) {
                         const int rr = 4 * (4 * hb + i) + tr;
                         const int grow = rbase + rr, gcol = col0 + 32 * j + tc4;
-                        float4 o;
-                        o.x = alpha * st[rr * 33 + tc4 + 0];
-                        o.y = alpha * st[rr * 33 + tc4 + 1];
-                        o.z = alpha * st[rr * 33 + tc4 + 2];
-                        o.w = alpha * st[rr * 33 + tc4 + 3];
-                        if (Cin) {
+                        float o[4];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) o[u] = alpha * st[rr * 33 + tc4 + u];
+                        if constexpr (FUSE == 1) {
+                            // squaring with the parts of its output: alpha acc + beta E', and with
+                            // the previous level's normalisation deferred here (OPB_FIX_SQUARE):
+                            // inv_i [alpha acc + (beta - s_i - s_j) E'_ij + (s_i^2 - beta s_i) [i == j]]
+                            // in FP32 (s ~ 1e-5: the products with s are far below an ulp of the
+                            // result's terms' rounding; inv's own rounding scales a whole row, which
+                            // the next level's row sums renormalise)
+                            const float c4[4] = {cv[i].x, cv[i].y, cv[i].z, cv[i].w};
+                            if (fm == OPB_FIX_SQUARE) {
+                                const double2 fx = fix[grow];
+                                const float si = (float)fx.x, inv = (float)fx.y, bi = beta - si;
+#pragma unroll
+                                for (int u = 0; u < 4; u++) {
+                                    float x = fmaf(bi - sj[u], c4[u], o[u]);
+                                    if (grow == gcol + u) x += si * (si - beta);
+                                    o[u] = x * inv;
+                                }
+                            } else {
+#pragma unroll
+                                for (int u = 0; u < 4; u++) o[u] = fmaf(beta, c4[u], o[u]);
+                            }
+                        } else if constexpr (FUSE == 2) {
+                            // parts only, A's rows normalised here (OPB_FIX_ROWSCALE; FP32 inv:
+                            // its rounding scales the whole row, renormalised by the next row sums)
+                            if (fm == OPB_FIX_ROWSCALE) {
+                                const float inv = (float)fix[grow].y;
+#pragma unroll
+                                for (int u = 0; u < 4; u++) o[u] *= inv;
+                            }
+                        } else if (Cin) {
                             float c4[4] = {cv[i].x, cv[i].y, cv[i].z, cv[i].w};
-                            if (fix) {
+                            if (fm == OPB_FIX_CIN) {
                                 // deferred renormalisation of Cin (the arithmetic of the
                                 // E-form renormalisation kernel, so Cin reads exactly as if
                                 // that kernel had stored it)
@@ -823,13 +870,21 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                                     c4[u] = (float)(x * fx.y);
                                 }
                             }
-                            o.x = fmaf(beta, c4[0], o.x);
-                            o.y = fmaf(beta, c4[1], o.y);
-                            o.z = fmaf(beta, c4[2], o.z);
-                            o.w = fmaf(beta, c4[3], o.w);
+#pragma unroll
+                            for (int u = 0; u < 4; u++) o[u] = fmaf(beta, c4[u], o[u]);
                         }
-                        *reinterpret_cast<float4 *>(C + (long long)grow * ldc + gcol) = o;
-                        const double g = (double)o.x + (double)o.y + (double)o.z + (double)o.w;
+                        if (C) *reinterpret_cast<float4 *>(C + (long long)grow * ldc + gcol) = make_float4(o[0], o[1], o[2], o[3]);
+                        if constexpr (FUSE != 0) {
+                            if (Shi) {
+                                uint32_t hh[2], ll[2];
+                                split2x2(o[0], o[1], hh[0], ll[0], p.sscale);
+                                split2x2(o[2], o[3], hh[1], ll[1], p.sscale);
+                                const long long so = (long long)grow * ldc + gcol;
+                                *reinterpret_cast<uint2 *>(Shi + so) = make_uint2(hh[0], hh[1]);
+                                *reinterpret_cast<uint2 *>(Slo + so) = make_uint2(ll[0], ll[1]);
+                            }
+                        }
+                        const double g = (double)o[0] + (double)o[1] + (double)o[2] + (double)o[3];
                         st[rr * 33 + tc4] = __int_as_float(__double2loint(g));
                         st[rr * 33 + tc4 + 1] = __int_as_float(__double2hiint(g));
                     }
@@ -982,11 +1037,19 @@ int tc_gemm_nparts(int M, int N) {
 int tc_gemm_check(const TcGemmArgs &a) {
     if (a.M <= 0 || a.N <= 0 || a.K <= 0) return OPB_E_ARG;
     if (a.M % TC_BM || a.K % TC_BK || !tc_gemm_tile_n(a.N)) return OPB_E_UNSUPPORTED;
-    if (!a.Ahi || !a.Alo || !a.Bhi || !a.Blo || !a.C) return OPB_E_NULL;
+    if (!a.Ahi || !a.Alo || !a.Bhi || !a.Blo || (!a.C && !a.Shi)) return OPB_E_NULL;
+    if (!a.Shi != !a.Slo) return OPB_E_NULL;
+    if (a.Shi && (!aligned(a.Shi, 8) || !aligned(a.Slo, 8) || a.ksplit > 1)) return OPB_E_ARG;
+    if (a.fixmode < 0 || a.fixmode > OPB_FIX_ROWSCALE || (a.fixmode && !a.cin_fix)) return OPB_E_ARG;
+    // the fused epilogues: no Cin-form fix with parts, no Cin with the row scaling
+    if ((a.Shi && a.fixmode == OPB_FIX_CIN) || (a.fixmode == OPB_FIX_ROWSCALE && a.Cin)) return OPB_E_ARG;
+    if (a.Shi && !a.Cin && a.fixmode == OPB_FIX_NONE && a.cin_fix) return OPB_E_ARG;
+    // the deferred squaring reads E' (Cin) and the column fixes of a square product
+    if (a.fixmode == OPB_FIX_SQUARE && (!a.Cin || a.M != a.N)) return OPB_E_ARG;
     if (a.lda < a.K || a.ldb < (a.b_kn ? a.N : a.K) || a.ldc < a.N) return OPB_E_ARG;
     // TMA: 16-byte aligned bases and row strides; float4 epilogue: 16-byte aligned rows
     if (!aligned(a.Ahi, 16) || !aligned(a.Alo, 16) || !aligned(a.Bhi, 16) || !aligned(a.Blo, 16)) return OPB_E_ALIGN;
-    if ((a.lda * 2) % 16 || (a.ldb * 2) % 16 || a.ldc % 4 || !aligned(a.C, 16)) return OPB_E_ALIGN;
+    if ((a.lda * 2) % 16 || (a.ldb * 2) % 16 || a.ldc % 4 || (a.C && !aligned(a.C, 16))) return OPB_E_ALIGN;
     if (a.Cin && !aligned(a.Cin, 16)) return OPB_E_ALIGN;
     if (a.cin_fix && !aligned(a.cin_fix, 16)) return OPB_E_ALIGN;
     if (a.ksplit > 1) {
@@ -1000,14 +1063,14 @@ int tc_gemm_check(const TcGemmArgs &a) {
 }
 
 template <int BN, int STAGES, bool BATCHED, bool F16, int NPROD = 3, int EPIMODE = 0, int BK = TC_BK,
-          bool PAIR = false, bool BMN = false>
+          bool PAIR = false, bool BMN = false, int FUSE = 0>
 static int set_smem_attr() {
     using Cfg = TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>;
     static bool attr_set[64] = {false};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED, F16, NPROD, EPIMODE, BK, PAIR, BMN>,
+        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES, BATCHED, F16, NPROD, EPIMODE, BK, PAIR, BMN, FUSE>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              Cfg::SMEM);
         if (e != cudaSuccess) return (int)e;
@@ -1016,10 +1079,10 @@ static int set_smem_attr() {
     return 0;
 }
 
-template <int BN, int STAGES, bool F16, int BK = TC_BK, bool BMN = false>
+template <int BN, int STAGES, bool F16, int BK = TC_BK, bool BMN = false, int FUSE = 0>
 static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
     using Cfg = TcCfg<BN, STAGES, 3, BK>;
-    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, BK, false, BMN>();
+    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, BK, false, BMN, FUSE>();
     if (e0) return e0;
     CUtensorMap mAh, mAl, mBh, mBl;
     int r;
@@ -1035,23 +1098,27 @@ static int launch_tc_impl(const TcGemmArgs &a, cudaStream_t s) {
     p.level = a.level;
     p.lolo = a.lolo;
     p.band_skip = a.band_skip;
+    p.fixmode = a.fixmode;
+    p.Shi = a.Shi;
+    p.Slo = a.Slo;
+    p.sscale = a.sscale;
     const int ntiles = (a.M / TC_BM) * (a.N / BN) * p.ksplit;
     const int grid = ntiles < num_sms() ? ntiles : num_sms();
     TcBatch none{nullptr, nullptr, nullptr, 0};
-    k_tc_gemm<BN, STAGES, false, F16, 3, 0, BK, false, BMN><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mAh, mAl, mBh, mBl,
-                                                                                                  p, none);
+    k_tc_gemm<BN, STAGES, false, F16, 3, 0, BK, false, BMN, FUSE><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(
+        mAh, mAl, mBh, mBl, p, none);
     return (int)cudaGetLastError();
 }
 
 // 256 x 256 output tiles on 2-CTA clusters: each CTA loads its 128 rows of A and 128 rows
 // of B, the even CTA issues cta_group::2 MMAs over both CTAs' shared memory.  The grid is
 // as many clusters as can be resident at once (at most one per SM pair).
-template <bool F16, bool BMN, int STAGES = 3, int BK = TC_BK>
+template <bool F16, bool BMN, int STAGES = 3, int BK = TC_BK, int FUSE = 0>
 static int launch_tc_pair(const TcGemmArgs &a, cudaStream_t s) {
     constexpr int BN = 256;
     using Cfg = TcCfg<BN, STAGES, 3, BK, true>;
-    auto kern = k_tc_gemm<BN, STAGES, false, F16, 3, 0, BK, true, BMN>;
-    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, BK, true, BMN>();
+    auto kern = k_tc_gemm<BN, STAGES, false, F16, 3, 0, BK, true, BMN, FUSE>;
+    int e0 = set_smem_attr<BN, STAGES, false, F16, 3, 0, BK, true, BMN, FUSE>();
     if (e0) return e0;
     CUtensorMap mAh, mAl, mBh, mBl;
     int r;
@@ -1065,6 +1132,10 @@ static int launch_tc_pair(const TcGemmArgs &a, cudaStream_t s) {
     p.level = a.level;
     p.lolo = a.lolo;
     p.band_skip = a.band_skip;
+    p.fixmode = a.fixmode;
+    p.Shi = a.Shi;
+    p.Slo = a.Slo;
+    p.sscale = a.sscale;
     TcBatch none{nullptr, nullptr, nullptr, 0};
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -1111,11 +1182,12 @@ int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat1
     return OPB_OK;
 }
 
-template <int BN, int STAGES, bool F16, bool BMN>
+template <int BN, int STAGES, bool F16, bool BMN, int FUSE>
 static int launch_batched_impl(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                               int grid, cudaStream_t s, int level, int lolo, int band_skip) {
+                               int grid, cudaStream_t s, int level, int lolo, int band_skip, int fixmode,
+                               float sscale) {
     using Cfg = TcCfg<BN, STAGES>;
-    int e0 = set_smem_attr<BN, STAGES, true, F16, 3, 0, TC_BK, false, BMN>();
+    int e0 = set_smem_attr<BN, STAGES, true, F16, 3, 0, TC_BK, false, BMN, FUSE>();
     if (e0) return e0;
     CUtensorMap dummy;
     std::memset(&dummy, 0, sizeof(dummy));
@@ -1123,8 +1195,10 @@ static int launch_batched_impl(const CUtensorMap *maps, const TcProblem *probs, 
     p.level = level;
     p.lolo = lolo;
     p.band_skip = band_skip;
+    p.fixmode = fixmode;
+    p.sscale = sscale;
     TcBatch bt{maps, probs, work, nwork};
-    k_tc_gemm<BN, STAGES, true, F16, 3, 0, TC_BK, false, BMN><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(
+    k_tc_gemm<BN, STAGES, true, F16, 3, 0, TC_BK, false, BMN, FUSE><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(
         dummy, dummy, dummy, dummy, p, bt);
     return (int)cudaGetLastError();
 }
@@ -1132,13 +1206,13 @@ static int launch_batched_impl(const CUtensorMap *maps, const TcProblem *probs, 
 // Batched 256 x 256 items on 2-CTA clusters: work items (problem << 16 | m-tile << 8 |
 // n-tile) in 256-row / 256-column units, maps with 128-row boxes for A and B (each CTA
 // loads its own half), problems with M % 256 == 0 and N % 256 == 0.
-template <bool F16, bool BMN>
+template <bool F16, bool BMN, int FUSE>
 static int launch_batched_pair_impl(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                                    cudaStream_t s, int level, int lolo, int band_skip) {
+                                    cudaStream_t s, int level, int lolo, int band_skip, int fixmode, float sscale) {
     constexpr int BN = 256, STAGES = 3;
     using Cfg = TcCfg<BN, STAGES, 3, TC_BK, true>;
-    auto kern = k_tc_gemm<BN, STAGES, true, F16, 3, 0, TC_BK, true, BMN>;
-    int e0 = set_smem_attr<BN, STAGES, true, F16, 3, 0, TC_BK, true, BMN>();
+    auto kern = k_tc_gemm<BN, STAGES, true, F16, 3, 0, TC_BK, true, BMN, FUSE>;
+    int e0 = set_smem_attr<BN, STAGES, true, F16, 3, 0, TC_BK, true, BMN, FUSE>();
     if (e0) return e0;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -1171,6 +1245,8 @@ static int launch_batched_pair_impl(const CUtensorMap *maps, const TcProblem *pr
     p.level = level;
     p.lolo = lolo;
     p.band_skip = band_skip;
+    p.fixmode = fixmode;
+    p.sscale = sscale;
     TcBatch bt{maps, probs, work, nwork};
     cudaError_t e = cudaLaunchKernelEx(&cfg, kern, dummy, dummy, dummy, dummy, p, bt);
     return e == cudaSuccess ? (int)cudaGetLastError() : (int)e;
@@ -1178,38 +1254,70 @@ static int launch_batched_pair_impl(const CUtensorMap *maps, const TcProblem *pr
 
 // Batched squaring and chain products take MN-major B maps (b_kn = 1): pair and 256/128
 // tiles exist only in that form; 64-wide tiles in both (pricing is K-major).
+template <int FUSE>
+static int batched_pair_fused(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
+                              cudaStream_t s, int f16, int level, int lolo, int band_skip, int fixmode, float sscale) {
+    return f16 ? launch_batched_pair_impl<true, true, FUSE>(maps, probs, work, nwork, s, level, lolo, band_skip,
+                                                            fixmode, sscale)
+               : launch_batched_pair_impl<false, true, FUSE>(maps, probs, work, nwork, s, level, lolo, band_skip,
+                                                             fixmode, sscale);
+}
+
 int launch_tc_gemm_batched_pair(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                                cudaStream_t s, int f16, int b_kn, int level, int lolo, int band_skip) {
+                                cudaStream_t s, int f16, int b_kn, int level, int lolo, int band_skip, int fixmode,
+                                float sscale, int fuse) {
     if (nwork <= 0) return OPB_OK;
     if (!b_kn) return OPB_E_UNSUPPORTED;
-    return f16 ? launch_batched_pair_impl<true, true>(maps, probs, work, nwork, s, level, lolo, band_skip)
-               : launch_batched_pair_impl<false, true>(maps, probs, work, nwork, s, level, lolo, band_skip);
+    if (fuse == 1) return batched_pair_fused<1>(maps, probs, work, nwork, s, f16, level, lolo, band_skip, fixmode, sscale);
+    if (fuse == 2) return batched_pair_fused<2>(maps, probs, work, nwork, s, f16, level, lolo, band_skip, fixmode, sscale);
+    return batched_pair_fused<0>(maps, probs, work, nwork, s, f16, level, lolo, band_skip, fixmode, sscale);
+}
+
+// MN-major B (b_kn) in every tile width and epilogue form; K-major B (pricing) 64-wide only.
+template <int FUSE>
+static int batched_kn(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
+                      int grid, cudaStream_t s, int f16, int level, int lolo, int band_skip, int fixmode,
+                      float sscale) {
+    switch (bn * 2 + (f16 ? 1 : 0)) {
+        case 512:
+            return launch_batched_impl<256, 2, false, true, FUSE>(maps, probs, work, nwork, grid, s, level, lolo,
+                                                                  band_skip, fixmode, sscale);
+        case 513:
+            return launch_batched_impl<256, 2, true, true, FUSE>(maps, probs, work, nwork, grid, s, level, lolo,
+                                                                 band_skip, fixmode, sscale);
+        case 256:
+            return launch_batched_impl<128, 3, false, true, FUSE>(maps, probs, work, nwork, grid, s, level, lolo,
+                                                                  band_skip, fixmode, sscale);
+        case 257:
+            return launch_batched_impl<128, 3, true, true, FUSE>(maps, probs, work, nwork, grid, s, level, lolo,
+                                                                 band_skip, fixmode, sscale);
+        case 128:
+            return launch_batched_impl<64, 4, false, true, FUSE>(maps, probs, work, nwork, grid, s, level, lolo,
+                                                                 band_skip, fixmode, sscale);
+        case 129:
+            return launch_batched_impl<64, 4, true, true, FUSE>(maps, probs, work, nwork, grid, s, level, lolo,
+                                                                band_skip, fixmode, sscale);
+        default: return OPB_E_UNSUPPORTED;
+    }
 }
 
 int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
-                           int grid, cudaStream_t s, int f16, int b_kn, int level, int lolo, int band_skip) {
+                           int grid, cudaStream_t s, int f16, int b_kn, int level, int lolo, int band_skip, int fixmode,
+                           float sscale, int fuse) {
     if (nwork <= 0) return OPB_OK;
     if (grid <= 0 || grid > nwork) grid = nwork < num_sms() ? nwork : num_sms();
-    if (!b_kn && bn != 64) return OPB_E_UNSUPPORTED;
-    switch (bn * 4 + (f16 ? 2 : 0) + (b_kn ? 1 : 0)) {
-        case 1025:
-            return launch_batched_impl<256, 2, false, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
-        case 1027:
-            return launch_batched_impl<256, 2, true, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
-        case 513:
-            return launch_batched_impl<128, 3, false, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
-        case 515:
-            return launch_batched_impl<128, 3, true, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
-        case 256:
-            return launch_batched_impl<64, 4, false, false>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
-        case 257:
-            return launch_batched_impl<64, 4, false, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
-        case 258:
-            return launch_batched_impl<64, 4, true, false>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
-        case 259:
-            return launch_batched_impl<64, 4, true, true>(maps, probs, work, nwork, grid, s, level, lolo, band_skip);
-        default: return OPB_E_UNSUPPORTED;
+    if (b_kn) {
+        if (fuse == 1)
+            return batched_kn<1>(bn, maps, probs, work, nwork, grid, s, f16, level, lolo, band_skip, fixmode, sscale);
+        if (fuse == 2)
+            return batched_kn<2>(bn, maps, probs, work, nwork, grid, s, f16, level, lolo, band_skip, fixmode, sscale);
+        return batched_kn<0>(bn, maps, probs, work, nwork, grid, s, f16, level, lolo, band_skip, fixmode, sscale);
     }
+    if (bn != 64 || fuse) return OPB_E_UNSUPPORTED;
+    return f16 ? launch_batched_impl<64, 4, true, false, 0>(maps, probs, work, nwork, grid, s, level, lolo, band_skip,
+                                                            fixmode, sscale)
+               : launch_batched_impl<64, 4, false, false, 0>(maps, probs, work, nwork, grid, s, level, lolo, band_skip,
+                                                             fixmode, sscale);
 }
 
 // One network layer on the tensor cores: H[M, N] = GELU(alpha * A[M, K] . W[N, K]^T + bias)
@@ -1242,29 +1350,49 @@ int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, 
     return (int)cudaGetLastError();
 }
 
+// The epilogue form of a product (the FUSE template parameter of k_tc_gemm).
+static int fuse_of(const TcGemmArgs &a) {
+    if (a.fixmode == OPB_FIX_SQUARE || (a.Shi && a.Cin)) return 1;
+    if (a.fixmode == OPB_FIX_ROWSCALE || a.Shi) return 2;
+    return 0;
+}
+
+// Products with B given K x N row-major (MN-major operand; BK = 64 only): the squaring and
+// chain products, in any of the three epilogue forms.
+template <int FUSE>
+static int launch_tc_kn(const TcGemmArgs &a, cudaStream_t s, bool pair) {
+    switch (tile_for(a.M, a.N, a.ksplit) * 2 + (a.f16 ? 1 : 0)) {
+        case 512:
+            if (pair)
+                return g_bk256 == 32 ? launch_tc_pair<false, true, 6, 32, FUSE>(a, s)
+                                     : launch_tc_pair<false, true, 3, TC_BK, FUSE>(a, s);
+            return launch_tc_impl<256, 2, false, 64, true, FUSE>(a, s);
+        case 513:
+            if (pair)
+                return g_bk256 == 32 ? launch_tc_pair<true, true, 6, 32, FUSE>(a, s)
+                                     : launch_tc_pair<true, true, 3, TC_BK, FUSE>(a, s);
+            return launch_tc_impl<256, 2, true, 64, true, FUSE>(a, s);
+        case 256: return launch_tc_impl<128, 3, false, 64, true, FUSE>(a, s);
+        case 257: return launch_tc_impl<128, 3, true, 64, true, FUSE>(a, s);
+        case 128: return launch_tc_impl<64, 4, false, 64, true, FUSE>(a, s);
+        case 129: return launch_tc_impl<64, 4, true, 64, true, FUSE>(a, s);
+        default: return OPB_E_UNSUPPORTED;
+    }
+}
+
 int launch_tc_gemm(const TcGemmArgs &a, cudaStream_t s) {
     int c = tc_gemm_check(a);
     if (c != OPB_OK) return c;
     // K-sliced products (pricing, induction) stay on one CTA per tile: on CTA pairs, which
     // share the B tile and so hold four stages of A instead of three, they ran 6% slower
     const bool pair = g_pair && a.M % (2 * TC_BM) == 0 && a.ksplit <= 1;
-    if (a.b_kn) {  // MN-major B (K x N): BK = 64 only
-        switch (tile_for(a.M, a.N, a.ksplit) * 2 + (a.f16 ? 1 : 0)) {
-            case 512:
-                if (pair)
-                    return g_bk256 == 32 ? launch_tc_pair<false, true, 6, 32>(a, s) : launch_tc_pair<false, true>(a, s);
-                return launch_tc_impl<256, 2, false, 64, true>(a, s);
-            case 513:
-                if (pair)
-                    return g_bk256 == 32 ? launch_tc_pair<true, true, 6, 32>(a, s) : launch_tc_pair<true, true>(a, s);
-                return launch_tc_impl<256, 2, true, 64, true>(a, s);
-            case 256: return launch_tc_impl<128, 3, false, 64, true>(a, s);
-            case 257: return launch_tc_impl<128, 3, true, 64, true>(a, s);
-            case 128: return launch_tc_impl<64, 4, false, 64, true>(a, s);
-            case 129: return launch_tc_impl<64, 4, true, 64, true>(a, s);
-            default: return OPB_E_UNSUPPORTED;
-        }
+    const int fuse = fuse_of(a);
+    if (a.b_kn) {
+        if (fuse == 1) return launch_tc_kn<1>(a, s, pair);
+        if (fuse == 2) return launch_tc_kn<2>(a, s, pair);
+        return launch_tc_kn<0>(a, s, pair);
     }
+    if (fuse) return OPB_E_UNSUPPORTED;  // fused epilogues: MN-major B only
     switch (tile_for(a.M, a.N, a.ksplit) * 2 + (a.f16 ? 1 : 0)) {
         case 512:
             if (pair) return launch_tc_pair<false, false>(a, s);

@@ -182,7 +182,9 @@ int g_ksplit = 0;
 int tc_gemm_ksplit(const opb::TcGemmArgs &a, cudaStream_t s) {
     int S = g_ksplit > 0 ? g_ksplit : 1;
     int kb = a.K / 64;
-    if (S <= 1 || kb < S || kb % S || a.ksplit > 1 || a.band) return opb::launch_tc_gemm(a, s);
+    // (products that fuse their normalisation or splits into the epilogue run in one launch)
+    if (S <= 1 || kb < S || kb % S || a.ksplit > 1 || a.band || a.Shi || a.fixmode >= opb::OPB_FIX_SQUARE)
+        return opb::launch_tc_gemm(a, s);
     const int kslice = a.K / S;
     for (int i = 0; i < S; i++) {
         opb::TcGemmArgs t = a;
@@ -226,12 +228,32 @@ int square_tc(const opb_lattice_desc &L, Bufs &b, cudaStream_t s, bool f16, opb:
     g = opb::TcGemmArgs{};
     g.M = d; g.N = d; g.K = d; g.lda = d; g.ldb = d; g.ldc = d; g.f16 = f16 ? 1 : 0; g.b_kn = 1;
     g.Ahi = b.Ahi; g.Alo = b.Alo; g.Bhi = b.Ahi; g.Blo = b.Alo;
+    // The squarings write the next level's parts themselves, ping-ponging between the A and
+    // the B part buffers; the normalisation of level r's output is deferred into level r + 1's
+    // epilogue (OPB_FIX_SQUARE).  A level skips the output tiles that no K-block reaches,
+    // so its part buffer must be zero there: A holds E0's parts (zero outside the band) and
+    // B starts zeroed; the band only grows, so the tiles a level skips are zero in both.
+    // (lattices above g_fused_max_d states: a renormalisation kernel after every level, which
+    // writes the next level's parts; its traffic is small against a squaring's there)
+    const bool fused = d <= opb::g_fused_max_d;
+    if (fused && L.niter > 1) {
+        LT((int)cudaMemsetAsync(b.Bhi, 0, sizeof(__nv_bfloat16) * (size_t)d * d, s));
+        LT((int)cudaMemsetAsync(b.Blo, 0, sizeof(__nv_bfloat16) * (size_t)d * d, s));
+    }
+    __nv_bfloat16 *ph[2] = {b.Ahi, b.Bhi}, *pl[2] = {b.Alo, b.Blo};
     for (int r = 0; r < L.niter; r++) {
-        // D = 2E + E.E in place of E, with FP64 row-sum partials.  From the second level on,
-        // X holds the previous product as it left the GEMM, and its renormalisation (b.fix)
-        // is applied as the epilogue reads it.
+        // E' = 2E + E.E in place of E (X), with FP64 row-sum partials.  From the second level
+        // on, X and the parts hold the previous level's output as its epilogue left it, and
+        // that output's normalisation (b.fix, from its row sums) is applied in this epilogue.
+        const bool last = r + 1 == L.niter;
+        const int cur = fused ? (r & 1) : 0;
+        g.Ahi = ph[cur]; g.Alo = pl[cur]; g.Bhi = ph[cur]; g.Blo = pl[cur];
         g.C = b.X; g.Cin = b.X; g.alpha = unscale; g.beta = 2.f; g.rowsum = b.part;
         g.cin_fix = r > 0 ? b.fix : nullptr;
+        g.fixmode = r == 0 ? opb::OPB_FIX_NONE : fused ? opb::OPB_FIX_SQUARE : opb::OPB_FIX_CIN;
+        g.Shi = (last || !fused) ? nullptr : ph[cur ^ 1];
+        g.Slo = (last || !fused) ? nullptr : pl[cur ^ 1];
+        g.sscale = ss;
         g.band = L.ell_width > 0 ? b.band : nullptr;
         g.band_skip = opb::g_band_skip;
         g.level = r;
@@ -239,12 +261,16 @@ int square_tc(const opb_lattice_desc &L, Bufs &b, cudaStream_t s, bool f16, opb:
         g.lolo = (!f16 && r < opb::g_lolo_levels) ? 1 : 0;
         LT(tc_gemm_ksplit(g, s));
         // the last level emits P1 = I + E and its splits (row-major into A: the first
-        // chain's A and pricing's; row-major into B: every chain's B); the others write only
-        // the A splits and the row fixes
-        if (r + 1 == L.niter) LT(opb::launch_renorm_to_p(d, b.X, b.part, np, b.Ahi, b.Alo, b.Bhi, b.Blo, s, ss));
+        // chain's A and pricing's; row-major into B: every chain's B); the others only the
+        // row fixes of their output
+        if (last) LT(opb::launch_renorm_to_p(d, b.X, b.part, np, b.Ahi, b.Alo, b.Bhi, b.Blo, s, ss));
+        else if (fused) LT(opb::launch_rowfix(d, b.part, np, 1, b.fix, s));
         else LT(opb::launch_renorm(d, b.X, b.part, np, 1, b.Ahi, b.Alo, nullptr, nullptr, s, ss, 0, b.fix));
     }
+    g.Ahi = b.Ahi; g.Alo = b.Alo;
     g.cin_fix = nullptr;
+    g.fixmode = opb::OPB_FIX_NONE;
+    g.Shi = g.Slo = nullptr;
     g.band = nullptr;
     g.band_skip = 0;
     g.level = 0;
@@ -284,18 +310,41 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
     // K-slices fill the GPU with this small-N product's tiles; the discount sums them
     pg.ksplit = opb::tc_gemm_split_for(d, nKp, d);
     pg.c_slice = (long long)d * nKp;
+    // The chain products write only the parts of their output, ping-ponging between the A
+    // part buffers and a second pair carved from the FP32 chain buffer (unused in the split
+    // modes); each output's row normalisation is deferred into the next chain product's
+    // epilogue and into its own pricing's discount (row scaling commutes with the products).
+    // (above g_fused_max_d states: FP32 chain products renormalised by a kernel that writes the
+    // parts into A, as the squarings are)
+    const bool fused = d <= opb::g_fused_max_d;
+    const size_t dd = (size_t)d * d;
+    __nv_bfloat16 *ch_hi[2] = {b.Ahi, reinterpret_cast<__nv_bfloat16 *>(b.Pa)};
+    __nv_bfloat16 *ch_lo[2] = {b.Alo, reinterpret_cast<__nv_bfloat16 *>(b.Pa) + dd};
+    int cur = 0;
     for (int m = 1; m <= L.nmat; m++) {
-        if (m > 1) {
+        if (m > 1 && fused) {
+            // P_m = P_{m-1} . P1 (A: P_{m-1}'s parts, B: P1's), scaled by P_{m-1}'s row fix
+            g.Ahi = ch_hi[cur]; g.Alo = ch_lo[cur];
+            g.C = nullptr; g.Cin = nullptr; g.alpha = unscale; g.beta = 0.f; g.rowsum = b.part;
+            g.cin_fix = m > 2 ? b.fix : nullptr;
+            g.fixmode = m > 2 ? opb::OPB_FIX_ROWSCALE : opb::OPB_FIX_NONE;
+            g.Shi = ch_hi[cur ^ 1]; g.Slo = ch_lo[cur ^ 1]; g.sscale = ss;
+            LT(tc_gemm_ksplit(g, s));
+            LT(opb::launch_rowfix(d, b.part, np, 0, b.fix, s));
+            cur ^= 1;
+        } else if (m > 1) {
             // P_m = P_{m-1} . P1 (A splits hold P_{m-1}, B splits P1), renormalise, split
             // row-major into A
             g.C = b.Pa; g.Cin = nullptr; g.alpha = unscale; g.beta = 0.f; g.rowsum = b.part;
             LT(tc_gemm_ksplit(g, s));
             LT(opb::launch_renorm(d, b.Pa, b.part, np, 0, b.Ahi, b.Alo, nullptr, nullptr, s, ss, 0));
         }
+        pg.Ahi = ch_hi[cur]; pg.Alo = ch_lo[cur];
         LT(tc_gemm_ksplit(pg, s));
         const double disc = std::exp(-L.rate * L.period * m);
         LT(opb::launch_discount(d_gen, nK, nKp, b.V, disc, V_all ? V_all + (size_t)(m - 1) * d_gen * nK : nullptr,
-                                L.y0, quotes + (size_t)(m - 1) * nK, s, gs, pg.ksplit, pg.c_slice));
+                                L.y0, quotes + (size_t)(m - 1) * nK, s, gs, pg.ksplit, pg.c_slice,
+                                (m > 1 && fused) ? b.fix : nullptr));
     }
     return 0;
 }
@@ -385,7 +434,18 @@ int prepare_padded(const opb_lattice_desc &L, int mode, Bufs &b, opb_lattice_des
 namespace opb {
 int g_lolo_levels = OPB_LOLO_LEVELS;
 int g_band_skip = 1;
+int g_fused_max_d = OPB_FUSED_MAX_D;
 }  // namespace opb
+
+// Tuning knob: the largest lattice (states) whose single-lattice solve defers each product's
+// row normalisation into the next product's epilogue, which also writes the next operand's
+// parts (no renormalisation kernel between products); larger lattices renormalise with a
+// kernel after every product.  0 = never; default OPB_FUSED_MAX_D.
+OPB_API int opb_set_fused_normalisation(int max_d) {
+    OPB_REQUIRE(max_d >= 0, OPB_E_ARG);
+    opb::g_fused_max_d = max_d;
+    return opb::set_status(OPB_OK);
+}
 
 OPB_API int opb_set_lolo_levels(int n) {
     OPB_REQUIRE(n >= 0 && n <= 64, OPB_E_ARG);

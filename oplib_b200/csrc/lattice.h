@@ -3,10 +3,51 @@
 
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace opb {
+
+// Two-part split of an FP32 value into 16-bit storage.  sscale == 0: BF16 parts,
+// hi = bf16(f), lo = bf16(f - hi).  sscale > 0 (a power of two): FP16 parts of f*sscale,
+// hi = fp16(f*s), lo = fp16(f*s - hi) -- 11 + 11 significant bits instead of 8 + 8; the
+// GEMM removes the scale through alpha.  The differences are exact in FP32.
+__device__ __forceinline__ void split2(float f, __nv_bfloat16 &hi, __nv_bfloat16 &lo, float sscale = 0.f) {
+    if (sscale == 0.f) {
+        hi = __float2bfloat16_rn(f);
+        lo = __float2bfloat16_rn(f - __bfloat162float(hi));
+    } else {
+        const float fs = f * sscale;
+        const __half h = __float2half_rn(fs);
+        const __half l = __float2half_rn(fs - __half2float(h));
+        hi = __ushort_as_bfloat16(__half_as_ushort(h));
+        lo = __ushort_as_bfloat16(__half_as_ushort(l));
+    }
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) {
+    return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+
+// split2 of two values at once with the paired conversions, the parts packed (a in the low
+// half): the same parts as split2 on each.
+__device__ __forceinline__ void split2x2(float a, float b, uint32_t &hi, uint32_t &lo, float sscale = 0.f) {
+    if (sscale == 0.f) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        const float2 hf = __bfloat1622float2(h);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+        hi = *reinterpret_cast<const uint32_t *>(&h);
+        lo = *reinterpret_cast<const uint32_t *>(&l);
+    } else {
+        const float as = a * sscale, bs = b * sscale;
+        const __half2 h = __floats2half2_rn(as, bs);
+        const float2 hf = __half22float2(h);
+        const __half2 l = __floats2half2_rn(as - hf.x, bs - hf.y);
+        hi = *reinterpret_cast<const uint32_t *>(&h);
+        lo = *reinterpret_cast<const uint32_t *>(&l);
+    }
+}
 
 // gemm_simt.cu
 int sgemm_rm(int M, int N, int K, float alpha, const float *A, int lda, const float *B, int ldb, float beta,
@@ -46,8 +87,15 @@ int launch_payoff(int d, int nK, int ldk, const double *x, const double *K, floa
                   __nv_bfloat16 *GTlo, cudaStream_t s, const float *dscale = nullptr);
 // V32 may hold nslice K-slices' partial products slice_stride elements apart, summed in
 // FP64 in slice order
+// rowfix (optional): per-row (s, inv) of a P-form product whose normalisation was deferred;
+// row y of V is multiplied by inv_y
 int launch_discount(int d, int nK, int ldk, const float *V32, double disc, double *V64, int y0, double *quotes,
-                    cudaStream_t s, const float *dscale = nullptr, int nslice = 1, long long slice_stride = 0);
+                    cudaStream_t s, const float *dscale = nullptr, int nslice = 1, long long slice_stride = 0,
+                    const double2 *rowfix = nullptr);
+// fix[row] = (s, inv) from a product's FP64 row-sum partials (nparts per row, partial[p*d +
+// row]): s = the row sum; inv = 1 / (1 + s) for an E-form product (eform), 1 / s for a
+// P-form one (the arithmetic of the renormalisation kernels' row sums)
+int launch_rowfix(int d, const double *partial, int nparts, int eform, double2 *fix, cudaStream_t s);
 
 // Batched lattice tables (device memory).
 struct BatchLattice {
@@ -60,6 +108,9 @@ struct BatchLattice {
     __nv_bfloat16 *GThi, *GTlo;  // ldk x d payoff splits (or, in the induction, d x ldk value splits)
     float *gscale;        // device scalar: FP16 payoff split scale
     double *Vd;           // d x ldk FP64 option values of the backward induction
+    int niter;            // squaring levels
+    const double *partial;  // the last product's FP64 row-sum partials (partial[p*d + row])
+    double2 *fix;         // per-row (s, inv) of the last product's deferred normalisation
 };
 // Renormalisation staging: tiles in flight per block, and column tiles per batched work
 // item (a batched item renormalises the tiles chunk, chunk + renorm_chunks(d), ... of one
@@ -99,8 +150,14 @@ int launch_ek_batched(const BatchLattice *lats, int nlat, long long total_rows, 
                       const double *vals, cudaStream_t s);
 int launch_payoff_batched(const BatchLattice *lats, int nlat, long long total_rows, int nK, int ldk, const double *x,
                           const double *strikes, cudaStream_t s, int f16 = 0);
+// rowfix: scale each lattice's V row y0 by its fix (P-form products with deferred normalisation)
 int launch_quotes_batched(const BatchLattice *lats, int nlat, int nK, int ldk, int m, int nmat, double *quotes,
-                          cudaStream_t s, int f16 = 0);
+                          cudaStream_t s, int f16 = 0, int rowfix = 0);
+// BatchLattice::fix from BatchLattice::partial (parts_div columns per partial) for every
+// lattice still squaring after `level` (eform, niter > level + 1), or for all (P-form,
+// level < 0)
+int launch_rowfix_batched(const BatchLattice *lats, int nlat, long long total_rows, int parts_div, int level,
+                          int eform, cudaStream_t s);
 
 // gemm_tc.cu -- split-BF16 tensor-core GEMM.
 //   C[M,N] = alpha * (Ahi.Bhi^T + Ahi.Blo^T + Alo.Bhi^T) + beta * Cin[M,N]
@@ -136,7 +193,25 @@ struct TcGemmArgs {
     // 1: also issue the fourth split product lo.lo (split modes); where the band is known,
     // only while the operands are banded (2 * (h0 << level) < K)
     int lolo;
+    // how cin_fix applies (OPB_FIX_*; 0 = OPB_FIX_CIN when cin_fix is given)
+    int fixmode;
+    // optional: the epilogue also stores the two 16-bit parts (split2 with sscale) of every
+    // value it stores, row-major with leading dimension ldc; C may then be null (parts only)
+    __nv_bfloat16 *Shi, *Slo;
+    float sscale;
 };
+// Deferred normalisation in the epilogue, with cin_fix[i] = (s_i, inv_i) of the operand
+// rows (E-form: the row sums s of P = I + E' are 1 + s, inv = 1 / (1 + s); P-form: s the row
+// sum, inv = 1 / s):
+//   OPB_FIX_CIN     Cin is read as (Cin - s_i [i == j]) * inv_i (the operands are normalised)
+//   OPB_FIX_SQUARE  the operands are the parts of the unnormalised E' (= Cin), E = D (E' - S)
+//                   with D = diag(inv), S = diag(s); the output is
+//                   D [alpha acc + (beta - s_i - s_j) E'_ij + (s_i^2 - beta s_i) [i == j]],
+//                   i.e. alpha E.E + beta E with the D between the two factors left out (a
+//                   relative change of |s| <= 1e-5 in the product, below its split rounding)
+//   OPB_FIX_ROWSCALE the A operand is the parts of an unnormalised P-form product: the
+//                   output is inv_i * alpha * acc (exact: row scaling commutes)
+enum { OPB_FIX_NONE = 0, OPB_FIX_CIN = 1, OPB_FIX_SQUARE = 2, OPB_FIX_ROWSCALE = 3 };
 // Split-BF16 squarings add the fourth product lo.lo on their first OPB_LOLO_LEVELS levels,
 // as long as the operands are still banded (twice the band below the size; every level up
 // to OPB_LOLO_LEVELS when the band is not known).  hi.hi + hi.lo + lo.hi leaves out lo.lo,
@@ -148,6 +223,16 @@ constexpr int OPB_LOLO_LEVELS = 8;
 // knobs shared by the single and batched solves (opb_set_lolo_levels, opb_set_band_skip)
 extern int g_lolo_levels;  // leading squaring levels with the lo.lo product (BF16 parts)
 extern int g_band_skip;    // 1: squarings leave out the K-blocks outside the operands' band
+// The single-lattice solve fuses the row normalisation into the products' epilogues (which
+// then also write the next operand's parts) up to this many states; 0 by default.  A fused
+// epilogue lengthens each tile's output phase, which sits on the tile's critical path,
+// about as much as the renormalisation kernel it replaces costs at these sizes: measured
+// whole solves (SV lattices, CUDA-graph replay) 26.20 against 26.34 ms at d = 6144, 9.02
+// against 9.06 ms at 4096, and 2.38 against 2.25 ms at 2048, where a one-wave product has
+// no later tile to hide the longer output phase behind.  The batched sweep, where the
+// renormalisation of hundreds of small lattices took 19% of the time, always fuses.
+constexpr int OPB_FUSED_MAX_D = 0;
+extern int g_fused_max_d;  // opb_set_fused_normalisation
 // K-slices that fill the GPU with the tiles of a small-N product (1 = none), at most 4
 int tc_gemm_split_for(int M, int N, int K);
 int tc_gemm_tile_n(int N);                    // tile width chosen for N (0 if unsupported)
@@ -171,6 +256,7 @@ struct TcProblem {
     long long ldc;
     float alpha, beta;
     const double2 *cin_fix;  // as TcGemmArgs::cin_fix
+    __nv_bfloat16 *Shi, *Slo;  // as TcGemmArgs::Shi / Slo (optional)
 };
 // Four maps (Ahi, Alo, Bhi, Blo) of one problem: A with 128-row boxes; B K-major (N x K,
 // bn-row boxes) or, with b_kn, K x N row-major read as an MN-major operand (64 x 64
@@ -181,14 +267,17 @@ int tc_make_maps(CUtensorMap *out4, const __nv_bfloat16 *Ahi, const __nv_bfloat1
 // work: packed (problem << 16 | m-tile << 8 | n-tile); bn in {64, 128, 256}; K-major B
 // (b_kn = 0) only for bn = 64
 // level, lolo: as TcGemmArgs (band per problem in TcProblem::band)
+// fixmode, sscale: as TcGemmArgs (the problems' cin_fix and Shi / Slo); fuse: the epilogue
+// form (0: FP32 output, OPB_FIX_CIN; 1: squaring with its output's parts, OPB_FIX_SQUARE;
+// 2: parts only, OPB_FIX_ROWSCALE), MN-major B only
 int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
                            int grid, cudaStream_t s, int f16, int b_kn, int level = 0, int lolo = 0,
-                           int band_skip = 0);
+                           int band_skip = 0, int fixmode = 0, float sscale = 0.f, int fuse = 0);
 // 256 x 256 items (256-row / 256-column units) on 2-CTA clusters, each CTA loading its
 // 128 rows of A and 128 columns of B; MN-major B maps; problems with M, N multiples of 256
 int launch_tc_gemm_batched_pair(const CUtensorMap *maps, const TcProblem *probs, const uint32_t *work, int nwork,
                                 cudaStream_t s, int f16, int b_kn, int level = 0,
-                                int lolo = 0, int band_skip = 0);
+                                int lolo = 0, int band_skip = 0, int fixmode = 0, float sscale = 0.f, int fuse = 0);
 
 // sck.cu
 int launch_sck_rm(int d, int nrows, const float *P, float *C, cudaStream_t s);

@@ -85,23 +85,6 @@ __global__ void k_pad_x(int d, int dpad, const double *__restrict__ x, double *_
     if (i < dpad) xpad[i] = x[i < d ? i : d - 1];
 }
 
-// Two-part split of an FP32 value into 16-bit storage.  sscale == 0: BF16 parts,
-// hi = bf16(f), lo = bf16(f - hi).  sscale > 0 (a power of two): FP16 parts of f*sscale,
-// hi = fp16(f*s), lo = fp16(f*s - hi) -- 11 + 11 significant bits instead of 8 + 8; the
-// GEMM removes the scale through alpha.  The differences are exact in FP32.
-__device__ __forceinline__ void split2(float f, __nv_bfloat16 &hi, __nv_bfloat16 &lo, float sscale = 0.f) {
-    if (sscale == 0.f) {
-        hi = __float2bfloat16_rn(f);
-        lo = __float2bfloat16_rn(f - __bfloat162float(hi));
-    } else {
-        const float fs = f * sscale;
-        const __half h = __float2half_rn(fs);
-        const __half l = __float2half_rn(fs - __half2float(h));
-        hi = __ushort_as_bfloat16(__half_as_ushort(h));
-        lo = __ushort_as_bfloat16(__half_as_ushort(l));
-    }
-}
-
 // 32x32 tiles, 256 threads.  X is (rows x cols) row-major with leading dimension ld.
 // Writes hi/lo of X (row-major, ld) and of X^T (cols x rows, leading dimension ldt).
 __global__ void k_split_tr(int rows, int cols, const float *__restrict__ X, long long ld,
@@ -218,10 +201,6 @@ struct RenormSmem {
     double s_sum[64], s_inv[64];
     uint32_t t[64][65];
 };
-
-__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) {
-    return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
-}
 
 // Input staging: a ring of RN_RING tiles in shared memory filled by cp.async (16 bytes per
 // thread and copy), so that RN_RING - 1 tiles are in flight per block while one is
@@ -478,14 +457,57 @@ __global__ void k_payoff_batched(const BatchLattice *__restrict__ lats, int nlat
 
 // quotes[(i*nmat + m-1)*nK + k] = exp(-r_i T_m) * V_i[y0_i, k]
 __global__ void k_quotes_batched(const BatchLattice *__restrict__ lats, int nlat, int nK, int ldk, int m, int nmat,
-                                 double *__restrict__ quotes, int f16) {
+                                 double *__restrict__ quotes, int f16, int rowfix) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nlat * nK) return;
     int i = t / nK, k = t - i * nK;
     const BatchLattice &L = lats[i];
     double disc = exp(-L.rate * L.period * m);
     if (f16) disc /= (double)L.gscale[0];
+    if (rowfix) disc *= L.fix[L.y0].y;  // the deferred normalisation of the priced row
     quotes[((long long)i * nmat + (m - 1)) * nK + k] = disc * (double)L.V[(long long)L.y0 * ldk + k];
+}
+
+// Row fixes from FP64 row-sum partials, with the arithmetic of the renormalisation
+// kernels' row sums (renorm64_sums): s = sum of the nparts partials in order; E-form inv =
+// 1 / (1 + s), P-form inv = 1 / s.
+__device__ __forceinline__ double2 row_fix(const double *__restrict__ partial, int d, int nparts, int row, int eform) {
+    double s = 0.0;
+    const double *q = partial + row;
+    int p = 0;
+    for (; p + 8 <= nparts; p += 8) {
+        double v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) v[j] = q[(long long)(p + j) * d];
+#pragma unroll
+        for (int j = 0; j < 8; j++) s += v[j];
+    }
+    for (; p < nparts; p++) s += q[(long long)p * d];
+    const double den = nparts == 0 ? 1.0 : (eform ? 1.0 + s : s);
+    return make_double2(s, den != 0.0 ? 1.0 / den : 0.0);
+}
+
+__global__ void k_rowfix(int d, const double *__restrict__ partial, int nparts, int eform, double2 *__restrict__ fix) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < d) fix[r] = row_fix(partial, d, nparts, r, eform);
+}
+
+// Thread per global row of all lattices (rows concatenated); level >= 0: only the lattices
+// whose next level is an intermediate squaring (niter > level + 1), E-form; level < 0: all,
+// P-form.
+__global__ void k_rowfix_batched(const BatchLattice *__restrict__ lats, int nlat, long long total_rows, int parts_div,
+                                 int level, int eform) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= total_rows) return;
+    int lo = 0, hi = nlat - 1;
+    while (lo < hi) {  // last lattice with row_off <= t
+        int mid = (lo + hi + 1) >> 1;
+        if (lats[mid].row_off <= t) lo = mid; else hi = mid - 1;
+    }
+    const BatchLattice &L = lats[lo];
+    if (level >= 0 && L.niter <= level + 1) return;
+    const int row = (int)(t - L.row_off);
+    L.fix[row] = row_fix(L.partial, L.d, L.d / parts_div, row, eform);
 }
 
 // E-form -> P-form: P = I + E (in place), FP32.
@@ -529,12 +551,13 @@ __device__ __forceinline__ double sum_slices(const float *__restrict__ P, long l
 // nslice K-slices; gscale = the payoff split scale, 1 without one); quotes[k] = V64[y0, k].
 __global__ void k_discount(int d, int nK, int ldk, const float *__restrict__ V32, double disc,
                            double *__restrict__ V64, int y0, double *__restrict__ quotes, const float *__restrict__ dscale,
-                           int nslice, long long slice_stride) {
+                           int nslice, long long slice_stride, const double2 *__restrict__ rowfix) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)d * nK) return;
     int y = (int)(t / nK), k = (int)(t - (long long)y * nK);
     if (dscale) disc /= (double)*dscale;
     double v = disc * sum_slices(V32, (long long)y * ldk + k, nslice, slice_stride);
+    if (rowfix) v *= rowfix[y].y;  // the deferred row normalisation of the priced product
     if (V64) V64[t] = v;
     if (quotes && y == y0) quotes[k] = v;
 }
@@ -896,9 +919,21 @@ int launch_payoff_batched(const BatchLattice *lats, int nlat, long long total_ro
 }
 
 int launch_quotes_batched(const BatchLattice *lats, int nlat, int nK, int ldk, int m, int nmat, double *quotes,
-                          cudaStream_t s, int f16) {
+                          cudaStream_t s, int f16, int rowfix) {
     int n = nlat * nK;
-    k_quotes_batched<<<(n + 255) / 256, 256, 0, s>>>(lats, nlat, nK, ldk, m, nmat, quotes, f16);
+    k_quotes_batched<<<(n + 255) / 256, 256, 0, s>>>(lats, nlat, nK, ldk, m, nmat, quotes, f16, rowfix);
+    return (int)cudaGetLastError();
+}
+
+int launch_rowfix(int d, const double *partial, int nparts, int eform, double2 *fix, cudaStream_t s) {
+    k_rowfix<<<blocks_for(d, 256), 256, 0, s>>>(d, partial, nparts, eform, fix);
+    return (int)cudaGetLastError();
+}
+
+int launch_rowfix_batched(const BatchLattice *lats, int nlat, long long total_rows, int parts_div, int level,
+                          int eform, cudaStream_t s) {
+    if (parts_div <= 0) return OPB_E_ARG;
+    k_rowfix_batched<<<blocks_for(total_rows, 256), 256, 0, s>>>(lats, nlat, total_rows, parts_div, level, eform);
     return (int)cudaGetLastError();
 }
 
@@ -968,10 +1003,10 @@ int launch_berm_step(int d, int nK, int ldk, const float *C, double disc, const 
 }
 
 int launch_discount(int d, int nK, int ldk, const float *V32, double disc, double *V64, int y0, double *quotes,
-                    cudaStream_t s, const float *dscale, int nslice, long long slice_stride) {
+                    cudaStream_t s, const float *dscale, int nslice, long long slice_stride, const double2 *rowfix) {
     long long n = (long long)d * nK;
     k_discount<<<blocks_for(n, 256), 256, 0, s>>>(d, nK, ldk, V32, disc, V64, y0, quotes, dscale,
-                                                  nslice > 1 ? nslice : 1, slice_stride);
+                                                  nslice > 1 ? nslice : 1, slice_stride, rowfix);
     return (int)cudaGetLastError();
 }
 

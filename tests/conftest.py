@@ -23,11 +23,44 @@ def oracle_c():
     return oc.load()
 
 
+# Device memory below 4 GB of address space for the reference's kernels that read 32-bit
+# device pointers (tests/test_gpu_ref_kernels.py).  It is reserved when the session's first
+# GPU test starts, while that part of the address space is still free: later in a long
+# session the library's and torch's allocations may occupy it.
+LOW_BYTES = 96 << 20
+_low = {}
+
+
+def _reserve_low_memory():
+    import ctypes as C
+    try:
+        from oracle import ref_opcuda
+        if not ref_opcuda.available():
+            _low["status"] = "oracle/_ref not built"
+            return
+        ref = ref_opcuda.load()
+        p = C.c_ulonglong()
+        r = ref.ref_low_alloc(LOW_BYTES, C.byref(p))
+        _low["status"] = r
+        if r == 0:
+            _low["base"] = p.value
+    except OSError as e:  # the harness library cannot be loaded here
+        _low["status"] = str(e)
+
+
+@pytest.fixture(scope="session")
+def low_reservation():
+    """(base, size) of the session's memory below 4 GB, or the reason it is missing."""
+    return (_low.get("base"), LOW_BYTES, _low.get("status"))
+
+
 @pytest.fixture(scope="session")
 def cuda():
     import torch
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
+    if not _low:
+        _reserve_low_memory()
     from oplib_b200 import _lib
     _lib.load()
     return torch.device("cuda:0")

@@ -171,16 +171,14 @@ def test_sset_bit_exact_vs_reference_kernel(lib, ref, cuda):
 # sgemv4), run on memory placed below 4 GB of device address space
 
 @pytest.fixture(scope="module")
-def low(ref):
-    import ctypes as C
-    p = C.c_ulonglong()
-    size = 96 << 20
-    r = ref.ref_low_alloc(size, C.byref(p))
-    if r != 0:
-        pytest.skip(f"no device memory below 4 GB of address space here (ref_low_alloc: {r})")
-    assert 0 < p.value and p.value + size <= 1 << 32
-    yield ref_opcuda.LowArena(ref, p.value, size)
-    ref.ref_low_free_all()
+def low(ref, cuda, low_reservation):
+    """The session's memory below 4 GB (reserved when its first GPU test started); each
+    module using it starts carving from its base."""
+    base, size, status = low_reservation
+    if base is None:
+        pytest.skip(f"no device memory below 4 GB of address space here (ref_low_alloc: {status})")
+    assert 0 < base and base + size <= 1 << 32
+    return ref_opcuda.LowArena(ref, base, size)
 
 
 def _colmajor(a):
