@@ -31,6 +31,7 @@ def knobs(cuda):
     yield lib
     assert lib.opb_set_band_skip(1) == 0
     assert lib.opb_set_lolo_levels(8) == 0
+    assert lib.opb_set_fused_normalisation(0) == 0
 
 
 def _equal(a, b):
@@ -117,8 +118,11 @@ def test_sweep_extremes_within_1e5(knobs, sweep_extremes):
         b = Batch(lats, STRIKES, NMAT, PERIOD, DT0, mode=mode, autotune=True)
         q = b.execute().cpu().numpy()
         errs[(mode, lolo)] = [float(np.abs(q[j] - refs[i][0]).max()) for j, i in enumerate(pick)]
-        # the single-lattice solve applies the same rule
+        # the single-lattice solve applies the same rule (with the batch's fused row
+        # normalisation, so that the two differ only by the pricing's K-slices)
+        assert knobs.opb_set_fused_normalisation(8192) == 0
         qs, _ = lats[0].solve(STRIKES, NMAT, PERIOD, DT0, mode=mode)
+        assert knobs.opb_set_fused_normalisation(0) == 0
         assert np.abs(qs.cpu().numpy() - q[0]).max() < 1e-6
     from oplib_b200 import _lib
     assert _lib.load().opb_tc_error() == 0

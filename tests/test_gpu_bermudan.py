@@ -103,7 +103,7 @@ def test_bermudan_ragged_strike_count(cuda):
 
 
 @pytest.mark.parametrize("mode", ["fp16x3", "bf16x3", "fp32"])
-def test_batched_bermudan_matches_single_lattices(cuda, mode):
+def test_batched_bermudan_matches_single_lattices(cuda, fused_single, mode):
     """Seven uneven local-vol lattices (sizes 256..1024, three of them odd multiples of 128)
     priced together by opb_batch_execute_bermudan against one opb_lattice_bermudan per
     lattice, under every launch configuration of the squarings; and one lattice against

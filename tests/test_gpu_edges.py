@@ -150,7 +150,7 @@ def test_split_modes_on_sizes_off_the_tile_grid(cuda, mode, n):
     assert np.abs(qb.cpu().numpy() - Vb[O.nearest_node(x)]).max() < 1e-5
 
 
-def test_batch_of_one_lattice_matches_its_single_solve(cuda):
+def test_batch_of_one_lattice_matches_its_single_solve(cuda, fused_single):
     from oplib_b200.model import Batch, Lattice
     lat = Lattice.local_vol(n=384, level=0.25, skew=-0.1, width=0.6, rate=0.02, floor=0.01)
     K = np.linspace(0.8, 1.2, 8)
