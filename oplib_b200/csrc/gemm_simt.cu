@@ -149,6 +149,22 @@ __device__ __forceinline__ void sf_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Packed FP32 (sm_100): two independent FMAs per lane and instruction, each rounded as a
+// scalar fmaf, so every output still sums its products in k order with the same bits.
+__device__ __forceinline__ uint64_t f2_pack(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(uint64_t v, float &lo, float &hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
 __global__ void __launch_bounds__(SG_THREADS, 2) k_sgemm_pipe(SgemmArgs p) {
     extern __shared__ __align__(16) float sm[];
     const int z = blockIdx.z;
@@ -179,11 +195,12 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_sgemm_pipe(SgemmArgs p) {
         sf_commit();
     };
 
-    float acc[8][8];
+    // acc2[i][jp] holds the outputs (row i, columns 2jp and 2jp + 1) of this thread's 8 x 8
+    uint64_t acc2[8][4];
 #pragma unroll
     for (int i = 0; i < 8; i++)
 #pragma unroll
-        for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+        for (int j = 0; j < 4; j++) acc2[i][j] = 0ull;
 
     const int nk = p.K / SF_BK;
 #pragma unroll
@@ -211,18 +228,25 @@ __global__ void __launch_bounds__(SG_THREADS, 2) k_sgemm_pipe(SgemmArgs p) {
             for (int u = 0; u < 4; u++) {
                 const float4 b0 = *reinterpret_cast<const float4 *>(Bs + (kk + u) * SG_BN + tx * 4);
                 const float4 b1 = *reinterpret_cast<const float4 *>(Bs + (kk + u) * SG_BN + 64 + tx * 4);
-                const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+                const uint64_t b2[4] = {f2_pack(b0.x, b0.y), f2_pack(b0.z, b0.w), f2_pack(b1.x, b1.y),
+                                        f2_pack(b1.z, b1.w)};
 #pragma unroll
                 for (int i = 0; i < 8; i++) {
                     const float a = u == 0 ? a4[i].x : u == 1 ? a4[i].y : u == 2 ? a4[i].z : a4[i].w;
+                    const uint64_t a2 = f2_pack(a, a);
 #pragma unroll
-                    for (int j = 0; j < 8; j++) acc[i][j] = fmaf(a, b[j], acc[i][j]);
+                    for (int j = 0; j < 4; j++) acc2[i][j] = f2_fma(a2, b2[j], acc2[i][j]);
                 }
             }
         }
     }
     sf_wait<0>();
 
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) f2_unpack(acc2[i][j], acc[i][2 * j], acc[i][2 * j + 1]);
 #pragma unroll
     for (int i = 0; i < 8; i++) {
         const int r = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
