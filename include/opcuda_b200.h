@@ -338,9 +338,13 @@ int opb_batch_launches(const opb_batch_plan *plan);
  * (GELU) from (level, skew, width, kappa, rho, r, log-moneyness, T) to implied vol.  theta: FP32
  * master parameters (layer l: W [out x in] row-major then b); training uses BF16-rounded
  * working weights thb (FP32 storage), FP32 activations, Adam on theta.  loss receives the sum
- * of squared errors. */
+ * of squared errors.  The hidden layers' training products run on the tensor cores as
+ * split-BF16 products (activations and gradients as hi + lo parts, FP32 accumulation) when
+ * B is a multiple of 128; the first and output layers on SIMT kernels. */
 int opb_mlp_param_count(void);
 long long opb_mlp_workspace_floats(int B);
+/* new: 1 (default) tensor-core training products as above, 0 SIMT FP32 throughout */
+int opb_mlp_set_tensor_cores(int on);
 int opb_mlp_init(float *theta, unsigned long long seed);
 int opb_mlp_round(const float *theta, float *theta_bf, void *theta_b16);
 int opb_mlp_forward(const float *thb, const float *X, int B, float *ws, float *y);

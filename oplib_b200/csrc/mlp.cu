@@ -7,8 +7,9 @@
 // Parameters live in one flat FP32 master vector theta (layer l: W_l [out x in] row-major,
 // then b_l [out]); training uses BF16-rounded working weights (kept as FP32 values), FP32
 // activations and gradients, and Adam on the FP32 master copy.  All kernels are this
-// project's: SIMT GEMMs (gemm_simt.cu, with transpose flags) plus the fused element-wise
-// kernels below.  Batched inference of the trained network runs through
+// project's: the hidden layers' products on the tensor cores (gemm_tc.cu, split-BF16 parts
+// of the activations and gradients), the first and output layers on SIMT GEMMs
+// (gemm_simt.cu, with transpose flags), plus the fused element-wise kernels below.  Batched inference of the trained network runs through
 // opb_mlp_infer (BF16 weights and activations, FP32 accumulation).
 #include <cuda_bf16.h>
 
@@ -85,14 +86,17 @@ __device__ __forceinline__ float gelu_grad(float z) {
     return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
-// Z += b (per column), H = GELU(Z).  Z, H: [B x n] row-major.
+// Z += b (per column), H = GELU(Z).  Z, H: [B x n] row-major.  H (optional) in FP32 and/or
+// its BF16 parts Hhi / Hlo (optional, for the tensor-core products).
 __global__ void k_bias_gelu(long long total, int n, float *__restrict__ Z, const float *__restrict__ b,
-                            float *__restrict__ H) {
+                            float *__restrict__ H, __nv_bfloat16 *__restrict__ Hhi, __nv_bfloat16 *__restrict__ Hlo) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
         const float z = Z[i] + b[i % n];
         Z[i] = z;
-        H[i] = gelu(z);
+        const float h = gelu(z);
+        if (H) H[i] = h;
+        if (Hhi) split2(h, Hhi[i], Hlo[i]);
     }
 }
 
@@ -121,42 +125,82 @@ __global__ void k_out_layer(int B, const float *__restrict__ H, const float *__r
     if (loss_part && lane == 0) atomicAdd(loss_part, se);
 }
 
-// dZ = dH * GELU'(Z)
+// dZ = dH * GELU'(Z); its BF16 parts (optional) row-major too.
 __global__ void k_gelu_back(long long total, const float *__restrict__ Z, const float *__restrict__ dH,
-                            float *__restrict__ dZ) {
+                            float *__restrict__ dZ, __nv_bfloat16 *__restrict__ dZhi, __nv_bfloat16 *__restrict__ dZlo) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x)
-        dZ[i] = dH[i] * gelu_grad(Z[i]);
-}
-
-// db[c] = sum_r dZ[r, c] (block per column group of 32, deterministic order)
-__global__ void k_colsum(int B, int n, const float *__restrict__ dZ, float *__restrict__ db) {
-    __shared__ float red[8][33];
-    const int c = blockIdx.x * 32 + (threadIdx.x & 31), rg = threadIdx.x >> 5;  // 8 row groups
-    float s = 0.f;
-    if (c < n)
-        for (int r = rg; r < B; r += 8) s += dZ[(long long)r * n + c];
-    red[rg][threadIdx.x & 31] = s;
-    __syncthreads();
-    if (rg == 0 && c < n) {
-        float t = 0.f;
-        for (int i = 0; i < 8; i++) t += red[i][threadIdx.x & 31];
-        db[c] = t;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float g = dH[i] * gelu_grad(Z[i]);
+        dZ[i] = g;
+        if (dZhi) split2(g, dZhi[i], dZlo[i]);
     }
 }
 
-// Output-layer weight gradient dw5[j] = sum_r dy[r] H4[r, j] and db5 = sum_r dy[r].
-__global__ void k_out_grad(int B, const float *__restrict__ H, const float *__restrict__ dy, float *__restrict__ dw,
-                           float *__restrict__ db) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j > MLP_H) return;
+// First-layer weight gradient dW[c][k] = sum_r dZ[r, c] X[r, k] (n columns, 8 inputs) in the
+// two fixed-order passes of the column sums: block (x, y) forms the 8 sums of its rows for 32
+// columns into part[(y * 8 + k) * n + c]; k_wgrad_in_fin adds the row blocks in order.
+__global__ void k_wgrad_in_part(int B, int n, int rows_per, const float *__restrict__ dZ, const float *__restrict__ X,
+                                float *__restrict__ part) {
+    __shared__ float red[8][MLP_IN][33];
+    const int lane = threadIdx.x & 31, c = blockIdx.x * 32 + lane, rg = threadIdx.x >> 5;
+    const int r0 = blockIdx.y * rows_per, r1 = min(B, r0 + rows_per);
+    float s[MLP_IN];
+#pragma unroll
+    for (int k = 0; k < MLP_IN; k++) s[k] = 0.f;
+    if (c < n)
+        for (int r = r0 + rg; r < r1; r += 8) {
+            const float g = dZ[(long long)r * n + c];
+#pragma unroll
+            for (int k = 0; k < MLP_IN; k++) s[k] = fmaf(g, X[(long long)r * MLP_IN + k], s[k]);
+        }
+#pragma unroll
+    for (int k = 0; k < MLP_IN; k++) red[rg][k][lane] = s[k];
+    __syncthreads();
+    if (rg == 0 && c < n) {
+        for (int k = 0; k < MLP_IN; k++) {
+            float t = 0.f;
+            for (int i = 0; i < 8; i++) t += red[i][k][lane];
+            part[((long long)blockIdx.y * MLP_IN + k) * n + c] = t;
+        }
+    }
+}
+
+__global__ void k_wgrad_in_fin(int nb, int n, const float *__restrict__ part, float *__restrict__ dW) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // i = c * 8 + k
+    if (i >= n * MLP_IN) return;
+    const int c = i / MLP_IN, k = i - c * MLP_IN;
+    float t = 0.f;
+    for (int b = 0; b < nb; b++) t += part[((long long)b * MLP_IN + k) * n + c];
+    dW[i] = t;
+}
+
+// Weighted column sums over the batch in two fixed-order passes, so that the reduction
+// spreads over many SMs: block (x, y) sums rows [y * rows_per, (y + 1) * rows_per) of 32
+// columns (8 row groups, then in order) into part[y * n + c]; k_colsum_fin adds the row
+// blocks in order.  w (optional): row weights.
+__global__ void k_colsum_part(int B, int n, int rows_per, const float *__restrict__ M, const float *__restrict__ w,
+                              float *__restrict__ part) {
+    __shared__ float red[8][33];
+    const int lane = threadIdx.x & 31, c = blockIdx.x * 32 + lane, rg = threadIdx.x >> 5;
+    const int r0 = blockIdx.y * rows_per, r1 = min(B, r0 + rows_per);
     float s = 0.f;
-    if (j < MLP_H)
-        for (int r = 0; r < B; r++) s = fmaf(dy[r], H[(long long)r * MLP_H + j], s);
-    else
-        for (int r = 0; r < B; r++) s += dy[r];
-    if (j < MLP_H) dw[j] = s;
-    else db[0] = s;
+    if (c < n)
+        for (int r = r0 + rg; r < r1; r += 8) s = w ? fmaf(w[r], M[(long long)r * n + c], s) : s + M[(long long)r * n + c];
+    red[rg][lane] = s;
+    __syncthreads();
+    if (rg == 0 && c < n) {
+        float t = 0.f;
+        for (int i = 0; i < 8; i++) t += red[i][lane];
+        part[(long long)blockIdx.y * n + c] = t;
+    }
+}
+
+__global__ void k_colsum_fin(int nb, int n, const float *__restrict__ part, float *__restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    float t = 0.f;
+    for (int b = 0; b < nb; b++) t += part[(long long)b * n + c];
+    out[c] = t;
 }
 
 // dH4 = dy (outer) w5
@@ -244,6 +288,10 @@ namespace {
 struct MlpWs {  // training workspace carve (floats)
     float *Z[4], *H[4], *dZ, *dH, *y, *dy, *part;
     double *loss;
+    // 16-bit parts for the tensor-core products of the hidden layers 1..3 (split2, BF16):
+    // Hp[l][0/1] of H[l] (l = 0..2, B x 256 row-major), dZp of dZ (B x 256), dZt of dZ^T
+    // (256 x B), Wp[l][0/1] of the working weights W_{l+1} (256 x 256, exact BF16: lo = 0)
+    __nv_bfloat16 *Hp[3][2], *dZp[2], *dZt[2], *Wp[3][2];
 };
 
 // Weight gradients reduce over the batch (K = B): split into at most MLP_KSPLIT chunks,
@@ -268,7 +316,42 @@ MlpWs carve_mlp(float *ws, int B) {
     w.part = ws + o; o += (size_t)MLP_KSPLIT * MLP_H * MLP_H;
     o = (o + 1) & ~size_t(1);
     w.loss = reinterpret_cast<double *>(ws + o);
+    o += 2;
+    // parts: 64-float (256-byte) aligned pieces, each n bf16 values in n / 2 floats
+    auto parts = [&](size_t n) {
+        o = (o + 63) & ~size_t(63);
+        __nv_bfloat16 *q = reinterpret_cast<__nv_bfloat16 *>(ws + o);
+        o += n / 2;
+        return q;
+    };
+    const size_t bh = (size_t)B * MLP_H;
+    for (int l = 0; l < 3; l++)
+        for (int k = 0; k < 2; k++) w.Hp[l][k] = parts(bh);
+    for (int k = 0; k < 2; k++) w.dZp[k] = parts(bh);
+    for (int k = 0; k < 2; k++) w.dZt[k] = parts(bh);
+    for (int l = 0; l < 3; l++)
+        for (int k = 0; k < 2; k++) w.Wp[l][k] = parts((size_t)MLP_H * MLP_H);
     return w;
+}
+
+// The hidden layers' products run on the tensor cores (split-BF16, three products, FP32
+// accumulation) when the batch is a multiple of 128 rows; the first layer (8 inputs) and
+// the output layer stay on the SIMT kernels.  opb_mlp_set_tensor_cores(0): SIMT throughout.
+int g_mlp_tc = 1;
+bool mlp_tc(int B) { return g_mlp_tc && B % 128 == 0; }
+
+// C[M x N] = A[M x K] . B^T with A's parts row-major (lda) and B's parts N x K row-major
+// (b_kn = 0) or K x N row-major (b_kn = 1); ksplit > 1: K-slices into C + s * M * N.
+int mlp_tc_gemm(int M, int N, int K, __nv_bfloat16 *const *A, long long lda, __nv_bfloat16 *const *Bp,
+                long long ldb, int b_kn, float *C, int ksplit, cudaStream_t s) {
+    TcGemmArgs a{};
+    a.M = M; a.N = N; a.K = K; a.Ahi = A[0]; a.Alo = A[1]; a.lda = lda; a.Bhi = Bp[0]; a.Blo = Bp[1]; a.ldb = ldb;
+    a.b_kn = b_kn; a.C = C; a.ldc = N; a.alpha = 1.f; a.beta = 0.f;
+    if (ksplit > 1) {
+        a.ksplit = ksplit;
+        a.c_slice = (long long)M * N;
+    }
+    return launch_tc_gemm(a, s);
 }
 
 __global__ void k_sum_parts(int nparts, long long n, const float *__restrict__ part, float *__restrict__ out) {
@@ -302,6 +385,15 @@ int mlp_weight_grad(int out, int in, int B, const float *dZ, const float *X, flo
     return (int)cudaGetLastError();
 }
 
+// out[c] = sum_r (w[r] *) M[r, c] for c < n over B rows (part: scratch of 32 n floats).
+int mlp_colsum(int B, int n, const float *M, const float *w, float *part, float *out, cudaStream_t s) {
+    const int nb = B < 32 * 128 ? (B + 127) / 128 : 32;
+    const int rows_per = (B + nb - 1) / nb;
+    k_colsum_part<<<dim3((n + 31) / 32, nb), 256, 0, s>>>(B, n, rows_per, M, w, part);
+    k_colsum_fin<<<(n + 255) / 256, 256, 0, s>>>(nb, n, part, out);
+    return (int)cudaGetLastError();
+}
+
 int grid_ew(long long n) {
     long long b = (n + 255) / 256;
     long long cap = 8LL * num_sms();
@@ -316,13 +408,25 @@ int grid_ew(long long n) {
 
 int mlp_forward(const float *thb, const float *X, int B, MlpWs &w, cudaStream_t s) {
     const MlpLayout L = mlp_layout();
+    const bool tc = mlp_tc(B);
+    if (tc)
+        for (int l = 1; l < 4; l++)
+            MT(launch_split(MLP_H, MLP_H, thb + L.w[l], MLP_H, w.Wp[l - 1][0], w.Wp[l - 1][1], nullptr, nullptr, 0,
+                            s));
     const float *in = X;
     for (int l = 0; l < 4; l++) {
         // Z = in . W^T  (W stored out x in: the TB form)
-        MT(sgemm_rm_t(false, true, B, L.out[l], L.in[l], 1.f, in, L.in[l], thb + L.w[l], L.in[l], 0.f, w.Z[l],
-                      L.out[l], s));
+        if (tc && l > 0)
+            MT(mlp_tc_gemm(B, MLP_H, MLP_H, w.Hp[l - 1], MLP_H, w.Wp[l - 1], MLP_H, 0, w.Z[l], 1, s));
+        else
+            MT(sgemm_rm_t(false, true, B, L.out[l], L.in[l], 1.f, in, L.in[l], thb + L.w[l], L.in[l], 0.f, w.Z[l],
+                          L.out[l], s));
         const long long tot = (long long)B * L.out[l];
-        k_bias_gelu<<<grid_ew(tot), 256, 0, s>>>(tot, L.out[l], w.Z[l], thb + L.b[l], w.H[l]);
+        // with the tensor cores, layers 0..2 store only their activations' parts (the next
+        // product's A and the weight gradient's B); the last one FP32 for the output layer
+        const bool parts = tc && l < 3;
+        k_bias_gelu<<<grid_ew(tot), 256, 0, s>>>(tot, L.out[l], w.Z[l], thb + L.b[l], parts ? nullptr : w.H[l],
+                                                 parts ? w.Hp[l][0] : nullptr, parts ? w.Hp[l][1] : nullptr);
         in = w.H[l];
     }
     return (int)cudaGetLastError();
@@ -334,7 +438,18 @@ OPB_API int opb_mlp_param_count(void) { return MLP_NPARAM; }
 
 // floats of training workspace for batch B
 OPB_API long long opb_mlp_workspace_floats(int B) {
-    return 10LL * B * MLP_H + 2LL * B + 4 + (long long)MLP_KSPLIT * MLP_H * MLP_H + 8;
+    // FP32 buffers, then the tensor-core parts (5 B x 256 + 3 x 256 x 256 floats of BF16 pairs)
+    // with their alignment
+    return 10LL * B * MLP_H + 2LL * B + 4 + (long long)MLP_KSPLIT * MLP_H * MLP_H + 8 + 5LL * B * MLP_H +
+           3LL * MLP_H * MLP_H + 14 * 64;
+}
+
+// 1 (default): the hidden layers' training products on the tensor cores (batches of a
+// multiple of 128 rows); 0: SIMT FP32 throughout.
+OPB_API int opb_mlp_set_tensor_cores(int on) {
+    OPB_REQUIRE(on == 0 || on == 1, OPB_E_ARG);
+    g_mlp_tc = on;
+    return set_status(OPB_OK);
 }
 
 OPB_API int opb_mlp_init(float *theta, unsigned long long seed) {
@@ -378,17 +493,45 @@ OPB_API int opb_mlp_loss_grad(const float *thb, const float *X, const float *t, 
     MT((int)cudaMemsetAsync(w.loss, 0, sizeof(double), s));
     k_out_layer<<<(B * 32 + 255) / 256, 256, 0, s>>>(B, w.H[3], thb + L.w[4], thb + L.b[4], w.y, t, w.dy, w.loss);
     // output layer
-    k_out_grad<<<(MLP_H + 1 + 255) / 256 * 1 + 1, 256, 0, s>>>(B, w.H[3], w.dy, grad + L.w[4], grad + L.b[4]);
+    // (column sums over the batch in two fixed-order passes over many blocks)
+    MT(mlp_colsum(B, MLP_H, w.H[3], w.dy, w.part, grad + L.w[4], s));
+    MT(mlp_colsum(B, 1, w.dy, nullptr, w.part, grad + L.b[4], s));
     k_out_back<<<grid_ew((long long)B * MLP_H), 256, 0, s>>>(B, w.dy, thb + L.w[4], w.dH);
+    const bool tc = mlp_tc(B);
+    // weight-gradient K-slices on the tensor cores: at most MLP_KSPLIT, dividing B / 64
+    int ks = B / 64 < MLP_KSPLIT ? B / 64 : MLP_KSPLIT;
+    while (ks > 1 && (B / 64) % ks) ks--;
     for (int l = 3; l >= 0; l--) {
         const long long tot = (long long)B * L.out[l];
-        k_gelu_back<<<grid_ew(tot), 256, 0, s>>>(tot, w.Z[l], w.dH, w.dZ);
-        // dW = dZ^T . in  (A = dZ stored B x out: the TA form)
+        const bool parts = tc && l > 0;
+        k_gelu_back<<<grid_ew(tot), 256, 0, s>>>(tot, w.Z[l], w.dH, w.dZ, parts ? w.dZp[0] : nullptr,
+                                                 parts ? w.dZp[1] : nullptr);
         const float *in = l > 0 ? w.H[l - 1] : X;
-        MT(mlp_weight_grad(L.out[l], L.in[l], B, w.dZ, in, grad + L.w[l], w.part, s));
-        k_colsum<<<(L.out[l] + 31) / 32, 256, 0, s>>>(B, L.out[l], w.dZ, grad + L.b[l]);
-        if (l > 0) MT(sgemm_rm_t(false, false, B, L.in[l], L.out[l], 1.f, w.dZ, L.out[l], thb + L.w[l], L.in[l], 0.f,
-                                 w.dH, L.in[l], s));
+        if (parts) {
+            // dZ's parts transposed (for dW; the row-major ones, for dH, came with dZ)
+            MT(launch_split(B, MLP_H, w.dZ, MLP_H, nullptr, nullptr, w.dZt[0], w.dZt[1], B, s));
+            // dW = dZ^T . in: A = dZ^T's parts (256 x B), B = in's parts read K x N (B x 256)
+            MT(mlp_tc_gemm(MLP_H, MLP_H, B, w.dZt, B, w.Hp[l - 1], MLP_H, 1, w.part, ks, s));
+            k_sum_parts<<<grid_ew((long long)MLP_H * MLP_H), 256, 0, s>>>(ks, (long long)MLP_H * MLP_H, w.part,
+                                                                          grad + L.w[l]);
+        } else if (l == 0) {
+            // dW = dZ^T . X (8 inputs): eight weighted column sums
+            const int nb = B < 32 * 128 ? (B + 127) / 128 : 32;
+            const int rows_per = (B + nb - 1) / nb;
+            k_wgrad_in_part<<<dim3(MLP_H / 32, nb), 256, 0, s>>>(B, MLP_H, rows_per, w.dZ, X, w.part);
+            k_wgrad_in_fin<<<(MLP_H * MLP_IN + 255) / 256, 256, 0, s>>>(nb, MLP_H, w.part, grad + L.w[0]);
+        } else {
+            // dW = dZ^T . in  (A = dZ stored B x out: the TA form)
+            MT(mlp_weight_grad(L.out[l], L.in[l], B, w.dZ, in, grad + L.w[l], w.part, s));
+        }
+        MT(mlp_colsum(B, L.out[l], w.dZ, nullptr, w.part, grad + L.b[l], s));
+        if (l > 0) {
+            // dH = dZ . W: B = W's parts read K x N (out x in)
+            if (tc) MT(mlp_tc_gemm(B, MLP_H, MLP_H, w.dZp, MLP_H, w.Wp[l - 1], MLP_H, 1, w.dH, 1, s));
+            else
+                MT(sgemm_rm_t(false, false, B, L.in[l], L.out[l], 1.f, w.dZ, L.out[l], thb + L.w[l], L.in[l], 0.f,
+                              w.dH, L.in[l], s));
+        }
     }
     if (loss) {
         // mean of the squared errors
