@@ -294,7 +294,8 @@ int opb_set_fused_normalisation(int max_d);
 /* ------------------------------------------------------------------ batched lattices */
 typedef struct opb_batch_desc {
     int nlat;
-    const int *d;            /* host [nlat], multiples of 128 for OPB_BF16X3, <= 8064 */
+    const int *d;            /* host [nlat], 2..8064 (split modes: solved padded to the next
+                                multiple of 128 with absorbing states) */
     const int *y0;           /* host [nlat] */
     const int *niter;        /* host [nlat], >= 1 */
     const double *dt;        /* host [nlat] */

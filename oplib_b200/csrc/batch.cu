@@ -92,6 +92,13 @@ struct opb_batch_plan {
     int ell_width = 0;
     const int *cols = nullptr;
     const double *vals = nullptr, *x = nullptr, *strikes = nullptr;
+    // lattices off the 128 grid (split modes): the caller's arrays, padded into these before
+    // every execution (cols / vals / x then point to the padded copies)
+    bool padded = false;
+    const int *cols_src = nullptr;
+    const double *vals_src = nullptr, *x_src = nullptr;
+    int *cols_pad = nullptr;
+    double *vals_pad = nullptr, *x_pad = nullptr;
     double period = 0.0;
     // device tables
     opb::BatchLattice *lats = nullptr;
@@ -148,12 +155,36 @@ int check_batch(const opb_batch_desc *b, int mode) {
     if (mode < 0 || mode > 3) return OPB_E_ARG;
     for (int i = 0; i < b->nlat; i++) {
         int d = b->d[i];
-        if (d < 128 || d > 8064 || b->y0[i] < 0 || b->y0[i] >= d || b->niter[i] < 1 || !(b->dt[i] > 0.0))
+        if (d < 2 || d > 8064 || b->y0[i] < 0 || b->y0[i] >= d || b->niter[i] < 1 || !(b->dt[i] > 0.0))
             return OPB_E_ARG;
-        if (tc_mode_b(mode) && d % 128) return OPB_E_UNSUPPORTED;
     }
     return OPB_OK;
 }
+
+// The split modes run every lattice on a multiple of 128 states: a lattice of another size
+// is solved as one padded with absorbing states (zero generator rows and columns), whose
+// rows of every product, renormalisation and price are the unpadded lattice's (no state of
+// the lattice reaches a padding state).
+std::vector<int> plan_sizes(const opb_batch_desc *b, int mode) {
+    std::vector<int> d(b->d, b->d + b->nlat);
+    if (tc_mode_b(mode))
+        for (int &v : d) v = (v + 127) / 128 * 128;
+    return d;
+}
+
+bool plan_padded(const opb_batch_desc *b, int mode) {
+    if (!tc_mode_b(mode)) return false;
+    for (int i = 0; i < b->nlat; i++)
+        if (b->d[i] % 128) return true;
+    return false;
+}
+
+// The layout works on the plan's (padded) sizes: a copy of the descriptor with them.
+struct PlanDesc {
+    std::vector<int> d;
+    opb_batch_desc desc;
+    PlanDesc(const opb_batch_desc *b, int mode) : d(plan_sizes(b, mode)), desc(*b) { desc.d = d.data(); }
+};
 
 // Layout of all device buffers and tables; with base == nullptr it only measures.
 // K-blocks of 64 that a squaring tile (rows [m0, m0 + tm), columns [n0, n0 + tn)) issues at
@@ -174,7 +205,7 @@ int host_band_kblocks(int h0, int level, int m0, int tm, int n0, int tn, int K) 
 // work lists of the longest-first configurations are then ordered by the K-blocks each item
 // issues at that level, longest first.
 size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, std::vector<uint32_t> *work_out,
-              const std::vector<int> *bands = nullptr) {
+              const std::vector<int> *bands = nullptr, bool padded = false) {
     Carve c{base, 0};
     const int n = b->nlat;
     std::vector<long long> off(n + 1, 0);
@@ -302,8 +333,18 @@ size_t layout(const opb_batch_desc *b, int mode, opb_batch_plan *P, char *base, 
         for (int i = 0; i < n; i++) inter[lv] |= b->niter[i] > lv + 1 ? 1 : 0;
     }
     uint32_t *work = c.take<uint32_t>(W.size());
+    // padded copies of the generator and spot values (lattices off the 128 grid)
+    int *cols_pad = nullptr;
+    double *vals_pad = nullptr, *x_pad = nullptr;
+    if (padded) {
+        cols_pad = c.take<int>((size_t)off[n] * b->ell_width);
+        vals_pad = c.take<double>((size_t)off[n] * b->ell_width);
+        x_pad = c.take<double>((size_t)off[n]);
+    }
     size_t total = c.used + 256;
     if (!P) return total;
+    P->padded = padded;
+    P->cols_pad = cols_pad; P->vals_pad = vals_pad; P->x_pad = x_pad;
 
     // ---- fill the plan and host copies of the tables
     P->nlat = n; P->nmat = b->nmat; P->nK = b->nK; P->ldk = ldk; P->maxn = maxn;
@@ -336,7 +377,8 @@ using opb::set_status;
 
 OPB_API unsigned long long opb_batch_workspace_size(const opb_batch_desc *b, int mode) {
     if (check_batch(b, mode) != OPB_OK) return 0;
-    return (unsigned long long)layout(b, mode, nullptr, nullptr, nullptr);
+    PlanDesc pd(b, mode);
+    return (unsigned long long)layout(&pd.desc, mode, nullptr, nullptr, nullptr, nullptr, plan_padded(b, mode));
 }
 
 // Builds the plan: tables, tensor maps and work lists are written into `workspace`
@@ -346,7 +388,9 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     int c = check_batch(b, mode);
     if (c != OPB_OK) return set_status(c);
     OPB_REQUIRE(workspace && out, OPB_E_NULL);
-    size_t need = layout(b, mode, nullptr, nullptr, nullptr);
+    const bool padded = plan_padded(b, mode);
+    PlanDesc pd(b, mode);
+    size_t need = layout(&pd.desc, mode, nullptr, nullptr, nullptr, nullptr, padded);
     OPB_REQUIRE(ws_bytes >= need, OPB_E_ARG);
     char *base = reinterpret_cast<char *>(workspace);
     base += (256 - (reinterpret_cast<uintptr_t>(base) & 255)) & 255;
@@ -379,8 +423,15 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
             ro += b->d[i];
         }
     }
+    // from here on the plan's (padded) sizes; cb keeps the caller's
+    const opb_batch_desc *cb = b;
+    b = &pd.desc;
     std::vector<uint32_t> W;
-    layout(b, mode, P, base, &W, &bands);
+    layout(b, mode, P, base, &W, &bands, padded);
+    if (padded) {
+        P->cols_src = cb->gen_cols; P->vals_src = cb->gen_vals; P->x_src = cb->x;
+        P->cols = P->cols_pad; P->vals = P->vals_pad; P->x = P->x_pad;
+    }
     if (!tc_mode_b(mode)) {
         P->nlat = n; P->nmat = b->nmat; P->nK = b->nK;
         long long roff = 0;
@@ -425,13 +476,15 @@ OPB_API int opb_batch_plan_create(const opb_batch_desc *b, int mode, void *works
     P->f16 = f16;
     const float un2 = f16 ? 1.f / (F16S * F16S) : 1.f, un1 = f16 ? 1.f / F16S : 1.f;
     size_t eo = 0, po = 0;
-    long long ro = 0;
+    long long ro = 0, so = 0;
     int rc_status = OPB_OK;
     for (int i = 0; i < n && rc_status == OPB_OK; i++) {
         const int d = b->d[i];
         const size_t dd = (size_t)d * d;
         opb::BatchLattice &L = lats[i];
         L.d = d; L.y0 = b->y0[i]; L.row_off = ro; L.dt = b->dt[i]; L.rate = b->rate[i]; L.period = b->period;
+        L.d_src = cb->d[i]; L.src_off = so;
+        so += cb->d[i];
         L.E = E + eo; L.Pa = Pa + eo; L.V = V + (size_t)ro * P->ldk;
         L.GThi = Gh + (size_t)ro * P->ldk; L.GTlo = Gl + (size_t)ro * P->ldk;
         L.gscale = gsc + i;
@@ -568,7 +621,13 @@ int chain_gemm(opb_batch_plan *P, int cfg, cudaStream_t s, int set = 0, bool sca
 int batch_square(opb_batch_plan *P, cudaStream_t s) {
     const int cfg = P->cfg, bn = CFG_BN[cfg], pdiv = bn < 128 ? bn : 128;
     const float ss = P->f16 ? F16S : 0.f;
-    int r = (int)cudaMemsetAsync(P->E_base, 0, P->E_bytes, s);
+    int r = 0;
+    // lattices off the 128 grid: the caller's generators and spot values into the padded rows
+    // (every execution: a calibration rewrites the generators' values between runs)
+    if (P->padded)
+        r = opb::launch_pad_batched(P->lats, P->nlat, P->total_rows, P->ell_width, P->cols_src, P->vals_src,
+                                    P->x_src, P->cols_pad, P->vals_pad, P->x_pad, s);
+    if (r == 0) r = (int)cudaMemsetAsync(P->E_base, 0, P->E_bytes, s);
     // the B part set starts zeroed: a level skips the output tiles outside its operands'
     // band, which must read as zeros when the next level issues their K-blocks
     if (r == 0) r = (int)cudaMemsetAsync(P->B_hi, 0, P->B_bytes, s);
@@ -712,5 +771,5 @@ OPB_API int opb_batch_launches(const opb_batch_plan *P) {
     int per_level = 0;  // GEMM, row fixes (some lattice squares on), renormalisation (some ends)
     for (int lv = 0; lv < P->maxn; lv++)
         per_level += 1 + (P->level_inter[lv] ? 1 : 0) + (P->rn_level[lv].n > 0 ? 1 : 0);
-    return 5 + per_level + 1 + (P->f16 ? 1 : 0) + 2 * P->nmat + 2 * (P->nmat - 1) + extra;
+    return 5 + (P->padded ? 1 : 0) + per_level + 1 + (P->f16 ? 1 : 0) + 2 * P->nmat + 2 * (P->nmat - 1) + extra;
 }

@@ -111,7 +111,17 @@ struct BatchLattice {
     int niter;            // squaring levels
     const double *partial;  // the last product's FP64 row-sum partials (partial[p*d + row])
     double2 *fix;         // per-row (s, inv) of the last product's deferred normalisation
+    // split modes, lattices of a size off the 128 grid: d above is the padded size (its states
+    // d_src..d-1 absorbing), d_src the caller's, src_off the lattice's first row in the
+    // caller's generator and spot arrays
+    int d_src;
+    long long src_off;
 };
+// Padded copies of the caller's ELL generator (w slots per row; padding rows get column -1)
+// and spot values (padding rows repeat the last state's) in the plan's padded row space.
+int launch_pad_batched(const BatchLattice *lats, int nlat, long long total_rows, int w, const int *cols_src,
+                       const double *vals_src, const double *x_src, int *cols, double *vals, double *x,
+                       cudaStream_t s);
 // Renormalisation staging: tiles in flight per block, and column tiles per batched work
 // item (a batched item renormalises the tiles chunk, chunk + renorm_chunks(d), ... of one
 // 64-row strip).

@@ -752,6 +752,43 @@ int launch_renorm_batched(const RenormProblem *probs, const uint32_t *work, int 
     return (int)cudaGetLastError();
 }
 
+// Thread per padded ELL slot (row-major rows of all lattices, w slots each).
+__global__ void k_pad_batched(const BatchLattice *__restrict__ lats, int nlat, long long total_rows, int w,
+                              const int *__restrict__ cols_src, const double *__restrict__ vals_src,
+                              const double *__restrict__ x_src, int *__restrict__ cols, double *__restrict__ vals,
+                              double *__restrict__ x) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= total_rows * w) return;
+    const long long grow = t / w;
+    const int k = (int)(t - grow * w);
+    int lo = 0, hi = nlat - 1;
+    while (lo < hi) {  // last lattice with row_off <= grow
+        int mid = (lo + hi + 1) >> 1;
+        if (lats[mid].row_off <= grow) lo = mid; else hi = mid - 1;
+    }
+    const BatchLattice &L = lats[lo];
+    const int y = (int)(grow - L.row_off);
+    if (y < L.d_src) {
+        const long long src = (L.src_off + y) * w + k;
+        cols[t] = cols_src[src];
+        vals[t] = vals_src[src];
+    } else {
+        cols[t] = -1;
+        vals[t] = 0.0;
+    }
+    if (k == 0) x[grow] = x_src[L.src_off + (y < L.d_src ? y : L.d_src - 1)];
+}
+
+int launch_pad_batched(const BatchLattice *lats, int nlat, long long total_rows, int w, const int *cols_src,
+                       const double *vals_src, const double *x_src, int *cols, double *vals, double *x,
+                       cudaStream_t s) {
+    const long long n = total_rows * w;
+    if (n <= 0) return OPB_OK;
+    k_pad_batched<<<(int)((n + 255) / 256), 256, 0, s>>>(lats, nlat, total_rows, w, cols_src, vals_src, x_src, cols,
+                                                          vals, x);
+    return (int)cudaGetLastError();
+}
+
 int launch_ek_batched(const BatchLattice *lats, int nlat, long long total_rows, int w, const int *cols,
                       const double *vals, cudaStream_t s) {
     long long n = total_rows * w;

@@ -264,8 +264,10 @@ class BatchDesc(C.Structure):
 
 
 class Batch:
-    """Many uneven lattices solved together: one persistent tensor-core launch and one
-    renormalisation launch per squaring level for all of them (``opb_batch_*``)."""
+    """Many uneven lattices solved together (``opb_batch_*``): one persistent tensor-core
+    launch per squaring level for all of them, whose epilogue writes the next level's
+    operand parts and applies the deferred row normalisation.  In the split modes a lattice
+    of a size off the 128 grid is solved padded with absorbing states."""
 
     def __init__(self, lattices: list, strikes, nmat: int, period: float, dt0: float, mode="bf16x3",
                  autotune: bool = True):

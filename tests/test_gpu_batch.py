@@ -109,10 +109,11 @@ def test_batch_fp32_mode(cuda):
 
 
 def test_batch_rejects_bad_sizes(cuda):
+    """Sizes off the 128 grid are padded; sizes beyond the plan's tables are refused."""
     from oplib_b200.model import Batch, Lattice
-    lats = [Lattice.local_vol(n=200, device=cuda)]
+    lats = [Lattice.local_vol(n=8128, device=cuda)]
     with pytest.raises(Exception):
-        Batch(lats, STRIKES, NMAT, PERIOD, DT0, mode="bf16x3")
+        Batch(lats, STRIKES, NMAT, PERIOD, DT0, mode="bf16x3", autotune=False)
 
 
 def test_batch_fp16x3_mode(cuda):
@@ -124,3 +125,31 @@ def test_batch_fp16x3_mode(cuda):
         err = np.abs(q[i] - _oracle_quotes(s)).max()
         print(f"fp16x3 lattice {i}: {err:.2e}")
         assert err <= 1e-5
+
+
+@pytest.mark.parametrize("mode", ["bf16x3", "fp16x3"])
+def test_batch_of_sizes_off_the_128_grid(cuda, fused_single, mode):
+    """Split-mode plans take lattices of any size: each is solved padded to the next multiple
+    of 128 with absorbing states, so its quotes match the FP64 oracle of the unpadded lattice
+    and the single-lattice solve (which pads the same way)."""
+    from oplib_b200.model import Batch, Lattice
+    specs = [dict(n=300, level=0.25, skew=0.1, width=0.5, rate=0.02, floor=0.01),
+             dict(n=200, level=0.15, skew=-0.2, width=0.3, rate=0.04, floor=0.01),
+             dict(n=640, level=0.35, skew=0.25, width=0.9, rate=0.0, floor=0.01),
+             dict(n=1000, level=0.2, skew=0.05, width=0.6, rate=0.03, floor=0.01)]
+    lats = [Lattice.local_vol(device=cuda, **s) for s in specs]
+    b = Batch(lats, STRIKES, NMAT, PERIOD, DT0, mode=mode, autotune=False)
+    for cfg in (0, 6):
+        b.set_config(cfg)
+        q = b.execute().cpu().numpy()
+        for i, (lat, spec) in enumerate(zip(lats, specs)):
+            err = np.abs(q[i] - _oracle_quotes(spec)).max()
+            assert err <= 1e-5, (cfg, spec["n"], err)
+            qs, _ = lat.solve(STRIKES, NMAT, PERIOD, DT0, mode=mode)
+            assert np.abs(q[i] - qs.cpu().numpy()).max() < 1e-6, (cfg, spec["n"])
+    qb = b.execute_bermudan(put=True).cpu().numpy()
+    for i, lat in enumerate(lats):
+        single = lat.bermudan(STRIKES, nmat=NMAT, period=PERIOD, dt0=DT0, mode=mode, put=True).cpu().numpy()
+        assert np.abs(qb[i] - single).max() < 1e-6
+    from oplib_b200 import _lib
+    assert _lib.load().opb_tc_error() == 0
