@@ -491,6 +491,22 @@ def surrogate_summary(args):
     return res
 
 
+def mc_summary(args):
+    """Config 2 beside the headline: the Monte Carlo of the LV(512) lattice, 2^20 paths x 504
+    daily steps, one MT19937 stream per path, barrier and Asian calls (one step = step-kernel
+    build + cumulative rows + guide table as one CUDA graph, then the MC kernel)."""
+    a = argparse.Namespace(**vars(args))
+    a.steps, a.warmup, a.mc_steps, a.cpu = 5, 3, 504, False
+    t0 = time.perf_counter()
+    line = run_mc(a)
+    keep = ["value", "unit", "ms_per_step", "mc_kernel_only", "with_state_output", "prices"]
+    res = {"metric": line["metric"], "config": line["config"]["workload"]}
+    res.update({k: line[k] for k in keep if k in line})
+    res["path_steps_per_s"] = res.pop("value")
+    res["wall_s"] = round(time.perf_counter() - t0, 1)
+    return res
+
+
 def _host_info():
     """Host threads and CPU model string (recorded with every CPU number)."""
     model = "unknown"
@@ -1221,8 +1237,8 @@ def run_refbench(args):
     put("sgemv_576x100", 2.0 * d * d / (ms * 1e-3) / 1e9, "GF/s")
     # ---- MT uniforms: 20 batches of 102,400 (25 per stream, 4096 streams)
     nb, ns = 20, 4096 * 25
-    mt = torch.zeros(4, dtype=torch.int32, device=dev)
-    seed = np.array([5489], dtype=np.uint32)
+    mt = torch.zeros(lib.opcuda_mc_status_sz(), dtype=torch.int32, device=dev)
+    seed = np.random.default_rng(5489).integers(0, 2**31 - 1, lib.opcuda_mc_nrng()).astype(np.uint32)
     assert lib.opcuda_mc_setseed(seed.ctypes.data, mt.data_ptr()) == 0
     unif = torch.empty(ns, device=dev)
     host = torch.empty(ns, dtype=torch.float32).pin_memory()
@@ -1633,6 +1649,10 @@ def main():
                 out["config3_sweep"] = sweep_summary(args)
             except Exception as e:  # a secondary figure must not cost the headline line
                 out["config3_sweep"] = {"error": f"{type(e).__name__}: {e}"[:300]}
+            try:
+                out["config2_mc"] = mc_summary(args)
+            except Exception as e:
+                out["config2_mc"] = {"error": f"{type(e).__name__}: {e}"[:300]}
             try:
                 out["config4_surrogate"] = surrogate_summary(args)
             except Exception as e:

@@ -375,14 +375,18 @@ int opcuda_sck(int d, int nm, uint64_t tpker_yy_m, uint64_t ctpker_yy_m);
  * the device analogue of CModel Host Double.cs:434-455 */
 int opb_sck_rm(int d, int nrows, const float *P, float *C);
 int opb_guide_table(int d, int nrows, int nb, const float *C, uint32_t *guide);
-/* replace oplib/opcuda/smc.cu:87-106 */
+/* replace oplib/opcuda/smc.cu:87-106: nrng = 4096 stream seeds, status record of
+ * 4 + 4096 int32 words */
 int opcuda_mc_load_mt_gpu(const char *MT_stream, long sz);
 int opcuda_mc_nrng(void);
 int opcuda_mc_status_sz(void);
-/* replaces oplib/opcuda/smc.cu:137-156: first uint32 at host_seedptr is the base seed;
- * mtptr is the device continuation record (opcuda_mc_status_sz() words) */
+/* replaces oplib/opcuda/smc.cu:137-156: host_seedptr holds opcuda_mc_nrng() = 4096 uint32
+ * stream seeds; mtptr is the device status record (opcuda_mc_status_sz() words: next path
+ * id and the seeds).  Path g (counted from this call) is path g / 4096 of stream g % 4096
+ * and draws from MT19937 init_genrand(seeds[g % 4096]) with g / 4096 added to mt[1]. */
 int opcuda_mc_setseed(uint64_t host_seedptr, uint64_t mtptr);
-/* replaces oplib/opcuda/smc.cu:610-656 (per-path MT19937 streams; any nk >= 1, d <= 32767) */
+/* replaces oplib/opcuda/smc.cu:610-656 (per-path MT19937 generators keyed from the stream
+ * seeds; any nk >= 1, d <= 32767) */
 int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk, int d, uint64_t ctpker_m_yy, uint64_t m_k,
                 uint64_t yhostptr);
 /* new, the device side of the reference's opcuda_mc1f + CMCEvaluator.eval pair
@@ -393,7 +397,8 @@ int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk, int d,
  * copied to the host; y_sk optional (0).  Blocking, as opcuda_mc1f. */
 int opcuda_mc1f_eval(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk, int d, uint64_t ctpker_m_yy,
                      uint64_t m_k, uint64_t cashflow, uint64_t knockout, uint64_t results);
-/* replaces oplib/opcuda/smc.cu:731-736 (nscen % 4096 == 0) */
+/* replaces oplib/opcuda/smc.cu:731-736 (nscen % 4096 == 0): stream s of the status
+ * record's 4096 writes nscen/4096 uniforms from init_genrand(seeds[s]) */
 int opcuda_mt_benchmark(uint64_t mtptr, uint64_t unif_ptr, int nscen);
 /* new: MT19937 Monte Carlo, path p seeded init_genrand(seed + path0 + p); see mc.cu.
  * Runs of up to 623 steps keep the generator in registers; longer runs hold the

@@ -3,7 +3,10 @@
 // Path p draws its uniforms from MT19937 seeded with init_genrand(seed + p) (Matsumoto &
 // Nishimura 1998; the seeding recurrence 1812433253*(x ^ x>>30) + i is the one the
 // reference's twisters use, oplib/opcuda/smc.cu:127-131) and consumes the first
-// genrand_int32 outputs in order, one per step.  Each step converts the output to
+// genrand_int32 outputs in order, one per step.  The reference-facing entry points seed
+// from a table of 4096 stream seeds instead (opcuda_mc_setseed): path p is path p / 4096 of
+// stream p % 4096, its generator MT19937 keyed by (seeds[p % 4096], p / 4096)
+// (mt19937.cuh).  Each step converts the output to
 // u = ((float)x + 1.0f) * 2^-32 in (0, 1] (oplib/opcuda/smc.cu:329) and moves to the
 // smallest state z with u < C[y, z], capped at d-1 (oplib/opcuda/smc.cu:336-350).
 //
@@ -18,13 +21,22 @@
 // Payoffs (discretely monitored down-and-out call, arithmetic-Asian call) are reduced per
 // path in registers and per block in FP64; the optional int16 state output uses the
 // reference's layout y_sk[path + npaths*k] (oplib/opcuda/smc.cu:331).
+#include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "lattice.h"
 #include "mt19937.cuh"
 
 namespace opb {
+
+// Stream seeds the reference-facing entry points take (the reference's MT_RNG_COUNT
+// twisters, oplib/opcuda/smc.cu:98-101).
+constexpr int kMcStreamsLog2 = 12;
+constexpr int kMcStreams = 1 << kMcStreamsLog2;
+// Status record: 4 header words, then the stream seeds.
+constexpr int kMcStatusHeader = 4;
 
 __device__ __forceinline__ float mt_uniform_open0(uint32_t x) {
     float f = __uint2float_rn(x);
@@ -41,6 +53,7 @@ struct McArgs {
     int nb;
     int d, y0, nsteps;
     uint32_t seed;
+    const uint32_t *seeds;   // optional [kMcStreams] stream seeds (replaces seed)
     unsigned long long path0;
     long long npaths;
     short *ypaths;           // optional, y[p + npaths*k]
@@ -62,12 +75,17 @@ __global__ void __launch_bounds__(256) k_mc(McArgs a) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     const float nbf = (float)a.nb;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < a.npaths; p += stride) {
-        const uint32_t seed = a.seed + (uint32_t)(a.path0 + (unsigned long long)p);
+        const unsigned long long g = a.path0 + (unsigned long long)p;
+        uint32_t seed = a.seed + (uint32_t)g, key1 = 0u;
+        if (a.seeds) {
+            seed = __ldg(a.seeds + (g & (kMcStreams - 1)));
+            key1 = (uint32_t)(g >> kMcStreamsLog2);
+        }
         int y = a.y0;
         double xmin = 1e300, xsum = 0.0, xlast = 0.0;
         double v = 0.0;
         bool alive = true;
-        mt19937_stream<ANY_LENGTH>(seed, a.nsteps, [&](int k, uint32_t bits) {
+        mt19937_stream<ANY_LENGTH>(seed, key1, a.nsteps, [&](int k, uint32_t bits) {
             const float u = mt_uniform_open0(bits);
             const float *row = a.C + (long long)y * a.rs + (a.m_k ? (long long)__ldg(a.m_k + k) * a.ms : 0LL);
             int lo = 0, hi = a.d - 1;
@@ -142,12 +160,15 @@ __global__ void k_reduce_pairs(int n, const double *__restrict__ in, double *__r
 
 // Uniform-generation throughput kernel (the gmt workload): stream s of nstreams writes
 // its first nper uniforms u = x * 2^-32 (oplib/opcuda/smc.cu:711-714) to
-// unif[s + nstreams*j].
+// unif[s + nstreams*j].  Stream s is seeded seeds[s] when a seed table is given (nstreams
+// <= its length), else seed + s.
 template <bool ANY_LENGTH>
-__global__ void __launch_bounds__(256) k_mt_bench(uint32_t seed, long long nstreams, int nper, float *__restrict__ unif) {
+__global__ void __launch_bounds__(256) k_mt_bench(uint32_t seed, const uint32_t *__restrict__ seeds,
+                                                  long long nstreams, int nper, float *__restrict__ unif) {
     long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (s >= nstreams) return;
-    mt19937_stream<ANY_LENGTH>(seed + (uint32_t)s, nper, [&](int j, uint32_t bits) {
+    const uint32_t sd = seeds ? __ldg(seeds + s) : seed + (uint32_t)s;
+    mt19937_stream<ANY_LENGTH>(sd, 0u, nper, [&](int j, uint32_t bits) {
         unif[s + nstreams * (long long)j] = __fmul_rn(__uint2float_rn(bits), 2.3283064365386963e-10f);
     });
 }
@@ -157,7 +178,7 @@ template <bool ANY_LENGTH>
 __global__ void k_mt_raw(uint32_t seed, long long nstreams, int n, uint32_t *__restrict__ out) {
     long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (s >= nstreams) return;
-    mt19937_stream<ANY_LENGTH>(seed + (uint32_t)s, n, [&](int j, uint32_t bits) { out[s * n + j] = bits; });
+    mt19937_stream<ANY_LENGTH>(seed + (uint32_t)s, 0u, n, [&](int j, uint32_t bits) { out[s * n + j] = bits; });
 }
 
 // The register-only generator up to 623 steps, the cursor/state-array one beyond; the
@@ -172,9 +193,9 @@ void launch_mc(int grid, const McArgs &a) {
         k_mc<true><<<grid, 256, 0, stream()>>>(a);
     }
 }
-void launch_mt_bench(int grid, uint32_t seed, long long nstreams, int nper, float *unif) {
-    if (nper <= kMtCursorMax) k_mt_bench<false><<<grid, 256, 0, stream()>>>(seed, nstreams, nper, unif);
-    else k_mt_bench<true><<<grid, 256, 0, stream()>>>(seed, nstreams, nper, unif);
+void launch_mt_bench(int grid, uint32_t seed, const uint32_t *seeds, long long nstreams, int nper, float *unif) {
+    if (nper <= kMtCursorMax) k_mt_bench<false><<<grid, 256, 0, stream()>>>(seed, seeds, nstreams, nper, unif);
+    else k_mt_bench<true><<<grid, 256, 0, stream()>>>(seed, seeds, nstreams, nper, unif);
 }
 
 int mc_grid(long long npaths) {
@@ -265,14 +286,18 @@ OPB_API int opb_mt19937_raw(uint32_t seed, long long nstreams, int n, uint32_t *
 
 // ---------------------------------------------------------------- reference MC entry points
 //
-// The reference keeps 4096 MT607 twister states in a device buffer between calls
-// (oplib/opcuda/smc.cu:118-156, 610-656).  Here the status buffer holds the generator's
-// continuation record instead: word 0 = base seed, words 1-2 = the next path id (64-bit).
-// Successive opcuda_mc1f calls continue with fresh paths, which keeps the reference's
-// "successive batches continue the same streams" contract with per-path MT19937 streams.
+// The reference keeps 4096 MT607 twister states in a device buffer between calls, each
+// seeded from one of 4096 host seeds (oplib/opcuda/smc.cu:118-156, 610-656); twister r
+// draws its paths one after another.  Here the status buffer holds a continuation record
+// and the seed table instead: word 0 = seeds[0], words 1-2 = the next path id (64-bit),
+// word 3 = 0, words 4 .. 4099 = the 4096 stream seeds.  Path g (counted over all calls
+// since opcuda_mc_setseed) is path g / 4096 of stream g % 4096, with its own MT19937 keyed
+// by (seeds[g % 4096], g / 4096), so every path can run on its own thread; successive
+// opcuda_mc1f calls continue with fresh paths, which keeps the reference's "successive
+// batches continue the same streams" contract.  Paths 0 .. 4095 are init_genrand(seeds[g]).
 
-OPB_API int opcuda_mc_nrng(void) { return 1 << 20; }   // independent streams per call (advisory)
-OPB_API int opcuda_mc_status_sz(void) { return 4; }    // uint32 words of continuation record
+OPB_API int opcuda_mc_nrng(void) { return kMcStreams; }                        // stream seeds setseed reads
+OPB_API int opcuda_mc_status_sz(void) { return kMcStatusHeader + kMcStreams; }  // int32 words of the record
 
 // Accepted for ABI compatibility: MT19937 needs no per-stream parameter file
 // (the reference's MersenneTwister.dat, oplib/opcuda/smc.cu:87-96).
@@ -282,14 +307,16 @@ OPB_API int opcuda_mc_load_mt_gpu(const char *MT_stream, long sz) {
     return set_status(OPB_OK);
 }
 
-// host_seedptr: host array whose first uint32 is the base seed (the reference passes
-// 4096 seeds, one per twister).  mtptr: device status buffer of opcuda_mc_status_sz() words.
+// host_seedptr: host array of opcuda_mc_nrng() = 4096 uint32 stream seeds (the
+// reference's layout).  mtptr: device status buffer of opcuda_mc_status_sz() words.
 OPB_API int opcuda_mc_setseed(uint64_t host_seedptr, uint64_t mtptr) {
     OPB_REQUIRE(host_seedptr != 0 && mtptr != 0, OPB_E_NULL);
-    uint32_t rec[4];
-    rec[0] = reinterpret_cast<const uint32_t *>(host_seedptr)[0];
-    rec[1] = rec[2] = rec[3] = 0;
-    OPB_TRY(cudaMemcpyAsync(reinterpret_cast<void *>(mtptr), rec, sizeof(rec), cudaMemcpyHostToDevice, stream()));
+    std::vector<uint32_t> rec(kMcStatusHeader + kMcStreams, 0u);
+    const uint32_t *seeds = reinterpret_cast<const uint32_t *>(host_seedptr);
+    std::copy(seeds, seeds + kMcStreams, rec.begin() + kMcStatusHeader);
+    rec[0] = seeds[0];
+    OPB_TRY(cudaMemcpyAsync(reinterpret_cast<void *>(mtptr), rec.data(), rec.size() * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, stream()));
     OPB_TRY(cudaStreamSynchronize(stream()));
     return set_status(OPB_OK);
 }
@@ -313,7 +340,8 @@ OPB_API int opcuda_mc1f(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, int nk
         McArgs a{};
         a.C = reinterpret_cast<const float *>(ctpker_m_yy);
         a.rs = 1; a.cs = d; a.m_k = reinterpret_cast<const int *>(m_k); a.ms = (long long)d * d;
-        a.d = d; a.y0 = y0; a.nsteps = nk; a.seed = rec[0]; a.path0 = path0; a.npaths = nscen;
+        a.d = d; a.y0 = y0; a.nsteps = nk; a.path0 = path0; a.npaths = nscen;
+        a.seeds = reinterpret_cast<const uint32_t *>(mtptr) + kMcStatusHeader;
         a.ypaths = reinterpret_cast<short *>(y_sk);
         launch_mc(mc_grid(nscen), a);
         OPB_TRY(cudaGetLastError());
@@ -349,7 +377,8 @@ OPB_API int opcuda_mc1f_eval(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, i
         McArgs a{};
         a.C = reinterpret_cast<const float *>(ctpker_m_yy);
         a.rs = 1; a.cs = d; a.m_k = reinterpret_cast<const int *>(m_k); a.ms = (long long)d * d;
-        a.d = d; a.y0 = y0; a.nsteps = nk; a.seed = rec[0]; a.path0 = path0; a.npaths = nscen;
+        a.d = d; a.y0 = y0; a.nsteps = nk; a.path0 = path0; a.npaths = nscen;
+        a.seeds = reinterpret_cast<const uint32_t *>(mtptr) + kMcStatusHeader;
         a.ypaths = reinterpret_cast<short *>(y_sk);
         a.cf = reinterpret_cast<const double *>(cashflow);
         a.ko = reinterpret_cast<const unsigned char *>(knockout);
@@ -365,18 +394,16 @@ OPB_API int opcuda_mc1f_eval(uint64_t mtptr, int y0, uint64_t y_sk, int nscen, i
     return set_status(OPB_OK);
 }
 
-// Uniform throughput benchmark (oplib/opcuda/smc.cu:664-736): nscen uniforms from
-// opcuda_mc_nrng-independent per-stream MT19937 generators -- 4096 streams of nscen/4096
-// values each, stream s seeded with base seed + s.
+// Uniform throughput benchmark (oplib/opcuda/smc.cu:664-736): nscen uniforms from the
+// 4096 streams of the status record, nscen/4096 values each, stream s an MT19937 seeded
+// init_genrand(seeds[s]) (the reference's twister s seeded seed[s]).
 OPB_API int opcuda_mt_benchmark(uint64_t mtptr, uint64_t unif_ptr, int nscen) {
     OPB_REQUIRE(mtptr != 0 && unif_ptr != 0, OPB_E_NULL);
-    OPB_REQUIRE(nscen >= 0 && nscen % 4096 == 0, OPB_E_ARG);
-    int nper = nscen / 4096;
+    OPB_REQUIRE(nscen >= 0 && nscen % kMcStreams == 0, OPB_E_ARG);
+    int nper = nscen / kMcStreams;
     if (nper == 0) return set_status(OPB_OK);
-    uint32_t rec[4];
-    OPB_TRY(cudaMemcpyAsync(rec, reinterpret_cast<const void *>(mtptr), sizeof(rec), cudaMemcpyDeviceToHost, stream()));
-    OPB_TRY(cudaStreamSynchronize(stream()));
-    launch_mt_bench(4096 / 256, rec[0], 4096, nper, reinterpret_cast<float *>(unif_ptr));
+    launch_mt_bench(kMcStreams / 256, 0u, reinterpret_cast<const uint32_t *>(mtptr) + kMcStatusHeader, kMcStreams,
+                    nper, reinterpret_cast<float *>(unif_ptr));
     return launch_check();
 }
 
@@ -385,7 +412,7 @@ OPB_API int opb_mt_uniforms(uint32_t seed, long long nstreams, int nper, float *
     OPB_REQUIRE(nstreams >= 0 && nper >= 1, OPB_E_ARG);
     if (nstreams == 0) return set_status(OPB_OK);
     OPB_REQUIRE(unif != nullptr, OPB_E_NULL);
-    launch_mt_bench((int)((nstreams + 255) / 256), seed, nstreams, nper, unif);
+    launch_mt_bench((int)((nstreams + 255) / 256), seed, nullptr, nstreams, nper, unif);
     return launch_check();
 }
 

@@ -2,6 +2,11 @@
 // init_genrand(seed): mt[0] = seed, mt[i] = 1812433253*(mt[i-1] ^ mt[i-1]>>30) + i, the
 // seeding recurrence the reference's twisters use (oplib/opcuda/smc.cu:127-131).
 //
+// Keyed seeding (key1 != 0): the same recurrence with key1 added to mt[1] before the
+// recurrence continues from it (mt[1] = 1812433253*(seed ^ seed>>30) + 1 + key1).  Two
+// (seed, key1) pairs give equal initial states only if both members are equal, so one
+// seed yields 2^32 distinct generators; key1 = 0 is init_genrand(seed).
+//
 // Two forms, bit-identical on the outputs they share:
 //
 // mt19937_first (n <= 623): the whole generator in registers.  The first 623 outputs of
@@ -61,15 +66,16 @@ OPB_MT_FN uint32_t mt_temper(uint32_t y) {
 }
 
 // Calls f(k, w_k) with the regenerated (untempered) state word w_k = mt'[k] for the first
-// n (<= 623) words of MT19937 seeded with `seed`; returns the initial word mt[n].
+// n (<= 623) words of MT19937 seeded with (seed, key1); returns the initial word mt[n].
 template <class F>
-OPB_MT_FN uint32_t mt19937_cursor_words(uint32_t seed, int n, F &&f) {
+OPB_MT_FN uint32_t mt19937_cursor_words(uint32_t seed, uint32_t key1, int n, F &&f) {
+    const uint32_t m1 = mt_init_next(seed, 1u) + key1;
     // cursor A at i: (a0, a1) = (mt[i], mt[i+1])
-    uint32_t a0 = seed, a1 = mt_init_next(seed, 1u);
+    uint32_t a0 = seed, a1 = m1;
     // cursor B at i + 397
-    uint32_t b = seed;
+    uint32_t b = m1;
 #pragma unroll 1
-    for (uint32_t j = 1; j <= 397; j++) b = mt_init_next(b, j);
+    for (uint32_t j = 2; j <= 397; j++) b = mt_init_next(b, j);
     const uint32_t m397 = b;
     uint32_t bi = 397;
     int i = 0;
@@ -82,7 +88,7 @@ OPB_MT_FN uint32_t mt19937_cursor_words(uint32_t seed, int n, F &&f) {
     }
     if (i >= n) return a0;
     // phase 2: cursor C at i-227 from the seed, cursor B restarted at 397
-    uint32_t c0 = seed, c1 = mt_init_next(seed, 1u);
+    uint32_t c0 = seed, c1 = m1;
     b = m397; bi = 397;
     const int n2 = n < 454 ? n : 454;
 #pragma unroll 1
@@ -94,7 +100,7 @@ OPB_MT_FN uint32_t mt19937_cursor_words(uint32_t seed, int n, F &&f) {
     }
     if (i >= n) return a0;
     // phase 3: cursor D at i-454 from the seed, B restarted at 397 (= i-57 at i = 454)
-    uint32_t d0 = seed, d1 = mt_init_next(seed, 1u);
+    uint32_t d0 = seed, d1 = m1;
     b = m397; bi = 397;
 #pragma unroll 1
     for (; i < n; i++) {
@@ -107,18 +113,18 @@ OPB_MT_FN uint32_t mt19937_cursor_words(uint32_t seed, int n, F &&f) {
     return a0;
 }
 
-// Calls f(k, x_k) for the first n (<= 623) outputs of MT19937 seeded with `seed`.
+// Calls f(k, x_k) for the first n (<= 623) outputs of MT19937 seeded with (seed, key1).
 template <class F>
-OPB_MT_FN void mt19937_first(uint32_t seed, int n, F &&f) {
-    mt19937_cursor_words(seed, n, [&](int i, uint32_t w) { f(i, mt_temper(w)); });
+OPB_MT_FN void mt19937_first(uint32_t seed, uint32_t key1, int n, F &&f) {
+    mt19937_cursor_words(seed, key1, n, [&](int i, uint32_t w) { f(i, mt_temper(w)); });
 }
 
-// Calls f(k, x_k) for the first n outputs of MT19937 seeded with `seed`, any n >= 0.
+// Calls f(k, x_k) for the first n outputs of MT19937 seeded with (seed, key1), any n >= 0.
 template <class F>
-OPB_MT_FN void mt19937_any(uint32_t seed, int n, F &&f) {
+OPB_MT_FN void mt19937_any(uint32_t seed, uint32_t key1, int n, F &&f) {
     uint32_t mt[624];
     const int n1 = n < kMtCursorMax ? n : kMtCursorMax;
-    const uint32_t init623 = mt19937_cursor_words(seed, n1, [&](int k, uint32_t w) {
+    const uint32_t init623 = mt19937_cursor_words(seed, key1, n1, [&](int k, uint32_t w) {
         mt[k] = w;
         f(k, mt_temper(w));
     });
@@ -142,9 +148,9 @@ OPB_MT_FN void mt19937_any(uint32_t seed, int n, F &&f) {
 
 // mt19937_first when ANY_LENGTH is false (n <= 623), mt19937_any otherwise.
 template <bool ANY_LENGTH, class F>
-OPB_MT_FN void mt19937_stream(uint32_t seed, int n, F &&f) {
-    if constexpr (ANY_LENGTH) mt19937_any(seed, n, static_cast<F &&>(f));
-    else mt19937_first(seed, n, static_cast<F &&>(f));
+OPB_MT_FN void mt19937_stream(uint32_t seed, uint32_t key1, int n, F &&f) {
+    if constexpr (ANY_LENGTH) mt19937_any(seed, key1, n, static_cast<F &&>(f));
+    else mt19937_first(seed, key1, n, static_cast<F &&>(f));
 }
 
 }  // namespace opb

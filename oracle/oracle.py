@@ -741,10 +741,12 @@ _UPPER = np.uint32(0x80000000)
 _LOWER = np.uint32(0x7FFFFFFF)
 
 
-def mt19937_init(seeds: np.ndarray) -> np.ndarray:
+def mt19937_init(seeds: np.ndarray, key1: np.ndarray | None = None) -> np.ndarray:
     """init_genrand for a vector of seeds: mt[0] = s, mt[i] = 1812433253 *
     (mt[i-1] ^ (mt[i-1] >> 30)) + i (mod 2^32).  The same recurrence seeds the
-    reference's twisters (``oplib/opcuda/smc.cu:127-131``).  Returns (nseeds, 624)."""
+    reference's twisters (``oplib/opcuda/smc.cu:127-131``).  ``key1`` (optional, one per
+    seed) is added to mt[1] before the recurrence continues: the keyed generators of the
+    library's stream-seed-table Monte Carlo.  Returns (nseeds, 624)."""
     seeds = np.asarray(seeds, dtype=np.uint64) & np.uint64(0xFFFFFFFF)
     mt = np.empty((seeds.shape[0], _MT_N), dtype=np.uint64)
     mt[:, 0] = seeds
@@ -752,6 +754,8 @@ def mt19937_init(seeds: np.ndarray) -> np.ndarray:
     for i in range(1, _MT_N):
         prev = mt[:, i - 1]
         mt[:, i] = (np.uint64(1812433253) * (prev ^ (prev >> np.uint64(30))) + np.uint64(i)) & mask
+        if i == 1 and key1 is not None:
+            mt[:, 1] = (mt[:, 1] + (np.asarray(key1, dtype=np.uint64) & mask)) & mask
     return mt.astype(np.uint32)
 
 
@@ -774,9 +778,9 @@ def mt19937_temper(y: np.ndarray) -> np.ndarray:
     return y
 
 
-def mt19937_outputs(seeds: np.ndarray, count: int) -> np.ndarray:
+def mt19937_outputs(seeds: np.ndarray, count: int, key1: np.ndarray | None = None) -> np.ndarray:
     """First ``count`` genrand_int32 outputs of each seeded stream, (nseeds, count)."""
-    st = mt19937_init(seeds)
+    st = mt19937_init(seeds, key1)
     outs = []
     while sum(o.shape[1] for o in outs) < count:
         st = mt19937_twist(st)

@@ -36,12 +36,20 @@ typedef struct {
     int mti;
 } mt_state;
 
-static void mt_init(mt_state *s, uint32_t seed) {
+/* init_genrand(seed) with key1 added to mt[1] before the recurrence continues from it
+ * (key1 = 0: init_genrand itself).  The keyed form seeds the per-path generators of the
+ * library's reference-facing Monte Carlo: path g of a 4096-stream seed table is keyed by
+ * (seeds[g % 4096], g / 4096). */
+static void mt_init_keyed(mt_state *s, uint32_t seed, uint32_t key1) {
     s->mt[0] = seed;
-    for (int i = 1; i < MT_N; i++)
+    for (int i = 1; i < MT_N; i++) {
         s->mt[i] = 1812433253U * (s->mt[i - 1] ^ (s->mt[i - 1] >> 30)) + (uint32_t)i;
+        if (i == 1) s->mt[1] += key1;
+    }
     s->mti = MT_N;
 }
+
+static void mt_init(mt_state *s, uint32_t seed) { mt_init_keyed(s, seed, 0u); }
 
 static uint32_t mt_next(mt_state *s) {
     uint32_t y;
@@ -70,6 +78,12 @@ static uint32_t mt_next(mt_state *s) {
 void oracle_mt19937_outputs(uint32_t seed, int n, uint32_t *out) {
     mt_state s;
     mt_init(&s, seed);
+    for (int i = 0; i < n; i++) out[i] = mt_next(&s);
+}
+
+void oracle_mt19937_outputs_keyed(uint32_t seed, uint32_t key1, int n, uint32_t *out) {
+    mt_state s;
+    mt_init_keyed(&s, seed, key1);
     for (int i = 0; i < n; i++) out[i] = mt_next(&s);
 }
 
@@ -118,6 +132,7 @@ typedef struct {
     long rs, cs;
     int d, y0, nsteps;
     uint32_t seed;
+    const uint32_t *seeds; /* optional [4096] stream seeds: path g keyed (seeds[g % 4096], g / 4096) */
     uint64_t path0;
     long p_begin, p_end; /* path range relative to path0 */
     int16_t *ypaths;     /* optional: [path][step] */
@@ -131,7 +146,9 @@ static void *mc_worker(void *arg) {
     mt_state s;
     double sb = 0.0, sa = 0.0;
     for (long p = j->p_begin; p < j->p_end; p++) {
-        mt_init(&s, (uint32_t)(j->seed + (uint32_t)(j->path0 + (uint64_t)p)));
+        const uint64_t g = j->path0 + (uint64_t)p;
+        if (j->seeds) mt_init_keyed(&s, j->seeds[g & 4095u], (uint32_t)(g >> 12));
+        else mt_init(&s, (uint32_t)(j->seed + (uint32_t)g));
         int y = j->y0;
         double xmin = 1e300, xsum = 0.0, xv = 0.0;
         for (int k = 0; k < j->nsteps; k++) {
@@ -158,10 +175,10 @@ static void *mc_worker(void *arg) {
 
 /* Runs npaths paths (ids path0 .. path0+npaths-1) over nthreads POSIX threads.
  * Returns 0 on success.  sums[0] = sum of discounted barrier payoffs, sums[1] = Asian. */
-int oracle_mc_paths(const float *C, long rs, long cs, int d, int y0, uint32_t seed,
-                    uint64_t path0, long npaths, int nsteps, int16_t *ypaths,
-                    const double *x, double strike, double barrier, double disc,
-                    double *sums, int nthreads) {
+static int mc_paths_run(const float *C, long rs, long cs, int d, int y0, uint32_t seed, const uint32_t *seeds,
+                        uint64_t path0, long npaths, int nsteps, int16_t *ypaths,
+                        const double *x, double strike, double barrier, double disc,
+                        double *sums, int nthreads) {
     if (nthreads < 1) nthreads = 1;
     if (nthreads > 1024) nthreads = 1024;
     pthread_t *th = (pthread_t *)calloc((size_t)nthreads, sizeof(pthread_t));
@@ -171,7 +188,7 @@ int oracle_mc_paths(const float *C, long rs, long cs, int d, int y0, uint32_t se
     for (int t = 0; t < nthreads; t++) {
         mc_job *j = &jobs[t];
         j->C = C; j->rs = rs; j->cs = cs; j->d = d; j->y0 = y0; j->nsteps = nsteps;
-        j->seed = seed; j->path0 = path0;
+        j->seed = seed; j->seeds = seeds; j->path0 = path0;
         j->p_begin = (long)t * per;
         j->p_end = j->p_begin + per < npaths ? j->p_begin + per : npaths;
         if (j->p_begin > j->p_end) j->p_begin = j->p_end;
@@ -189,6 +206,24 @@ int oracle_mc_paths(const float *C, long rs, long cs, int d, int y0, uint32_t se
     free(th);
     free(jobs);
     return 0;
+}
+
+int oracle_mc_paths(const float *C, long rs, long cs, int d, int y0, uint32_t seed,
+                    uint64_t path0, long npaths, int nsteps, int16_t *ypaths,
+                    const double *x, double strike, double barrier, double disc,
+                    double *sums, int nthreads) {
+    return mc_paths_run(C, rs, cs, d, y0, seed, NULL, path0, npaths, nsteps, ypaths, x, strike, barrier, disc,
+                        sums, nthreads);
+}
+
+/* The same paths with generators keyed from a 4096-entry stream seed table. */
+int oracle_mc_paths_seeded(const float *C, long rs, long cs, int d, int y0, const uint32_t *seeds,
+                           uint64_t path0, long npaths, int nsteps, int16_t *ypaths,
+                           const double *x, double strike, double barrier, double disc,
+                           double *sums, int nthreads) {
+    if (!seeds) return -1;
+    return mc_paths_run(C, rs, cs, d, y0, 0u, seeds, path0, npaths, nsteps, ypaths, x, strike, barrier, disc,
+                        sums, nthreads);
 }
 
 typedef struct {

@@ -34,6 +34,12 @@ def load():
                                     C.c_long, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double,
                                     C.c_void_p, C.c_int]
     lib.oracle_mc_paths.restype = C.c_int
+    lib.oracle_mt19937_outputs_keyed.argtypes = [C.c_uint32, C.c_uint32, C.c_int, C.c_void_p]
+    lib.oracle_mt19937_outputs_keyed.restype = None
+    lib.oracle_mc_paths_seeded.argtypes = [C.c_void_p, C.c_long, C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_uint64,
+                                           C.c_long, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                           C.c_double, C.c_void_p, C.c_int]
+    lib.oracle_mc_paths_seeded.restype = C.c_int
     lib.oracle_mt_benchmark.argtypes = [C.c_long, C.c_long, C.c_int, C.c_uint32]
     lib.oracle_mt_benchmark.restype = C.c_double
     _lib = lib
@@ -43,6 +49,13 @@ def load():
 def mt_outputs(seed: int, n: int) -> np.ndarray:
     out = np.empty(n, dtype=np.uint32)
     load().oracle_mt19937_outputs(seed & 0xFFFFFFFF, n, out.ctypes.data)
+    return out
+
+
+def mt_outputs_keyed(seed: int, key1: int, n: int) -> np.ndarray:
+    """First n outputs of MT19937 seeded init_genrand(seed) with key1 added to mt[1]."""
+    out = np.empty(n, dtype=np.uint32)
+    load().oracle_mt19937_outputs_keyed(seed & 0xFFFFFFFF, key1 & 0xFFFFFFFF, n, out.ctypes.data)
     return out
 
 
@@ -70,3 +83,21 @@ def mc_paths(Cm: np.ndarray, y0: int, seed: int, path0: int, npaths: int, nsteps
     if r != 0:
         raise RuntimeError("oracle_mc_paths failed")
     return paths, sums
+
+
+def mc_paths_seeded(Cm: np.ndarray, y0: int, seeds: np.ndarray, path0: int, npaths: int, nsteps: int,
+                    nthreads=8) -> np.ndarray:
+    """Paths [npaths, nsteps] int16 of path ids path0 .. path0+npaths-1 with generators keyed
+    from the 4096-entry stream seed table: path g uses MT19937 (seeds[g % 4096], g / 4096)."""
+    Cm = np.ascontiguousarray(Cm, dtype=np.float32)
+    seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+    if seeds.shape != (4096,):
+        raise ValueError("seeds must hold 4096 stream seeds")
+    d = Cm.shape[1]
+    paths = np.empty((npaths, nsteps), dtype=np.int16)
+    sums = np.zeros(2, dtype=np.float64)
+    r = load().oracle_mc_paths_seeded(Cm.ctypes.data, d, 1, d, y0, seeds.ctypes.data, path0, npaths, nsteps,
+                                      paths.ctypes.data, None, 1.0, 0.0, 1.0, sums.ctypes.data, nthreads)
+    if r != 0:
+        raise RuntimeError("oracle_mc_paths_seeded failed")
+    return paths

@@ -121,6 +121,14 @@ def test_host_argument_errors(lib, call, expect):
     assert lib.opcuda_get_status() == expect
 
 
+def test_mc_seed_table_sizes(lib):
+    """The reference's callers allocate opcuda_mc_nrng() seeds and a status record of
+    opcuda_mc_status_sz() int32 words (oplib/opmodel/models/CModel Device.cs:320-338)."""
+    assert lib.opcuda_mc_nrng() == 4096
+    assert lib.opcuda_mc_status_sz() == 4 + 4096
+    assert lib.opcuda_mc_setseed(0, 1) == -2
+
+
 def test_lattice_desc_rejected_on_host(lib):
     from oplib_b200._lib import LatticeDesc
     L = LatticeDesc()

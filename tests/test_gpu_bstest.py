@@ -43,7 +43,7 @@ def test_bstest_through_the_opcuda_drop_ins(cuda):
 
     nscen, nbatch = 4096 * 25, 12
     st = torch.zeros(lib.opcuda_mc_status_sz(), dtype=torch.int32, device=cuda)
-    seed = np.array([4242], dtype=np.uint32)
+    seed = np.random.default_rng(4242).integers(0, 2**31 - 1, lib.opcuda_mc_nrng()).astype(np.uint32)
     assert lib.opcuda_mc_setseed(seed.ctypes.data, st.data_ptr()) == 0
     mk = torch.zeros(1, dtype=torch.int32, device=cuda)
     yd = torch.empty(nscen, dtype=torch.int16, device=cuda)

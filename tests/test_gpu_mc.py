@@ -130,34 +130,80 @@ def test_opcuda_mc1f_reference_layout_and_continuation(cuda):
         _mc1f_batches(lib, cuda, Cr, d, nk, nscen, y0)
 
 
+def _stream_seeds(seed):
+    """4096 stream seeds as the reference's callers draw them: uniform in [0, 2^31 - 1)."""
+    return np.random.default_rng(seed).integers(0, 2**31 - 1, 4096).astype(np.uint32)
+
+
 def _mc1f_batches(lib, cuda, Cr, d, nk, nscen, y0):
     ccm = torch.from_numpy(np.asfortranarray(Cr).ravel(order="K").copy()).to(cuda)
     mk = torch.zeros(nk, dtype=torch.int32, device=cuda)
+    assert lib.opcuda_mc_nrng() == 4096
     st = torch.zeros(lib.opcuda_mc_status_sz(), dtype=torch.int32, device=cuda)
     yd = torch.empty(nscen * nk, dtype=torch.int16, device=cuda)
-    seed = np.array([4242], dtype=np.uint32)
-    assert lib.opcuda_mc_setseed(seed.ctypes.data, st.data_ptr()) == 0
+    seeds = _stream_seeds(4242)
+    assert lib.opcuda_mc_setseed(seeds.ctypes.data, st.data_ptr()) == 0
     for batch in range(2):
         yh = np.empty(nscen * nk, dtype=np.int16)
         assert lib.opcuda_mc1f(st.data_ptr(), y0, yd.data_ptr(), nscen, nk, d, ccm.data_ptr(), mk.data_ptr(),
                                yh.ctypes.data) == 0
-        ref, _ = OC.mc_paths(Cr, y0, 4242, batch * nscen, nscen, nk)
+        ref = OC.mc_paths_seeded(Cr, y0, seeds, batch * nscen, nscen, nk)
         assert np.array_equal(yh.reshape(nk, nscen).T, ref)
+
+
+def test_opcuda_mc1f_uses_every_stream_seed(cuda):
+    """Path g is path g / 4096 of stream g % 4096: changing one stream's seed changes that
+    stream's paths and no other; paths 0 .. 4095 draw from init_genrand(seeds[g])."""
+    from oplib_b200 import _lib
+    lib = _lib.load()
+    cfg = O.LVLattice(n=128)
+    L, x = cfg.generator()
+    niter, dt = O.plan_niter(L, 1 / 52, cfg.dt0)
+    Cr = O.cumrows_f32(O.square(O.ek(L, dt), niter))
+    d, nk, nscen, y0 = 128, 30, 3 * 4096, O.nearest_node(x)
+    ccm = torch.from_numpy(np.asfortranarray(Cr).ravel(order="K").copy()).to(cuda)
+    mk = torch.zeros(nk, dtype=torch.int32, device=cuda)
+    yd = torch.empty(nscen * nk, dtype=torch.int16, device=cuda)
+    out = []
+    seeds = _stream_seeds(7)
+    for change in (False, True):
+        s = seeds.copy()
+        if change:
+            s[5] ^= 0x5A5A5A5A
+        st = torch.zeros(lib.opcuda_mc_status_sz(), dtype=torch.int32, device=cuda)
+        assert lib.opcuda_mc_setseed(s.ctypes.data, st.data_ptr()) == 0
+        assert int(st[4 + 5].item()) & 0xFFFFFFFF == int(s[5])
+        yh = np.empty(nscen * nk, dtype=np.int16)
+        assert lib.opcuda_mc1f(st.data_ptr(), y0, yd.data_ptr(), nscen, nk, d, ccm.data_ptr(), mk.data_ptr(),
+                               yh.ctypes.data) == 0
+        out.append(yh.reshape(nk, nscen).T.copy())
+        assert np.array_equal(out[-1], OC.mc_paths_seeded(Cr, y0, s, 0, nscen, nk))
+    differs = np.any(out[0] != out[1], axis=1)
+    stream5 = np.arange(nscen) % 4096 == 5
+    assert not differs[~stream5].any()
+    assert differs[stream5].all()
+    # the first path of each stream is plain init_genrand(seed)
+    for g in (0, 5, 4095):
+        u = O.uniform_f32(OC.mt_outputs(int(seeds[g]), nk))
+        y = y0
+        for k in range(nk):
+            y = int(O.sample_next(Cr[y][None, :], u[k:k + 1])[0])
+            assert out[0][g, k] == y
 
 
 @pytest.mark.parametrize("nper", [20, 700])
 def test_mt_benchmark_uniforms(cuda, nper):
     from oplib_b200 import _lib
     lib = _lib.load()
-    st = torch.zeros(4, dtype=torch.int32, device=cuda)
-    seed = np.array([7], dtype=np.uint32)
-    assert lib.opcuda_mc_setseed(seed.ctypes.data, st.data_ptr()) == 0
+    st = torch.zeros(lib.opcuda_mc_status_sz(), dtype=torch.int32, device=cuda)
+    seeds = _stream_seeds(7)
+    assert lib.opcuda_mc_setseed(seeds.ctypes.data, st.data_ptr()) == 0
     n = 4096 * nper
     u = torch.empty(n, device=cuda)
     assert lib.opcuda_mt_benchmark(st.data_ptr(), u.data_ptr(), n) == 0
     got = u.cpu().numpy().reshape(nper, 4096)
-    for s in [0, 5, 4095]:
-        ref = (OC.mt_outputs(7 + s, nper).astype(np.float32) * np.float32(2.0 ** -32)).astype(np.float32)
+    for s in [0, 5, 4095]:  # stream s: init_genrand(seeds[s]), as the reference's twister s
+        ref = (OC.mt_outputs(int(seeds[s]), nper).astype(np.float32) * np.float32(2.0 ** -32)).astype(np.float32)
         assert np.array_equal(got[:, s], ref)
 
 

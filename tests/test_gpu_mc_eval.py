@@ -115,7 +115,7 @@ def test_opcuda_mc1f_eval_matches_mc1f_with_host_evaluator(cuda):
     cf = np.zeros((nk, d))
     cf[-1] = np.maximum(x - 1.0, 0.0)  # the reference's VanillaPayoffEvaluator, strike 1
     dcf = torch.from_numpy(cf).to(cuda)
-    seed = np.array([99], dtype=np.uint32)
+    seed = np.random.default_rng(99).integers(0, 2**31 - 1, 4096).astype(np.uint32)
     st_a = torch.zeros(lib.opcuda_mc_status_sz(), dtype=torch.int32, device=cuda)
     st_b = torch.zeros_like(st_a)
     assert lib.opcuda_mc_setseed(seed.ctypes.data, st_a.data_ptr()) == 0

@@ -61,7 +61,7 @@ def test_mc1f_over_the_plan_bit_exact(plan_and_kernels, cuda):
     assert lib.opcuda_sck(d, nm, kcm.data_ptr(), ccm.data_ptr()) == 0
     mk = torch.tensor(plan.m_k, dtype=torch.int32, device=cuda)
     st = torch.zeros(lib.opcuda_mc_status_sz(), dtype=torch.int32, device=cuda)
-    s = np.array([seed], dtype=np.uint32)
+    s = (seed + np.arange(4096)).astype(np.uint32)  # paths 0 .. 4095: init_genrand(seed + p)
     assert lib.opcuda_mc_setseed(s.ctypes.data, st.data_ptr()) == 0
     yd = torch.empty(nscen * nk, dtype=torch.int16, device=cuda)
     yh = np.empty(nscen * nk, dtype=np.int16)
