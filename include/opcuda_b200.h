@@ -367,6 +367,9 @@ int opb_mlp_pack(const float *theta, void *packed);
 long long opb_mlp_infer_workspace_bytes(long long n, int nmem);
 int opb_mlp_infer(const void *packed, int nmem, long long member_stride, const float *X, long long n, void *ws,
                   long long ws_bytes, float *mean, float *spread);
+/* new: 1 (default) one kernel per member runs all layers with the activations in shared
+ * memory; 0 one launch per layer, activations through device memory (bit-identical) */
+int opb_mlp_set_fused_inference(int on);
 
 /* ------------------------------------------------------------------ cumulative rows, MC */
 /* replaces oplib/opcuda/sck.cu:88-93: nm column-major kernels -> cumulative normalised rows */

@@ -127,6 +127,7 @@ PROTOTYPES: dict[str, tuple] = {
     "opb_mlp_param_count": (i32, []),
     "opb_mlp_workspace_floats": (i64, [i32]),
     "opb_mlp_set_tensor_cores": (i32, [i32]),
+    "opb_mlp_set_fused_inference": (i32, [i32]),
     "opb_mlp_init": (i32, [vp, ull]),
     "opb_mlp_round": (i32, [vp, vp, vp]),
     "opb_mlp_forward": (i32, [vp, vp, i32, vp, vp]),

@@ -269,16 +269,25 @@ struct TcCfg {
     static constexpr int B_BYTES = B_ROWS * BK * 2;                 // one of Bhi/Blo
     static constexpr int TILE_M = PAIR ? 2 * TC_BM : TC_BM;         // output rows per work item
     static constexpr int NPARTS = NPROD == 1 ? 1 : 2;  // parts loaded per operand
-    static constexpr int STAGE_BYTES = NPARTS * (A_BYTES + B_BYTES);
+    // network layers (single products with one column tile, K <= 256): the whole B, the
+    // layer's weights, stays resident in shared memory, loaded once per CTA, and the stage
+    // ring carries A alone -- each 128-row tile then moves 64 KB from L2 instead of 192 KB
+    static constexpr bool BRES = NPROD == 1 && EPIMODE != 0 && !PAIR;
+    static constexpr int BRES_KB = BRES ? 256 / BK : 0;           // resident K-blocks of B
+    static constexpr int STAGE_BYTES = BRES ? A_BYTES : NPARTS * (A_BYTES + B_BYTES);
+    static constexpr int RING_BYTES = STAGES * STAGE_BYTES + BRES_KB * B_BYTES;
     static constexpr int CPT = BN < CPT_MAX ? BN : CPT_MAX;  // accumulator columns per epilogue thread
     static constexpr int HALVES = BN / CPT;                 // column groups per TMEM lane
     static constexpr int EPI_WARPS = 4 * HALVES;            // epilogue warps (4 lane quadrants x groups)
     // FP32 output: each epilogue warp transposes 32 x 32 blocks through shared memory
-    // (row stride 33 words) so that Cin loads and C stores are whole 128-byte lines
-    static constexpr int OUT_BYTES = EPIMODE == 0 ? EPI_WARPS * 32 * 33 * 4 : 0;
+    // (row stride 33 words) so that Cin loads and C stores are whole 128-byte lines.
+    // Network layers (EPIMODE 1): each warp stages its 32 rows x CPT/2 BF16 activations
+    // (row stride CPT + 16 bytes) so that its global stores cover 64-byte row segments
+    static constexpr int OUT_BYTES =
+        EPIMODE == 0 ? EPI_WARPS * 32 * 33 * 4 : EPIMODE == 1 ? EPI_WARPS * 32 * (CPT + 16) : 0;
     // network layers: the tile's bias (and output weights) staged in shared memory once
     static constexpr int VEC_BYTES = EPIMODE ? 2 * BN * 4 : 0;
-    static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ + OUT_BYTES + VEC_BYTES;
+    static constexpr int SMEM = RING_BYTES + 1024 /*align*/ + 256 /*barriers*/ + OUT_BYTES + VEC_BYTES;
     static constexpr int THREADS = 32 * (EPI_WARPS + 2);    // + TMA producer warp + MMA warp
     static constexpr int TMEM_COLS = 2 * BN;                // two accumulators (ping-pong chunks)
     // K-blocks accumulated in TMEM per chunk: K = 128 for the split products (bounds the
@@ -387,7 +396,9 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t *gbase = smem_raw + (base - raw);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + STAGES * Cfg::STAGE_BYTES);
+    static_assert(!(Cfg::BRES && BATCHED), "resident B: single products");
+    static_assert(2 * STAGES + 8 <= 32, "barrier slots");
+    uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + Cfg::RING_BYTES);
     const uint32_t bar0 = smem_u32(bars);
     auto full_bar = [&](int s) { return bar0 + 8u * s; };
     auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
@@ -396,6 +407,8 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
     const uint32_t drain_bar = bar0 + 8u * (2 * STAGES + 4);
     volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bars + 2 * STAGES + 5);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * STAGES + 6);
+    const uint32_t bres_bar = bar0 + 8u * (2 * STAGES + 7);        // resident B loaded
+    const uint32_t bres_base = base + STAGES * Cfg::STAGE_BYTES;   // resident B, K-block kb at + kb * B_BYTES
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mtiles = p.M / Cfg::TILE_M, ntiles_n = p.N / BN;
@@ -463,6 +476,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             mbar_init(acce_bar(a), PAIR ? 2 * EPI : EPI * 32);  // pair: one lane per epilogue warp of both CTAs
         }
         mbar_init(drain_bar, 1);
+        if constexpr (Cfg::BRES) mbar_init(bres_bar, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -484,7 +498,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
     // network layers with one column tile (N == BN, every layer of the surrogate): the bias
     // and output weights are read from shared memory in the epilogue, not from L1/L2 on the
     // dependent path of every element
-    float *svec = reinterpret_cast<float *>(gbase + STAGES * Cfg::STAGE_BYTES + 256 + Cfg::OUT_BYTES);
+    float *svec = reinterpret_cast<float *>(gbase + Cfg::RING_BYTES + 256 + Cfg::OUT_BYTES);
     const bool vec_smem = EPIMODE != 0 && p.N == BN;
     if (vec_smem) {
         for (int i = threadIdx.x; i < BN; i += blockDim.x) {
@@ -503,6 +517,15 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             // ---------------- TMA producer
             long kbg = 0;  // K-blocks issued over the CTA's lifetime (stage ring position)
             bool ok = true;
+            if constexpr (Cfg::BRES) {
+                // every item's B is the whole weight matrix (N == BN, K <= 256): load it once
+                if (item0 < nitems) {
+                    const int nkb_all = p.K / BK;
+                    mbar_expect_tx(bres_bar, (uint32_t)(nkb_all * Cfg::B_BYTES));
+                    for (int kb = 0; kb < nkb_all; kb++)
+                        tma_load_2d(bres_base + kb * Cfg::B_BYTES, &mBhi, bres_bar, kb * BK, 0);
+                }
+            }
             for (int t = item0; t < nitems && ok; t += istep) {
                 int prob, m0, n0, nkb, kb0, slice;
                 get_item(t, prob, m0, n0, nkb, kb0, slice);
@@ -541,7 +564,9 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                     } else {
                         mbar_expect_tx(full_bar(s), Cfg::STAGE_BYTES);
                         tma_load_2d(st, mp[0], full_bar(s), kx, ma);
-                        if constexpr (NPROD == 1) {
+                        if constexpr (Cfg::BRES) {
+                            // B is resident
+                        } else if constexpr (NPROD == 1) {
                             tma_load_2d(st + Cfg::A_BYTES, mp[2], full_bar(s), kx, nb);
                         } else {
                             tma_load_2d(st + Cfg::A_BYTES, mp[1], full_bar(s), kx, ma);
@@ -581,6 +606,12 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             const uint32_t idesc = umma_idesc_16(BN, F16, Cfg::TILE_M, BMN);
             long kbg = 0, g = 0;  // K-blocks consumed, chunks issued
             bool ok = true;
+            if constexpr (Cfg::BRES) {
+                if (item0 < nitems) {
+                    ok = mbar_wait(bres_bar, 0u, abort_flag, TC_WAIT_NS);
+                    tc_fence_after();
+                }
+            }
             for (int t = item0; t < nitems && ok; t += istep) {
                 int prob, m0, n0, nkb, kb0, slice;
                 get_item(t, prob, m0, n0, nkb, kb0, slice);
@@ -605,7 +636,8 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                         const uint32_t st = base + s * Cfg::STAGE_BYTES;
                         const uint64_t dAh = umma_desc_sw<BK>(st);
                         const uint64_t dAl = umma_desc_sw<BK>(st + Cfg::A_BYTES);
-                        const uint32_t sBh = st + Cfg::NPARTS * Cfg::A_BYTES;
+                        const uint32_t sBh = Cfg::BRES ? bres_base + (uint32_t)((kb0 + kb) * Cfg::B_BYTES)
+                                                       : st + Cfg::NPARTS * Cfg::A_BYTES;
                         const uint32_t sBl = st + 2 * Cfg::A_BYTES + Cfg::B_BYTES;
                         const uint64_t dBh = BMN ? umma_desc_mn<BK>(sBh) : umma_desc_sw<BK>(sBh);
                         const uint64_t dBl = BMN ? umma_desc_mn<BK>(sBl) : umma_desc_sw<BK>(sBl);
@@ -743,22 +775,42 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
                 }
             }
             if constexpr (EPIMODE == 1) {
-                // network layer: BF16 GELU(alpha * acc + bias), 8 values per 16-byte store
-                __nv_bfloat16 *hrow = p.H + (long long)row * p.ldh + col0;
+                // network layer: BF16 GELU(alpha * acc + bias) in two halves of CPT/2 columns.
+                // Lane = row while the values are in the accumulator layout, so each lane
+                // writes its row segment to the warp's staging rows (stride RS, conflict-free
+                // 16-byte stores); read back, lane l stores row 8i + l/4, 16-byte chunk l%4:
+                // every global store of the warp covers eight whole 64-byte row segments,
+                // where stores straight from the accumulator layout touched 32 rows each
                 const float4 *b4 = reinterpret_cast<const float4 *>((vec_smem ? svec - n0 : p.bias) + col0);
+                constexpr int HC = CPT / 2, RS = HC * 2 + 16;
+                static_assert(HC == 32, "four 16-byte chunks per staged row segment");
+                uint8_t *stg = gbase + Cfg::RING_BYTES + 256 + warp * (32 * RS);
+                const int rb = m0 + (int)rank * TC_BM + q * 32;
 #pragma unroll
-                for (int j = 0; j < CPT; j += 8) {
-                    const float4 ba = b4[j / 4], bb = b4[j / 4 + 1];
-                    const float bv[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
-                    uint32_t pk[4];
+                for (int hh = 0; hh < 2; hh++) {
 #pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        const __nv_bfloat162 h2 =
-                            __floats2bfloat162_rn(gelu_as(fmaf(alpha, sum[j + 2 * u], bv[2 * u])),
-                                                  gelu_as(fmaf(alpha, sum[j + 2 * u + 1], bv[2 * u + 1])));
-                        pk[u] = *reinterpret_cast<const uint32_t *>(&h2);
+                    for (int j = 0; j < HC; j += 8) {
+                        const int jj = hh * HC + j;
+                        const float4 ba = b4[jj / 4], bb = b4[jj / 4 + 1];
+                        const float bv[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
+                        uint32_t pk[4];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            const __nv_bfloat162 h2 =
+                                __floats2bfloat162_rn(gelu_as(fmaf(alpha, sum[jj + 2 * u], bv[2 * u])),
+                                                      gelu_as(fmaf(alpha, sum[jj + 2 * u + 1], bv[2 * u + 1])));
+                            pk[u] = *reinterpret_cast<const uint32_t *>(&h2);
+                        }
+                        *reinterpret_cast<uint4 *>(stg + lane * RS + j * 2) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
                     }
-                    *reinterpret_cast<uint4 *>(hrow + j) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                    __syncwarp();
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const int r = i * 8 + (lane >> 2), c = lane & 3;
+                        const uint4 v = *reinterpret_cast<const uint4 *>(stg + r * RS + c * 16);
+                        *reinterpret_cast<uint4 *>(p.H + (long long)(rb + r) * p.ldh + col0 + hh * HC + c * 8) = v;
+                    }
+                    __syncwarp();
                 }
                 continue;
             }
@@ -791,7 +843,7 @@ __global__ void __launch_bounds__(TcCfg<BN, STAGES, NPROD, BK, PAIR, EPIMODE>::T
             // its order (float4 groups in column order): each group sum is parked in the
             // first two words of its group's slots (read by this lane alone) and the row's
             // lane adds them up.
-            float *st = reinterpret_cast<float *>(gbase + STAGES * Cfg::STAGE_BYTES + 256) + warp * (32 * 33);
+            float *st = reinterpret_cast<float *>(gbase + Cfg::RING_BYTES + 256) + warp * (32 * 33);
             const int rbase = m0 + (int)rank * TC_BM + q * 32;
             const int tr = lane >> 3, tc4 = (lane & 7) * 4;
             double rs = 0.0;
@@ -1321,16 +1373,20 @@ int launch_tc_gemm_batched(int bn, const CUtensorMap *maps, const TcProblem *pro
 }
 
 // One network layer on the tensor cores: H[M, N] = GELU(alpha * A[M, K] . W[N, K]^T + bias)
-// with BF16 A, W and H (single product, FP32 accumulation); M % 128, N % 256, K % 64.
+// with BF16 A, W and H (single product, FP32 accumulation); M % 128, N = 256, K % 64 and
+// K <= 256 (W stays resident in shared memory).
 // With w5 and ypart (N = 256): no H; instead ypart[g * M + row], g < 256 / TC_LAYER_CPT, =
 // the dot of the BF16 activations of column group g with w5 (the output layer, fused).
 int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, const __nv_bfloat16 *W,
                     long long ldw, float alpha, const float *bias, __nv_bfloat16 *H, long long ldh, cudaStream_t s,
                     const float *w5, float *ypart) {
-    constexpr int BN = 256, STAGES = 4;
+    constexpr int BN = 256, STAGES = 3;
     using Cfg = TcCfg<BN, STAGES, 1, TC_BK, false, 1>;
+    using Cfg2 = TcCfg<BN, STAGES, 1, TC_BK, false, 2>;  // the last layer, output fused
+    static_assert(Cfg::BRES && Cfg::SMEM <= 227 * 1024 && Cfg2::SMEM <= 227 * 1024, "layer kernel: resident weights");
     const bool fused = w5 != nullptr;
-    if (M <= 0 || M % TC_BM || N % BN || K % TC_BK || (fused && N != BN)) return OPB_E_UNSUPPORTED;
+    // one column tile and K <= 256: the weights stay resident in shared memory
+    if (M <= 0 || M % TC_BM || N != BN || K % TC_BK || K > Cfg::BRES_KB * TC_BK) return OPB_E_UNSUPPORTED;
     if (!A || !W || !bias || (fused ? !ypart : !H)) return OPB_E_NULL;
     int e0 = fused ? set_smem_attr<BN, STAGES, false, false, 1, 2>() : set_smem_attr<BN, STAGES, false, false, 1, 1>();
     if (e0) return e0;
@@ -1344,9 +1400,290 @@ int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, 
     const int grid = ntiles < num_sms() ? ntiles : num_sms();
     TcBatch none{nullptr, nullptr, nullptr, 0};
     if (fused)
-        k_tc_gemm<BN, STAGES, false, false, 1, 2><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mA, mA, mW, mW, p, none);
+        k_tc_gemm<BN, STAGES, false, false, 1, 2><<<grid, Cfg2::THREADS, Cfg2::SMEM, s>>>(mA, mA, mW, mW, p, none);
     else
         k_tc_gemm<BN, STAGES, false, false, 1, 1><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(mA, mA, mW, mW, p, none);
+    return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- fused network inference
+//
+// The four hidden layers of one ensemble member (8 -> 256 x 4 with GELU) and the output
+// layer's partial dots in one persistent kernel.  A 128-row tile's activations stay in
+// shared memory between layers, written by the epilogue as BF16 in the layout the next
+// layer's MMA reads (K-major, 128-byte swizzle: row r of K-block kb at kb * 16 KB + r * 128,
+// its 16-byte chunk c at position c ^ (r & 7)), so HBM carries only the padded inputs and
+// the output partials.  Two tiles are in flight per CTA (slots 0 and 1, each with a 64 KB
+// activation buffer and a 256-column TMEM accumulator): the MMAs run the layers in the order
+// (tile a, layer l), (tile b, l), (a, l + 1), (b, l + 1), ..., so the epilogue of one tile's
+// layer overlaps the MMAs of the other's.  The weights stream through a two-stage ring of
+// 256 x 64 K-blocks in the MMAs' order; the input tile is loaded into its slot's first
+// K-block once the slot's previous tile has finished.
+//
+// Warp roles (576 threads): 16 epilogue warps (lane quadrant q = warp & 3, column group
+// h = warp >> 2 = the K-block of the next layer's A that the warp writes), one TMA warp, one
+// MMA warp.  Barriers, per slot s: xfull (input tile loaded), accf (layer's MMAs done),
+// hready (epilogue done: accumulator read and, for layers 1-3, activations written and
+// fenced for the async proxy), hfree (the tile's last MMA done: the slot's buffer may take
+// the next input); per ring stage: wfull, wempty.  Every wait is bounded as in k_tc_gemm.
+//
+// Each layer is computed as launch_tc_layer computes it -- the same MMA K order into FP32
+// TMEM, the same bias + GELU and BF16 rounding, the same partial dots of the output layer --
+// so ypart is bit-identical to the layer-by-layer path.
+
+constexpr int FM_EPI = 16, FM_THREADS = 32 * (FM_EPI + 2);
+constexpr int FM_KB_BYTES = TC_BM * TC_BK * 2;      // one K-block of a slot's activations
+constexpr int FM_HBYTES = 4 * FM_KB_BYTES;          // a slot: 128 rows x 256 BF16
+constexpr int FM_WBYTES = 256 * TC_BK * 2;          // one weight K-block: 256 rows x 64 BF16
+constexpr int FM_WST = 2;                           // weight ring stages
+constexpr int FM_RING = 2 * FM_HBYTES + FM_WST * FM_WBYTES;
+constexpr int FM_VEC = 5 * 256 * 4;                 // b1 | b2 | b3 | b4 | w5
+constexpr int FM_SMEM = FM_RING + 1024 + 256 + FM_VEC;
+static_assert(FM_SMEM <= 227 * 1024, "fused inference: shared memory");
+
+struct FmParams {
+    long long M;       // rows, a multiple of 128
+    const float *vec;  // b1 | b2 | b3 | b4 | w5, 5 x 256 floats
+    float *ypart;      // [4][M]: partial dot of column group g with w5
+};
+
+__global__ void __launch_bounds__(FM_THREADS, 1)
+    k_mlp_fused(const __grid_constant__ CUtensorMap mX, const __grid_constant__ CUtensorMap mW1,
+                const __grid_constant__ CUtensorMap mWH, FmParams p) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    uint8_t *gbase = smem_raw + (base - raw);
+    const uint32_t wbase = base + 2 * FM_HBYTES;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(gbase + FM_RING);
+    const uint32_t bar0 = smem_u32(bars);
+    auto wfull = [&](int w) { return bar0 + 8u * w; };
+    auto wempty = [&](int w) { return bar0 + 8u * (2 + w); };
+    auto xfull = [&](int s) { return bar0 + 8u * (4 + s); };
+    auto accf = [&](int s) { return bar0 + 8u * (6 + s); };
+    auto hready = [&](int s) { return bar0 + 8u * (8 + s); };
+    auto hfree = [&](int s) { return bar0 + 8u * (10 + s); };
+    const uint32_t drain_bar = bar0 + 8u * 12;
+    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(bars + 13);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 14);
+    float *svec = reinterpret_cast<float *>(gbase + FM_RING + 256);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntiles = (int)(p.M / TC_BM);
+    const int item0 = blockIdx.x, istep = gridDim.x;
+    const int nmine = item0 < ntiles ? (ntiles - item0 + istep - 1) / istep : 0;  // this CTA's tiles
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 12; i++) mbar_init(bar0 + 8u * i, (i == 8 || i == 9) ? FM_EPI : 1);
+        mbar_init(drain_bar, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 0) {
+        const uint32_t slot = smem_u32(const_cast<uint32_t *>(tmem_slot));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(512)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    for (int i = threadIdx.x; i < 5 * 256; i += blockDim.x) svec[i] = p.vec[i];
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    // The steps (tile j of this CTA, layer l) in MMA order: pairs of tiles, layer by layer,
+    // the pair's two tiles alternating; tile j lives in slot j & 1 as that slot's use j >> 1.
+#define FM_STEPS_BEGIN                                                     \
+    for (int pp = 0; pp < nmine && ok; pp += 2)                            \
+        for (int l = 0; l < 4 && ok; l++)                                  \
+            for (int s = 0; s < 2 && ok; s++) {                            \
+                const int j = pp + s;                                      \
+                if (j >= nmine) continue;                                  \
+                const int u = j >> 1;
+#define FM_STEPS_END }
+
+    if (warp == FM_EPI) {
+        if (lane == 0) {
+            // ---------------- TMA producer: input tiles and the weight K-blocks in MMA order
+            long wk = 0;
+            bool ok = true;
+            FM_STEPS_BEGIN
+            if (l == 0) {
+                if (u >= 1 && !mbar_wait(hfree(s), (uint32_t)((u - 1) & 1), abort_flag, TC_WAIT_NS)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(xfull(s), FM_KB_BYTES);
+                tma_load_2d(base + s * FM_HBYTES, &mX, xfull(s), 0, (item0 + j * istep) * TC_BM);
+            }
+            const int nkb = l == 0 ? 1 : 4;
+            for (int kb = 0; kb < nkb; kb++, wk++) {
+                const int w = (int)(wk & 1);
+                if (wk >= FM_WST &&
+                    !mbar_wait(wempty(w), (uint32_t)(((wk / FM_WST) + 1) & 1), abort_flag, TC_WAIT_NS)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(wfull(w), FM_WBYTES);
+                if (l == 0) tma_load_2d(wbase + w * FM_WBYTES, &mW1, wfull(w), 0, 0);
+                else tma_load_2d(wbase + w * FM_WBYTES, &mWH, wfull(w), kb * TC_BK, (l - 1) * 256);
+            }
+            FM_STEPS_END
+            if (!ok) {
+                atomicExch(&g_tc_error, 11);
+                *abort_flag = 1;
+            }
+        }
+        __syncwarp();
+    } else if (warp == FM_EPI + 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer
+            const uint32_t idesc = umma_idesc_16(256, false);
+            long wk = 0;
+            bool ok = true;
+            FM_STEPS_BEGIN
+            // operands of (j, l): the input tile, or layer l - 1's activations; and the
+            // accumulator drained by the slot's previous epilogue (hready completion
+            // 4u + l - 1 of this slot)
+            if (l == 0) {
+                if (u >= 1 && !mbar_wait(hready(s), 1u, abort_flag, TC_WAIT_NS)) ok = false;
+                if (ok && !mbar_wait(xfull(s), (uint32_t)(u & 1), abort_flag, TC_WAIT_NS)) ok = false;
+            } else if (!mbar_wait(hready(s), (uint32_t)((l - 1) & 1), abort_flag, TC_WAIT_NS)) {
+                ok = false;
+            }
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t dacc = tmem + (uint32_t)(s * 256);
+            const int nkb = l == 0 ? 1 : 4;
+            for (int kb = 0; kb < nkb; kb++, wk++) {
+                const int w = (int)(wk & 1);
+                if (!mbar_wait(wfull(w), (uint32_t)((wk / FM_WST) & 1), abort_flag, TC_WAIT_NS)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint64_t dA = umma_desc_sw<TC_BK>(base + s * FM_HBYTES + kb * FM_KB_BYTES);
+                const uint64_t dB = umma_desc_sw<TC_BK>(wbase + w * FM_WBYTES);
+#pragma unroll
+                for (int k16 = 0; k16 < TC_BK / 16; k16++) {
+                    const uint64_t adv = (uint64_t)((k16 * 32) >> 4);
+                    umma_bf16(dacc, dA + adv, dB + adv, idesc, (kb > 0 || k16 > 0) ? 1u : 0u);
+                }
+                umma_commit(wempty(w));
+            }
+            if (!ok) break;
+            umma_commit(accf(s));
+            if (l == 3) umma_commit(hfree(s));
+            FM_STEPS_END
+            if (!ok) {
+                atomicExch(&g_tc_error, 12);
+                *abort_flag = 1;
+            }
+            umma_commit(drain_bar);
+            (void)mbar_wait(drain_bar, 0, abort_flag, TC_WAIT_NS);
+        }
+        __syncwarp();
+    } else {
+        // ---------------- epilogue warps
+        const int q = warp & 3, h = warp >> 2;
+        const int r = q * 32 + lane;  // row within the tile (TMEM lane)
+        const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+        float sum[64];
+        bool ok = true;
+        FM_STEPS_BEGIN
+        if (!mbar_wait(accf(s), (uint32_t)(l & 1), abort_flag, TC_WAIT_NS)) {
+            ok = false;
+            break;
+        }
+        tc_fence_after();
+        const uint32_t tacc = tmem + lane_base + (uint32_t)(s * 256 + h * 64);
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) {
+            uint32_t v[16];
+            tmem_ld16(tacc + (uint32_t)(16 * jj), v);
+#pragma unroll
+            for (int i = 0; i < 16; i++) sum[16 * jj + i] = __uint_as_float(v[i]);
+        }
+        const float4 *b4 = reinterpret_cast<const float4 *>(svec + l * 256 + h * 64);
+        if (l < 3) {
+            // activations of layer l + 1: K-block h of the slot, row r, chunks swizzled
+            uint8_t *hrow = gbase + s * FM_HBYTES + h * FM_KB_BYTES + r * 128;
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const float4 ba = b4[2 * c], bb = b4[2 * c + 1];
+                const float bv[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
+                uint32_t pk[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const __nv_bfloat162 h2 = __floats2bfloat162_rn(gelu_as(fmaf(1.f, sum[8 * c + 2 * e], bv[2 * e])),
+                                                                    gelu_as(fmaf(1.f, sum[8 * c + 2 * e + 1], bv[2 * e + 1])));
+                    pk[e] = *reinterpret_cast<const uint32_t *>(&h2);
+                }
+                *reinterpret_cast<uint4 *>(hrow + ((c ^ (r & 7)) << 4)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            }
+            // the MMAs read these through the async proxy
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        } else {
+            // output layer: partial dot of the BF16-rounded activations with w5
+            const float4 *w4 = reinterpret_cast<const float4 *>(svec + 4 * 256 + h * 64);
+            float acc = 0.f;
+#pragma unroll
+            for (int c = 0; c < 64; c += 4) {
+                const float4 bv = b4[c / 4], wv = w4[c / 4];
+                const __nv_bfloat162 h01 = __floats2bfloat162_rn(gelu_as(fmaf(1.f, sum[c], bv.x)),
+                                                                 gelu_as(fmaf(1.f, sum[c + 1], bv.y)));
+                const __nv_bfloat162 h23 = __floats2bfloat162_rn(gelu_as(fmaf(1.f, sum[c + 2], bv.z)),
+                                                                 gelu_as(fmaf(1.f, sum[c + 3], bv.w)));
+                const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+                acc = fmaf(f01.x, wv.x, acc);
+                acc = fmaf(f01.y, wv.y, acc);
+                acc = fmaf(f23.x, wv.z, acc);
+                acc = fmaf(f23.y, wv.w, acc);
+            }
+            p.ypart[(long long)h * p.M + (long long)(item0 + j * istep) * TC_BM + r] = acc;
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(hready(s)) : "memory");
+        FM_STEPS_END
+        if (!ok) atomicExch(&g_tc_error, 13);
+    }
+#undef FM_STEPS_BEGIN
+#undef FM_STEPS_END
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+    }
+}
+
+// One ensemble member's inference: Xp [M x 64] padded BF16 inputs, W1 [256 x 64], WH three
+// [256 x 256] matrices back to back (BF16, K-major), vec = b1 | b2 | b3 | b4 | w5 (FP32);
+// ypart [4][M] receives the output layer's partial dots (as launch_tc_layer's fused last
+// layer writes them).  M % 128 == 0.
+int launch_mlp_fused(long long M, const __nv_bfloat16 *Xp, const __nv_bfloat16 *W1, const __nv_bfloat16 *WH,
+                     const float *vec, float *ypart, cudaStream_t s) {
+    if (M <= 0 || M % TC_BM || M / TC_BM > 0x7fffffffLL) return OPB_E_UNSUPPORTED;
+    if (!Xp || !W1 || !WH || !vec || !ypart) return OPB_E_NULL;
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, FM_SMEM);
+        if (e != cudaSuccess) return (int)e;
+        attr_set[dev] = true;
+    }
+    CUtensorMap mX, mW1, mWH;
+    int r;
+    if ((r = make_map(&mX, Xp, M, 64, 64, TC_BM)) != OPB_OK) return r;
+    if ((r = make_map(&mW1, W1, 256, 64, 64, 256)) != OPB_OK) return r;
+    if ((r = make_map(&mWH, WH, 3 * 256, 256, 256, 256)) != OPB_OK) return r;
+    FmParams p{M, vec, ypart};
+    const long long ntiles = M / TC_BM;
+    const int grid = ntiles < num_sms() ? (int)ntiles : num_sms();
+    k_mlp_fused<<<grid, FM_THREADS, FM_SMEM, s>>>(mX, mW1, mWH, p);
     return (int)cudaGetLastError();
 }
 

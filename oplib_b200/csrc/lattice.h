@@ -254,6 +254,10 @@ constexpr int TC_LAYER_CPT = 64;
 int launch_tc_layer(int M, int N, int K, const __nv_bfloat16 *A, long long lda, const __nv_bfloat16 *W,
                     long long ldw, float alpha, const float *bias, __nv_bfloat16 *H, long long ldh, cudaStream_t s,
                     const float *w5 = nullptr, float *ypart = nullptr);
+// The four hidden layers and the output layer's partial dots of one network in one kernel
+// (activations kept in shared memory); writes what the layer-by-layer launches write.
+int launch_mlp_fused(long long M, const __nv_bfloat16 *Xp, const __nv_bfloat16 *W1, const __nv_bfloat16 *WH,
+                     const float *vec, float *ypart, cudaStream_t s);
 int tc_gemm_nparts(int M, int N);             // number of row-sum partials written
 
 // Batched launches: problem descriptors and tensor maps live in device memory.

@@ -655,6 +655,10 @@ OPB_API long long opb_mlp_infer_workspace_bytes(long long n, int nmem) {
     return np * 64 * 2 + 2 * np * 256 * 2 + (long long)MLP_YPARTS * nmem * np * 4 + 1024;
 }
 
+// Inference form: 1 = one fused kernel per member (default), 0 = one launch per layer with
+// the activations through HBM.  Both give bit-identical outputs.
+static int g_mlp_fused = 1;
+
 // Ensemble inference on the tensor cores: members m = 0..nmem-1 with packed weights at
 // packed + m * member_stride bytes; X [n x 8] normalised features (FP32).  mean [n] and
 // spread [n] (optional) receive the ensemble mean and max - min of the member outputs.
@@ -679,6 +683,10 @@ OPB_API int opb_mlp_infer(const void *packed, int nmem, long long member_stride,
         const __nv_bfloat16 *W1 = reinterpret_cast<const __nv_bfloat16 *>(pk);
         const __nv_bfloat16 *WH = reinterpret_cast<const __nv_bfloat16 *>(pk + MLP_PACK_W1);
         const float *f = reinterpret_cast<const float *>(pk + MLP_PACK_W1 + 3 * MLP_PACK_WH);
+        if (g_mlp_fused) {  // all layers in one kernel, the activations in shared memory
+            MT(launch_mlp_fused(np, Xp, W1, WH, f, ym + (long long)MLP_YPARTS * m * np, s));
+            continue;
+        }
         MT(launch_tc_layer((int)np, 256, 64, Xp, 64, W1, 64, 1.f, f, Ha, 256, s));
         MT(launch_tc_layer((int)np, 256, 256, Ha, 256, WH, 256, 1.f, f + 256, Hb, 256, s));
         MT(launch_tc_layer((int)np, 256, 256, Hb, 256, WH + 65536, 256, 1.f, f + 512, Ha, 256, s));
@@ -689,4 +697,10 @@ OPB_API int opb_mlp_infer(const void *packed, int nmem, long long member_stride,
     k_mlp_ensemble<<<grid_ew(n), 256, 0, s>>>(n, np, nmem, ym, reinterpret_cast<const uint8_t *>(packed),
                                               member_stride, MLP_PACK_W1 + 3 * MLP_PACK_WH + 1280LL * 4, mean, spread);
     return launch_check();
+}
+
+OPB_API int opb_mlp_set_fused_inference(int on) {
+    OPB_REQUIRE(on == 0 || on == 1, OPB_E_ARG);
+    g_mlp_fused = on;
+    return set_status(OPB_OK);
 }

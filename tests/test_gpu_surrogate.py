@@ -93,6 +93,35 @@ def test_tensor_core_inference_matches_training_forward(cuda):
     assert (spread - ref_spread).abs().max().item() <= 0.04 * scale + 1e-6
 
 
+@pytest.mark.parametrize("n,members", [(1000, 2), (128, 1), (148 * 128 * 3 + 7, 4), (1 << 18, 3)])
+def test_fused_inference_is_bit_identical_to_the_layers(cuda, n, members):
+    """One fused kernel per member (activations in shared memory, two tiles in flight per
+    CTA) against one launch per layer: the same products, GELU and roundings, so the same
+    bits -- with an odd number of tiles per CTA, fewer tiles than SMs, and padded rows."""
+    from oplib_b200 import _lib as L
+    from oplib_b200.surrogate import RANGES, Surrogate
+    lib = L.load()
+    s = Surrogate(members=members, device=cuda)
+    for m in range(members):
+        L.call("opb_mlp_pack", s.theta[m].data_ptr(), s.packed[m * s.stride:].data_ptr())
+    rng = np.random.default_rng(n)
+    feat = torch.from_numpy(np.column_stack([rng.uniform(lo, hi, n) for lo, hi in RANGES])).to(cuda)
+    base = torch.zeros(n, dtype=torch.float64, device=cuda)
+    out = {}
+    try:
+        for fused in (1, 0):
+            assert lib.opb_mlp_set_fused_inference(fused) == 0
+            mean, spread = s.predict(feat, base)
+            torch.cuda.synchronize()
+            out[fused] = (mean.clone(), spread.clone())
+    finally:
+        assert lib.opb_mlp_set_fused_inference(1) == 0
+    assert lib.opb_tc_error() == 0
+    assert torch.isfinite(out[1][0]).all()
+    assert torch.equal(out[1][0], out[0][0])
+    assert torch.equal(out[1][1], out[0][1])
+
+
 @pytest.mark.timeout(900)
 def test_surrogate_improves_on_baseline(cuda):
     """Short training on lattice quotes: the network's error is well below the closed-form
