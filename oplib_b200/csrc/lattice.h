@@ -10,13 +10,22 @@
 namespace opb {
 
 // Two-part split of an FP32 value into 16-bit storage.  sscale == 0: BF16 parts,
-// hi = bf16(f), lo = bf16(f - hi).  sscale > 0 (a power of two): FP16 parts of f*sscale,
+// hi = bf16(f), lo = bf16(f - hi), with an absolute floor: |f| < 2^-40 gives hi = lo = 0
+// and |f| < 2^-30 gives lo = 0 (BF16 keeps FP32's exponent range, so without the floor the
+// far tails of a transition matrix, 1e-38 .. 1e-9, stay live bit patterns; FP16 parts of
+// 2^15-scaled values drop them by underflow).  The floor moves an entry by at most 2^-40,
+// or by its lo part, below 2^-39, so a product row over d <= 32768 entries of size <= 1 moves
+// by under 2^-24 / 2^-25 in the worst case, and by far less when the
+// discarded parts carry random signs.  sscale > 0 (a power of two): FP16 parts of f*sscale,
 // hi = fp16(f*s), lo = fp16(f*s - hi) -- 11 + 11 significant bits instead of 8 + 8; the
 // GEMM removes the scale through alpha.  The differences are exact in FP32.
+constexpr float kSplitZeroBelow = 0x1p-40f, kSplitNoLoBelow = 0x1p-30f;
+
 __device__ __forceinline__ void split2(float f, __nv_bfloat16 &hi, __nv_bfloat16 &lo, float sscale = 0.f) {
     if (sscale == 0.f) {
-        hi = __float2bfloat16_rn(f);
-        lo = __float2bfloat16_rn(f - __bfloat162float(hi));
+        const float a = fabsf(f);
+        hi = __float2bfloat16_rn(a < kSplitZeroBelow ? 0.f : f);
+        lo = __float2bfloat16_rn(a < kSplitNoLoBelow ? 0.f : f - __bfloat162float(hi));
     } else {
         const float fs = f * sscale;
         const __half h = __float2half_rn(fs);
@@ -34,9 +43,12 @@ __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 a, __nv_bfloat16 b) 
 // half): the same parts as split2 on each.
 __device__ __forceinline__ void split2x2(float a, float b, uint32_t &hi, uint32_t &lo, float sscale = 0.f) {
     if (sscale == 0.f) {
-        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        const float aa = fabsf(a), ab = fabsf(b);
+        const __nv_bfloat162 h =
+            __floats2bfloat162_rn(aa < kSplitZeroBelow ? 0.f : a, ab < kSplitZeroBelow ? 0.f : b);
         const float2 hf = __bfloat1622float2(h);
-        const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+        const __nv_bfloat162 l =
+            __floats2bfloat162_rn(aa < kSplitNoLoBelow ? 0.f : a - hf.x, ab < kSplitNoLoBelow ? 0.f : b - hf.y);
         hi = *reinterpret_cast<const uint32_t *>(&h);
         lo = *reinterpret_cast<const uint32_t *>(&l);
     } else {

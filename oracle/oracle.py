@@ -868,7 +868,10 @@ def bf16_round(a: np.ndarray) -> np.ndarray:
 
 
 def split_bf16(a: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """The library's BF16 two-part split: hi = bf16(a), lo = bf16(a - hi), with its absolute
+    floor (|a| < 2^-40: both parts zero; |a| < 2^-30: no lo part)."""
     a32 = np.asarray(a, dtype=np.float32)
-    hi = bf16_round(a32)
-    lo = bf16_round((a32 - hi).astype(np.float32))
+    mag = np.abs(a32)
+    hi = bf16_round(np.where(mag < np.float32(2.0 ** -40), np.float32(0), a32))
+    lo = bf16_round(np.where(mag < np.float32(2.0 ** -30), np.float32(0), (a32 - hi).astype(np.float32)))
     return hi, lo

@@ -179,8 +179,9 @@ def test_renorm_rows_bit_exact(cuda, mode, f16):
         lo = (rs - hi.float()).to(torch.float16)
         hi, lo = hi.view(torch.int16), lo.view(torch.int16)
     else:
-        hi = r.to(torch.bfloat16)
-        lo = (r - hi.float()).to(torch.bfloat16)
+        # BF16 parts with the split's absolute floor: |x| < 2^-40 -> 0, |x| < 2^-30 -> no lo part
+        hi = torch.where(r.abs() < 2.0 ** -40, 0.0, r).to(torch.bfloat16)
+        lo = torch.where(r.abs() < 2.0 ** -30, 0.0, r - hi.float()).to(torch.bfloat16)
         hi, lo = hi.view(torch.int16), lo.view(torch.int16)
     g = [t.view(torch.int16).cpu() for t in parts]
     assert torch.equal(g[0], hi) and torch.equal(g[1], lo)
