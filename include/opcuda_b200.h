@@ -287,8 +287,10 @@ int opb_set_band_skip(int on);
  * renormalisation kernel runs between products (squarings: the next level applies
  * D [E'.E' - S E' - E' S + S^2] + 2 D (E' - S) with D = diag(1/(1+s)), S = diag(s), the D
  * between the factors left out; chain products: the row scaling, exact).  The batched
- * sweep always does; a single-lattice solve does up to max_d states (default 0: a
- * renormalisation kernel after every product, which costs about the same for one lattice). */
+ * sweep always does; a single-lattice solve does up to max_d states (max_d >= 0; 0: a
+ * renormalisation kernel after every product).  max_d = -1 restores the default: lattices of
+ * 4096 states or more fuse, smaller ones run the kernel, which is the faster form where one
+ * wave of tiles leaves the longer fused output phase nothing to hide behind. */
 int opb_set_fused_normalisation(int max_d);
 
 /* ------------------------------------------------------------------ batched lattices */

@@ -233,9 +233,9 @@ int square_tc(const opb_lattice_desc &L, Bufs &b, cudaStream_t s, bool f16, opb:
     // epilogue (OPB_FIX_SQUARE).  A level skips the output tiles that no K-block reaches,
     // so its part buffer must be zero there: A holds E0's parts (zero outside the band) and
     // B starts zeroed; the band only grows, so the tiles a level skips are zero in both.
-    // (lattices above g_fused_max_d states: a renormalisation kernel after every level, which
-    // writes the next level's parts; its traffic is small against a squaring's there)
-    const bool fused = d <= opb::g_fused_max_d;
+    // (lattices not fused, opb::fused_single: a renormalisation kernel after every level,
+    // which writes the next level's parts)
+    const bool fused = opb::fused_single(d);
     if (fused && L.niter > 1) {
         LT((int)cudaMemsetAsync(b.Bhi, 0, sizeof(__nv_bfloat16) * (size_t)d * d, s));
         LT((int)cudaMemsetAsync(b.Blo, 0, sizeof(__nv_bfloat16) * (size_t)d * d, s));
@@ -314,9 +314,9 @@ int solve_tc(const opb_lattice_desc &L, Bufs &b, double *quotes, double *V_all, 
     // part buffers and a second pair carved from the FP32 chain buffer (unused in the split
     // modes); each output's row normalisation is deferred into the next chain product's
     // epilogue and into its own pricing's discount (row scaling commutes with the products).
-    // (above g_fused_max_d states: FP32 chain products renormalised by a kernel that writes the
+    // (lattices not fused: FP32 chain products renormalised by a kernel that writes the
     // parts into A, as the squarings are)
-    const bool fused = d <= opb::g_fused_max_d;
+    const bool fused = opb::fused_single(d);
     const size_t dd = (size_t)d * d;
     __nv_bfloat16 *ch_hi[2] = {b.Ahi, reinterpret_cast<__nv_bfloat16 *>(b.Pa)};
     __nv_bfloat16 *ch_lo[2] = {b.Alo, reinterpret_cast<__nv_bfloat16 *>(b.Pa) + dd};
@@ -434,15 +434,17 @@ int prepare_padded(const opb_lattice_desc &L, int mode, Bufs &b, opb_lattice_des
 namespace opb {
 int g_lolo_levels = OPB_LOLO_LEVELS;
 int g_band_skip = 1;
-int g_fused_max_d = OPB_FUSED_MAX_D;
+int g_fused_max_d = -1;
 }  // namespace opb
 
-// Tuning knob: the largest lattice (states) whose single-lattice solve defers each product's
-// row normalisation into the next product's epilogue, which also writes the next operand's
-// parts (no renormalisation kernel between products); larger lattices renormalise with a
-// kernel after every product.  0 = never; default OPB_FUSED_MAX_D.
+// Tuning knob: max_d >= 0 makes single-lattice solves of at most max_d states defer each
+// product's row normalisation into the next product's epilogue, which also writes the next
+// operand's parts (no renormalisation kernel between products), and larger ones renormalise
+// with a kernel after every product (0: every size uses the kernel).  max_d = -1 restores
+// the default: lattices of OPB_FUSED_AUTO_MIN_D states or more fuse, smaller ones use the
+// kernel.
 OPB_API int opb_set_fused_normalisation(int max_d) {
-    OPB_REQUIRE(max_d >= 0, OPB_E_ARG);
+    OPB_REQUIRE(max_d >= -1, OPB_E_ARG);
     opb::g_fused_max_d = max_d;
     return opb::set_status(OPB_OK);
 }

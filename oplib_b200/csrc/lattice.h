@@ -245,16 +245,20 @@ constexpr int OPB_LOLO_LEVELS = 8;
 // knobs shared by the single and batched solves (opb_set_lolo_levels, opb_set_band_skip)
 extern int g_lolo_levels;  // leading squaring levels with the lo.lo product (BF16 parts)
 extern int g_band_skip;    // 1: squarings leave out the K-blocks outside the operands' band
-// The single-lattice solve fuses the row normalisation into the products' epilogues (which
-// then also write the next operand's parts) up to this many states; 0 by default.  A fused
-// epilogue lengthens each tile's output phase, which sits on the tile's critical path,
-// about as much as the renormalisation kernel it replaces costs at these sizes: measured
-// whole solves (SV lattices, CUDA-graph replay) 26.20 against 26.34 ms at d = 6144, 9.02
-// against 9.06 ms at 4096, and 2.38 against 2.25 ms at 2048, where a one-wave product has
-// no later tile to hide the longer output phase behind.  The batched sweep, where the
-// renormalisation of hundreds of small lattices took 19% of the time, always fuses.
-constexpr int OPB_FUSED_MAX_D = 0;
-extern int g_fused_max_d;  // opb_set_fused_normalisation
+// Whether the single-lattice solve fuses the row normalisation into the products'
+// epilogues (which then also write the next operand's parts) or runs a renormalisation
+// kernel after every product.  By default (g_fused_max_d < 0) lattices of at least
+// OPB_FUSED_AUTO_MIN_D states fuse; opb_set_fused_normalisation(max_d >= 0) fuses exactly
+// the lattices of at most max_d states (0: none).  A fused epilogue lengthens each tile's
+// output phase, which sits on the tile's critical path: a one-wave product has no later
+// tile to hide it behind (d = 2048: 2.38 ms fused against 2.25 with the kernel), while on
+// larger lattices it costs less than the kernel's pass over the matrix (SV solves, CUDA-graph
+// replay: 9.02 against 9.06 ms at d = 4096; 24.13 against 24.58 ms at d = 6144, alternated
+// three times in one run).  The batched sweep, where the renormalisation of hundreds of
+// small lattices took 19% of the time, always fuses.
+constexpr int OPB_FUSED_AUTO_MIN_D = 4096;
+extern int g_fused_max_d;  // opb_set_fused_normalisation; < 0: automatic
+inline bool fused_single(int d) { return g_fused_max_d < 0 ? d >= OPB_FUSED_AUTO_MIN_D : d <= g_fused_max_d; }
 // K-slices that fill the GPU with the tiles of a small-N product (1 = none), at most 4
 int tc_gemm_split_for(int M, int N, int K);
 int tc_gemm_tile_n(int N);                    // tile width chosen for N (0 if unsupported)

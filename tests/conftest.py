@@ -70,9 +70,9 @@ def cuda():
 def fused_single(cuda):
     """Single-lattice solves with the row normalisation fused into the products' epilogues,
     as the batched sweep runs it (for batch-against-single comparisons); restores the
-    default (a renormalisation kernel) afterwards."""
+    default (fused from 4096 states, a renormalisation kernel below) afterwards."""
     from oplib_b200 import _lib
     lib = _lib.load()
     assert lib.opb_set_fused_normalisation(1 << 30) == 0
     yield
-    assert lib.opb_set_fused_normalisation(0) == 0
+    assert lib.opb_set_fused_normalisation(-1) == 0

@@ -115,6 +115,7 @@ def test_version_and_status_strings(lib):
     (lambda L: L.opb_lv_generator_ell(2, 1, 1, 1, 1, 1), -1),
     (lambda L: L.opcuda_sgemv(4, 4, 1.0, 0, 4, 1, 1, 0.0, 1, 1), -2),
     (lambda L: L.opcuda_sdot2(0, 1, 1, 4, 4), -2),
+    (lambda L: L.opb_set_fused_normalisation(-2), -1),  # -1 (automatic) is the lowest value
 ])
 def test_host_argument_errors(lib, call, expect):
     assert call(lib) == expect
@@ -186,3 +187,9 @@ def test_injected_alloc_failure(lib):
     assert lib.opb_test_fail_next_alloc(1) == 0
     assert lib.opcuda_mem_alloc(1024) == 0
     assert lib.opcuda_get_status() == -5
+
+
+def test_fused_normalisation_knob_values(lib):
+    """-1 restores the automatic rule, 0 and above set a size limit; neither needs a device."""
+    for v in (0, 8192, -1):
+        assert lib.opb_set_fused_normalisation(v) == 0

@@ -31,7 +31,7 @@ def knobs(cuda):
     yield lib
     assert lib.opb_set_band_skip(1) == 0
     assert lib.opb_set_lolo_levels(8) == 0
-    assert lib.opb_set_fused_normalisation(0) == 0
+    assert lib.opb_set_fused_normalisation(-1) == 0
 
 
 def _equal(a, b):
@@ -122,7 +122,7 @@ def test_sweep_extremes_within_1e5(knobs, sweep_extremes):
         # normalisation, so that the two differ only by the pricing's K-slices)
         assert knobs.opb_set_fused_normalisation(8192) == 0
         qs, _ = lats[0].solve(STRIKES, NMAT, PERIOD, DT0, mode=mode)
-        assert knobs.opb_set_fused_normalisation(0) == 0
+        assert knobs.opb_set_fused_normalisation(-1) == 0
         assert np.abs(qs.cpu().numpy() - q[0]).max() < 1e-6
     from oplib_b200 import _lib
     assert _lib.load().opb_tc_error() == 0

@@ -57,7 +57,7 @@ def test_batch_vs_fp64_and_single(batch_and_refs):
             qs, _ = lat.solve(STRIKES, NMAT, PERIOD, DT0, mode="bf16x3")
             assert np.abs(q[i] - qs.cpu().numpy()).max() < 1e-6
     finally:
-        assert lib.opb_set_fused_normalisation(0) == 0
+        assert lib.opb_set_fused_normalisation(-1) == 0
 
 
 def test_batch_configs_agree(batch_and_refs):

@@ -24,7 +24,7 @@ def knob(cuda):
     from oplib_b200 import _lib
     lib = _lib.load()
     yield lib
-    assert lib.opb_set_fused_normalisation(0) == 0  # the default
+    assert lib.opb_set_fused_normalisation(-1) == 0  # the default
 
 
 def _lv_ref(n, nmat, dt0, **p):
