@@ -278,3 +278,23 @@ def test_mc_cashflow_values_by_hand():
     ko = np.zeros((3, 3), dtype=np.uint8)
     ko[1, 1] = 1
     assert np.array_equal(O.mc_cashflow_values(paths, cf, ko), [1.0, 2.0])
+
+
+def test_split_bf16_floor():
+    """The library's BF16 split, restated: hi = bf16(a), lo = bf16(a - hi), except that an
+    entry below 2^-40 in magnitude has no parts and one below 2^-30 has no lo part."""
+    third = np.float32(1.0 / 3.0)
+    a = np.array([third, -third, 2.0 ** -41, -(2.0 ** -41), 1.7 * 2.0 ** -31, 1.7 * 2.0 ** -29, 0.0],
+                 dtype=np.float32)
+    hi, lo = O.split_bf16(a)
+    assert hi[0] == np.float32(0.333984375) and lo[0] == O.bf16_round(np.float32(third - np.float32(0.333984375)))
+    assert hi[1] == -hi[0] and lo[1] == -lo[0]
+    assert hi[2] == 0 and lo[2] == 0 and hi[3] == 0 and lo[3] == 0
+    assert hi[4] == O.bf16_round(a[4:5])[0] and hi[4] != 0 and lo[4] == 0  # below 2^-30: hi only
+    assert lo[5] == O.bf16_round(np.float32(a[5] - hi[5]))                # above: both parts
+    assert lo[5] != 0
+    assert hi[6] == 0 and lo[6] == 0
+    # hi + lo carries 16 significant bits wherever the floor does not apply
+    big = np.abs(a) >= 2.0 ** -30
+    assert np.all(np.abs((hi + lo).astype(np.float64) - a.astype(np.float64))[big]
+                  <= 2.0 ** -16 * np.abs(a[big]).astype(np.float64))
