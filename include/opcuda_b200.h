@@ -216,7 +216,9 @@ int opb_gemm_f16x3_kn(int M, int N, int K, const uint16_t *Ahi, const uint16_t *
 /* new: FP64 row renormalisation of a source-major d x d FP32 matrix from row-sum partials
  * partial[p*d + y] (p < nparts), with optional 16-bit splits (A row-major, B transposed);
  * mode 0 E-form, 1 E-form in / P-form out, 2 P-form (no B); f16: FP16 parts of 2^15-scaled
- * values instead of BF16; d % 64 == 0 (probability conservation, no reference counterpart) */
+ * values instead of BF16; d % 64 == 0 (probability conservation, no reference counterpart).
+ * BF16 parts: hi = bf16(x), lo = bf16(x - hi), except that |x| < 2^-40 gives no parts and
+ * |x| < 2^-30 no lo part (the split every solve uses) */
 int opb_renorm_rows(int d, float *X, const double *partial, int nparts, int mode, void *Ahi, void *Alo, void *Bhi,
                     void *Blo, int f16);
 /* reads and clears the device error word of the tensor-core kernels (0 = none) */
